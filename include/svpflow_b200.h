@@ -1,0 +1,116 @@
+/*
+ * svpflow_b200.h -- C ABI of the B200 motion-analysis library (libsvpflow_b200.so).
+ *
+ * Drop-in for open-svpflow's svpflow1 motion-analysis path: the Super pyramid builder
+ * and the Analyse block search, computed on an NVIDIA B200 (sm_100a), byte-identical to
+ * the reference's CPU output. Plain pointers and sizes only. Each entry point names the
+ * reference interface it replaces (paths inside the reference project).
+ *
+ * Buffers
+ *   source frame  packed I420/YUV420P8: Y (w*h) | U (w/2*h/2) | V (w/2*h/2)
+ *   super frame   Y (w * H) | U (w/2 * H/2) | V (w/2 * H/2), H = svpf_super_height();
+ *                 the layout of crates/svpflow1/src/portable.rs:104-106 (SuperFrame::bytes)
+ *   payload       the Analyse output frame row: crates/svpflow1/src/analyse_search.rs:2740-2811
+ * Functions returning int return 0 on success, else a negative code; the message is in
+ * svpf_last_error() (thread-local). Handles are immutable after creation; the host-buffer
+ * entry points of one analyser serialise on an internal lock, the device entry points
+ * take caller-owned buffers and a cudaStream_t (passed as void*) and never allocate.
+ */
+#ifndef SVPFLOW_B200_H
+#define SVPFLOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct svpf_super svpf_super;
+typedef struct svpf_analyser svpf_analyser;
+
+#define SVPF_OK 0
+#define SVPF_EINVAL (-1)   /* bad argument or option (message as the reference's setError text) */
+#define SVPF_ECUDA (-2)    /* CUDA runtime error or no usable device */
+#define SVPF_EPANIC (-3)   /* input on which the reference indexes out of range (it would panic) */
+#define SVPF_EUNSUP (-4)   /* option combination not available on the device path */
+
+/* Thread-local text of the last error. */
+const char *svpf_last_error(void);
+/* Library version of the reference plugin this replaces: svpGetVersion(),
+ * crates/svpflow1/src/abi.rs:3-9 (1174405393). */
+int64_t svpf_reference_version(void);
+
+/* ---------------------------------------------------------------- Super */
+/* Super filter creation: SuperOpts::from_opt + pack_data + super_height
+ * (crates/svpflow1/src/super_opts.rs:17-95, super_filter.rs:67-82). `opt` is the
+ * VapourSynth `opt:data` string (lenient JSON, crates/svpflow-core/src/params.rs);
+ * NULL or an unparsable string means defaults, as in super_filter.rs:107-121. */
+int svpf_super_create(int32_t width, int32_t height, const char *opt, size_t opt_len, svpf_super **out);
+/* SuperBuilder::new(width, height, pel) (crates/svpflow1/src/portable.rs:30-62). */
+int svpf_super_create_portable(int32_t width, int32_t height, int32_t pel, svpf_super **out);
+void svpf_super_destroy(svpf_super *s);
+int64_t svpf_super_sdata(const svpf_super *s);       /* SuperOpts::pack_data, super_opts.rs:51-63 */
+int32_t svpf_super_height(const svpf_super *s);      /* SuperOpts::super_height, super_opts.rs:65-67 */
+int32_t svpf_super_levels(const svpf_super *s);      /* SuperBuilder::levels, portable.rs:79-82 */
+int32_t svpf_super_pel(const svpf_super *s);
+size_t svpf_super_source_len(const svpf_super *s);   /* SuperBuilder::source_len, portable.rs:84-87 */
+size_t svpf_super_output_len(const svpf_super *s);   /* SuperBuilder::output_len, portable.rs:89-92 */
+/* SuperBuilder::build (portable.rs:94-148) / get_frame_super (super_filter.rs:143-268)
+ * over nframes frames, host buffers in and out. */
+int svpf_super_build(const svpf_super *s, const uint8_t *src, uint8_t *dst, int32_t nframes);
+/* Same on device buffers: nframes source frames at `src_pitch`-strided planes
+ * (src_y_stride / src_c_stride bytes per row; 0 = packed) -> nframes super frames. */
+int svpf_super_build_device(const svpf_super *s, const uint8_t *src_dev, int64_t src_y_stride,
+                            int64_t src_c_stride, uint8_t *dst_dev, int32_t nframes, void *stream);
+
+/* ---------------------------------------------------------------- Analyse */
+/* Analyse filter creation: AnalyseOpts::from_opt with the super clip's `sdata`
+ * (crates/svpflow1/src/analyse_opts.rs:45-219, analyse_filter.rs:84-101); src_width /
+ * src_height (> 0) override the frame size as analyse_filter.rs:96-101 does. */
+int svpf_analyser_create(int64_t sdata, const char *opt, size_t opt_len, int32_t src_width,
+                         int32_t src_height, svpf_analyser **out);
+/* Analyser::new(super_builder, block w, block h, overlap mode, vectors)
+ * (crates/svpflow1/src/portable.rs:189-229). */
+int svpf_analyser_create_portable(const svpf_super *s, int32_t block_w, int32_t block_h,
+                                  int32_t overlap_mode, int32_t vectors, svpf_analyser **out);
+void svpf_analyser_destroy(svpf_analyser *a);
+/* The 16-int vector header whose address the reference publishes as `vdata`
+ * (pack_vdata_header, analyse_search.rs:2813-2841; Analyser::vector_header,
+ * portable.rs:231-234). Valid for the analyser's lifetime. */
+const int32_t *svpf_analyser_vdata(const svpf_analyser *a);
+/* Bytes of one Analyse output frame (analyse_filter.rs:122-129). */
+size_t svpf_analyser_payload_len(const svpf_analyser *a);
+int32_t svpf_analyser_delta(const svpf_analyser *a);
+/* Device scratch the *_device entry points need for `npairs` concurrent pairs. */
+size_t svpf_analyser_scratch_bytes(const svpf_analyser *a, int32_t npairs);
+/* Analyser::analyse(current, reference) (portable.rs:236-250) on host super frames. */
+int svpf_analyse(svpf_analyser *a, const uint8_t *cur_super, const uint8_t *ref_super, uint8_t *payload);
+/* analyse_pair + pack_vector_frame for npairs pairs of device super frames:
+ * cur_dev[i] / ref_dev[i] are device pointers (host arrays of them), payloads_dev holds
+ * npairs * payload_len bytes, scratch_dev svpf_analyser_scratch_bytes(npairs). */
+int svpf_analyse_pairs_device(const svpf_analyser *a, const uint8_t *const *cur_dev,
+                              const uint8_t *const *ref_dev, int32_t npairs, uint8_t *payloads_dev,
+                              void *scratch_dev, void *stream);
+/* A clip as the VapourSynth Analyse filter sees it: output frame n pairs super frame n
+ * with super frame min(n + delta, nframes - 1) (analyse_filter.rs:240-282). Frames
+ * [first, first + count) of `supers_dev` (nframes contiguous super frames) -> payloads. */
+int svpf_clip_analyse_device(const svpf_analyser *a, const uint8_t *supers_dev, int32_t nframes,
+                             int32_t first, int32_t count, uint8_t *payloads_dev, void *scratch_dev,
+                             void *stream);
+/* Status of the last device launch that used `scratch_dev` (synchronises `stream`):
+ * SVPF_OK, or SVPF_EPANIC when a pair hit an input the reference cannot process. */
+int svpf_device_status(const void *scratch_dev, void *stream);
+/* Whole clip from host source frames: Super over every frame, then Analyse for output
+ * frames [first, first + count); payloads = count * payload_len host bytes. */
+int svpf_clip_analyse(svpf_analyser *a, const svpf_super *s, const uint8_t *frames, int32_t nframes,
+                      int32_t first, int32_t count, uint8_t *payloads);
+
+/* Number of kernels this thread launched through the library since the last reset. */
+int64_t svpf_kernel_launches(void);
+void svpf_kernel_launches_reset(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

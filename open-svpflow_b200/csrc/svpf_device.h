@@ -1,0 +1,46 @@
+// svpf_device.h -- launch-side declarations shared by the CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "svpf_internal.h"
+
+namespace svpf {
+
+// Everything the Super kernels need about one (options, layout, source pitch) triple.
+struct SuperDev {
+    int32_t width, height, pel, levels, full, gpu, scale_up, scale_down;
+    int64_t y_stride, c_stride, y_rows, c_rows, y_len, c_len, frame_bytes;
+    int64_t src_y_stride, src_c_stride, src_y_len, src_c_len, src_frame_bytes;
+    int32_t lw[kMaxLevels], lh[kMaxLevels];   // reduce_dim(luma_w/h, level)
+    int64_t row_y[kMaxLevels], row_c[kMaxLevels];  // first row of each level in Y / chroma
+};
+
+bool make_super_dev(const SuperOpts &so, const SuperLayout &L, int64_t src_y_stride, int64_t src_c_stride,
+                    SuperDev &D);
+// src: nframes source frames (Y|U|V at src pitches, src_frame_bytes apart);
+// dst: nframes super frames (frame_bytes apart). Adds its kernel launches to *launches.
+cudaError_t launch_super(const SuperDev &D, const uint8_t *src, uint8_t *dst, int nframes, cudaStream_t stream,
+                         int *launches);
+
+// One frame pair of an Analyse launch: super frames of the current and reference frame.
+struct PairRef {
+    const uint8_t *cur;
+    const uint8_t *ref;
+};
+
+// Where the pairs of a launch come from: an explicit device table, or a clip of
+// contiguous super frames where pair b is (first + b, min(first + b + delta, nframes - 1)).
+struct PairSrc {
+    const PairRef *table;
+    const uint8_t *clip;
+    int64_t frame_bytes;
+    int32_t first, nframes, delta;
+};
+
+// Analyse over npairs pairs; payloads npairs x P.payload_len bytes, scratch npairs x
+// P.scratch_per_pair bytes, status one int (0 = ok), cleared by the caller.
+cudaError_t launch_analyse(const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,
+                           uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches);
+
+}  // namespace svpf

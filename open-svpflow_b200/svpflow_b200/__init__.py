@@ -1,0 +1,276 @@
+"""svpflow_b200 -- host-side mirror of open-svpflow's motion-analysis interface.
+
+Python face of libsvpflow_b200.so (the C ABI in include/svpflow_b200.h). Names and
+argument meanings follow the reference:
+
+  SuperBuilder / SuperFrame / Analyser   crates/svpflow1/src/portable.rs:8-251
+  Super(width, height, opt)              the `svp1.Super` filter, super_filter.rs:9-105
+  Analyse(sdata, opt, width, height)     the `svp1.Analyse` filter, analyse_filter.rs:29-171
+
+Errors raise ValueError with the reference's message text. Everything computes on the
+GPU; without a usable CUDA device or without the compiled library the calls fail
+loudly -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+__all__ = ["SuperBuilder", "SuperFrame", "Analyser", "Super", "Analyse", "lib", "LIB_PATH", "SvpfError",
+           "REFERENCE_VERSION"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libsvpflow_b200.so")
+REFERENCE_VERSION = 1_174_405_393  # svpGetVersion, crates/svpflow1/src/abi.rs:3
+
+SVPF_OK, SVPF_EINVAL, SVPF_ECUDA, SVPF_EPANIC, SVPF_EUNSUP = 0, -1, -2, -3, -4
+
+
+class SvpfError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+_lib = None
+_VP = ctypes.c_void_p
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is not built: run `python __graft_entry__.py` (build()) first")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I32, I64, SZ = ctypes.POINTER, ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t
+        sig = {
+            "svpf_last_error": (ctypes.c_char_p, []),
+            "svpf_reference_version": (I64, []),
+            "svpf_super_create": (I32, [I32, I32, ctypes.c_char_p, SZ, P(_VP)]),
+            "svpf_super_create_portable": (I32, [I32, I32, I32, P(_VP)]),
+            "svpf_super_destroy": (None, [_VP]),
+            "svpf_super_sdata": (I64, [_VP]),
+            "svpf_super_height": (I32, [_VP]),
+            "svpf_super_levels": (I32, [_VP]),
+            "svpf_super_pel": (I32, [_VP]),
+            "svpf_super_source_len": (SZ, [_VP]),
+            "svpf_super_output_len": (SZ, [_VP]),
+            "svpf_super_build": (I32, [_VP, _VP, _VP, I32]),
+            "svpf_super_build_device": (I32, [_VP, _VP, I64, I64, _VP, I32, _VP]),
+            "svpf_analyser_create": (I32, [I64, ctypes.c_char_p, SZ, I32, I32, P(_VP)]),
+            "svpf_analyser_create_portable": (I32, [_VP, I32, I32, I32, I32, P(_VP)]),
+            "svpf_analyser_destroy": (None, [_VP]),
+            "svpf_analyser_vdata": (P(I32), [_VP]),
+            "svpf_analyser_payload_len": (SZ, [_VP]),
+            "svpf_analyser_delta": (I32, [_VP]),
+            "svpf_analyser_scratch_bytes": (SZ, [_VP, I32]),
+            "svpf_analyse": (I32, [_VP, _VP, _VP, _VP]),
+            "svpf_analyse_pairs_device": (I32, [_VP, P(_VP), P(_VP), I32, _VP, _VP, _VP]),
+            "svpf_clip_analyse_device": (I32, [_VP, _VP, I32, I32, I32, _VP, _VP, _VP]),
+            "svpf_device_status": (I32, [_VP, _VP]),
+            "svpf_clip_analyse": (I32, [_VP, _VP, _VP, I32, I32, I32, _VP]),
+            "svpf_kernel_launches": (I64, []),
+            "svpf_kernel_launches_reset": (None, []),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != SVPF_OK:
+        msg = lib().svpf_last_error().decode(errors="replace")
+        if rc == SVPF_EINVAL:
+            raise ValueError(msg)
+        raise SvpfError(rc, msg)
+
+
+def _buf(a) -> np.ndarray:
+    if isinstance(a, (bytes, bytearray, memoryview)):
+        return np.frombuffer(a, dtype=np.uint8)
+    return np.ascontiguousarray(a, dtype=np.uint8)
+
+
+class SuperFrame:
+    """A super frame in the portable layout (portable.rs:151-186)."""
+
+    def __init__(self, builder: "SuperBuilder", data: np.ndarray):
+        self.builder = builder
+        self.data = data
+
+    def bytes(self) -> bytes:
+        return self.data.tobytes()
+
+    def __len__(self) -> int:
+        return int(self.data.size)
+
+
+class SuperBuilder:
+    """SuperBuilder::new(width, height, pel) (portable.rs:29-62); Super(...) for the filter form."""
+
+    def __init__(self, width: int, height: int, pel: int = 2, *, _handle=None):
+        h = _VP()
+        if _handle is None:
+            _check(lib().svpf_super_create_portable(width, height, pel, ctypes.byref(h)))
+        else:
+            h = _handle
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.svpf_super_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def levels(self) -> int:
+        return lib().svpf_super_levels(self._h)
+
+    @property
+    def pel(self) -> int:
+        return lib().svpf_super_pel(self._h)
+
+    @property
+    def sdata(self) -> int:
+        """The `data` int the Super filter publishes (SuperOpts::pack_data)."""
+        return lib().svpf_super_sdata(self._h)
+
+    @property
+    def super_height(self) -> int:
+        return lib().svpf_super_height(self._h)
+
+    def source_len(self) -> int:
+        return lib().svpf_super_source_len(self._h)
+
+    def output_len(self) -> int:
+        return lib().svpf_super_output_len(self._h)
+
+    def build(self, source) -> SuperFrame:
+        """SuperBuilder::build: one packed I420 frame -> its super frame."""
+        src = _buf(source)
+        if src.size != self.source_len():
+            raise ValueError("invalid source buffer length")
+        out = np.empty(self.output_len(), dtype=np.uint8)
+        _check(lib().svpf_super_build(self._h, src.ctypes.data, out.ctypes.data, 1))
+        return SuperFrame(self, out)
+
+    def build_many(self, frames: np.ndarray) -> np.ndarray:
+        frames = np.ascontiguousarray(frames, dtype=np.uint8)
+        n = frames.shape[0]
+        out = np.empty((n, self.output_len()), dtype=np.uint8)
+        _check(lib().svpf_super_build(self._h, frames.ctypes.data, out.ctypes.data, n))
+        return out
+
+    def build_device(self, src_ptr: int, dst_ptr: int, nframes: int, stream: int = 0,
+                     src_y_stride: int = 0, src_c_stride: int = 0):
+        """Device buffers (e.g. torch tensors' data_ptr()) on `stream`; no allocation."""
+        _check(lib().svpf_super_build_device(self._h, src_ptr, src_y_stride, src_c_stride, dst_ptr, nframes, stream))
+
+
+def Super(width: int, height: int, opt: Optional[str] = None) -> SuperBuilder:
+    """The `svp1.Super(clip, opt)` filter's configuration for a clip of this size."""
+    h = _VP()
+    b = opt.encode() if opt is not None else None
+    _check(lib().svpf_super_create(width, height, b, len(b) if b else 0, ctypes.byref(h)))
+    return SuperBuilder(0, 0, _handle=h)
+
+
+class Analyser:
+    """Analyser::new(super_builder, block w, block h, overlap mode, vectors) (portable.rs:188-250);
+    Analyse(...) for the filter form."""
+
+    def __init__(self, super_builder: Optional[SuperBuilder] = None, block_width: int = 16, block_height: int = 16,
+                 overlap_mode: int = 2, vectors: int = 3, *, _handle=None):
+        h = _VP()
+        if _handle is None:
+            _check(lib().svpf_analyser_create_portable(super_builder.handle, block_width, block_height, overlap_mode,
+                                                        vectors, ctypes.byref(h)))
+        else:
+            h = _handle
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.svpf_analyser_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def vector_header(self) -> list:
+        """The `vdata` header (pack_vdata_header)."""
+        p = lib().svpf_analyser_vdata(self._h)
+        return [p[i] for i in range(16)]
+
+    def payload_len(self) -> int:
+        return lib().svpf_analyser_payload_len(self._h)
+
+    @property
+    def delta(self) -> int:
+        return lib().svpf_analyser_delta(self._h)
+
+    def scratch_bytes(self, npairs: int) -> int:
+        return lib().svpf_analyser_scratch_bytes(self._h, npairs)
+
+    def analyse(self, current, reference) -> bytes:
+        """Analyser::analyse(current, reference) -> the Analyse output frame bytes."""
+        cur = _buf(current.data if isinstance(current, SuperFrame) else current)
+        ref = _buf(reference.data if isinstance(reference, SuperFrame) else reference)
+        out = np.empty(self.payload_len(), dtype=np.uint8)
+        _check(lib().svpf_analyse(self._h, cur.ctypes.data, ref.ctypes.data, out.ctypes.data))
+        return out.tobytes()
+
+    def analyse_clip(self, super_builder: SuperBuilder, frames: np.ndarray, first: int = 0,
+                     count: Optional[int] = None) -> np.ndarray:
+        """Super + Analyse over a clip of packed I420 frames (host buffers) -> payload rows."""
+        frames = np.ascontiguousarray(frames, dtype=np.uint8)
+        n = frames.shape[0]
+        count = n - first if count is None else count
+        out = np.empty((count, self.payload_len()), dtype=np.uint8)
+        _check(lib().svpf_clip_analyse(self._h, super_builder.handle, frames.ctypes.data, n, first, count,
+                                       out.ctypes.data))
+        return out
+
+    def analyse_clip_device(self, supers_ptr: int, nframes: int, first: int, count: int, payloads_ptr: int,
+                            scratch_ptr: int, stream: int = 0):
+        """Device-resident clip of super frames -> payloads; caller-owned buffers, no allocation."""
+        _check(lib().svpf_clip_analyse_device(self._h, supers_ptr, nframes, first, count, payloads_ptr, scratch_ptr,
+                                              stream))
+
+    def analyse_pairs_device(self, cur_ptrs: Sequence[int], ref_ptrs: Sequence[int], payloads_ptr: int,
+                             scratch_ptr: int, stream: int = 0):
+        n = len(cur_ptrs)
+        c = (_VP * n)(*cur_ptrs)
+        r = (_VP * n)(*ref_ptrs)
+        _check(lib().svpf_analyse_pairs_device(self._h, c, r, n, payloads_ptr, scratch_ptr, stream))
+
+    @staticmethod
+    def device_status(scratch_ptr: int, stream: int = 0):
+        _check(lib().svpf_device_status(scratch_ptr, stream))
+
+
+def Analyse(sdata: int, opt: Optional[str] = None, width: int = 0, height: int = 0) -> Analyser:
+    """The `svp1.Analyse(clip, sdata, src, opt)` filter's configuration; width/height are the
+    src clip's size (analyse_filter.rs:96-101)."""
+    h = _VP()
+    b = opt.encode() if opt is not None else None
+    _check(lib().svpf_analyser_create(sdata, b, len(b) if b else 0, width, height, ctypes.byref(h)))
+    return Analyser(_handle=h)
+
+
+def kernel_launches() -> int:
+    return lib().svpf_kernel_launches()
+
+
+def reset_kernel_launches():
+    lib().svpf_kernel_launches_reset()

@@ -1,0 +1,109 @@
+"""Seeded synthetic YUV420P8 clips for tests and benchmarks.
+
+Stands in for real video (the reference publishes no dataset for this path):
+frame 0 is uniform noise in 0..255 blurred by a separable Gaussian (sigma 2 luma,
+1 chroma; radius ceil(3 sigma); float accumulation, rounded). Each following clean
+frame is the previous one shifted by an integer global motion drawn uniformly from
+[-R, R]^2 (edges replicated), with `objects` textured rectangles (32-96 px sides)
+pasted on top, each moving with its own constant velocity from [-M, M]^2. Every
+output frame adds fresh Gaussian noise (sigma `noise`) to its clean frame, rounded
+and clamped to 0..255. Chroma planes move by half the luma motion.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+
+def _kernel(sigma: float) -> np.ndarray:
+    r = int(math.ceil(3 * sigma))
+    x = np.arange(-r, r + 1, dtype=np.float64)
+    k = np.exp(-(x * x) / (2 * sigma * sigma))
+    return (k / k.sum()).astype(np.float32)
+
+
+def _blur(img: np.ndarray, sigma: float) -> np.ndarray:
+    k = _kernel(sigma)
+    r = len(k) // 2
+    a = np.pad(img.astype(np.float32), ((0, 0), (r, r)), mode="edge")
+    h = sum(k[i] * a[:, i:i + img.shape[1]] for i in range(len(k)))
+    a = np.pad(h, ((r, r), (0, 0)), mode="edge")
+    v = sum(k[i] * a[i:i + img.shape[0], :] for i in range(len(k)))
+    return v
+
+
+def _shift(img: np.ndarray, dy: int, dx: int) -> np.ndarray:
+    h, w = img.shape
+    ys = np.clip(np.arange(h) - dy, 0, h - 1)
+    xs = np.clip(np.arange(w) - dx, 0, w - 1)
+    return img[ys][:, xs]
+
+
+@dataclass
+class _Obj:
+    h: int
+    w: int
+    y: float
+    x: float
+    vy: int
+    vx: int
+    tex: list  # per plane textures
+
+
+def make_clip(width: int, height: int, frames: int, seed: int, motion: int = 8, objects: int = 4,
+              object_motion: int = 16, noise: float = 2.0) -> np.ndarray:
+    """Returns uint8 [frames, w*h + 2*(w/2*h/2)] packed I420 frames."""
+    assert width % 2 == 0 and height % 2 == 0
+    rng = np.random.default_rng(seed)
+    cw, ch = width // 2, height // 2
+    dims = [(height, width, 2.0), (ch, cw, 1.0), (ch, cw, 1.0)]
+    clean = [_blur(rng.integers(0, 256, size=(h, w)).astype(np.float32), s) for h, w, s in dims]
+    objs = []
+    for _ in range(objects):
+        oh = int(rng.integers(32, 97))
+        ow = int(rng.integers(32, 97))
+        tex = [_blur(rng.integers(0, 256, size=(oh, ow)).astype(np.float32), 2.0)]
+        tex += [_blur(rng.integers(0, 256, size=(max(oh // 2, 1), max(ow // 2, 1))).astype(np.float32), 1.0)
+                for _ in range(2)]
+        objs.append(_Obj(oh, ow, float(rng.integers(0, max(height - oh, 1))), float(rng.integers(0, max(width - ow, 1))),
+                         int(rng.integers(-object_motion, object_motion + 1)),
+                         int(rng.integers(-object_motion, object_motion + 1)), tex))
+    ysz, csz = width * height, cw * ch
+    out = np.empty((frames, ysz + 2 * csz), dtype=np.uint8)
+    for f in range(frames):
+        if f > 0:
+            dy = int(rng.integers(-motion, motion + 1))
+            dx = int(rng.integers(-motion, motion + 1))
+            clean = [_shift(clean[0], dy, dx), _shift(clean[1], dy // 2, dx // 2), _shift(clean[2], dy // 2, dx // 2)]
+        planes = [p.copy() for p in clean]
+        for o in objs:
+            oy = int(o.y + f * o.vy) % max(height - o.h, 1)
+            ox = int(o.x + f * o.vx) % max(width - o.w, 1)
+            planes[0][oy:oy + o.h, ox:ox + o.w] = o.tex[0][:min(o.h, height - oy), :min(o.w, width - ox)]
+            for p in (1, 2):
+                t = o.tex[p]
+                cy, cx = oy // 2, ox // 2
+                planes[p][cy:cy + t.shape[0], cx:cx + t.shape[1]] = t[:min(t.shape[0], ch - cy), :min(t.shape[1], cw - cx)]
+        for i, p in enumerate(planes):
+            noisy = p + rng.normal(0.0, noise, size=p.shape).astype(np.float32)
+            q = np.clip(np.rint(noisy), 0, 255).astype(np.uint8)
+            if i == 0:
+                out[f, :ysz] = q.reshape(-1)
+            else:
+                out[f, ysz + (i - 1) * csz: ysz + i * csz] = q.reshape(-1)
+    return out
+
+
+# Workloads of the reference's benchmark configurations (shapes, motion ranges).
+CONFIGS = {
+    "640x360": dict(width=640, height=360, frames=32, motion=8, objects=4, object_motion=16),
+    "1080p": dict(width=1920, height=1080, frames=240, motion=24, objects=8, object_motion=48),
+}
+# Option strings of those configurations for the reference's Super / Analyse filters.
+SUPER_OPT = {"640x360": "{pel:1}", "1080p": "{pel:2}"}
+ANALYSE_OPT = {
+    "640x360": "{block:{w:16,overlap:0},main:{search:{type:2,distance:2,satd:false,coarse:{satd:false}}}}",
+    "1080p": "{block:{w:16,overlap:3},main:{search:{type:3,distance:16,satd:true}}}",
+}

@@ -1,0 +1,574 @@
+"""ctypes front end of the CPU oracle (oracle/svpf_oracle.c) -- TEST INFRASTRUCTURE.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline / reference leg use
+this module: it is the checker, never the product. PARITY UNPINNED: the Rust reference
+cannot be built in this image and ships no golden vectors (see svpf_oracle.h).
+
+It also holds `parse_opt`, a restatement of the reference's lenient opt parser
+(crates/svpflow-core/src/params.rs:1-450), used to turn an opt string into the looked-up
+values the C restatement of SuperOpts/AnalyseOpts::from_opt consumes.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+from typing import Any, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libsvpf_oracle.so")
+
+
+# --------------------------------------------------------------------------- parser
+class Obj(list):
+    """JSON-ish object: ordered (key, value) members; the LAST duplicate wins (params.rs:77-85)."""
+
+    def get(self, key):  # type: ignore[override]
+        for k, v in reversed(self):
+            if k == key:
+                return v
+        return None
+
+
+class Arr(list):
+    pass
+
+
+class _Null:
+    def __repr__(self):
+        return "null"
+
+
+NULL = _Null()
+
+
+class ParseError(ValueError):
+    pass
+
+
+def parse_opt(text):
+    """params::parse (params.rs:1-11): returns the value tree or raises ParseError."""
+    b = text.encode() if isinstance(text, str) else bytes(text)
+    p = _Parser(b)
+    p.skip_ws()
+    v = p.value()
+    p.skip_ws()
+    if p.pos == len(b) or isinstance(v, Obj):
+        return v
+    raise ParseError("extra data after JSON value")
+
+
+class _Parser:
+    def __init__(self, b):
+        self.b = b
+        self.pos = 0
+
+    def peek(self):
+        return self.b[self.pos] if self.pos < len(self.b) else None
+
+    def at2(self, t):
+        return self.b[self.pos:self.pos + 2] == t
+
+    def consume(self, c):
+        if self.peek() == c:
+            self.pos += 1
+            return True
+        return False
+
+    def skip_space(self):
+        while self.peek() in (0x20, 0x0A, 0x0D, 0x09):
+            self.pos += 1
+
+    def skip_ws(self):
+        while True:
+            self.skip_space()
+            if self.at2(b"//"):
+                self.pos += 2
+                while self.peek() not in (None, 0x0A, 0x0D):
+                    self.pos += 1
+            elif self.at2(b"/*"):
+                self.pos += 2
+                while not self.at2(b"*/"):
+                    if self.peek() is None:
+                        return
+                    self.pos += 1
+                self.pos += 2
+            else:
+                return
+
+    def skip_member_space(self):
+        self.skip_space()
+        if self.at2(b"//") or self.at2(b"/*"):
+            raise ParseError("Missing '}' or object member name")
+
+    def value(self):
+        self.skip_ws()
+        c = self.peek()
+        if c == ord("{"):
+            return self.obj()
+        if c == ord("["):
+            return self.arr()
+        if c == ord('"'):
+            return self.string()
+        if c is not None and (c == ord("-") or 48 <= c <= 57):
+            return self.number()
+        for lit, val in ((b"true", True), (b"false", False), (b"null", NULL)):
+            if c == lit[0]:
+                if self.b[self.pos:self.pos + len(lit)] == lit:
+                    self.pos += len(lit)
+                    return val
+                raise ParseError("invalid literal")
+        raise ParseError("Syntax error: value, object or array expected.")
+
+    def obj(self):
+        self.pos += 1
+        self.skip_ws()
+        out = Obj()
+        if self.consume(ord("}")):
+            return out
+        while True:
+            self.skip_member_space()
+            if self.peek() == ord('"'):
+                key = self.string()
+            else:
+                key = self.ident()
+            self.skip_ws()
+            if not self.consume(ord(":")):
+                raise ParseError("Missing ':' after object member name")
+            out.append((key, self.value()))
+            self.skip_ws()
+            if self.consume(ord("}")):
+                return out
+            if not self.consume(ord(",")):
+                raise ParseError("Missing ',' or '}' in object declaration")
+
+    def arr(self):
+        self.pos += 1
+        self.skip_ws()
+        out = Arr()
+        if self.consume(ord("]")):
+            return out
+        while True:
+            out.append(self.value())
+            self.skip_ws()
+            if self.consume(ord("]")):
+                return out
+            if not self.consume(ord(",")):
+                raise ParseError("unexpected token")
+
+    def ident(self):
+        st = self.pos
+        c = self.peek()
+        if c is None or not (chr(c).isascii() and (chr(c).isalpha() or c == ord("_"))):
+            raise ParseError("Missing '}' or object member name")
+        self.pos += 1
+        while True:
+            c = self.peek()
+            if c is not None and chr(c).isascii() and (chr(c).isalnum() or c == ord("_")):
+                self.pos += 1
+            else:
+                break
+        return self.b[st:self.pos].decode()
+
+    def string(self):
+        self.pos += 1
+        out = bytearray()
+        while self.pos < len(self.b):
+            c = self.b[self.pos]
+            self.pos += 1
+            if c == ord('"'):
+                return out.decode("utf-8", errors="replace")
+            if c != ord("\\"):
+                out.append(c)
+                continue
+            e = self.peek()
+            if e is not None:
+                self.pos += 1
+            simple = {ord('"'): b'"', ord("\\"): b"\\", ord("/"): b"/", ord("b"): b"\b", ord("f"): b"\f",
+                      ord("n"): b"\n", ord("r"): b"\r", ord("t"): b"\t"}
+            if e in simple:
+                out += simple[e]
+            elif e == ord("u"):
+                code = self.hex4()
+                if 0xD800 <= code <= 0xDBFF:
+                    if not (self.consume(ord("\\")) and self.consume(ord("u"))):
+                        raise ParseError("surrogate")
+                    low = self.hex4()
+                    if not 0xDC00 <= low <= 0xDFFF:
+                        raise ParseError("surrogate")
+                    out += chr(0x10000 + ((code - 0xD800) << 10) + (low - 0xDC00)).encode()
+                elif 0xDC00 <= code <= 0xDFFF:
+                    out += "�".encode()
+                else:
+                    out += chr(code).encode()
+            else:
+                raise ParseError("Bad escape sequence in string")
+        raise ParseError("unterminated string")
+
+    def hex4(self):
+        code = 0
+        for _ in range(4):
+            c = self.peek()
+            if c is None or chr(c) not in "0123456789abcdefABCDEF":
+                raise ParseError("hex digit expected")
+            self.pos += 1
+            code = code * 16 + int(chr(c), 16)
+        return code
+
+    def digits(self):
+        st = self.pos
+        while self.peek() is not None and 48 <= self.peek() <= 57:
+            self.pos += 1
+        return self.pos != st
+
+    def number(self):
+        st = self.pos
+        neg = self.consume(ord("-"))
+        lead = False
+        c = self.peek()
+        if c is not None and 48 <= c <= 57:
+            self.pos += 1
+            self.digits()
+        elif neg and self.consume(ord(".")):
+            if not self.digits():
+                raise ParseError("not a number")
+            lead = True
+        elif neg:
+            return 0.0
+        else:
+            raise ParseError("invalid number")
+        if not lead and self.consume(ord(".")):
+            self.digits()
+        if self.consume(ord("e")) or self.consume(ord("E")):
+            if not self.consume(ord("+")):
+                self.consume(ord("-"))
+            if not self.digits():
+                raise ParseError("not a number")
+        text = self.b[st:self.pos].decode()
+        if lead:
+            text = "-0" + text[1:]
+        return float(text)
+
+
+def lookup(tree, path):
+    """Value::at (params.rs:69-75)."""
+    v = tree
+    for k in path:
+        if not isinstance(v, Obj):
+            return None
+        v = v.get(k)
+        if v is None:
+            return None
+    return v
+
+
+# key paths of the C oracle (svpf_oracle.h OK_*), in enum order
+KEYS = [
+    ("pel",), ("gpu",), ("scale", "down"), ("scale", "up"), ("full",), ("rc",),
+    ("vectors",), ("block", "w"), ("block", "h"), ("block", "overlap"), ("special", "delta"), ("delta",),
+    ("main", "penalty", "lambda"), ("penalty", "lambda"),
+    ("main", "penalty", "lsad"), ("penalty", "lsad"),
+    ("main", "penalty", "plevel"), ("penalty", "plevel"),
+    ("main", "penalty", "pnew"), ("penalty", "pnew"),
+    ("main", "penalty", "pglobal"), ("penalty", "pglobal"),
+    ("main", "penalty", "pzero"), ("penalty", "pzero"),
+    ("main", "penalty", "pnbour"), ("penalty", "pnbour"),
+    ("main", "penalty", "prev"), ("penalty", "prev"),
+    ("main", "search", "type"), ("search", "type"),
+    ("main", "search", "distance"), ("search", "distance"),
+    ("main", "search", "coarse", "type"), ("search", "coarse", "type"),
+    ("main", "search", "coarse", "distance"), ("search", "coarse", "distance"),
+    ("main", "search", "coarse", "trymany"), ("search", "coarse", "trymany"),
+    ("main", "search", "coarse", "bad", "sad"), ("search", "coarse", "bad", "sad"),
+    ("main", "search", "coarse", "bad", "range"),
+    ("main", "search", "satd"), ("search", "satd"),
+    ("main", "search", "coarse", "satd"),
+    ("main", "search", "sort"), ("sort",),
+    "REFINE0", ("REFINE0", "thsad"), ("REFINE0", "search", "type"), ("REFINE0", "search", "distance"),
+    ("REFINE0", "search", "satd"),
+    ("main", "levels"),
+]
+OR_ABSENT, OR_NUMBER, OR_BOOL, OR_NULL, OR_STRING, OR_ARRAY, OR_OBJECT = range(7)
+
+
+class OrVal(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("nonempty", ctypes.c_int32), ("num", ctypes.c_double)]
+
+
+def _val(v) -> tuple:
+    if v is None:
+        return (OR_ABSENT, 0, 0.0)
+    if v is NULL:
+        return (OR_NULL, 0, 0.0)
+    if isinstance(v, bool):
+        return (OR_BOOL, 0, 1.0 if v else 0.0)
+    if isinstance(v, float):
+        return (OR_NUMBER, 0, v)
+    if isinstance(v, str):
+        return (OR_STRING, int(len(v) > 0), 0.0)
+    if isinstance(v, Arr):
+        return (OR_ARRAY, int(len(v) > 0), 0.0)
+    if isinstance(v, Obj):
+        return (OR_OBJECT, int(len(v) > 0), 0.0)
+    raise TypeError(v)
+
+
+def raw_values(opt: Optional[str]):
+    """Array of OrVal for svpf_oracle's from_opt functions (None / parse error -> absent)."""
+    arr = (OrVal * len(KEYS))()
+    tree = None
+    if opt is not None:
+        try:
+            tree = parse_opt(opt)
+        except ParseError:
+            tree = None  # super_filter.rs:120 / analyse_filter.rs:85: params::parse(..).ok()
+    refine0 = None
+    r = lookup(tree, ("refine",)) if tree is not None else None
+    if isinstance(r, Arr) and len(r) > 0:
+        refine0 = r[0]
+    for i, k in enumerate(KEYS):
+        if tree is None:
+            v = None
+        elif k == "REFINE0":
+            v = refine0
+        elif k[0] == "REFINE0":
+            v = lookup(refine0, k[1:]) if refine0 is not None else None
+        else:
+            v = lookup(tree, k)
+        arr[i].kind, arr[i].nonempty, arr[i].num = _val(v)
+    return arr
+
+
+# --------------------------------------------------------------------------- structs
+class SuperOpts(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in
+                ("pel", "gpu", "scale_down", "scale_up", "full", "rc", "levels", "width", "height")]
+
+
+class AnalyseOpts(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in
+                ("vectors", "block_w", "block_h", "overlap_mode", "overlap_x", "overlap_y", "delta", "pel",
+                 "selector", "levels", "super_levels", "width", "height", "lambda_", "lsad")] + \
+               [("plevel", ctypes.c_double)] + \
+               [(n, ctypes.c_int32) for n in
+                ("pnew", "pglobal", "pzero", "pnbour", "prev", "search_type", "coarse_search_type", "distance",
+                 "coarse_distance", "coarse_trymany", "coarse_bad_sad", "coarse_bad_range", "fine_satd",
+                 "coarse_satd", "has_refine_thsad", "refine_thsad", "refine_search_type", "refine_distance",
+                 "refine_satd", "sort")]
+
+
+class Vec8(ctypes.Structure):
+    _fields_ = [("dx", ctypes.c_int16), ("dy", ctypes.c_int16), ("score", ctypes.c_uint32),
+                ("luma", ctypes.c_uint8), ("pad", ctypes.c_uint8 * 3)]
+
+
+class Planes(ctypes.Structure):
+    _fields_ = [("y", ctypes.c_void_p), ("y_len", ctypes.c_size_t), ("y_stride", ctypes.c_size_t),
+                ("u", ctypes.c_void_p), ("u_len", ctypes.c_size_t), ("u_stride", ctypes.c_size_t),
+                ("v", ctypes.c_void_p), ("v_len", ctypes.c_size_t), ("v_stride", ctypes.c_size_t),
+                ("luma_w", ctypes.c_size_t), ("luma_h", ctypes.c_size_t),
+                ("pel", ctypes.c_int32), ("levels", ctypes.c_int32), ("full", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def build():
+    """Compiles the oracle with its own Makefile (gcc)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        L.or_super_opts_from_opt.argtypes = [P(OrVal), ctypes.c_int32, ctypes.c_int32, P(SuperOpts), ctypes.c_char_p, ctypes.c_size_t]
+        L.or_super_pack_data.restype = ctypes.c_int64
+        L.or_super_pack_data.argtypes = [P(SuperOpts)]
+        L.or_super_height.argtypes = [P(SuperOpts)]
+        L.or_super_output_len.restype = ctypes.c_size_t
+        L.or_super_output_len.argtypes = [P(SuperOpts)]
+        L.or_analyse_opts_from_opt.argtypes = [P(OrVal), ctypes.c_int64, P(SuperOpts), P(AnalyseOpts), ctypes.c_char_p, ctypes.c_size_t]
+        L.or_analyser_portable.argtypes = [P(SuperOpts), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                           P(AnalyseOpts), ctypes.c_char_p, ctypes.c_size_t]
+        L.or_build_super_portable.argtypes = [P(SuperOpts), ctypes.c_void_p, ctypes.c_void_p]
+        L.or_build_super_many.argtypes = [P(SuperOpts), P(ctypes.c_void_p), P(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int32]
+        L.or_build_plane.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                                     ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
+                                     ctypes.c_int32, P(SuperOpts)]
+        L.or_payload_len.restype = ctypes.c_size_t
+        L.or_payload_len.argtypes = [P(AnalyseOpts)]
+        L.or_analyse_portable.argtypes = [P(AnalyseOpts), P(SuperOpts), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.or_analyse_clip.argtypes = [P(AnalyseOpts), P(SuperOpts), P(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]
+        L.or_analyse_pair.argtypes = [P(Planes), P(Planes), P(AnalyseOpts), ctypes.c_void_p, ctypes.c_void_p]
+        L.or_pack_vdata_header.argtypes = [P(AnalyseOpts), P(ctypes.c_int32)]
+        L.or_hadamard4_satd.restype = ctypes.c_uint32
+        L.or_hadamard4_satd.argtypes = [P(ctypes.c_int32)]
+        L.or_adapt_lambda.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
+        L.or_exact_lambda.argtypes = [P(AnalyseOpts), ctypes.c_int32, ctypes.c_int32]
+        L.or_rescale_scores.argtypes = [P(Vec8), ctypes.c_size_t, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+        L.or_global_doubled.argtypes = [P(Vec8), ctypes.c_size_t, P(ctypes.c_int32), P(ctypes.c_int32)]
+        L.or_block_cost_lc.argtypes = [P(Planes), P(Planes)] + [ctypes.c_int32] * 9 + [P(ctypes.c_uint32), P(ctypes.c_uint32)]
+        L.or_last_counters.argtypes = [P(ctypes.c_uint64)]
+        for f in ("or_reduce_dim", "or_auto_levels", "or_super_plane_height", "or_auto_search_levels"):
+            getattr(L, f).argtypes = [ctypes.c_int32] * {"or_reduce_dim": 2, "or_auto_levels": 2,
+                                                           "or_super_plane_height": 4, "or_auto_search_levels": 6}[f]
+        L.or_level_grid.argtypes = [P(AnalyseOpts), ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32)]
+        _lib = L
+    return _lib
+
+
+def _err():
+    return ctypes.create_string_buffer(512)
+
+
+def super_opts(width: int, height: int, opt: Optional[str] = None) -> SuperOpts:
+    o = SuperOpts()
+    e = _err()
+    if lib().or_super_opts_from_opt(raw_values(opt), width, height, ctypes.byref(o), e, 512):
+        raise ValueError(e.value.decode())
+    return o
+
+
+def super_opts_portable(width: int, height: int, pel: int) -> SuperOpts:
+    """SuperBuilder::new (portable.rs:30-62)."""
+    if pel not in (1, 2, 4):
+        raise ValueError("pel must be 1, 2 or 4")
+    if width <= 0 or height <= 0 or width % 2 or height % 2:
+        raise ValueError("dimensions must be positive and even")
+    o = super_opts(width, height, None)
+    o.pel = pel
+    return o
+
+
+def analyse_opts(sdata: int, opt: Optional[str] = None, hint: Optional[SuperOpts] = None,
+                 src_width: int = 0, src_height: int = 0) -> AnalyseOpts:
+    """AnalyseOpts::from_opt + the src-clip size override of analyse_filter.rs:96-101."""
+    o = AnalyseOpts()
+    e = _err()
+    if lib().or_analyse_opts_from_opt(raw_values(opt), sdata, ctypes.byref(hint) if hint else None,
+                                      ctypes.byref(o), e, 512):
+        raise ValueError(e.value.decode())
+    if src_width > 0:
+        o.width = src_width
+    if src_height > 0:
+        o.height = src_height
+    return o
+
+
+def analyser_portable(so: SuperOpts, bw: int, bh: int, overlap_mode: int, vectors: int) -> AnalyseOpts:
+    o = AnalyseOpts()
+    e = _err()
+    if lib().or_analyser_portable(ctypes.byref(so), bw, bh, overlap_mode, vectors, ctypes.byref(o), e, 512):
+        raise ValueError(e.value.decode())
+    return o
+
+
+def sdata(so: SuperOpts) -> int:
+    return lib().or_super_pack_data(ctypes.byref(so))
+
+
+def super_height(so: SuperOpts) -> int:
+    return lib().or_super_height(ctypes.byref(so))
+
+
+def super_output_len(so: SuperOpts) -> int:
+    return lib().or_super_output_len(ctypes.byref(so))
+
+
+def _ptr(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def build_super(so: SuperOpts, src: np.ndarray) -> np.ndarray:
+    """SuperBuilder::build on one packed I420 frame -> the super frame bytes."""
+    src = np.ascontiguousarray(src, dtype=np.uint8)
+    out = np.zeros(super_output_len(so), dtype=np.uint8)
+    lib().or_build_super_portable(ctypes.byref(so), _ptr(src), _ptr(out))
+    return out
+
+
+def build_super_many(so: SuperOpts, frames: np.ndarray, threads: int = 1) -> np.ndarray:
+    frames = np.ascontiguousarray(frames, dtype=np.uint8)
+    n = frames.shape[0]
+    out = np.zeros((n, super_output_len(so)), dtype=np.uint8)
+    srcp = (ctypes.c_void_p * n)(*[frames[i].ctypes.data for i in range(n)])
+    dstp = (ctypes.c_void_p * n)(*[out[i].ctypes.data for i in range(n)])
+    lib().or_build_super_many(ctypes.byref(so), srcp, dstp, n, threads)
+    return out
+
+
+def payload_len(ao: AnalyseOpts) -> int:
+    return lib().or_payload_len(ctypes.byref(ao))
+
+
+def vdata_header(ao: AnalyseOpts) -> list:
+    h = (ctypes.c_int32 * 16)()
+    lib().or_pack_vdata_header(ctypes.byref(ao), h)
+    return list(h)
+
+
+def analyse(ao: AnalyseOpts, so: SuperOpts, cur: np.ndarray, ref: np.ndarray) -> np.ndarray:
+    """Analyser::analyse on two portable super frames -> payload bytes."""
+    out = np.zeros(payload_len(ao), dtype=np.uint8)
+    cur = np.ascontiguousarray(cur, dtype=np.uint8)
+    ref = np.ascontiguousarray(ref, dtype=np.uint8)
+    rc = lib().or_analyse_portable(ctypes.byref(ao), ctypes.byref(so), _ptr(cur), _ptr(ref), _ptr(out))
+    if rc:
+        raise RuntimeError("the reference panics on this input (index out of range)")
+    return out
+
+
+def counters() -> list:
+    c = (ctypes.c_uint64 * 3)()
+    lib().or_last_counters(c)
+    return list(c)
+
+
+def analyse_clip(ao: AnalyseOpts, so: SuperOpts, supers: np.ndarray, first: int, count: int,
+                 threads: int = 1) -> np.ndarray:
+    """Output frames [first, first+count) of a clip of portable super frames."""
+    supers = np.ascontiguousarray(supers, dtype=np.uint8)
+    n = supers.shape[0]
+    pl = payload_len(ao)
+    out = np.zeros((count, pl), dtype=np.uint8)
+    ptrs = (ctypes.c_void_p * n)(*[supers[i].ctypes.data for i in range(n)])
+    rc = lib().or_analyse_clip(ctypes.byref(ao), ctypes.byref(so), ptrs, n, first, count, _ptr(out), threads)
+    if rc:
+        raise RuntimeError("the reference panics on this input (index out of range)")
+    return out
+
+
+def hadamard4(diff16) -> int:
+    a = (ctypes.c_int32 * 16)(*[int(v) for v in diff16])
+    return lib().or_hadamard4_satd(a)
+
+
+def adapt_lambda(nlambda: int, lsad: int, score: int) -> int:
+    return lib().or_adapt_lambda(nlambda, lsad, score & 0xFFFFFFFF)
+
+
+def reduce_dim(d: int, n: int) -> int:
+    return lib().or_reduce_dim(d, n)
+
+
+def auto_levels(w: int, h: int) -> int:
+    return lib().or_auto_levels(w, h)
+
+
+def auto_search_levels(w, h, bw, bh, ox, oy) -> int:
+    return lib().or_auto_search_levels(w, h, bw, bh, ox, oy)
+
+
+def level_grid(ao: AnalyseOpts, level: int):
+    gw, gh = ctypes.c_int32(), ctypes.c_int32()
+    lib().or_level_grid(ctypes.byref(ao), level, ctypes.byref(gw), ctypes.byref(gh))
+    return gw.value, gh.value

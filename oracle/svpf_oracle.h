@@ -1,0 +1,182 @@
+/*
+ * svpf_oracle.h -- CPU restatement of open-svpflow's svpflow1 motion-analysis path
+ * (Super pyramid + Analyse block search), used ONLY as a test checker.
+ *
+ * TEST INFRASTRUCTURE. Only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline / reference leg may load this library. The product (the CUDA
+ * library under open-svpflow_b200/) never links or calls it.
+ *
+ * PARITY UNPINNED: the reference (Rust, crates/svpflow1) cannot be built in this
+ * image (no cargo/rustc) and ships no tests, fixtures or golden vectors. This file
+ * is a line-by-line restatement of the reference's scalar semantics; it is guarded
+ * by an independent Python restatement (oracle/svpf_oracle_py.py) on small cases
+ * and by primitive-level known-answer tests, not by reference outputs.
+ *
+ * All citations are paths inside the reference project.
+ */
+#ifndef SVPF_ORACLE_H
+#define SVPF_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One looked-up option value: the result of Value::at(path) in
+ * crates/svpflow-core/src/params.rs:69-85 (absent when the path does not exist). */
+enum {
+    OR_ABSENT = 0,
+    OR_NUMBER = 1,
+    OR_BOOL = 2,
+    OR_NULL = 3,
+    OR_STRING = 4,
+    OR_ARRAY = 5,
+    OR_OBJECT = 6
+};
+
+typedef struct {
+    int32_t kind;     /* OR_* */
+    int32_t nonempty; /* strings / arrays / objects: !is_empty() */
+    double num;       /* OR_NUMBER: the parsed f64; OR_BOOL: 0 or 1 */
+} or_val;
+
+/* Key paths read by SuperOpts::from_opt (super_opts.rs:17-36) and
+ * AnalyseOpts::from_opt (analyse_opts.rs:45-174). "refine0." means the first
+ * element of the `refine` array (analyse_opts.rs:150-152). */
+enum {
+    OK_PEL = 0, OK_GPU, OK_SCALE_DOWN, OK_SCALE_UP, OK_FULL, OK_RC,
+    OK_VECTORS, OK_BLOCK_W, OK_BLOCK_H, OK_BLOCK_OVERLAP, OK_SPECIAL_DELTA, OK_DELTA,
+    OK_MAIN_PENALTY_LAMBDA, OK_PENALTY_LAMBDA,
+    OK_MAIN_PENALTY_LSAD, OK_PENALTY_LSAD,
+    OK_MAIN_PENALTY_PLEVEL, OK_PENALTY_PLEVEL,
+    OK_MAIN_PENALTY_PNEW, OK_PENALTY_PNEW,
+    OK_MAIN_PENALTY_PGLOBAL, OK_PENALTY_PGLOBAL,
+    OK_MAIN_PENALTY_PZERO, OK_PENALTY_PZERO,
+    OK_MAIN_PENALTY_PNBOUR, OK_PENALTY_PNBOUR,
+    OK_MAIN_PENALTY_PREV, OK_PENALTY_PREV,
+    OK_MAIN_SEARCH_TYPE, OK_SEARCH_TYPE,
+    OK_MAIN_SEARCH_DISTANCE, OK_SEARCH_DISTANCE,
+    OK_MAIN_SEARCH_COARSE_TYPE, OK_SEARCH_COARSE_TYPE,
+    OK_MAIN_SEARCH_COARSE_DISTANCE, OK_SEARCH_COARSE_DISTANCE,
+    OK_MAIN_SEARCH_COARSE_TRYMANY, OK_SEARCH_COARSE_TRYMANY,
+    OK_MAIN_SEARCH_COARSE_BAD_SAD, OK_SEARCH_COARSE_BAD_SAD,
+    OK_MAIN_SEARCH_COARSE_BAD_RANGE,
+    OK_MAIN_SEARCH_SATD, OK_SEARCH_SATD,
+    OK_MAIN_SEARCH_COARSE_SATD,
+    OK_MAIN_SEARCH_SORT, OK_SORT,
+    OK_REFINE0, /* the first element of `refine` itself (present or not) */
+    OK_REFINE0_THSAD, OK_REFINE0_SEARCH_TYPE, OK_REFINE0_SEARCH_DISTANCE, OK_REFINE0_SEARCH_SATD,
+    OK_MAIN_LEVELS,
+    OK_COUNT
+};
+
+/* SuperOpts, super_opts.rs:3-14 */
+typedef struct {
+    int32_t pel, gpu, scale_down, scale_up;
+    int32_t full, rc;
+    int32_t levels, width, height;
+} or_super_opts;
+
+/* AnalyseOpts, analyse_opts.rs:4-42 */
+typedef struct {
+    int32_t vectors, block_w, block_h, overlap_mode, overlap_x, overlap_y, delta, pel, selector;
+    int32_t levels, super_levels, width, height, lambda, lsad;
+    double plevel;
+    int32_t pnew, pglobal, pzero, pnbour, prev;
+    int32_t search_type, coarse_search_type, distance, coarse_distance;
+    int32_t coarse_trymany, coarse_bad_sad, coarse_bad_range;
+    int32_t fine_satd, coarse_satd;
+    int32_t has_refine_thsad, refine_thsad, refine_search_type, refine_distance, refine_satd;
+    int32_t sort;
+} or_analyse_opts;
+
+/* Vec8, analyse_search.rs:25-31 */
+typedef struct {
+    int16_t dx, dy;
+    uint32_t score;
+    uint8_t luma;
+    uint8_t pad_[3];
+} or_vec8;
+
+/* SuperPlanes, analyse_search.rs:33-46 (slices carry their lengths). */
+typedef struct {
+    const uint8_t *y; size_t y_len, y_stride;
+    const uint8_t *u; size_t u_len, u_stride;
+    const uint8_t *v; size_t v_len, v_stride;
+    size_t luma_w, luma_h;
+    int32_t pel, levels, full;
+} or_planes;
+
+/* ---- options ---- */
+int or_super_opts_from_opt(const or_val *raw, int32_t width, int32_t height, or_super_opts *out,
+                           char *err, size_t err_len);
+int64_t or_super_pack_data(const or_super_opts *o);
+int32_t or_super_height(const or_super_opts *o);
+int32_t or_reduce_dim(int32_t dim, int32_t n);
+int32_t or_auto_levels(int32_t width, int32_t height);
+int32_t or_super_plane_height(int32_t base_h, int32_t pel, int32_t levels, int32_t full);
+int or_analyse_opts_from_opt(const or_val *raw, int64_t sdata, const or_super_opts *hint,
+                             or_analyse_opts *out, char *err, size_t err_len);
+int or_overlap_from_mode(int32_t bw, int32_t bh, int32_t mode, int32_t *ox, int32_t *oy,
+                         char *err, size_t err_len);
+int32_t or_auto_search_levels(int32_t w, int32_t h, int32_t bw, int32_t bh, int32_t ox, int32_t oy);
+/* Analyser::new (portable.rs:189-229) */
+int or_analyser_portable(const or_super_opts *sopts, int32_t bw, int32_t bh, int32_t overlap_mode,
+                         int32_t vectors, or_analyse_opts *out, char *err, size_t err_len);
+void or_output_block(const or_analyse_opts *o, int32_t *bw, int32_t *bh, int32_t *ox, int32_t *oy);
+void or_grid(const or_analyse_opts *o, int32_t bw, int32_t bh, int32_t ox, int32_t oy,
+             int32_t *gw, int32_t *gh);
+void or_level_grid(const or_analyse_opts *o, int32_t level, int32_t *gw, int32_t *gh);
+
+/* ---- Super (super_build.rs) ---- */
+void or_build_plane(uint8_t *dst, size_t dst_len, size_t dst_stride, const uint8_t *src,
+                    size_t src_len, size_t src_stride, size_t src_w, size_t src_h, size_t luma_w,
+                    size_t luma_h, int32_t chroma, const or_super_opts *o);
+/* SuperBuilder::build (portable.rs:94-148): src = packed I420 (w*h + 2*(w/2*h/2)),
+ * out = y (w*H) | u (w/2*H/2) | v (w/2*H/2), H = super height. */
+void or_build_super_portable(const or_super_opts *o, const uint8_t *src, uint8_t *out);
+size_t or_super_output_len(const or_super_opts *o);
+
+/* ---- Analyse (analyse_search.rs) ---- */
+/* analyse_pair: bwd/fwd are gw*gh arrays of the OUTPUT grid (or NULL when that
+ * direction is not requested). Returns 0 or -1 when the level-0 grid is smaller than
+ * 2x2 (the reference indexes field[-1] there and panics, analyse_search.rs:534-535). */
+int or_analyse_pair(const or_planes *cur, const or_planes *ref, const or_analyse_opts *o,
+                    or_vec8 *bwd, or_vec8 *fwd);
+size_t or_payload_len(const or_analyse_opts *o);
+void or_pack_vector_frame(const or_analyse_opts *o, const or_vec8 *previous, const or_vec8 *current,
+                          uint8_t *out);
+void or_pack_vdata_header(const or_analyse_opts *o, int32_t out[16]);
+/* Analyser::analyse over two portable super frames -> payload bytes. */
+int or_analyse_portable(const or_analyse_opts *o, const or_super_opts *so, const uint8_t *cur_super,
+                        const uint8_t *ref_super, uint8_t *payload);
+/* Clip driver used by the CPU baseline: frame n pairs with min(n+delta, nframes-1)
+ * (analyse_filter.rs:277-279); pairs [first, first+count) are analysed on `threads`
+ * host threads (frames in parallel, fwd/bwd as two tasks, analyse_search.rs:160-191).
+ * supers[i] points at the portable super frame of frame i. */
+int or_analyse_clip(const or_analyse_opts *o, const or_super_opts *so, const uint8_t *const *supers,
+                    int32_t nframes, int32_t first, int32_t count, uint8_t *payloads, int32_t threads);
+/* Super over many frames on `threads` host threads. */
+void or_build_super_many(const or_super_opts *o, const uint8_t *const *src, uint8_t *const *out,
+                         int32_t nframes, int32_t threads);
+
+/* ---- primitives exposed for known-answer tests ---- */
+uint32_t or_hadamard4_satd(const int32_t diff[16]);
+int32_t or_adapt_lambda(int32_t nlambda, int32_t lsad, uint32_t pred_score);
+int32_t or_exact_lambda(const or_analyse_opts *o, int32_t level, int32_t pel);
+void or_rescale_scores(or_vec8 *field, size_t n, int32_t width, int32_t height, int32_t blk);
+void or_global_doubled(const or_vec8 *field, size_t n, int32_t *gx, int32_t *gy);
+/* Cost of one candidate: (luma, chroma) exactly as block_cost_lc (analyse_search.rs:1683). */
+void or_block_cost_lc(const or_planes *src, const or_planes *ref, int32_t level, int32_t px,
+                      int32_t py, int32_t bw, int32_t bh, int32_t mvx, int32_t mvy, int32_t satd,
+                      int32_t pel, uint32_t *luma, uint32_t *chroma);
+/* Work counters of the last or_analyse_pair on this thread (cost evaluations,
+ * luma and chroma pixels compared): the algorithmic work of the control flow. */
+void or_last_counters(uint64_t out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
