@@ -7,19 +7,22 @@
 //     backward field of the level above projected onto it, and vice versa (:128-191).
 //   * inside a level the blocks run in the reference's serial order (serpentine at
 //     level 0, score-sorted at coarser levels, :302-419): each block takes already
-//     searched neighbours as candidates, so the order is a true dependency chain.
-//   * inside a block every step of the search is a batch of candidate motion vectors
-//     whose positions are known before any of them is evaluated (the special
-//     candidates; a UMH cross + hexagon set; an exhaustive square; a hexagon step; an
-//     expanding ring). A batch is evaluated by all NT threads as (candidate, 4x4 tile)
-//     tasks, then reduced to the FIRST candidate of minimal cost below the running
-//     best. That equals the reference's sequential `if cost < best.cost` scan (:1122-
-//     1155) whenever cost >= motion penalty, i.e. pnew >= -256; below that the leader
-//     thread replays the sequential scan over the batch's precomputed costs.
-//   * a candidate's cost is a pure function of (block, vector); each candidate picks one
-//     of the reference's read paths (interior, clamped, edge-shifted; :1638-2351) once,
-//     and tiles then read pixels accordingly. Direct paths keep the reference's
-//     wrapping index arithmetic, so out-of-range origins read what it reads.
+//     searched neighbours as candidates, so the order is a true dependency chain and
+//     its latency is what the design minimises. Every thread of a half holds the same
+//     block state and takes the same decisions, so a search step costs one barrier.
+//   * every step of a block's search is a batch of candidate vectors whose positions are
+//     known before any is evaluated (special candidates; the UMH cross + hexagons; an
+//     exhaustive square; a hexagon step; an expanding ring). A candidate is evaluated by
+//     a group of G lanes of one warp, one 4x4 tile per lane (SATD, SAD or pixel sums),
+//     reduced with shuffles; each warp keeps the first candidate of minimal cost and
+//     the half combines its warps after the step's barrier. First-minimum equals the
+//     reference's sequential `if cost < best.cost` scan (:1122-1155) whenever
+//     cost >= motion penalty, i.e. pnew >= -256; below that the step replays the
+//     sequential scan over each round's costs.
+//   * a candidate whose block and reference block lie inside their planes takes the fast
+//     path (word loads, packed byte ops); any other candidate takes the reference's own
+//     read path (edge-shifted, clamped, masked; :1638-2351) through cand_setup, which
+//     keeps the reference's wrapping index arithmetic.
 //
 // Integer/indexing work: no tensor cores, no reduced precision. The two f64 formulas
 // (adapt_lambda, exact_lambda) are IEEE-exact (exact_lambda is host-precomputed).
@@ -34,18 +37,16 @@ namespace svpf {
 
 namespace {
 
-constexpr int NT = 256;        // threads per search direction
+constexpr int NT = 128;            // threads per search direction
 constexpr int NW = NT / 32;
-constexpr int MAXC = 320;      // candidate slots per evaluation chunk
-constexpr int MAXLIST = 16;    // special-candidate batch slots
+constexpr int NGMAX = NW * 32;     // candidate groups of a direction when a group is one lane
+constexpr int MAXSLOT = 16;        // special-candidate slots of a block
 
 enum : uint8_t { LM_DIRECT = 1, LM_SATD_MASK = 2, LM_SAD_BREAK = 3, LM_EDGE = 4, LM_DC = 5 };
 enum : uint8_t { CM_NONE = 0, CM_DIRECT = 1, CM_SAD_BREAK = 3, CM_EDGE = 4 };
-enum : int { BK_DONE = 0, BK_EXH, BK_UMH, BK_HEX6, BK_HEX3, BK_RING };
+enum : int { BK_EXH = 1, BK_UMH, BK_HEX6, BK_HEX3, BK_RING };
 
-// status bits
-constexpr int ST_PANIC = 1;      // the reference indexes out of range here (it would panic)
-constexpr int ST_UNSUPPORTED = 2;
+constexpr int ST_PANIC = 1;  // status bit: the reference indexes out of range here (it would panic)
 
 struct Cand {
     int64_t l_sbase, l_rbase, c_sbase, c_rbase;  // flat bases of the direct read paths
@@ -57,34 +58,17 @@ struct Cand {
 };
 
 struct DirSh {
-    Cand cand[MAXC];
-    unsigned accL[MAXC], accU[MAXC], accV[MAXC];
-    int2 mv[MAXC];
-    long long motion[MAXC];
-    long long kcost[MAXC];
-    unsigned ksad[MAXC];
-    unsigned short vlist[MAXC];
-    unsigned char valid[MAXC];
-    // special-candidate batch
-    int lx[MAXLIST], ly[MAXLIST], lpx[MAXLIST], lpy[MAXLIST];
-    unsigned char lch[MAXLIST], ldc[MAXLIST];
-    unsigned resL[MAXLIST], resC[MAXLIST];
-    int ln;
-    // generated batch
-    int bkind, bn, bcx, bcy, br, bstep, bodir;
-    int nvalid;
-    long long redK[NW];
-    int redI[NW];
-    int win;
-    unsigned win_sad;
-    long long best_cost;  // running best of the batch (pruning + acceptance)
-    // block state shared by the search steps
-    int px, py, bw, bh, chroma, pred_x, pred_y, lambda;
-    int bnd[4];
+    long long K[2][NW];                   // per-warp best (cost, index, sad) of a step, double-buffered
+    int I[2][NW];
+    unsigned S[2][NW];
+    unsigned slotL[2][MAXSLOT];                     // special-candidate results (exact_sad values)
+    long long rk[2][NGMAX], rm[2][NGMAX];           // exact sequential scan: per-group cost, motion
+    unsigned rs[2][NGMAX];
+    int ri[2][NGMAX];
+    unsigned char rv[2][NGMAX];
     int gx, gy;           // global predictor (doubled) for the next level
     int order_len;
     int abort_;
-    // reductions
     long long r64[NW][3];
     int r32[NW][2];
 };
@@ -121,7 +105,8 @@ __device__ __forceinline__ long long motion_penalty(int lambda, int px_, int py_
     return ((long long)lambda * (dx * dx + dy * dy)) >> 8;
 }
 
-// hadamard4_satd, analyse_search.rs:2681-2702
+// hadamard4_satd, analyse_search.rs:2681-2702: rows, then columns; the last column
+// stage and its absolute values use |a+b| + |a-b| = 2 max(|a|, |b|).
 __device__ __forceinline__ unsigned hadamard4(const int d[16]) {
     int t[16];
 #pragma unroll
@@ -134,13 +119,13 @@ __device__ __forceinline__ unsigned hadamard4(const int d[16]) {
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         int s0 = t[j] + t[4 + j], s1 = t[j] - t[4 + j], s2 = t[8 + j] + t[12 + j], s3 = t[8 + j] - t[12 + j];
-        s += abs(s0 + s2) + abs(s1 + s3) + abs(s0 - s2) + abs(s1 - s3);
+        s += max(abs(s0), abs(s2)) + max(abs(s1), abs(s3));
     }
-    return (unsigned)(s > 0 ? s : 0);
+    return (unsigned)(2 * s);
 }
 
 // -------------------------------------------------------------------------------------------
-// Candidate set-up: the reference's choice of read path for one (block, vector).
+// Candidate set-up on the reference's read paths (any candidate; the general path).
 //   edge_shift_origins :1638-1676 / block_cost_edge_lc :1996-2167
 //   block_cost_luma_interior :1719-1852 / satd_luma_clamp :2353-2436
 //   chroma_sad_x4 :2169-2303
@@ -353,30 +338,28 @@ __device__ unsigned luma_tile(const Cand &c, const Planes &S, const Planes &R, c
 }
 
 // One 4x4 tile of both chroma planes of a candidate.
-__device__ void chroma_tile(const Cand &c, const Planes &S, const Planes &R, const Geo &G, int cw, int tile, unsigned &ou,
-                            unsigned &ov) {
-    ou = 0; ov = 0;
-    if (c.cmode == CM_NONE) return;
+
+// One 4x4 tile of one chroma plane of a candidate on the general path.
+__device__ unsigned chroma_tile1(const Cand &c, const uint8_t *sp, const uint8_t *rp, const Geo &G, int cw, int tile) {
+    if (c.cmode == CM_NONE) return 0;
     const int txn = (cw + 3) >> 2;
     const int ty = tile / txn, tx = tile - ty * txn;
     const int r0 = ty * 4, c0 = tx * 4;
-    if (r0 >= c.c_rows || c0 >= cw) return;
+    if (r0 >= c.c_rows || c0 >= cw) return 0;
     const int hh = imin(4, c.c_rows - r0), ww = imin(4, cw - c0);
     const int64_t cs = G.cs, clen = G.clen;
     const int clw = G.clw, clh = G.clh;
-    int du[16], dv[16];
+    int d[16];
 #pragma unroll
-    for (int i = 0; i < 16; i++) { du[i] = 0; dv[i] = 0; }
+    for (int i = 0; i < 16; i++) d[i] = 0;
     if (c.cmode == CM_DIRECT) {
 #pragma unroll
         for (int r = 0; r < 4; r++)
 #pragma unroll
             for (int q = 0; q < 4; q++)
-                if (r < hh && q < ww) {
-                    const int64_t so = c.c_sbase + (int64_t)(r0 + r) * cs + c0 + q, ro = c.c_rbase + (int64_t)(r0 + r) * cs + c0 + q;
-                    du[r * 4 + q] = (int)rd(S.u, clen, so, 0) - (int)rd(R.u, clen, ro, 0);
-                    dv[r * 4 + q] = (int)rd(S.v, clen, so, 0) - (int)rd(R.v, clen, ro, 0);
-                }
+                if (r < hh && q < ww)
+                    d[r * 4 + q] = (int)rd(sp, clen, c.c_sbase + (int64_t)(r0 + r) * cs + c0 + q, 0) -
+                                   (int)rd(rp, clen, c.c_rbase + (int64_t)(r0 + r) * cs + c0 + q, 0);
     } else if (c.cmode == CM_SAD_BREAK) {
 #pragma unroll
         for (int r = 0; r < 4; r++) {
@@ -387,9 +370,8 @@ __device__ void chroma_tile(const Cand &c, const Planes &S, const Planes &R, con
                 const long long sx = (long long)c.c_sx + c0 + q;
                 if (r < hh && q < ww && sy < clh && sx < clw) {
                     const int rx = iclamp(c.c_rx + c0 + q, 0, clw - 1);
-                    const int64_t so = ((int64_t)c.c_srow + sy) * cs + sx, ro = ((int64_t)c.c_rrow + ry) * cs + rx;
-                    du[r * 4 + q] = (int)rd(S.u, clen, so, 128) - (int)rd(R.u, clen, ro, 128);
-                    dv[r * 4 + q] = (int)rd(S.v, clen, so, 128) - (int)rd(R.v, clen, ro, 128);
+                    d[r * 4 + q] = (int)rd(sp, clen, ((int64_t)c.c_srow + sy) * cs + sx, 128) -
+                                   (int)rd(rp, clen, ((int64_t)c.c_rrow + ry) * cs + rx, 128);
                 }
             }
         }
@@ -403,26 +385,48 @@ __device__ void chroma_tile(const Cand &c, const Planes &S, const Planes &R, con
             for (int q = 0; q < 4; q++)
                 if (r < hh && q < ww) {
                     const int sx = iclamp(c.c_sx + c0 + q, 0, mw), rx = iclamp(c.c_rx + c0 + q, 0, mw);
-                    const int64_t so = ((int64_t)c.c_srow + sy) * cs + sx, ro = ((int64_t)c.c_rrow + ry) * cs + rx;
-                    du[r * 4 + q] = (int)rd(S.u, clen, so, dflt) - (int)rd(R.u, clen, ro, dflt);
-                    dv[r * 4 + q] = (int)rd(S.v, clen, so, dflt) - (int)rd(R.v, clen, ro, dflt);
+                    d[r * 4 + q] = (int)rd(sp, clen, ((int64_t)c.c_srow + sy) * cs + sx, dflt) -
+                                   (int)rd(rp, clen, ((int64_t)c.c_rrow + ry) * cs + rx, dflt);
                 }
         }
     }
-    if (c.csatd) {
-        ou = hadamard4(du);
-        ov = hadamard4(dv);
-    } else {
+    if (c.csatd) return hadamard4(d);
+    unsigned s = 0;
 #pragma unroll
-        for (int i = 0; i < 16; i++) { ou += (unsigned)abs(du[i]); ov += (unsigned)abs(dv[i]); }
-    }
+    for (int i = 0; i < 16; i++) s += (unsigned)abs(d[i]);
+    return s;
 }
 
-__device__ __forceinline__ unsigned final_luma(const Cand &c, unsigned acc) { return c.lsatd ? (acc >> 1) : acc; }
-__device__ __forceinline__ unsigned final_chroma(const Cand &c, unsigned u, unsigned v) {
-    if (c.cmode == CM_NONE) return 0;
-    if (c.csatd) return sat_mul(sat_add(u >> 1, v >> 1), 4);
-    return sat_mul(u + v, 4);
+// -------------------------------------------------------------------------------------------
+// Fast path: candidates whose source and reference blocks lie inside their planes.
+// Bytes are read as 32-bit words from 4-byte aligned addresses and funnel-shifted; the
+// caller guarantees 8 readable bytes after the first byte of every row (see fast_setup).
+__device__ __forceinline__ uint32_t ld4u(const uint8_t *p) {
+    const uintptr_t a = (uintptr_t)p;
+    const uint32_t *q = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+    return __funnelshift_r(__ldg(q), __ldg(q + 1), (unsigned)(a & 3) * 8u);
+}
+__device__ __forceinline__ unsigned tile_satd(const uint8_t *sp, const uint8_t *rp, int64_t st) {
+    int d[16];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const uint32_t a = ld4u(sp + r * st), b = ld4u(rp + r * st);
+#pragma unroll
+        for (int q = 0; q < 4; q++) d[r * 4 + q] = (int)((a >> (8 * q)) & 255u) - (int)((b >> (8 * q)) & 255u);
+    }
+    return hadamard4(d);
+}
+__device__ __forceinline__ unsigned tile_sad(const uint8_t *sp, const uint8_t *rp, int64_t st) {
+    unsigned s = 0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) s = __dp4a(__vabsdiffu4(ld4u(sp + r * st), ld4u(rp + r * st)), 0x01010101u, s);
+    return s;
+}
+__device__ __forceinline__ unsigned tile_sum(const uint8_t *sp, int64_t st) {
+    unsigned s = 0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) s = __dp4a(ld4u(sp + r * st), 0x01010101u, s);
+    return s;
 }
 
 // -------------------------------------------------------------------------------------------
@@ -432,22 +436,24 @@ __constant__ int c_mod6m1[8] = {5, 0, 1, 2, 3, 4, 5, 0};
 __constant__ int2 c_hex4[16] = {{-4, 2}, {-4, 1}, {-4, 0}, {-4, -1}, {-4, -2}, {4, -2}, {4, -1}, {4, 0},
                                 {4, 1},  {4, 2},  {2, 3},  {0, 4},   {-2, 3},  {-2, -3}, {0, -4}, {2, -3}};  // :1075-1092
 
-__device__ __forceinline__ int ring_m(int r, int step) { return 2 * r > step ? (2 * r - step + step - 1) / step : 0; }
-
-__device__ int batch_size(int kind, int r, int step) {
+struct Gen {
+    int kind, cx, cy, r, step, odir, n;
+};
+__device__ __forceinline__ int ring_m(int r, int step) { return 2 * r > step ? (2 * r - 1) / step : 0; }
+__device__ __forceinline__ Gen make_gen(int kind, int cx, int cy, int r, int step, int odir) {
+    Gen g{kind, cx, cy, r, step, odir, 0};
     switch (kind) {
-    case BK_EXH: return (2 * r + 1) * (2 * r + 1);
-    case BK_UMH: return 4 * (r / 2 > 0 ? r / 2 : 0) + 16 * imax(r / 4, 1);
-    case BK_HEX6: return 6;
-    case BK_HEX3: return 3;
-    case BK_RING: return 4 * ring_m(r, step) + 4;
+    case BK_EXH: g.n = (2 * r + 1) * (2 * r + 1); break;
+    case BK_UMH: g.n = 4 * (r / 2 > 0 ? r / 2 : 0) + 16 * imax(r / 4, 1); break;
+    case BK_HEX6: g.n = 6; break;
+    case BK_HEX3: g.n = 3; break;
+    case BK_RING: g.n = 4 * ring_m(r, step) + 4; break;
     }
-    return 0;
+    return g;
 }
-
-__device__ int2 batch_mv(const DirSh &s, int i) {
-    const int cx = s.bcx, cy = s.bcy, r = s.br;
-    switch (s.bkind) {
+__device__ int2 gen_mv(const Gen &g, int i) {
+    const int cx = g.cx, cy = g.cy, r = g.r;
+    switch (g.kind) {
     case BK_EXH: {  // exact_refine_search type 4, :799-823 (raster over the square)
         const int w = 2 * r + 1;
         return make_int2(cx - r + i % w, cy - r + i / w);
@@ -463,9 +469,9 @@ __device__ int2 batch_mv(const DirSh &s, int i) {
         return make_int2(cx + h.x * scale, cy + h.y * scale);
     }
     case BK_HEX6: { int2 h = c_hex2[i + 1]; return make_int2(cx + h.x, cy + h.y); }
-    case BK_HEX3: { int2 h = c_hex2[s.bodir + i]; return make_int2(cx + h.x, cy + h.y); }
+    case BK_HEX3: { int2 h = c_hex2[g.odir + i]; return make_int2(cx + h.x, cy + h.y); }
     case BK_RING: {  // exact_expanding, :849-885
-        const int step = s.bstep, m = ring_m(r, step);
+        const int step = g.step, m = ring_m(r, step);
         if (i < 2 * m) { int off = -r + step + (i >> 1) * step; return make_int2(cx + off, (i & 1) ? cy + r : cy - r); }
         i -= 2 * m;
         if (i < 2 * m) { int off = -r + step + (i >> 1) * step; return make_int2((i & 1) ? cx + r : cx - r, cy + off); }
@@ -477,151 +483,319 @@ __device__ int2 batch_mv(const DirSh &s, int i) {
     return make_int2(0, 0);
 }
 
+// -------------------------------------------------------------------------------------------
 struct Ctx {
     const AnalyseParams *P;
     const LevelInfo *L;
     Geo G;
     Planes S, R;
     int level, d, tid, satd, pel;
+    int grp_lanes;   // G: lanes per candidate (power of two)
+    int tl, tcp;     // 4x4 luma tiles, 4x4 tiles per chroma plane of one candidate
 };
 
-// Evaluates the special-candidate batch (explicit list, per-slot block position).
-__device__ void eval_list(const Ctx &x, DirSh &s) {
-    const int n = s.ln;
-    const int bw = s.bw, bh = s.bh;
-    for (int i = x.tid; i < n; i += NT) {
-        Cand &c = s.cand[i];
-        cand_setup(c, *x.P, *x.L, x.G, x.level, s.lpx[i], s.lpy[i], bw, bh, s.lx[i], s.ly[i], s.lch[i] != 0, x.satd, x.pel,
-                   s.ldc[i] != 0);
-        s.accL[i] = 0; s.accU[i] = 0; s.accV[i] = 0;
-    }
-    dbar(x.d);
-    const int TL = x.L->tl, TC = x.L->tc, T = TL + TC;
-    const int cw = bw / 2;
-    for (int t = x.tid; t < n * T; t += NT) {
-        const int i = t / T, tile = t - i * T;
-        const Cand &c = s.cand[i];
-        if (tile < TL) {
-            unsigned v = luma_tile(c, x.S, x.R, x.G, bw, bh, tile);
-            if (v) atomicAdd(&s.accL[i], v);
-        } else if (c.cmode != CM_NONE) {
-            unsigned u, w;
-            chroma_tile(c, x.S, x.R, x.G, cw, tile - TL, u, w);
-            if (u) atomicAdd(&s.accU[i], u);
-            if (w) atomicAdd(&s.accV[i], w);
-        }
-    }
-    dbar(x.d);
-    for (int i = x.tid; i < n; i += NT) {
-        const Cand &c = s.cand[i];
-        if (s.ldc[i]) { s.resL[i] = s.accL[i]; s.resC[i] = 0; continue; }
-        s.resL[i] = final_luma(c, s.accL[i]);
-        s.resC[i] = final_chroma(c, s.accU[i], s.accV[i]);
-    }
-    dbar(x.d);
+// Per-block constants, identical in every thread of a direction.
+struct BlkC {
+    int px, py, bw, bh, px2, py2;
+    int bnd0, bnd1, bnd2, bnd3, ubx, uby;  // mv_bounds; ub = bound above which the edge shift starts
+    int chroma, satd_mode, fastable, fast_src, cfast_src, dc_fast;
+    int cw, ch, crows, cpx, cpy, tilesx, ctilesx;
+    int64_t lsrc, csrc, dsrc;              // flat index of the source block (luma, chroma, luma at (px, py))
+};
+
+__device__ __forceinline__ void make_blk(const Ctx &x, int px, int py, bool chroma, BlkC &b) {
+    const LevelInfo &L = *x.L;
+    const Geo &G = x.G;
+    const int bw = L.bw, bh = L.bh, pel = imax(x.pel, 1);
+    b.px = px; b.py = py; b.bw = bw; b.bh = bh;
+    b.px2 = px - (x.level > 0 && px + bw >= G.lw);
+    b.py2 = py - (x.level > 0 && py + bh >= G.lh);
+    b.bnd0 = -pel * px; b.bnd1 = -pel * py;
+    b.bnd2 = pel * (G.lw - px - bw) + 1; b.bnd3 = pel * (G.lh - py - bh) + 1;
+    b.ubx = b.bnd2 > b.bnd0 ? b.bnd2 : 0x7FFFFFFF;
+    b.uby = b.bnd3 > b.bnd1 ? b.bnd3 : 0x7FFFFFFF;
+    b.chroma = chroma;
+    b.satd_mode = x.satd && is_blk(bw) && is_blk(bh) && bw == bh;
+    b.fastable = bw > 0 && bh > 0 && (bw & 3) == 0 && (bh & 3) == 0;
+    b.tilesx = bw >> 2;
+    b.lsrc = ((int64_t)L.y_off + b.py2) * G.ys + b.px2;
+    b.fast_src = b.fastable && b.px2 >= 0 && b.py2 >= 0 && b.px2 + bw <= G.lw && b.py2 + bh <= G.lh &&
+                 b.lsrc + (int64_t)(bh - 1) * G.ys + bw + 8 <= G.ylen;
+    b.dsrc = ((int64_t)L.y_off + py) * G.ys + px;
+    b.dc_fast = b.fastable && px >= 0 && py >= 0 && px + bw <= G.lw && py + bh <= G.lh &&
+                b.dsrc + (int64_t)(bh - 1) * G.ys + bw + 8 <= G.ylen;
+    b.cw = bw / 2; b.ch = bh / 2;
+    b.crows = x.satd ? b.cw : b.ch;
+    b.ctilesx = (b.cw + 3) >> 2;
+    b.cpx = px / 2; b.cpy = py / 2;
+    b.csrc = ((int64_t)L.c_off + b.cpy) * G.cs + b.cpx;
+    b.cfast_src = (b.cw == 4 || b.cw == 8 || b.cw == 16) && b.ch >= 4 && (b.ch & 3) == 0 && px >= 0 && py >= 0 &&
+                  b.cpx + b.cw <= G.clw && b.cpy + b.ch <= G.clh &&
+                  b.csrc + (int64_t)(b.crows - 1) * G.cs + b.cw + 8 <= G.clen;
 }
 
-// Evaluates a generated batch against the running best (s.best_cost). On return
-// s.win is the accepted candidate (-1 if none), s.win_sad / s.best_cost its sad / cost.
-__device__ void eval_gen(const Ctx &x, DirSh &s) {
-    const int n = s.bn;
-    const int bw = s.bw, bh = s.bh;
-    const int TL = x.L->tl, TC = s.chroma ? x.L->tc : 0, T = TL + TC;
-    const int cw = bw / 2;
+// Does (block, mv) take the fast path? If so, the flat indices of its reference blocks.
+// It does when the reference takes its direct reads for both luma and chroma: no edge
+// shift, the luma block and the reference block inside the level, the chroma blocks too.
+__device__ __forceinline__ bool fast_setup(const Ctx &x, const BlkC &b, int mvx, int mvy, int64_t &lref,
+                                           int64_t &cref) {
+    if (!(b.fast_src && mvx >= b.bnd0 && mvx < b.ubx && mvy >= b.bnd1 && mvy < b.uby)) return false;
+    const LevelInfo &L = *x.L;
+    const Geo &G = x.G;
+    const int pel = imax(x.pel, 1);
+    int mx = mvx, my = mvy, sub = 0;
+    const bool l0sub = x.level == 0 && pel >= 2;
+    if (l0sub) { sub = (mvy & 1) * pel + (mvx & 1); mx = mvx >> 1; my = mvy >> 1; }
+    const int rx0 = b.px2 + mx, ry0 = b.py2 + my;
+    if (rx0 < 0 || ry0 < 0 || rx0 + b.bw > G.lw || ry0 + b.bh > G.lh) return false;
+    lref = ((int64_t)L.y_off + (int64_t)sub * G.lh + ry0) * G.ys + rx0;
+    if (lref + (int64_t)(b.bh - 1) * G.ys + b.bw + 8 > G.ylen) return false;
+    cref = 0;
+    if (b.chroma && b.cw >= 4 && b.ch >= 4) {
+        if (!b.cfast_src) return false;
+        int mcx, mcy;
+        if (l0sub) { mcx = mvx >> 2; mcy = mvy >> 2; }
+        else { mcx = mvx >> 1; mcy = mvy >> 1; }
+        const int crx = b.cpx + mcx, cry = b.cpy + mcy;
+        if (crx < 0 || cry < 0 || crx + b.cw > G.clw || cry + b.ch > G.clh) return false;
+        const int64_t crow0 = (int64_t)L.c_off + ((x.level == 0 && pel > 1) ? (int64_t)sub * G.clh : 0);
+        cref = (crow0 + cry) * G.cs + crx;
+        if (cref + (int64_t)(b.crows - 1) * G.cs + b.cw + 8 > G.clen) return false;
+    }
+    return true;
+}
+
+struct Res {
+    unsigned L, U, V;
+    int lsatd, cmode, csatd;
+};
+
+// The general path for one lane: the reference's own read path through cand_setup.
+// Arguments by value only, so nothing of the caller's state lives in local memory.
+__device__ __noinline__ Res slow_lane(const AnalyseParams *P, const LevelInfo *L, Geo G, Planes S, Planes R, int level,
+                                      int px, int py, int bw, int bh, int mvx, int mvy, bool chroma, int satd, int pel,
+                                      bool dc, int sub, int Gl, int TL, int TCp) {
+    Res r{0, 0, 0, 0, 0, 0};
+    Cand c;
+    cand_setup(c, *P, *L, G, level, px, py, bw, bh, mvx, mvy, chroma, satd, pel, dc);
+    r.lsatd = c.lsatd; r.cmode = c.cmode; r.csatd = c.csatd;
+    const int T = TL + (chroma ? 2 * TCp : 0);
+    for (int t = sub; t < T; t += Gl) {
+        if (t < TL) r.L += luma_tile(c, S, R, G, bw, bh, t);
+        else if (c.cmode != CM_NONE) {
+            int ct = t - TL;
+            const int pl = ct >= TCp;
+            ct -= pl * TCp;
+            const unsigned v = chroma_tile1(c, pl ? S.v : S.u, pl ? R.v : R.u, G, bw / 2, ct);
+            if (pl) r.V += v; else r.U += v;
+        }
+    }
+    return r;
+}
+
+// Work of one lane (`sub` of G) on one candidate: its share of the 4x4 tiles.
+// kind 0: block at (b.px, b.py); 1: the same mv on the block at (px, py) (general path);
+// 2: the block's luma pixel sum (block_luma_dc).
+__device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, int px, int py, int mvx, int mvy,
+                                         bool chroma, int sub) {
+    const int G = x.grp_lanes, TL = x.tl, TCp = x.tcp;
+    int64_t lref = 0, cref = 0;
+    bool fast = false;
+    if (kind == 0) fast = fast_setup(x, b, mvx, mvy, lref, cref);
+    else if (kind == 2) fast = b.dc_fast;
+    if (!fast)
+        return slow_lane(x.P, x.L, x.G, x.S, x.R, x.level, kind == 1 ? px : b.px, kind == 1 ? py : b.py, b.bw, b.bh,
+                         mvx, mvy, chroma, x.satd, x.pel, kind == 2, sub, G, TL, TCp);
+    Res r{0, 0, 0, 0, 0, 0};
+    const int T = TL + (chroma ? 2 * TCp : 0);
+    const int64_t ys = x.G.ys, cs = x.G.cs;
+    r.lsatd = kind == 2 ? 0 : b.satd_mode;
+    r.cmode = (chroma && b.cw >= 4 && b.ch >= 4) ? CM_DIRECT : CM_NONE;
+    r.csatd = x.satd;
+    const uint8_t *sl = x.S.y + (kind == 2 ? b.dsrc : b.lsrc);
+    for (int t = sub; t < T; t += G) {
+        if (t < TL) {
+            const int ty = t / b.tilesx, tx = t - ty * b.tilesx;
+            const int64_t o = (int64_t)ty * 4 * ys + tx * 4;
+            if (kind == 2) r.L += tile_sum(sl + o, ys);
+            else if (r.lsatd) r.L += tile_satd(sl + o, x.R.y + lref + o, ys);
+            else r.L += tile_sad(sl + o, x.R.y + lref + o, ys);
+        } else if (r.cmode != CM_NONE) {
+            int ct = t - TL;
+            const int pl = ct >= TCp;
+            ct -= pl * TCp;
+            const int ty = ct / b.ctilesx, tx = ct - ty * b.ctilesx;
+            if (ty * 4 >= b.crows) continue;
+            const int64_t o = (int64_t)ty * 4 * cs + tx * 4;
+            const uint8_t *sp = (pl ? x.S.v : x.S.u) + b.csrc + o, *rp = (pl ? x.R.v : x.R.u) + cref + o;
+            const unsigned v = r.csatd ? tile_satd(sp, rp, cs) : tile_sad(sp, rp, cs);
+            if (pl) r.V += v; else r.U += v;
+        }
+    }
+    return r;
+}
+
+__device__ __forceinline__ unsigned group_sum(unsigned v, int G) {
+    for (int o = G >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+__device__ __forceinline__ void finalize(const Res &r, unsigned &L, unsigned &C) {
+    L = r.lsatd ? (r.L >> 1) : r.L;
+    if (r.cmode == CM_NONE) C = 0;
+    else if (r.csatd) C = sat_mul(sat_add(r.U >> 1, r.V >> 1), 4);
+    else C = sat_mul(r.U + r.V, 4);
+}
+
+constexpr int MW = 4;  // validity mask words per chunk: 128 candidates
+
+// One search step: candidates g over the block against the running best `best_cost`.
+// Every warp computes which candidates pass exact_ok and the motion-penalty cut (a
+// ballot bitmask, identical in every warp), then groups take the passing candidates
+// in order. On return, identically in every thread: win = accepted candidate or -1,
+// and the new best cost / sad when accepted.
+__device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s, int &ph, const Gen &g, int lambda,
+                                          int predx, int predy, long long &best_cost, unsigned &best_sad, int &win) {
+    const int G = x.grp_lanes, gpw = 32 / G;
+    const int lane = x.tid & 31, warp = x.tid >> 5;
+    const int grp = warp * gpw + lane / G, sub = lane & (G - 1), NG = NW * gpw;
+    const bool serial = x.P->pnew < -256;
     const int pnew = x.P->pnew;
-    const bool serial = pnew < -256;
-    if (x.tid == 0) s.win = -1;
-    for (int base = 0; base < n; base += MAXC) {
-        const int cn = imin(MAXC, n - base);
-        if (x.tid == 0) s.nvalid = 0;
-        dbar(x.d);
-        const long long bestc = s.best_cost;
-        for (int i = x.tid; i < cn; i += NT) {
-            const int2 mv = batch_mv(s, base + i);
-            bool ok = mv.x >= s.bnd[0] && mv.y >= s.bnd[1] && mv.x < s.bnd[2] && mv.y < s.bnd[3];
-            long long motion = 0;
-            if (ok) {
-                motion = motion_penalty(s.lambda, s.pred_x, s.pred_y, mv.x, mv.y);
-                if (motion >= bestc) ok = false;
-            }
-            s.mv[i] = mv;
-            s.motion[i] = motion;
-            s.valid[i] = ok;
-            if (ok) {
-                cand_setup(s.cand[i], *x.P, *x.L, x.G, x.level, s.px, s.py, bw, bh, mv.x, mv.y, s.chroma != 0, x.satd, x.pel, false);
-                s.accL[i] = 0; s.accU[i] = 0; s.accV[i] = 0;
-                const int slot = atomicAdd(&s.nvalid, 1);
-                s.vlist[slot] = (unsigned short)i;
-            }
-        }
-        dbar(x.d);
-        const int nv = s.nvalid;
-        for (int t = x.tid; t < nv * T; t += NT) {
-            const int j = t / T, tile = t - j * T;
-            const int i = s.vlist[j];
-            const Cand &c = s.cand[i];
-            if (tile < TL) {
-                unsigned v = luma_tile(c, x.S, x.R, x.G, bw, bh, tile);
-                if (v) atomicAdd(&s.accL[i], v);
-            } else if (c.cmode != CM_NONE) {
-                unsigned u, w;
-                chroma_tile(c, x.S, x.R, x.G, cw, tile - TL, u, w);
-                if (u) atomicAdd(&s.accU[i], u);
-                if (w) atomicAdd(&s.accV[i], w);
-            }
-        }
-        dbar(x.d);
-        // finalize: cost = motion + pen(luma) + pen(chroma) (:1158-1221)
-        long long bk = 0x7FFFFFFFFFFFFFFFLL;
-        int bi = 0x7FFFFFFF;
-        for (int i = x.tid; i < cn; i += NT) {
-            if (!s.valid[i]) continue;
-            const Cand &c = s.cand[i];
-            const unsigned L = final_luma(c, s.accL[i]);
-            const unsigned C = s.chroma ? final_chroma(c, s.accU[i], s.accV[i]) : 0u;
-            const long long K = s.motion[i] + pen(pnew, L) + (s.chroma ? pen(pnew, C) : 0LL);
-            s.kcost[i] = K;
-            s.ksad[i] = sat_add(L, C);
-            if (K < bk || (K == bk && i < bi)) { bk = K; bi = i; }
-        }
-        if (!serial) {
+    long long bk = 0x7FFFFFFFFFFFFFFFLL;
+    int bi = 0x7FFFFFFF;
+    unsigned bs = 0;
+    win = -1;
+    for (int base = 0; base < g.n; base += 32 * MW) {
+        unsigned mask[MW];
+        int total = 0;
+        const long long cut = best_cost;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                long long ok_ = __shfl_xor_sync(0xFFFFFFFFu, bk, o);
-                int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
-                if (ok_ < bk || (ok_ == bk && oi < bi)) { bk = ok_; bi = oi; }
+        for (int w = 0; w < MW; w++) {
+            const int i = base + w * 32 + lane;
+            bool ok = i < g.n;
+            if (ok) {
+                const int2 mv = gen_mv(g, i);
+                ok = mv.x >= b.bnd0 && mv.y >= b.bnd1 && mv.x < b.bnd2 && mv.y < b.bnd3;  // exact_ok
+                if (ok) ok = motion_penalty(lambda, predx, predy, mv.x, mv.y) < cut;  // a later candidate faces a lower best
             }
-            if ((x.tid & 31) == 0) { s.redK[x.tid >> 5] = bk; s.redI[x.tid >> 5] = bi; }
+            mask[w] = __ballot_sync(0xFFFFFFFFu, ok);
+            total += __popc(mask[w]);
         }
-        dbar(x.d);
-        if (x.tid == 0) {
-            if (!serial) {
-                long long k = s.redK[0];
-                int ii = s.redI[0];
-                for (int w = 1; w < NW; w++)
-                    if (s.redK[w] < k || (s.redK[w] == k && s.redI[w] < ii)) { k = s.redK[w]; ii = s.redI[w]; }
-                if (ii != 0x7FFFFFFF && k < s.best_cost) {
-                    s.best_cost = k;
-                    s.win = base + ii;
-                    s.win_sad = s.ksad[ii];
-                }
-            } else {  // exact sequential scan (penalties may be negative)
-                for (int i = 0; i < cn; i++) {
-                    if (!s.valid[i]) continue;
-                    if (s.motion[i] >= s.best_cost) continue;
-                    if (s.kcost[i] < s.best_cost) {
-                        s.best_cost = s.kcost[i];
-                        s.win = base + i;
-                        s.win_sad = s.ksad[i];
-                    }
+        for (int r0 = 0; r0 < total; r0 += NG) {
+            const int rk = r0 + grp;
+            const bool act = rk < total;
+            int i = 0;
+            if (act) {  // the rk-th passing candidate
+                int rem = rk;
+#pragma unroll
+                for (int w = 0; w < MW; w++) {
+                    const int c = __popc(mask[w]);
+                    if (rem >= 0 && rem < c) i = base + w * 32 + (int)__fns(mask[w], 0, rem + 1);
+                    rem -= c;
                 }
             }
+            Res r{0, 0, 0, 0, 0, 0};
+            int2 mv = make_int2(0, 0);
+            if (act) {
+                mv = gen_mv(g, i);
+                r = eval_lane(x, b, 0, 0, 0, mv.x, mv.y, b.chroma != 0, sub);
+            }
+            r.L = group_sum(r.L, G);
+            r.U = group_sum(r.U, G);
+            r.V = group_sum(r.V, G);
+            long long K = 0x7FFFFFFFFFFFFFFFLL, motion = 0;
+            unsigned sad = 0;
+            if (act) {
+                unsigned L, C;
+                finalize(r, L, C);
+                if (!b.chroma) C = 0;
+                motion = motion_penalty(lambda, predx, predy, mv.x, mv.y);
+                K = motion + pen(pnew, L) + (b.chroma ? pen(pnew, C) : 0LL);  // :1158-1221
+                sad = sat_add(L, C);
+            }
+            if (serial) {  // exact sequential semantics for penalties that can be negative
+                if (sub == 0) {
+                    s.rk[ph][grp] = K; s.rm[ph][grp] = motion; s.rs[ph][grp] = sad; s.rv[ph][grp] = act;
+                    s.ri[ph][grp] = i;
+                }
+                dbar(x.d);
+                const int m = imin(NG, total - r0);
+                for (int j = 0; j < m; j++) {
+                    if (s.rm[ph][j] >= best_cost) continue;
+                    if (s.rk[ph][j] < best_cost) { best_cost = s.rk[ph][j]; best_sad = s.rs[ph][j]; win = s.ri[ph][j]; }
+                }
+                ph ^= 1;
+            } else if (act && sub == 0 && (K < bk || (K == bk && i < bi))) {
+                bk = K; bi = i; bs = sad;
+            }
         }
-        dbar(x.d);
     }
+    if (serial) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const long long ok_ = __shfl_xor_sync(0xFFFFFFFFu, bk, o);
+        const int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+        const unsigned os = __shfl_xor_sync(0xFFFFFFFFu, bs, o);
+        if (ok_ < bk || (ok_ == bk && oi < bi)) { bk = ok_; bi = oi; bs = os; }
+    }
+    if (lane == 0) { s.K[ph][warp] = bk; s.I[ph][warp] = bi; s.S[ph][warp] = bs; }
+    dbar(x.d);
+    bk = s.K[ph][0]; bi = s.I[ph][0]; bs = s.S[ph][0];
+#pragma unroll
+    for (int w = 1; w < NW; w++) {
+        const long long k = s.K[ph][w];
+        const int ii = s.I[ph][w];
+        if (k < bk || (k == bk && ii < bi)) { bk = k; bi = ii; bs = s.S[ph][w]; }
+    }
+    ph ^= 1;
+    if (bi != 0x7FFFFFFF && bk < best_cost) { best_cost = bk; best_sad = bs; win = bi; }
 }
 
-// -------------------------------------------------------------------------------------------
+// adapt_lambda, :1555-1564 (f64, IEEE-exact: one add, one division, two products)
+__device__ __forceinline__ int adapt_lambda(int nlambda, int lsad, unsigned pred_score) {
+    const double l = (double)imax(lsad, 1);
+    const double half = pred_score == 0xFFFFFFFFu ? -1.0 : (double)(pred_score >> 1);
+    const double t = __ddiv_rn(l, __dadd_rn(l, half));
+    double v = __dmul_rn(__dmul_rn((double)nlambda, t), t);
+    v = fmin(v, 21474836.47);
+    if (v != v) return 0;
+    if (v >= 2147483647.0) return 2147483647;
+    if (v <= -2147483648.0) return (int)0x80000000;
+    return (int)v;
+}
+
+// block_activity / plane_activity (:1486-1553): used only when search.coarse.distance < 0.
+__device__ __noinline__ unsigned plane_activity(const uint8_t *data, int64_t len, int64_t stride, int64_t row, int64_t x,
+                                                int w, int h, bool satd) {
+    const unsigned area = (unsigned)(w * h);
+    unsigned sum = 0;
+    for (int y = 0; y < h; y++)
+        for (int c = 0; c < w; c++) sum += rd(data, len, (row + y) * stride + x + c, 0);
+    const unsigned mean = area ? sum / area : 0;
+    if (!satd) {
+        unsigned s = 0;
+        for (int y = 0; y < h; y++)
+            for (int c = 0; c < w; c++) {
+                unsigned v = rd(data, len, (row + y) * stride + x + c, 0);
+                s += v > mean ? v - mean : mean - v;
+            }
+        return area ? s / area : 0;
+    }
+    unsigned total = 0;
+    for (int y = 0; y < h; y += 4)
+        for (int x0 = 0; x0 < w; x0 += 4) {
+            int dd[16];
+            for (int r = 0; r < 4; r++)
+                for (int q = 0; q < 4; q++) dd[r * 4 + q] = (int)rd(data, len, (row + y + r) * stride + x + x0 + q, 0) - (int)mean;
+            total += hadamard4(dd);
+        }
+    return area ? (total >> 1) / area : 0;
+}
+
+__device__ __forceinline__ int adaptive_radius(int radius, unsigned act) {
+    if (act < 2) return 0;
+    unsigned a = 255u * act / 150u;
+    return ((radius * (int)(a < 255 ? a : 255)) >> 8) + 1;
+}
 // search orders (:302-419)
 __device__ __forceinline__ int64_t initial_order_len(int gw, int gh) {
     const int64_t ni = (int64_t)imax(gh - 2, 0) * imax(gw - 2, 0);
@@ -684,55 +858,13 @@ __device__ __forceinline__ uint2 mkvec(int dx, int dy, unsigned score) {
     return make_uint2((uint32_t)(uint16_t)(short)dx | ((uint32_t)(uint16_t)(short)dy << 16), score);
 }
 
-// adapt_lambda, :1555-1564 (f64, IEEE-exact: one add, one division, two products)
-__device__ int adapt_lambda(int nlambda, int lsad, unsigned pred_score) {
-    const double l = (double)imax(lsad, 1);
-    const double half = pred_score == 0xFFFFFFFFu ? -1.0 : (double)(pred_score >> 1);
-    const double t = __ddiv_rn(l, __dadd_rn(l, half));
-    double v = __dmul_rn(__dmul_rn((double)nlambda, t), t);
-    v = fmin(v, 21474836.47);
-    if (v != v) return 0;
-    if (v >= 2147483647.0) return 2147483647;
-    if (v <= -2147483648.0) return (int)0x80000000;
-    return (int)v;
-}
+// search states of one block (exact_search_block :684-768, exact_refine_search :771-826,
+// exact_hex2 :942-1033, exact_umh :1036-1119, bad-SAD expansion :611-672)
+enum { S_REFINE, S_HEX_START, S_HEX_ITER, S_HEX_EXIT, S_BAD, S_BAD_RING, S_FINAL_RING, S_STORE };
 
-// block_activity / plane_activity (:1486-1553): used only when search.coarse.distance < 0.
-__device__ unsigned plane_activity(const uint8_t *data, int64_t len, int64_t stride, int64_t row, int64_t x, int w, int h,
-                                   bool satd) {
-    const unsigned area = (unsigned)(w * h);
-    unsigned sum = 0;
-    for (int y = 0; y < h; y++)
-        for (int c = 0; c < w; c++) sum += rd(data, len, (row + y) * stride + x + c, 0);
-    const unsigned mean = area ? sum / area : 0;
-    if (!satd) {
-        unsigned s = 0;
-        for (int y = 0; y < h; y++)
-            for (int c = 0; c < w; c++) {
-                unsigned v = rd(data, len, (row + y) * stride + x + c, 0);
-                s += v > mean ? v - mean : mean - v;
-            }
-        return area ? s / area : 0;
-    }
-    unsigned total = 0;
-    for (int y = 0; y < h; y += 4)
-        for (int x0 = 0; x0 < w; x0 += 4) {
-            int dd[16];
-            for (int r = 0; r < 4; r++)
-                for (int q = 0; q < 4; q++) dd[r * 4 + q] = (int)rd(data, len, (row + y + r) * stride + x + x0 + q, 0) - (int)mean;
-            total += hadamard4(dd);
-        }
-    return area ? (total >> 1) / area : 0;
-}
-
-__device__ int adaptive_radius(int radius, unsigned act) {
-    if (act < 2) return 0;
-    unsigned a = 255u * act / 150u;
-    return ((radius * (int)(a < 255 ? a : 255)) >> 8) + 1;
-}
-
-// The per-direction search of one level (exact_search_level, :480-681).
-__device__ void search_level(const Ctx &x, DirSh &s, DirScratch &ds, const uint2 *prevp, int *status) {
+// The per-direction search of one level (exact_search_level, :480-681). Every thread
+// of the direction runs this with identical values; only the evaluation work is split.
+__device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch &ds, const uint2 *prevp, int *status) {
     const AnalyseParams &P = *x.P;
     const LevelInfo &L = *x.L;
     const int level = x.level, gw = L.gw, gh = L.gh;
@@ -740,235 +872,241 @@ __device__ void search_level(const Ctx &x, DirSh &s, DirScratch &ds, const uint2
     uint2 *field = ds.vec[level & 1];
     uint8_t *lumaf = ds.luma[level & 1];
     const int64_t order_len = s.order_len;
-    // leader-only state
+    const bool smallest = L.smallest != 0;
+    const int G = x.grp_lanes, gpw = 32 / G;
+    const int lane = x.tid & 31, warp = x.tid >> 5;
+    const int grp = warp * gpw + lane / G, sub = lane & (G - 1), NG = NW * gpw;
     int bad_count = 0;
+    int ph = 0;
+    // The previous block's result: stored by thread 0 after the block's last barrier, so
+    // the other warps take it from here until the next block's barrier publishes it.
+    int64_t last_idx = -1;
+    uint2 last_val = make_uint2(0, 0);
     for (int64_t k = 0; k < order_len; k++) {
-        int bx = 0, by = 0, idx = 0, edge = 0, smallest = L.smallest;
-        int sxi = 0, syi = 0;
-        uint2 interp = make_uint2(0, 0);
-        int nseeds = 0, prev_slot = -1, rs_slot = -1, zslot = 0, gslot = 0, nslot0 = 0;
-        if (x.tid == 0) {
-            int2 b;
-            if (level == 0) b = initial_order_at(gw, gh, k);
-            else b = unpack_xy(ds.order[k]);
-            bx = b.x; by = b.y;
-            idx = by * gw + bx;
-            int px = (level > 0 && bx == gw - 1) ? L.lw - P.block_w : bx * P.step_x;
-            int py = (level > 0 && by == gh - 1) ? L.lh - P.block_h : by * P.step_y;
-            px += L.pxoff; py += L.pyoff;
-            s.px = px; s.py = py; s.bw = L.bw; s.bh = L.bh;
-            s.bnd[0] = -L.pel * px; s.bnd[1] = -L.pel * py;
-            s.bnd[2] = L.pel * (L.lw - px - L.bw) + 1; s.bnd[3] = L.pel * (L.lh - py - L.bh) + 1;
-            edge = level > 0 && (bx == gw - 1 || by == gh - 1);
-            sxi = imin(bx, gw - 2); syi = imin(by, gh - 2);
-            const int sidx = syi * gw + sxi;
-            if (sidx < 0 || (int64_t)sidx >= ncell || idx < 0 || (int64_t)idx >= ncell) {
-                atomicOr(status, ST_PANIC);
-                s.abort_ = 1;
-            } else {
-                interp = edge ? field[sidx] : field[idx];
-                const int2 imv = vmv(interp);
-                int n = 0;
-                // slot 0: the interpolated predictor at the block
-                s.lx[n] = imv.x; s.ly[n] = imv.y; s.lpx[n] = px; s.lpy[n] = py; s.lch[n] = !smallest; s.ldc[n] = 0; n++;
-                // edge blocks re-score the predictor at its source block (:536-549)
-                if (edge && !smallest) {
-                    rs_slot = n;
-                    s.lx[n] = imv.x; s.ly[n] = imv.y; s.lpx[n] = sxi * P.step_x; s.lpy[n] = syi * P.step_y;
-                    s.lch[n] = 1; s.ldc[n] = 0; n++;
-                }
-                if (prevp) {
-                    const uint2 pv = prevp[idx];
-                    if (pv.y != 0xFFFFFFFFu && pv.y > 0) {
-                        const int2 pm = vmv(pv);
-                        prev_slot = n;
-                        s.lx[n] = pm.x; s.ly[n] = pm.y; s.lpx[n] = px; s.lpy[n] = py; s.lch[n] = !smallest; s.ldc[n] = 0; n++;
-                    }
-                }
-                zslot = n;
-                s.lx[n] = 0; s.ly[n] = 0; s.lpx[n] = px; s.lpy[n] = py; s.lch[n] = !smallest; s.ldc[n] = 0; n++;  // zero
-                gslot = n;
-                s.lx[n] = s.gx; s.ly[n] = s.gy; s.lpx[n] = px; s.lpy[n] = py; s.lch[n] = !smallest; s.ldc[n] = 0; n++;  // global
-                nslot0 = n;
-                for (int ny = imax(by - 1, 0); ny <= imin(by + 1, gh - 1); ny++)
-                    for (int nx = imax(bx - 1, 0); nx <= imin(bx + 1, gw - 1); nx++) {
-                        const int64_t p = level == 0 ? initial_order_pos(gw, gh, nx, ny) : (int64_t)ds.pos[ny * gw + nx];
-                        if (p < k) {
-                            if (nseeds >= 8) { atomicOr(status, ST_PANIC); s.abort_ = 1; break; }
-                            const int2 nm = vmv(field[ny * gw + nx]);
-                            s.lx[n] = nm.x; s.ly[n] = nm.y; s.lpx[n] = px; s.lpy[n] = py; s.lch[n] = !smallest; s.ldc[n] = 0;
-                            n++; nseeds++;
-                        }
-                    }
-                // luma DC of the block (:1566-1617)
-                s.lx[n] = 0; s.ly[n] = 0; s.lpx[n] = px; s.lpy[n] = py; s.lch[n] = 0; s.ldc[n] = 1; n++;
-                s.ln = n;
-                s.chroma = !smallest;
+        const int2 bxy = level == 0 ? initial_order_at(gw, gh, k) : unpack_xy(ds.order[k]);
+        const int bx = bxy.x, by = bxy.y;
+        const int64_t idx = (int64_t)by * gw + bx;
+        int px = (level > 0 && bx == gw - 1) ? L.lw - P.block_w : bx * P.step_x;
+        int py = (level > 0 && by == gh - 1) ? L.lh - P.block_h : by * P.step_y;
+        px += L.pxoff;
+        py += L.pyoff;
+        const bool edge = level > 0 && (bx == gw - 1 || by == gh - 1);
+        const int sxi = imin(bx, gw - 2), syi = imin(by, gh - 2);
+        const int64_t sidx = (int64_t)syi * gw + sxi;
+        if (sidx < 0 || sidx >= ncell || idx < 0 || idx >= ncell) {  // field[-1]: the reference panics
+            if (x.tid == 0) { atomicOr(status, ST_PANIC); s.abort_ = 1; }
+            break;
+        }
+        const int64_t fi = edge ? sidx : idx;
+        const uint2 interp = fi == last_idx ? last_val : field[fi];
+        const int2 imv = vmv(interp);
+        BlkC b;
+        make_blk(x, px, py, !smallest, b);
+        // ---- special candidates (exact_search_block, :708-746): slot list in the
+        // reference's evaluation roles; slot j is evaluated by group j
+        int n = 0, rs_slot = -1, prev_slot = -1, nseeds = 0;
+        int m0x = imv.x, m0y = imv.y;                    // slot 0: the interpolated predictor
+        n = 1;
+        if (edge && !smallest) rs_slot = n++;            // re-score the predictor at its source block (:536-549)
+        int pmx = 0, pmy = 0;
+        if (prevp) {
+            const uint2 pv = prevp[idx];
+            if (pv.y != 0xFFFFFFFFu && pv.y > 0) {
+                const int2 pm = vmv(pv);
+                pmx = pm.x; pmy = pm.y;
+                prev_slot = n++;
+            }
+        }
+        const int zslot = n++, gslot = n++, nslot0 = n;
+        const int gxv = s.gx, gyv = s.gy;
+        int sdx[8], sdy[8];
+        bool panic = false;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            const int ny = by - 1 + q / 3, nx = bx - 1 + q % 3;
+            if (ny < 0 || ny >= gh || nx < 0 || nx >= gw) continue;
+            const int64_t ci = (int64_t)ny * gw + nx;
+            const int64_t p = level == 0 ? initial_order_pos(gw, gh, nx, ny) : (int64_t)ds.pos[ci];
+            if (p < k) {
+                if (nseeds >= 8) { panic = true; continue; }  // seeds[8] overflows: the reference panics
+                const int2 nm = vmv(ci == last_idx ? last_val : field[ci]);
+#pragma unroll
+                for (int t = 0; t < 8; t++)
+                    if (t == nseeds) { sdx[t] = nm.x; sdy[t] = nm.y; }
+                nseeds++;
+            }
+        }
+        if (panic) {
+            if (x.tid == 0) { atomicOr(status, ST_PANIC); s.abort_ = 1; }
+            break;
+        }
+        n += nseeds;
+        const int dcslot = n++;
+        // ---- evaluate the special slots
+        for (int j0 = 0; j0 < n; j0 += NG) {
+            const int j = j0 + grp;
+            const bool act = j < n;
+            int kind = 0, mx = 0, my = 0;
+            bool ch = !smallest;
+            if (j == 0) { mx = m0x; my = m0y; }
+            else if (j == rs_slot) { mx = m0x; my = m0y; kind = 1; ch = true; }
+            else if (j == prev_slot) { mx = pmx; my = pmy; }
+            else if (j == zslot) { mx = 0; my = 0; }
+            else if (j == gslot) { mx = gxv; my = gyv; }
+            else if (j == dcslot) { kind = 2; ch = false; }
+            else if (j >= nslot0 && j < nslot0 + nseeds) {
+#pragma unroll
+                for (int t = 0; t < 8; t++)
+                    if (t == j - nslot0) { mx = sdx[t]; my = sdy[t]; }
+            }
+            Res r{0, 0, 0, 0, 0, 0};
+            if (act) r = eval_lane(x, b, kind, sxi * P.step_x, syi * P.step_y, mx, my, ch, sub);
+            r.L = group_sum(r.L, G);
+            r.U = group_sum(r.U, G);
+            r.V = group_sum(r.V, G);
+            if (act && sub == 0) {
+                unsigned Lv, Cv;
+                if (kind == 2) { Lv = r.L; Cv = 0; }
+                else finalize(r, Lv, Cv);
+                s.slotL[ph][j] = ch ? sat_add(Lv, Cv) : Lv;  // exact_sad: luma (+ chroma)
             }
         }
         dbar(x.d);
-        if (s.abort_) break;
-        eval_list(x, s);
-        // ---- leader: exact_search_block (:684-768) on the special candidates
-        int stype = 0, radius = 0, lambda = 0;
-        int bmx = 0, bmy = 0, pred_x = 0, pred_y = 0;
-        unsigned bsad = 0;
-        long long bcost = 0;
+        const int phs = ph;
+        ph ^= 1;
+        // ---- selection among the special candidates (:716-747)
+        const unsigned pred_score = rs_slot >= 0 ? s.slotL[phs][rs_slot] : interp.y;
+        const bool field_valid = pred_score != 0xFFFFFFFFu;
+        int bmx = 0, bmy = 0;
+        unsigned bsad;
+        long long bcost;
         bool refine = false;
-        if (x.tid == 0) {
-            const int2 imv = vmv(interp);
-            pred_x = imv.x; pred_y = imv.y;
-            const unsigned pred_score = rs_slot >= 0 ? sat_add(s.resL[rs_slot], s.resC[rs_slot]) : interp.y;
-            const bool field_valid = pred_score != 0xFFFFFFFFu;
-            auto sadof = [&](int i) { return s.lch[i] ? sat_add(s.resL[i], s.resC[i]) : s.resL[i]; };
-            if (level == 0 && P.distance == 0) {
-                if (field_valid) { bmx = imv.x; bmy = imv.y; bsad = sadof(0); }
-                else { bmx = 0; bmy = 0; bsad = sadof(zslot); }
-            } else {
-                if (field_valid) { bmx = imv.x; bmy = imv.y; bsad = sadof(0); bcost = (long long)bsad; }
-                else { bmx = 0; bmy = 0; bsad = 0xFFFFFFFFu; bcost = 0x7FFFFFFFFFFFFFFFLL; }
-                int ppx = imv.x, ppy = imv.y;
-                if (prev_slot >= 0) {
-                    const unsigned sd = sadof(prev_slot);
-                    const long long cst = (long long)sd + (((long long)P.prev * sd) >> 8);
-                    if (cst < bcost) { bmx = s.lx[prev_slot]; bmy = s.ly[prev_slot]; bsad = sd; bcost = cst; ppx = bmx; ppy = bmy; }
-                }
-                {
-                    const unsigned sd = sadof(gslot);
-                    const long long cst = (long long)sd + (((long long)P.pglobal * sd) >> 8);
-                    if (cst < bcost) { bmx = s.lx[gslot]; bmy = s.ly[gslot]; bsad = sd; bcost = cst; }
-                }
-                {
-                    const unsigned sd = sadof(zslot);
-                    const long long cst = (long long)sd + (((long long)P.pzero * sd) >> 8);
-                    if (cst < bcost) { bmx = 0; bmy = 0; bsad = sd; bcost = cst; }
-                }
-                for (int j = 0; j < nseeds; j++) {
-                    const int i = nslot0 + j;
-                    const unsigned sd = sadof(i);
-                    const long long cst = (long long)sd + (((long long)P.pnbour * sd) >> 8);
-                    if (cst < bcost) { bmx = s.lx[i]; bmy = s.ly[i]; bsad = sd; bcost = cst; }
-                }
-                bcost = (long long)bsad;
-                lambda = adapt_lambda(L.lambda_base, L.lsad, pred_score);
-                radius = L.base_radius;
-                if (level > 0 && P.coarse_distance < 0) {
-                    const int ax = s.px - (level > 0 && s.px + s.bw >= L.lw), ay = s.py - (level > 0 && s.py + s.bh >= L.lh);
-                    unsigned act = plane_activity(x.S.y, x.G.ylen, x.G.ys, L.y_off + ay, ax, s.bw, s.bh, x.satd) +
-                                   plane_activity(x.S.u, x.G.clen, x.G.cs, L.c_off + s.py / 2, s.px / 2, s.bw / 2, s.bh / 2, x.satd) +
-                                   plane_activity(x.S.v, x.G.clen, x.G.cs, L.c_off + s.py / 2, s.px / 2, s.bw / 2, s.bh / 2, x.satd);
-                    radius = adaptive_radius(radius, act);
-                }
-                stype = (edge && level == 1) ? 0 : L.search_type;
-                refine = true;
-                s.pred_x = ppx; s.pred_y = ppy;  // refinement uses the (possibly re-anchored) predictor
+        int lambda = 0, radius = 0, stype = 0, ppx = imv.x, ppy = imv.y;
+        if (level == 0 && P.distance == 0) {
+            if (field_valid) { bmx = imv.x; bmy = imv.y; bsad = s.slotL[phs][0]; }
+            else bsad = s.slotL[phs][zslot];
+            bcost = (long long)bsad;
+        } else {
+            if (field_valid) { bmx = imv.x; bmy = imv.y; bsad = s.slotL[phs][0]; bcost = (long long)bsad; }
+            else { bsad = 0xFFFFFFFFu; bcost = 0x7FFFFFFFFFFFFFFFLL; }
+            if (prev_slot >= 0) {
+                const unsigned sd = s.slotL[phs][prev_slot];
+                const long long cst = (long long)sd + (((long long)P.prev * sd) >> 8);
+                if (cst < bcost) { bmx = pmx; bmy = pmy; bsad = sd; bcost = cst; ppx = pmx; ppy = pmy; }
             }
-            s.lambda = lambda;
+            {
+                const unsigned sd = s.slotL[phs][gslot];
+                const long long cst = (long long)sd + (((long long)P.pglobal * sd) >> 8);
+                if (cst < bcost) { bmx = gxv; bmy = gyv; bsad = sd; bcost = cst; }
+            }
+            {
+                const unsigned sd = s.slotL[phs][zslot];
+                const long long cst = (long long)sd + (((long long)P.pzero * sd) >> 8);
+                if (cst < bcost) { bmx = 0; bmy = 0; bsad = sd; bcost = cst; }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (q >= nseeds) break;
+                const unsigned sd = s.slotL[phs][nslot0 + q];
+                const long long cst = (long long)sd + (((long long)P.pnbour * sd) >> 8);
+                if (cst < bcost) { bmx = sdx[q]; bmy = sdy[q]; bsad = sd; bcost = cst; }
+            }
+            bcost = (long long)bsad;
+            lambda = adapt_lambda(L.lambda_base, L.lsad, pred_score);
+            radius = L.base_radius;
+            if (level > 0 && P.coarse_distance < 0) {
+                const unsigned act = plane_activity(x.S.y, x.G.ylen, x.G.ys, L.y_off + b.py2, b.px2, b.bw, b.bh, x.satd) +
+                                     plane_activity(x.S.u, x.G.clen, x.G.cs, L.c_off + py / 2, px / 2, b.bw / 2, b.bh / 2, x.satd) +
+                                     plane_activity(x.S.v, x.G.clen, x.G.cs, L.c_off + py / 2, px / 2, b.bw / 2, b.bh / 2, x.satd);
+                radius = adaptive_radius(radius, act);
+            }
+            stype = (edge && level == 1) ? 0 : L.search_type;
+            refine = true;
         }
-        // ---- refinement + bad-SAD expansion: leader-driven state machine, batches evaluated by all
-        // states: 0 start, 1 after EXH, 2 after UMH(refine), 3 after HEX6, 4 after HEX3, 5 after hex2 ring,
-        //         10 bad-start, 11 after bad ring, 12 after bad UMH, 13 after final ring, 99 store
-        int st = 0, ret = 0;           // ret: where hex2 returns (0 = refine done -> bad check, 1 = bad UMH -> final ring)
-        int hdir = -2, hi = 1, hbx = 0, hby = 0, hrad = 0, bad_r = 0, bad_max = 0;
+        const unsigned dcsum = s.slotL[phs][dcslot];
+        // ---- refinement and bad-SAD expansion: a replicated state machine issuing steps
+        int predx = ppx, predy = ppy;
+        int state = refine ? S_REFINE : S_STORE;
+        int hbx = 0, hby = 0, hdir = -2, hi = 0, hrad = 0, hret = 0, bad_r = 0, bad_max = 0;
         unsigned found = 0;
-        if (x.tid == 0) st = refine ? 0 : 10;
         for (;;) {
-            if (x.tid == 0) {
-                int issue = BK_DONE;
-                for (;;) {  // advance until a batch is issued or the block is done
-                    if (st == 0) {
-                        if (stype == 4) { s.bkind = BK_EXH; s.bcx = bmx; s.bcy = bmy; s.br = radius; issue = 1; st = 1; }
-                        else if (stype == 3) { s.bkind = BK_UMH; s.bcx = bmx; s.bcy = bmy; s.br = radius; issue = 1; st = 2; }
-                        else if (stype == 2) { st = 20; ret = 0; hrad = radius; }
-                        else st = 10;
-                    } else if (st == 1) { st = 10; }
-                    else if (st == 2) { st = 20; ret = 0; hrad = radius; }
-                    else if (st == 20) {  // exact_hex2 entry (:942-1033)
-                        hbx = bmx; hby = bmy;
-                        if (hrad > 1) { hdir = -2; s.bkind = BK_HEX6; s.bcx = hbx; s.bcy = hby; issue = 1; st = 3; }
-                        else { s.bkind = BK_RING; s.bcx = hbx; s.bcy = hby; s.br = 1; s.bstep = 1; issue = 1; st = 5; }
-                    } else if (st == 21) {  // hex2 iteration test
-                        if (hi < hrad / 2 && hbx >= s.bnd[0] && hby >= s.bnd[1] && hbx < s.bnd[2] && hby < s.bnd[3]) {
-                            const int odir = c_mod6m1[hdir + 1];
-                            s.bodir = odir; s.bkind = BK_HEX3; s.bcx = hbx; s.bcy = hby; issue = 1; st = 4;
-                        } else st = 22;
-                    } else if (st == 22) {  // hex2 exit: best.mv = (bmx, bmy), then radius-1 ring
-                        bmx = hbx; bmy = hby;
-                        s.bkind = BK_RING; s.bcx = hbx; s.bcy = hby; s.br = 1; s.bstep = 1; issue = 1; st = 5;
-                    } else if (st == 5) { st = ret == 0 ? 10 : 13; if (ret == 1) { s.bkind = BK_RING; s.bcx = bmx; s.bcy = bmy; s.br = 1; s.bstep = 1; issue = 1; st = 13; } }
-                    else if (st == 10) {  // bad-SAD expansion, :611-672
-                        found = bsad;
-                        const int bl = sat_i32((long long)P.coarse_bad_sad + (long long)(sat_i32((long long)P.coarse_bad_sad * bad_count) / 16));
-                        if (refine && level > 0 && idx > 1 && P.coarse_bad_sad > 0 && (int)bsad > bl) {
-                            bad_count++;
-                            s.pred_x = pred_x; s.pred_y = pred_y;  // the block's own predictor
-                            if (P.coarse_bad_range < 0) {
-                                bad_max = -P.coarse_bad_range * L.pel; bad_r = L.pel;
-                                if (bad_r < bad_max) { s.bkind = BK_RING; s.bcx = 0; s.bcy = 0; s.br = bad_r; s.bstep = L.pel; issue = 1; st = 11; }
-                                else { s.bkind = BK_RING; s.bcx = bmx; s.bcy = bmy; s.br = 1; s.bstep = 1; issue = 1; st = 13; }
-                            } else if (P.coarse_bad_range > 0) {
-                                s.bkind = BK_UMH; s.bcx = 0; s.bcy = 0; s.br = P.coarse_bad_range * L.pel; hrad = s.br; issue = 1; st = 12;
-                            } else {
-                                s.bkind = BK_RING; s.bcx = bmx; s.bcy = bmy; s.br = 1; s.bstep = 1; issue = 1; st = 13;
-                            }
-                        } else st = 99;
-                    } else if (st == 11) {
-                        if (bsad < found / 4) st = 14;
-                        else {
-                            bad_r += L.pel;
-                            if (bad_r < bad_max) { s.bkind = BK_RING; s.bcx = 0; s.bcy = 0; s.br = bad_r; s.bstep = L.pel; issue = 1; st = 11; }
-                            else st = 14;
-                        }
-                    } else if (st == 14) { s.bkind = BK_RING; s.bcx = bmx; s.bcy = bmy; s.br = 1; s.bstep = 1; issue = 1; st = 13; }
-                    else if (st == 12) { st = 20; ret = 1; }
-                    else if (st == 13) { st = 99; }
-                    else { st = 99; }
-                    if (issue || st == 99) break;
-                }
-                if (!issue) s.bkind = BK_DONE;
-                else { s.best_cost = bcost; s.bn = batch_size(s.bkind, s.br, s.bkind == BK_RING ? s.bstep : 1); }
-            }
-            dbar(x.d);
-            if (s.bkind == BK_DONE) break;
-            eval_gen(x, s);
-            if (x.tid == 0) {
-                const int w = s.win;
-                const int kind = s.bkind;
-                if (w >= 0) {
-                    bsad = s.win_sad;
-                    bcost = s.best_cost;
-                    if (kind == BK_HEX6 || kind == BK_HEX3) {
-                        hdir = kind == BK_HEX6 ? w : s.bodir + w - 1;  // check_dir label; best.mv is set at hex2 exit
-                    } else {
-                        const int2 mv = batch_mv(s, w);
-                        bmx = mv.x; bmy = mv.y;
+            Gen g{0, 0, 0, 0, 0, 0, 0};
+            bool sets_mv = true, issue = false;
+            while (!issue && state != S_STORE) {
+                if (state == S_REFINE) {
+                    if (stype == 4) { g = make_gen(BK_EXH, bmx, bmy, radius, 0, 0); issue = true; state = S_BAD; }
+                    else if (stype == 3) {
+                        g = make_gen(BK_UMH, bmx, bmy, radius, 0, 0); issue = true;
+                        state = S_HEX_START; hrad = radius; hret = 0;
+                    } else if (stype == 2) { state = S_HEX_START; hrad = radius; hret = 0; }
+                    else state = S_BAD;
+                } else if (state == S_HEX_START) {
+                    hbx = bmx; hby = bmy;
+                    if (hrad > 1) { g = make_gen(BK_HEX6, hbx, hby, 0, 0, 0); sets_mv = false; issue = true; state = S_HEX_ITER; }
+                    else { g = make_gen(BK_RING, hbx, hby, 1, 1, 0); issue = true; state = hret ? S_FINAL_RING : S_BAD; }
+                } else if (state == S_HEX_ITER) {
+                    if (hi < hrad / 2 && hbx >= b.bnd0 && hby >= b.bnd1 && hbx < b.bnd2 && hby < b.bnd3) {
+                        g = make_gen(BK_HEX3, hbx, hby, 0, 0, c_mod6m1[hdir + 1]); sets_mv = false; issue = true;
+                    } else state = S_HEX_EXIT;
+                } else if (state == S_HEX_EXIT) {
+                    bmx = hbx; bmy = hby;
+                    g = make_gen(BK_RING, hbx, hby, 1, 1, 0); issue = true; state = hret ? S_FINAL_RING : S_BAD;
+                } else if (state == S_BAD) {
+                    found = bsad;
+                    const int bl = sat_i32((long long)P.coarse_bad_sad + (long long)(sat_i32((long long)P.coarse_bad_sad * bad_count) / 16));
+                    if (level > 0 && idx > 1 && P.coarse_bad_sad > 0 && (int)bsad > bl) {
+                        bad_count++;
+                        predx = imv.x; predy = imv.y;  // the block's own predictor
+                        if (P.coarse_bad_range < 0) {
+                            bad_max = -P.coarse_bad_range * L.pel; bad_r = L.pel;
+                            if (bad_r < bad_max) { g = make_gen(BK_RING, 0, 0, bad_r, L.pel, 0); issue = true; state = S_BAD_RING; }
+                            else state = S_FINAL_RING;
+                        } else if (P.coarse_bad_range > 0) {
+                            hrad = P.coarse_bad_range * L.pel; hret = 1;
+                            g = make_gen(BK_UMH, 0, 0, hrad, 0, 0); issue = true; state = S_HEX_START;
+                        } else state = S_FINAL_RING;
+                    } else state = S_STORE;
+                } else if (state == S_BAD_RING) {
+                    if (bsad < found / 4) state = S_FINAL_RING;
+                    else {
+                        bad_r += L.pel;
+                        if (bad_r < bad_max) { g = make_gen(BK_RING, 0, 0, bad_r, L.pel, 0); issue = true; }
+                        else state = S_FINAL_RING;
                     }
+                } else {  // S_FINAL_RING
+                    g = make_gen(BK_RING, bmx, bmy, 1, 1, 0); issue = true; state = S_STORE;
                 }
-                if (kind == BK_HEX6) {
-                    if (w >= 0) {
-                        hbx += c_hex2[hdir + 1].x; hby += c_hex2[hdir + 1].y; hi = 1; st = 21;
-                    } else st = 22;
-                } else if (kind == BK_HEX3) {
-                    if (w >= 0) { hbx += c_hex2[hdir + 1].x; hby += c_hex2[hdir + 1].y; hi++; st = 21; }
-                    else st = 22;
-                }
+            }
+            if (!issue) break;
+            int w;
+            eval_step(x, b, s, ph, g, lambda, predx, predy, bcost, bsad, w);
+            if (g.kind == BK_HEX6 || g.kind == BK_HEX3) {  // exact_check_dir: a label, best.mv set at exit
+                if (w >= 0) {
+                    hdir = g.kind == BK_HEX6 ? w : g.odir + w - 1;
+                    hbx += c_hex2[hdir + 1].x; hby += c_hex2[hdir + 1].y;
+                    hi = g.kind == BK_HEX6 ? 1 : hi + 1;
+                    state = S_HEX_ITER;
+                } else state = S_HEX_EXIT;
+            } else if (w >= 0 && sets_mv) {
+                const int2 m = gen_mv(g, w);
+                bmx = m.x; bmy = m.y;
             }
         }
         // ---- store (:673-679)
+        const int rows = b.py >= 0 ? imax(0, imin(b.bh, L.lh - b.py)) : 0;
+        const int cols = b.px >= 0 ? imax(0, imin(b.bw, L.lw - b.px)) : 0;
+        const unsigned cnt = (unsigned)(rows * cols);
+        unsigned dc = cnt ? dcsum / cnt : 0;
+        if (dc > 255) dc = 255;
+        const uint2 v = mkvec(bmx, bmy, smallest ? sat_mul(bsad, 3) : bsad);
         if (x.tid == 0) {
-            const int ln = s.ln - 1;  // the DC slot
-            const int rows = (s.py >= 0) ? imax(0, imin(s.bh, L.lh - s.py)) : 0;
-            const int cols = (s.px >= 0) ? imax(0, imin(s.bw, L.lw - s.px)) : 0;
-            const unsigned cnt = (unsigned)(rows * cols);
-            unsigned dc = cnt ? s.resL[ln] / cnt : 0;
-            if (dc > 255) dc = 255;
-            field[idx] = mkvec(bmx, bmy, smallest ? sat_mul(bsad, 3) : bsad);
+            field[idx] = v;
             lumaf[idx] = (uint8_t)dc;
         }
-        // the next block's leader reads field[] written above by the same thread: no barrier needed
+        last_idx = idx;
+        last_val = v;
     }
 }
-
 // exact_global_doubled (:1285-1324) over the dir's threads
 __device__ void global_doubled(const Ctx &x, DirSh &s, const uint2 *field, int64_t n, unsigned *hist) {
     int mode[2];
@@ -1084,7 +1222,7 @@ __device__ void reorder(const Ctx &x, DirSh &s, const uint2 *field, int gw, int 
     dbar(x.d);
 }
 
-__global__ void __launch_bounds__(2 * NT, 1)
+__global__ void __launch_bounds__(2 * NT, 2)
     analyse_kernel(const __grid_constant__ AnalyseParams P, const PairSrc psrc, uint8_t *__restrict__ payloads,
                    uint8_t *__restrict__ scratch, int *status) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1145,6 +1283,15 @@ __global__ void __launch_bounds__(2 * NT, 1)
         x.pel = L.pel;
         x.G.lw = L.lw; x.G.lh = L.lh; x.G.clw = L.lw / 2; x.G.clh = L.lh / 2;
         x.G.ys = P.y_stride; x.G.cs = P.c_stride; x.G.ylen = P.y_len; x.G.clen = P.c_len;
+        x.tl = L.tl;
+        x.tcp = L.tc;
+        {  // lanes per candidate: about four 4x4 tiles per lane
+            const int T = L.tl + (L.smallest ? 0 : 2 * L.tc);
+            const int want = (T + 3) / 4;
+            int g = 1;
+            while (g < want && g < 32) g <<= 1;
+            x.grp_lanes = g;
+        }
         const int gw = L.gw, gh = L.gh;
         const int64_t ncell = (int64_t)gw * gh;
         const bool first = level == P.nlevels - 1;

@@ -79,6 +79,9 @@ static void set_err(char *err, size_t n, const char *msg) {
 /* per-thread work counters: cost evaluations, luma px, chroma px */
 static _Thread_local u64 g_cnt[3];
 void or_last_counters(uint64_t out[3]) { memcpy(out, g_cnt, sizeof(g_cnt)); }
+/* per level: blocks, cost evaluations, blocks that ran the bad-SAD expansion, its evaluations */
+static _Thread_local u64 g_lvl[16][4];
+void or_level_counters(uint64_t out[64]) { memcpy(out, g_lvl, sizeof(g_lvl)); }
 
 /* ------------------------------------------------------------------ params lookups
  * Value::{int_at,bool_at,float_at}, crates/svpflow-core/src/params.rs:23-53 */
@@ -1406,8 +1409,11 @@ static int search_level(const or_planes *src, const or_planes *ref, const or_ana
                                          (edge && level == 1) ? 0 : search_type, radius);
         u32 found = best.sad;
         i32 bad_limit = sat_add_i32(o->coarse_bad_sad, sat_mul_i32(o->coarse_bad_sad, bad_count) / 16);
+        if (level < 16) g_lvl[level][1] = g_cnt[0];
         if (level > 0 && idx > 1 && o->coarse_bad_sad > 0 && (i32)best.sad > bad_limit) {
             bad_count += 1;
+            u64 e0 = g_cnt[0];
+            if (level < 16) g_lvl[level][2]++;
             ctx_t e = c; /* pred_mv of the block, not a re-anchored one */
             e.predictor = pred_mv;
             if (o->coarse_bad_range < 0) {
@@ -1421,7 +1427,9 @@ static int search_level(const or_planes *src, const or_planes *ref, const or_ana
             }
             pt center = best.mv;
             exact_expanding(&e, center, 1, 1, &best);
+            if (level < 16) g_lvl[level][3] += g_cnt[0] - e0;
         }
+        if (level < 16) { g_lvl[level][0]++; }
         field[idx].dx = (int16_t)best.mv.x;
         field[idx].dy = (int16_t)best.mv.y;
         field[idx].score = sat_mul_u32(best.sad, smallest ? 3 : 1);
@@ -1535,6 +1543,7 @@ typedef struct {
 int or_analyse_pair(const or_planes *cur, const or_planes *ref, const or_analyse_opts *o, or_vec8 *bwd_out,
                     or_vec8 *fwd_out) {
     memset(g_cnt, 0, sizeof(g_cnt));
+    memset(g_lvl, 0, sizeof(g_lvl));
     int do_bwd = (o->vectors & 1) != 0, do_fwd = (o->vectors & 2) != 0;
     /* In the bidir form fwd searches cur->ref and bwd searches ref->cur with the other
      * direction's projection as `prev`; single-direction forms pass an empty prev. */

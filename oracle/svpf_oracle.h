@@ -175,6 +175,7 @@ void or_block_cost_lc(const or_planes *src, const or_planes *ref, int32_t level,
 /* Work counters of the last or_analyse_pair on this thread (cost evaluations,
  * luma and chroma pixels compared): the algorithmic work of the control flow. */
 void or_last_counters(uint64_t out[3]);
+void or_level_counters(uint64_t out[64]);
 
 #ifdef __cplusplus
 }
