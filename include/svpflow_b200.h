@@ -101,6 +101,18 @@ int svpf_clip_analyse_device(const svpf_analyser *a, const uint8_t *supers_dev, 
 /* Status of the last device launch that used `scratch_dev` (synchronises `stream`):
  * SVPF_OK, or SVPF_EPANIC when a pair hit an input the reference cannot process. */
 int svpf_device_status(const void *scratch_dev, void *stream);
+/* No counterpart in the reference. The same Analyse over a clip as
+ * svpf_clip_analyse_device, for callers that cannot allocate device memory (a frame
+ * server's per-frame callback, where cudaMalloc can synchronise the device and stall other
+ * streams, or a host that forbids allocations after start-up): the kernel's scratch is a
+ * fixed 32 MiB array inside this library (every GPU that loads the library holds it until
+ * exit), so no scratch argument is taken and nothing is allocated. Returns SVPF_EINVAL when
+ * `count` pairs need more than that array (use fewer pairs per call). The first call on a
+ * device looks the array up (set-up); make that first call before any stream capture. Calls
+ * share the array: calls whose kernels overlap on the GPU race, so order them on one
+ * stream. Synchronises `stream` and returns the kernel's status (SVPF_OK, SVPF_EPANIC). */
+int svpf_clip_analyse_device_noalloc(const svpf_analyser *a, const uint8_t *supers_dev, int32_t nframes,
+                                     int32_t first, int32_t count, uint8_t *payloads_dev, void *stream);
 /* Whole clip from host source frames: Super over every frame, then Analyse for output
  * frames [first, first + count); payloads = count * payload_len host bytes. */
 int svpf_clip_analyse(svpf_analyser *a, const svpf_super *s, const uint8_t *frames, int32_t nframes,

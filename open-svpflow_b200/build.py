@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 CORE = os.path.join(LIB_DIR, "libsvpflow_b200.so")
-SOURCES = ["analyse.cu", "super.cu", "opts.cpp", "capi.cpp"]
+SOURCES = ["analyse.cu", "super.cu", "opts.cpp", "capi.cpp", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-v", "-cudart", "static",
          "--diag-suppress", "177"]

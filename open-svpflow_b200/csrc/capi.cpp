@@ -163,6 +163,15 @@ int read_status(const void *scratch_dev, cudaStream_t st) {
 
 }  // namespace
 
+namespace svpf {
+// internals used by noalloc.cu
+const AnalyseParams *analyser_params(const svpf_analyser *a) { return &a->P; }
+const SuperLayout *analyser_layout(const svpf_analyser *a) { return &a->L; }
+int32_t analyser_delta(const svpf_analyser *a) { return a->o.delta; }
+void set_last_error(const std::string &msg) { g_err = msg; }
+void add_launches(int n) { g_launches += n; }
+}  // namespace svpf
+
 extern "C" {
 
 const char *svpf_last_error(void) { return g_err.c_str(); }
