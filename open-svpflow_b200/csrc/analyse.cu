@@ -69,6 +69,7 @@ struct DirSh {
     int gx, gy;           // global predictor (doubled) for the next level
     int order_len;
     int abort_;
+    uint32_t srcw[384];   // the block's source pixels as words: luma (bw/4 x bh), then U and V (cw/4 x crows)
     long long r64[NW][3];
     int r32[NW][2];
 };
@@ -422,6 +423,23 @@ __device__ __forceinline__ unsigned tile_sad(const uint8_t *sp, const uint8_t *r
     for (int r = 0; r < 4; r++) s = __dp4a(__vabsdiffu4(ld4u(sp + r * st), ld4u(rp + r * st)), 0x01010101u, s);
     return s;
 }
+// Same tiles with the source rows already in shared memory as words (row pitch swp words).
+__device__ __forceinline__ unsigned tile_satd_w(const uint32_t *sw, int swp, const uint8_t *rp, int64_t st) {
+    int d[16];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const uint32_t a = sw[r * swp], b = ld4u(rp + r * st);
+#pragma unroll
+        for (int q = 0; q < 4; q++) d[r * 4 + q] = (int)((a >> (8 * q)) & 255u) - (int)((b >> (8 * q)) & 255u);
+    }
+    return hadamard4(d);
+}
+__device__ __forceinline__ unsigned tile_sad_w(const uint32_t *sw, int swp, const uint8_t *rp, int64_t st) {
+    unsigned s = 0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) s = __dp4a(__vabsdiffu4(sw[r * swp], ld4u(rp + r * st)), 0x01010101u, s);
+    return s;
+}
 __device__ __forceinline__ unsigned tile_sum(const uint8_t *sp, int64_t st) {
     unsigned s = 0;
 #pragma unroll
@@ -593,6 +611,9 @@ __device__ __noinline__ Res slow_lane(const AnalyseParams *P, const LevelInfo *L
     return r;
 }
 
+constexpr int MAXTPL = 4;  // 4x4 tiles per lane (lanes per candidate G = pow2 >= tiles / 4)
+
+
 // Work of one lane (`sub` of G) on one candidate: its share of the 4x4 tiles.
 // kind 0: block at (b.px, b.py); 1: the same mv on the block at (px, py) (general path);
 // 2: the block's luma pixel sum (block_luma_dc).
@@ -613,7 +634,10 @@ __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, 
     r.cmode = (chroma && b.cw >= 4 && b.ch >= 4) ? CM_DIRECT : CM_NONE;
     r.csatd = x.satd;
     const uint8_t *sl = x.S.y + (kind == 2 ? b.dsrc : b.lsrc);
-    for (int t = sub; t < T; t += G) {
+#pragma unroll 1
+    for (int j = 0; j < MAXTPL; j++) {
+        const int t = sub + j * G;
+        if (t >= T) break;
         if (t < TL) {
             const int ty = t / b.tilesx, tx = t - ty * b.tilesx;
             const int64_t o = (int64_t)ty * 4 * ys + tx * 4;
@@ -693,22 +717,55 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                     rem -= c;
                 }
             }
-            Res r{0, 0, 0, 0, 0, 0};
             int2 mv = make_int2(0, 0);
+            int64_t lref = 0, cref = 0;
+            bool fast = false;
+            Res r{0, 0, 0, 0, 0, 0};
+            long long motion = 0;
             if (act) {
                 mv = gen_mv(g, i);
-                r = eval_lane(x, b, 0, 0, 0, mv.x, mv.y, b.chroma != 0, sub);
+                motion = motion_penalty(lambda, predx, predy, mv.x, mv.y);
+                fast = fast_setup(x, b, mv.x, mv.y, lref, cref);
+                if (!fast)
+                    r = slow_lane(x.P, x.L, x.G, x.S, x.R, x.level, b.px, b.py, b.bw, b.bh, mv.x, mv.y, b.chroma != 0,
+                                  x.satd, x.pel, false, sub, G, x.tl, x.tcp);
+            }
+            // this lane's 4x4 tiles: luma, then U, then V (the source block is staged in shared memory)
+            if (act && fast) {
+                r.lsatd = b.satd_mode;
+                r.cmode = (b.chroma && b.cw >= 4 && b.ch >= 4) ? CM_DIRECT : CM_NONE;
+                r.csatd = x.satd;
+                const int T = x.tl + (r.cmode != CM_NONE ? 2 * x.tcp : 0);
+                const int swp = b.tilesx, cwp = b.ctilesx, nlw = b.tilesx * b.bh;
+#pragma unroll 1
+                for (int t = sub; t < T; t += G) {
+                    if (t < x.tl) {
+                        const int ty = t / swp, tx = t - ty * swp;
+                        const uint8_t *rp = x.R.y + lref + (int64_t)ty * 4 * x.G.ys + tx * 4;
+                        const uint32_t *sw = s.srcw + ty * 4 * swp + tx;
+                        r.L += b.satd_mode ? tile_satd_w(sw, swp, rp, x.G.ys) : tile_sad_w(sw, swp, rp, x.G.ys);
+                    } else {
+                        const int ct0 = t - x.tl;
+                        const int pl = ct0 >= x.tcp;
+                        const int ct = ct0 - pl * x.tcp;
+                        const int ty = ct / cwp, tx = ct - ty * cwp;
+                        if (ty * 4 >= b.crows) continue;
+                        const uint8_t *rp = (pl ? x.R.v : x.R.u) + cref + (int64_t)ty * 4 * x.G.cs + tx * 4;
+                        const uint32_t *sw = s.srcw + nlw + pl * cwp * b.crows + ty * 4 * cwp + tx;
+                        const unsigned v = x.satd ? tile_satd_w(sw, cwp, rp, x.G.cs) : tile_sad_w(sw, cwp, rp, x.G.cs);
+                        if (pl) r.V += v; else r.U += v;
+                    }
+                }
             }
             r.L = group_sum(r.L, G);
             r.U = group_sum(r.U, G);
             r.V = group_sum(r.V, G);
-            long long K = 0x7FFFFFFFFFFFFFFFLL, motion = 0;
+            long long K = 0x7FFFFFFFFFFFFFFFLL;
             unsigned sad = 0;
             if (act) {
                 unsigned L, C;
                 finalize(r, L, C);
                 if (!b.chroma) C = 0;
-                motion = motion_penalty(lambda, predx, predy, mv.x, mv.y);
                 K = motion + pen(pnew, L) + (b.chroma ? pen(pnew, C) : 0LL);  // :1158-1221
                 sad = sat_add(L, C);
             }
@@ -902,6 +959,22 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
         const int2 imv = vmv(interp);
         BlkC b;
         make_blk(x, px, py, !smallest, b);
+        // stage the source block for the refinement steps (read after the next barrier)
+        if (b.fast_src) {
+            const int nlw = b.tilesx * b.bh;
+            for (int t = x.tid; t < nlw; t += NT) {
+                const int row = t / b.tilesx, col = t - row * b.tilesx;
+                s.srcw[t] = ld4u(x.S.y + b.lsrc + (int64_t)row * x.G.ys + col * 4);
+            }
+            if (b.chroma && b.cfast_src) {
+                const int nc = b.ctilesx * b.crows;
+                for (int t = x.tid; t < 2 * nc; t += NT) {
+                    const int pl = t >= nc, u = t - pl * nc;
+                    const int row = u / b.ctilesx, col = u - row * b.ctilesx;
+                    s.srcw[nlw + t] = ld4u((pl ? x.S.v : x.S.u) + b.csrc + (int64_t)row * x.G.cs + col * 4);
+                }
+            }
+        }
         // ---- special candidates (exact_search_block, :708-746): slot list in the
         // reference's evaluation roles; slot j is evaluated by group j
         int n = 0, rs_slot = -1, prev_slot = -1, nseeds = 0;
@@ -921,15 +994,25 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
         const int gxv = s.gx, gyv = s.gy;
         int sdx[8], sdy[8];
         bool panic = false;
+        // the 3x3 neighbourhood: positions in the order and current vectors, loaded together
+        int64_t npos[9];
+        uint2 nval[9];
 #pragma unroll
         for (int q = 0; q < 9; q++) {
             const int ny = by - 1 + q / 3, nx = bx - 1 + q % 3;
+            npos[q] = 0x7FFFFFFFFFFFFFFFLL;
+            nval[q] = make_uint2(0, 0);
             if (ny < 0 || ny >= gh || nx < 0 || nx >= gw) continue;
             const int64_t ci = (int64_t)ny * gw + nx;
-            const int64_t p = level == 0 ? initial_order_pos(gw, gh, nx, ny) : (int64_t)ds.pos[ci];
+            npos[q] = level == 0 ? initial_order_pos(gw, gh, nx, ny) : (int64_t)ds.pos[ci];
+            nval[q] = ci == last_idx ? last_val : field[ci];
+        }
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            const int64_t p = npos[q];
             if (p < k) {
                 if (nseeds >= 8) { panic = true; continue; }  // seeds[8] overflows: the reference panics
-                const int2 nm = vmv(ci == last_idx ? last_val : field[ci]);
+                const int2 nm = vmv(nval[q]);
 #pragma unroll
                 for (int t = 0; t < 8; t++)
                     if (t == nseeds) { sdx[t] = nm.x; sdy[t] = nm.y; }

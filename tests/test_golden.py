@@ -1,0 +1,35 @@
+"""Frozen digests (tests/golden/oracle_digests.json, made by tests/golden/make_golden.py):
+the oracle must keep producing them (CPU), and the GPU path must produce the same bytes."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from golden.make_golden import CASES, compute
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = json.load(open(os.path.join(HERE, "golden", "oracle_digests.json")))["cases"]
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_matches_frozen_digests(name):
+    assert compute(name) == GOLD[name]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_gpu_matches_frozen_digests(name):
+    import svpflow_b200 as sv
+    from svpflow_b200.synth import make_clip
+
+    w, h, n, seed, kw, sopt, aopt = CASES[name]
+    clip = make_clip(w, h, n, seed=seed, **kw)
+    sb = sv.Super(w, h, sopt)
+    an = sv.Analyse(sb.sdata, aopt, w, h)
+    supers = sb.build_many(clip)
+    pays = an.analyse_clip(sb, clip)
+    d = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+    assert [d(supers[i]) for i in range(n)] == GOLD[name]["super"]
+    assert [d(pays[i]) for i in range(n)] == GOLD[name]["payload"]
