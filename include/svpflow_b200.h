@@ -122,6 +122,72 @@ int svpf_clip_analyse(svpf_analyser *a, const svpf_super *s, const uint8_t *fram
 int64_t svpf_kernel_launches(void);
 void svpf_kernel_launches_reset(void);
 
+/* ---------------------------------------------------------------- batched form */
+/* No counterpart in the reference, which analyses one clip at a time, one output frame
+ * per getFrame call (crates/svpflow1/src/analyse_filter.rs:229-334). A batch holds many
+ * clips of any size and length (each with its own Super and Analyse handles, as for
+ * svpf_clip_analyse) and analyses every output frame of every clip in one persistent
+ * launch replayed from a CUDA graph; each payload is byte-identical to the per-clip
+ * call's. Creation allocates all device memory of the batch (svpf_batch_device_bytes):
+ * the clips' source frames, super frames and payloads plus the work list and scratch.
+ * A batch serialises its own calls. */
+typedef struct svpf_batch svpf_batch;
+int svpf_batch_create(int32_t nclips, const svpf_super *const *supers, const svpf_analyser *const *analysers,
+                      const int32_t *nframes, svpf_batch **out);
+void svpf_batch_destroy(svpf_batch *b);
+int32_t svpf_batch_clips(const svpf_batch *b);
+int64_t svpf_batch_pairs(const svpf_batch *b);           /* output frames over all clips */
+size_t svpf_batch_device_bytes(const svpf_batch *b);
+/* Device address of clip `clip`'s source frames (nframes packed I420 frames, in order),
+ * for callers that fill them on the device; NULL for a bad index. */
+uint8_t *svpf_batch_frames_device(svpf_batch *b, int32_t clip);
+/* Device address of clip `clip`'s payloads (nframes x payload_len bytes). */
+const uint8_t *svpf_batch_payloads_device(const svpf_batch *b, int32_t clip);
+/* Host buffers in and out: copies every clip's frames in, runs, copies every payload
+ * out, synchronises and returns the first failing clip's status. */
+int svpf_batch_run(svpf_batch *b, const uint8_t *const *frames, uint8_t *const *payloads);
+/* Device-resident form: replays the run on `stream` over the frames already in place;
+ * NULL means the batch's own stream, not the legacy default stream. svpf_batch_status
+ * synchronises that stream and reports. */
+int svpf_batch_launch(svpf_batch *b, void *stream);
+int svpf_batch_status(svpf_batch *b, void *stream);
+/* Launch shape: compiled variant (threads per search direction, see
+ * svpf_analyse_variant_name) and 4x4 tiles per lane (2, 4 or 8). Results do not depend
+ * on it. svpf_batch_autotune times the shapes on the batch's largest pairs (frames must be
+ * in place), keeps the fastest and remembers it per device and clip mix (and in the file
+ * named by the SVPF_TUNE_CACHE environment variable, when set). */
+int svpf_batch_set_shape(svpf_batch *b, int32_t variant, int32_t tiles_per_lane);
+const char *svpf_batch_shape(const svpf_batch *b, int32_t *variant, int32_t *tiles_per_lane, int32_t *grid);
+int svpf_batch_autotune(svpf_batch *b, int32_t *variant, int32_t *tiles_per_lane, double *pairs_per_s);
+int32_t svpf_batch_graph_launches(const svpf_batch *b);  /* kernels in one replay */
+int32_t svpf_analyse_variant_count(void);
+const char *svpf_analyse_variant_name(int32_t i);
+
+/* ---------------------------------------------------------------- served form */
+/* No counterpart in the reference. A server analyses clips that arrive over time with
+ * continuous batching: a scheduler thread admits submitted clips in arrival order while
+ * their device memory fits `hbm_budget_bytes` and fewer than `max_active` clips are in
+ * flight; each admitted clip runs on its own stream (frames in, Super, Analyse in chunks
+ * of `chunk_pairs` output frames, each chunk's payloads out as it completes), overlapping
+ * on the device with the others. Payloads are byte-identical to svpf_clip_analyse's. */
+typedef struct svpf_server svpf_server;
+int svpf_server_create(size_t hbm_budget_bytes, int32_t max_active, int32_t chunk_pairs, svpf_server **out);
+/* Stops admitting, waits for the admitted clips; clips never admitted fail. */
+void svpf_server_destroy(svpf_server *s);
+/* Queues a clip: `frames` (nframes packed I420 frames) and `payloads` (nframes x
+ * payload_len bytes) are host buffers that must stay valid until svpf_server_wait
+ * returns (pinned memory lets the copies run asynchronously). When `pair_done_ns` is
+ * given (nframes entries), entry n receives the server-clock time at which payload n
+ * reached host memory. The Super and Analyse handles must outlive the request. */
+int svpf_server_submit(svpf_server *s, const svpf_super *sup, const svpf_analyser *an, const uint8_t *frames,
+                       int32_t nframes, uint8_t *payloads, int64_t *pair_done_ns, int64_t *request);
+/* Blocks until the request finished and returns its status; times[0..2] (optional)
+ * receive its arrival, admission and completion times on the server clock. */
+int svpf_server_wait(svpf_server *s, int64_t request, int64_t *times);
+int64_t svpf_server_now_ns(const svpf_server *s);       /* the server clock, ns */
+void svpf_server_stats(svpf_server *s, int64_t *admitted, int64_t *completed, int64_t *peak_device_bytes,
+                       int32_t *peak_active, int64_t *kernel_launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,4 +1,10 @@
-// analyse.cu -- hierarchical block search (Analyse) on sm_100a.
+// analyse_body.cuh -- hierarchical block search (Analyse) on sm_100a.
+//
+// Included by one translation unit per launch variant (analyse_nt128.cu, analyse_nt64.cu,
+// analyse_nt32.cu): SVPF_NT = threads per search direction, SVPF_MINB = resident CTAs per
+// SM the register budget is cut for, SVPF_VARIANT = the variant's namespace. Each variant
+// exports a plain launcher (one CTA per pair) and a persistent batch launcher (CTAs
+// drain a device work queue of frame pairs from many clips).
 //
 // Restates crates/svpflow1/src/analyse_search.rs:68-2811 for the GPU:
 //   * one CTA per frame pair; its two halves (NT threads each) run the forward search
@@ -33,11 +39,17 @@
 
 #include "svpf_device.h"
 
+#if !defined(SVPF_NT) || !defined(SVPF_MINB) || !defined(SVPF_VARIANT)
+#error "define SVPF_NT, SVPF_MINB and SVPF_VARIANT before including analyse_body.cuh"
+#endif
+
 namespace svpf {
+namespace SVPF_VARIANT {
 
 namespace {
 
-constexpr int NT = 128;            // threads per search direction
+constexpr int NT = SVPF_NT;        // threads per search direction
+static_assert(NT == 32 || NT == 64 || NT == 128, "threads per direction");
 constexpr int NW = NT / 32;
 constexpr int NGMAX = NW * 32;     // candidate groups of a direction when a group is one lane
 constexpr int MAXSLOT = 16;        // special-candidate slots of a block
@@ -611,8 +623,6 @@ __device__ __noinline__ Res slow_lane(const AnalyseParams *P, const LevelInfo *L
     return r;
 }
 
-constexpr int MAXTPL = 4;  // 4x4 tiles per lane (lanes per candidate G = pow2 >= tiles / 4)
-
 
 // Work of one lane (`sub` of G) on one candidate: its share of the 4x4 tiles.
 // kind 0: block at (b.px, b.py); 1: the same mv on the block at (px, py) (general path);
@@ -635,9 +645,7 @@ __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, 
     r.csatd = x.satd;
     const uint8_t *sl = x.S.y + (kind == 2 ? b.dsrc : b.lsrc);
 #pragma unroll 1
-    for (int j = 0; j < MAXTPL; j++) {
-        const int t = sub + j * G;
-        if (t >= T) break;
+    for (int t = sub; t < T; t += G) {
         if (t < TL) {
             const int ty = t / b.tilesx, tx = t - ty * b.tilesx;
             const int64_t o = (int64_t)ty * 4 * ys + tx * 4;
@@ -1305,30 +1313,21 @@ __device__ void reorder(const Ctx &x, DirSh &s, const uint2 *field, int gw, int 
     dbar(x.d);
 }
 
-__global__ void __launch_bounds__(2 * NT, 2)
-    analyse_kernel(const __grid_constant__ AnalyseParams P, const PairSrc psrc, uint8_t *__restrict__ payloads,
-                   uint8_t *__restrict__ scratch, int *status) {
+// One frame pair, both directions: the whole of analyse_pair (:68-226) plus the payload
+// (:2740-2811). Called by every thread of the CTA; threads of a direction the
+// configuration does not search (vectors 1 or 2 under a 2-direction batch CTA) only
+// take part in the CTA-wide barriers. Status bits go to *status.
+__device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const PairRef pr, uint8_t *__restrict__ pay,
+                                                 uint8_t *__restrict__ scr, int *status, int &cta_abort) {
     extern __shared__ __align__(16) unsigned char smem[];
     const bool bidir = P.vectors == 3;
-    const int half = bidir ? (int)(threadIdx.x / NT) : 0;
+    const int half = (int)(threadIdx.x / NT);
+    const bool idle = !bidir && half == 1;
     const int d = bidir ? half : ((P.vectors & 2) ? 0 : 1);  // 0 = forward (cur -> ref), 1 = backward
     const int tid = threadIdx.x % NT;
     DirSh &s = reinterpret_cast<DirSh *>(smem)[half];
-    __shared__ int cta_abort;
-    const int64_t pair = blockIdx.x;
-    PairRef pr;
-    if (psrc.table) {
-        pr = psrc.table[pair];
-    } else {  // analyse_filter.rs:277-282: frame n pairs with min(n + delta, num_frames - 1)
-        const int64_t n = (int64_t)psrc.first + pair;
-        int64_t n2 = n + psrc.delta;
-        if (n2 > psrc.nframes - 1) n2 = psrc.nframes - 1;
-        pr.cur = psrc.clip + n * psrc.frame_bytes;
-        pr.ref = psrc.clip + n2 * psrc.frame_bytes;
-    }
     const uint8_t *src = d == 0 ? pr.cur : pr.ref;
     const uint8_t *ref = d == 0 ? pr.ref : pr.cur;
-    uint8_t *scr = scratch + pair * P.scratch_per_pair;
     DirScratch ds;
     ds.vec[0] = (uint2 *)(scr + P.off_field[d]);
     ds.vec[1] = (uint2 *)(scr + P.off_next[d]);
@@ -1349,7 +1348,7 @@ __global__ void __launch_bounds__(2 * NT, 2)
     x.S = Planes{src, src + P.y_len, src + P.y_len + P.c_len};
     x.R = Planes{ref, ref + P.y_len, ref + P.y_len + P.c_len};
     if (threadIdx.x == 0) cta_abort = 0;
-    if (tid == 0) { s.abort_ = 0; s.gx = 0; s.gy = 0; s.order_len = 0; }
+    if (tid == 0) { s.abort_ = idle ? 2 : 0; s.gx = 0; s.gy = 0; s.order_len = 0; }
     __syncthreads();
     const uint2 *other_proj[2] = {nullptr, nullptr};
     {
@@ -1368,9 +1367,10 @@ __global__ void __launch_bounds__(2 * NT, 2)
         x.G.ys = P.y_stride; x.G.cs = P.c_stride; x.G.ylen = P.y_len; x.G.clen = P.c_len;
         x.tl = L.tl;
         x.tcp = L.tc;
-        {  // lanes per candidate: about four 4x4 tiles per lane
+        {  // lanes per candidate: about `tiles_per_lane` 4x4 tiles per lane
             const int T = L.tl + (L.smallest ? 0 : 2 * L.tc);
-            const int want = (T + 3) / 4;
+            const int tpl = iclamp(P.tiles_per_lane, 1, 8);
+            const int want = (T + tpl - 1) / tpl;
             int g = 1;
             while (g < want && g < 32) g <<= 1;
             x.grp_lanes = g;
@@ -1501,16 +1501,15 @@ __global__ void __launch_bounds__(2 * NT, 2)
             reorder(x, s, f, gw, gh, ds, status);
         }
         pgw = gw; pgh = gh;
-        if (tid == 0 && s.abort_) cta_abort = 1;
+        if (tid == 0 && s.abort_ == 1) cta_abort = 1;
         __syncthreads();
     }
-    if (cta_abort) return;
+    if (cta_abort || idle) return;
     // ---- refine pass (exact_recalculate :1326-1451) runs on the host-selected configs only
     // ---- rescale_scores (:2716-2738) + pack_vector_frame (:2740-2811)
     const uint2 *f = ds.vec[0];
     const uint8_t *fl = ds.luma[0];
     const int64_t count = (int64_t)P.out_gw * P.out_gh;
-    uint8_t *pay = payloads + pair * P.payload_len;
     const int64_t region = bidir ? (d == 1 ? 0x40 : 0x40 + 4 + count * 8) : 0x40;
     if (threadIdx.x == 0) {
         for (int i = 0; i < 16; i++) reinterpret_cast<int *>(pay)[i] = P.header[i];
@@ -1537,148 +1536,92 @@ __global__ void __launch_bounds__(2 * NT, 2)
     }
 }
 
+__global__ void __launch_bounds__(2 * NT, SVPF_MINB)
+    analyse_kernel(const __grid_constant__ AnalyseParams P, const PairSrc psrc, uint8_t *__restrict__ payloads,
+                   uint8_t *__restrict__ scratch, int *status) {
+    __shared__ int cta_abort;
+    const int64_t pair = blockIdx.x;
+    PairRef pr;
+    if (psrc.table) {
+        pr = psrc.table[pair];
+    } else {  // analyse_filter.rs:277-282: frame n pairs with min(n + delta, num_frames - 1)
+        const int64_t n = (int64_t)psrc.first + pair;
+        int64_t n2 = n + psrc.delta;
+        if (n2 > psrc.nframes - 1) n2 = psrc.nframes - 1;
+        pr.cur = psrc.clip + n * psrc.frame_bytes;
+        pr.ref = psrc.clip + n2 * psrc.frame_bytes;
+    }
+    analyse_pair_dev(P, pr, payloads + pair * P.payload_len, scratch + pair * P.scratch_per_pair, status, cta_abort);
+}
+
+// Persistent form: a grid sized to the resident CTAs drains the item list in order (the
+// host sorts it largest-first); each CTA pulls the next item with one atomic, copies the
+// item's clip parameters into shared memory and runs the pair on its own scratch slot.
+__global__ void __launch_bounds__(2 * NT, SVPF_MINB)
+    analyse_batch_kernel(const AnalyseParams *__restrict__ clips, const BatchItem *__restrict__ items, int nitems,
+                         unsigned *__restrict__ next_item, uint8_t *__restrict__ scratch, int64_t scratch_per_cta,
+                         int *__restrict__ clip_status) {
+    __shared__ int cta_abort;
+    __shared__ int item_sh;
+    __shared__ __align__(16) AnalyseParams P;
+    uint8_t *scr = scratch + (int64_t)blockIdx.x * scratch_per_cta;
+    for (;;) {
+        if (threadIdx.x == 0) item_sh = (int)atomicAdd(next_item, 1u);
+        __syncthreads();
+        const int it = item_sh;
+        if (it >= nitems) break;
+        const BatchItem bi = items[it];
+        {
+            const int4 *src = reinterpret_cast<const int4 *>(clips + bi.clip);
+            int4 *dst = reinterpret_cast<int4 *>(&P);
+            for (int i = threadIdx.x; i < (int)(sizeof(AnalyseParams) / 16); i += blockDim.x) dst[i] = src[i];
+        }
+        __syncthreads();
+        analyse_pair_dev(P, bi.pair, bi.payload, scr, clip_status + bi.clip, cta_abort);
+        __syncthreads();  // P, item_sh and the shared search state are reused by the next item
+    }
+}
+
 }  // namespace
 
-cudaError_t launch_analyse(const AnalyseParams &P, const PairSrc &psrc, int npairs, uint8_t *payloads,
-                           uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches) {
+size_t dir_shared_bytes() { return sizeof(DirSh); }
+
+cudaError_t prepare() {
+    static cudaError_t once = [] {
+        const int smem = (int)(2 * sizeof(DirSh));
+        cudaError_t e = cudaFuncSetAttribute(analyse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(analyse_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        return e;
+    }();
+    return once;
+}
+
+cudaError_t launch_plain(const AnalyseParams &P, const PairSrc &psrc, int npairs, uint8_t *payloads, uint8_t *scratch,
+                         int *status_dev, cudaStream_t stream, int *launches) {
     if (npairs <= 0) return cudaSuccess;
+    if (cudaError_t e = prepare()) return e;
     const int ndir = P.vectors == 3 ? 2 : 1;
-    const size_t smem = sizeof(DirSh) * ndir;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(analyse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sizeof(DirSh)));
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
-    analyse_kernel<<<npairs, NT * ndir, smem, stream>>>(P, psrc, payloads, scratch, status_dev);
+    analyse_kernel<<<npairs, NT * ndir, sizeof(DirSh) * ndir, stream>>>(P, psrc, payloads, scratch, status_dev);
     if (launches) *launches += 1;
     return cudaGetLastError();
 }
 
-size_t analyse_dir_shared_bytes() { return sizeof(DirSh); }
-
-// -------------------------------------------------------------------------------------------
-bool build_analyse_params(const AnalyseOpts &o, const SuperLayout &Lay, AnalyseParams &P, std::string &err) {
-    memset(&P, 0, sizeof(P));
-    if (o.levels < 1 || o.levels > kMaxLevels) { err = "unsupported level count"; return false; }
-    if (!Lay.full) { err = "SVAnalyse: the super clip must hold the finest level (full=true)"; return false; }
-    P.nlevels = o.levels;
-    P.block_w = o.block_w; P.block_h = o.block_h; P.ox = o.overlap_x; P.oy = o.overlap_y;
-    P.step_x = o.block_w - o.overlap_x > 1 ? o.block_w - o.overlap_x : 1;
-    P.step_y = o.block_h - o.overlap_y > 1 ? o.block_h - o.overlap_y : 1;
-    P.pnew = o.pnew; P.prev = o.prev; P.pzero = o.pzero; P.pglobal = o.pglobal; P.pnbour = o.pnbour;
-    P.distance = o.distance; P.coarse_bad_sad = o.coarse_bad_sad; P.coarse_bad_range = o.coarse_bad_range;
-    P.coarse_distance = o.coarse_distance; P.vectors = o.vectors;
-    P.luma_w = o.width; P.luma_h = o.height; P.pel = o.pel;
-    P.y_stride = Lay.y_stride; P.c_stride = Lay.c_stride; P.y_len = Lay.y_len; P.c_len = Lay.c_len;
-    P.frame_bytes = Lay.frame_bytes;
-    P.lambda = o.lambda;
-    // per level
-    int64_t max_cells = 1, max_order = 1;
-    for (int lv = 0; lv < o.levels; lv++) {
-        LevelInfo &L = P.lv[lv];
-        level_grid(o, lv, L.gw, L.gh);
-        L.lw = reduce_dim(o.width, lv);
-        L.lh = reduce_dim(o.height, lv);
-        int64_t y = 0, c = 0;  // level_y_offset / chroma_level_offset (:49-58, :2704-2713)
-        for (int k = 0; k < lv; k++) {
-            const int64_t h = reduce_dim(Lay.height, k);
-            const int64_t sub = (k == 0 && Lay.full) ? (int64_t)Lay.pel * Lay.pel : 1;
-            y += h * sub;
-            const int64_t hc = h / 2;
-            c += (hc > 1 ? hc : 1) * sub;
-        }
-        L.y_off = y; L.c_off = c;
-        L.pel = lv == 0 ? (o.pel > 1 ? o.pel : 1) : 1;
-        L.smallest = lv == o.levels - 1;
-        // exact_lambda (:1279-1283), f64: lambda / plevel^(levels-level-1) / pel^2
-        {
-            double a = o.plevel, r = 1.0;
-            int b = o.levels - lv - 1;
-            for (;;) {  // compiler-rt __powidf2 order
-                if (b & 1) r *= a;
-                b /= 2;
-                if (b == 0) break;
-                a *= a;
-            }
-            const double v = (double)o.lambda / r / (double)((L.pel * L.pel) > 1 ? L.pel * L.pel : 1);
-            int32_t iv;
-            if (v != v) iv = 0;
-            else if (v >= 2147483647.0) iv = INT32_MAX;
-            else if (v <= -2147483648.0) iv = INT32_MIN;
-            else iv = (int32_t)v;
-            L.lambda_base = L.smallest ? 0 : iv;
-        }
-        L.lsad = L.smallest ? o.lsad / 3 : o.lsad;
-        L.satd = lv == 0 ? o.fine_satd : o.coarse_satd;
-        L.search_type = lv == 0 ? o.search_type : o.coarse_search_type;
-        {  // search_radius (:1465-1476)
-            const int dd = lv == 0 ? o.distance : o.coarse_distance;
-            const int nl = o.levels > 1 ? o.levels : 1;
-            L.base_radius = dd == 0 ? ((lv == 0 && nl > 1) ? 0 : 10) : (dd < 0 ? -dd : dd);
-        }
-        if (L.smallest) {
-            L.bw = o.block_w >> 1; L.bh = o.block_h >> 1; L.pxoff = o.block_w >> 2; L.pyoff = o.block_h >> 2;
-        } else {
-            L.bw = o.block_w; L.bh = o.block_h; L.pxoff = 0; L.pyoff = 0;
-        }
-        L.tl = ((L.bw + 3) / 4) * ((L.bh + 3) / 4);
-        const int cw = L.bw / 2, ch = L.bh / 2;
-        L.tc = cw > 0 ? ((cw + 3) / 4) * (((cw > ch ? cw : ch) + 3) / 4) : 0;
-        const int64_t cells = (int64_t)L.gw * L.gh;
-        if (cells > max_cells) max_cells = cells;
-        const int64_t ol = cells + L.gw + L.gh + 8;
-        if (ol > max_order) max_order = ol;
-        if (L.tl + L.tc > 96 || L.gw > 65535 || L.gh > 65535) { err = "unsupported block / grid size"; return false; }
-    }
-    {  // level-0 grid must be at least 2x2: below that the reference indexes field[-1]
-        if (P.lv[0].gw < 2 || P.lv[0].gh < 2) { err = "SVAnalyse: frame too small for the block grid"; return false; }
-    }
-    int32_t bw, bh, ox, oy, gw, gh;
-    output_block(o, bw, bh, ox, oy);
-    output_grid(o, bw, bh, ox, oy, gw, gh);
-    P.out_bw = bw; P.out_bh = bh; P.out_ox = ox; P.out_oy = oy; P.out_gw = gw; P.out_gh = gh;
-    P.has_refine = o.has_refine_thsad;
-    if (P.has_refine) { err = "refine (recalculate) pass is not available on the device path yet"; return false; }
-    {  // rescale_scores denominators (:2716-2721)
-        double f = sqrt((double)o.width * (double)o.width + (double)o.height * (double)o.height);
-        int32_t diag = f != f ? 0 : (f >= 2147483647.0 ? INT32_MAX : (int32_t)f);
-        if (diag < 0) diag = 0;
-        int64_t den = (int64_t)diag * (bw > 1 ? bw : 1);
-        if (den > INT32_MAX) den = INT32_MAX;
-        P.rescale_denom = den > 1 ? (int32_t)den : 1;
-    }
-    P.payload_len = (int64_t)payload_len(o);
-    int32_t hdr[16];
-    vdata_header(o, hdr);
-    // payload words: 16, 0xA0, flags, bw, bh, pel, levels, 0, w, h, ox, oy, gw, gh, selector, delta
-    P.header[0] = 16; P.header[1] = 0xA0; P.header[2] = hdr[1]; P.header[3] = bw; P.header[4] = bh;
-    P.header[5] = o.pel; P.header[6] = hdr[5]; P.header[7] = 0; P.header[8] = o.width; P.header[9] = o.height;
-    P.header[10] = ox; P.header[11] = oy; P.header[12] = gw; P.header[13] = gh; P.header[14] = o.selector;
-    P.header[15] = o.delta;
-    if ((int64_t)gw * gh != (int64_t)P.lv[0].gw * P.lv[0].gh) { err = "output grid differs from the level-0 grid"; return false; }
-    // scratch layout per pair
-    int64_t np2 = 1;
-    while (np2 < max_cells) np2 <<= 1;
-    P.max_cells = max_cells;
-    P.max_order = max_order;
-    int64_t off = 0;
-    auto take = [&](int64_t bytes) { int64_t o_ = off; off += (bytes + 255) & ~(int64_t)255; return o_; };
-    for (int dd = 0; dd < 2; dd++) {
-        P.off_field[dd] = take(max_cells * 8);
-        P.off_next[dd] = take(max_cells * 8);
-        P.off_proj[dd][0] = take(max_cells * 8);
-        P.off_proj[dd][1] = take(max_cells * 8);
-        P.off_order[dd] = take(max_order * 4);
-        P.off_order2[dd] = take(max_order * 4);
-        P.off_pos[dd] = take(max_cells * 4);
-        P.off_keys[dd] = take(np2 * 8 > max_order * 4 ? np2 * 8 : max_order * 4);
-        P.off_hist[dd] = take(65536 * 4);
-        P.off_seen[dd] = take(max_cells);
-        P.off_out[dd] = take(max_cells * 2);
-    }
-    P.scratch_per_pair = off;
-    return true;
+cudaError_t batch_blocks_per_sm(int *blocks) {
+    if (cudaError_t e = prepare()) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, analyse_batch_kernel, 2 * NT, 2 * sizeof(DirSh));
 }
 
+cudaError_t launch_batch(const AnalyseParams *clips_dev, const BatchItem *items_dev, int nitems, unsigned *next_item_dev,
+                         uint8_t *scratch, int64_t scratch_per_cta, int *clip_status_dev, int grid, cudaStream_t stream,
+                         int *launches) {
+    if (nitems <= 0 || grid <= 0) return cudaSuccess;
+    if (cudaError_t e = prepare()) return e;
+    analyse_batch_kernel<<<grid, 2 * NT, 2 * sizeof(DirSh), stream>>>(clips_dev, items_dev, nitems, next_item_dev,
+                                                                      scratch, scratch_per_cta, clip_status_dev);
+    if (launches) *launches += 1;
+    return cudaGetLastError();
+}
+
+}  // namespace SVPF_VARIANT
 }  // namespace svpf

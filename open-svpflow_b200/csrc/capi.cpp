@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/svpflow_b200.h"
+#include "handles.h"
 #include "svpf_device.h"
 
 using namespace svpf;
@@ -164,7 +165,12 @@ int read_status(const void *scratch_dev, cudaStream_t st) {
 }  // namespace
 
 namespace svpf {
-// internals used by noalloc.cu
+// internals used by the other host translation units (handles.h)
+const SuperOpts *super_opts_of(const svpf_super *s) { return &s->so; }
+const SuperLayout *super_layout_of(const svpf_super *s) { return &s->L; }
+const SuperDev *super_dev_of(const svpf_super *s) { return &s->D; }
+const AnalyseOpts *analyser_opts(const svpf_analyser *a) { return &a->o; }
+int require_device() { return check_device(); }
 const AnalyseParams *analyser_params(const svpf_analyser *a) { return &a->P; }
 const SuperLayout *analyser_layout(const svpf_analyser *a) { return &a->L; }
 int32_t analyser_delta(const svpf_analyser *a) { return a->o.delta; }

@@ -21,6 +21,7 @@
 #include <string>
 
 #include "../../include/svpflow_b200.h"
+#include "handles.h"
 #include "svpf_device.h"
 
 namespace {
@@ -35,15 +36,6 @@ std::mutex g_setup_mu;
 unsigned char *g_scratch_addr[kMaxDevices] = {};
 
 }  // namespace
-
-namespace svpf {
-// internals of capi.cpp
-const AnalyseParams *analyser_params(const svpf_analyser *a);
-const SuperLayout *analyser_layout(const svpf_analyser *a);
-int32_t analyser_delta(const svpf_analyser *a);
-void set_last_error(const std::string &msg);
-void add_launches(int n);
-}  // namespace svpf
 
 namespace {
 

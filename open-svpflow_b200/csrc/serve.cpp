@@ -1,0 +1,345 @@
+// serve.cpp -- the served form: a request loop with continuous batching.
+//
+// Clips arrive at any time (svpf_server_submit). A scheduler thread admits them in
+// arrival order while the device memory they need fits the server's HBM budget and an
+// execution slot is free. An admitted clip gets a stream of its own and, in stream
+// order: its source frames copied in, its super frames built (kept resident for all of
+// its pairs: every super frame serves two adjacent pairs), its frame pairs analysed in
+// chunks of `chunk_pairs`, each chunk's payloads copied out as soon as it finishes, and
+// its memory released. Chunks of different clips run concurrently on the device, so a
+// clip admitted while others are being analysed starts at once, and one that finishes
+// frees its slot and memory for the next. Memory comes from the stream-ordered pool
+// (cudaMallocAsync / cudaFreeAsync), so admission never synchronises the device.
+//
+// Per-pair completion times are taken by a host function queued behind each chunk's
+// payload copy: the time the payload is in host memory. A clip's arrival time is taken at
+// submit, so pair latency = done - arrival includes queueing for admission.
+//
+// Results do not depend on the mix: every pair runs the same kernel on its own two super
+// frames, whatever else shares the device.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/svpflow_b200.h"
+#include "handles.h"
+#include "svpf_device.h"
+
+using namespace svpf;
+
+namespace {
+
+inline int64_t al256(int64_t v) { return (v + 255) & ~(int64_t)255; }
+
+struct Request;
+
+struct Chunk {
+    Request *req;
+    int32_t first, count;
+};
+
+struct Request {
+    int64_t id = 0;
+    SuperDev D;
+    AnalyseParams P;
+    int32_t nframes = 0, delta = 1;
+    const uint8_t *frames = nullptr;
+    uint8_t *payloads = nullptr;
+    int64_t *pair_done_ns = nullptr;
+    int64_t arrival_ns = 0, admit_ns = 0, done_ns = 0;
+    int64_t need = 0;
+    int slot = -1;
+    uint8_t *dev = nullptr;
+    int *status_host = nullptr;  // pinned
+    int status = 0;
+    bool done = false;
+    std::vector<Chunk> chunks;
+    std::atomic<int> chunks_left{0};
+    svpf_server *server = nullptr;
+};
+
+}  // namespace
+
+struct svpf_server {
+    int device = 0;
+    int64_t budget = 0, used = 0, peak_used = 0;
+    int max_active = 0, active = 0, peak_active = 0;
+    int32_t chunk_pairs = 32;
+    std::vector<cudaStream_t> streams;
+    std::vector<bool> slot_busy;
+    std::deque<Request *> pending;
+    std::map<int64_t, std::unique_ptr<Request>> requests;
+    int64_t next_id = 1, admitted = 0, completed = 0;
+    std::atomic<int64_t> launches{0};
+    std::mutex mu;
+    std::condition_variable cv;       // scheduler wake-ups
+    std::condition_variable done_cv;  // request completions
+    bool stopping = false;
+    std::thread worker;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    int64_t now_ns() const {
+        return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+int sfail(int code, const std::string &msg) {
+    set_last_error(msg);
+    return code;
+}
+
+int64_t request_bytes(const Request &r, int32_t chunk) {
+    const int64_t c = chunk < r.nframes ? chunk : r.nframes;
+    return al256(r.D.src_frame_bytes * r.nframes) + al256(r.D.frame_bytes * r.nframes) +
+           al256(r.P.payload_len * r.nframes) + al256(r.P.scratch_per_pair * c) + 256;
+}
+
+// Host function behind a chunk's payload copy (no CUDA calls allowed here).
+void CUDART_CB chunk_done(void *arg) {
+    Chunk *ch = (Chunk *)arg;
+    Request *r = ch->req;
+    svpf_server *s = r->server;
+    const int64_t t = s->now_ns();
+    if (r->pair_done_ns)
+        for (int32_t i = 0; i < ch->count; i++) r->pair_done_ns[ch->first + i] = t;
+    if (r->chunks_left.fetch_sub(1) == 1) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->done_ns = t;
+        r->status = *r->status_host;
+        r->done = true;
+        s->used -= r->need;
+        s->active--;
+        s->slot_busy[(size_t)r->slot] = false;
+        s->completed++;
+        s->cv.notify_all();
+        s->done_cv.notify_all();
+    }
+}
+
+// Queues the whole of one admitted request on its slot's stream.
+int enqueue(svpf_server *s, Request *r) {
+    cudaStream_t st = s->streams[(size_t)r->slot];
+    const int64_t fb = r->D.frame_bytes, sb = r->D.src_frame_bytes;
+    cudaError_t e = cudaMallocAsync((void **)&r->dev, (size_t)r->need, st);
+    if (e != cudaSuccess) {
+        r->dev = nullptr;
+        return SVPF_ECUDA;
+    }
+    uint8_t *frames = r->dev;
+    uint8_t *supers = frames + al256(sb * r->nframes);
+    uint8_t *pays = supers + al256(fb * r->nframes);
+    uint8_t *scr = pays + al256(r->P.payload_len * r->nframes);
+    int *status = (int *)(scr + al256(r->P.scratch_per_pair * (r->chunks.empty() ? 1 : r->chunks[0].count)));
+    int nl = 0;
+    e = cudaMemsetAsync(status, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(frames, r->frames, (size_t)(sb * r->nframes), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_super(r->D, frames, supers, r->nframes, st, &nl);
+    for (size_t k = 0; e == cudaSuccess && k < r->chunks.size(); k++) {
+        Chunk &c = r->chunks[k];
+        PairSrc src{};
+        src.clip = supers;
+        src.frame_bytes = fb;
+        src.first = c.first;
+        src.nframes = r->nframes;
+        src.delta = r->delta;
+        e = launch_analyse(r->P, src, c.count, pays + (int64_t)c.first * r->P.payload_len, scr, status, st, &nl);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(r->payloads + (int64_t)c.first * r->P.payload_len, pays + (int64_t)c.first * r->P.payload_len,
+                                (size_t)(r->P.payload_len * c.count), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && k + 1 == r->chunks.size()) {
+            e = cudaMemcpyAsync(r->status_host, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaFreeAsync(r->dev, st);
+            if (e == cudaSuccess) r->dev = nullptr;
+        }
+        if (e == cudaSuccess) e = cudaLaunchHostFunc(st, chunk_done, &c);
+    }
+    s->launches += nl;
+    return e == cudaSuccess ? SVPF_OK : SVPF_ECUDA;
+}
+
+void scheduler(svpf_server *s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        s->cv.wait(lk, [&] {
+            if (s->stopping) return true;
+            if (s->pending.empty() || s->active >= s->max_active) return false;
+            return s->used + s->pending.front()->need <= s->budget;
+        });
+        if (s->stopping) {  // requests never admitted fail
+            for (Request *r : s->pending) {
+                r->status = -1;
+                r->done = true;
+            }
+            s->pending.clear();
+            s->done_cv.notify_all();
+            break;
+        }
+        Request *r = s->pending.front();
+        s->pending.pop_front();
+        int slot = 0;
+        while (s->slot_busy[(size_t)slot]) slot++;
+        s->slot_busy[(size_t)slot] = true;
+        r->slot = slot;
+        s->used += r->need;
+        s->peak_used = s->used > s->peak_used ? s->used : s->peak_used;
+        s->active++;
+        s->peak_active = s->active > s->peak_active ? s->active : s->peak_active;
+        s->admitted++;
+        r->admit_ns = s->now_ns();
+        lk.unlock();
+        const int rc = enqueue(s, r);
+        lk.lock();
+        if (rc != SVPF_OK) {  // its last chunk will never report: wait out what was queued, release it here
+            lk.unlock();
+            cudaStreamSynchronize(s->streams[(size_t)slot]);
+            if (r->dev) cudaFree(r->dev);
+            r->dev = nullptr;
+            lk.lock();
+            r->status = 4;
+            r->done = true;
+            r->done_ns = s->now_ns();
+            s->used -= r->need;
+            s->active--;
+            s->slot_busy[(size_t)slot] = false;
+            s->completed++;
+            s->done_cv.notify_all();
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int svpf_server_create(size_t hbm_budget_bytes, int32_t max_active, int32_t chunk_pairs, svpf_server **out) {
+    if (!out) return sfail(SVPF_EINVAL, "null output handle");
+    *out = nullptr;
+    if (hbm_budget_bytes == 0 || max_active <= 0 || chunk_pairs <= 0)
+        return sfail(SVPF_EINVAL, "budget, active clips and chunk size must be positive");
+    if (int rc = require_device()) return rc;
+    auto *s = new svpf_server;
+    s->budget = (int64_t)hbm_budget_bytes;
+    s->max_active = max_active;
+    s->chunk_pairs = chunk_pairs;
+    cudaGetDevice(&s->device);
+    {  // keep freed blocks in the pool: clips come and go, their sizes repeat
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    s->streams.assign((size_t)max_active, nullptr);
+    s->slot_busy.assign((size_t)max_active, false);
+    for (auto &st : s->streams) {
+        cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            for (auto &x : s->streams)
+                if (x) cudaStreamDestroy(x);
+            delete s;
+            return sfail(SVPF_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+        }
+    }
+    s->worker = std::thread(scheduler, s);
+    *out = s;
+    return SVPF_OK;
+}
+
+int svpf_server_submit(svpf_server *s, const svpf_super *sup, const svpf_analyser *an, const uint8_t *frames,
+                       int32_t nframes, uint8_t *payloads, int64_t *pair_done_ns, int64_t *request) {
+    if (!s || !sup || !an || !frames || !payloads || nframes <= 0) return sfail(SVPF_EINVAL, "bad request");
+    if (super_layout_of(sup)->frame_bytes != analyser_layout(an)->frame_bytes)
+        return sfail(SVPF_EINVAL, "super frame configuration mismatch");
+    auto r = std::make_unique<Request>();
+    r->arrival_ns = s->now_ns();
+    r->D = *super_dev_of(sup);
+    r->P = *analyser_params(an);
+    r->nframes = nframes;
+    r->delta = analyser_delta(an) > 1 ? analyser_delta(an) : 1;
+    r->frames = frames;
+    r->payloads = payloads;
+    r->pair_done_ns = pair_done_ns;
+    r->server = s;
+    for (int32_t f = 0; f < nframes; f += s->chunk_pairs)
+        r->chunks.push_back(Chunk{r.get(), f, (nframes - f) < s->chunk_pairs ? nframes - f : s->chunk_pairs});
+    r->chunks_left = (int)r->chunks.size();
+    r->need = request_bytes(*r, s->chunk_pairs);
+    if (r->need > s->budget) return sfail(SVPF_EINVAL, "clip needs more device memory than the server's budget");
+    if (cudaHostAlloc((void **)&r->status_host, sizeof(int), cudaHostAllocDefault) != cudaSuccess)
+        return sfail(SVPF_ECUDA, "cudaHostAlloc (status word)");
+    *r->status_host = 0;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) {
+        cudaFreeHost(r->status_host);
+        return sfail(SVPF_EINVAL, "server is shutting down");
+    }
+    r->id = s->next_id++;
+    if (request) *request = r->id;
+    s->pending.push_back(r.get());
+    s->requests[r->id] = std::move(r);
+    s->cv.notify_all();
+    return SVPF_OK;
+}
+
+int svpf_server_wait(svpf_server *s, int64_t request, int64_t *times) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->requests.find(request);
+    if (it == s->requests.end()) return sfail(SVPF_EINVAL, "unknown request");
+    Request *r = it->second.get();
+    s->done_cv.wait(lk, [&] { return r->done; });
+    if (times) { times[0] = r->arrival_ns; times[1] = r->admit_ns; times[2] = r->done_ns; }
+    const int st = r->status;
+    cudaFreeHost(r->status_host);
+    s->requests.erase(it);
+    if (st < 0) return sfail(SVPF_EINVAL, "server shut down before the request started");
+    if (st & 1) return sfail(SVPF_EPANIC, "SVAnalyse: the reference indexes out of range on this input (it panics)");
+    if (st == 4) return sfail(SVPF_ECUDA, "enqueueing the request failed");
+    if (st) return sfail(SVPF_EUNSUP, "SVAnalyse: unsupported input on the device path");
+    return SVPF_OK;
+}
+
+int64_t svpf_server_now_ns(const svpf_server *s) { return s->now_ns(); }
+
+void svpf_server_stats(svpf_server *s, int64_t *admitted, int64_t *completed, int64_t *peak_device_bytes,
+                       int32_t *peak_active, int64_t *kernel_launches) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (admitted) *admitted = s->admitted;
+    if (completed) *completed = s->completed;
+    if (peak_device_bytes) *peak_device_bytes = s->peak_used;
+    if (peak_active) *peak_active = s->peak_active;
+    if (kernel_launches) *kernel_launches = s->launches.load();
+}
+
+void svpf_server_destroy(svpf_server *s) {
+    if (!s) return;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->stopping = true;
+        s->cv.notify_all();
+    }
+    s->worker.join();
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->done_cv.wait(lk, [&] { return s->active == 0; });
+    }
+    for (auto &st : s->streams) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    for (auto &kv : s->requests)
+        if (kv.second->status_host) cudaFreeHost(kv.second->status_host);
+    delete s;
+}
+
+}  // extern "C"

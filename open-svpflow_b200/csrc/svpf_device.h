@@ -38,8 +38,46 @@ struct PairSrc {
     int32_t first, nframes, delta;
 };
 
-// Analyse over npairs pairs; payloads npairs x P.payload_len bytes, scratch npairs x
-// P.scratch_per_pair bytes, status one int (0 = ok), cleared by the caller.
+// One work item of a batch launch: a frame pair of some clip and where its payload goes.
+struct BatchItem {
+    PairRef pair;
+    uint8_t *payload;
+    int32_t clip;   // index into the launch's AnalyseParams table (and status array)
+    int32_t pad_;
+};
+
+// The launchers every Analyse variant TU exports (analyse_body.cuh).
+#define SVPF_DECLARE_ANALYSE_VARIANT(ns)                                                                          \
+    namespace ns {                                                                                                \
+    size_t dir_shared_bytes();                                                                                    \
+    cudaError_t launch_plain(const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,           \
+                             uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches);              \
+    cudaError_t batch_blocks_per_sm(int *blocks);                                                                 \
+    cudaError_t launch_batch(const AnalyseParams *clips_dev, const BatchItem *items_dev, int nitems,              \
+                             unsigned *next_item_dev, uint8_t *scratch, int64_t scratch_per_cta,                  \
+                             int *clip_status_dev, int grid, cudaStream_t stream, int *launches);                 \
+    }
+SVPF_DECLARE_ANALYSE_VARIANT(nt128)
+SVPF_DECLARE_ANALYSE_VARIANT(nt64)
+SVPF_DECLARE_ANALYSE_VARIANT(nt32)
+
+// A compiled launch shape of the Analyse kernels: threads per search direction and the
+// resident CTAs per SM its register budget was cut for. Results do not depend on it.
+struct AnalyseVariant {
+    const char *name;
+    int threads_per_dir, min_blocks;
+    cudaError_t (*launch_plain)(const AnalyseParams &, const PairSrc &, int, uint8_t *, uint8_t *, int *,
+                                cudaStream_t, int *);
+    cudaError_t (*batch_blocks_per_sm)(int *);
+    cudaError_t (*launch_batch)(const AnalyseParams *, const BatchItem *, int, unsigned *, uint8_t *, int64_t, int *,
+                                int, cudaStream_t, int *);
+};
+int analyse_variant_count();
+const AnalyseVariant &analyse_variant(int i);  // 0 = the plain path's default (nt128)
+
+// Analyse over npairs pairs with the default variant; payloads npairs x P.payload_len
+// bytes, scratch npairs x P.scratch_per_pair bytes, status one int (0 = ok), cleared by
+// the caller.
 cudaError_t launch_analyse(const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,
                            uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches);
 

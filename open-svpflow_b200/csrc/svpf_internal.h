@@ -85,7 +85,7 @@ struct LevelInfo {
     int32_t tl, tc;           // 4x4 luma tiles, 4x4 chroma tiles per plane of one candidate
 };
 
-struct AnalyseParams {
+struct alignas(16) AnalyseParams {
     int32_t nlevels;
     LevelInfo lv[kMaxLevels];
     int32_t block_w, block_h, ox, oy, step_x, step_y;
@@ -97,6 +97,7 @@ struct AnalyseParams {
     int32_t out_gw, out_gh, out_bw, out_bh, out_ox, out_oy;
     int32_t has_refine, refine_thsad, refine_search_type, refine_distance, refine_satd, lambda;
     int32_t rescale_denom;
+    int32_t tiles_per_lane;   // 4x4 tiles one lane evaluates per candidate (2, 4 or 8): a launch tuning knob
     int64_t payload_len;
     int32_t header[16];       // payload words 0x00..0x3C
     // per-pair scratch layout (bytes)
@@ -105,6 +106,8 @@ struct AnalyseParams {
     int64_t off_keys[2], off_hist[2], off_seen[2], off_out[2];
     int64_t scratch_per_pair;
 };
+
+static_assert(sizeof(AnalyseParams) % 16 == 0, "AnalyseParams is copied in 16-byte words");
 
 bool build_analyse_params(const AnalyseOpts &o, const SuperLayout &L, AnalyseParams &P, std::string &err);
 

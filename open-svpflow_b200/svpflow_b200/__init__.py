@@ -19,8 +19,8 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-__all__ = ["SuperBuilder", "SuperFrame", "Analyser", "Super", "Analyse", "lib", "LIB_PATH", "SvpfError",
-           "REFERENCE_VERSION"]
+__all__ = ["SuperBuilder", "SuperFrame", "Analyser", "Super", "Analyse", "Batch", "Server", "lib", "LIB_PATH",
+           "SvpfError", "REFERENCE_VERSION"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libsvpflow_b200.so")
@@ -74,6 +74,28 @@ def lib() -> ctypes.CDLL:
             "svpf_clip_analyse": (I32, [_VP, _VP, _VP, I32, I32, I32, _VP]),
             "svpf_kernel_launches": (I64, []),
             "svpf_kernel_launches_reset": (None, []),
+            "svpf_batch_create": (I32, [I32, P(_VP), P(_VP), P(I32), P(_VP)]),
+            "svpf_batch_destroy": (None, [_VP]),
+            "svpf_batch_clips": (I32, [_VP]),
+            "svpf_batch_pairs": (I64, [_VP]),
+            "svpf_batch_device_bytes": (SZ, [_VP]),
+            "svpf_batch_frames_device": (_VP, [_VP, I32]),
+            "svpf_batch_payloads_device": (_VP, [_VP, I32]),
+            "svpf_batch_run": (I32, [_VP, P(_VP), P(_VP)]),
+            "svpf_batch_launch": (I32, [_VP, _VP]),
+            "svpf_batch_status": (I32, [_VP, _VP]),
+            "svpf_batch_set_shape": (I32, [_VP, I32, I32]),
+            "svpf_batch_shape": (ctypes.c_char_p, [_VP, P(I32), P(I32), P(I32)]),
+            "svpf_batch_autotune": (I32, [_VP, P(I32), P(I32), P(ctypes.c_double)]),
+            "svpf_batch_graph_launches": (I32, [_VP]),
+            "svpf_analyse_variant_count": (I32, []),
+            "svpf_analyse_variant_name": (ctypes.c_char_p, [I32]),
+            "svpf_server_create": (I32, [SZ, I32, I32, P(_VP)]),
+            "svpf_server_destroy": (None, [_VP]),
+            "svpf_server_submit": (I32, [_VP, _VP, _VP, _VP, I32, _VP, _VP, P(I64)]),
+            "svpf_server_wait": (I32, [_VP, I64, P(I64)]),
+            "svpf_server_now_ns": (I64, [_VP]),
+            "svpf_server_stats": (None, [_VP, P(I64), P(I64), P(I64), P(I32), P(I64)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -274,3 +296,132 @@ def kernel_launches() -> int:
 
 def reset_kernel_launches():
     lib().svpf_kernel_launches_reset()
+
+
+class Batch:
+    """Many clips analysed by one persistent launch (no counterpart in the reference).
+
+    clips: sequence of (SuperBuilder, Analyser, nframes). Payloads equal each clip's
+    Analyser.analyse_clip output byte for byte."""
+
+    def __init__(self, clips):
+        self._keep = list(clips)  # the handles must outlive the batch
+        n = len(self._keep)
+        sups = (_VP * n)(*[c[0].handle for c in self._keep])
+        ans = (_VP * n)(*[c[1].handle for c in self._keep])
+        nf = (ctypes.c_int32 * n)(*[int(c[2]) for c in self._keep])
+        h = _VP()
+        _check(lib().svpf_batch_create(n, sups, ans, nf, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.svpf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def pairs(self) -> int:
+        return lib().svpf_batch_pairs(self._h)
+
+    @property
+    def device_bytes(self) -> int:
+        return lib().svpf_batch_device_bytes(self._h)
+
+    def frames_device(self, clip: int) -> int:
+        return lib().svpf_batch_frames_device(self._h, clip)
+
+    def payloads_device(self, clip: int) -> int:
+        return lib().svpf_batch_payloads_device(self._h, clip)
+
+    def run(self, frames, payloads=None):
+        """Host frames per clip in, payload arrays per clip out (allocated when not given)."""
+        n = len(self._keep)
+        frames = [np.ascontiguousarray(f, dtype=np.uint8) for f in frames]
+        if payloads is None:
+            payloads = [np.empty((c[2], c[1].payload_len()), dtype=np.uint8) for c in self._keep]
+        fp = (_VP * n)(*[f.ctypes.data for f in frames])
+        pp = (_VP * n)(*[p.ctypes.data for p in payloads])
+        _check(lib().svpf_batch_run(self._h, fp, pp))
+        return payloads
+
+    def launch(self, stream: int = 0):
+        """Replays the run on `stream` (0 = the batch's own stream)."""
+        _check(lib().svpf_batch_launch(self._h, stream))
+
+    def status(self, stream: int = 0):
+        _check(lib().svpf_batch_status(self._h, stream))
+
+    def set_shape(self, variant: int, tiles_per_lane: int):
+        _check(lib().svpf_batch_set_shape(self._h, variant, tiles_per_lane))
+
+    def shape(self) -> dict:
+        v, t, g = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        name = lib().svpf_batch_shape(self._h, ctypes.byref(v), ctypes.byref(t), ctypes.byref(g)).decode()
+        return {"variant": v.value, "name": name, "tiles_per_lane": t.value, "grid": g.value}
+
+    def autotune(self) -> dict:
+        v, t, r = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+        _check(lib().svpf_batch_autotune(self._h, ctypes.byref(v), ctypes.byref(t), ctypes.byref(r)))
+        return {"trial_pairs_per_s": r.value, **self.shape()}
+
+    @property
+    def graph_launches(self) -> int:
+        return lib().svpf_batch_graph_launches(self._h)
+
+    @staticmethod
+    def variants() -> list:
+        return [lib().svpf_analyse_variant_name(i).decode() for i in range(lib().svpf_analyse_variant_count())]
+
+
+class Server:
+    """Continuous-batching request loop (no counterpart in the reference)."""
+
+    def __init__(self, hbm_budget_bytes: int, max_active: int = 8, chunk_pairs: int = 32):
+        self._live = {}
+        h = _VP()
+        _check(lib().svpf_server_create(int(hbm_budget_bytes), max_active, chunk_pairs, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.svpf_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def now_ns(self) -> int:
+        return lib().svpf_server_now_ns(self._h)
+
+    def submit(self, super_builder: SuperBuilder, analyser: Analyser, frames: np.ndarray, payloads: np.ndarray = None,
+               pair_done_ns: np.ndarray = None) -> int:
+        frames = np.ascontiguousarray(frames, dtype=np.uint8)
+        n = frames.shape[0]
+        if payloads is None:
+            payloads = np.empty((n, analyser.payload_len()), dtype=np.uint8)
+        if pair_done_ns is None:
+            pair_done_ns = np.zeros(n, dtype=np.int64)
+        rid = ctypes.c_int64()
+        _check(lib().svpf_server_submit(self._h, super_builder.handle, analyser.handle, frames.ctypes.data, n,
+                                        payloads.ctypes.data, pair_done_ns.ctypes.data, ctypes.byref(rid)))
+        self._live[rid.value] = (super_builder, analyser, frames, payloads, pair_done_ns)
+        return rid.value
+
+    def wait(self, request: int):
+        """-> (payloads, pair_done_ns, (arrival, admit, done) ns on the server clock)."""
+        t = (ctypes.c_int64 * 3)()
+        rc = lib().svpf_server_wait(self._h, request, t)
+        keep = self._live.pop(request)
+        _check(rc)
+        return keep[3], keep[4], (t[0], t[1], t[2])
+
+    def stats(self) -> dict:
+        a, c, pb, l = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        pa = ctypes.c_int32()
+        lib().svpf_server_stats(self._h, ctypes.byref(a), ctypes.byref(c), ctypes.byref(pb), ctypes.byref(pa),
+                                ctypes.byref(l))
+        return {"admitted": a.value, "completed": c.value, "peak_device_bytes": pb.value, "peak_active": pa.value,
+                "kernel_launches": l.value}

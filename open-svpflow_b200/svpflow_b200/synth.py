@@ -96,6 +96,110 @@ def make_clip(width: int, height: int, frames: int, seed: int, motion: int = 8, 
     return out
 
 
+def make_clip_device(width: int, height: int, frames: int, seed: int, motion: int = 8, objects: int = 4,
+                     object_motion: int = 16, noise: float = 2.0, device="cuda"):
+    """The same generator as make_clip, run with torch on the device (for the large batched
+    and served workloads, where the host generator would take minutes). Same recipe and
+    statistics; a different random stream, so frames differ from make_clip's. Returns a
+    uint8 tensor [frames, w*h + 2*(w/2*h/2)] on `device`."""
+    import torch
+
+    assert width % 2 == 0 and height % 2 == 0
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    cw, ch = width // 2, height // 2
+    F = torch.nn.functional
+
+    def blur(img, sigma):
+        k = torch.from_numpy(_kernel(sigma)).to(device)
+        r = k.numel() // 2
+        x = F.pad(img[None, None], (r, r, 0, 0), mode="replicate")
+        x = F.conv2d(x, k.view(1, 1, 1, -1))
+        x = F.pad(x, (0, 0, r, r), mode="replicate")
+        return F.conv2d(x, k.view(1, 1, -1, 1))[0, 0]
+
+    def rint(lo, hi):  # uniform integer in [lo, hi)
+        return int(torch.randint(lo, hi, (1,), generator=g, device=device).item())
+
+    def noise_img(h, w):
+        return torch.randint(0, 256, (h, w), generator=g, device=device).float()
+
+    clean = [blur(noise_img(height, width), 2.0), blur(noise_img(ch, cw), 1.0), blur(noise_img(ch, cw), 1.0)]
+    objs = []
+    for _ in range(objects):
+        oh, ow = rint(32, 97), rint(32, 97)
+        tex = [blur(noise_img(oh, ow), 2.0), blur(noise_img(max(oh // 2, 1), max(ow // 2, 1)), 1.0),
+               blur(noise_img(max(oh // 2, 1), max(ow // 2, 1)), 1.0)]
+        objs.append((oh, ow, rint(0, max(height - oh, 1)), rint(0, max(width - ow, 1)),
+                     rint(-object_motion, object_motion + 1), rint(-object_motion, object_motion + 1), tex))
+
+    def shift(img, dy, dx):
+        h, w = img.shape
+        ys = (torch.arange(h, device=device) - dy).clamp(0, h - 1)
+        xs = (torch.arange(w, device=device) - dx).clamp(0, w - 1)
+        return img[ys][:, xs]
+
+    ysz, csz = width * height, cw * ch
+    out = torch.empty((frames, ysz + 2 * csz), dtype=torch.uint8, device=device)
+    for f in range(frames):
+        if f > 0:
+            dy, dx = rint(-motion, motion + 1), rint(-motion, motion + 1)
+            clean = [shift(clean[0], dy, dx), shift(clean[1], dy // 2, dx // 2), shift(clean[2], dy // 2, dx // 2)]
+        planes = [p.clone() for p in clean]
+        for oh, ow, y0, x0, vy, vx, tex in objs:
+            oy = (y0 + f * vy) % max(height - oh, 1)
+            ox = (x0 + f * vx) % max(width - ow, 1)
+            planes[0][oy:oy + oh, ox:ox + ow] = tex[0][:min(oh, height - oy), :min(ow, width - ox)]
+            for p in (1, 2):
+                t = tex[p]
+                cy, cx = oy // 2, ox // 2
+                planes[p][cy:cy + t.shape[0], cx:cx + t.shape[1]] = t[:min(t.shape[0], ch - cy), :min(t.shape[1], cw - cx)]
+        for i, p in enumerate(planes):
+            q = (p + noise * torch.randn(p.shape, generator=g, device=device)).round().clamp(0, 255).to(torch.uint8)
+            if i == 0:
+                out[f, :ysz] = q.reshape(-1)
+            else:
+                out[f, ysz + (i - 1) * csz: ysz + i * csz] = q.reshape(-1)
+    return out
+
+
+def batched_mix(nclips: int = 64, seed: int = 4, min_len: int = 16, max_len: int = 240):
+    """The batched workload: clips of uneven size and length. Resolution drawn per clip
+    from {640x360, 1280x720, 1920x1080, 2560x1440}, length log-uniform over
+    [min_len, max_len] frames, block size from {8, 16}; motion ranges of the 1080p
+    configuration. Returns [(width, height, frames, block, clip seed)]."""
+    rng = np.random.default_rng(seed)
+    res = [(640, 360), (1280, 720), (1920, 1080), (2560, 1440)]
+    out = []
+    for i in range(nclips):
+        w, h = res[int(rng.integers(0, len(res)))]
+        n = int(round(math.exp(rng.uniform(math.log(min_len), math.log(max_len)))))
+        blk = int(rng.choice([8, 16]))
+        out.append((w, h, n, blk, 1000 + 7 * i + seed))
+    return out
+
+
+def served_stream(nclips: int, rate: float, seed: int = 5, min_len: int = 8, max_len: int = 600):
+    """The served workload: Poisson arrivals at `rate` clips/s; resolution from {360p,
+    720p, 1080p, 1440p, 2160p}, length log-uniform over [min_len, max_len]. Returns
+    [(arrival s, width, height, frames, clip seed)]."""
+    rng = np.random.default_rng(seed)
+    res = [(640, 360), (1280, 720), (1920, 1080), (2560, 1440), (3840, 2160)]
+    t = 0.0
+    out = []
+    for i in range(nclips):
+        t += float(rng.exponential(1.0 / rate))
+        w, h = res[int(rng.integers(0, len(res)))]
+        n = int(round(math.exp(rng.uniform(math.log(min_len), math.log(max_len)))))
+        out.append((t, w, h, n, 5000 + 11 * i + seed))
+    return out
+
+
+def analyse_opt_for_block(block: int) -> str:
+    """Analyse options of the 1080p configuration with another block size (overlap = half)."""
+    return "{block:{w:%d,overlap:3},main:{search:{type:3,distance:16,satd:true}}}" % block
+
+
 # Workloads of the reference's benchmark configurations (shapes, motion ranges).
 CONFIGS = {
     "640x360": dict(width=640, height=360, frames=32, motion=8, objects=4, object_motion=16),

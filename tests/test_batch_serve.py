@@ -1,0 +1,135 @@
+"""The batched and served forms (GPU): every payload equals the plain per-clip path's
+(which the parity suite holds to the oracle), for every launch shape, alone and in a mix
+of clips of uneven size, length and options. Tolerance: zero (integer work)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# (w, h, frames, seed, super opt, analyse opt)
+MIX = [
+    (192, 128, 5, 11, "{pel:2}", "{block:{w:16,overlap:3},main:{search:{type:3,distance:8,satd:true}}}"),
+    (128, 96, 3, 12, "{pel:2}", "{block:{w:8,overlap:2},main:{search:{type:3,distance:6,satd:true}}}"),
+    (160, 96, 4, 13, "{pel:1}", "{vectors:1,block:{w:16,overlap:0},main:{search:{type:2,distance:2}}}"),
+    (256, 144, 2, 14, "{pel:4}", "{block:{w:8,overlap:3},main:{search:{type:4,distance:3,satd:true,coarse:{type:2}}}}"),
+    (96, 64, 6, 15, "{pel:2}", "{vectors:2,delta:2,block:{w:8,overlap:1},main:{search:{type:2,distance:4}}}"),
+]
+
+
+def _clips(mix=MIX):
+    import svpflow_b200 as sv
+    from svpflow_b200.synth import make_clip
+
+    out = []
+    for w, h, n, seed, sopt, aopt in mix:
+        sb = sv.Super(w, h, sopt)
+        an = sv.Analyse(sb.sdata, aopt, w, h)
+        clip = make_clip(w, h, n, seed=seed, motion=6, objects=2, object_motion=9)
+        out.append((sb, an, clip))
+    return out
+
+
+def _plain(clips):
+    return [an.analyse_clip(sb, clip) for sb, an, clip in clips]
+
+
+class _Dev:
+    """A raw device byte range as a torch tensor (CUDA array interface; no copy)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False), "version": 3}
+
+
+def _dev(ptr, n):
+    import torch
+
+    return torch.as_tensor(_Dev(ptr, n), device="cuda")
+
+
+def test_batch_matches_plain_for_every_shape():
+    import svpflow_b200 as sv
+
+    clips = _clips()
+    want = _plain(clips)
+    b = sv.Batch([(sb, an, clip.shape[0]) for sb, an, clip in clips])
+    assert b.pairs == sum(c[2].shape[0] for c in clips)
+    for v in range(len(sv.Batch.variants())):
+        for t in (2, 4, 8):
+            b.set_shape(v, t)
+            got = b.run([c[2] for c in clips])
+            for i, (g, w_) in enumerate(zip(got, want)):
+                assert np.array_equal(g, w_), f"variant {v} tiles/lane {t}: clip {i} differs"
+    b.close()
+
+
+def test_batch_device_replay_and_autotune():
+    import torch
+
+    import svpflow_b200 as sv
+
+    clips = _clips(MIX[:3])
+    want = _plain(clips)
+    b = sv.Batch([(sb, an, clip.shape[0]) for sb, an, clip in clips])
+    for i, (_, _, clip) in enumerate(clips):  # fill the batch's frame buffers on the device
+        ptr = b.frames_device(i)
+        assert ptr
+        _dev(ptr, clip.size).copy_(torch.from_numpy(clip.reshape(-1)))
+    torch.cuda.synchronize()
+    for _ in range(2):  # graph replays
+        b.launch()
+        b.status()
+        for i, (_, an, clip) in enumerate(clips):
+            n, L = clip.shape[0], an.payload_len()
+            got = _dev(b.payloads_device(i), n * L).cpu().numpy().reshape(n, L)
+            assert np.array_equal(got, want[i])
+    r = b.autotune()
+    assert 0 <= r["variant"] < len(sv.Batch.variants()) and r["tiles_per_lane"] in (2, 4, 8)
+    assert r["trial_pairs_per_s"] > 0
+    got = b.run([c[2] for c in clips])
+    assert all(np.array_equal(g, w_) for g, w_ in zip(got, want))
+    b.close()
+
+
+def test_server_results_equal_alone_and_in_the_mix():
+    import time
+
+    import svpflow_b200 as sv
+
+    clips = _clips()
+    want = _plain(clips)
+    # a budget below two of the largest clips, so admission has to wait for memory
+    chunk = 2
+    need = [c[2].nbytes + (c[0].output_len() + c[1].payload_len()) * c[2].shape[0] +
+            c[1].scratch_bytes(min(chunk, c[2].shape[0])) + 2048 for c in clips]
+    budget = int(1.6 * max(need))
+    srv = sv.Server(budget, max_active=3, chunk_pairs=chunk)
+    try:
+        ids = []
+        for k, (sb, an, clip) in enumerate(clips):
+            ids.append(srv.submit(sb, an, clip))
+            time.sleep(0.01 * (k % 2))
+        for k, rid in enumerate(ids):
+            pay, done, (arr, adm, fin) = srv.wait(rid)
+            assert np.array_equal(pay, want[k]), f"clip {k} differs in the mix"
+            assert arr <= adm <= fin and (done >= arr).all() and (done <= fin).all()
+        st = srv.stats()
+        assert st["completed"] == len(clips) and 1 <= st["peak_active"] <= 3
+        assert st["peak_device_bytes"] <= budget and st["kernel_launches"] > 0
+        # the same clip alone on the same server
+        sb, an, clip = clips[0]
+        pay, _, _ = srv.wait(srv.submit(sb, an, clip))
+        assert np.array_equal(pay, want[0])
+    finally:
+        srv.close()
+
+
+def test_server_rejects_a_clip_over_budget():
+    import svpflow_b200 as sv
+
+    (sb, an, clip), = _clips(MIX[:1])
+    srv = sv.Server(1 << 20, max_active=2, chunk_pairs=4)
+    try:
+        with pytest.raises(ValueError, match="more device memory than the server's budget"):
+            srv.submit(sb, an, clip)
+    finally:
+        srv.close()

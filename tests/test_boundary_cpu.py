@@ -112,3 +112,26 @@ def test_portable_constructors_match_oracle():
         sv.SuperBuilder(65, 64, 2)
     with pytest.raises(ValueError, match="block dimensions must be 4, 8, 16 or 32"):
         sv.Analyser(sv.SuperBuilder(64, 64, 2), 12, 16, 2, 3)
+
+
+def test_compute_entry_points_fail_loudly_without_a_gpu():
+    """No CPU fallback: with no CUDA device every compute call is an error (this container
+    has none; on a GPU machine the GPU suite covers these calls)."""
+    import numpy as np
+
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            pytest.skip("a CUDA device is present")
+    except ImportError:
+        pass
+    sv = _sv()
+    sb = sv.Super(64, 48, "{pel:2}")
+    an = sv.Analyse(sb.sdata, "{block:{w:8}}", 64, 48)
+    frames = np.zeros((2, sb.source_len()), np.uint8)
+    for call in (lambda: sb.build_many(frames), lambda: an.analyse_clip(sb, frames),
+                 lambda: sv.Batch([(sb, an, 2)]), lambda: sv.Server(1 << 30)):
+        with pytest.raises(sv.SvpfError, match="no CUDA device") as e:
+            call()
+        assert e.value.code == sv.SVPF_ECUDA
