@@ -53,6 +53,7 @@ static_assert(NT == 32 || NT == 64 || NT == 128, "threads per direction");
 constexpr int NW = NT / 32;
 constexpr int NGMAX = NW * 32;     // candidate groups of a direction when a group is one lane
 constexpr int MAXSLOT = 16;        // special-candidate slots of a block
+constexpr int MW = 4;              // validity mask words per chunk of a search step: 128 candidates
 
 enum : uint8_t { LM_DIRECT = 1, LM_SATD_MASK = 2, LM_SAD_BREAK = 3, LM_EDGE = 4, LM_DC = 5 };
 enum : uint8_t { CM_NONE = 0, CM_DIRECT = 1, CM_SAD_BREAK = 3, CM_EDGE = 4 };
@@ -81,7 +82,11 @@ struct DirSh {
     int gx, gy;           // global predictor (doubled) for the next level
     int order_len;
     int abort_;
-    uint32_t srcw[384];   // the block's source pixels as words: luma (bw/4 x bh), then U and V (cw/4 x crows)
+    // The block's source pixels, 4 per entry: luma (bw/4 x bh), then U and V (cw/4 x crows).
+    // A plane searched with SATD holds 16-bit pairs (x = pixels 0,1; y = pixels 2,3), a
+    // SAD plane the packed word in x.
+    uint2 srcp[384];
+    int2 clist[NW][32 * MW];  // per warp: the step's candidates passing the cuts, in order (mv, index)
     long long r64[NW][3];
     int r32[NW][2];
 };
@@ -93,6 +98,7 @@ struct Planes {
 struct Geo {  // per level
     int lw, lh, clw, clh;
     int64_t ys, cs, ylen, clen;
+    int ys32, cs32;   // the strides again, for 32-bit offsets (planes are below 2^30 bytes)
 };
 
 __device__ __forceinline__ void dbar(int d) { asm volatile("bar.sync %0, %1;" ::"r"(d + 1), "r"(NT) : "memory"); }
@@ -419,7 +425,7 @@ __device__ __forceinline__ uint32_t ld4u(const uint8_t *p) {
     const uint32_t *q = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
     return __funnelshift_r(__ldg(q), __ldg(q + 1), (unsigned)(a & 3) * 8u);
 }
-__device__ __forceinline__ unsigned tile_satd(const uint8_t *sp, const uint8_t *rp, int64_t st) {
+__device__ __forceinline__ unsigned tile_satd(const uint8_t *sp, const uint8_t *rp, int st) {
     int d[16];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
@@ -429,30 +435,53 @@ __device__ __forceinline__ unsigned tile_satd(const uint8_t *sp, const uint8_t *
     }
     return hadamard4(d);
 }
-__device__ __forceinline__ unsigned tile_sad(const uint8_t *sp, const uint8_t *rp, int64_t st) {
+__device__ __forceinline__ unsigned tile_sad(const uint8_t *sp, const uint8_t *rp, int st) {
     unsigned s = 0;
 #pragma unroll
     for (int r = 0; r < 4; r++) s = __dp4a(__vabsdiffu4(ld4u(sp + r * st), ld4u(rp + r * st)), 0x01010101u, s);
     return s;
 }
-// Same tiles with the source rows already in shared memory as words (row pitch swp words).
-__device__ __forceinline__ unsigned tile_satd_w(const uint32_t *sw, int swp, const uint8_t *rp, int64_t st) {
-    int d[16];
+// Packed-halfword forms over the staged source (see DirSh::srcp): a row's four byte
+// differences are two halfword pairs; the horizontal 4-point transform runs inside the
+// pairs, the vertical one across the rows, and the last vertical stage with its absolute
+// values is |a+b| + |a-b| = 2 max(|a|, |b|), as in hadamard4. Every intermediate fits a
+// signed halfword (|value| <= 2040) and the four-row sum an unsigned one (<= 8160).
+__device__ __forceinline__ uint32_t pairs_lo(uint32_t w) { return __byte_perm(w, 0u, 0x4140); }  // pixels 0, 1
+__device__ __forceinline__ uint32_t pairs_hi(uint32_t w) { return __byte_perm(w, 0u, 0x4342); }  // pixels 2, 3
+__device__ __forceinline__ unsigned tile_satd_p(const uint2 *sp, int spp, const uint8_t *rp, int st) {
+    uint32_t h0[4], h1[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
-        const uint32_t a = sw[r * swp], b = ld4u(rp + r * st);
-#pragma unroll
-        for (int q = 0; q < 4; q++) d[r * 4 + q] = (int)((a >> (8 * q)) & 255u) - (int)((b >> (8 * q)) & 255u);
+        const uint2 a = sp[r * spp];
+        const uint32_t b = ld4u(rp + r * st);
+        const uint32_t d01 = __vsub2(a.x, pairs_lo(b)), d23 = __vsub2(a.y, pairs_hi(b));
+        const uint32_t c = __vadd2(d01, d23), e = __vsub2(d01, d23);
+        const uint32_t p = __byte_perm(c, e, 0x5410), q = __byte_perm(c, e, 0x7632);
+        h0[r] = __vadd2(p, q);
+        h1[r] = __vsub2(p, q);
     }
-    return hadamard4(d);
+    uint32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const uint32_t *h = k ? h1 : h0;
+        const uint32_t a0 = __vadd2(h[0], h[1]), a1 = __vsub2(h[0], h[1]);
+        const uint32_t a2 = __vadd2(h[2], h[3]), a3 = __vsub2(h[2], h[3]);
+        acc = __vadd2(acc, __vmaxu2(__vabs2(a0), __vabs2(a2)));
+        acc = __vadd2(acc, __vmaxu2(__vabs2(a1), __vabs2(a3)));
+    }
+    return 2u * ((acc & 0xFFFFu) + (acc >> 16));
 }
-__device__ __forceinline__ unsigned tile_sad_w(const uint32_t *sw, int swp, const uint8_t *rp, int64_t st) {
+__device__ __forceinline__ unsigned tile_sad_p(const uint2 *sp, int spp, const uint8_t *rp, int st) {
     unsigned s = 0;
 #pragma unroll
-    for (int r = 0; r < 4; r++) s = __dp4a(__vabsdiffu4(sw[r * swp], ld4u(rp + r * st)), 0x01010101u, s);
+    for (int r = 0; r < 4; r++) s = __dp4a(__vabsdiffu4(sp[r * spp].x, ld4u(rp + r * st)), 0x01010101u, s);
     return s;
 }
-__device__ __forceinline__ unsigned tile_sum(const uint8_t *sp, int64_t st) {
+// The staged entry of 4 source pixels for a plane searched with SATD (pairs) or SAD (word).
+__device__ __forceinline__ uint2 stage4(uint32_t w, bool satd) {
+    return satd ? make_uint2(pairs_lo(w), pairs_hi(w)) : make_uint2(w, 0u);
+}
+__device__ __forceinline__ unsigned tile_sum(const uint8_t *sp, int st) {
     unsigned s = 0;
 #pragma unroll
     for (int r = 0; r < 4; r++) s = __dp4a(ld4u(sp + r * st), 0x01010101u, s);
@@ -530,6 +559,7 @@ struct BlkC {
     int bnd0, bnd1, bnd2, bnd3, ubx, uby;  // mv_bounds; ub = bound above which the edge shift starts
     int chroma, satd_mode, fastable, fast_src, cfast_src, dc_fast;
     int cw, ch, crows, cpx, cpy, tilesx, ctilesx;
+    int lgtx, lgctx;                       // log2 of tilesx / ctilesx (block sizes are powers of two)
     int64_t lsrc, csrc, dsrc;              // flat index of the source block (luma, chroma, luma at (px, py))
 };
 
@@ -548,6 +578,7 @@ __device__ __forceinline__ void make_blk(const Ctx &x, int px, int py, bool chro
     b.satd_mode = x.satd && is_blk(bw) && is_blk(bh) && bw == bh;
     b.fastable = bw > 0 && bh > 0 && (bw & 3) == 0 && (bh & 3) == 0;
     b.tilesx = bw >> 2;
+    b.lgtx = 31 - __clz(imax(b.tilesx, 1));
     b.lsrc = ((int64_t)L.y_off + b.py2) * G.ys + b.px2;
     b.fast_src = b.fastable && b.px2 >= 0 && b.py2 >= 0 && b.px2 + bw <= G.lw && b.py2 + bh <= G.lh &&
                  b.lsrc + (int64_t)(bh - 1) * G.ys + bw + 8 <= G.ylen;
@@ -557,6 +588,7 @@ __device__ __forceinline__ void make_blk(const Ctx &x, int px, int py, bool chro
     b.cw = bw / 2; b.ch = bh / 2;
     b.crows = x.satd ? b.cw : b.ch;
     b.ctilesx = (b.cw + 3) >> 2;
+    b.lgctx = 31 - __clz(imax(b.ctilesx, 1));
     b.cpx = px / 2; b.cpy = py / 2;
     b.csrc = ((int64_t)L.c_off + b.cpy) * G.cs + b.cpx;
     b.cfast_src = (b.cw == 4 || b.cw == 8 || b.cw == 16) && b.ch >= 4 && (b.ch & 3) == 0 && px >= 0 && py >= 0 &&
@@ -567,8 +599,7 @@ __device__ __forceinline__ void make_blk(const Ctx &x, int px, int py, bool chro
 // Does (block, mv) take the fast path? If so, the flat indices of its reference blocks.
 // It does when the reference takes its direct reads for both luma and chroma: no edge
 // shift, the luma block and the reference block inside the level, the chroma blocks too.
-__device__ __forceinline__ bool fast_setup(const Ctx &x, const BlkC &b, int mvx, int mvy, int64_t &lref,
-                                           int64_t &cref) {
+__device__ __forceinline__ bool fast_setup(const Ctx &x, const BlkC &b, int mvx, int mvy, int &lref, int &cref) {
     if (!(b.fast_src && mvx >= b.bnd0 && mvx < b.ubx && mvy >= b.bnd1 && mvy < b.uby)) return false;
     const LevelInfo &L = *x.L;
     const Geo &G = x.G;
@@ -578,8 +609,8 @@ __device__ __forceinline__ bool fast_setup(const Ctx &x, const BlkC &b, int mvx,
     if (l0sub) { sub = (mvy & 1) * pel + (mvx & 1); mx = mvx >> 1; my = mvy >> 1; }
     const int rx0 = b.px2 + mx, ry0 = b.py2 + my;
     if (rx0 < 0 || ry0 < 0 || rx0 + b.bw > G.lw || ry0 + b.bh > G.lh) return false;
-    lref = ((int64_t)L.y_off + (int64_t)sub * G.lh + ry0) * G.ys + rx0;
-    if (lref + (int64_t)(b.bh - 1) * G.ys + b.bw + 8 > G.ylen) return false;
+    lref = ((int)L.y_off + sub * G.lh + ry0) * G.ys32 + rx0;
+    if (lref + (b.bh - 1) * G.ys32 + b.bw + 8 > (int)G.ylen) return false;
     cref = 0;
     if (b.chroma && b.cw >= 4 && b.ch >= 4) {
         if (!b.cfast_src) return false;
@@ -588,9 +619,9 @@ __device__ __forceinline__ bool fast_setup(const Ctx &x, const BlkC &b, int mvx,
         else { mcx = mvx >> 1; mcy = mvy >> 1; }
         const int crx = b.cpx + mcx, cry = b.cpy + mcy;
         if (crx < 0 || cry < 0 || crx + b.cw > G.clw || cry + b.ch > G.clh) return false;
-        const int64_t crow0 = (int64_t)L.c_off + ((x.level == 0 && pel > 1) ? (int64_t)sub * G.clh : 0);
-        cref = (crow0 + cry) * G.cs + crx;
-        if (cref + (int64_t)(b.crows - 1) * G.cs + b.cw + 8 > G.clen) return false;
+        const int crow0 = (int)L.c_off + ((x.level == 0 && pel > 1) ? sub * G.clh : 0);
+        cref = (crow0 + cry) * G.cs32 + crx;
+        if (cref + (b.crows - 1) * G.cs32 + b.cw + 8 > (int)G.clen) return false;
     }
     return true;
 }
@@ -630,7 +661,7 @@ __device__ __noinline__ Res slow_lane(const AnalyseParams *P, const LevelInfo *L
 __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, int px, int py, int mvx, int mvy,
                                          bool chroma, int sub) {
     const int G = x.grp_lanes, TL = x.tl, TCp = x.tcp;
-    int64_t lref = 0, cref = 0;
+    int lref = 0, cref = 0;
     bool fast = false;
     if (kind == 0) fast = fast_setup(x, b, mvx, mvy, lref, cref);
     else if (kind == 2) fast = b.dc_fast;
@@ -639,7 +670,7 @@ __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, 
                          mvx, mvy, chroma, x.satd, x.pel, kind == 2, sub, G, TL, TCp);
     Res r{0, 0, 0, 0, 0, 0};
     const int T = TL + (chroma ? 2 * TCp : 0);
-    const int64_t ys = x.G.ys, cs = x.G.cs;
+    const int ys = x.G.ys32, cs = x.G.cs32;
     r.lsatd = kind == 2 ? 0 : b.satd_mode;
     r.cmode = (chroma && b.cw >= 4 && b.ch >= 4) ? CM_DIRECT : CM_NONE;
     r.csatd = x.satd;
@@ -647,8 +678,8 @@ __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, 
 #pragma unroll 1
     for (int t = sub; t < T; t += G) {
         if (t < TL) {
-            const int ty = t / b.tilesx, tx = t - ty * b.tilesx;
-            const int64_t o = (int64_t)ty * 4 * ys + tx * 4;
+            const int ty = t >> b.lgtx, tx = t & (b.tilesx - 1);
+            const int o = ty * 4 * ys + tx * 4;
             if (kind == 2) r.L += tile_sum(sl + o, ys);
             else if (r.lsatd) r.L += tile_satd(sl + o, x.R.y + lref + o, ys);
             else r.L += tile_sad(sl + o, x.R.y + lref + o, ys);
@@ -656,9 +687,9 @@ __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, 
             int ct = t - TL;
             const int pl = ct >= TCp;
             ct -= pl * TCp;
-            const int ty = ct / b.ctilesx, tx = ct - ty * b.ctilesx;
+            const int ty = ct >> b.lgctx, tx = ct & (b.ctilesx - 1);
             if (ty * 4 >= b.crows) continue;
-            const int64_t o = (int64_t)ty * 4 * cs + tx * 4;
+            const int o = ty * 4 * cs + tx * 4;
             const uint8_t *sp = (pl ? x.S.v : x.S.u) + b.csrc + o, *rp = (pl ? x.R.v : x.R.u) + cref + o;
             const unsigned v = r.csatd ? tile_satd(sp, rp, cs) : tile_sad(sp, rp, cs);
             if (pl) r.V += v; else r.U += v;
@@ -678,8 +709,6 @@ __device__ __forceinline__ void finalize(const Res &r, unsigned &L, unsigned &C)
     else C = sat_mul(r.U + r.V, 4);
 }
 
-constexpr int MW = 4;  // validity mask words per chunk: 128 candidates
-
 // One search step: candidates g over the block against the running best `best_cost`.
 // Every warp computes which candidates pass exact_ok and the motion-penalty cut (a
 // ballot bitmask, identical in every warp), then groups take the passing candidates
@@ -696,42 +725,44 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
     int bi = 0x7FFFFFFF;
     unsigned bs = 0;
     win = -1;
+    const unsigned lt_mask = (1u << lane) - 1u;
     for (int base = 0; base < g.n; base += 32 * MW) {
-        unsigned mask[MW];
         int total = 0;
         const long long cut = best_cost;
+        // this warp's copy of the passing candidates, in candidate order (every warp
+        // computes the same list, so no barrier is needed)
 #pragma unroll
         for (int w = 0; w < MW; w++) {
             const int i = base + w * 32 + lane;
             bool ok = i < g.n;
+            int2 mv = make_int2(0, 0);
             if (ok) {
-                const int2 mv = gen_mv(g, i);
+                mv = gen_mv(g, i);
                 ok = mv.x >= b.bnd0 && mv.y >= b.bnd1 && mv.x < b.bnd2 && mv.y < b.bnd3;  // exact_ok
                 if (ok) ok = motion_penalty(lambda, predx, predy, mv.x, mv.y) < cut;  // a later candidate faces a lower best
             }
-            mask[w] = __ballot_sync(0xFFFFFFFFu, ok);
-            total += __popc(mask[w]);
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, ok);
+            if (ok)  // |mv| <= pel * plane size, so each component fits a halfword
+                s.clist[warp][total + __popc(m & lt_mask)] =
+                    make_int2((int)(((unsigned)mv.x & 0xFFFFu) | ((unsigned)mv.y << 16)), i);
+            total += __popc(m);
         }
+        __syncwarp();
         for (int r0 = 0; r0 < total; r0 += NG) {
             const int rk = r0 + grp;
             const bool act = rk < total;
             int i = 0;
-            if (act) {  // the rk-th passing candidate
-                int rem = rk;
-#pragma unroll
-                for (int w = 0; w < MW; w++) {
-                    const int c = __popc(mask[w]);
-                    if (rem >= 0 && rem < c) i = base + w * 32 + (int)__fns(mask[w], 0, rem + 1);
-                    rem -= c;
-                }
-            }
             int2 mv = make_int2(0, 0);
-            int64_t lref = 0, cref = 0;
+            if (act) {  // the rk-th passing candidate
+                const int2 e = s.clist[warp][rk];
+                i = e.y;
+                mv = make_int2((int)(short)(e.x & 0xFFFF), e.x >> 16);
+            }
+            int lref = 0, cref = 0;
             bool fast = false;
             Res r{0, 0, 0, 0, 0, 0};
             long long motion = 0;
             if (act) {
-                mv = gen_mv(g, i);
                 motion = motion_penalty(lambda, predx, predy, mv.x, mv.y);
                 fast = fast_setup(x, b, mv.x, mv.y, lref, cref);
                 if (!fast)
@@ -744,23 +775,24 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                 r.cmode = (b.chroma && b.cw >= 4 && b.ch >= 4) ? CM_DIRECT : CM_NONE;
                 r.csatd = x.satd;
                 const int T = x.tl + (r.cmode != CM_NONE ? 2 * x.tcp : 0);
-                const int swp = b.tilesx, cwp = b.ctilesx, nlw = b.tilesx * b.bh;
+                const int ys = x.G.ys32, cs = x.G.cs32, nlw = b.tilesx * b.bh;
+                const uint8_t *rl = x.R.y + lref;
 #pragma unroll 1
                 for (int t = sub; t < T; t += G) {
                     if (t < x.tl) {
-                        const int ty = t / swp, tx = t - ty * swp;
-                        const uint8_t *rp = x.R.y + lref + (int64_t)ty * 4 * x.G.ys + tx * 4;
-                        const uint32_t *sw = s.srcw + ty * 4 * swp + tx;
-                        r.L += b.satd_mode ? tile_satd_w(sw, swp, rp, x.G.ys) : tile_sad_w(sw, swp, rp, x.G.ys);
+                        const int ty = t >> b.lgtx, tx = t & (b.tilesx - 1);
+                        const uint8_t *rp = rl + (ty * 4 * ys + tx * 4);
+                        const uint2 *sp = s.srcp + ((ty * 4) << b.lgtx) + tx;
+                        r.L += b.satd_mode ? tile_satd_p(sp, b.tilesx, rp, ys) : tile_sad_p(sp, b.tilesx, rp, ys);
                     } else {
                         const int ct0 = t - x.tl;
                         const int pl = ct0 >= x.tcp;
                         const int ct = ct0 - pl * x.tcp;
-                        const int ty = ct / cwp, tx = ct - ty * cwp;
+                        const int ty = ct >> b.lgctx, tx = ct & (b.ctilesx - 1);
                         if (ty * 4 >= b.crows) continue;
-                        const uint8_t *rp = (pl ? x.R.v : x.R.u) + cref + (int64_t)ty * 4 * x.G.cs + tx * 4;
-                        const uint32_t *sw = s.srcw + nlw + pl * cwp * b.crows + ty * 4 * cwp + tx;
-                        const unsigned v = x.satd ? tile_satd_w(sw, cwp, rp, x.G.cs) : tile_sad_w(sw, cwp, rp, x.G.cs);
+                        const uint8_t *rp = (pl ? x.R.v : x.R.u) + cref + (ty * 4 * cs + tx * 4);
+                        const uint2 *sp = s.srcp + nlw + pl * b.ctilesx * b.crows + ((ty * 4) << b.lgctx) + tx;
+                        const unsigned v = x.satd ? tile_satd_p(sp, b.ctilesx, rp, cs) : tile_sad_p(sp, b.ctilesx, rp, cs);
                         if (pl) r.V += v; else r.U += v;
                     }
                 }
@@ -793,6 +825,7 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                 bk = K; bi = i; bs = sad;
             }
         }
+        __syncwarp();  // the next chunk rewrites this warp's list
     }
     if (serial) return;
 #pragma unroll
@@ -971,15 +1004,15 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
         if (b.fast_src) {
             const int nlw = b.tilesx * b.bh;
             for (int t = x.tid; t < nlw; t += NT) {
-                const int row = t / b.tilesx, col = t - row * b.tilesx;
-                s.srcw[t] = ld4u(x.S.y + b.lsrc + (int64_t)row * x.G.ys + col * 4);
+                const int row = t >> b.lgtx, col = t & (b.tilesx - 1);
+                s.srcp[t] = stage4(ld4u(x.S.y + b.lsrc + row * x.G.ys32 + col * 4), b.satd_mode != 0);
             }
             if (b.chroma && b.cfast_src) {
                 const int nc = b.ctilesx * b.crows;
                 for (int t = x.tid; t < 2 * nc; t += NT) {
                     const int pl = t >= nc, u = t - pl * nc;
-                    const int row = u / b.ctilesx, col = u - row * b.ctilesx;
-                    s.srcw[nlw + t] = ld4u((pl ? x.S.v : x.S.u) + b.csrc + (int64_t)row * x.G.cs + col * 4);
+                    const int row = u >> b.lgctx, col = u & (b.ctilesx - 1);
+                    s.srcp[nlw + t] = stage4(ld4u((pl ? x.S.v : x.S.u) + b.csrc + row * x.G.cs32 + col * 4), x.satd != 0);
                 }
             }
         }
@@ -1365,6 +1398,7 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
         x.pel = L.pel;
         x.G.lw = L.lw; x.G.lh = L.lh; x.G.clw = L.lw / 2; x.G.clh = L.lh / 2;
         x.G.ys = P.y_stride; x.G.cs = P.c_stride; x.G.ylen = P.y_len; x.G.clen = P.c_len;
+        x.G.ys32 = (int)P.y_stride; x.G.cs32 = (int)P.c_stride;
         x.tl = L.tl;
         x.tcp = L.tc;
         {  // lanes per candidate: about `tiles_per_lane` 4x4 tiles per lane

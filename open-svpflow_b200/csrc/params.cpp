@@ -25,6 +25,10 @@ bool build_analyse_params(const AnalyseOpts &o, const SuperLayout &Lay, AnalyseP
     P.distance = o.distance; P.coarse_bad_sad = o.coarse_bad_sad; P.coarse_bad_range = o.coarse_bad_range;
     P.coarse_distance = o.coarse_distance; P.vectors = o.vectors;
     P.luma_w = o.width; P.luma_h = o.height; P.pel = o.pel;
+    if (Lay.y_len >= (int64_t)1 << 30 || Lay.c_len >= (int64_t)1 << 30) {  // offsets are 32-bit on the device
+        err = "SVAnalyse: super frames of 2^30 bytes or more are not available on the device path";
+        return false;
+    }
     P.y_stride = Lay.y_stride; P.c_stride = Lay.c_stride; P.y_len = Lay.y_len; P.c_len = Lay.c_len;
     P.frame_bytes = Lay.frame_bytes;
     P.lambda = o.lambda;
