@@ -16,6 +16,17 @@ Multi-GPU: one process per GPU; each rank analyses its own clip (weak scaling, n
 collective); time = max over ranks.
 --impl reference times the CPU restatement of the reference (oracle/) on all host
 threads over a bounded sample of the same workload.
+
+Other workloads (one JSON line each, same keys):
+  --workload batched   64 clips of uneven size and length (resolution from 360p..1440p,
+                       16-240 frames log-uniform, block 8 or 16, else the 1080p options)
+                       analysed by one persistent launch replayed from a CUDA graph, with the
+                       autotuned launch shape; `plain_per_clip` times the same clips through
+                       the per-clip path one after another, and every payload is compared.
+  --workload served    Poisson arrivals of clips (360p..2160p, 8-600 frames) into the
+                       continuous-batching server under an HBM budget, at each --rates value;
+                       p50 / p99 per-frame-pair latency (arrival of the clip to its payload in
+                       host memory) and aggregate frame-pairs/s.
 """
 from __future__ import annotations
 
@@ -34,7 +45,8 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-from svpflow_b200.synth import ANALYSE_OPT, CONFIGS, SUPER_OPT, make_clip  # noqa: E402
+from svpflow_b200.synth import (ANALYSE_OPT, CONFIGS, SUPER_OPT, analyse_opt_for_block, batched_mix,  # noqa: E402
+                                 make_clip, make_clip_device, served_stream)
 
 WORKLOAD = "1080p"
 METRIC = "Analyse frame-pairs/s at 1080p (bit-exact MVs)"
@@ -166,6 +178,248 @@ def run_reference(args, rank: int):
     print(json.dumps(line), flush=True)
 
 
+class _DevBytes:
+    """A device byte range as a torch tensor (CUDA array interface; no copy)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False), "version": 3}
+
+
+def _init_dist(world, local):
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900))
+    return torch, dist
+
+
+def _max_over_ranks(torch, dist, world, v: float, dev) -> float:
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_batched(args, world: int, rank: int, local: int):
+    """Config 4: many clips of uneven size in one persistent launch, against per-clip launches."""
+    torch, dist = _init_dist(world, local)
+    import svpflow_b200 as sv
+
+    dev = torch.device("cuda", local)
+    nclips = args.clips or 64
+    mix = batched_mix(nclips, max_len=args.max_len or 240)
+    mine = [c for i, c in enumerate(mix) if i % world == rank]  # clips are sharded whole across ranks
+    c2 = CONFIGS["1080p"]
+    clips = []
+    t0 = time.perf_counter()
+    for (w, h, n, blk, seed) in mine:
+        sb = sv.Super(w, h, SUPER_OPT["1080p"])
+        an = sv.Analyse(sb.sdata, analyse_opt_for_block(blk), w, h)
+        frames = make_clip_device(w, h, n, seed=seed, motion=c2["motion"], objects=c2["objects"],
+                                  object_motion=c2["object_motion"], device=dev)
+        clips.append((sb, an, frames))
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    b = sv.Batch([(sb, an, fr.shape[0]) for sb, an, fr in clips])
+    for i, (_, _, fr) in enumerate(clips):
+        torch.as_tensor(_DevBytes(b.frames_device(i), fr.numel()), device=dev).copy_(fr.reshape(-1))
+    torch.cuda.synchronize()
+    tune = b.autotune() if not args.no_autotune else {"trial_pairs_per_s": None, **b.shape()}
+    stream = torch.cuda.Stream(dev)
+    sh = stream.cuda_stream
+    pairs = b.pairs
+    for _ in range(args.warmup):
+        b.launch(sh)
+    b.status(sh)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sv.reset_kernel_launches()
+    with ClockSampler(_gpu_id(torch, local)) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            b.launch(sh)
+        stop.record(stream)
+        torch.cuda.synchronize()
+    launches = sv.kernel_launches()
+    b.status(sh)
+    ms = _max_over_ranks(torch, dist, world, start.elapsed_time(stop), dev)
+    total_pairs = sum(n for (_, _, n, _, _) in mix)  # all ranks' clips; time is the slowest rank's
+    assert world > 1 or total_pairs == pairs
+    value = total_pairs * args.steps / (ms / 1000.0)
+
+    # the same clips through the per-clip (plain) path, one launch sequence per clip
+    max_src = max(fr.numel() for _, _, fr in clips)
+    max_sup = max(sb.output_len() * fr.shape[0] for sb, _, fr in clips)
+    max_pay = max(an.payload_len() * fr.shape[0] for _, an, fr in clips)
+    max_scr = max(an.scratch_bytes(fr.shape[0]) for _, an, fr in clips)
+    sup_d = torch.empty(max_sup, dtype=torch.uint8, device=dev)
+    pay_d = torch.empty(max_pay, dtype=torch.uint8, device=dev)
+    scr_d = torch.empty(max_scr, dtype=torch.uint8, device=dev)
+    del max_src
+    same = True
+    plain_ms = 0.0
+    with torch.cuda.stream(stream):
+        for i, (sb, an, fr) in enumerate(clips):
+            n = fr.shape[0]
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sb.build_device(fr.data_ptr(), sup_d.data_ptr(), n, sh)
+            an.analyse_clip_device(sup_d.data_ptr(), n, 0, n, pay_d.data_ptr(), scr_d.data_ptr(), sh)
+            e1.record(stream)
+            sv.Analyser.device_status(scr_d.data_ptr(), sh)
+            plain_ms += e0.elapsed_time(e1)
+            L = an.payload_len() * n
+            got = torch.as_tensor(_DevBytes(b.payloads_device(i), L), device=dev)
+            same = same and bool(torch.equal(got, pay_d[:L]))
+    plain_ms = _max_over_ranks(torch, dist, world, plain_ms, dev)
+    plain_value = total_pairs / (plain_ms / 1000.0)
+
+    # end to end through the host-buffer batch call (pinned frames in, payloads out)
+    host_frames = [fr.cpu().pin_memory() for _, _, fr in clips]
+    host_pay = [torch.empty((fr.shape[0], an.payload_len()), dtype=torch.uint8).pin_memory() for _, an, fr in clips]
+    hf = [t.numpy() for t in host_frames]
+    hp = [t.numpy() for t in host_pay]
+    b.run(hf, hp)
+    e2e_value = None
+    if args.e2e_steps > 0:
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            b.run(hf, hp)
+        e2e_s = _max_over_ranks(torch, dist, world, time.perf_counter() - t0, dev)
+        e2e_value = total_pairs * args.e2e_steps / e2e_s
+    e2e_same = all(bool(np.array_equal(hp[i].reshape(-1), torch.as_tensor(
+        _DevBytes(b.payloads_device(i), hp[i].size), device=dev).cpu().numpy())) for i in range(len(clips)))
+    if rank == 0:
+        res = {}
+        for (w, h, n, blk, _) in mix:
+            k = f"{w}x{h}/b{blk}"
+            res[k] = res.get(k, 0) + n
+        line = {
+            "metric": "Analyse frame-pairs/s, batched (64 mixed clips, one persistent launch; bit-exact MVs)",
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "u8", "data": "synthetic",
+            "config": {"workload": f"batched: {nclips} clips, resolution from 640x360/1280x720/1920x1080/2560x1440, "
+                                   f"{min(n for _, _, n, _, _ in mix)}-{max(n for _, _, n, _, _ in mix)} frames "
+                                   f"(log-uniform 16-{args.max_len or 240}), block 8 or 16 with overlap half a block, "
+                                   f"Super {{pel:2}}, UMH r16, SATD + chroma, fwd+bwd",
+                       "clips": nclips, "pairs": total_pairs, "pairs_by_shape": res,
+                       "l2": "inputs larger than L2", "parallelism": f"clips sharded over {world} GPU(s)",
+                       "device_bytes_per_gpu": b.device_bytes, "generation_s": gen_s},
+            "launch_shape": tune,
+            "clocks": clk.summary(),
+            "plain_per_clip": {"value": plain_value, "unit": UNIT, "ms": plain_ms,
+                               "how": "Super + svpf_clip_analyse_device per clip, clips one after another"},
+            "batched_over_plain": value / plain_value,
+            "payloads_equal_plain": same,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(sum(t.numel() for t in host_frames)),
+                    "d2h_bytes_per_step": int(sum(t.numel() for t in host_pay)),
+                    "api": "svpf_batch_run (host buffers)", "matches_device_path": e2e_same},
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_served(args, world: int, rank: int, local: int):
+    """Config 5: Poisson arrivals into the continuous-batching server; per-pair latency."""
+    torch, dist = _init_dist(world, local)
+    import svpflow_b200 as sv
+
+    dev = torch.device("cuda", local)
+    nclips = args.clips or 16
+    rates = [float(r) for r in args.rates.split(",") if r]
+    c2 = CONFIGS["1080p"]
+    base = served_stream(nclips, 1.0, seed=5 + rank, max_len=args.max_len or 600)  # clip shapes (same for every rate)
+    handles, frames = {}, []
+    t0 = time.perf_counter()
+    for (_, w, h, n, seed) in base:
+        if (w, h) not in handles:
+            sb = sv.Super(w, h, SUPER_OPT["1080p"])
+            handles[(w, h)] = (sb, sv.Analyse(sb.sdata, ANALYSE_OPT["1080p"], w, h))
+        fr = make_clip_device(w, h, n, seed=seed, motion=c2["motion"], objects=c2["objects"],
+                              object_motion=c2["object_motion"], device=dev)
+        frames.append(fr.cpu().pin_memory().numpy())
+        del fr
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    budget = int(args.budget_gb * (1 << 30))
+    total_pairs = sum(n for (_, _, _, n, _) in base)
+    # identity: a small clip served alone equals the plain path
+    k_small = min(range(nclips), key=lambda i: base[i][3] * base[i][1] * base[i][2])
+    sb0, an0 = handles[(base[k_small][1], base[k_small][2])]
+    want_small = an0.analyse_clip(sb0, frames[k_small])
+    sweep = []
+    for wi, rate in enumerate(rates):
+        arrivals = [t for (t, _, _, _, _) in served_stream(nclips, rate, seed=5 + rank, max_len=args.max_len or 600)]
+        srv = sv.Server(budget, max_active=8, chunk_pairs=32)
+        ids = []
+        if wi == 0:  # warm-up request (not measured)
+            rid = srv.submit(sb0, an0, frames[k_small])
+            srv.wait(rid)
+        if world > 1:
+            dist.barrier()
+        t_start = srv.now_ns()
+        for k, (_, w, h, n, _) in enumerate(base):
+            due = t_start + int(arrivals[k] * 1e9)
+            while srv.now_ns() < due:
+                time.sleep(min(0.002, max(0.0, (due - srv.now_ns()) / 1e9)))
+            sb, an = handles[(w, h)]
+            ids.append(srv.submit(sb, an, frames[k]))
+        lat = []
+        done_last = 0
+        identical = True
+        for k, rid in enumerate(ids):
+            pay, done, (arr, adm, fin) = srv.wait(rid)
+            lat.extend(((done - arr) / 1e6).tolist())
+            done_last = max(done_last, fin)
+            if k == k_small:
+                identical = bool(np.array_equal(pay, want_small))
+        span_s = (done_last - t_start) / 1e9
+        st = srv.stats()
+        srv.close()
+        lat = np.asarray(lat)
+        sweep.append({"rate_clips_per_s": rate, "pairs": total_pairs, "span_s": span_s,
+                      "pairs_per_s": total_pairs / span_s, "p50_ms": float(np.percentile(lat, 50)),
+                      "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
+                      "peak_active_clips": st["peak_active"], "peak_device_gb": st["peak_device_bytes"] / 2 ** 30,
+                      "kernel_launches": st["kernel_launches"], "small_clip_identical_to_alone": identical})
+    if rank == 0:
+        best = max(sweep, key=lambda r: r["pairs_per_s"])
+        line = {
+            "metric": "served Analyse frame-pairs/s and p50/p99 per-frame-pair latency (bit-exact MVs)",
+            "value": best["pairs_per_s"], "unit": UNIT, "n_gpus": world, "steps": len(rates), "warmup": 1,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8", "data": "synthetic",
+            "config": {"workload": f"served: {nclips} clips per rate, Poisson arrivals, resolution from "
+                                   f"360p/720p/1080p/1440p/2160p, 8-{args.max_len or 600} frames log-uniform, "
+                                   f"1080p Analyse options, HBM budget {args.budget_gb} GB, 8 active clips, "
+                                   f"chunks of 32 pairs", "pairs_per_rate": total_pairs, "generation_s": gen_s,
+                       "latency": "clip arrival to that pair's payload in host memory"},
+            "sweep": sweep,
+            "e2e": {"value": best["pairs_per_s"], "unit": UNIT,
+                    "h2d_bytes_per_step": int(sum(f.nbytes for f in frames)),
+                    "d2h_bytes_per_step": int(sum(handles[(w, h)][1].payload_len() * n for (_, w, h, n, _) in base)),
+                    "api": "svpf_server_submit / svpf_server_wait (host buffers)"},
+            "gpu_launches": int(sum(r["kernel_launches"] for r in sweep)),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -176,6 +430,12 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-pairs", type=int, default=0, help="CPU baseline sample (0 = one per host thread)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="1080p", choices=["1080p", "batched", "served"])
+    ap.add_argument("--clips", type=int, default=0, help="batched: clips (default 64); served: clips per rate (16)")
+    ap.add_argument("--max-len", type=int, default=0, help="longest clip in frames (default: the workload's)")
+    ap.add_argument("--rates", default="5,50,200", help="served: arrival rates, clips/s")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="served: HBM budget")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -183,6 +443,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.workload == "batched":
+        return run_batched(args, world, rank, local)
+    if args.workload == "served":
+        return run_served(args, world, rank, local)
 
     import torch
     import torch.distributed as dist

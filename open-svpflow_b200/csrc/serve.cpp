@@ -15,9 +15,16 @@
 // payload copy: the time the payload is in host memory. A clip's arrival time is taken at
 // submit, so pair latency = done - arrival includes queueing for admission.
 //
+// Payloads go to page-locked memory directly. A pageable destination would make each
+// copy wait for its chunk inside the scheduler thread, so those chunks land in the
+// slot's page-locked staging buffer and the host function copies them out. No CUDA call
+// is ever made while the server's lock is held: host functions take that lock, and a
+// synchronising call (cudaFreeHost, cudaFree) under it could wait on them for ever.
+//
 // Results do not depend on the mix: every pair runs the same kernel on its own two super
 // frames, whatever else shares the device.
 #include <cuda_runtime.h>
+#include <string.h>
 
 #include <atomic>
 #include <chrono>
@@ -45,6 +52,7 @@ struct Request;
 struct Chunk {
     Request *req;
     int32_t first, count;
+    uint8_t *stage;  // page-locked staging of the chunk's payloads, or null (copied to the destination directly)
 };
 
 struct Request {
@@ -59,7 +67,7 @@ struct Request {
     int64_t need = 0;
     int slot = -1;
     uint8_t *dev = nullptr;
-    int *status_host = nullptr;  // pinned
+    bool pinned_out = false;     // payloads are page-locked host memory
     int status = 0;
     bool done = false;
     std::vector<Chunk> chunks;
@@ -76,6 +84,10 @@ struct svpf_server {
     int32_t chunk_pairs = 32;
     std::vector<cudaStream_t> streams;
     std::vector<bool> slot_busy;
+    int *slot_status = nullptr;                 // page-locked status word per slot
+    std::vector<uint8_t *> stage;               // page-locked payload staging per slot (scheduler-owned)
+    std::vector<size_t> stage_cap;
+    std::vector<uint8_t *> retired;             // outgrown staging buffers, freed at destroy
     std::deque<Request *> pending;
     std::map<int64_t, std::unique_ptr<Request>> requests;
     int64_t next_id = 1, admitted = 0, completed = 0;
@@ -109,13 +121,16 @@ void CUDART_CB chunk_done(void *arg) {
     Chunk *ch = (Chunk *)arg;
     Request *r = ch->req;
     svpf_server *s = r->server;
-    const int64_t t = s->now_ns();
+    const int64_t t0 = s->now_ns();
+    if (ch->stage)
+        memcpy(r->payloads + (int64_t)ch->first * r->P.payload_len, ch->stage, (size_t)(r->P.payload_len * ch->count));
+    const int64_t t = ch->stage ? s->now_ns() : t0;
     if (r->pair_done_ns)
         for (int32_t i = 0; i < ch->count; i++) r->pair_done_ns[ch->first + i] = t;
     if (r->chunks_left.fetch_sub(1) == 1) {
         std::lock_guard<std::mutex> lk(s->mu);
         r->done_ns = t;
-        r->status = *r->status_host;
+        r->status = s->slot_status[r->slot];
         r->done = true;
         s->used -= r->need;
         s->active--;
@@ -140,6 +155,19 @@ int enqueue(svpf_server *s, Request *r) {
     uint8_t *pays = supers + al256(fb * r->nframes);
     uint8_t *scr = pays + al256(r->P.payload_len * r->nframes);
     int *status = (int *)(scr + al256(r->P.scratch_per_pair * (r->chunks.empty() ? 1 : r->chunks[0].count)));
+    uint8_t *stage = nullptr;
+    if (!r->pinned_out) {  // this thread owns the slot's staging buffer while the slot is busy
+        const size_t need = (size_t)(r->P.payload_len * (r->chunks.empty() ? 1 : r->chunks[0].count));
+        const size_t k = (size_t)r->slot;
+        if (s->stage_cap[k] < need) {
+            if (s->stage[k]) s->retired.push_back(s->stage[k]);
+            s->stage[k] = nullptr;
+            s->stage_cap[k] = 0;
+            if (cudaHostAlloc((void **)&s->stage[k], need, cudaHostAllocDefault) != cudaSuccess) return SVPF_ECUDA;
+            s->stage_cap[k] = need;
+        }
+        stage = s->stage[k];
+    }
     int nl = 0;
     e = cudaMemsetAsync(status, 0, sizeof(int), st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(frames, r->frames, (size_t)(sb * r->nframes), cudaMemcpyHostToDevice, st);
@@ -153,11 +181,13 @@ int enqueue(svpf_server *s, Request *r) {
         src.nframes = r->nframes;
         src.delta = r->delta;
         e = launch_analyse(r->P, src, c.count, pays + (int64_t)c.first * r->P.payload_len, scr, status, st, &nl);
+        c.stage = stage;
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(r->payloads + (int64_t)c.first * r->P.payload_len, pays + (int64_t)c.first * r->P.payload_len,
-                                (size_t)(r->P.payload_len * c.count), cudaMemcpyDeviceToHost, st);
+            e = cudaMemcpyAsync(stage ? stage : r->payloads + (int64_t)c.first * r->P.payload_len,
+                                pays + (int64_t)c.first * r->P.payload_len, (size_t)(r->P.payload_len * c.count),
+                                cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess && k + 1 == r->chunks.size()) {
-            e = cudaMemcpyAsync(r->status_host, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+            e = cudaMemcpyAsync(&s->slot_status[r->slot], status, sizeof(int), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaFreeAsync(r->dev, st);
             if (e == cudaSuccess) r->dev = nullptr;
         }
@@ -242,6 +272,12 @@ int svpf_server_create(size_t hbm_budget_bytes, int32_t max_active, int32_t chun
     }
     s->streams.assign((size_t)max_active, nullptr);
     s->slot_busy.assign((size_t)max_active, false);
+    s->stage.assign((size_t)max_active, nullptr);
+    s->stage_cap.assign((size_t)max_active, 0);
+    if (cudaHostAlloc((void **)&s->slot_status, sizeof(int) * (size_t)max_active, cudaHostAllocDefault) != cudaSuccess) {
+        delete s;
+        return sfail(SVPF_ECUDA, "cudaHostAlloc (status words)");
+    }
     for (auto &st : s->streams) {
         cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
         if (e != cudaSuccess) {
@@ -276,14 +312,13 @@ int svpf_server_submit(svpf_server *s, const svpf_super *sup, const svpf_analyse
     r->chunks_left = (int)r->chunks.size();
     r->need = request_bytes(*r, s->chunk_pairs);
     if (r->need > s->budget) return sfail(SVPF_EINVAL, "clip needs more device memory than the server's budget");
-    if (cudaHostAlloc((void **)&r->status_host, sizeof(int), cudaHostAllocDefault) != cudaSuccess)
-        return sfail(SVPF_ECUDA, "cudaHostAlloc (status word)");
-    *r->status_host = 0;
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (s->stopping) {
-        cudaFreeHost(r->status_host);
-        return sfail(SVPF_EINVAL, "server is shutting down");
+    {
+        cudaPointerAttributes pa;
+        r->pinned_out = cudaPointerGetAttributes(&pa, payloads) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+        cudaGetLastError();  // a pageable pointer is not an error here
     }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) return sfail(SVPF_EINVAL, "server is shutting down");
     r->id = s->next_id++;
     if (request) *request = r->id;
     s->pending.push_back(r.get());
@@ -300,7 +335,6 @@ int svpf_server_wait(svpf_server *s, int64_t request, int64_t *times) {
     s->done_cv.wait(lk, [&] { return r->done; });
     if (times) { times[0] = r->arrival_ns; times[1] = r->admit_ns; times[2] = r->done_ns; }
     const int st = r->status;
-    cudaFreeHost(r->status_host);
     s->requests.erase(it);
     if (st < 0) return sfail(SVPF_EINVAL, "server shut down before the request started");
     if (st & 1) return sfail(SVPF_EPANIC, "SVAnalyse: the reference indexes out of range on this input (it panics)");
@@ -337,8 +371,10 @@ void svpf_server_destroy(svpf_server *s) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
     }
-    for (auto &kv : s->requests)
-        if (kv.second->status_host) cudaFreeHost(kv.second->status_host);
+    for (uint8_t *p : s->stage)
+        if (p) cudaFreeHost(p);
+    for (uint8_t *p : s->retired) cudaFreeHost(p);
+    if (s->slot_status) cudaFreeHost(s->slot_status);
     delete s;
 }
 

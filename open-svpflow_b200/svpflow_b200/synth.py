@@ -97,18 +97,19 @@ def make_clip(width: int, height: int, frames: int, seed: int, motion: int = 8, 
 
 
 def make_clip_device(width: int, height: int, frames: int, seed: int, motion: int = 8, objects: int = 4,
-                     object_motion: int = 16, noise: float = 2.0, device="cuda"):
-    """The same generator as make_clip, run with torch on the device (for the large batched
-    and served workloads, where the host generator would take minutes). Same recipe and
-    statistics; a different random stream, so frames differ from make_clip's. Returns a
-    uint8 tensor [frames, w*h + 2*(w/2*h/2)] on `device`."""
+                     object_motion: int = 16, noise: float = 2.0, device="cuda", chunk: int = 32):
+    """The recipe of make_clip, run with torch on the device and vectorised over frames (for
+    the large batched and served workloads, where the host generator would take minutes).
+    Differences: its own random stream, and frame k's background is frame 0's shifted once
+    by the accumulated global motion (edges replicated) rather than shifted frame by frame.
+    Returns a uint8 tensor [frames, w*h + 2*(w/2*h/2)] on `device`."""
     import torch
 
     assert width % 2 == 0 and height % 2 == 0
+    F = torch.nn.functional
     g = torch.Generator(device=device)
     g.manual_seed(int(seed))
     cw, ch = width // 2, height // 2
-    F = torch.nn.functional
 
     def blur(img, sigma):
         k = torch.from_numpy(_kernel(sigma)).to(device)
@@ -118,48 +119,52 @@ def make_clip_device(width: int, height: int, frames: int, seed: int, motion: in
         x = F.pad(x, (0, 0, r, r), mode="replicate")
         return F.conv2d(x, k.view(1, 1, -1, 1))[0, 0]
 
-    def rint(lo, hi):  # uniform integer in [lo, hi)
-        return int(torch.randint(lo, hi, (1,), generator=g, device=device).item())
-
     def noise_img(h, w):
         return torch.randint(0, 256, (h, w), generator=g, device=device).float()
 
-    clean = [blur(noise_img(height, width), 2.0), blur(noise_img(ch, cw), 1.0), blur(noise_img(ch, cw), 1.0)]
+    rng = np.random.default_rng(int(seed))
+    base = [blur(noise_img(height, width), 2.0), blur(noise_img(ch, cw), 1.0), blur(noise_img(ch, cw), 1.0)]
     objs = []
     for _ in range(objects):
-        oh, ow = rint(32, 97), rint(32, 97)
+        oh, ow = int(rng.integers(32, 97)), int(rng.integers(32, 97))
         tex = [blur(noise_img(oh, ow), 2.0), blur(noise_img(max(oh // 2, 1), max(ow // 2, 1)), 1.0),
                blur(noise_img(max(oh // 2, 1), max(ow // 2, 1)), 1.0)]
-        objs.append((oh, ow, rint(0, max(height - oh, 1)), rint(0, max(width - ow, 1)),
-                     rint(-object_motion, object_motion + 1), rint(-object_motion, object_motion + 1), tex))
-
-    def shift(img, dy, dx):
-        h, w = img.shape
-        ys = (torch.arange(h, device=device) - dy).clamp(0, h - 1)
-        xs = (torch.arange(w, device=device) - dx).clamp(0, w - 1)
-        return img[ys][:, xs]
-
+        objs.append((oh, ow, int(rng.integers(0, max(height - oh, 1))), int(rng.integers(0, max(width - ow, 1))),
+                     int(rng.integers(-object_motion, object_motion + 1)),
+                     int(rng.integers(-object_motion, object_motion + 1)), tex))
+    steps = rng.integers(-motion, motion + 1, size=(frames, 2))
+    steps[0] = 0
+    cum = np.cumsum(steps, axis=0)  # accumulated (dy, dx) of every frame
     ysz, csz = width * height, cw * ch
     out = torch.empty((frames, ysz + 2 * csz), dtype=torch.uint8, device=device)
-    for f in range(frames):
-        if f > 0:
-            dy, dx = rint(-motion, motion + 1), rint(-motion, motion + 1)
-            clean = [shift(clean[0], dy, dx), shift(clean[1], dy // 2, dx // 2), shift(clean[2], dy // 2, dx // 2)]
-        planes = [p.clone() for p in clean]
-        for oh, ow, y0, x0, vy, vx, tex in objs:
-            oy = (y0 + f * vy) % max(height - oh, 1)
-            ox = (x0 + f * vx) % max(width - ow, 1)
-            planes[0][oy:oy + oh, ox:ox + ow] = tex[0][:min(oh, height - oy), :min(ow, width - ox)]
-            for p in (1, 2):
-                t = tex[p]
-                cy, cx = oy // 2, ox // 2
-                planes[p][cy:cy + t.shape[0], cx:cx + t.shape[1]] = t[:min(t.shape[0], ch - cy), :min(t.shape[1], cw - cx)]
-        for i, p in enumerate(planes):
-            q = (p + noise * torch.randn(p.shape, generator=g, device=device)).round().clamp(0, 255).to(torch.uint8)
-            if i == 0:
-                out[f, :ysz] = q.reshape(-1)
+    dims = [(height, width, 1), (ch, cw, 2), (ch, cw, 2)]
+    for f0 in range(0, frames, chunk):
+        f1 = min(frames, f0 + chunk)
+        n = f1 - f0
+        fidx = torch.arange(n, device=device)
+        for pi, (h, w, div) in enumerate(dims):
+            dy = torch.from_numpy(cum[f0:f1, 0] // div).to(device)
+            dx = torch.from_numpy(cum[f0:f1, 1] // div).to(device)
+            ys = (torch.arange(h, device=device)[None, :] - dy[:, None]).clamp(0, h - 1)  # [n, h]
+            xs = (torch.arange(w, device=device)[None, :] - dx[:, None]).clamp(0, w - 1)  # [n, w]
+            planes = base[pi][ys[:, :, None], xs[:, None, :]]                               # [n, h, w]
+            for oh, ow, y0, x0, vy, vx, tex in objs:
+                t = tex[pi]
+                th, tw = t.shape
+                for k in range(n):  # per-frame rectangle paste (position wraps like make_clip's)
+                    f = f0 + k
+                    oy = (y0 + f * vy) % max(height - oh, 1)
+                    ox = (x0 + f * vx) % max(width - ow, 1)
+                    if div == 2:
+                        oy, ox = oy // 2, ox // 2
+                    hh, ww = min(th, h - oy), min(tw, w - ox)
+                    planes[k, oy:oy + hh, ox:ox + ww] = t[:hh, :ww]
+            q = (planes + noise * torch.randn(planes.shape, generator=g, device=device)).round_().clamp_(0, 255)
+            q = q.to(torch.uint8).reshape(n, -1)
+            if pi == 0:
+                out[f0:f1, :ysz] = q
             else:
-                out[f, ysz + (i - 1) * csz: ysz + i * csz] = q.reshape(-1)
+                out[f0:f1, ysz + (pi - 1) * csz: ysz + pi * csz] = q
     return out
 
 
