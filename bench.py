@@ -228,6 +228,9 @@ def run_batched(args, world: int, rank: int, local: int):
     for i, (_, _, fr) in enumerate(clips):
         torch.as_tensor(_DevBytes(b.frames_device(i), fr.numel()), device=dev).copy_(fr.reshape(-1))
     torch.cuda.synchronize()
+    host_frames = [fr.cpu().pin_memory() for _, _, fr in clips]  # for the end-to-end run
+    clips = [(sb, an, fr.shape[0]) for sb, an, fr in clips]      # the batch holds the device frames now
+    torch.cuda.empty_cache()
     tune = b.autotune() if not args.no_autotune else {"trial_pairs_per_s": None, **b.shape()}
     stream = torch.cuda.Stream(dev)
     sh = stream.cuda_stream
@@ -254,22 +257,19 @@ def run_batched(args, world: int, rank: int, local: int):
     value = total_pairs * args.steps / (ms / 1000.0)
 
     # the same clips through the per-clip (plain) path, one launch sequence per clip
-    max_src = max(fr.numel() for _, _, fr in clips)
-    max_sup = max(sb.output_len() * fr.shape[0] for sb, _, fr in clips)
-    max_pay = max(an.payload_len() * fr.shape[0] for _, an, fr in clips)
-    max_scr = max(an.scratch_bytes(fr.shape[0]) for _, an, fr in clips)
+    max_sup = max(sb.output_len() * n for sb, _, n in clips)
+    max_pay = max(an.payload_len() * n for _, an, n in clips)
+    max_scr = max(an.scratch_bytes(n) for _, an, n in clips)
     sup_d = torch.empty(max_sup, dtype=torch.uint8, device=dev)
     pay_d = torch.empty(max_pay, dtype=torch.uint8, device=dev)
     scr_d = torch.empty(max_scr, dtype=torch.uint8, device=dev)
-    del max_src
     same = True
     plain_ms = 0.0
     with torch.cuda.stream(stream):
-        for i, (sb, an, fr) in enumerate(clips):
-            n = fr.shape[0]
+        for i, (sb, an, n) in enumerate(clips):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            sb.build_device(fr.data_ptr(), sup_d.data_ptr(), n, sh)
+            sb.build_device(b.frames_device(i), sup_d.data_ptr(), n, sh)
             an.analyse_clip_device(sup_d.data_ptr(), n, 0, n, pay_d.data_ptr(), scr_d.data_ptr(), sh)
             e1.record(stream)
             sv.Analyser.device_status(scr_d.data_ptr(), sh)
@@ -281,8 +281,8 @@ def run_batched(args, world: int, rank: int, local: int):
     plain_value = total_pairs / (plain_ms / 1000.0)
 
     # end to end through the host-buffer batch call (pinned frames in, payloads out)
-    host_frames = [fr.cpu().pin_memory() for _, _, fr in clips]
-    host_pay = [torch.empty((fr.shape[0], an.payload_len()), dtype=torch.uint8).pin_memory() for _, an, fr in clips]
+    del sup_d, pay_d, scr_d
+    host_pay = [torch.empty((n, an.payload_len()), dtype=torch.uint8).pin_memory() for _, an, n in clips]
     hf = [t.numpy() for t in host_frames]
     hp = [t.numpy() for t in host_pay]
     b.run(hf, hp)
