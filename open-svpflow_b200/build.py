@@ -21,6 +21,9 @@ CORE = os.path.join(LIB_DIR, "libsvpflow_b200.so")
 SOURCES = ["analyse_nt128.cu", "analyse_nt64.cu", "analyse_nt32.cu", "variants.cpp", "params.cpp", "super.cu",
            "opts.cpp", "capi.cpp", "noalloc.cu", "batch.cpp", "serve.cpp"]
 OBJ_DIR = os.path.join(LIB_DIR, "obj")
+# the VapourSynth plugin: the reference plugin's exports over the same objects
+VS_PLUGIN = os.path.join(LIB_DIR, "libsvpflow1_vs.so")
+VS_SOURCES = ["vs_plugin.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-v", "-cudart", "static",
          "--diag-suppress", "177"]
@@ -43,18 +46,22 @@ def _compile(src: str):
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(OBJ_DIR, exist_ok=True)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "svpflow_b200.h")]
-    if force or _stale(CORE, deps):
-        srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    if force or _stale(CORE, deps) or _stale(VS_PLUGIN, deps):
+        srcs = [os.path.join(CSRC, s) for s in SOURCES + VS_SOURCES]
         with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
             results = list(ex.map(_compile, srcs))
         log = "".join(f"==== {os.path.basename(o)}\n{out}" for o, _, out in results)
         bad = [o for o, rc, _ in results if rc != 0]
-        if not bad:
-            cmd = ["nvcc", *ARCH, "-shared", "-cudart", "static", "-o", CORE] + [o for o, _, _ in results]
+        core_objs = [o for o, _, _ in results[:len(SOURCES)]]
+        vs_objs = [o for o, _, _ in results[len(SOURCES):]]
+        for target, objs in ((CORE, core_objs), (VS_PLUGIN, core_objs + vs_objs)):
+            if bad:
+                break
+            cmd = ["nvcc", *ARCH, "-shared", "-cudart", "static", "-o", target] + objs
             r = subprocess.run(cmd, capture_output=True, text=True)
-            log += "==== link\n" + r.stdout + r.stderr
+            log += f"==== link {os.path.basename(target)}\n" + r.stdout + r.stderr
             if r.returncode != 0:
-                bad = ["link"]
+                bad = ["link " + os.path.basename(target)]
         with open(os.path.join(LIB_DIR, "ptxas.log"), "w") as f:
             f.write(log)
         if bad:

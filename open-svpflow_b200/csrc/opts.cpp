@@ -592,12 +592,14 @@ void vdata_header(const AnalyseOpts &o, int32_t h[16]) {
     h[5] = o.has_refine_thsad ? 1 : o.levels; h[7] = o.width; h[8] = o.height; h[9] = ox; h[10] = oy;
     h[11] = gw; h[12] = gh; h[13] = o.selector; h[14] = o.delta;
 }
-SuperLayout portable_layout(const SuperOpts &so) {
+SuperLayout portable_layout(const SuperOpts &so) { return strided_layout(so, so.width, so.width / 2); }
+
+SuperLayout strided_layout(const SuperOpts &so, int64_t y_stride, int64_t c_stride) {
     SuperLayout L;
     L.width = so.width; L.height = so.height; L.pel = so.pel; L.levels = so.levels; L.full = so.full;
     L.super_h = super_plane_height(so.height, so.pel, so.levels, so.full);
-    L.y_stride = so.width;
-    L.c_stride = so.width / 2;
+    L.y_stride = y_stride;
+    L.c_stride = c_stride;
     L.y_len = L.y_stride * (int64_t)L.super_h;
     L.c_len = L.c_stride * (int64_t)(L.super_h / 2);
     L.frame_bytes = L.y_len + 2 * L.c_len;

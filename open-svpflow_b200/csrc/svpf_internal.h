@@ -71,6 +71,9 @@ void level_grid(const AnalyseOpts &o, int32_t level, int32_t &gw, int32_t &gh);
 size_t payload_len(const AnalyseOpts &o);
 void vdata_header(const AnalyseOpts &o, int32_t h[16]);
 SuperLayout portable_layout(const SuperOpts &so);
+// The same planes with other row pitches (a frame server's frames): Y y_stride x H, then U
+// and V c_stride x H/2 each, contiguous.
+SuperLayout strided_layout(const SuperOpts &so, int64_t y_stride, int64_t c_stride);
 
 // ---- device parameter block for one Analyse configuration (analyse.cu) ----
 struct LevelInfo {

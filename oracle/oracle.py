@@ -572,3 +572,54 @@ def level_grid(ao: AnalyseOpts, level: int):
     gw, gh = ctypes.c_int32(), ctypes.c_int32()
     lib().or_level_grid(ctypes.byref(ao), level, ctypes.byref(gw), ctypes.byref(gh))
     return gw.value, gh.value
+
+
+def build_super_strided(so: SuperOpts, src: np.ndarray, y_stride: int, c_stride: int) -> np.ndarray:
+    """A frame server's Super frame (super_filter.rs:210-262): zeroed planes at the given row
+    pitches (Y y_stride x H, then U and V c_stride x H/2), each built by build_plane from
+    the packed I420 source. Returned as one buffer Y | U | V."""
+    src = np.ascontiguousarray(src, dtype=np.uint8)
+    w, h = so.width, so.height
+    cw, ch = w // 2, h // 2
+    H = super_height(so)
+    out = np.zeros(y_stride * H + 2 * c_stride * (H // 2), dtype=np.uint8)
+    planes = [(0, y_stride, H, src[: w * h], w, w, h, 0),
+              (y_stride * H, c_stride, H // 2, src[w * h: w * h + cw * ch], cw, cw, ch, 1),
+              (y_stride * H + c_stride * (H // 2), c_stride, H // 2, src[w * h + cw * ch:], cw, cw, ch, 1)]
+    for off, st, rows, s, sst, pw, ph, chroma in planes:
+        s = np.ascontiguousarray(s)
+        dst = out[off: off + st * rows]
+        lib().or_build_plane(_ptr(dst), dst.size, st, _ptr(s), s.size, sst, pw, ph, w, h, chroma, ctypes.byref(so))
+    return out
+
+
+def analyse_strided(ao: AnalyseOpts, cur: np.ndarray, ref: np.ndarray, y_stride: int, c_stride: int) -> np.ndarray:
+    """get_frame_analyse's payload (analyse_filter.rs:287-325) for two super frames laid out
+    as build_super_strided returns them."""
+    y_h = lib().or_super_plane_height(ao.height, ao.pel, ao.super_levels, 1)
+    uv_h = y_h // 2
+    keep = []
+
+    def planes(buf):
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        keep.append(buf)
+        base = buf.ctypes.data
+        yl, cl = y_stride * y_h, c_stride * uv_h
+        return Planes(base, yl, y_stride, base + yl, cl, c_stride, base + yl + cl, cl, c_stride,
+                      ao.width, ao.height, ao.pel, ao.super_levels, 1)
+
+    pc, pr = planes(cur), planes(ref)
+    bw, bh, ox, oy = (ctypes.c_int32() for _ in range(4))
+    lib().or_output_block(ctypes.byref(ao), ctypes.byref(bw), ctypes.byref(bh), ctypes.byref(ox), ctypes.byref(oy))
+    gw, gh = ctypes.c_int32(), ctypes.c_int32()
+    lib().or_grid(ctypes.byref(ao), bw, bh, ox, oy, ctypes.byref(gw), ctypes.byref(gh))
+    n = gw.value * gh.value
+    bwd, fwd = (Vec8 * n)(), (Vec8 * n)()
+    rc = lib().or_analyse_pair(ctypes.byref(pc), ctypes.byref(pr), ctypes.byref(ao),
+                               bwd if ao.vectors & 1 else None, fwd if ao.vectors & 2 else None)
+    if rc:
+        raise RuntimeError("the reference panics on this input (index out of range)")
+    out = np.zeros(payload_len(ao), dtype=np.uint8)
+    lib().or_pack_vector_frame(ctypes.byref(ao), bwd if ao.vectors & 1 else None, fwd if ao.vectors & 2 else None,
+                               _ptr(out))
+    return out
