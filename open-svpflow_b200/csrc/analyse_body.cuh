@@ -550,6 +550,7 @@ struct Ctx {
     Planes S, R;
     int level, d, tid, satd, pel;
     int grp_lanes;   // G: lanes per candidate (power of two)
+    int pnew;        // new-candidate penalty of the current search (opts.pnew; pnew / factor in the refine pass)
     int tl, tcp;     // 4x4 luma tiles, 4x4 tiles per chroma plane of one candidate
 };
 
@@ -719,8 +720,8 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
     const int G = x.grp_lanes, gpw = 32 / G;
     const int lane = x.tid & 31, warp = x.tid >> 5;
     const int grp = warp * gpw + lane / G, sub = lane & (G - 1), NG = NW * gpw;
-    const bool serial = x.P->pnew < -256;
-    const int pnew = x.P->pnew;
+    const bool serial = x.pnew < -256;
+    const int pnew = x.pnew;
     long long bk = 0x7FFFFFFFFFFFFFFFLL;
     int bi = 0x7FFFFFFF;
     unsigned bs = 0;
@@ -960,6 +961,106 @@ __device__ __forceinline__ uint2 mkvec(int dx, int dy, unsigned score) {
 // exact_hex2 :942-1033, exact_umh :1036-1119, bad-SAD expansion :611-672)
 enum { S_REFINE, S_HEX_START, S_HEX_ITER, S_HEX_EXIT, S_BAD, S_BAD_RING, S_FINAL_RING, S_STORE };
 
+// The block's source pixels into shared memory (DirSh::srcp) for the fast path.
+__device__ __forceinline__ void stage_source(const Ctx &x, DirSh &s, const BlkC &b) {
+    if (b.fast_src) {
+        const int nlw = b.tilesx * b.bh;
+        for (int t = x.tid; t < nlw; t += NT) {
+            const int row = t >> b.lgtx, col = t & (b.tilesx - 1);
+            s.srcp[t] = stage4(ld4u(x.S.y + b.lsrc + row * x.G.ys32 + col * 4), b.satd_mode != 0);
+        }
+        if (b.chroma && b.cfast_src) {
+            const int nc = b.ctilesx * b.crows;
+            for (int t = x.tid; t < 2 * nc; t += NT) {
+                const int pl = t >= nc, u = t - pl * nc;
+                const int row = u >> b.lgctx, col = u & (b.ctilesx - 1);
+                s.srcp[nlw + t] = stage4(ld4u((pl ? x.S.v : x.S.u) + b.csrc + row * x.G.cs32 + col * 4), x.satd != 0);
+            }
+        }
+    }
+}
+
+// The refinement and bad-SAD expansion of one block (exact_refine_search :771-826,
+// exact_hex2 :942-1033, exact_umh :1036-1119, the expansion :611-672): a state machine
+// replicated in every thread of the direction, issuing one evaluation step at a time.
+// (ppx, ppy): predictor of the motion penalty; (own_x, own_y): the block's own predictor,
+// which the bad-SAD expansion switches to.
+__device__ __forceinline__ void run_search_steps(const Ctx &x, const BlkC &b, DirSh &s, int &ph, bool refine, int stype,
+                                                 int radius, int lambda, int ppx, int ppy, int own_x, int own_y,
+                                                 int64_t idx, int &bad_count, int &bmx, int &bmy, unsigned &bsad,
+                                                 long long &bcost) {
+    const AnalyseParams &P = *x.P;
+    const LevelInfo &L = *x.L;
+    const int level = x.level;
+    int predx = ppx, predy = ppy;
+    int state = refine ? S_REFINE : S_STORE;
+    int hbx = 0, hby = 0, hdir = -2, hi = 0, hrad = 0, hret = 0, bad_r = 0, bad_max = 0;
+    unsigned found = 0;
+    for (;;) {
+        Gen g{0, 0, 0, 0, 0, 0, 0};
+        bool sets_mv = true, issue = false;
+        while (!issue && state != S_STORE) {
+            if (state == S_REFINE) {
+                if (stype == 4) { g = make_gen(BK_EXH, bmx, bmy, radius, 0, 0); issue = true; state = S_BAD; }
+                else if (stype == 3) {
+                    g = make_gen(BK_UMH, bmx, bmy, radius, 0, 0); issue = true;
+                    state = S_HEX_START; hrad = radius; hret = 0;
+                } else if (stype == 2) { state = S_HEX_START; hrad = radius; hret = 0; }
+                else state = S_BAD;
+            } else if (state == S_HEX_START) {
+                hbx = bmx; hby = bmy;
+                if (hrad > 1) { g = make_gen(BK_HEX6, hbx, hby, 0, 0, 0); sets_mv = false; issue = true; state = S_HEX_ITER; }
+                else { g = make_gen(BK_RING, hbx, hby, 1, 1, 0); issue = true; state = hret ? S_FINAL_RING : S_BAD; }
+            } else if (state == S_HEX_ITER) {
+                if (hi < hrad / 2 && hbx >= b.bnd0 && hby >= b.bnd1 && hbx < b.bnd2 && hby < b.bnd3) {
+                    g = make_gen(BK_HEX3, hbx, hby, 0, 0, c_mod6m1[hdir + 1]); sets_mv = false; issue = true;
+                } else state = S_HEX_EXIT;
+            } else if (state == S_HEX_EXIT) {
+                bmx = hbx; bmy = hby;
+                g = make_gen(BK_RING, hbx, hby, 1, 1, 0); issue = true; state = hret ? S_FINAL_RING : S_BAD;
+            } else if (state == S_BAD) {
+                found = bsad;
+                const int bl = sat_i32((long long)P.coarse_bad_sad + (long long)(sat_i32((long long)P.coarse_bad_sad * bad_count) / 16));
+                if (level > 0 && idx > 1 && P.coarse_bad_sad > 0 && (int)bsad > bl) {
+                    bad_count++;
+                    predx = own_x; predy = own_y;  // the block's own predictor
+                    if (P.coarse_bad_range < 0) {
+                        bad_max = -P.coarse_bad_range * L.pel; bad_r = L.pel;
+                        if (bad_r < bad_max) { g = make_gen(BK_RING, 0, 0, bad_r, L.pel, 0); issue = true; state = S_BAD_RING; }
+                        else state = S_FINAL_RING;
+                    } else if (P.coarse_bad_range > 0) {
+                        hrad = P.coarse_bad_range * L.pel; hret = 1;
+                        g = make_gen(BK_UMH, 0, 0, hrad, 0, 0); issue = true; state = S_HEX_START;
+                    } else state = S_FINAL_RING;
+                } else state = S_STORE;
+            } else if (state == S_BAD_RING) {
+                if (bsad < found / 4) state = S_FINAL_RING;
+                else {
+                    bad_r += L.pel;
+                    if (bad_r < bad_max) { g = make_gen(BK_RING, 0, 0, bad_r, L.pel, 0); issue = true; }
+                    else state = S_FINAL_RING;
+                }
+            } else {  // S_FINAL_RING
+                g = make_gen(BK_RING, bmx, bmy, 1, 1, 0); issue = true; state = S_STORE;
+            }
+        }
+        if (!issue) break;
+        int w;
+        eval_step(x, b, s, ph, g, lambda, predx, predy, bcost, bsad, w);
+        if (g.kind == BK_HEX6 || g.kind == BK_HEX3) {  // exact_check_dir: a label, best.mv set at exit
+            if (w >= 0) {
+                hdir = g.kind == BK_HEX6 ? w : g.odir + w - 1;
+                hbx += c_hex2[hdir + 1].x; hby += c_hex2[hdir + 1].y;
+                hi = g.kind == BK_HEX6 ? 1 : hi + 1;
+                state = S_HEX_ITER;
+            } else state = S_HEX_EXIT;
+        } else if (w >= 0 && sets_mv) {
+            const int2 m = gen_mv(g, w);
+            bmx = m.x; bmy = m.y;
+        }
+    }
+}
+
 // The per-direction search of one level (exact_search_level, :480-681). Every thread
 // of the direction runs this with identical values; only the evaluation work is split.
 __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch &ds, const uint2 *prevp, int *status) {
@@ -1000,22 +1101,7 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
         const int2 imv = vmv(interp);
         BlkC b;
         make_blk(x, px, py, !smallest, b);
-        // stage the source block for the refinement steps (read after the next barrier)
-        if (b.fast_src) {
-            const int nlw = b.tilesx * b.bh;
-            for (int t = x.tid; t < nlw; t += NT) {
-                const int row = t >> b.lgtx, col = t & (b.tilesx - 1);
-                s.srcp[t] = stage4(ld4u(x.S.y + b.lsrc + row * x.G.ys32 + col * 4), b.satd_mode != 0);
-            }
-            if (b.chroma && b.cfast_src) {
-                const int nc = b.ctilesx * b.crows;
-                for (int t = x.tid; t < 2 * nc; t += NT) {
-                    const int pl = t >= nc, u = t - pl * nc;
-                    const int row = u >> b.lgctx, col = u & (b.ctilesx - 1);
-                    s.srcp[nlw + t] = stage4(ld4u((pl ? x.S.v : x.S.u) + b.csrc + row * x.G.cs32 + col * 4), x.satd != 0);
-                }
-            }
-        }
+        stage_source(x, s, b);  // read by the refinement steps, after the next barrier
         // ---- special candidates (exact_search_block, :708-746): slot list in the
         // reference's evaluation roles; slot j is evaluated by group j
         int n = 0, rs_slot = -1, prev_slot = -1, nseeds = 0;
@@ -1148,74 +1234,8 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
             refine = true;
         }
         const unsigned dcsum = s.slotL[phs][dcslot];
-        // ---- refinement and bad-SAD expansion: a replicated state machine issuing steps
-        int predx = ppx, predy = ppy;
-        int state = refine ? S_REFINE : S_STORE;
-        int hbx = 0, hby = 0, hdir = -2, hi = 0, hrad = 0, hret = 0, bad_r = 0, bad_max = 0;
-        unsigned found = 0;
-        for (;;) {
-            Gen g{0, 0, 0, 0, 0, 0, 0};
-            bool sets_mv = true, issue = false;
-            while (!issue && state != S_STORE) {
-                if (state == S_REFINE) {
-                    if (stype == 4) { g = make_gen(BK_EXH, bmx, bmy, radius, 0, 0); issue = true; state = S_BAD; }
-                    else if (stype == 3) {
-                        g = make_gen(BK_UMH, bmx, bmy, radius, 0, 0); issue = true;
-                        state = S_HEX_START; hrad = radius; hret = 0;
-                    } else if (stype == 2) { state = S_HEX_START; hrad = radius; hret = 0; }
-                    else state = S_BAD;
-                } else if (state == S_HEX_START) {
-                    hbx = bmx; hby = bmy;
-                    if (hrad > 1) { g = make_gen(BK_HEX6, hbx, hby, 0, 0, 0); sets_mv = false; issue = true; state = S_HEX_ITER; }
-                    else { g = make_gen(BK_RING, hbx, hby, 1, 1, 0); issue = true; state = hret ? S_FINAL_RING : S_BAD; }
-                } else if (state == S_HEX_ITER) {
-                    if (hi < hrad / 2 && hbx >= b.bnd0 && hby >= b.bnd1 && hbx < b.bnd2 && hby < b.bnd3) {
-                        g = make_gen(BK_HEX3, hbx, hby, 0, 0, c_mod6m1[hdir + 1]); sets_mv = false; issue = true;
-                    } else state = S_HEX_EXIT;
-                } else if (state == S_HEX_EXIT) {
-                    bmx = hbx; bmy = hby;
-                    g = make_gen(BK_RING, hbx, hby, 1, 1, 0); issue = true; state = hret ? S_FINAL_RING : S_BAD;
-                } else if (state == S_BAD) {
-                    found = bsad;
-                    const int bl = sat_i32((long long)P.coarse_bad_sad + (long long)(sat_i32((long long)P.coarse_bad_sad * bad_count) / 16));
-                    if (level > 0 && idx > 1 && P.coarse_bad_sad > 0 && (int)bsad > bl) {
-                        bad_count++;
-                        predx = imv.x; predy = imv.y;  // the block's own predictor
-                        if (P.coarse_bad_range < 0) {
-                            bad_max = -P.coarse_bad_range * L.pel; bad_r = L.pel;
-                            if (bad_r < bad_max) { g = make_gen(BK_RING, 0, 0, bad_r, L.pel, 0); issue = true; state = S_BAD_RING; }
-                            else state = S_FINAL_RING;
-                        } else if (P.coarse_bad_range > 0) {
-                            hrad = P.coarse_bad_range * L.pel; hret = 1;
-                            g = make_gen(BK_UMH, 0, 0, hrad, 0, 0); issue = true; state = S_HEX_START;
-                        } else state = S_FINAL_RING;
-                    } else state = S_STORE;
-                } else if (state == S_BAD_RING) {
-                    if (bsad < found / 4) state = S_FINAL_RING;
-                    else {
-                        bad_r += L.pel;
-                        if (bad_r < bad_max) { g = make_gen(BK_RING, 0, 0, bad_r, L.pel, 0); issue = true; }
-                        else state = S_FINAL_RING;
-                    }
-                } else {  // S_FINAL_RING
-                    g = make_gen(BK_RING, bmx, bmy, 1, 1, 0); issue = true; state = S_STORE;
-                }
-            }
-            if (!issue) break;
-            int w;
-            eval_step(x, b, s, ph, g, lambda, predx, predy, bcost, bsad, w);
-            if (g.kind == BK_HEX6 || g.kind == BK_HEX3) {  // exact_check_dir: a label, best.mv set at exit
-                if (w >= 0) {
-                    hdir = g.kind == BK_HEX6 ? w : g.odir + w - 1;
-                    hbx += c_hex2[hdir + 1].x; hby += c_hex2[hdir + 1].y;
-                    hi = g.kind == BK_HEX6 ? 1 : hi + 1;
-                    state = S_HEX_ITER;
-                } else state = S_HEX_EXIT;
-            } else if (w >= 0 && sets_mv) {
-                const int2 m = gen_mv(g, w);
-                bmx = m.x; bmy = m.y;
-            }
-        }
+        run_search_steps(x, b, s, ph, refine, stype, radius, lambda, ppx, ppy, imv.x, imv.y, idx, bad_count, bmx, bmy,
+                         bsad, bcost);
         // ---- store (:673-679)
         const int rows = b.py >= 0 ? imax(0, imin(b.bh, L.lh - b.py)) : 0;
         const int cols = b.px >= 0 ? imax(0, imin(b.bw, L.lw - b.px)) : 0;
@@ -1231,6 +1251,118 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
         last_val = v;
     }
 }
+__device__ __forceinline__ long long floor_div(long long a, long long b) {  // i64::div_euclid for b > 0
+    const long long q = a / b;
+    return (a % b != 0 && a < 0) ? q - 1 : q;
+}
+
+// exact_recalculate (:1326-1451): when refine[0].thsad is set, the level-0 field is
+// interpolated onto the half-size output blocks and each block whose interpolated score is
+// above the threshold is searched again. Blocks do not read each other's results, so the
+// visiting order does not matter; the direction's threads take them one after another with
+// the same evaluation machinery as the hierarchy. Output: ds.vec[1] / ds.luma[1].
+__device__ __forceinline__ void refine_pass(Ctx &x, DirSh &s, DirScratch &ds) {
+    const AnalyseParams &P = *x.P;
+    const uint2 *field = ds.vec[0];
+    uint2 *out = ds.vec[1];
+    uint8_t *outl = ds.luma[1];
+    const int ogw = P.lv[0].gw, ogh = P.lv[0].gh;
+    const int obw = P.block_w, obh = P.block_h, osx = P.step_x, osy = P.step_y;
+    const int bw = P.out_bw, bh = P.out_bh;
+    const int sx = imax(bw - P.out_ox, 1), sy = imax(bh - P.out_oy, 1);
+    const int gw = P.out_gw, gh = P.out_gh;
+    const int lw = P.lv[0].lw, lh = P.lv[0].lh;
+    x.level = 0;
+    x.pel = P.lv[0].pel;
+    x.satd = P.refine_satd;
+    int ph = 0;
+    for (int by = 0; by < gh; by++) {
+        for (int bx = 0; bx < gw; bx++) {
+            const int cx = bw / 2 + sx * bx, cy = bh / 2 + sy * by;
+            const int ox_ = (cx - obw / 2) / osx, oy_ = (cy - obh / 2) / osy;
+            const long long dx_ = imax(cx - (obw / 2 + osx * ox_), 0), dy_ = imax(cy - (obh / 2 + osy * oy_), 0);
+            const uint2 p00 = field[(int64_t)iclamp(oy_, 0, ogh - 1) * ogw + iclamp(ox_, 0, ogw - 1)];
+            const uint2 p10 = field[(int64_t)iclamp(oy_, 0, ogh - 1) * ogw + iclamp(ox_ + 1, 0, ogw - 1)];
+            const uint2 p01 = field[(int64_t)iclamp(oy_ + 1, 0, ogh - 1) * ogw + iclamp(ox_, 0, ogw - 1)];
+            const uint2 p11 = field[(int64_t)iclamp(oy_ + 1, 0, ogh - 1) * ogw + iclamp(ox_ + 1, 0, ogw - 1)];
+            auto interp = [&](long long a, long long b_, long long c, long long d) {
+                const long long top = a * osx + dx_ * (b_ - a);
+                const long long bottom = c * osx + dx_ * (d - c);
+                return floor_div(top + floor_div(dy_ * (bottom - top), osy), osx);
+            };
+            const int2 m00 = vmv(p00), m10 = vmv(p10), m01 = vmv(p01), m11 = vmv(p11);
+            const int mvx = (int)interp(m00.x, m10.x, m01.x, m11.x);
+            const int mvy = (int)interp(m00.y, m10.y, m01.y, m11.y);
+            const long long parent = interp(p00.y, p10.y, p01.y, p11.y) * (long long)(bw * bh) / (long long)(obw * obh);
+            const int px = bx * sx, py = by * sy;
+            const bool border = bx == 0 || by == 0 || bx == gw - 1 || by == gh - 1;
+            const int factor = (border && bw > 4) ? 3 : 1;
+            const int epx = px + (factor == 3 ? bw / 4 : 0), epy = py + (factor == 3 ? bh / 4 : 0);
+            x.L = &P.rlv[factor == 3 ? 1 : 0];
+            const LevelInfo &L = *x.L;
+            x.tl = L.tl;
+            x.tcp = L.tc;
+            {
+                const int T = L.tl + 2 * L.tc;
+                const int tpl = iclamp(P.tiles_per_lane, 1, 8);
+                const int want = (T + tpl - 1) / tpl;
+                int g = 1;
+                while (g < want && g < 32) g <<= 1;
+                x.grp_lanes = g;
+            }
+            x.pnew = P.pnew / factor;
+            BlkC b;
+            make_blk(x, epx, epy, true, b);
+            // exact_clip (:1269-1273) of the interpolated vector into mv_bounds
+            const int pmx = iclamp(mvx, b.bnd0, imax(b.bnd2 - 1, b.bnd0)), pmy = iclamp(mvy, b.bnd1, imax(b.bnd3 - 1, b.bnd1));
+            const int threshold = P.refine_thsad / factor;
+            const bool search = parent > (long long)threshold;
+            stage_source(x, s, b);
+            {  // slot 0: exact_sad at the clipped predictor (when searching); slot 1: block_luma_dc
+                const int Gl = x.grp_lanes, lane = x.tid & 31, grp = (x.tid >> 5) * (32 / Gl) + lane / Gl;
+                const int sub = lane & (Gl - 1);
+                const bool act = (grp == 0 && search) || grp == 1;
+                Res r{0, 0, 0, 0, 0, 0};
+                if (act) r = eval_lane(x, b, grp == 1 ? 2 : 0, 0, 0, pmx, pmy, grp == 0, sub);
+                r.L = group_sum(r.L, Gl);
+                r.U = group_sum(r.U, Gl);
+                r.V = group_sum(r.V, Gl);
+                if (act && sub == 0) {
+                    unsigned Lv, Cv;
+                    if (grp == 1) { Lv = r.L; Cv = 0; }
+                    else finalize(r, Lv, Cv);
+                    s.slotL[ph][grp] = grp == 0 ? sat_add(Lv, Cv) : Lv;
+                }
+            }
+            dbar(x.d);
+            const int phs = ph;
+            ph ^= 1;
+            int bmx = pmx, bmy = pmy;
+            unsigned bsad = parent < 0 ? 0u : (parent > 0xFFFFFFFFLL ? 0xFFFFFFFFu : (unsigned)parent);
+            long long bcost = parent < 0 ? 0 : parent;
+            if (search) {
+                bsad = s.slotL[phs][0];
+                bcost = (long long)bsad;
+                const int lambda = by == 0 ? 0 : (P.lambda >> 2) / factor;
+                int bad = 0;
+                run_search_steps(x, b, s, ph, true, P.refine_search_type, abs(P.refine_distance), lambda, pmx, pmy, pmx,
+                                 pmy, 0, bad, bmx, bmy, bsad, bcost);
+            }
+            const unsigned dcsum = s.slotL[phs][1];
+            const int rows = b.py >= 0 ? imax(0, imin(b.bh, lh - b.py)) : 0;
+            const int cols = b.px >= 0 ? imax(0, imin(b.bw, lw - b.px)) : 0;
+            const unsigned cnt = (unsigned)(rows * cols);
+            unsigned dc = cnt ? dcsum / cnt : 0;
+            if (dc > 255) dc = 255;
+            if (x.tid == 0) {
+                out[(int64_t)by * gw + bx] = mkvec(bmx, bmy, sat_mul(bsad, (unsigned)factor));
+                outl[(int64_t)by * gw + bx] = (uint8_t)dc;
+            }
+        }
+    }
+    dbar(x.d);
+}
+
 // exact_global_doubled (:1285-1324) over the dir's threads
 __device__ void global_doubled(const Ctx &x, DirSh &s, const uint2 *field, int64_t n, unsigned *hist) {
     int mode[2];
@@ -1399,6 +1531,7 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
         x.G.lw = L.lw; x.G.lh = L.lh; x.G.clw = L.lw / 2; x.G.clh = L.lh / 2;
         x.G.ys = P.y_stride; x.G.cs = P.c_stride; x.G.ylen = P.y_len; x.G.clen = P.c_len;
         x.G.ys32 = (int)P.y_stride; x.G.cs32 = (int)P.c_stride;
+        x.pnew = P.pnew;
         x.tl = L.tl;
         x.tcp = L.tc;
         {  // lanes per candidate: about `tiles_per_lane` 4x4 tiles per lane
@@ -1538,11 +1671,43 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
         if (tid == 0 && s.abort_ == 1) cta_abort = 1;
         __syncthreads();
     }
-    if (cta_abort || idle) return;
-    // ---- refine pass (exact_recalculate :1326-1451) runs on the host-selected configs only
+}
+
+// After the hierarchy: the refine pass when configured, then rescale_scores (:2716-2738)
+// and pack_vector_frame (:2740-2811). Out of line, called where little else is live, so
+// neither adds to the hierarchy's register pressure. Every thread of the CTA calls it.
+__device__ __noinline__ void finish_pair(const AnalyseParams *Pp, const PairRef pr, uint8_t *pay, uint8_t *scr) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const AnalyseParams &P = *Pp;
+    const bool bidir = P.vectors == 3;
+    const int half = (int)(threadIdx.x / NT);
+    if (!bidir && half == 1) return;
+    const int d = bidir ? half : ((P.vectors & 2) ? 0 : 1);
+    const int tid = threadIdx.x % NT;
+    DirSh &s = reinterpret_cast<DirSh *>(smem)[half];
+    DirScratch ds;
+    ds.vec[0] = (uint2 *)(scr + P.off_field[d]);
+    ds.vec[1] = (uint2 *)(scr + P.off_next[d]);
+    ds.luma[0] = scr + P.off_out[d];
+    ds.luma[1] = scr + P.off_out[d] + P.max_cells;
+    if (P.has_refine) {
+        const uint8_t *src = d == 0 ? pr.cur : pr.ref;
+        const uint8_t *ref = d == 0 ? pr.ref : pr.cur;
+        Ctx x;
+        x.P = &P;
+        x.d = half;
+        x.tid = tid;
+        x.S = Planes{src, src + P.y_len, src + P.y_len + P.c_len};
+        x.R = Planes{ref, ref + P.y_len, ref + P.y_len + P.c_len};
+        const LevelInfo &L0 = P.lv[0];
+        x.G.lw = L0.lw; x.G.lh = L0.lh; x.G.clw = L0.lw / 2; x.G.clh = L0.lh / 2;
+        x.G.ys = P.y_stride; x.G.cs = P.c_stride; x.G.ylen = P.y_len; x.G.clen = P.c_len;
+        x.G.ys32 = (int)P.y_stride; x.G.cs32 = (int)P.c_stride;
+        refine_pass(x, s, ds);
+    }
     // ---- rescale_scores (:2716-2738) + pack_vector_frame (:2740-2811)
-    const uint2 *f = ds.vec[0];
-    const uint8_t *fl = ds.luma[0];
+    const uint2 *f = ds.vec[P.has_refine ? 1 : 0];
+    const uint8_t *fl = ds.luma[P.has_refine ? 1 : 0];
     const int64_t count = (int64_t)P.out_gw * P.out_gh;
     const int64_t region = bidir ? (d == 1 ? 0x40 : 0x40 + 4 + count * 8) : 0x40;
     if (threadIdx.x == 0) {
@@ -1585,7 +1750,10 @@ __global__ void __launch_bounds__(2 * NT, SVPF_MINB)
         pr.cur = psrc.clip + n * psrc.frame_bytes;
         pr.ref = psrc.clip + n2 * psrc.frame_bytes;
     }
-    analyse_pair_dev(P, pr, payloads + pair * P.payload_len, scratch + pair * P.scratch_per_pair, status, cta_abort);
+    uint8_t *scr = scratch + pair * P.scratch_per_pair;
+    analyse_pair_dev(P, pr, payloads + pair * P.payload_len, scr, status, cta_abort);
+    __syncthreads();
+    if (!cta_abort) finish_pair(&P, pr, payloads + pair * P.payload_len, scr);
 }
 
 // Persistent form: a grid sized to the resident CTAs drains the item list in order (the
@@ -1612,6 +1780,8 @@ __global__ void __launch_bounds__(2 * NT, SVPF_MINB)
         }
         __syncthreads();
         analyse_pair_dev(P, bi.pair, bi.payload, scr, clip_status + bi.clip, cta_abort);
+        __syncthreads();
+        if (!cta_abort) finish_pair(&P, bi.pair, bi.payload, scr);
         __syncthreads();  // P, item_sh and the shared search state are reused by the next item
     }
 }

@@ -99,7 +99,27 @@ bool build_analyse_params(const AnalyseOpts &o, const SuperLayout &Lay, AnalyseP
     output_grid(o, bw, bh, ox, oy, gw, gh);
     P.out_bw = bw; P.out_bh = bh; P.out_ox = ox; P.out_oy = oy; P.out_gw = gw; P.out_gh = gh;
     P.has_refine = o.has_refine_thsad;
-    if (P.has_refine) { err = "refine (recalculate) pass is not available on the device path yet"; return false; }
+    P.refine_thsad = o.refine_thsad;
+    P.refine_search_type = o.refine_search_type;
+    P.refine_distance = o.refine_distance;
+    P.refine_satd = o.refine_satd;
+    if (P.has_refine) {  // exact_recalculate (:1326-1451) block shapes at level 0
+        for (int k = 0; k < 2; k++) {
+            LevelInfo &R = P.rlv[k];
+            R = P.lv[0];
+            R.gw = gw; R.gh = gh;
+            R.bw = k ? bw / 2 : bw; R.bh = k ? bh / 2 : bh;
+            R.pxoff = 0; R.pyoff = 0; R.smallest = 0; R.lambda_base = 0; R.lsad = 0;
+            R.satd = o.refine_satd;
+            R.search_type = o.refine_search_type;
+            R.base_radius = o.refine_distance < 0 ? -o.refine_distance : o.refine_distance;
+            R.tl = ((R.bw + 3) / 4) * ((R.bh + 3) / 4);
+            const int cw = R.bw / 2, ch = R.bh / 2;
+            R.tc = cw > 0 ? ((cw + 3) / 4) * (((cw > ch ? cw : ch) + 3) / 4) : 0;
+            if (R.tl + R.tc > 96) { err = "unsupported block / grid size"; return false; }
+        }
+        if ((int64_t)gw * gh > max_cells) max_cells = (int64_t)gw * gh;
+    }
     {  // rescale_scores denominators (:2716-2721)
         double f = sqrt((double)o.width * (double)o.width + (double)o.height * (double)o.height);
         int32_t diag = f != f ? 0 : (f >= 2147483647.0 ? INT32_MAX : (int32_t)f);
@@ -116,7 +136,10 @@ bool build_analyse_params(const AnalyseOpts &o, const SuperLayout &Lay, AnalyseP
     P.header[5] = o.pel; P.header[6] = hdr[5]; P.header[7] = 0; P.header[8] = o.width; P.header[9] = o.height;
     P.header[10] = ox; P.header[11] = oy; P.header[12] = gw; P.header[13] = gh; P.header[14] = o.selector;
     P.header[15] = o.delta;
-    if ((int64_t)gw * gh != (int64_t)P.lv[0].gw * P.lv[0].gh) { err = "output grid differs from the level-0 grid"; return false; }
+    if (!P.has_refine && (int64_t)gw * gh != (int64_t)P.lv[0].gw * P.lv[0].gh) {
+        err = "output grid differs from the level-0 grid";
+        return false;
+    }
     // scratch layout per pair
     int64_t np2 = 1;
     while (np2 < max_cells) np2 <<= 1;

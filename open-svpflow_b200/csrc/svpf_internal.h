@@ -99,6 +99,7 @@ struct alignas(16) AnalyseParams {
     // output grid (after the optional refine pass)
     int32_t out_gw, out_gh, out_bw, out_bh, out_ox, out_oy;
     int32_t has_refine, refine_thsad, refine_search_type, refine_distance, refine_satd, lambda;
+    LevelInfo rlv[2];         // refine pass block shapes: output block, half of it (border blocks)
     int32_t rescale_denom;
     int32_t tiles_per_lane;   // 4x4 tiles one lane evaluates per candidate (2, 4 or 8): a launch tuning knob
     int64_t payload_len;

@@ -72,6 +72,12 @@ ANALYSE_CASES = [
     (192, 128, "{pel:2}", "{main:{search:{coarse:{distance:-6,bad:{range:5}}}}}", 2),
     (192, 128, "{pel:2}", "{main:{search:{coarse:{bad:{sad:30}}},penalty:{lambda:3,plevel:2}}}", 2),
     (256, 144, "{pel:2}", "{block:{w:16,h:8,overlap:2},main:{search:{type:3,distance:6,satd:true}}}", 2),
+    # refine[0].thsad set: exact_recalculate onto half-size output blocks
+    (192, 128, "{pel:2}", "{refine:[{thsad:200,search:{type:2,distance:3,satd:true}}]}", 2),
+    (256, 144, "{pel:2}", "{block:{w:16,overlap:2},main:{search:{type:3,distance:6}},refine:[{thsad:50}]}", 2),
+    (192, 128, "{pel:4}", "{block:{w:8,overlap:0},refine:[{thsad:0,search:{type:4,distance:2}}]}", 2),
+    (160, 96, "{pel:1}", "{vectors:1,block:{w:32,overlap:1},refine:[{thsad:100,search:{type:3,distance:8}}]}", 2),
+    (192, 128, "{pel:2}", "{vectors:2,main:{penalty:{pnew:90}},refine:[{thsad:20000,search:{type:2}}]}", 2),
 ]
 
 
