@@ -153,6 +153,23 @@ def cpu_reference(nframes_total: int, threads: int, pairs: int, seed: int = 1000
     return dt, pay, clip
 
 
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _one_core(pairs: int = 2) -> dict:
+    """The same oracle on one host thread over `pairs` output frames (the per-core figure)."""
+    dt, _, _ = cpu_reference(240, 1, pairs, seed=1999)
+    return {"value": pairs / dt, "unit": UNIT, "cores": 1, "sample": f"{pairs} output frames, 1 thread"}
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return
@@ -172,7 +189,8 @@ def run_reference(args, rank: int):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": _config(240, 1),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                         "cpu_model": _cpu_model(), "one_core": _one_core()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -565,7 +583,8 @@ def main():
             dt, pay_cpu, _ = cpu_reference(nf, threads, pairs, seed=1000 + rank)
             cpu = {"value": pairs / dt, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"output frames 0..{pairs - 1} of the same clip (Super + Analyse) on {threads} host "
-                             f"threads, oracle/ C restatement of the reference"}
+                             f"threads, oracle/ C restatement of the reference (AVX2 interior SAD/SATD)",
+                   "cpu_model": _cpu_model(), "one_core": _one_core()}
             parity = {"pairs_checked": pairs,
                       "bit_exact": bool(np.array_equal(pay_cpu, pay_d[:pairs].cpu().numpy()))}
         line = {

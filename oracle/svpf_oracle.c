@@ -25,6 +25,7 @@
 #include <stdbool.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include <immintrin.h>
 #include <string.h>
 #ifdef _OPENMP
 #include <omp.h>
@@ -608,9 +609,68 @@ uint32_t or_hadamard4_satd(const int32_t d[16]) { /* hadamard4_satd, :2681-2702 
     return (u32)(s > 0 ? s : 0);
 }
 
+/* Vector forms of the interior SAD / SATD for blocks whose every byte is in its slice, as
+ * the reference's own sad_u8_simd (:1857-1994) and hadamard4_satd_sse2/avx2 (:2523-2679)
+ * are: the same sums, in 16-bit lanes (|coefficient| <= 16 * 255 never overflows). Used by
+ * the CPU baseline's speed only; the scalar forms below remain the definition. */
+static int in_slice(usize len, usize i, usize stride, usize w, usize h) {
+    if (i > len || h == 0) return 0;
+    usize rest = len - i;
+    if (h - 1 > 0 && stride > (rest - (w <= rest ? w : rest)) / (h - 1)) return 0;
+    return (h - 1) * stride + w <= rest;
+}
+static inline u32 sad_row_simd(const u8 *a, const u8 *b, usize w) {
+    if (w == 32) {
+        __m256i d = _mm256_sad_epu8(_mm256_loadu_si256((const __m256i *)a), _mm256_loadu_si256((const __m256i *)b));
+        __m128i t = _mm_add_epi64(_mm256_castsi256_si128(d), _mm256_extracti128_si256(d, 1));
+        return (u32)(_mm_cvtsi128_si32(t) + _mm_extract_epi32(t, 2));
+    }
+    if (w == 16) {
+        __m128i d = _mm_sad_epu8(_mm_loadu_si128((const __m128i *)a), _mm_loadu_si128((const __m128i *)b));
+        return (u32)(_mm_cvtsi128_si32(d) + _mm_extract_epi32(d, 2));
+    }
+    u64 x = 0, y = 0;
+    memcpy(&x, a, w);
+    memcpy(&y, b, w);
+    return (u32)_mm_cvtsi128_si32(_mm_sad_epu8(_mm_cvtsi64_si128((long long)x), _mm_cvtsi64_si128((long long)y)));
+}
+/* sum of |H4 D H4| over the 4x4 tiles of a 4-row strip, 16 columns (4 tiles) at a time */
+static inline __m256i satd_strip16(const u8 *a, usize as, const u8 *b, usize bs) {
+    __m256i d[4];
+    for (int r = 0; r < 4; r++)
+        d[r] = _mm256_sub_epi16(_mm256_cvtepu8_epi16(_mm_loadu_si128((const __m128i *)(a + r * as))),
+                                _mm256_cvtepu8_epi16(_mm_loadu_si128((const __m128i *)(b + r * bs))));
+    __m256i s0 = _mm256_add_epi16(d[0], d[1]), s1 = _mm256_sub_epi16(d[0], d[1]);
+    __m256i s2 = _mm256_add_epi16(d[2], d[3]), s3 = _mm256_sub_epi16(d[2], d[3]);
+    __m256i v[4] = {_mm256_add_epi16(s0, s2), _mm256_add_epi16(s1, s3), _mm256_sub_epi16(s0, s2),
+                    _mm256_sub_epi16(s1, s3)};
+    __m256i acc = _mm256_setzero_si256();
+    const __m256i ones = _mm256_set1_epi16(1);
+    for (int k = 0; k < 4; k++) { /* horizontal 4-point transform inside each group of 4 lanes */
+        __m256i x = v[k];
+        __m256i sw = _mm256_shufflehi_epi16(_mm256_shufflelo_epi16(x, 0xB1), 0xB1); /* 1 0 3 2 */
+        __m256i t = _mm256_blend_epi16(_mm256_add_epi16(x, sw), _mm256_sub_epi16(sw, x), 0xAA);
+        __m256i sw2 = _mm256_shufflehi_epi16(_mm256_shufflelo_epi16(t, 0x4E), 0x4E); /* 2 3 0 1 */
+        __m256i u = _mm256_blend_epi16(_mm256_add_epi16(t, sw2), _mm256_sub_epi16(sw2, t), 0xCC);
+        acc = _mm256_add_epi32(acc, _mm256_madd_epi16(_mm256_abs_epi16(u), ones));
+    }
+    return acc;
+}
+static inline u32 hsum_epi32(__m256i v) {
+    __m128i t = _mm_add_epi32(_mm256_castsi256_si128(v), _mm256_extracti128_si256(v, 1));
+    t = _mm_add_epi32(t, _mm_shuffle_epi32(t, 0x4E));
+    t = _mm_add_epi32(t, _mm_shuffle_epi32(t, 0xB1));
+    return (u32)_mm_cvtsi128_si32(t);
+}
+
 /* sad_u8_simd (:1857-1951): plain sum of |a-b| at (possibly wrapped) base indices */
 static u32 sad_raw(const u8 *a, usize alen, usize ai, usize as, const u8 *b, usize blen, usize bi,
                    usize bs, usize w, usize h) {
+    if ((w == 4 || w == 8 || w == 16 || w == 32) && in_slice(alen, ai, as, w, h) && in_slice(blen, bi, bs, w, h)) {
+        u32 t = 0;
+        for (usize r = 0; r < h; r++) t += sad_row_simd(a + ai + r * as, b + bi + r * bs, w);
+        return t;
+    }
     u32 s = 0;
     for (usize r = 0; r < h; r++)
         for (usize c = 0; c < w; c++) {
@@ -622,6 +682,13 @@ static u32 sad_raw(const u8 *a, usize alen, usize ai, usize as, const u8 *b, usi
 /* satd_interior (:2439-2521) == (sum of per-tile hadamard4_satd) >> 1 */
 static u32 satd_raw(const u8 *a, usize alen, usize ai, usize as, const u8 *b, usize blen, usize bi,
                     usize bs, usize n) {
+    if ((n == 16 || n == 32) && in_slice(alen, ai, as, n, n) && in_slice(blen, bi, bs, n, n)) {
+        __m256i acc = _mm256_setzero_si256();
+        for (usize ty = 0; ty < n; ty += 4)
+            for (usize tx = 0; tx < n; tx += 16)
+                acc = _mm256_add_epi32(acc, satd_strip16(a + ai + ty * as + tx, as, b + bi + ty * bs + tx, bs));
+        return hsum_epi32(acc) >> 1;
+    }
     u32 total = 0;
     usize tiles = n / 4;
     for (usize ty = 0; ty < tiles; ty++)
