@@ -381,7 +381,7 @@ def run_served(args, world: int, rank: int, local: int):
     sweep = []
     for wi, rate in enumerate(rates):
         arrivals = [t for (t, _, _, _, _) in served_stream(nclips, rate, seed=5 + rank, max_len=args.max_len or 600)]
-        srv = sv.Server(budget, max_active=8, chunk_pairs=32)
+        srv = sv.Server(budget, max_active=args.max_active, chunk_pairs=args.chunk)
         ids = []
         if wi == 0:  # warm-up request (not measured)
             rid = srv.submit(sb0, an0, frames[k_small])
@@ -422,8 +422,9 @@ def run_served(args, world: int, rank: int, local: int):
             "dtype": "u8", "data": "synthetic",
             "config": {"workload": f"served: {nclips} clips per rate, Poisson arrivals, resolution from "
                                    f"360p/720p/1080p/1440p/2160p, 8-{args.max_len or 600} frames log-uniform, "
-                                   f"1080p Analyse options, HBM budget {args.budget_gb} GB, 8 active clips, "
-                                   f"chunks of 32 pairs", "pairs_per_rate": total_pairs, "generation_s": gen_s,
+                                   f"1080p Analyse options, HBM budget {args.budget_gb} GB, {args.max_active} active "
+                                   f"clips, chunks of {args.chunk} pairs", "pairs_per_rate": total_pairs,
+                       "generation_s": gen_s,
                        "latency": "clip arrival to that pair's payload in host memory"},
             "sweep": sweep,
             "e2e": {"value": best["pairs_per_s"], "unit": UNIT,
@@ -453,6 +454,8 @@ def main():
     ap.add_argument("--max-len", type=int, default=0, help="longest clip in frames (default: the workload's)")
     ap.add_argument("--rates", default="5,50,200", help="served: arrival rates, clips/s")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="served: HBM budget")
+    ap.add_argument("--max-active", type=int, default=8, help="served: clips in flight")
+    ap.add_argument("--chunk", type=int, default=32, help="served: output frames per launch")
     ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
 

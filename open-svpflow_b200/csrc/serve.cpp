@@ -6,7 +6,8 @@
 // order: its source frames copied in, its super frames built (kept resident for all of
 // its pairs: every super frame serves two adjacent pairs), its frame pairs analysed in
 // chunks of `chunk_pairs`, each chunk's payloads copied out as soon as it finishes, and
-// its memory released. Chunks of different clips run concurrently on the device, so a
+// its memory released. A clip's chunks are spread over the slot's kLanes streams (they are
+// independent frame pairs), and chunks of different clips run concurrently on the device, so a
 // clip admitted while others are being analysed starts at once, and one that finishes
 // frees its slot and memory for the next. Memory comes from the stream-ordered pool
 // (cudaMallocAsync / cudaFreeAsync), so admission never synchronises the device.
@@ -47,6 +48,8 @@ namespace {
 
 inline int64_t al256(int64_t v) { return (v + 255) & ~(int64_t)255; }
 
+constexpr int kLanes = 4;  // streams per slot: a clip's chunks run on them round-robin
+
 struct Request;
 
 struct Chunk {
@@ -71,7 +74,6 @@ struct Request {
     int status = 0;
     bool done = false;
     std::vector<Chunk> chunks;
-    std::atomic<int> chunks_left{0};
     svpf_server *server = nullptr;
 };
 
@@ -82,7 +84,8 @@ struct svpf_server {
     int64_t budget = 0, used = 0, peak_used = 0;
     int max_active = 0, active = 0, peak_active = 0;
     int32_t chunk_pairs = 32;
-    std::vector<cudaStream_t> streams;
+    std::vector<cudaStream_t> streams;          // kLanes per slot
+    std::vector<cudaEvent_t> events;            // kLanes + 1 per slot: lane joins, super frames ready
     std::vector<bool> slot_busy;
     int *slot_status = nullptr;                 // page-locked status word per slot
     std::vector<uint8_t *> stage;               // page-locked payload staging per slot (scheduler-owned)
@@ -110,10 +113,12 @@ int sfail(int code, const std::string &msg) {
     return code;
 }
 
+int64_t lanes_of(const Request &r) { return r.chunks.size() < (size_t)kLanes ? (int64_t)r.chunks.size() : kLanes; }
+
 int64_t request_bytes(const Request &r, int32_t chunk) {
     const int64_t c = chunk < r.nframes ? chunk : r.nframes;
     return al256(r.D.src_frame_bytes * r.nframes) + al256(r.D.frame_bytes * r.nframes) +
-           al256(r.P.payload_len * r.nframes) + al256(r.P.scratch_per_pair * c) + 256;
+           al256(r.P.payload_len * r.nframes) + lanes_of(r) * al256(r.P.scratch_per_pair * c) + 256;
 }
 
 // Host function behind a chunk's payload copy (no CUDA calls allowed here).
@@ -121,30 +126,41 @@ void CUDART_CB chunk_done(void *arg) {
     Chunk *ch = (Chunk *)arg;
     Request *r = ch->req;
     svpf_server *s = r->server;
-    const int64_t t0 = s->now_ns();
     if (ch->stage)
         memcpy(r->payloads + (int64_t)ch->first * r->P.payload_len, ch->stage, (size_t)(r->P.payload_len * ch->count));
-    const int64_t t = ch->stage ? s->now_ns() : t0;
+    const int64_t t = s->now_ns();
     if (r->pair_done_ns)
         for (int32_t i = 0; i < ch->count; i++) r->pair_done_ns[ch->first + i] = t;
-    if (r->chunks_left.fetch_sub(1) == 1) {
-        std::lock_guard<std::mutex> lk(s->mu);
-        r->done_ns = t;
-        r->status = s->slot_status[r->slot];
-        r->done = true;
-        s->used -= r->need;
-        s->active--;
-        s->slot_busy[(size_t)r->slot] = false;
-        s->completed++;
-        s->cv.notify_all();
-        s->done_cv.notify_all();
-    }
 }
 
-// Queues the whole of one admitted request on its slot's stream.
+// Host function after the request's lanes have joined, its status word has been copied
+// and its memory released.
+void CUDART_CB request_done(void *arg) {
+    Request *r = (Request *)arg;
+    svpf_server *s = r->server;
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->done_ns = s->now_ns();
+    r->status = s->slot_status[r->slot];
+    r->done = true;
+    s->used -= r->need;
+    s->active--;
+    s->slot_busy[(size_t)r->slot] = false;
+    s->completed++;
+    s->cv.notify_all();
+    s->done_cv.notify_all();
+}
+
+// Queues the whole of one admitted request on its slot's lanes: lane 0 allocates, copies the
+// frames in and builds the super frames; every lane then analyses its chunks (own scratch,
+// own staging) and copies their payloads out; lane 0 joins the lanes, copies the status word
+// out, releases the memory and reports.
 int enqueue(svpf_server *s, Request *r) {
-    cudaStream_t st = s->streams[(size_t)r->slot];
+    const int nl_lanes = (int)lanes_of(*r);
+    cudaStream_t lane[kLanes];
+    for (int k = 0; k < kLanes; k++) lane[k] = s->streams[(size_t)r->slot * kLanes + k];
+    cudaStream_t st = lane[0];
     const int64_t fb = r->D.frame_bytes, sb = r->D.src_frame_bytes;
+    const int64_t cmax = r->chunks.empty() ? 1 : r->chunks[0].count;
     cudaError_t e = cudaMallocAsync((void **)&r->dev, (size_t)r->need, st);
     if (e != cudaSuccess) {
         r->dev = nullptr;
@@ -153,45 +169,59 @@ int enqueue(svpf_server *s, Request *r) {
     uint8_t *frames = r->dev;
     uint8_t *supers = frames + al256(sb * r->nframes);
     uint8_t *pays = supers + al256(fb * r->nframes);
-    uint8_t *scr = pays + al256(r->P.payload_len * r->nframes);
-    int *status = (int *)(scr + al256(r->P.scratch_per_pair * (r->chunks.empty() ? 1 : r->chunks[0].count)));
-    uint8_t *stage = nullptr;
-    if (!r->pinned_out) {  // this thread owns the slot's staging buffer while the slot is busy
-        const size_t need = (size_t)(r->P.payload_len * (r->chunks.empty() ? 1 : r->chunks[0].count));
-        const size_t k = (size_t)r->slot;
-        if (s->stage_cap[k] < need) {
-            if (s->stage[k]) s->retired.push_back(s->stage[k]);
-            s->stage[k] = nullptr;
-            s->stage_cap[k] = 0;
-            if (cudaHostAlloc((void **)&s->stage[k], need, cudaHostAllocDefault) != cudaSuccess) return SVPF_ECUDA;
-            s->stage_cap[k] = need;
+    uint8_t *scr0 = pays + al256(r->P.payload_len * r->nframes);
+    const int64_t scr_lane = al256(r->P.scratch_per_pair * cmax);
+    int *status = (int *)(scr0 + nl_lanes * scr_lane);
+    uint8_t *stage[kLanes] = {nullptr, nullptr, nullptr, nullptr};
+    if (!r->pinned_out) {  // this thread owns the slot's staging buffers while the slot is busy
+        const size_t need = (size_t)(r->P.payload_len * cmax);
+        for (int k = 0; k < nl_lanes; k++) {
+            const size_t i = (size_t)r->slot * kLanes + k;
+            if (s->stage_cap[i] < need) {
+                if (s->stage[i]) s->retired.push_back(s->stage[i]);
+                s->stage[i] = nullptr;
+                s->stage_cap[i] = 0;
+                if (cudaHostAlloc((void **)&s->stage[i], need, cudaHostAllocDefault) != cudaSuccess) return SVPF_ECUDA;
+                s->stage_cap[i] = need;
+            }
+            stage[k] = s->stage[i];
         }
-        stage = s->stage[k];
     }
+    cudaEvent_t *ev = &s->events[(size_t)r->slot * (kLanes + 1)];
     int nl = 0;
     e = cudaMemsetAsync(status, 0, sizeof(int), st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(frames, r->frames, (size_t)(sb * r->nframes), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = launch_super(r->D, frames, supers, r->nframes, st, &nl);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[kLanes], st);
+    for (int k = 1; k < nl_lanes && e == cudaSuccess; k++) e = cudaStreamWaitEvent(lane[k], ev[kLanes], 0);
     for (size_t k = 0; e == cudaSuccess && k < r->chunks.size(); k++) {
         Chunk &c = r->chunks[k];
+        const int li = (int)(k % (size_t)nl_lanes);
+        cudaStream_t ls = lane[li];
         PairSrc src{};
         src.clip = supers;
         src.frame_bytes = fb;
         src.first = c.first;
         src.nframes = r->nframes;
         src.delta = r->delta;
-        e = launch_analyse(r->P, src, c.count, pays + (int64_t)c.first * r->P.payload_len, scr, status, st, &nl);
-        c.stage = stage;
+        e = launch_analyse(r->P, src, c.count, pays + (int64_t)c.first * r->P.payload_len, scr0 + li * scr_lane, status,
+                           ls, &nl);
+        c.stage = stage[li];
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(stage ? stage : r->payloads + (int64_t)c.first * r->P.payload_len,
+            e = cudaMemcpyAsync(c.stage ? c.stage : r->payloads + (int64_t)c.first * r->P.payload_len,
                                 pays + (int64_t)c.first * r->P.payload_len, (size_t)(r->P.payload_len * c.count),
-                                cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess && k + 1 == r->chunks.size()) {
-            e = cudaMemcpyAsync(&s->slot_status[r->slot], status, sizeof(int), cudaMemcpyDeviceToHost, st);
-            if (e == cudaSuccess) e = cudaFreeAsync(r->dev, st);
-            if (e == cudaSuccess) r->dev = nullptr;
-        }
-        if (e == cudaSuccess) e = cudaLaunchHostFunc(st, chunk_done, &c);
+                                cudaMemcpyDeviceToHost, ls);
+        if (e == cudaSuccess) e = cudaLaunchHostFunc(ls, chunk_done, &c);
+    }
+    for (int k = 1; k < nl_lanes && e == cudaSuccess; k++) {
+        e = cudaEventRecord(ev[k], lane[k]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev[k], 0);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&s->slot_status[r->slot], status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaFreeAsync(r->dev, st);
+    if (e == cudaSuccess) {
+        r->dev = nullptr;
+        e = cudaLaunchHostFunc(st, request_done, r);
     }
     s->launches += nl;
     return e == cudaSuccess ? SVPF_OK : SVPF_ECUDA;
@@ -232,7 +262,7 @@ void scheduler(svpf_server *s) {
         lk.lock();
         if (rc != SVPF_OK) {  // its last chunk will never report: wait out what was queued, release it here
             lk.unlock();
-            cudaStreamSynchronize(s->streams[(size_t)slot]);
+            for (int k = 0; k < kLanes; k++) cudaStreamSynchronize(s->streams[(size_t)slot * kLanes + k]);
             if (r->dev) cudaFree(r->dev);
             r->dev = nullptr;
             lk.lock();
@@ -270,22 +300,24 @@ int svpf_server_create(size_t hbm_budget_bytes, int32_t max_active, int32_t chun
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
         }
     }
-    s->streams.assign((size_t)max_active, nullptr);
+    s->streams.assign((size_t)max_active * kLanes, nullptr);
+    s->events.assign((size_t)max_active * (kLanes + 1), nullptr);
     s->slot_busy.assign((size_t)max_active, false);
-    s->stage.assign((size_t)max_active, nullptr);
-    s->stage_cap.assign((size_t)max_active, 0);
-    if (cudaHostAlloc((void **)&s->slot_status, sizeof(int) * (size_t)max_active, cudaHostAllocDefault) != cudaSuccess) {
+    s->stage.assign((size_t)max_active * kLanes, nullptr);
+    s->stage_cap.assign((size_t)max_active * kLanes, 0);
+    cudaError_t e = cudaHostAlloc((void **)&s->slot_status, sizeof(int) * (size_t)max_active, cudaHostAllocDefault);
+    for (auto &ev : s->events)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    for (auto &st : s->streams)
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        for (auto &x : s->streams)
+            if (x) cudaStreamDestroy(x);
+        for (auto &x : s->events)
+            if (x) cudaEventDestroy(x);
+        if (s->slot_status) cudaFreeHost(s->slot_status);
         delete s;
-        return sfail(SVPF_ECUDA, "cudaHostAlloc (status words)");
-    }
-    for (auto &st : s->streams) {
-        cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-        if (e != cudaSuccess) {
-            for (auto &x : s->streams)
-                if (x) cudaStreamDestroy(x);
-            delete s;
-            return sfail(SVPF_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
-        }
+        return sfail(SVPF_ECUDA, std::string("server set-up: ") + cudaGetErrorString(e));
     }
     s->worker = std::thread(scheduler, s);
     *out = s;
@@ -309,7 +341,6 @@ int svpf_server_submit(svpf_server *s, const svpf_super *sup, const svpf_analyse
     r->server = s;
     for (int32_t f = 0; f < nframes; f += s->chunk_pairs)
         r->chunks.push_back(Chunk{r.get(), f, (nframes - f) < s->chunk_pairs ? nframes - f : s->chunk_pairs});
-    r->chunks_left = (int)r->chunks.size();
     r->need = request_bytes(*r, s->chunk_pairs);
     if (r->need > s->budget) return sfail(SVPF_EINVAL, "clip needs more device memory than the server's budget");
     {
@@ -371,6 +402,8 @@ void svpf_server_destroy(svpf_server *s) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
     }
+    for (auto &ev : s->events)
+        if (ev) cudaEventDestroy(ev);
     for (uint8_t *p : s->stage)
         if (p) cudaFreeHost(p);
     for (uint8_t *p : s->retired) cudaFreeHost(p);
