@@ -656,12 +656,20 @@ __device__ __noinline__ Res slow_lane(const AnalyseParams *P, const LevelInfo *L
 }
 
 
+// Lanes per candidate for a step of n candidates: the widest power-of-two group (at most a
+// warp, at least the level's G) that still puts every candidate in one round. Small steps
+// (a hexagon, a ring, the special candidates) then finish in fewer tiles per lane.
+__device__ __forceinline__ int step_lanes(int G, int n) {
+    while (G < 32 && NW * (16 / G) >= n) G <<= 1;
+    return G;
+}
+
 // Work of one lane (`sub` of G) on one candidate: its share of the 4x4 tiles.
 // kind 0: block at (b.px, b.py); 1: the same mv on the block at (px, py) (general path);
 // 2: the block's luma pixel sum (block_luma_dc).
 __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, int px, int py, int mvx, int mvy,
-                                         bool chroma, int sub) {
-    const int G = x.grp_lanes, TL = x.tl, TCp = x.tcp;
+                                         bool chroma, int sub, int G) {
+    const int TL = x.tl, TCp = x.tcp;
     int lref = 0, cref = 0;
     bool fast = false;
     if (kind == 0) fast = fast_setup(x, b, mvx, mvy, lref, cref);
@@ -717,9 +725,7 @@ __device__ __forceinline__ void finalize(const Res &r, unsigned &L, unsigned &C)
 // and the new best cost / sad when accepted.
 __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s, int &ph, const Gen &g, int lambda,
                                           int predx, int predy, long long &best_cost, unsigned &best_sad, int &win) {
-    const int G = x.grp_lanes, gpw = 32 / G;
     const int lane = x.tid & 31, warp = x.tid >> 5;
-    const int grp = warp * gpw + lane / G, sub = lane & (G - 1), NG = NW * gpw;
     const bool serial = x.pnew < -256;
     const int pnew = x.pnew;
     long long bk = 0x7FFFFFFFFFFFFFFFLL;
@@ -734,6 +740,7 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
         // computes the same list, so no barrier is needed)
 #pragma unroll
         for (int w = 0; w < MW; w++) {
+            if (base + w * 32 >= g.n) break;  // uniform
             const int i = base + w * 32 + lane;
             bool ok = i < g.n;
             int2 mv = make_int2(0, 0);
@@ -749,6 +756,8 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
             total += __popc(m);
         }
         __syncwarp();
+        const int G = step_lanes(x.grp_lanes, total);
+        const int grp = warp * (32 / G) + lane / G, sub = lane & (G - 1), NG = NW * (32 / G);
         for (int r0 = 0; r0 < total; r0 += NG) {
             const int rk = r0 + grp;
             const bool act = rk < total;
@@ -1072,9 +1081,7 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
     uint8_t *lumaf = ds.luma[level & 1];
     const int64_t order_len = s.order_len;
     const bool smallest = L.smallest != 0;
-    const int G = x.grp_lanes, gpw = 32 / G;
     const int lane = x.tid & 31, warp = x.tid >> 5;
-    const int grp = warp * gpw + lane / G, sub = lane & (G - 1), NG = NW * gpw;
     int bad_count = 0;
     int ph = 0;
     // The previous block's result: stored by thread 0 after the block's last barrier, so
@@ -1153,6 +1160,8 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
         n += nseeds;
         const int dcslot = n++;
         // ---- evaluate the special slots
+        const int G = step_lanes(x.grp_lanes, n);
+        const int grp = warp * (32 / G) + lane / G, sub = lane & (G - 1), NG = NW * (32 / G);
         for (int j0 = 0; j0 < n; j0 += NG) {
             const int j = j0 + grp;
             const bool act = j < n;
@@ -1170,7 +1179,7 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
                     if (t == j - nslot0) { mx = sdx[t]; my = sdy[t]; }
             }
             Res r{0, 0, 0, 0, 0, 0};
-            if (act) r = eval_lane(x, b, kind, sxi * P.step_x, syi * P.step_y, mx, my, ch, sub);
+            if (act) r = eval_lane(x, b, kind, sxi * P.step_x, syi * P.step_y, mx, my, ch, sub, G);
             r.L = group_sum(r.L, G);
             r.U = group_sum(r.U, G);
             r.V = group_sum(r.V, G);
@@ -1319,11 +1328,11 @@ __device__ __forceinline__ void refine_pass(Ctx &x, DirSh &s, DirScratch &ds) {
             const bool search = parent > (long long)threshold;
             stage_source(x, s, b);
             {  // slot 0: exact_sad at the clipped predictor (when searching); slot 1: block_luma_dc
-                const int Gl = x.grp_lanes, lane = x.tid & 31, grp = (x.tid >> 5) * (32 / Gl) + lane / Gl;
+                const int Gl = step_lanes(x.grp_lanes, 2), lane = x.tid & 31, grp = (x.tid >> 5) * (32 / Gl) + lane / Gl;
                 const int sub = lane & (Gl - 1);
                 const bool act = (grp == 0 && search) || grp == 1;
                 Res r{0, 0, 0, 0, 0, 0};
-                if (act) r = eval_lane(x, b, grp == 1 ? 2 : 0, 0, 0, pmx, pmy, grp == 0, sub);
+                if (act) r = eval_lane(x, b, grp == 1 ? 2 : 0, 0, 0, pmx, pmy, grp == 0, sub, Gl);
                 r.L = group_sum(r.L, Gl);
                 r.U = group_sum(r.U, Gl);
                 r.V = group_sum(r.V, Gl);
