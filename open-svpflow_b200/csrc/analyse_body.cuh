@@ -119,9 +119,11 @@ __device__ __forceinline__ unsigned rd(const uint8_t *p, int64_t len, int64_t i,
     return (i >= 0 && i < len) ? (unsigned)__ldg(p + i) : dflt;
 }
 __device__ __forceinline__ long long pen(int pnew, unsigned x) { return (long long)x + (((long long)pnew * (long long)x) >> 8); }
+// (lambda * |pred - mv|^2) >> 8; vectors are below 2^16 in magnitude, so the differences
+// fit 32 bits and the squares are single widening multiplies
 __device__ __forceinline__ long long motion_penalty(int lambda, int px_, int py_, int mx, int my) {
-    long long dx = (long long)px_ - mx, dy = (long long)py_ - my;
-    return ((long long)lambda * (dx * dx + dy * dy)) >> 8;
+    const int dx = px_ - mx, dy = py_ - my;
+    return ((long long)lambda * ((long long)dx * dx + (long long)dy * dy)) >> 8;
 }
 
 // hadamard4_satd, analyse_search.rs:2681-2702: rows, then columns; the last column
@@ -561,6 +563,8 @@ struct BlkC {
     int chroma, satd_mode, fastable, fast_src, cfast_src, dc_fast;
     int cw, ch, crows, cpx, cpy, tilesx, ctilesx;
     int lgtx, lgctx;                       // log2 of tilesx / ctilesx (block sizes are powers of two)
+    int fx0, fx1, fy0, fy1;                // vectors taking the fast path lie in this box (inclusive) ...
+    int lbase, llim, cbase, clim;          // ... and have lref <= llim, cref <= clim (offsets from these bases)
     int64_t lsrc, csrc, dsrc;              // flat index of the source block (luma, chroma, luma at (px, py))
 };
 
@@ -595,34 +599,44 @@ __device__ __forceinline__ void make_blk(const Ctx &x, int px, int py, bool chro
     b.cfast_src = (b.cw == 4 || b.cw == 8 || b.cw == 16) && b.ch >= 4 && (b.ch & 3) == 0 && px >= 0 && py >= 0 &&
                   b.cpx + b.cw <= G.clw && b.cpy + b.ch <= G.clh &&
                   b.csrc + (int64_t)(b.crows - 1) * G.cs + b.cw + 8 <= G.clen;
+    // the fast-path box: no edge shift, reference block inside the level (luma, and chroma when
+    // it is evaluated); with l0sub the luma offset is mv >> 1 and the chroma one mv >> 2
+    const bool l0sub = x.level == 0 && pel >= 2;
+    const int ls = l0sub ? 1 : 0, cshift = l0sub ? 2 : 1;
+    b.fx0 = imax(b.bnd0, (-b.px2) * (1 << ls));
+    b.fx1 = imin(b.ubx - 1, (G.lw - bw - b.px2) * (1 << ls) + (1 << ls) - 1);
+    b.fy0 = imax(b.bnd1, (-b.py2) * (1 << ls));
+    b.fy1 = imin(b.uby - 1, (G.lh - bh - b.py2) * (1 << ls) + (1 << ls) - 1);
+    if (b.chroma && b.cw >= 4 && b.ch >= 4) {
+        b.fx0 = imax(b.fx0, (-b.cpx) * (1 << cshift));
+        b.fx1 = imin(b.fx1, (G.clw - b.cw - b.cpx) * (1 << cshift) + (1 << cshift) - 1);
+        b.fy0 = imax(b.fy0, (-b.cpy) * (1 << cshift));
+        b.fy1 = imin(b.fy1, (G.clh - b.ch - b.cpy) * (1 << cshift) + (1 << cshift) - 1);
+        if (!b.cfast_src) b.fx1 = b.fx0 - 1;
+    }
+    if (!b.fast_src) b.fx1 = b.fx0 - 1;  // empty box
+    b.lbase = (int)L.y_off * G.ys32;
+    b.llim = (int)G.ylen - (bh - 1) * G.ys32 - bw - 8;
+    b.cbase = (int)L.c_off * G.cs32;
+    b.clim = (int)G.clen - (b.crows - 1) * G.cs32 - b.cw - 8;
 }
 
 // Does (block, mv) take the fast path? If so, the flat indices of its reference blocks.
 // It does when the reference takes its direct reads for both luma and chroma: no edge
 // shift, the luma block and the reference block inside the level, the chroma blocks too.
 __device__ __forceinline__ bool fast_setup(const Ctx &x, const BlkC &b, int mvx, int mvy, int &lref, int &cref) {
-    if (!(b.fast_src && mvx >= b.bnd0 && mvx < b.ubx && mvy >= b.bnd1 && mvy < b.uby)) return false;
-    const LevelInfo &L = *x.L;
-    const Geo &G = x.G;
+    if (mvx < b.fx0 || mvx > b.fx1 || mvy < b.fy0 || mvy > b.fy1) return false;
     const int pel = imax(x.pel, 1);
-    int mx = mvx, my = mvy, sub = 0;
     const bool l0sub = x.level == 0 && pel >= 2;
-    if (l0sub) { sub = (mvy & 1) * pel + (mvx & 1); mx = mvx >> 1; my = mvy >> 1; }
-    const int rx0 = b.px2 + mx, ry0 = b.py2 + my;
-    if (rx0 < 0 || ry0 < 0 || rx0 + b.bw > G.lw || ry0 + b.bh > G.lh) return false;
-    lref = ((int)L.y_off + sub * G.lh + ry0) * G.ys32 + rx0;
-    if (lref + (b.bh - 1) * G.ys32 + b.bw + 8 > (int)G.ylen) return false;
+    const int sub = l0sub ? (mvy & 1) * pel + (mvx & 1) : 0;
+    const int mx = l0sub ? mvx >> 1 : mvx, my = l0sub ? mvy >> 1 : mvy;
+    lref = b.lbase + (sub * x.G.lh + b.py2 + my) * x.G.ys32 + b.px2 + mx;
+    if (lref > b.llim) return false;
     cref = 0;
     if (b.chroma && b.cw >= 4 && b.ch >= 4) {
-        if (!b.cfast_src) return false;
-        int mcx, mcy;
-        if (l0sub) { mcx = mvx >> 2; mcy = mvy >> 2; }
-        else { mcx = mvx >> 1; mcy = mvy >> 1; }
-        const int crx = b.cpx + mcx, cry = b.cpy + mcy;
-        if (crx < 0 || cry < 0 || crx + b.cw > G.clw || cry + b.ch > G.clh) return false;
-        const int crow0 = (int)L.c_off + ((x.level == 0 && pel > 1) ? sub * G.clh : 0);
-        cref = (crow0 + cry) * G.cs32 + crx;
-        if (cref + (b.crows - 1) * G.cs32 + b.cw + 8 > (int)G.clen) return false;
+        const int mcx = l0sub ? mvx >> 2 : mvx >> 1, mcy = l0sub ? mvy >> 2 : mvy >> 1;
+        cref = b.cbase + ((l0sub ? sub * x.G.clh : 0) + b.cpy + mcy) * x.G.cs32 + b.cpx + mcx;
+        if (cref > b.clim) return false;
     }
     return true;
 }
