@@ -1,8 +1,9 @@
 // analyse_body.cuh -- hierarchical block search (Analyse) on sm_100a.
 //
 // Included by one translation unit per launch variant (analyse_nt128.cu, analyse_nt64.cu,
-// analyse_nt32.cu): SVPF_NT = threads per search direction, SVPF_MINB = resident CTAs per
-// SM the register budget is cut for, SVPF_VARIANT = the variant's namespace. Each variant
+// analyse_nt32.cu, analyse_nt128b3.cu, analyse_nt64b6.cu): SVPF_NT = threads per search
+// direction, SVPF_MINB = resident CTAs per SM the register budget is cut for (2, 4, 8: 128
+// registers per thread; 3, 6: 80), SVPF_VARIANT = the variant's namespace. Each variant
 // exports a plain launcher (one CTA per pair) and a persistent batch launcher (CTAs
 // drain a device work queue of frame pairs from many clips).
 //
@@ -101,7 +102,12 @@ struct Geo {  // per level
     int ys32, cs32;   // the strides again, for 32-bit offsets (planes are below 2^30 bytes)
 };
 
-__device__ __forceinline__ void dbar(int d) { asm volatile("bar.sync %0, %1;" ::"r"(d + 1), "r"(NT) : "memory"); }
+// Named barrier of one search direction (ids 1 and 2; 0 is __syncthreads). Immediate ids,
+// so the kernel reserves three barriers, not all sixteen (barriers bound CTAs per SM).
+__device__ __forceinline__ void dbar(int d) {
+    if (d) asm volatile("bar.sync 2, %0;" ::"n"(NT) : "memory");
+    else asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
+}
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
 __device__ __forceinline__ int iclamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }

@@ -60,6 +60,9 @@ struct BatchItem {
 SVPF_DECLARE_ANALYSE_VARIANT(nt128)
 SVPF_DECLARE_ANALYSE_VARIANT(nt64)
 SVPF_DECLARE_ANALYSE_VARIANT(nt32)
+SVPF_DECLARE_ANALYSE_VARIANT(nt128b3)
+SVPF_DECLARE_ANALYSE_VARIANT(nt64b6)
+
 
 // A compiled launch shape of the Analyse kernels: threads per search direction and the
 // resident CTAs per SM its register budget was cut for. Results do not depend on it.

@@ -8,6 +8,9 @@ const AnalyseVariant kVariants[] = {
     {"nt128_b2", 128, 2, nt128::launch_plain, nt128::batch_blocks_per_sm, nt128::launch_batch},
     {"nt64_b4", 64, 4, nt64::launch_plain, nt64::batch_blocks_per_sm, nt64::launch_batch},
     {"nt32_b8", 32, 8, nt32::launch_plain, nt32::batch_blocks_per_sm, nt32::launch_batch},
+    {"nt128_b3", 128, 3, nt128b3::launch_plain, nt128b3::batch_blocks_per_sm, nt128b3::launch_batch},
+    {"nt64_b6", 64, 6, nt64b6::launch_plain, nt64b6::batch_blocks_per_sm, nt64b6::launch_batch},
+
 };
 }  // namespace
 
