@@ -51,6 +51,9 @@ from svpflow_b200.synth import (ANALYSE_OPT, CONFIGS, SUPER_OPT, analyse_opt_for
 WORKLOAD = "1080p"
 METRIC = "Analyse frame-pairs/s at 1080p (bit-exact MVs)"
 UNIT = "frame-pairs/s"
+# DRAM bytes per frame pair of the Analyse kernel at 1080p (ncu capture of a 17-pair launch:
+# 294.6 MB read + 55.2 MB written)
+TRAFFIC_PER_PAIR = 349.8e6 / 17
 
 
 def _peaks():
@@ -570,7 +573,9 @@ def main():
         roof = {
             "kernel": "analyse_kernel (one CTA per frame pair, fwd/bwd halves)",
             "bound": "hbm", "achieved": alg_analyse / (a_ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
-            "frac": alg_analyse / (a_ms / 1000) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+            "frac": alg_analyse / (a_ms / 1000) / 1e9 / peak, "traffic": TRAFFIC_PER_PAIR * nf,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 17-pair launch, per pair x pairs",
+            "peak_source": peak_kind,
             "algorithmic_bytes_per_launch": alg_analyse, "avg_launch_ms": a_ms,
             "note": "integer- and dependency-chain-bound block search; the HBM fraction shows how far from "
                     "HBM-bound it is",

@@ -204,8 +204,8 @@ int enqueue(svpf_server *s, Request *r) {
         src.first = c.first;
         src.nframes = r->nframes;
         src.delta = r->delta;
-        e = launch_analyse(r->P, src, c.count, pays + (int64_t)c.first * r->P.payload_len, scr0 + li * scr_lane, status,
-                           ls, &nl);
+        e = launch_analyse_shape(kShapeShared, r->P, src, c.count, pays + (int64_t)c.first * r->P.payload_len,
+                                 scr0 + li * scr_lane, status, ls, &nl);
         c.stage = stage[li];
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(c.stage ? c.stage : r->payloads + (int64_t)c.first * r->P.payload_len,

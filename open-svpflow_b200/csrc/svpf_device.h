@@ -83,5 +83,9 @@ const AnalyseVariant &analyse_variant(int i);  // 0 = the plain path's default (
 // the caller.
 cudaError_t launch_analyse(const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,
                            uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches);
+// The same with a given launch shape (analyse_variant index).
+cudaError_t launch_analyse_shape(int variant, const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,
+                                 uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches);
+constexpr int kShapeShared = 3;  // nt128_b3: the shape for launches that share SMs with others
 
 }  // namespace svpf

@@ -19,9 +19,24 @@ const AnalyseVariant &analyse_variant(int i) {
     return kVariants[(i >= 0 && i < analyse_variant_count()) ? i : 0];
 }
 
+// More pairs than two per SM: the 80-register shape keeps three pairs per SM resident (the
+// fastest for full launches); otherwise the 128-register shape, which is faster per pair.
 cudaError_t launch_analyse(const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,
                            uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches) {
+    static int sms = [] {
+        int dev = 0, n = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return 0;
+        return n;
+    }();
+    if (sms > 0 && npairs > 2 * sms)
+        return nt128b3::launch_plain(P, src, npairs, payloads, scratch, status_dev, stream, launches);
     return nt128::launch_plain(P, src, npairs, payloads, scratch, status_dev, stream, launches);
+}
+
+cudaError_t launch_analyse_shape(int variant, const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,
+                                 uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches) {
+    return analyse_variant(variant).launch_plain(P, src, npairs, payloads, scratch, status_dev, stream, launches);
 }
 
 }  // namespace svpf
