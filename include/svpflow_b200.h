@@ -122,6 +122,20 @@ int svpf_clip_analyse(svpf_analyser *a, const svpf_super *s, const uint8_t *fram
 int64_t svpf_kernel_launches(void);
 void svpf_kernel_launches_reset(void);
 
+/* ---------------------------------------------------------------- payload consumers */
+/* The motion-vector grid a frame interpolator samples for a vdata header: metadata.rs
+ * vector_data (:89-115) and motion_grid / extended_grid (crates/svpflow-core/src/metadata.rs:211-244). */
+int svpf_vector_grid(const int32_t *vdata, int32_t *motion_w, int32_t *motion_h);
+/* decode_vectors (crates/svpflow-core/src/metadata.rs:246-273) and vector_planes
+ * (crates/svpflow-core/src/renderer.rs:1680-1726) as SmoothFps applies them (svpflow2 core.rs:962-1001),
+ * on the device: `npayloads` Analyse payloads (payload_len bytes apart) -> per payload four uint16
+ * planes mvx0 | mvy0 | mvx1 | mvy1 of motion_w x motion_h (centred on 1024; 0 = previous set,
+ * 1 = current set), vectors clamped to the frame_w x frame_h frame unless `raw`. status_dev[i]
+ * becomes 1 where payload i does not decode (the reference's None). Asynchronous on `stream`. */
+int svpf_vector_planes_device(const int32_t *vdata, const uint8_t *payloads_dev, size_t payload_len, int32_t npayloads,
+                              int32_t frame_w, int32_t frame_h, int32_t raw, uint16_t *planes_dev, int32_t *status_dev,
+                              void *stream);
+
 /* ---------------------------------------------------------------- batched form */
 /* No counterpart in the reference, which analyses one clip at a time, one output frame
  * per getFrame call (crates/svpflow1/src/analyse_filter.rs:229-334). A batch holds many

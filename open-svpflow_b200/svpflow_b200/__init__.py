@@ -96,6 +96,8 @@ def lib() -> ctypes.CDLL:
             "svpf_server_wait": (I32, [_VP, I64, P(I64)]),
             "svpf_server_now_ns": (I64, [_VP]),
             "svpf_server_stats": (None, [_VP, P(I64), P(I64), P(I64), P(I32), P(I64)]),
+            "svpf_vector_grid": (I32, [P(I32), P(I32), P(I32)]),
+            "svpf_vector_planes_device": (I32, [P(I32), _VP, SZ, I32, I32, I32, I32, _VP, _VP, _VP]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -425,3 +427,19 @@ class Server:
                                 ctypes.byref(l))
         return {"admitted": a.value, "completed": c.value, "peak_device_bytes": pb.value, "peak_active": pa.value,
                 "kernel_launches": l.value}
+
+
+def vector_grid(vdata) -> tuple:
+    """(motion_w, motion_h) of the motion-vector planes for a vdata header (metadata.rs:211-244)."""
+    v = (ctypes.c_int32 * 16)(*vdata)
+    mw, mh = ctypes.c_int32(), ctypes.c_int32()
+    _check(lib().svpf_vector_grid(v, ctypes.byref(mw), ctypes.byref(mh)))
+    return mw.value, mh.value
+
+
+def vector_planes_device(vdata, payloads_ptr: int, payload_len: int, npayloads: int, frame_w: int, frame_h: int,
+                         planes_ptr: int, status_ptr: int, raw: bool = False, stream: int = 0):
+    """decode_vectors + vector_planes on device buffers (see include/svpflow_b200.h)."""
+    v = (ctypes.c_int32 * 16)(*vdata)
+    _check(lib().svpf_vector_planes_device(v, payloads_ptr, payload_len, npayloads, frame_w, frame_h, int(raw),
+                                           planes_ptr, status_ptr, stream))

@@ -410,6 +410,9 @@ def lib():
         L.or_analyse_pair.argtypes = [P(Planes), P(Planes), P(AnalyseOpts), ctypes.c_void_p, ctypes.c_void_p]
         L.or_pack_vdata_header.argtypes = [P(AnalyseOpts), P(ctypes.c_int32)]
         L.or_hadamard4_satd.restype = ctypes.c_uint32
+        L.or_vector_grid.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.or_vector_planes.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
         L.or_hadamard4_satd.argtypes = [P(ctypes.c_int32)]
         L.or_adapt_lambda.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
         L.or_exact_lambda.argtypes = [P(AnalyseOpts), ctypes.c_int32, ctypes.c_int32]
@@ -623,3 +626,21 @@ def analyse_strided(ao: AnalyseOpts, cur: np.ndarray, ref: np.ndarray, y_stride:
     lib().or_pack_vector_frame(ctypes.byref(ao), bwd if ao.vectors & 1 else None, fwd if ao.vectors & 2 else None,
                                _ptr(out))
     return out
+
+
+def vector_grid(vdata) -> tuple:
+    v = (ctypes.c_int32 * 16)(*vdata)
+    mw, mh = ctypes.c_int32(), ctypes.c_int32()
+    lib().or_vector_grid(v, ctypes.byref(mw), ctypes.byref(mh))
+    return mw.value, mh.value
+
+
+def vector_planes(vdata, payload: np.ndarray, frame_w: int, frame_h: int, raw: bool = False):
+    """decode_vectors + vector_planes (svpflow-core) for both sets -> uint16 [4, mh, mw], or None
+    when the payload does not decode."""
+    mw, mh = vector_grid(vdata)
+    out = np.zeros(4 * max(mw, 0) * max(mh, 0), dtype=np.uint16)
+    payload = np.ascontiguousarray(payload, dtype=np.uint8)
+    v = (ctypes.c_int32 * 16)(*vdata)
+    rc = lib().or_vector_planes(v, _ptr(payload), payload.size, frame_w, frame_h, int(raw), out.ctypes.data)
+    return None if rc else out.reshape(4, mh, mw)

@@ -1784,3 +1784,83 @@ int or_analyse_clip(const or_analyse_opts *o, const or_super_opts *so, const uin
     (void)threads;
     return rc;
 }
+
+/* ------------------------------------------------------------------ svpflow-core consumers */
+/* metadata.rs:241-244 extended_grid */
+static int32_t ext_grid(int32_t block, int32_t overlap, int32_t grid, int32_t source) {
+    i64 span = (i64)(block - overlap) * grid + overlap;
+    return grid + (span < source ? 1 : 0);
+}
+void or_vector_grid(const int32_t vdata[16], int32_t *mw, int32_t *mh) {
+    *mw = ext_grid(vdata[2], vdata[9], vdata[11], vdata[7]);
+    *mh = ext_grid(vdata[3], vdata[10], vdata[12], vdata[8]);
+}
+static int rd_i32(const uint8_t *p, size_t len, size_t off, int32_t *v) { /* read_i32_slice, :498-502 */
+    if (off > len || len - off < 4) return 0;
+    memcpy(v, p + off, 4);
+    return 1;
+}
+/* decode_region (:455-481): 0 when the region does not decode */
+static int decode_region(const uint8_t *p, size_t len, size_t off, size_t count, int16_t *dx, int16_t *dy) {
+    int32_t m;
+    if (!rd_i32(p, len, off, &m) || (i64)m != (i64)(2 * count + 1)) return 0;
+    for (size_t i = 0; i < count; i++) {
+        int32_t r0, r1;
+        if (!rd_i32(p, len, off + 4 + i * 8, &r0) || !rd_i32(p, len, off + 8 + i * 8, &r1)) return 0;
+        uint32_t rot = ((uint32_t)r0 >> 16) | ((uint32_t)r0 << 16); /* rotate_right(16) */
+        dx[i] = (int16_t)(rot & 0xFFFF);
+        dy[i] = (int16_t)(rot >> 16);
+    }
+    return 1;
+}
+static int clamp_frame(int v, int pos, int block, int frame) { /* renderer.rs:1728-1736 */
+    if (v + pos < 0) return -pos;
+    if (v + block + pos > frame) return imax(frame - block - pos, 0);
+    return v;
+}
+static uint16_t centered16(int v) { return (v > 1023 || v < -1023) ? 1024 : (uint16_t)(v + 1024); } /* :3237-3243 */
+/* decode_vectors (metadata.rs:246-273) with SmoothFps' fallbacks (svpflow2 core.rs:962-1001) and
+ * vector_planes (renderer.rs:1680-1726) for both sets: out = mvx0 | mvy0 | mvx1 | mvy1. */
+int or_vector_planes(const int32_t vdata[16], const uint8_t *p, size_t len, int32_t frame_w, int32_t frame_h,
+                     int32_t raw, uint16_t *out) {
+    int32_t flags = vdata[1], gw = imax(vdata[11], 0), gh = imax(vdata[12], 0), v;
+    if (vdata[0] != 0xA0) return -1;
+    if (!rd_i32(p, len, 0, &v) || v != 16 || !rd_i32(p, len, 4, &v) || v != 0xA0 || !rd_i32(p, len, 8, &v) ||
+        v != flags)
+        return -1;
+    size_t count = (size_t)gw * (size_t)gh, first = 0x40, second = first + 4 + count * 8;
+    int16_t *px = calloc(count + 1, 2), *py = calloc(count + 1, 2), *cx = calloc(count + 1, 2),
+            *cy = calloc(count + 1, 2);
+    int okp = (flags & 1) ? decode_region(p, len, first, count, px, py) : 0;
+    int okc = (flags & 2) ? decode_region(p, len, second, count, cx, cy) : 0;
+    int rc = 0;
+    if (((flags & 1) && !okp) || ((flags & 2) && !okc) || (!okp && !okc)) rc = -1;
+    else {
+        if (!okp) { memcpy(px, cx, count * 2); memcpy(py, cy, count * 2); }
+        if (!okc) { memcpy(cx, px, count * 2); memcpy(cy, py, count * 2); }
+        int32_t mw, mh;
+        or_vector_grid(vdata, &mw, &mh);
+        mw = imax(mw, 0); mh = imax(mh, 0);
+        int32_t bw = imax(vdata[2], 1), bh = imax(vdata[3], 1), stx = bw - vdata[9], sty = bh - vdata[10];
+        size_t n = (size_t)mw * (size_t)mh;
+        for (int32_t y = 0; y < mh; y++)
+            for (int32_t x = 0; x < mw; x++) {
+                size_t sx = (size_t)imin(x, imax(gw - 1, 0)), sy = (size_t)imin(y, imax(gh - 1, 0));
+                size_t si = sy * (size_t)gw + sx, o = (size_t)y * mw + x;
+                for (int w = 0; w < 2; w++) {
+                    int dx = 0, dy = 0;
+                    if (si < count) { dx = w ? cx[si] : px[si]; dy = w ? cy[si] : py[si]; }
+                    uint16_t ox, oy;
+                    if (dx > 1023 || dx < -1023 || dy > 1023 || dy < -1023) ox = oy = 1024;
+                    else {
+                        if (!raw) { dx = clamp_frame(dx, x * stx, bw, frame_w); dy = clamp_frame(dy, y * sty, bh, frame_h); }
+                        ox = centered16(dx); oy = centered16(dy);
+                    }
+                    out[(size_t)(2 * w) * n + o] = ox;
+                    out[(size_t)(2 * w + 1) * n + o] = oy;
+                }
+            }
+    }
+    free(px); free(py); free(cx); free(cy);
+    return rc;
+}

@@ -162,6 +162,13 @@ int or_analyse_clip(const or_analyse_opts *o, const or_super_opts *so, const uin
 void or_build_super_many(const or_super_opts *o, const uint8_t *const *src, uint8_t *const *out,
                          int32_t nframes, int32_t threads);
 
+/* ---- consumers of the payload (svpflow-core metadata.rs / renderer.rs) ---- */
+void or_vector_grid(const int32_t vdata[16], int32_t *mw, int32_t *mh);
+/* decode_vectors + vector_planes for both sets; out = mvx0 | mvy0 | mvx1 | mvy1 (mw x mh each);
+ * returns -1 when the payload does not decode (the reference's None). */
+int or_vector_planes(const int32_t vdata[16], const uint8_t *payload, size_t len, int32_t frame_w, int32_t frame_h,
+                     int32_t raw, uint16_t *out);
+
 /* ---- primitives exposed for known-answer tests ---- */
 uint32_t or_hadamard4_satd(const int32_t diff[16]);
 int32_t or_adapt_lambda(int32_t nlambda, int32_t lsad, uint32_t pred_score);
