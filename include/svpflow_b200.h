@@ -47,6 +47,13 @@ int64_t svpf_reference_version(void);
  * VapourSynth `opt:data` string (lenient JSON, crates/svpflow-core/src/params.rs);
  * NULL or an unparsable string means defaults, as in super_filter.rs:107-121. */
 int svpf_super_create(int32_t width, int32_t height, const char *opt, size_t opt_len, svpf_super **out);
+/* svpf_super_create for `bits` = 8 (identical) or 10: this project's 10-bit extension, which
+ * the reference does not have (it is 8-bit only). Frames are then uint16 samples 0..1023,
+ * every size and offset of the API counts samples except the *_len / buffer sizes, which are
+ * bytes; the Super arithmetic is the same with its clamps at 1023. */
+int svpf_super_create_bits(int32_t width, int32_t height, const char *opt, size_t opt_len, int32_t bits,
+                           svpf_super **out);
+int32_t svpf_super_bits(const svpf_super *s);
 /* SuperBuilder::new(width, height, pel) (crates/svpflow1/src/portable.rs:30-62). */
 int svpf_super_create_portable(int32_t width, int32_t height, int32_t pel, svpf_super **out);
 void svpf_super_destroy(svpf_super *s);
@@ -60,7 +67,7 @@ size_t svpf_super_output_len(const svpf_super *s);   /* SuperBuilder::output_len
  * over nframes frames, host buffers in and out. */
 int svpf_super_build(const svpf_super *s, const uint8_t *src, uint8_t *dst, int32_t nframes);
 /* Same on device buffers: nframes source frames at `src_pitch`-strided planes
- * (src_y_stride / src_c_stride bytes per row; 0 = packed) -> nframes super frames. */
+ * (src_y_stride / src_c_stride samples per row; 0 = packed) -> nframes super frames. */
 int svpf_super_build_device(const svpf_super *s, const uint8_t *src_dev, int64_t src_y_stride,
                             int64_t src_c_stride, uint8_t *dst_dev, int32_t nframes, void *stream);
 
@@ -70,6 +77,11 @@ int svpf_super_build_device(const svpf_super *s, const uint8_t *src_dev, int64_t
  * src_height (> 0) override the frame size as analyse_filter.rs:96-101 does. */
 int svpf_analyser_create(int64_t sdata, const char *opt, size_t opt_len, int32_t src_width,
                          int32_t src_height, svpf_analyser **out);
+/* svpf_analyser_create over super frames of `bits` = 8 or 10 (uint16 samples; the 10-bit
+ * extension: chroma default 512 on clamped reads, payload luma byte = block mean >> 2, all
+ * else as for 8 bits). Batches and the server take 8-bit clips only. */
+int svpf_analyser_create_bits(int64_t sdata, const char *opt, size_t opt_len, int32_t src_width,
+                              int32_t src_height, int32_t bits, svpf_analyser **out);
 /* Analyser::new(super_builder, block w, block h, overlap mode, vectors)
  * (crates/svpflow1/src/portable.rs:189-229). */
 int svpf_analyser_create_portable(const svpf_super *s, int32_t block_w, int32_t block_h,

@@ -49,6 +49,15 @@ namespace SVPF_VARIANT {
 
 namespace {
 
+#ifdef SVPF_PX16
+typedef uint16_t px_t;             // this project's 10-bit extension (no reference behaviour)
+constexpr unsigned PX_MID = 512;   // chroma default of the clamped read paths
+constexpr unsigned DC_SHIFT = 2;   // the payload's block luma byte is mean >> 2
+#else
+typedef uint8_t px_t;
+constexpr unsigned PX_MID = 128;
+constexpr unsigned DC_SHIFT = 0;
+#endif
 constexpr int NT = SVPF_NT;        // threads per search direction
 static_assert(NT == 32 || NT == 64 || NT == 128, "threads per direction");
 constexpr int NW = NT / 32;
@@ -93,7 +102,7 @@ struct DirSh {
 };
 
 struct Planes {
-    const uint8_t *y, *u, *v;
+    const px_t *y, *u, *v;
 };
 
 struct Geo {  // per level
@@ -121,7 +130,7 @@ __device__ __forceinline__ int sat_i32(long long r) {
 }
 __device__ __forceinline__ bool is_blk(int n) { return n == 4 || n == 8 || n == 16 || n == 32; }
 // reads of a slice: an index past the end (or a wrapped, i.e. negative, one) is None
-__device__ __forceinline__ unsigned rd(const uint8_t *p, int64_t len, int64_t i, unsigned dflt) {
+__device__ __forceinline__ unsigned rd(const px_t *p, int64_t len, int64_t i, unsigned dflt) {
     return (i >= 0 && i < len) ? (unsigned)__ldg(p + i) : dflt;
 }
 __device__ __forceinline__ long long pen(int pnew, unsigned x) { return (long long)x + (((long long)pnew * (long long)x) >> 8); }
@@ -367,7 +376,7 @@ __device__ unsigned luma_tile(const Cand &c, const Planes &S, const Planes &R, c
 // One 4x4 tile of both chroma planes of a candidate.
 
 // One 4x4 tile of one chroma plane of a candidate on the general path.
-__device__ unsigned chroma_tile1(const Cand &c, const uint8_t *sp, const uint8_t *rp, const Geo &G, int cw, int tile) {
+__device__ unsigned chroma_tile1(const Cand &c, const px_t *sp, const px_t *rp, const Geo &G, int cw, int tile) {
     if (c.cmode == CM_NONE) return 0;
     const int txn = (cw + 3) >> 2;
     const int ty = tile / txn, tx = tile - ty * txn;
@@ -397,14 +406,14 @@ __device__ unsigned chroma_tile1(const Cand &c, const uint8_t *sp, const uint8_t
                 const long long sx = (long long)c.c_sx + c0 + q;
                 if (r < hh && q < ww && sy < clh && sx < clw) {
                     const int rx = iclamp(c.c_rx + c0 + q, 0, clw - 1);
-                    d[r * 4 + q] = (int)rd(sp, clen, ((int64_t)c.c_srow + sy) * cs + sx, 128) -
-                                   (int)rd(rp, clen, ((int64_t)c.c_rrow + ry) * cs + rx, 128);
+                    d[r * 4 + q] = (int)rd(sp, clen, ((int64_t)c.c_srow + sy) * cs + sx, PX_MID) -
+                                   (int)rd(rp, clen, ((int64_t)c.c_rrow + ry) * cs + rx, PX_MID);
                 }
             }
         }
     } else {  // CM_EDGE
         const int mh = imax(clh - 1, 0), mw = imax(clw - 1, 0);
-        const unsigned dflt = c.csatd ? 0u : 128u;
+        const unsigned dflt = c.csatd ? 0u : PX_MID;
 #pragma unroll
         for (int r = 0; r < 4; r++) {
             const int sy = iclamp(c.c_sy + r0 + r, 0, mh), ry = iclamp(c.c_ry + r0 + r, 0, mh);
@@ -426,44 +435,19 @@ __device__ unsigned chroma_tile1(const Cand &c, const uint8_t *sp, const uint8_t
 
 // -------------------------------------------------------------------------------------------
 // Fast path: candidates whose source and reference blocks lie inside their planes.
-// Bytes are read as 32-bit words from 4-byte aligned addresses and funnel-shifted; the
-// caller guarantees 8 readable bytes after the first byte of every row (see fast_setup).
-__device__ __forceinline__ uint32_t ld4u(const uint8_t *p) {
-    const uintptr_t a = (uintptr_t)p;
-    const uint32_t *q = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
-    return __funnelshift_r(__ldg(q), __ldg(q + 1), (unsigned)(a & 3) * 8u);
-}
-__device__ __forceinline__ unsigned tile_satd(const uint8_t *sp, const uint8_t *rp, int st) {
-    int d[16];
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-        const uint32_t a = ld4u(sp + r * st), b = ld4u(rp + r * st);
-#pragma unroll
-        for (int q = 0; q < 4; q++) d[r * 4 + q] = (int)((a >> (8 * q)) & 255u) - (int)((b >> (8 * q)) & 255u);
-    }
-    return hadamard4(d);
-}
-__device__ __forceinline__ unsigned tile_sad(const uint8_t *sp, const uint8_t *rp, int st) {
-    unsigned s = 0;
-#pragma unroll
-    for (int r = 0; r < 4; r++) s = __dp4a(__vabsdiffu4(ld4u(sp + r * st), ld4u(rp + r * st)), 0x01010101u, s);
-    return s;
-}
-// Packed-halfword forms over the staged source (see DirSh::srcp): a row's four byte
-// differences are two halfword pairs; the horizontal 4-point transform runs inside the
-// pairs, the vertical one across the rows, and the last vertical stage with its absolute
-// values is |a+b| + |a-b| = 2 max(|a|, |b|), as in hadamard4. Every intermediate fits a
-// signed halfword (|value| <= 2040) and the four-row sum an unsigned one (<= 8160).
-__device__ __forceinline__ uint32_t pairs_lo(uint32_t w) { return __byte_perm(w, 0u, 0x4140); }  // pixels 0, 1
-__device__ __forceinline__ uint32_t pairs_hi(uint32_t w) { return __byte_perm(w, 0u, 0x4342); }  // pixels 2, 3
-__device__ __forceinline__ unsigned tile_satd_p(const uint2 *sp, int spp, const uint8_t *rp, int st) {
+// Samples are read as 32-bit words from 4-byte aligned addresses and funnel-shifted; the
+// caller guarantees 8 readable samples after the first sample of every row (see fast_setup).
+//
+// SATD runs in packed halfwords: a row's four sample differences are two halfword pairs
+// (samples 0,1 and 2,3); the horizontal 4-point transform runs inside the pairs, the vertical
+// one across the rows, and the last vertical stage with its absolute values is
+// |a+b| + |a-b| = 2 max(|a|, |b|), as in hadamard4. Every intermediate fits a signed halfword
+// (|value| <= 8 * max sample) and the four-row sum an unsigned one.
+__device__ __forceinline__ unsigned satd_rows(const uint32_t d01[4], const uint32_t d23[4]) {
     uint32_t h0[4], h1[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
-        const uint2 a = sp[r * spp];
-        const uint32_t b = ld4u(rp + r * st);
-        const uint32_t d01 = __vsub2(a.x, pairs_lo(b)), d23 = __vsub2(a.y, pairs_hi(b));
-        const uint32_t c = __vadd2(d01, d23), e = __vsub2(d01, d23);
+        const uint32_t c = __vadd2(d01[r], d23[r]), e = __vsub2(d01[r], d23[r]);
         const uint32_t p = __byte_perm(c, e, 0x5410), q = __byte_perm(c, e, 0x7632);
         h0[r] = __vadd2(p, q);
         h1[r] = __vsub2(p, q);
@@ -479,20 +463,91 @@ __device__ __forceinline__ unsigned tile_satd_p(const uint2 *sp, int spp, const 
     }
     return 2u * ((acc & 0xFFFFu) + (acc >> 16));
 }
-__device__ __forceinline__ unsigned tile_sad_p(const uint2 *sp, int spp, const uint8_t *rp, int st) {
-    unsigned s = 0;
-#pragma unroll
-    for (int r = 0; r < 4; r++) s = __dp4a(__vabsdiffu4(sp[r * spp].x, ld4u(rp + r * st)), 0x01010101u, s);
-    return s;
+__device__ __forceinline__ uint32_t pairs_lo(uint32_t w) { return __byte_perm(w, 0u, 0x4140); }  // bytes 0, 1
+__device__ __forceinline__ uint32_t pairs_hi(uint32_t w) { return __byte_perm(w, 0u, 0x4342); }  // bytes 2, 3
+
+#ifndef SVPF_PX16
+__device__ __forceinline__ uint32_t ld4u(const uint8_t *p) {
+    const uintptr_t a = (uintptr_t)p;
+    const uint32_t *q = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+    return __funnelshift_r(__ldg(q), __ldg(q + 1), (unsigned)(a & 3) * 8u);
 }
-// The staged entry of 4 source pixels for a plane searched with SATD (pairs) or SAD (word).
-__device__ __forceinline__ uint2 stage4(uint32_t w, bool satd) {
+// four samples as halfword pairs
+__device__ __forceinline__ uint2 ld4p(const px_t *p) {
+    const uint32_t w = ld4u(p);
+    return make_uint2(pairs_lo(w), pairs_hi(w));
+}
+// The staged entry of 4 source samples for a plane searched with SATD (pairs) or SAD (word).
+__device__ __forceinline__ uint2 stage4(const px_t *p, bool satd) {
+    const uint32_t w = ld4u(p);
     return satd ? make_uint2(pairs_lo(w), pairs_hi(w)) : make_uint2(w, 0u);
 }
-__device__ __forceinline__ unsigned tile_sum(const uint8_t *sp, int st) {
+__device__ __forceinline__ unsigned sad4(uint2 staged, const px_t *rp) {
+    return __dp4a(__vabsdiffu4(staged.x, ld4u(rp)), 0x01010101u, 0u);
+}
+__device__ __forceinline__ unsigned sad4g(const px_t *sp, const px_t *rp) {
+    return __dp4a(__vabsdiffu4(ld4u(sp), ld4u(rp)), 0x01010101u, 0u);
+}
+__device__ __forceinline__ unsigned sum4(const px_t *p) { return __dp4a(ld4u(p), 0x01010101u, 0u); }
+#else
+// four 16-bit samples (2-byte aligned): three aligned words funnel-shifted into two pairs
+__device__ __forceinline__ uint2 ld4p(const px_t *p) {
+    const uintptr_t a = (uintptr_t)p;
+    const uint32_t *q = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+    const unsigned sh = (unsigned)(a & 3) * 8u;
+    const uint32_t w0 = __ldg(q), w1 = __ldg(q + 1), w2 = __ldg(q + 2);
+    return make_uint2(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh));
+}
+__device__ __forceinline__ uint2 stage4(const px_t *p, bool) { return ld4p(p); }
+__device__ __forceinline__ unsigned sad4(uint2 staged, const px_t *rp) {
+    const uint2 r = ld4p(rp);
+    return __vsadu2(staged.x, r.x) + __vsadu2(staged.y, r.y);
+}
+__device__ __forceinline__ unsigned sad4g(const px_t *sp, const px_t *rp) { return sad4(ld4p(sp), rp); }
+__device__ __forceinline__ unsigned sum4(const px_t *p) {
+    const uint2 w = ld4p(p);
+    return (w.x & 0xFFFFu) + (w.x >> 16) + (w.y & 0xFFFFu) + (w.y >> 16);
+}
+#endif
+
+// tiles with both blocks in global memory (special candidates)
+__device__ __forceinline__ unsigned tile_satd(const px_t *sp, const px_t *rp, int st) {
+    uint32_t d01[4], d23[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const uint2 a = ld4p(sp + r * st), b = ld4p(rp + r * st);
+        d01[r] = __vsub2(a.x, b.x);
+        d23[r] = __vsub2(a.y, b.y);
+    }
+    return satd_rows(d01, d23);
+}
+__device__ __forceinline__ unsigned tile_sad(const px_t *sp, const px_t *rp, int st) {
     unsigned s = 0;
 #pragma unroll
-    for (int r = 0; r < 4; r++) s = __dp4a(ld4u(sp + r * st), 0x01010101u, s);
+    for (int r = 0; r < 4; r++) s += sad4g(sp + r * st, rp + r * st);
+    return s;
+}
+// tiles over the staged source (see DirSh::srcp)
+__device__ __forceinline__ unsigned tile_satd_p(const uint2 *sp, int spp, const px_t *rp, int st) {
+    uint32_t d01[4], d23[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const uint2 a = sp[r * spp], b = ld4p(rp + r * st);
+        d01[r] = __vsub2(a.x, b.x);
+        d23[r] = __vsub2(a.y, b.y);
+    }
+    return satd_rows(d01, d23);
+}
+__device__ __forceinline__ unsigned tile_sad_p(const uint2 *sp, int spp, const px_t *rp, int st) {
+    unsigned s = 0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) s += sad4(sp[r * spp], rp + r * st);
+    return s;
+}
+__device__ __forceinline__ unsigned tile_sum(const px_t *sp, int st) {
+    unsigned s = 0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) s += sum4(sp + r * st);
     return s;
 }
 
@@ -703,7 +758,7 @@ __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, 
     r.lsatd = kind == 2 ? 0 : b.satd_mode;
     r.cmode = (chroma && b.cw >= 4 && b.ch >= 4) ? CM_DIRECT : CM_NONE;
     r.csatd = x.satd;
-    const uint8_t *sl = x.S.y + (kind == 2 ? b.dsrc : b.lsrc);
+    const px_t *sl = x.S.y + (kind == 2 ? b.dsrc : b.lsrc);
 #pragma unroll 1
     for (int t = sub; t < T; t += G) {
         if (t < TL) {
@@ -719,7 +774,7 @@ __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, 
             const int ty = ct >> b.lgctx, tx = ct & (b.ctilesx - 1);
             if (ty * 4 >= b.crows) continue;
             const int o = ty * 4 * cs + tx * 4;
-            const uint8_t *sp = (pl ? x.S.v : x.S.u) + b.csrc + o, *rp = (pl ? x.R.v : x.R.u) + cref + o;
+            const px_t *sp = (pl ? x.S.v : x.S.u) + b.csrc + o, *rp = (pl ? x.R.v : x.R.u) + cref + o;
             const unsigned v = r.csatd ? tile_satd(sp, rp, cs) : tile_sad(sp, rp, cs);
             if (pl) r.V += v; else r.U += v;
         }
@@ -806,12 +861,12 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                 r.csatd = x.satd;
                 const int T = x.tl + (r.cmode != CM_NONE ? 2 * x.tcp : 0);
                 const int ys = x.G.ys32, cs = x.G.cs32, nlw = b.tilesx * b.bh;
-                const uint8_t *rl = x.R.y + lref;
+                const px_t *rl = x.R.y + lref;
 #pragma unroll 1
                 for (int t = sub; t < T; t += G) {
                     if (t < x.tl) {
                         const int ty = t >> b.lgtx, tx = t & (b.tilesx - 1);
-                        const uint8_t *rp = rl + (ty * 4 * ys + tx * 4);
+                        const px_t *rp = rl + (ty * 4 * ys + tx * 4);
                         const uint2 *sp = s.srcp + ((ty * 4) << b.lgtx) + tx;
                         r.L += b.satd_mode ? tile_satd_p(sp, b.tilesx, rp, ys) : tile_sad_p(sp, b.tilesx, rp, ys);
                     } else {
@@ -820,7 +875,7 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                         const int ct = ct0 - pl * x.tcp;
                         const int ty = ct >> b.lgctx, tx = ct & (b.ctilesx - 1);
                         if (ty * 4 >= b.crows) continue;
-                        const uint8_t *rp = (pl ? x.R.v : x.R.u) + cref + (ty * 4 * cs + tx * 4);
+                        const px_t *rp = (pl ? x.R.v : x.R.u) + cref + (ty * 4 * cs + tx * 4);
                         const uint2 *sp = s.srcp + nlw + pl * b.ctilesx * b.crows + ((ty * 4) << b.lgctx) + tx;
                         const unsigned v = x.satd ? tile_satd_p(sp, b.ctilesx, rp, cs) : tile_sad_p(sp, b.ctilesx, rp, cs);
                         if (pl) r.V += v; else r.U += v;
@@ -892,7 +947,7 @@ __device__ __forceinline__ int adapt_lambda(int nlambda, int lsad, unsigned pred
 }
 
 // block_activity / plane_activity (:1486-1553): used only when search.coarse.distance < 0.
-__device__ __noinline__ unsigned plane_activity(const uint8_t *data, int64_t len, int64_t stride, int64_t row, int64_t x,
+__device__ __noinline__ unsigned plane_activity(const px_t *data, int64_t len, int64_t stride, int64_t row, int64_t x,
                                                 int w, int h, bool satd) {
     const unsigned area = (unsigned)(w * h);
     unsigned sum = 0;
@@ -996,14 +1051,14 @@ __device__ __forceinline__ void stage_source(const Ctx &x, DirSh &s, const BlkC 
         const int nlw = b.tilesx * b.bh;
         for (int t = x.tid; t < nlw; t += NT) {
             const int row = t >> b.lgtx, col = t & (b.tilesx - 1);
-            s.srcp[t] = stage4(ld4u(x.S.y + b.lsrc + row * x.G.ys32 + col * 4), b.satd_mode != 0);
+            s.srcp[t] = stage4(x.S.y + b.lsrc + row * x.G.ys32 + col * 4, b.satd_mode != 0);
         }
         if (b.chroma && b.cfast_src) {
             const int nc = b.ctilesx * b.crows;
             for (int t = x.tid; t < 2 * nc; t += NT) {
                 const int pl = t >= nc, u = t - pl * nc;
                 const int row = u >> b.lgctx, col = u & (b.ctilesx - 1);
-                s.srcp[nlw + t] = stage4(ld4u((pl ? x.S.v : x.S.u) + b.csrc + row * x.G.cs32 + col * 4), x.satd != 0);
+                s.srcp[nlw + t] = stage4((pl ? x.S.v : x.S.u) + b.csrc + row * x.G.cs32 + col * 4, x.satd != 0);
             }
         }
     }
@@ -1269,7 +1324,7 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
         const int rows = b.py >= 0 ? imax(0, imin(b.bh, L.lh - b.py)) : 0;
         const int cols = b.px >= 0 ? imax(0, imin(b.bw, L.lw - b.px)) : 0;
         const unsigned cnt = (unsigned)(rows * cols);
-        unsigned dc = cnt ? dcsum / cnt : 0;
+        unsigned dc = (cnt ? dcsum / cnt : 0) >> DC_SHIFT;
         if (dc > 255) dc = 255;
         const uint2 v = mkvec(bmx, bmy, smallest ? sat_mul(bsad, 3) : bsad);
         if (x.tid == 0) {
@@ -1381,7 +1436,7 @@ __device__ __forceinline__ void refine_pass(Ctx &x, DirSh &s, DirScratch &ds) {
             const int rows = b.py >= 0 ? imax(0, imin(b.bh, lh - b.py)) : 0;
             const int cols = b.px >= 0 ? imax(0, imin(b.bw, lw - b.px)) : 0;
             const unsigned cnt = (unsigned)(rows * cols);
-            unsigned dc = cnt ? dcsum / cnt : 0;
+            unsigned dc = (cnt ? dcsum / cnt : 0) >> DC_SHIFT;
             if (dc > 255) dc = 255;
             if (x.tid == 0) {
                 out[(int64_t)by * gw + bx] = mkvec(bmx, bmy, sat_mul(bsad, (unsigned)factor));
@@ -1520,8 +1575,8 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
     const int d = bidir ? half : ((P.vectors & 2) ? 0 : 1);  // 0 = forward (cur -> ref), 1 = backward
     const int tid = threadIdx.x % NT;
     DirSh &s = reinterpret_cast<DirSh *>(smem)[half];
-    const uint8_t *src = d == 0 ? pr.cur : pr.ref;
-    const uint8_t *ref = d == 0 ? pr.ref : pr.cur;
+    const px_t *src = (const px_t *)(d == 0 ? pr.cur : pr.ref);
+    const px_t *ref = (const px_t *)(d == 0 ? pr.ref : pr.cur);
     DirScratch ds;
     ds.vec[0] = (uint2 *)(scr + P.off_field[d]);
     ds.vec[1] = (uint2 *)(scr + P.off_next[d]);
@@ -1720,8 +1775,8 @@ __device__ __noinline__ void finish_pair(const AnalyseParams *Pp, const PairRef 
     ds.luma[0] = scr + P.off_out[d];
     ds.luma[1] = scr + P.off_out[d] + P.max_cells;
     if (P.has_refine) {
-        const uint8_t *src = d == 0 ? pr.cur : pr.ref;
-        const uint8_t *ref = d == 0 ? pr.ref : pr.cur;
+        const px_t *src = (const px_t *)(d == 0 ? pr.cur : pr.ref);
+        const px_t *ref = (const px_t *)(d == 0 ? pr.ref : pr.cur);
         Ctx x;
         x.P = &P;
         x.d = half;

@@ -229,6 +229,10 @@ int svpf_batch_create(int32_t nclips, const svpf_super *const *supers, const svp
             delete b;
             return bfail(SVPF_EINVAL, "clip " + std::to_string(i) + ": super frame configuration mismatch");
         }
+        if (super_layout_of(s)->px_bytes != 1 || analyser_layout(a)->px_bytes != 1) {
+            delete b;
+            return bfail(SVPF_EUNSUP, "clip " + std::to_string(i) + ": batches take 8-bit clips only");
+        }
         svpf_batch::Clip c;
         c.D = *super_dev_of(s);
         c.P = *analyser_params(a);

@@ -79,6 +79,7 @@ struct svpf_super {
 
 struct svpf_analyser {
     AnalyseOpts o;
+    int32_t bits = 8;
     AnalyseParams P;
     SuperLayout L;
     int32_t vdata[16];
@@ -111,6 +112,7 @@ int finish_analyser(svpf_analyser *a, svpf_analyser **out) {
     so.full = 1;
     so.width = a->o.width;
     so.height = a->o.height;
+    so.bits = a->bits;
     a->L = portable_layout(so);
     std::string err;
     if (!build_analyse_params(a->o, a->L, a->P, err)) {
@@ -197,6 +199,21 @@ int svpf_super_create(int32_t width, int32_t height, const char *opt, size_t opt
     return make_super(so, out);
 }
 
+int svpf_super_create_bits(int32_t width, int32_t height, const char *opt, size_t opt_len, int32_t bits,
+                           svpf_super **out) {
+    if (!out) return fail(SVPF_EINVAL, "null output handle");
+    if (bits != 8 && bits != 10) return fail(SVPF_EINVAL, "bits must be 8 or 10");
+    if (width <= 0 || height <= 0) return fail(SVPF_EINVAL, "SVSuper: Clip must be YV12");
+    OptTree tree;
+    std::string err;
+    const OptTree *t = nullptr;
+    if (opt && opt_len > 0 && parse_opt(opt, opt_len, tree, err)) t = &tree;
+    SuperOpts so;
+    if (!super_opts_from_opt(t, width, height, so, err)) return fail(SVPF_EINVAL, err);
+    so.bits = bits;
+    return make_super(so, out);
+}
+
 int svpf_super_create_portable(int32_t width, int32_t height, int32_t pel, svpf_super **out) {
     if (!out) return fail(SVPF_EINVAL, "null output handle");
     if (!(pel == 1 || pel == 2 || pel == 4)) return fail(SVPF_EINVAL, "pel must be 1, 2 or 4");
@@ -216,8 +233,9 @@ int32_t svpf_super_levels(const svpf_super *s) { return s->so.levels; }
 int32_t svpf_super_pel(const svpf_super *s) { return s->so.pel; }
 size_t svpf_super_source_len(const svpf_super *s) {
     size_t w = (size_t)s->so.width, h = (size_t)s->so.height;
-    return w * h + 2 * ((w / 2) * (h / 2));
+    return (w * h + 2 * ((w / 2) * (h / 2))) * (size_t)s->L.px_bytes;
 }
+int32_t svpf_super_bits(const svpf_super *s) { return s->so.bits; }
 size_t svpf_super_output_len(const svpf_super *s) { return (size_t)s->L.frame_bytes; }
 
 int svpf_super_build_device(const svpf_super *s, const uint8_t *src_dev, int64_t src_y_stride, int64_t src_c_stride,
@@ -281,6 +299,25 @@ int svpf_analyser_create_portable(const svpf_super *s, int32_t bw, int32_t bh, i
         delete a;
         return fail(SVPF_EINVAL, err);
     }
+    return finish_analyser(a, out);
+}
+
+int svpf_analyser_create_bits(int64_t sdata, const char *opt, size_t opt_len, int32_t src_width, int32_t src_height,
+                              int32_t bits, svpf_analyser **out) {
+    if (!out) return fail(SVPF_EINVAL, "null output handle");
+    if (bits != 8 && bits != 10) return fail(SVPF_EINVAL, "bits must be 8 or 10");
+    OptTree tree;
+    std::string err;
+    const OptTree *t = nullptr;
+    if (opt && opt_len > 0 && parse_opt(opt, opt_len, tree, err)) t = &tree;
+    auto *a = new svpf_analyser;
+    if (!analyse_opts_from_opt(t, sdata, nullptr, a->o, err)) {
+        delete a;
+        return fail(SVPF_EINVAL, err);
+    }
+    if (src_width > 0) a->o.width = src_width;
+    if (src_height > 0) a->o.height = src_height;
+    a->bits = bits;
     return finish_analyser(a, out);
 }
 

@@ -602,7 +602,8 @@ SuperLayout strided_layout(const SuperOpts &so, int64_t y_stride, int64_t c_stri
     L.c_stride = c_stride;
     L.y_len = L.y_stride * (int64_t)L.super_h;
     L.c_len = L.c_stride * (int64_t)(L.super_h / 2);
-    L.frame_bytes = L.y_len + 2 * L.c_len;
+    L.px_bytes = so.bits > 8 ? 2 : 1;
+    L.frame_bytes = (L.y_len + 2 * L.c_len) * L.px_bytes;
     return L;
 }
 

@@ -31,6 +31,7 @@ bool build_analyse_params(const AnalyseOpts &o, const SuperLayout &Lay, AnalyseP
     }
     P.y_stride = Lay.y_stride; P.c_stride = Lay.c_stride; P.y_len = Lay.y_len; P.c_len = Lay.c_len;
     P.frame_bytes = Lay.frame_bytes;
+    P.px_bytes = Lay.px_bytes;
     P.lambda = o.lambda;
     P.tiles_per_lane = 4;
     // per level

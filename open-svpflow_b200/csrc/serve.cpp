@@ -329,6 +329,8 @@ int svpf_server_submit(svpf_server *s, const svpf_super *sup, const svpf_analyse
     if (!s || !sup || !an || !frames || !payloads || nframes <= 0) return sfail(SVPF_EINVAL, "bad request");
     if (super_layout_of(sup)->frame_bytes != analyser_layout(an)->frame_bytes)
         return sfail(SVPF_EINVAL, "super frame configuration mismatch");
+    if (super_layout_of(sup)->px_bytes != 1 || analyser_layout(an)->px_bytes != 1)
+        return sfail(SVPF_EUNSUP, "the server takes 8-bit clips only");
     auto r = std::make_unique<Request>();
     r->arrival_ns = s->now_ns();
     r->D = *super_dev_of(sup);

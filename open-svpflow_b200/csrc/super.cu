@@ -10,6 +10,10 @@
 // byte independent and the kernels free of intra-launch dependencies.
 //
 // HBM-bound streaming work: a frame is read once per level and written once.
+//
+// The kernels are templates on the sample type: uint8_t is the reference's format; uint16_t
+// carries this project's 10-bit extension (samples 0..1023, the same arithmetic with the
+// clamps at 1023 instead of 255).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -19,7 +23,7 @@ namespace svpf {
 
 namespace {
 
-__device__ __forceinline__ uint8_t avg8(unsigned a, unsigned b) { return (uint8_t)((a + b + 1u) >> 1); }
+__device__ __forceinline__ unsigned avg8(unsigned a, unsigned b) { return (a + b + 1u) >> 1; }
 
 struct PlaneGeo {
     int w, h;            // level-0 plane size (chroma: luma/2)
@@ -45,8 +49,9 @@ __device__ __forceinline__ PlaneGeo plane_geo(const SuperDev &D, int plane) {
 
 // Level-0 plane with its row padding: the copy is edge-extended to the pitch
 // (super_build.rs:45-67).
+template <typename T>
 struct L0View {
-    const uint8_t *s;
+    const T *s;
     int64_t sst;
     int w, h;
     int64_t stride;
@@ -76,22 +81,25 @@ struct L0View {
 
 // half(), super_build.rs:162-177 (cubic8 at :138-160 computes the same value)
 template <typename Get>
-__device__ __forceinline__ unsigned half_tap(Get g, int p, int n) {
+__device__ __forceinline__ unsigned half_tap(Get g, int p, int n, int pmax) {
     if (p < 2 || p + 4 >= n) return p + 1 == n ? g(p) : avg8(g(p), g(p + 1));
     int v = (int)g(p - 2) + (int)g(p + 3) + 5 * (4 * (int)g(p) - (int)g(p - 1) + 4 * (int)g(p + 1) - (int)g(p + 2)) + 16;
     v >>= 5;
-    return (unsigned)(v < 0 ? 0 : (v > 255 ? 255 : v));
+    return (unsigned)(v < 0 ? 0 : (v > pmax ? pmax : v));
 }
 
-__global__ void __launch_bounds__(256) super_level0_kernel(SuperDev D, const uint8_t *__restrict__ src,
-                                                           uint8_t *__restrict__ dst) {
+template <typename T>
+__global__ void __launch_bounds__(256) super_level0_kernel(SuperDev D, const T *__restrict__ src,
+                                                           T *__restrict__ dst) {
     const int row = blockIdx.x, plane = blockIdx.y;
     const int64_t f = blockIdx.z;
     PlaneGeo g = plane_geo(D, plane);
     const int nsub = D.full ? D.pel * D.pel : 1;
     if (g.h <= 0 || row >= nsub * g.h || row >= g.rows) return;
-    L0View V{src + f * D.src_frame_bytes + g.src_off, g.src_stride, g.w, g.h, g.stride};
-    uint8_t *out = dst + f * D.frame_bytes + g.out_off + (int64_t)row * g.stride;
+    const int64_t src_frame = D.src_frame_bytes / (int64_t)sizeof(T), frame = D.frame_bytes / (int64_t)sizeof(T);
+    L0View<T> V{src + f * src_frame + g.src_off, g.src_stride, g.w, g.h, g.stride};
+    T *out = dst + f * frame + g.out_off + (int64_t)row * g.stride;
+    const int pmax = D.px_max;
     const int p = row / g.h, y = row % g.h;
     const bool subpel = D.pel >= 2 && D.gpu <= 1 && D.full && p >= 1 && p <= 3;
     for (int64_t x = threadIdx.x; x < g.stride; x += blockDim.x) {
@@ -107,12 +115,12 @@ __global__ void __launch_bounds__(256) super_level0_kernel(SuperDev D, const uin
             } else if (D.scale_up == 2) {  // fill_bicubic_pel2, super_build.rs:95-135
                 auto row_h = [&](int yy) { return [&, yy](int xx) { return V.L(yy, xx); }; };
                 auto colv = [&](int xx) { return [&, xx](int yy) { return V.L(yy, xx); }; };
-                if (p == 1) v = half_tap(row_h(y), xi, g.w);
-                else if (p == 2) v = half_tap(colv(xi), y, g.h);
-                else v = half_tap([&](int xx) { return half_tap(colv(xx), y, g.h); }, xi, g.w);
+                if (p == 1) v = half_tap(row_h(y), xi, g.w, pmax);
+                else if (p == 2) v = half_tap(colv(xi), y, g.h, pmax);
+                else v = half_tap([&](int xx) { return half_tap(colv(xx), y, g.h, pmax); }, xi, g.w, pmax);
             }
         }
-        out[x] = (uint8_t)v;
+        out[x] = (T)v;
     }
 }
 
@@ -121,8 +129,11 @@ __global__ void __launch_bounds__(256) super_level0_kernel(SuperDev D, const uin
 // Each output row receives src_w bytes: dst_w filtered values followed by the
 // vertical-only intermediates of the remaining columns (the reference copies the whole
 // intermediate row, :302-306), then zeros up to the pitch.
-__global__ void __launch_bounds__(256) super_reduce_kernel(SuperDev D, uint8_t *__restrict__ dst, int lv) {
-    extern __shared__ uint8_t inter[];
+template <typename T>
+__global__ void __launch_bounds__(256) super_reduce_kernel(SuperDev D, T *__restrict__ dst, int lv) {
+    extern __shared__ __align__(16) uint8_t inter_raw[];
+    T *inter = reinterpret_cast<T *>(inter_raw);
+    const unsigned pmax = (unsigned)D.px_max;
     const int dy = blockIdx.x, plane = blockIdx.y;
     const int64_t f = blockIdx.z;
     PlaneGeo g = plane_geo(D, plane);
@@ -133,8 +144,8 @@ __global__ void __launch_bounds__(256) super_reduce_kernel(SuperDev D, uint8_t *
     const int64_t src_row0 = c ? D.row_c[lv] : D.row_y[lv];
     const int64_t drow = (c ? D.row_c[lv + 1] : D.row_y[lv + 1]) + dy;
     if (drow >= g.rows) return;
-    uint8_t *base = dst + f * D.frame_bytes + g.out_off;
-    uint8_t *out = base + drow * g.stride;
+    T *base = dst + f * (D.frame_bytes / (int64_t)sizeof(T)) + g.out_off;
+    T *out = base + drow * g.stride;
     const int64_t plane_len = g.rows * g.stride;
     const bool active = D.scale_down == 4 && dst_w > 0 && src_w > 0 && src_h > 0;
     if (!active) {
@@ -157,9 +168,9 @@ __global__ void __launch_bounds__(256) super_reduce_kernel(SuperDev D, uint8_t *
             unsigned s = sample(st, x) + sample(st + 5, x) + 5u * (sample(st + 1, x) + sample(st + 4, x)) +
                          10u * (sample(st + 2, x) + sample(st + 3, x)) + 16u;
             v = s >> 5;
-            v = v < 255 ? v : 255;
+            v = v < pmax ? v : pmax;
         }
-        inter[x] = (uint8_t)v;
+        inter[x] = (T)v;
     }
     __syncthreads();
     auto get = [&](int i, unsigned dflt) -> unsigned { return i < src_w ? inter[i] : dflt; };
@@ -178,32 +189,43 @@ __global__ void __launch_bounds__(256) super_reduce_kernel(SuperDev D, uint8_t *
                 unsigned pk = get(2 * i + 3, inter[src_w - 1]);
                 unsigned s = left + pk + 10u * (get(2 * i, 0) + get(2 * i + 1, 0)) + 5u * (get(2 * i - 1, 0) + get(2 * i + 2, 0)) + 16u;
                 v = s >> 5;
-                v = v < 255 ? v : 255;
+                v = v < pmax ? v : pmax;
             }
         } else if (x < src_w) {
             v = inter[x];
         }
-        out[x] = (uint8_t)v;
+        out[x] = (T)v;
     }
 }
 
 }  // namespace
 
-cudaError_t launch_super(const SuperDev &D, const uint8_t *src, uint8_t *dst, int nframes, cudaStream_t stream,
-                         int *launches) {
-    if (nframes <= 0) return cudaSuccess;
+namespace {
+template <typename T>
+int launch_super_t(const SuperDev &D, const T *src, T *dst, int nframes, cudaStream_t stream) {
     const int nsub = D.full ? D.pel * D.pel : 1;
     dim3 g0((unsigned)(nsub * D.height), 3, (unsigned)nframes);
-    super_level0_kernel<<<g0, 256, 0, stream>>>(D, src, dst);
+    super_level0_kernel<T><<<g0, 256, 0, stream>>>(D, src, dst);
     int n = 1;
     for (int lv = 0; lv + 1 < D.levels; lv++) {
         int rows = D.lh[lv + 1];
         if (rows <= 0) continue;
-        size_t smem = (size_t)(D.lw[lv] > 0 ? D.lw[lv] : 1);
+        size_t smem = (size_t)(D.lw[lv] > 0 ? D.lw[lv] : 1) * sizeof(T);
         dim3 g((unsigned)rows, 3, (unsigned)nframes);
-        super_reduce_kernel<<<g, 256, smem, stream>>>(D, dst, lv);
+        super_reduce_kernel<T><<<g, 256, smem, stream>>>(D, dst, lv);
         n++;
     }
+    return n;
+}
+}  // namespace
+
+cudaError_t launch_super(const SuperDev &D, const uint8_t *src, uint8_t *dst, int nframes, cudaStream_t stream,
+                         int *launches) {
+    if (nframes <= 0) return cudaSuccess;
+    const int n = D.px_bytes == 2
+                      ? launch_super_t(D, reinterpret_cast<const uint16_t *>(src), reinterpret_cast<uint16_t *>(dst),
+                                       nframes, stream)
+                      : launch_super_t(D, src, dst, nframes, stream);
     if (launches) *launches += n;
     return cudaGetLastError();
 }
@@ -216,10 +238,12 @@ bool make_super_dev(const SuperOpts &so, const SuperLayout &L, int64_t src_y_str
     D.y_stride = L.y_stride; D.c_stride = L.c_stride;
     D.y_rows = L.super_h; D.c_rows = L.super_h / 2;
     D.y_len = L.y_len; D.c_len = L.c_len; D.frame_bytes = L.frame_bytes;
+    D.px_bytes = so.bits > 8 ? 2 : 1;
+    D.px_max = so.bits > 8 ? (1 << so.bits) - 1 : 255;
     D.src_y_stride = src_y_stride; D.src_c_stride = src_c_stride;
     D.src_y_len = src_y_stride * so.height;
     D.src_c_len = src_c_stride * (so.height / 2);
-    D.src_frame_bytes = D.src_y_len + 2 * D.src_c_len;
+    D.src_frame_bytes = (D.src_y_len + 2 * D.src_c_len) * D.px_bytes;
     int64_t ry = 0, rc = 0;
     for (int lv = 0; lv < kMaxLevels; lv++) {
         D.lw[lv] = reduce_dim(so.width, lv);

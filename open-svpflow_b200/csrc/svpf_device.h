@@ -10,8 +10,11 @@ namespace svpf {
 // Everything the Super kernels need about one (options, layout, source pitch) triple.
 struct SuperDev {
     int32_t width, height, pel, levels, full, gpu, scale_up, scale_down;
-    int64_t y_stride, c_stride, y_rows, c_rows, y_len, c_len, frame_bytes;
-    int64_t src_y_stride, src_c_stride, src_y_len, src_c_len, src_frame_bytes;
+    int32_t px_bytes, px_max;                 // sample size (1, 2) and largest sample (255, 1023)
+    int64_t y_stride, c_stride, y_rows, c_rows, y_len, c_len;   // in samples
+    int64_t frame_bytes;                      // bytes between super frames
+    int64_t src_y_stride, src_c_stride, src_y_len, src_c_len;   // in samples
+    int64_t src_frame_bytes;                  // bytes between source frames
     int32_t lw[kMaxLevels], lh[kMaxLevels];   // reduce_dim(luma_w/h, level)
     int64_t row_y[kMaxLevels], row_c[kMaxLevels];  // first row of each level in Y / chroma
 };
@@ -62,6 +65,7 @@ SVPF_DECLARE_ANALYSE_VARIANT(nt64)
 SVPF_DECLARE_ANALYSE_VARIANT(nt32)
 SVPF_DECLARE_ANALYSE_VARIANT(nt128b3)
 SVPF_DECLARE_ANALYSE_VARIANT(nt64b6)
+SVPF_DECLARE_ANALYSE_VARIANT(nt128p16)  // uint16 samples (AnalyseParams::px_bytes == 2)
 
 
 // A compiled launch shape of the Analyse kernels: threads per search direction and the

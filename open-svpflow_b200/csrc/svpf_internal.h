@@ -18,6 +18,7 @@ struct SuperOpts {
     int32_t pel = 2, gpu = 1, scale_down = 4, scale_up = 0;
     int32_t full = 1, rc = 0;
     int32_t levels = 0, width = 0, height = 0;
+    int32_t bits = 8;  // sample depth: 8 (the reference) or 10 (this project's extension, uint16 samples)
 };
 
 struct AnalyseOpts {
@@ -37,8 +38,10 @@ struct AnalyseOpts {
 // crates/svpflow1/src/portable.rs:104-106 is y_stride = width, c_stride = width/2.
 struct SuperLayout {
     int32_t width, height, pel, levels, full, super_h;
-    int64_t y_stride, c_stride;
-    int64_t y_len, c_len, frame_bytes;  // plane byte counts; y + u + v
+    int64_t y_stride, c_stride;         // in samples
+    int64_t y_len, c_len;               // plane sizes in samples
+    int64_t frame_bytes;                // (y + u + v) * px_bytes
+    int32_t px_bytes;                   // 1 (8-bit) or 2 (uint16 samples)
 };
 
 // ---- options (opts.cpp) ----
@@ -102,6 +105,7 @@ struct alignas(16) AnalyseParams {
     LevelInfo rlv[2];         // refine pass block shapes: output block, half of it (border blocks)
     int32_t rescale_denom;
     int32_t tiles_per_lane;   // 4x4 tiles one lane evaluates per candidate (2, 4 or 8): a launch tuning knob
+    int32_t px_bytes;         // 1: 8-bit samples; 2: uint16 samples (the 10-bit extension)
     int64_t payload_len;
     int32_t header[16];       // payload words 0x00..0x3C
     // per-pair scratch layout (bytes)

@@ -21,8 +21,10 @@ const AnalyseVariant &analyse_variant(int i) {
 
 // More pairs than two per SM: the 80-register shape keeps three pairs per SM resident (the
 // fastest for full launches); otherwise the 128-register shape, which is faster per pair.
+// uint16 samples have one compiled shape.
 cudaError_t launch_analyse(const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,
                            uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches) {
+    if (P.px_bytes == 2) return nt128p16::launch_plain(P, src, npairs, payloads, scratch, status_dev, stream, launches);
     static int sms = [] {
         int dev = 0, n = 0;
         if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -36,6 +38,7 @@ cudaError_t launch_analyse(const AnalyseParams &P, const PairSrc &src, int npair
 
 cudaError_t launch_analyse_shape(int variant, const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,
                                  uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches) {
+    if (P.px_bytes == 2) return nt128p16::launch_plain(P, src, npairs, payloads, scratch, status_dev, stream, launches);
     return analyse_variant(variant).launch_plain(P, src, npairs, payloads, scratch, status_dev, stream, launches);
 }
 

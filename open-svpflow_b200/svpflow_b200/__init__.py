@@ -51,6 +51,9 @@ def lib() -> ctypes.CDLL:
             "svpf_reference_version": (I64, []),
             "svpf_super_create": (I32, [I32, I32, ctypes.c_char_p, SZ, P(_VP)]),
             "svpf_super_create_portable": (I32, [I32, I32, I32, P(_VP)]),
+            "svpf_super_create_bits": (I32, [I32, I32, ctypes.c_char_p, SZ, I32, P(_VP)]),
+            "svpf_super_bits": (I32, [_VP]),
+            "svpf_analyser_create_bits": (I32, [I64, ctypes.c_char_p, SZ, I32, I32, I32, P(_VP)]),
             "svpf_super_destroy": (None, [_VP]),
             "svpf_super_sdata": (I64, [_VP]),
             "svpf_super_height": (I32, [_VP]),
@@ -116,9 +119,16 @@ def _check(rc: int):
 
 
 def _buf(a) -> np.ndarray:
+    """Bytes of a buffer: uint8 data as is, uint16 samples (the 10-bit extension) viewed as bytes."""
     if isinstance(a, (bytes, bytearray, memoryview)):
         return np.frombuffer(a, dtype=np.uint8)
+    if isinstance(a, np.ndarray) and a.dtype == np.uint16:
+        return np.ascontiguousarray(a).reshape(-1).view(np.uint8)
     return np.ascontiguousarray(a, dtype=np.uint8)
+
+
+def _sample_type(bits: int):
+    return np.uint16 if bits > 8 else np.uint8
 
 
 class SuperFrame:
@@ -172,25 +182,40 @@ class SuperBuilder:
     def super_height(self) -> int:
         return lib().svpf_super_height(self._h)
 
+    @property
+    def bits(self) -> int:
+        """Sample depth: 8 (the reference's), or 10 (uint16 samples; this project's extension)."""
+        return lib().svpf_super_bits(self._h)
+
+    @property
+    def sample_type(self):
+        return _sample_type(self.bits)
+
     def source_len(self) -> int:
+        """Bytes of one packed I420 source frame."""
         return lib().svpf_super_source_len(self._h)
 
     def output_len(self) -> int:
+        """Bytes of one super frame."""
         return lib().svpf_super_output_len(self._h)
 
     def build(self, source) -> SuperFrame:
         """SuperBuilder::build: one packed I420 frame -> its super frame."""
-        src = _buf(source)
-        if src.size != self.source_len():
+        dt = self.sample_type
+        src = np.ascontiguousarray(source, dtype=dt) if dt is np.uint16 else _buf(source)
+        if src.nbytes != self.source_len():
             raise ValueError("invalid source buffer length")
-        out = np.empty(self.output_len(), dtype=np.uint8)
+        out = np.empty(self.output_len() // np.dtype(dt).itemsize, dtype=dt)
         _check(lib().svpf_super_build(self._h, src.ctypes.data, out.ctypes.data, 1))
         return SuperFrame(self, out)
 
     def build_many(self, frames: np.ndarray) -> np.ndarray:
-        frames = np.ascontiguousarray(frames, dtype=np.uint8)
+        dt = self.sample_type
+        frames = np.ascontiguousarray(frames, dtype=dt)
         n = frames.shape[0]
-        out = np.empty((n, self.output_len()), dtype=np.uint8)
+        if frames.nbytes != n * self.source_len():
+            raise ValueError("invalid source buffer length")
+        out = np.empty((n, self.output_len() // np.dtype(dt).itemsize), dtype=dt)
         _check(lib().svpf_super_build(self._h, frames.ctypes.data, out.ctypes.data, n))
         return out
 
@@ -200,11 +225,15 @@ class SuperBuilder:
         _check(lib().svpf_super_build_device(self._h, src_ptr, src_y_stride, src_c_stride, dst_ptr, nframes, stream))
 
 
-def Super(width: int, height: int, opt: Optional[str] = None) -> SuperBuilder:
-    """The `svp1.Super(clip, opt)` filter's configuration for a clip of this size."""
+def Super(width: int, height: int, opt: Optional[str] = None, bits: int = 8) -> SuperBuilder:
+    """The `svp1.Super(clip, opt)` filter's configuration for a clip of this size. bits=10 is this
+    project's 10-bit extension (uint16 samples); the reference is 8-bit only."""
     h = _VP()
     b = opt.encode() if opt is not None else None
-    _check(lib().svpf_super_create(width, height, b, len(b) if b else 0, ctypes.byref(h)))
+    if bits == 8:
+        _check(lib().svpf_super_create(width, height, b, len(b) if b else 0, ctypes.byref(h)))
+    else:
+        _check(lib().svpf_super_create_bits(width, height, b, len(b) if b else 0, bits, ctypes.byref(h)))
     return SuperBuilder(0, 0, _handle=h)
 
 
@@ -213,7 +242,8 @@ class Analyser:
     Analyse(...) for the filter form."""
 
     def __init__(self, super_builder: Optional[SuperBuilder] = None, block_width: int = 16, block_height: int = 16,
-                 overlap_mode: int = 2, vectors: int = 3, *, _handle=None):
+                 overlap_mode: int = 2, vectors: int = 3, *, _handle=None, _bits: int = 8):
+        self.bits = super_builder.bits if super_builder is not None and _handle is None else _bits
         h = _VP()
         if _handle is None:
             _check(lib().svpf_analyser_create_portable(super_builder.handle, block_width, block_height, overlap_mode,
@@ -257,8 +287,10 @@ class Analyser:
     def analyse_clip(self, super_builder: SuperBuilder, frames: np.ndarray, first: int = 0,
                      count: Optional[int] = None) -> np.ndarray:
         """Super + Analyse over a clip of packed I420 frames (host buffers) -> payload rows."""
-        frames = np.ascontiguousarray(frames, dtype=np.uint8)
+        frames = np.ascontiguousarray(frames, dtype=_sample_type(self.bits))
         n = frames.shape[0]
+        if frames.nbytes != n * super_builder.source_len():
+            raise ValueError("invalid source buffer length")
         count = n - first if count is None else count
         out = np.empty((count, self.payload_len()), dtype=np.uint8)
         _check(lib().svpf_clip_analyse(self._h, super_builder.handle, frames.ctypes.data, n, first, count,
@@ -283,13 +315,16 @@ class Analyser:
         _check(lib().svpf_device_status(scratch_ptr, stream))
 
 
-def Analyse(sdata: int, opt: Optional[str] = None, width: int = 0, height: int = 0) -> Analyser:
+def Analyse(sdata: int, opt: Optional[str] = None, width: int = 0, height: int = 0, bits: int = 8) -> Analyser:
     """The `svp1.Analyse(clip, sdata, src, opt)` filter's configuration; width/height are the
-    src clip's size (analyse_filter.rs:96-101)."""
+    src clip's size (analyse_filter.rs:96-101). bits=10: super frames of uint16 samples."""
     h = _VP()
     b = opt.encode() if opt is not None else None
-    _check(lib().svpf_analyser_create(sdata, b, len(b) if b else 0, width, height, ctypes.byref(h)))
-    return Analyser(_handle=h)
+    if bits == 8:
+        _check(lib().svpf_analyser_create(sdata, b, len(b) if b else 0, width, height, ctypes.byref(h)))
+    else:
+        _check(lib().svpf_analyser_create_bits(sdata, b, len(b) if b else 0, width, height, bits, ctypes.byref(h)))
+    return Analyser(_handle=h, _bits=bits)
 
 
 def kernel_launches() -> int:

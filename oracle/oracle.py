@@ -381,51 +381,70 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
+LIB16_PATH = os.path.join(HERE, "_build", "libsvpf_oracle16.so")
+_lib16 = None
+
+
+def lib16():
+    """The same restatement built for uint16 samples (this project's 10-bit extension: values
+    0..1023, chroma default 512, block luma byte = mean >> 2; no reference behaviour)."""
+    global _lib16
+    if _lib16 is None:
+        if not os.path.exists(LIB16_PATH):
+            build()
+        _lib16 = _setup(ctypes.CDLL(LIB16_PATH))
+    return _lib16
+
+
 def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             build()
-        L = ctypes.CDLL(LIB_PATH)
-        P = ctypes.POINTER
-        L.or_super_opts_from_opt.argtypes = [P(OrVal), ctypes.c_int32, ctypes.c_int32, P(SuperOpts), ctypes.c_char_p, ctypes.c_size_t]
-        L.or_super_pack_data.restype = ctypes.c_int64
-        L.or_super_pack_data.argtypes = [P(SuperOpts)]
-        L.or_super_height.argtypes = [P(SuperOpts)]
-        L.or_super_output_len.restype = ctypes.c_size_t
-        L.or_super_output_len.argtypes = [P(SuperOpts)]
-        L.or_analyse_opts_from_opt.argtypes = [P(OrVal), ctypes.c_int64, P(SuperOpts), P(AnalyseOpts), ctypes.c_char_p, ctypes.c_size_t]
-        L.or_analyser_portable.argtypes = [P(SuperOpts), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
-                                           P(AnalyseOpts), ctypes.c_char_p, ctypes.c_size_t]
-        L.or_build_super_portable.argtypes = [P(SuperOpts), ctypes.c_void_p, ctypes.c_void_p]
-        L.or_build_super_many.argtypes = [P(SuperOpts), P(ctypes.c_void_p), P(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int32]
-        L.or_build_plane.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
-                                     ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
-                                     ctypes.c_int32, P(SuperOpts)]
-        L.or_payload_len.restype = ctypes.c_size_t
-        L.or_payload_len.argtypes = [P(AnalyseOpts)]
-        L.or_analyse_portable.argtypes = [P(AnalyseOpts), P(SuperOpts), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
-        L.or_analyse_clip.argtypes = [P(AnalyseOpts), P(SuperOpts), P(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int32,
-                                      ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]
-        L.or_analyse_pair.argtypes = [P(Planes), P(Planes), P(AnalyseOpts), ctypes.c_void_p, ctypes.c_void_p]
-        L.or_pack_vdata_header.argtypes = [P(AnalyseOpts), P(ctypes.c_int32)]
-        L.or_hadamard4_satd.restype = ctypes.c_uint32
-        L.or_vector_grid.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
-        L.or_vector_planes.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32,
-                                       ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
-        L.or_hadamard4_satd.argtypes = [P(ctypes.c_int32)]
-        L.or_adapt_lambda.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
-        L.or_exact_lambda.argtypes = [P(AnalyseOpts), ctypes.c_int32, ctypes.c_int32]
-        L.or_rescale_scores.argtypes = [P(Vec8), ctypes.c_size_t, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
-        L.or_global_doubled.argtypes = [P(Vec8), ctypes.c_size_t, P(ctypes.c_int32), P(ctypes.c_int32)]
-        L.or_block_cost_lc.argtypes = [P(Planes), P(Planes)] + [ctypes.c_int32] * 9 + [P(ctypes.c_uint32), P(ctypes.c_uint32)]
-        L.or_last_counters.argtypes = [P(ctypes.c_uint64)]
-        for f in ("or_reduce_dim", "or_auto_levels", "or_super_plane_height", "or_auto_search_levels"):
-            getattr(L, f).argtypes = [ctypes.c_int32] * {"or_reduce_dim": 2, "or_auto_levels": 2,
-                                                           "or_super_plane_height": 4, "or_auto_search_levels": 6}[f]
-        L.or_level_grid.argtypes = [P(AnalyseOpts), ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32)]
-        _lib = L
+        _lib = _setup(ctypes.CDLL(LIB_PATH))
     return _lib
+
+
+def _setup(L):
+    """Argument and result types of the restatement's exports."""
+    P = ctypes.POINTER
+    L.or_super_opts_from_opt.argtypes = [P(OrVal), ctypes.c_int32, ctypes.c_int32, P(SuperOpts), ctypes.c_char_p, ctypes.c_size_t]
+    L.or_super_pack_data.restype = ctypes.c_int64
+    L.or_super_pack_data.argtypes = [P(SuperOpts)]
+    L.or_super_height.argtypes = [P(SuperOpts)]
+    L.or_super_output_len.restype = ctypes.c_size_t
+    L.or_super_output_len.argtypes = [P(SuperOpts)]
+    L.or_analyse_opts_from_opt.argtypes = [P(OrVal), ctypes.c_int64, P(SuperOpts), P(AnalyseOpts), ctypes.c_char_p, ctypes.c_size_t]
+    L.or_analyser_portable.argtypes = [P(SuperOpts), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                       P(AnalyseOpts), ctypes.c_char_p, ctypes.c_size_t]
+    L.or_build_super_portable.argtypes = [P(SuperOpts), ctypes.c_void_p, ctypes.c_void_p]
+    L.or_build_super_many.argtypes = [P(SuperOpts), P(ctypes.c_void_p), P(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int32]
+    L.or_build_plane.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                                 ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
+                                 ctypes.c_int32, P(SuperOpts)]
+    L.or_payload_len.restype = ctypes.c_size_t
+    L.or_payload_len.argtypes = [P(AnalyseOpts)]
+    L.or_analyse_portable.argtypes = [P(AnalyseOpts), P(SuperOpts), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.or_analyse_clip.argtypes = [P(AnalyseOpts), P(SuperOpts), P(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int32,
+                                  ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]
+    L.or_analyse_pair.argtypes = [P(Planes), P(Planes), P(AnalyseOpts), ctypes.c_void_p, ctypes.c_void_p]
+    L.or_pack_vdata_header.argtypes = [P(AnalyseOpts), P(ctypes.c_int32)]
+    L.or_hadamard4_satd.restype = ctypes.c_uint32
+    L.or_vector_grid.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.or_vector_planes.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32,
+                                   ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
+    L.or_hadamard4_satd.argtypes = [P(ctypes.c_int32)]
+    L.or_adapt_lambda.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
+    L.or_exact_lambda.argtypes = [P(AnalyseOpts), ctypes.c_int32, ctypes.c_int32]
+    L.or_rescale_scores.argtypes = [P(Vec8), ctypes.c_size_t, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+    L.or_global_doubled.argtypes = [P(Vec8), ctypes.c_size_t, P(ctypes.c_int32), P(ctypes.c_int32)]
+    L.or_block_cost_lc.argtypes = [P(Planes), P(Planes)] + [ctypes.c_int32] * 9 + [P(ctypes.c_uint32), P(ctypes.c_uint32)]
+    L.or_last_counters.argtypes = [P(ctypes.c_uint64)]
+    for f in ("or_reduce_dim", "or_auto_levels", "or_super_plane_height", "or_auto_search_levels"):
+        getattr(L, f).argtypes = [ctypes.c_int32] * {"or_reduce_dim": 2, "or_auto_levels": 2,
+                                                       "or_super_plane_height": 4, "or_auto_search_levels": 6}[f]
+    L.or_level_grid.argtypes = [P(AnalyseOpts), ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32)]
+    return L
 
 
 def _err():
@@ -644,3 +663,33 @@ def vector_planes(vdata, payload: np.ndarray, frame_w: int, frame_h: int, raw: b
     v = (ctypes.c_int32 * 16)(*vdata)
     rc = lib().or_vector_planes(v, _ptr(payload), payload.size, frame_w, frame_h, int(raw), out.ctypes.data)
     return None if rc else out.reshape(4, mh, mw)
+
+
+# ---- 10-bit extension (uint16 samples), same options as the 8-bit path
+def build_super16(so: SuperOpts, src: np.ndarray) -> np.ndarray:
+    src = np.ascontiguousarray(src, dtype=np.uint16)
+    out = np.zeros(super_output_len(so), dtype=np.uint16)
+    lib16().or_build_super_portable(ctypes.byref(so), _ptr(src), _ptr(out))
+    return out
+
+
+def build_super_many16(so: SuperOpts, frames: np.ndarray, threads: int = 1) -> np.ndarray:
+    frames = np.ascontiguousarray(frames, dtype=np.uint16)
+    n = frames.shape[0]
+    out = np.zeros((n, super_output_len(so)), dtype=np.uint16)
+    srcp = (ctypes.c_void_p * n)(*[frames[i].ctypes.data for i in range(n)])
+    dstp = (ctypes.c_void_p * n)(*[out[i].ctypes.data for i in range(n)])
+    lib16().or_build_super_many(ctypes.byref(so), srcp, dstp, n, threads)
+    return out
+
+
+def analyse_clip16(ao: AnalyseOpts, so: SuperOpts, supers: np.ndarray, first: int, count: int,
+                   threads: int = 1) -> np.ndarray:
+    supers = np.ascontiguousarray(supers, dtype=np.uint16)
+    n = supers.shape[0]
+    out = np.zeros((count, payload_len(ao)), dtype=np.uint8)
+    ptrs = (ctypes.c_void_p * n)(*[supers[i].ctypes.data for i in range(n)])
+    rc = lib16().or_analyse_clip(ctypes.byref(ao), ctypes.byref(so), ptrs, n, first, count, _ptr(out), threads)
+    if rc:
+        raise RuntimeError("the search indexes out of range on this input (the reference's panic)")
+    return out

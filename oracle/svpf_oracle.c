@@ -37,6 +37,16 @@ typedef uint32_t u32;
 typedef uint64_t u64;
 typedef uint8_t u8;
 typedef uint64_t usize;
+typedef or_px px; /* a sample */
+#ifdef OR_PX16
+#define PX_MAX 1023
+#define PX_MID 512
+#define DC_SHIFT 2
+#else
+#define PX_MAX 255
+#define PX_MID 128
+#define DC_SHIFT 0
+#endif
 
 /* ------------------------------------------------------------------ helpers */
 static inline u32 sat_add_u32(u32 a, u32 b) { u32 r = a + b; return r < a ? UINT32_MAX : r; }
@@ -68,8 +78,8 @@ static inline i32 f64_as_i32(double x) { /* Rust `as i32` */
 }
 static inline i32 i64_as_i32(i64 v) { return (i32)(u32)(u64)v; }
 static inline usize i32_as_usize(i32 v) { return (usize)(i64)v; }
-static inline u8 avg_u8(u8 a, u8 b) { return (u8)(((unsigned)a + b + 1u) >> 1); } /* super_build.rs:250 */
-static inline u8 read_or(const u8 *d, usize len, usize i, u8 dflt) { return i < len ? d[i] : dflt; }
+static inline px avg_u8(px a, px b) { return (px)(((unsigned)a + b + 1u) >> 1); } /* super_build.rs:250 */
+static inline px read_or(const px *d, usize len, usize i, px dflt) { return i < len ? d[i] : dflt; }
 static inline i32 iabs(i32 v) { return v < 0 ? -v : v; }
 static inline int is_blk(usize n) { return n == 4 || n == 8 || n == 16 || n == 32; }
 
@@ -201,52 +211,52 @@ static void level_size_b(usize lv, usize luma_w, usize luma_h, int chroma, usize
     usize yh = (usize)or_reduce_dim((i32)luma_h, (i32)lv);
     if (chroma) { *w = yw / 2; *h = yh / 2; } else { *w = yw; *h = yh; }
 }
-static inline u8 sample(const u8 *buf, usize len, usize stride, usize row0, usize y, usize x) {
+static inline px sample(const px *buf, usize len, usize stride, usize row0, usize y, usize x) {
     return read_or(buf, len, (row0 + y) * stride + x, 0); /* super_build.rs:359-361 */
 }
 
 /* horizontal_6tap_inplace, super_build.rs:310-357 */
-static void horizontal_6tap_inplace(u8 *row, usize row_len, usize dst_w, u8 *scratch) {
+static void horizontal_6tap_inplace(px *row, usize row_len, usize dst_w, px *scratch) {
     if (dst_w == 0 || row_len == 0) return;
     if (dst_w <= 2) {
         for (usize i = 0; i < dst_w; i++) {
-            u8 a = read_or(row, row_len, 2 * i, 0);
-            u8 b = read_or(row, row_len, 2 * i + 1, a);
+            px a = read_or(row, row_len, 2 * i, 0);
+            px b = read_or(row, row_len, 2 * i + 1, a);
             row[i] = avg_u8(a, b);
         }
         return;
     }
-    u8 *src = scratch;
-    memcpy(src, row, row_len);
+    px *src = scratch;
+    memcpy(src, row, row_len * sizeof(px));
     usize src_w = row_len;
     row[0] = avg_u8(src[0], read_or(src, src_w, 1, src[0]));
-    u8 left = row[0];
+    px left = row[0];
     usize interior = sat_sub_us(dst_w, 2);
     for (usize i = 0; i < interior; i++) {
         usize k = 5 + 2 * i;
-        u8 p_k = k < src_w ? src[k] : src[src_w - 1];
-        u8 p_km3 = read_or(src, src_w, k - 3, 0);
-        u8 p_km2 = read_or(src, src_w, k - 2, 0);
-        u8 p_km4 = read_or(src, src_w, k - 4, 0);
-        u8 p_even = read_or(src, src_w, (k - 1) & ~(usize)1, 0);
+        px p_k = k < src_w ? src[k] : src[src_w - 1];
+        px p_km3 = read_or(src, src_w, k - 3, 0);
+        px p_km2 = read_or(src, src_w, k - 2, 0);
+        px p_km4 = read_or(src, src_w, k - 4, 0);
+        px p_even = read_or(src, src_w, (k - 1) & ~(usize)1, 0);
         u32 v = ((u32)left + p_k + 10u * ((u32)p_km3 + p_km2) + 5u * ((u32)p_km4 + p_even) + 16u) >> 5;
-        row[i + 1] = (u8)(v < 255 ? v : 255);
+        row[i + 1] = (px)(v < PX_MAX ? v : PX_MAX);
         left = p_km3;
     }
     usize i = dst_w - 1 > 1 ? dst_w - 1 : 1;
     for (; i < dst_w; i++) {
-        u8 a = read_or(src, src_w, 2 * i, 0);
-        u8 b = read_or(src, src_w, 2 * i + 1, a);
+        px a = read_or(src, src_w, 2 * i, 0);
+        px b = read_or(src, src_w, 2 * i + 1, a);
         row[i] = avg_u8(a, b);
     }
 }
 
 /* reduce_6tap, super_build.rs:254-308 */
-static void reduce_6tap(u8 *buf, usize len, usize stride, usize dst_row0, usize dst_w, usize dst_h,
+static void reduce_6tap(px *buf, usize len, usize stride, usize dst_row0, usize dst_w, usize dst_h,
                         usize src_row0, usize src_w, usize src_h) {
     if (dst_w == 0 || dst_h == 0 || src_w == 0 || src_h == 0) return;
     usize inter_w = src_w;
-    u8 *inter = calloc(inter_w * dst_h, 1);
+    px *inter = calloc(inter_w * dst_h, sizeof(px));
     for (usize dy = 0; dy < dst_h; dy++) {
         usize sy = dy * 2;
         i64 win0 = (i64)sy - 2;
@@ -255,8 +265,8 @@ static void reduce_6tap(u8 *buf, usize len, usize stride, usize dst_row0, usize 
             usize y0 = umin(sy, sat_sub_us(src_h, 1));
             usize y1 = umin(sy + 1, sat_sub_us(src_h, 1));
             for (usize x = 0; x < inter_w; x++) {
-                u8 a = sample(buf, len, stride, src_row0, y0, x);
-                u8 b = sample(buf, len, stride, src_row0, y1, x);
+                px a = sample(buf, len, stride, src_row0, y0, x);
+                px b = sample(buf, len, stride, src_row0, y1, x);
                 inter[dy * inter_w + x] = avg_u8(a, b);
             }
         } else {
@@ -269,70 +279,70 @@ static void reduce_6tap(u8 *buf, usize len, usize stride, usize dst_row0, usize 
                 u32 p4 = sample(buf, len, stride, src_row0, st + 4, x);
                 u32 p5 = sample(buf, len, stride, src_row0, st + 5, x);
                 u32 v = (p0 + p5 + 5 * (p1 + p4) + 10 * (p2 + p3) + 16) >> 5;
-                inter[dy * inter_w + x] = (u8)(v < 255 ? v : 255);
+                inter[dy * inter_w + x] = (px)(v < PX_MAX ? v : PX_MAX);
             }
         }
     }
-    u8 *scratch = calloc(inter_w, 1);
+    px *scratch = calloc(inter_w, sizeof(px));
     for (usize dy = 0; dy < dst_h; dy++) {
-        u8 *row = inter + dy * inter_w;
+        px *row = inter + dy * inter_w;
         horizontal_6tap_inplace(row, inter_w, dst_w, scratch);
         usize dst_base = (dst_row0 + dy) * stride;
         usize n = umin(inter_w, sat_sub_us(len, dst_base));
-        if (n > 0) memcpy(buf + dst_base, row, n);
+        if (n > 0) memcpy(buf + dst_base, row, n * sizeof(px));
     }
     free(scratch);
     free(inter);
 }
 
 /* fill_bilinear_pel2, super_build.rs:179-224 (in-place, sequential semantics) */
-static void fill_bilinear_pel2(u8 *dst, usize len, usize stride, usize row0, usize w, usize h) {
+static void fill_bilinear_pel2(px *dst, usize len, usize stride, usize row0, usize w, usize h) {
     usize full = row0, hp = row0 + h, vp = row0 + 2 * h, hvp = row0 + 3 * h;
     for (usize y = 0; y < h; y++) {
         usize sb = (full + y) * stride, db = (hp + y) * stride;
         for (usize x = 0; x < w; x++) {
-            u8 a = read_or(dst, len, sb + x, 0);
-            u8 b = read_or(dst, len, sb + x + 1, a);
+            px a = read_or(dst, len, sb + x, 0);
+            px b = read_or(dst, len, sb + x + 1, a);
             if (db + x < len) dst[db + x] = avg_u8(a, b);
         }
     }
     for (usize y = 0; y < h; y++) {
         usize sb = (full + y) * stride, nb = (full + y + 1) * stride, db = (vp + y) * stride;
         for (usize x = 0; x < w; x++) {
-            u8 a = read_or(dst, len, sb + x, 0);
-            u8 b = read_or(dst, len, nb + x, a);
+            px a = read_or(dst, len, sb + x, 0);
+            px b = read_or(dst, len, nb + x, a);
             if (db + x < len) dst[db + x] = avg_u8(a, b);
         }
     }
     { /* copy_row(dst, v_plane*stride, full*stride, w): memmove semantics, :226-248 */
         usize d = vp * stride, s = full * stride;
         usize n = umin(umin(w, sat_sub_us(len, d)), sat_sub_us(len, s));
-        if (n && d != s) memmove(dst + d, dst + s, n);
+        if (n && d != s) memmove(dst + d, dst + s, n * sizeof(px));
     }
     for (usize y = 0; y < h; y++) {
         usize sb = (full + y) * stride, gb = (full + y + 1) * stride + 1, db = (hvp + y) * stride;
         for (usize x = 0; x < w; x++) {
-            u8 a = read_or(dst, len, sb + x, 0);
-            u8 b = read_or(dst, len, gb + x, a);
+            px a = read_or(dst, len, sb + x, 0);
+            px b = read_or(dst, len, gb + x, a);
             if (db + x < len) dst[db + x] = avg_u8(a, b);
         }
     }
     {
         usize d = hvp * stride, s = full * stride + 1;
         usize n = umin(umin(w, sat_sub_us(len, d)), sat_sub_us(len, s));
-        if (n && d != s) memmove(dst + d, dst + s, n);
+        if (n && d != s) memmove(dst + d, dst + s, n * sizeof(px));
     }
 }
 
 /* half(), super_build.rs:162-177; cubic8 (:138-160) computes the same value */
-static u8 half_tap(const u8 *buf, usize i, usize step, usize p, usize n) {
+static px half_tap(const px *buf, usize i, usize step, usize p, usize n) {
     if (p < 2 || p + 4 >= n) return p + 1 == n ? buf[i] : avg_u8(buf[i], buf[i + step]);
     i32 value = (i32)buf[i - 2 * step] + (i32)buf[i + 3 * step] +
                 5 * (4 * (i32)buf[i] - (i32)buf[i - step] + 4 * (i32)buf[i + step] - (i32)buf[i + 2 * step]) + 16;
-    return (u8)iclamp(value >> 5, 0, 255);
+    return (px)iclamp(value >> 5, 0, PX_MAX);
 }
 /* fill_bicubic_pel2 + bicubic_horizontal/vertical, super_build.rs:95-135 */
-static void fill_bicubic_pel2(u8 *buf, usize stride, usize row0, usize w, usize h) {
+static void fill_bicubic_pel2(px *buf, usize stride, usize row0, usize w, usize h) {
     usize p0 = row0, p1 = row0 + h, p2 = row0 + 2 * h, p3 = row0 + 3 * h;
     for (usize y = 0; y < h; y++) /* horizontal full -> p1 */
         for (usize x = 0; x < w; x++) buf[(p1 + y) * stride + x] = half_tap(buf, (p0 + y) * stride + x, 1, x, w);
@@ -344,7 +354,7 @@ static void fill_bicubic_pel2(u8 *buf, usize stride, usize row0, usize w, usize 
 }
 
 /* build_plane, super_build.rs:8-93 */
-void or_build_plane(uint8_t *dst, size_t dst_len, size_t dst_stride, const uint8_t *src,
+void or_build_plane(px *dst, size_t dst_len, size_t dst_stride, const px *src,
                     size_t src_len, size_t src_stride, size_t src_w, size_t src_h, size_t luma_w,
                     size_t luma_h, int32_t chroma, const or_super_opts *o) {
     usize levels = (usize)(i64)o->levels, pel = (usize)(i64)o->pel;
@@ -365,9 +375,9 @@ void or_build_plane(uint8_t *dst, size_t dst_len, size_t dst_stride, const uint8
         for (usize row = 0; row < umin(base_h, src_h); row++) {
             usize dst_off = (row0 + row) * dst_stride, src_off = row * src_stride;
             usize n = umin(umin(base_w, src_w), umin(sat_sub_us(dst_len, dst_off), sat_sub_us(src_len, src_off)));
-            if (n > 0) memcpy(dst + dst_off, src + src_off, n);
+            if (n > 0) memcpy(dst + dst_off, src + src_off, n * sizeof(px));
             if (base_w > 0 && dst_stride > base_w) {
-                u8 edge = dst[dst_off + base_w - 1];
+                px edge = dst[dst_off + base_w - 1];
                 for (usize p = base_w; p < dst_stride; p++)
                     if (dst_off + p < dst_len) dst[dst_off + p] = edge;
             }
@@ -393,17 +403,17 @@ size_t or_super_output_len(const or_super_opts *o) {
     return w * sh + 2 * ((w / 2) * (sh / 2));
 }
 
-void or_build_super_portable(const or_super_opts *o, const uint8_t *src, uint8_t *out) {
+void or_build_super_portable(const or_super_opts *o, const px *src, px *out) {
     usize w = (usize)o->width, h = (usize)o->height, cw = w / 2, ch = h / 2;
     usize sh = (usize)or_super_height(o);
     usize oy = w * sh, oc = cw * (sh / 2);
-    memset(out, 0, oy + 2 * oc);
+    memset(out, 0, (oy + 2 * oc) * sizeof(px));
     or_build_plane(out, oy, w, src, w * h, w, w, h, w, h, 0, o);
     or_build_plane(out + oy, oc, cw, src + w * h, cw * ch, cw, cw, ch, w, h, 1, o);
     or_build_plane(out + oy + oc, oc, cw, src + w * h + cw * ch, cw * ch, cw, cw, ch, w, h, 1, o);
 }
 
-void or_build_super_many(const or_super_opts *o, const uint8_t *const *src, uint8_t *const *out,
+void or_build_super_many(const or_super_opts *o, const px *const *src, px *const *out,
                          int32_t nframes, int32_t threads) {
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads > 0 ? threads : 1)
@@ -613,6 +623,7 @@ uint32_t or_hadamard4_satd(const int32_t d[16]) { /* hadamard4_satd, :2681-2702 
  * the reference's own sad_u8_simd (:1857-1994) and hadamard4_satd_sse2/avx2 (:2523-2679)
  * are: the same sums, in 16-bit lanes (|coefficient| <= 16 * 255 never overflows). Used by
  * the CPU baseline's speed only; the scalar forms below remain the definition. */
+#ifndef OR_PX16
 static int in_slice(usize len, usize i, usize stride, usize w, usize h) {
     if (i > len || h == 0) return 0;
     usize rest = len - i;
@@ -663,14 +674,18 @@ static inline u32 hsum_epi32(__m256i v) {
     return (u32)_mm_cvtsi128_si32(t);
 }
 
+#endif
+
 /* sad_u8_simd (:1857-1951): plain sum of |a-b| at (possibly wrapped) base indices */
-static u32 sad_raw(const u8 *a, usize alen, usize ai, usize as, const u8 *b, usize blen, usize bi,
+static u32 sad_raw(const px *a, usize alen, usize ai, usize as, const px *b, usize blen, usize bi,
                    usize bs, usize w, usize h) {
+#ifndef OR_PX16
     if ((w == 4 || w == 8 || w == 16 || w == 32) && in_slice(alen, ai, as, w, h) && in_slice(blen, bi, bs, w, h)) {
         u32 t = 0;
         for (usize r = 0; r < h; r++) t += sad_row_simd(a + ai + r * as, b + bi + r * bs, w);
         return t;
     }
+#endif
     u32 s = 0;
     for (usize r = 0; r < h; r++)
         for (usize c = 0; c < w; c++) {
@@ -680,8 +695,9 @@ static u32 sad_raw(const u8 *a, usize alen, usize ai, usize as, const u8 *b, usi
     return s;
 }
 /* satd_interior (:2439-2521) == (sum of per-tile hadamard4_satd) >> 1 */
-static u32 satd_raw(const u8 *a, usize alen, usize ai, usize as, const u8 *b, usize blen, usize bi,
+static u32 satd_raw(const px *a, usize alen, usize ai, usize as, const px *b, usize blen, usize bi,
                     usize bs, usize n) {
+#ifndef OR_PX16
     if ((n == 16 || n == 32) && in_slice(alen, ai, as, n, n) && in_slice(blen, bi, bs, n, n)) {
         __m256i acc = _mm256_setzero_si256();
         for (usize ty = 0; ty < n; ty += 4)
@@ -689,6 +705,7 @@ static u32 satd_raw(const u8 *a, usize alen, usize ai, usize as, const u8 *b, us
                 acc = _mm256_add_epi32(acc, satd_strip16(a + ai + ty * as + tx, as, b + bi + ty * bs + tx, bs));
         return hsum_epi32(acc) >> 1;
     }
+#endif
     u32 total = 0;
     usize tiles = n / 4;
     for (usize ty = 0; ty < tiles; ty++)
@@ -726,7 +743,7 @@ static int edge_shift_origins(i32 px, i32 py, i32 mvx, i32 mvy, i32 bw, i32 bh, 
 }
 
 /* satd_edge, :2305-2351 */
-static u32 satd_edge(const u8 *s, usize slen, usize sstride, usize srow, i32 sx0, i32 sy0, const u8 *r,
+static u32 satd_edge(const px *s, usize slen, usize sstride, usize srow, i32 sx0, i32 sy0, const px *r,
                      usize rlen, usize rstride, usize rrow, i32 rx0, i32 ry0, usize width, usize height,
                      usize n) {
     i32 w = (i32)width, h = (i32)height;
@@ -874,10 +891,10 @@ static u32 chroma_sad_x4(const or_planes *src, const or_planes *ref, i32 level, 
             usize sx = cpx + col;
             usize rx = (usize)iclamp((i32)cpx + (i32)col + mv_cx, 0, (i32)clw - 1);
             if (sx >= clw) break;
-            i32 au = read_or(src->u, src->u_len, (c_cur + sy) * src->u_stride + sx, 128);
-            i32 av = read_or(src->v, src->v_len, (c_cur + sy) * src->v_stride + sx, 128);
-            i32 bu = read_or(ref->u, ref->u_len, (c_ref + ry) * ref->u_stride + rx, 128);
-            i32 bv = read_or(ref->v, ref->v_len, (c_ref + ry) * ref->v_stride + rx, 128);
+            i32 au = read_or(src->u, src->u_len, (c_cur + sy) * src->u_stride + sx, PX_MID);
+            i32 av = read_or(src->v, src->v_len, (c_cur + sy) * src->v_stride + sx, PX_MID);
+            i32 bu = read_or(ref->u, ref->u_len, (c_ref + ry) * ref->u_stride + rx, PX_MID);
+            i32 bv = read_or(ref->v, ref->v_len, (c_ref + ry) * ref->v_stride + rx, PX_MID);
             sad_uv = sat_add_u32(sat_add_u32(sad_uv, (u32)iabs(au - bu)), (u32)iabs(av - bv));
         }
     }
@@ -941,10 +958,10 @@ static int block_cost_edge_lc(const or_planes *src, const or_planes *ref, i32 le
             for (usize col = 0; col < cw; col++) {
                 usize sx = (usize)iclamp(ccx + (i32)col, 0, imax(clw_i - 1, 0));
                 usize rx = (usize)iclamp(crx0 + (i32)col, 0, imax(clw_i - 1, 0));
-                i32 au = read_or(src->u, src->u_len, (c_off + sy) * src->u_stride + sx, 128);
-                i32 bu = read_or(ref->u, ref->u_len, (c_ref + ry) * ref->u_stride + rx, 128);
-                i32 av = read_or(src->v, src->v_len, (c_off + sy) * src->v_stride + sx, 128);
-                i32 bv = read_or(ref->v, ref->v_len, (c_ref + ry) * ref->v_stride + rx, 128);
+                i32 au = read_or(src->u, src->u_len, (c_off + sy) * src->u_stride + sx, PX_MID);
+                i32 bu = read_or(ref->u, ref->u_len, (c_ref + ry) * ref->u_stride + rx, PX_MID);
+                i32 av = read_or(src->v, src->v_len, (c_off + sy) * src->v_stride + sx, PX_MID);
+                i32 bv = read_or(ref->v, ref->v_len, (c_ref + ry) * ref->v_stride + rx, PX_MID);
                 sad = sat_add_u32(sat_add_u32(sad, (u32)iabs(au - bu)), (u32)iabs(av - bv));
             }
         }
@@ -1174,7 +1191,7 @@ static i32 adaptive_radius(i32 radius, u32 activity) { /* :1478-1484 */
     u32 a = 255u * activity / 150u;
     return ((radius * (i32)(a < 255 ? a : 255)) >> 8) + 1;
 }
-static u32 plane_activity(const u8 *data, usize len, usize stride, usize row, usize x, usize width, usize height,
+static u32 plane_activity(const px *data, usize len, usize stride, usize row, usize x, usize width, usize height,
                           int satd) { /* :1517-1553 */
     u32 area = (u32)(width * height);
     u32 sum = 0;
@@ -1249,6 +1266,7 @@ static u8 block_luma_dc(const or_planes *src, i32 level, i32 px, i32 py, i32 bw,
             for (usize r = 0; r < h; r++)
                 for (usize c = 0; c < w; c++) sum += src->y[start + r * src->y_stride + c];
             u32 m = sum / (u32)(w * h);
+            m >>= DC_SHIFT;
             return (u8)(m < 255 ? m : 255);
         }
     }
@@ -1265,6 +1283,7 @@ static u8 block_luma_dc(const or_planes *src, i32 level, i32 px, i32 py, i32 bw,
     }
     if (count == 0) return 0;
     u32 m = sum / count;
+    m >>= DC_SHIFT;
     return (u8)(m < 255 ? m : 255);
 }
 
@@ -1741,7 +1760,7 @@ void or_pack_vdata_header(const or_analyse_opts *o, int32_t h[16]) { /* :2813-28
     h[11] = gw; h[12] = gh; h[13] = o->selector; h[14] = o->delta;
 }
 
-static void portable_planes(const or_super_opts *so, const uint8_t *buf, or_planes *p) { /* SuperFrame::planes */
+static void portable_planes(const or_super_opts *so, const px *buf, or_planes *p) { /* SuperFrame::planes */
     usize w = (usize)so->width, sh = (usize)or_super_height(so), cw = w / 2;
     usize ylen = w * sh, clen = cw * (sh / 2);
     p->y = buf; p->y_len = ylen; p->y_stride = w;
@@ -1750,8 +1769,8 @@ static void portable_planes(const or_super_opts *so, const uint8_t *buf, or_plan
     p->luma_w = w; p->luma_h = (usize)so->height; p->pel = so->pel; p->levels = so->levels; p->full = so->full;
 }
 
-int or_analyse_portable(const or_analyse_opts *o, const or_super_opts *so, const uint8_t *cur_super,
-                        const uint8_t *ref_super, uint8_t *payload) {
+int or_analyse_portable(const or_analyse_opts *o, const or_super_opts *so, const px *cur_super,
+                        const px *ref_super, uint8_t *payload) {
     or_planes a, b;
     portable_planes(so, cur_super, &a);
     portable_planes(so, ref_super, &b);
@@ -1768,7 +1787,7 @@ int or_analyse_portable(const or_analyse_opts *o, const or_super_opts *so, const
     return rc;
 }
 
-int or_analyse_clip(const or_analyse_opts *o, const or_super_opts *so, const uint8_t *const *supers, int32_t nframes,
+int or_analyse_clip(const or_analyse_opts *o, const or_super_opts *so, const px *const *supers, int32_t nframes,
                     int32_t first, int32_t count, uint8_t *payloads, int32_t threads) {
     usize plen = or_payload_len(o);
     i32 delta = imax(o->delta, 1);
@@ -1829,15 +1848,15 @@ int or_vector_planes(const int32_t vdata[16], const uint8_t *p, size_t len, int3
         v != flags)
         return -1;
     size_t count = (size_t)gw * (size_t)gh, first = 0x40, second = first + 4 + count * 8;
-    int16_t *px = calloc(count + 1, 2), *py = calloc(count + 1, 2), *cx = calloc(count + 1, 2),
+    int16_t *pvx = calloc(count + 1, 2), *pvy = calloc(count + 1, 2), *cx = calloc(count + 1, 2),
             *cy = calloc(count + 1, 2);
-    int okp = (flags & 1) ? decode_region(p, len, first, count, px, py) : 0;
+    int okp = (flags & 1) ? decode_region(p, len, first, count, pvx, pvy) : 0;
     int okc = (flags & 2) ? decode_region(p, len, second, count, cx, cy) : 0;
     int rc = 0;
     if (((flags & 1) && !okp) || ((flags & 2) && !okc) || (!okp && !okc)) rc = -1;
     else {
-        if (!okp) { memcpy(px, cx, count * 2); memcpy(py, cy, count * 2); }
-        if (!okc) { memcpy(cx, px, count * 2); memcpy(cy, py, count * 2); }
+        if (!okp) { memcpy(pvx, cx, count * 2); memcpy(pvy, cy, count * 2); }
+        if (!okc) { memcpy(cx, pvx, count * 2); memcpy(cy, pvy, count * 2); }
         int32_t mw, mh;
         or_vector_grid(vdata, &mw, &mh);
         mw = imax(mw, 0); mh = imax(mh, 0);
@@ -1849,7 +1868,7 @@ int or_vector_planes(const int32_t vdata[16], const uint8_t *p, size_t len, int3
                 size_t si = sy * (size_t)gw + sx, o = (size_t)y * mw + x;
                 for (int w = 0; w < 2; w++) {
                     int dx = 0, dy = 0;
-                    if (si < count) { dx = w ? cx[si] : px[si]; dy = w ? cy[si] : py[si]; }
+                    if (si < count) { dx = w ? cx[si] : pvx[si]; dy = w ? cy[si] : pvy[si]; }
                     uint16_t ox, oy;
                     if (dx > 1023 || dx < -1023 || dy > 1023 || dy < -1023) ox = oy = 1024;
                     else {
@@ -1861,6 +1880,6 @@ int or_vector_planes(const int32_t vdata[16], const uint8_t *p, size_t len, int3
                 }
             }
     }
-    free(px); free(py); free(cx); free(cy);
+    free(pvx); free(pvy); free(cx); free(cy);
     return rc;
 }

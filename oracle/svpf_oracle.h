@@ -24,6 +24,15 @@
 extern "C" {
 #endif
 
+/* Sample type. The reference is 8-bit only; building with OR_PX16 gives this project's 10-bit
+ * extension (uint16 samples 0..1023, chroma default 512, block luma byte = mean >> 2), which
+ * has no reference behaviour and is checked against nothing but itself. */
+#ifdef OR_PX16
+typedef uint16_t or_px;
+#else
+typedef uint8_t or_px;
+#endif
+
 /* One looked-up option value: the result of Value::at(path) in
  * crates/svpflow-core/src/params.rs:69-85 (absent when the path does not exist). */
 enum {
@@ -102,9 +111,9 @@ typedef struct {
 
 /* SuperPlanes, analyse_search.rs:33-46 (slices carry their lengths). */
 typedef struct {
-    const uint8_t *y; size_t y_len, y_stride;
-    const uint8_t *u; size_t u_len, u_stride;
-    const uint8_t *v; size_t v_len, v_stride;
+    const or_px *y; size_t y_len, y_stride;
+    const or_px *u; size_t u_len, u_stride;
+    const or_px *v; size_t v_len, v_stride;
     size_t luma_w, luma_h;
     int32_t pel, levels, full;
 } or_planes;
@@ -131,12 +140,12 @@ void or_grid(const or_analyse_opts *o, int32_t bw, int32_t bh, int32_t ox, int32
 void or_level_grid(const or_analyse_opts *o, int32_t level, int32_t *gw, int32_t *gh);
 
 /* ---- Super (super_build.rs) ---- */
-void or_build_plane(uint8_t *dst, size_t dst_len, size_t dst_stride, const uint8_t *src,
+void or_build_plane(or_px *dst, size_t dst_len, size_t dst_stride, const or_px *src,
                     size_t src_len, size_t src_stride, size_t src_w, size_t src_h, size_t luma_w,
                     size_t luma_h, int32_t chroma, const or_super_opts *o);
 /* SuperBuilder::build (portable.rs:94-148): src = packed I420 (w*h + 2*(w/2*h/2)),
  * out = y (w*H) | u (w/2*H/2) | v (w/2*H/2), H = super height. */
-void or_build_super_portable(const or_super_opts *o, const uint8_t *src, uint8_t *out);
+void or_build_super_portable(const or_super_opts *o, const or_px *src, or_px *out);
 size_t or_super_output_len(const or_super_opts *o);
 
 /* ---- Analyse (analyse_search.rs) ---- */
@@ -150,16 +159,16 @@ void or_pack_vector_frame(const or_analyse_opts *o, const or_vec8 *previous, con
                           uint8_t *out);
 void or_pack_vdata_header(const or_analyse_opts *o, int32_t out[16]);
 /* Analyser::analyse over two portable super frames -> payload bytes. */
-int or_analyse_portable(const or_analyse_opts *o, const or_super_opts *so, const uint8_t *cur_super,
-                        const uint8_t *ref_super, uint8_t *payload);
+int or_analyse_portable(const or_analyse_opts *o, const or_super_opts *so, const or_px *cur_super,
+                        const or_px *ref_super, uint8_t *payload);
 /* Clip driver used by the CPU baseline: frame n pairs with min(n+delta, nframes-1)
  * (analyse_filter.rs:277-279); pairs [first, first+count) are analysed on `threads`
  * host threads (frames in parallel, fwd/bwd as two tasks, analyse_search.rs:160-191).
  * supers[i] points at the portable super frame of frame i. */
-int or_analyse_clip(const or_analyse_opts *o, const or_super_opts *so, const uint8_t *const *supers,
+int or_analyse_clip(const or_analyse_opts *o, const or_super_opts *so, const or_px *const *supers,
                     int32_t nframes, int32_t first, int32_t count, uint8_t *payloads, int32_t threads);
 /* Super over many frames on `threads` host threads. */
-void or_build_super_many(const or_super_opts *o, const uint8_t *const *src, uint8_t *const *out,
+void or_build_super_many(const or_super_opts *o, const or_px *const *src, or_px *const *out,
                          int32_t nframes, int32_t threads);
 
 /* ---- consumers of the payload (svpflow-core metadata.rs / renderer.rs) ---- */
