@@ -23,6 +23,9 @@ Other workloads (one JSON line each, same keys):
                        analysed by one persistent launch replayed from a CUDA graph, with the
                        autotuned launch shape; `plain_per_clip` times the same clips through
                        the per-clip path one after another, and every payload is compared.
+  --workload 2160p10   a 3840x2160 10-bit clip (uint16 samples) of 120 frames, Super {pel:4},
+                       Analyse block 8 / overlap 4 / exhaustive r8 / SATD + chroma; the CPU leg
+                       and the parity check use the oracle's uint16 build.
   --workload served    Poisson arrivals of clips (360p..2160p, 8-600 frames) into the
                        continuous-batching server under an HBM budget, at each --rates value;
                        p50 / p99 per-frame-pair latency (arrival of the clip to its payload in
@@ -54,6 +57,15 @@ UNIT = "frame-pairs/s"
 # DRAM bytes per frame pair of the Analyse kernel at 1080p (ncu capture of a 17-pair launch:
 # 294.6 MB read + 55.2 MB written)
 TRAFFIC_PER_PAIR = 349.8e6 / 17
+# int32 lanes per SM on sm_100 and the SM clock ceiling, for the nominal integer peak
+INT32_LANES_PER_SM = 128
+SM_MAX_MHZ = 1965.0
+
+
+def _sm_count() -> int:
+    import torch
+
+    return torch.cuda.get_device_properties(0).multi_processor_count
 
 
 def _peaks():
@@ -149,10 +161,12 @@ def cpu_reference(nframes_total: int, threads: int, pairs: int, seed: int = 1000
     clip = make_clip(w, h, n, seed=seed, motion=c["motion"], objects=c["objects"], object_motion=c["object_motion"])
     so = orc.super_opts(w, h, SUPER_OPT[WORKLOAD])
     ao = orc.analyse_opts(orc.sdata(so), ANALYSE_OPT[WORKLOAD], None, w, h)
+    orc.total_counters(reset=True)
     t0 = time.perf_counter()
     supers = orc.build_super_many(so, clip, threads)
     pay = orc.analyse_clip(ao, so, supers, 0, pairs, threads)
     dt = time.perf_counter() - t0
+    cpu_reference.counters = orc.total_counters(reset=True)  # the sample's compares (instrumentation)
     return dt, pay, clip
 
 
@@ -223,6 +237,149 @@ def _max_over_ranks(torch, dist, world, v: float, dev) -> float:
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def run_2160p10(args, world: int, rank: int, local: int):
+    """Config 3: one 2160p 10-bit clip per GPU (uint16 samples 0..1023), Super {pel:4}, Analyse
+    block 8 / overlap 4 / exhaustive radius 8 / SATD + chroma. The reference is 8-bit only, so
+    the CPU leg is the oracle's uint16 build, and parity is against it."""
+    torch, dist = _init_dist(world, local)
+    import svpflow_b200 as sv
+    from oracle import oracle as orc
+
+    wl = "2160p10"
+    c = CONFIGS[wl]
+    w, h = c["width"], c["height"]
+    nf = args.frames or c["frames"]
+    dev = torch.device("cuda", local)
+    t0 = time.perf_counter()
+    frames_d = make_clip_device(w, h, nf, seed=3000 + rank, motion=c["motion"], objects=c["objects"],
+                                object_motion=c["object_motion"], noise=c["noise"], device=dev, bits=c["bits"])
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    sb = sv.Super(w, h, SUPER_OPT[wl], bits=c["bits"])
+    an = sv.Analyse(sb.sdata, ANALYSE_OPT[wl], w, h, bits=c["bits"])
+    fb, pl = sb.output_len(), an.payload_len()
+    supers_d = torch.empty((nf, fb), dtype=torch.uint8, device=dev)
+    pay_d = torch.empty((nf, pl), dtype=torch.uint8, device=dev)
+    scratch_d = torch.empty(an.scratch_bytes(nf), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        sb.build_device(frames_d.data_ptr(), supers_d.data_ptr(), nf, sh)
+        if ev:
+            ev[1].record(stream)
+        an.analyse_clip_device(supers_d.data_ptr(), nf, 0, nf, pay_d.data_ptr(), scratch_d.data_ptr(), sh)
+        if ev:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    sv.Analyser.device_status(scratch_d.data_ptr(), sh)
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sv.reset_kernel_launches()
+    with ClockSampler(_gpu_id(torch, local)) as clk:
+        start.record(stream)
+        for i in range(args.steps):
+            step(evs[i])
+        stop.record(stream)
+        torch.cuda.synchronize()
+    launches = sv.kernel_launches()
+    sv.Analyser.device_status(scratch_d.data_ptr(), sh)
+    ms_max = _max_over_ranks(torch, dist, world, start.elapsed_time(stop), dev)
+    value = nf * world * args.steps / (ms_max / 1000.0)
+    super_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    a_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+    pay_host = pay_d.cpu().numpy()
+    # end to end through the host-buffer call; the device-path buffers are released first
+    host_frames = frames_d.cpu().pin_memory().numpy().view(np.uint16)
+    del supers_d, scratch_d, pay_d, frames_d
+    torch.cuda.empty_cache()
+    out_host = torch.empty((nf, pl), dtype=torch.uint8).pin_memory().numpy()
+    e2e_value, same = None, None
+    if args.e2e_steps > 0:
+        def e2e_step():
+            rc = sv.lib().svpf_clip_analyse(an.handle, sb.handle, host_frames.ctypes.data, nf, 0, nf,
+                                            out_host.ctypes.data)
+            if rc:
+                raise RuntimeError(sv.lib().svpf_last_error().decode())
+
+        e2e_step()  # the call's own device buffers are allocated on first use
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        e2e_value = nf * world * args.e2e_steps / _max_over_ranks(torch, dist, world, time.perf_counter() - t0, dev)
+        same = bool(np.array_equal(out_host, pay_host))
+    line = None
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        alg_analyse = nf * (2 * fb + pl)
+        alg_super = nf * (sb.source_len() + fb)
+        roof = {
+            "kernel": "analyse_kernel, uint16 build (one CTA per frame pair, fwd/bwd halves)",
+            "bound": "hbm", "achieved": alg_analyse / (a_ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+            "frac": alg_analyse / (a_ms / 1000) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": alg_analyse, "avg_launch_ms": a_ms,
+            "super": {"bound": "hbm", "achieved": alg_super / (super_ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+                      "frac": alg_super / (super_ms / 1000) / 1e9 / peak, "avg_launch_ms": super_ms,
+                      "algorithmic_bytes_per_launch": alg_super},
+        }
+        cpu, parity = None, None
+        if not args.no_cpu:
+            threads = os.cpu_count() or 1
+            pairs = min(args.cpu_pairs or threads, nf - 1)
+            so = orc.super_opts(w, h, SUPER_OPT[wl])
+            ao = orc.analyse_opts(orc.sdata(so), ANALYSE_OPT[wl], None, w, h)
+            orc.total_counters(reset=True, px16=True)
+            t0 = time.perf_counter()
+            sup_cpu = orc.build_super_many16(so, host_frames[: pairs + 1], threads)
+            pay_cpu = orc.analyse_clip16(ao, so, sup_cpu, 0, pairs, threads)
+            dt = time.perf_counter() - t0
+            cnt = orc.total_counters(reset=True, px16=True)
+            cpu = {"value": pairs / dt, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"output frames 0..{pairs - 1} of the same clip (Super + Analyse) on {threads} host "
+                             f"threads, the oracle's uint16 build (scalar SAD/SATD)",
+                   "cpu_model": _cpu_model()}
+            parity = {"pairs_checked": pairs, "bit_exact": bool(np.array_equal(pay_cpu, pay_host[:pairs]))}
+            ops_pair = orc.integer_ops(cnt) / pairs
+            int_peak = INT32_LANES_PER_SM * _sm_count() * SM_MAX_MHZ * 1e6
+            roof["integer"] = {
+                "bound": "int32 pipe", "achieved": ops_pair * nf / (a_ms / 1000) / 1e12, "peak": int_peak / 1e12,
+                "unit": "Tops/s", "frac": ops_pair * nf / (a_ms / 1000) / int_peak, "ops_per_pair": ops_pair,
+                "evaluations_per_pair": cnt[0] / pairs, "samples_compared_per_pair": (cnt[1] + cnt[2]) / pairs,
+                "satd_share": (cnt[3] + cnt[4]) / max(cnt[1] + cnt[2], 1),
+                "peak_source": "nominal: SMs x 128 int32 lanes x max SM clock (no measured integer peak)"}
+        line = {
+            "metric": "Analyse frame-pairs/s at 2160p 10-bit (bit-exact to the oracle)", "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "config": {"workload": f"2160p YUV420P10 (uint16) {nf}-frame synthetic clip per GPU, Super "
+                                   f"{SUPER_OPT[wl]}, Analyse {ANALYSE_OPT[wl]} (block 8, overlap 4, exhaustive r8 "
+                                   f"at level 0, hex2 above, SATD+chroma, fwd+bwd)",
+                       "width": w, "height": h, "frames_per_gpu": nf, "pairs_per_step": nf * world,
+                       "l2": f"inputs larger than L2 ({nf} super frames = {nf * fb / 1e9:.1f} GB per GPU)",
+                       "generator_s": gen_s},
+            "clocks": clk.summary(),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_frames.nbytes),
+                    "d2h_bytes_per_step": int(nf * pl), "api": "svpf_clip_analyse (host buffers)",
+                    "matches_device_path": same},
+            "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "parity_vs_oracle": parity,
+            "super_ms_per_step": super_ms, "analyse_ms_per_step": a_ms,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_batched(args, world: int, rank: int, local: int):
@@ -448,11 +605,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="svpflow_b200")
-    ap.add_argument("--frames", type=int, default=CONFIGS[WORKLOAD]["frames"])
+    ap.add_argument("--frames", type=int, default=0, help="frames per clip (default: the workload's)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-pairs", type=int, default=0, help="CPU baseline sample (0 = one per host thread)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="1080p", choices=["1080p", "batched", "served"])
+    ap.add_argument("--workload", default="1080p", choices=["1080p", "2160p10", "batched", "served"])
     ap.add_argument("--clips", type=int, default=0, help="batched: clips (default 64); served: clips per rate (16)")
     ap.add_argument("--max-len", type=int, default=0, help="longest clip in frames (default: the workload's)")
     ap.add_argument("--rates", default="5,50,200", help="served: arrival rates, clips/s")
@@ -471,6 +628,8 @@ def main():
         return run_batched(args, world, rank, local)
     if args.workload == "served":
         return run_served(args, world, rank, local)
+    if args.workload == "2160p10":
+        return run_2160p10(args, world, rank, local)
 
     import torch
     import torch.distributed as dist
@@ -484,7 +643,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     dev = torch.device("cuda", local)
     c = CONFIGS[WORKLOAD]
-    w, h, nf = c["width"], c["height"], args.frames
+    w, h, nf = c["width"], c["height"], args.frames or c["frames"]
     clip = make_clip(w, h, nf, seed=1000 + rank, motion=c["motion"], objects=c["objects"],
                      object_motion=c["object_motion"])
     sb = sv.Super(w, h, SUPER_OPT[WORKLOAD])
@@ -589,6 +748,20 @@ def main():
             threads = os.cpu_count() or 1
             pairs = min(args.cpu_pairs or threads, nf - 1)
             dt, pay_cpu, _ = cpu_reference(nf, threads, pairs, seed=1000 + rank)
+            from oracle import oracle as orc
+
+            cnt = cpu_reference.counters
+            ops_pair = orc.integer_ops(cnt) / pairs
+            int_peak = INT32_LANES_PER_SM * _sm_count() * SM_MAX_MHZ * 1e6
+            roof["integer"] = {
+                "bound": "int32 pipe", "achieved": ops_pair * nf / (a_ms / 1000) / 1e12,
+                "peak": int_peak / 1e12, "unit": "Tops/s", "frac": ops_pair * nf / (a_ms / 1000) / int_peak,
+                "ops_per_pair": ops_pair, "evaluations_per_pair": cnt[0] / pairs,
+                "samples_compared_per_pair": (cnt[1] + cnt[2]) / pairs,
+                "satd_share": (cnt[3] + cnt[4]) / max(cnt[1] + cnt[2], 1),
+                "ops_source": f"compares the oracle executed on output frames 0..{pairs - 1} (2 ops per SAD "
+                              f"sample, 111 per SATD 4x4 tile)",
+                "peak_source": "nominal: SMs x 128 int32 lanes x max SM clock (no measured integer peak)"}
             cpu = {"value": pairs / dt, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"output frames 0..{pairs - 1} of the same clip (Super + Analyse) on {threads} host "
                              f"threads, oracle/ C restatement of the reference (AVX2 interior SAD/SATD)",

@@ -97,12 +97,14 @@ def make_clip(width: int, height: int, frames: int, seed: int, motion: int = 8, 
 
 
 def make_clip_device(width: int, height: int, frames: int, seed: int, motion: int = 8, objects: int = 4,
-                     object_motion: int = 16, noise: float = 2.0, device="cuda", chunk: int = 32):
+                     object_motion: int = 16, noise: float = 2.0, device="cuda", chunk: int = 32, bits: int = 8):
     """The recipe of make_clip, run with torch on the device and vectorised over frames (for
     the large batched and served workloads, where the host generator would take minutes).
     Differences: its own random stream, and frame k's background is frame 0's shifted once
     by the accumulated global motion (edges replicated) rather than shifted frame by frame.
-    Returns a uint8 tensor [frames, w*h + 2*(w/2*h/2)] on `device`."""
+    Returns a uint8 tensor [frames, w*h + 2*(w/2*h/2)] on `device`; with bits=10 the textures
+    span 0..1023 (uniform noise before the blur), `noise` is in 10-bit units and the tensor
+    is int16 holding the uint16 samples."""
     import torch
 
     assert width % 2 == 0 and height % 2 == 0
@@ -119,8 +121,10 @@ def make_clip_device(width: int, height: int, frames: int, seed: int, motion: in
         x = F.pad(x, (0, 0, r, r), mode="replicate")
         return F.conv2d(x, k.view(1, 1, -1, 1))[0, 0]
 
+    top = (1 << bits) - 1
+
     def noise_img(h, w):
-        return torch.randint(0, 256, (h, w), generator=g, device=device).float()
+        return torch.randint(0, top + 1, (h, w), generator=g, device=device).float()
 
     rng = np.random.default_rng(int(seed))
     base = [blur(noise_img(height, width), 2.0), blur(noise_img(ch, cw), 1.0), blur(noise_img(ch, cw), 1.0)]
@@ -136,7 +140,7 @@ def make_clip_device(width: int, height: int, frames: int, seed: int, motion: in
     steps[0] = 0
     cum = np.cumsum(steps, axis=0)  # accumulated (dy, dx) of every frame
     ysz, csz = width * height, cw * ch
-    out = torch.empty((frames, ysz + 2 * csz), dtype=torch.uint8, device=device)
+    out = torch.empty((frames, ysz + 2 * csz), dtype=torch.uint8 if bits == 8 else torch.int16, device=device)
     dims = [(height, width, 1), (ch, cw, 2), (ch, cw, 2)]
     for f0 in range(0, frames, chunk):
         f1 = min(frames, f0 + chunk)
@@ -159,8 +163,8 @@ def make_clip_device(width: int, height: int, frames: int, seed: int, motion: in
                         oy, ox = oy // 2, ox // 2
                     hh, ww = min(th, h - oy), min(tw, w - ox)
                     planes[k, oy:oy + hh, ox:ox + ww] = t[:hh, :ww]
-            q = (planes + noise * torch.randn(planes.shape, generator=g, device=device)).round_().clamp_(0, 255)
-            q = q.to(torch.uint8).reshape(n, -1)
+            q = (planes + noise * torch.randn(planes.shape, generator=g, device=device)).round_().clamp_(0, top)
+            q = q.to(out.dtype).reshape(n, -1)
             if pi == 0:
                 out[f0:f1, :ysz] = q
             else:
@@ -209,10 +213,14 @@ def analyse_opt_for_block(block: int) -> str:
 CONFIGS = {
     "640x360": dict(width=640, height=360, frames=32, motion=8, objects=4, object_motion=16),
     "1080p": dict(width=1920, height=1080, frames=240, motion=24, objects=8, object_motion=48),
+    # 10-bit (uint16 samples 0..1023, noise sigma 8); the object motions keep the 1080p range
+    "2160p10": dict(width=3840, height=2160, frames=120, motion=64, objects=8, object_motion=48, noise=8.0, bits=10),
 }
 # Option strings of those configurations for the reference's Super / Analyse filters.
-SUPER_OPT = {"640x360": "{pel:1}", "1080p": "{pel:2}"}
+SUPER_OPT = {"640x360": "{pel:1}", "1080p": "{pel:2}", "2160p10": "{pel:4}"}
 ANALYSE_OPT = {
     "640x360": "{block:{w:16,overlap:0},main:{search:{type:2,distance:2,satd:false,coarse:{satd:false}}}}",
     "1080p": "{block:{w:16,overlap:3},main:{search:{type:3,distance:16,satd:true}}}",
+    # block 8 overlap 4, exhaustive radius 8 at the finest level, hex2 above it, SATD + chroma
+    "2160p10": "{block:{w:8,overlap:3},main:{search:{type:4,distance:8,satd:true,coarse:{type:2}}}}",
 }

@@ -440,6 +440,7 @@ def _setup(L):
     L.or_global_doubled.argtypes = [P(Vec8), ctypes.c_size_t, P(ctypes.c_int32), P(ctypes.c_int32)]
     L.or_block_cost_lc.argtypes = [P(Planes), P(Planes)] + [ctypes.c_int32] * 9 + [P(ctypes.c_uint32), P(ctypes.c_uint32)]
     L.or_last_counters.argtypes = [P(ctypes.c_uint64)]
+    L.or_total_counters.argtypes = [P(ctypes.c_uint64), ctypes.c_int32]
     for f in ("or_reduce_dim", "or_auto_levels", "or_super_plane_height", "or_auto_search_levels"):
         getattr(L, f).argtypes = [ctypes.c_int32] * {"or_reduce_dim": 2, "or_auto_levels": 2,
                                                        "or_super_plane_height": 4, "or_auto_search_levels": 6}[f]
@@ -550,9 +551,28 @@ def analyse(ao: AnalyseOpts, so: SuperOpts, cur: np.ndarray, ref: np.ndarray) ->
 
 
 def counters() -> list:
-    c = (ctypes.c_uint64 * 3)()
+    """[evaluations, luma samples, chroma samples, luma under SATD, chroma under SATD] of the
+    last pair analysed on this thread."""
+    c = (ctypes.c_uint64 * 5)()
     lib().or_last_counters(c)
     return list(c)
+
+
+def total_counters(reset: bool = False, px16: bool = False) -> list:
+    """counters() summed over every pair analysed (any thread) since the last reset; px16 reads
+    the uint16 build's."""
+    c = (ctypes.c_uint64 * 5)()
+    (lib16() if px16 else lib()).or_total_counters(c, int(reset))
+    return list(c)
+
+
+def integer_ops(c) -> float:
+    """Algorithmic integer operations of the compares counted in `c`: about 2 per sample for SAD
+    (absolute difference, accumulate) and 111 per 4x4 tile, 6.94 per sample, for SATD (16
+    differences, 64 butterfly adds, 16 absolute values, 15 adds)."""
+    satd = c[3] + c[4]
+    sad = c[1] + c[2] - satd
+    return 2.0 * sad + 111.0 / 16.0 * satd
 
 
 def analyse_clip(ao: AnalyseOpts, so: SuperOpts, supers: np.ndarray, first: int, count: int,

@@ -88,8 +88,16 @@ static void set_err(char *err, size_t n, const char *msg) {
 }
 
 /* per-thread work counters: cost evaluations, luma px, chroma px */
-static _Thread_local u64 g_cnt[3];
-void or_last_counters(uint64_t out[3]) { memcpy(out, g_cnt, sizeof(g_cnt)); }
+/* instrumentation (not part of the reference): [0] cost evaluations, [1] luma samples and
+ * [2] chroma samples compared, [3] / [4] the luma / chroma samples of [1] / [2] compared
+ * under SATD. Per thread for the last pair; g_tot sums every finished pair. */
+static _Thread_local u64 g_cnt[5];
+static u64 g_tot[5];
+void or_last_counters(uint64_t out[5]) { memcpy(out, g_cnt, sizeof(g_cnt)); }
+void or_total_counters(uint64_t out[5], int32_t reset) {
+    for (int i = 0; i < 5; i++) out[i] = reset ? __atomic_exchange_n(&g_tot[i], 0, __ATOMIC_RELAXED)
+                                               : __atomic_load_n(&g_tot[i], __ATOMIC_RELAXED);
+}
 /* per level: blocks, cost evaluations, blocks that ran the bad-SAD expansion, its evaluations */
 static _Thread_local u64 g_lvl[16][4];
 void or_level_counters(uint64_t out[64]) { memcpy(out, g_lvl, sizeof(g_lvl)); }
@@ -818,8 +826,10 @@ static u32 luma_interior(const or_planes *src, const or_planes *ref, i32 level, 
     usize sub_idx = i32_as_usize(sub_y * pel + sub_x);
     usize cur_row0 = y_off, ref_row0 = y_off + sub_idx * lh;
     g_cnt[1] += bw * bh;
-    if (use_satd && is_blk(bw) && is_blk(bh) && bw == bh)
+    if (use_satd && is_blk(bw) && is_blk(bh) && bw == bh) {
+        g_cnt[3] += bw * bh;
         return satd_luma_clamp(src, ref, cur_row0, ref_row0, px_u, py_u, mx, my, lw, lh, bw);
+    }
     i32 rx0 = px + mx, ry0 = py + my;
     int interior = px >= 0 && py >= 0 && rx0 >= 0 && ry0 >= 0 && (usize)px + bw <= lw &&
                    (usize)py + bh <= lh && (usize)rx0 + bw <= lw && (usize)ry0 + bh <= lh;
@@ -872,6 +882,7 @@ static u32 chroma_sad_x4(const or_planes *src, const or_planes *ref, i32 level, 
                 ru + (ch - 1) * ref->u_stride + cw <= ref->u_len && rv + (ch - 1) * ref->v_stride + cw <= ref->v_len) {
                 u32 a, b;
                 if (use_satd) { /* satd_interior(.., cw): an n x n square with n = cw */
+                    g_cnt[4] += 2 * cw * cw;
                     a = satd_raw(src->u, src->u_len, su, src->u_stride, ref->u, ref->u_len, ru, ref->u_stride, cw);
                     b = satd_raw(src->v, src->v_len, sv, src->v_stride, ref->v, ref->v_len, rv, ref->v_stride, cw);
                 } else {
@@ -918,6 +929,7 @@ static int block_cost_edge_lc(const or_planes *src, const or_planes *ref, i32 le
     u32 sad_l;
     g_cnt[1] += bw_u * bh_u;
     if (use_satd && is_blk(bw_u) && is_blk(bh_u) && bw_u == bh_u) {
+        g_cnt[3] += bw_u * bh_u;
         sad_l = satd_edge(src->y, src->y_len, src->y_stride, cur_row0, cx, cy, ref->y, ref->y_len, ref->y_stride,
                           ref_row0, rx0, ry0, lw, lh, bw_u);
     } else {
@@ -945,6 +957,7 @@ static int block_cost_edge_lc(const or_planes *src, const or_planes *ref, i32 le
     u32 sad_uv;
     g_cnt[2] += 2 * cw * ch;
     if (use_satd && cw == ch && (cw == 4 || cw == 8 || cw == 16)) {
+        g_cnt[4] += 2 * cw * ch;
         sad_uv = sat_add_u32(
             satd_edge(src->u, src->u_len, src->u_stride, c_off, ccx, ccy, ref->u, ref->u_len, ref->u_stride, c_ref,
                       crx0, cry0, clw, clh, cw),
@@ -1706,6 +1719,7 @@ int or_analyse_pair(const or_planes *cur, const or_planes *ref, const or_analyse
         free(st[d].order.v);
         free(st[d].next);
     }
+    for (int i = 0; i < 5; i++) __atomic_fetch_add(&g_tot[i], g_cnt[i], __ATOMIC_RELAXED);
     return rc;
 }
 

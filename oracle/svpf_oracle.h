@@ -190,7 +190,11 @@ void or_block_cost_lc(const or_planes *src, const or_planes *ref, int32_t level,
                       int32_t pel, uint32_t *luma, uint32_t *chroma);
 /* Work counters of the last or_analyse_pair on this thread (cost evaluations,
  * luma and chroma pixels compared): the algorithmic work of the control flow. */
-void or_last_counters(uint64_t out[3]);
+/* instrumentation: [0] cost evaluations, [1] / [2] luma / chroma samples compared, [3] / [4] of
+ * those under SATD; for the calling thread's last pair, or summed over all pairs since the last
+ * reset (or_total_counters). */
+void or_last_counters(uint64_t out[5]);
+void or_total_counters(uint64_t out[5], int32_t reset);
 void or_level_counters(uint64_t out[64]);
 
 #ifdef __cplusplus
