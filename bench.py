@@ -51,8 +51,14 @@ import numpy as np  # noqa: E402
 from svpflow_b200.synth import (ANALYSE_OPT, CONFIGS, SUPER_OPT, analyse_opt_for_block, batched_mix,  # noqa: E402
                                  make_clip, make_clip_device, served_stream)
 
-WORKLOAD = "1080p"
+WORKLOAD = "1080p"  # the single-clip workload of a run: "1080p" (default) or "640x360"
 METRIC = "Analyse frame-pairs/s at 1080p (bit-exact MVs)"
+DESC = {
+    "1080p": "1080p YUV420P8 {n}-frame synthetic clip per GPU, Super {s}, Analyse {a} (block 16, overlap 8, "
+             "UMH r16, SATD+chroma, fwd+bwd)",
+    "640x360": "640x360 YUV420P8 {n}-frame synthetic clip per GPU, Super {s}, Analyse {a} (block 16, overlap 0, "
+               "hex2 r2, luma SAD + chroma, fwd+bwd)",
+}
 UNIT = "frame-pairs/s"
 # DRAM bytes per frame pair of the Analyse kernel at 1080p (ncu capture of a 17-pair launch:
 # 294.6 MB read + 55.2 MB written)
@@ -80,11 +86,11 @@ def _peaks():
 def _config(nframes: int, world: int) -> dict:
     c = CONFIGS[WORKLOAD]
     return {
-        "workload": f"1080p YUV420P8 {nframes}-frame synthetic clip per GPU, Super {SUPER_OPT[WORKLOAD]}, "
-                    f"Analyse {ANALYSE_OPT[WORKLOAD]} (block 16, overlap 8, UMH r16, SATD+chroma, fwd+bwd)",
+        "workload": DESC[WORKLOAD].format(n=nframes, s=SUPER_OPT[WORKLOAD], a=ANALYSE_OPT[WORKLOAD]),
         "width": c["width"], "height": c["height"], "frames_per_gpu": nframes,
         "pairs_per_step": nframes * world,
-        "l2": "inputs larger than L2 (240 super frames = 3.7 GB per GPU)",
+        "l2": ("inputs larger than L2 (240 super frames = 3.7 GB per GPU)" if WORKLOAD == "1080p" else
+               "inputs smaller than L2: a 256 MB write flushes L2 before every step, outside the timed events"),
         "parallelism": f"dp{world} (frame ranges per GPU, no collective)" if world > 1 else "single GPU",
     }
 
@@ -609,7 +615,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-pairs", type=int, default=0, help="CPU baseline sample (0 = one per host thread)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="1080p", choices=["1080p", "2160p10", "batched", "served"])
+    ap.add_argument("--workload", default="1080p", choices=["1080p", "640x360", "2160p10", "batched", "served"])
     ap.add_argument("--clips", type=int, default=0, help="batched: clips (default 64); served: clips per rate (16)")
     ap.add_argument("--max-len", type=int, default=0, help="longest clip in frames (default: the workload's)")
     ap.add_argument("--rates", default="5,50,200", help="served: arrival rates, clips/s")
@@ -630,6 +636,9 @@ def main():
         return run_served(args, world, rank, local)
     if args.workload == "2160p10":
         return run_2160p10(args, world, rank, local)
+    global WORKLOAD, METRIC
+    if args.workload == "640x360":
+        WORKLOAD, METRIC = "640x360", "Analyse frame-pairs/s at 640x360 (bit-exact MVs)"
 
     import torch
     import torch.distributed as dist
@@ -656,7 +665,12 @@ def main():
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
 
+    # inputs smaller than L2: a 256 MB write before every step flushes it (outside the step's events)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if WORKLOAD != "1080p" else None
+
     def step(ev=None):
+        if flush is not None:
+            flush.fill_(1)
         if ev:
             ev[0].record(stream)
         sb.build_device(frames_d.data_ptr(), supers_d.data_ptr(), nf, sh)
@@ -690,6 +704,8 @@ def main():
     ms = start.elapsed_time(stop)
     super_ms = [e[0].elapsed_time(e[1]) for e in evs]
     analyse_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    if flush is not None:  # the steps' own time, without the L2 flushes between them
+        ms = sum(e[0].elapsed_time(e[2]) for e in evs)
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -732,7 +748,8 @@ def main():
         roof = {
             "kernel": "analyse_kernel (one CTA per frame pair, fwd/bwd halves)",
             "bound": "hbm", "achieved": alg_analyse / (a_ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
-            "frac": alg_analyse / (a_ms / 1000) / 1e9 / peak, "traffic": TRAFFIC_PER_PAIR * nf,
+            "frac": alg_analyse / (a_ms / 1000) / 1e9 / peak,
+            "traffic": TRAFFIC_PER_PAIR * nf if WORKLOAD == "1080p" else None,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 17-pair launch, per pair x pairs",
             "peak_source": peak_kind,
             "algorithmic_bytes_per_launch": alg_analyse, "avg_launch_ms": a_ms,
