@@ -782,9 +782,16 @@ __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, 
     return r;
 }
 
-__device__ __forceinline__ unsigned group_sum(unsigned v, int G) {
-    for (int o = G >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-    return v;
+// the three sums of a group of G lanes (independent shuffles, so they overlap)
+__device__ __forceinline__ void group_sum3(Res &r, int G) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        if (o < G) {
+            r.L += __shfl_xor_sync(0xFFFFFFFFu, r.L, o);
+            r.U += __shfl_xor_sync(0xFFFFFFFFu, r.U, o);
+            r.V += __shfl_xor_sync(0xFFFFFFFFu, r.V, o);
+        }
+    }
 }
 __device__ __forceinline__ void finalize(const Res &r, unsigned &L, unsigned &C) {
     L = r.lsatd ? (r.L >> 1) : r.L;
@@ -882,9 +889,7 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                     }
                 }
             }
-            r.L = group_sum(r.L, G);
-            r.U = group_sum(r.U, G);
-            r.V = group_sum(r.V, G);
+            group_sum3(r, G);
             long long K = 0x7FFFFFFFFFFFFFFFLL;
             unsigned sad = 0;
             if (act) {
@@ -1255,9 +1260,7 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
             }
             Res r{0, 0, 0, 0, 0, 0};
             if (act) r = eval_lane(x, b, kind, sxi * P.step_x, syi * P.step_y, mx, my, ch, sub, G);
-            r.L = group_sum(r.L, G);
-            r.U = group_sum(r.U, G);
-            r.V = group_sum(r.V, G);
+            group_sum3(r, G);
             if (act && sub == 0) {
                 unsigned Lv, Cv;
                 if (kind == 2) { Lv = r.L; Cv = 0; }
@@ -1408,9 +1411,7 @@ __device__ __forceinline__ void refine_pass(Ctx &x, DirSh &s, DirScratch &ds) {
                 const bool act = (grp == 0 && search) || grp == 1;
                 Res r{0, 0, 0, 0, 0, 0};
                 if (act) r = eval_lane(x, b, grp == 1 ? 2 : 0, 0, 0, pmx, pmy, grp == 0, sub, Gl);
-                r.L = group_sum(r.L, Gl);
-                r.U = group_sum(r.U, Gl);
-                r.V = group_sum(r.V, Gl);
+                group_sum3(r, Gl);
                 if (act && sub == 0) {
                     unsigned Lv, Cv;
                     if (grp == 1) { Lv = r.L; Cv = 0; }
