@@ -869,24 +869,25 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                 const int T = x.tl + (r.cmode != CM_NONE ? 2 * x.tcp : 0);
                 const int ys = x.G.ys32, cs = x.G.cs32, nlw = b.tilesx * b.bh;
                 const px_t *rl = x.R.y + lref;
+                int t = sub;  // luma tiles, then chroma: two loops, no per-tile branch on the plane
 #pragma unroll 1
-                for (int t = sub; t < T; t += G) {
-                    if (t < x.tl) {
-                        const int ty = t >> b.lgtx, tx = t & (b.tilesx - 1);
-                        const px_t *rp = rl + (ty * 4 * ys + tx * 4);
-                        const uint2 *sp = s.srcp + ((ty * 4) << b.lgtx) + tx;
-                        r.L += b.satd_mode ? tile_satd_p(sp, b.tilesx, rp, ys) : tile_sad_p(sp, b.tilesx, rp, ys);
-                    } else {
-                        const int ct0 = t - x.tl;
-                        const int pl = ct0 >= x.tcp;
-                        const int ct = ct0 - pl * x.tcp;
-                        const int ty = ct >> b.lgctx, tx = ct & (b.ctilesx - 1);
-                        if (ty * 4 >= b.crows) continue;
-                        const px_t *rp = (pl ? x.R.v : x.R.u) + cref + (ty * 4 * cs + tx * 4);
-                        const uint2 *sp = s.srcp + nlw + pl * b.ctilesx * b.crows + ((ty * 4) << b.lgctx) + tx;
-                        const unsigned v = x.satd ? tile_satd_p(sp, b.ctilesx, rp, cs) : tile_sad_p(sp, b.ctilesx, rp, cs);
-                        if (pl) r.V += v; else r.U += v;
-                    }
+                for (; t < x.tl; t += G) {
+                    const int ty = t >> b.lgtx, tx = t & (b.tilesx - 1);
+                    const px_t *rp = rl + (ty * 4 * ys + tx * 4);
+                    const uint2 *sp = s.srcp + ((ty * 4) << b.lgtx) + tx;
+                    r.L += b.satd_mode ? tile_satd_p(sp, b.tilesx, rp, ys) : tile_sad_p(sp, b.tilesx, rp, ys);
+                }
+#pragma unroll 1
+                for (; t < T; t += G) {
+                    const int ct0 = t - x.tl;
+                    const int pl = ct0 >= x.tcp;
+                    const int ct = ct0 - pl * x.tcp;
+                    const int ty = ct >> b.lgctx, tx = ct & (b.ctilesx - 1);
+                    if (ty * 4 >= b.crows) continue;
+                    const px_t *rp = (pl ? x.R.v : x.R.u) + cref + (ty * 4 * cs + tx * 4);
+                    const uint2 *sp = s.srcp + nlw + pl * b.ctilesx * b.crows + ((ty * 4) << b.lgctx) + tx;
+                    const unsigned v = x.satd ? tile_satd_p(sp, b.ctilesx, rp, cs) : tile_sad_p(sp, b.ctilesx, rp, cs);
+                    if (pl) r.V += v; else r.U += v;
                 }
             }
             group_sum3(r, G);

@@ -99,7 +99,7 @@ struct svpf_batch {
     int64_t scratch_per_cta = 0;
     int max_ctas = 0;          // scratch slots allocated
     int sms = 0;
-    int variant = 0, tiles_per_lane = 4, grid = 0;
+    int variant = 3, tiles_per_lane = 8, grid = 0;  // nt128_b3 until tuned
     std::string signature;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -430,13 +430,13 @@ int svpf_batch_autotune(svpf_batch *b, int32_t *variant, int32_t *tiles_per_lane
     };
     int rc = SVPF_OK;
     double best = -1.0;
-    int bv = 0, bt = 4;
+    int bv = 0, bt = 8;
     for (int v = 0; v < analyse_variant_count() && !rc; v++) {
         double r = 0;
-        rc = trial(v, 4, &r);
-        if (!rc && r > best) { best = r; bv = v; bt = 4; }
+        rc = trial(v, 8, &r);
+        if (!rc && r > best) { best = r; bv = v; bt = 8; }
     }
-    for (int t : {2, 8}) {
+    for (int t : {4, 2}) {
         if (rc) break;
         double r = 0;
         rc = trial(bv, t, &r);
