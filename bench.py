@@ -61,8 +61,8 @@ DESC = {
 }
 UNIT = "frame-pairs/s"
 # DRAM bytes per frame pair of the Analyse kernel at 1080p (ncu capture of a 17-pair launch:
-# 294.6 MB read + 55.2 MB written)
-TRAFFIC_PER_PAIR = 349.8e6 / 17
+# 291.6 MB read + 50.2 MB written)
+TRAFFIC_PER_PAIR = 341.8e6 / 17
 # int32 lanes per SM on sm_100 and the SM clock ceiling, for the nominal integer peak
 INT32_LANES_PER_SM = 128
 SM_MAX_MHZ = 1965.0
