@@ -26,6 +26,9 @@ Other workloads (one JSON line each, same keys):
   --workload 2160p10   a 3840x2160 10-bit clip (uint16 samples) of 120 frames, Super {pel:4},
                        Analyse block 8 / overlap 4 / exhaustive r8 / SATD + chroma; the CPU leg
                        and the parity check use the oracle's uint16 build.
+  --workload render    SmoothFps's single-warp render (algorithm 2, no masks) of 32 1080p frames
+                       from their pel-2 super frames and vector planes; frames/s, CPU leg = the
+                       oracle's render on all host threads, every frame compared.
   --workload served    Poisson arrivals of clips (360p..2160p, 8-600 frames) into the
                        continuous-batching server under an HBM budget, at each --rates value;
                        p50 / p99 per-frame-pair latency (arrival of the clip to its payload in
@@ -243,6 +246,166 @@ def _max_over_ranks(torch, dist, world, v: float, dev) -> float:
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def run_render(args, world: int, rank: int, local: int):
+    """SmoothFps's single-warp render (algorithm 2, interpolated motion, no masks) of 1080p frames on
+    the device: sources are the clip's pel-2 super frames, motion the vector planes of its own Analyse
+    payloads (both made on the device first, untimed). One step renders every frame's three planes;
+    `value` = frames/s. The CPU leg runs the oracle's render on the same frames, all host threads."""
+    torch, dist = _init_dist(world, local)
+    import concurrent.futures
+
+    import svpflow_b200 as sv
+    from oracle import oracle as orc
+
+    c = CONFIGS["1080p"]
+    w, h = c["width"], c["height"]
+    nf = args.frames or 32
+    dev = torch.device("cuda", local)
+    clip = make_clip(w, h, nf + 1, seed=1000 + rank, motion=c["motion"], objects=c["objects"],
+                     object_motion=c["object_motion"])
+    sb = sv.Super(w, h, SUPER_OPT["1080p"])
+    an = sv.Analyse(sb.sdata, ANALYSE_OPT["1080p"], w, h)
+    fb, pl = sb.output_len(), an.payload_len()
+    frames_d = torch.from_numpy(clip).to(dev)
+    sup_d = torch.empty((nf + 1, fb), dtype=torch.uint8, device=dev)
+    pay_d = torch.empty((nf, pl), dtype=torch.uint8, device=dev)
+    scr_d = torch.empty(an.scratch_bytes(nf), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    sb.build_device(frames_d.data_ptr(), sup_d.data_ptr(), nf + 1, sh)
+    an.analyse_clip_device(sup_d.data_ptr(), nf + 1, 0, nf, pay_d.data_ptr(), scr_d.data_ptr(), sh)
+    vd = an.vector_header()
+    mw, mh = sv.vector_grid(vd)
+    planes = torch.empty((nf, 4 * mw * mh), dtype=torch.int16, device=dev)
+    status = torch.zeros(nf, dtype=torch.int32, device=dev)
+    sv.vector_planes_device(vd, pay_d.data_ptr(), pl, nf, w, h, planes.data_ptr(), status.data_ptr(), stream=sh)
+    del scr_d
+    torch.cuda.synchronize()
+    hs = sb.super_height
+    offs = [0, w * hs, w * hs + (w // 2) * (hs // 2)]
+    lens = [w * hs, (w // 2) * (hs // 2), (w // 2) * (hs // 2)]
+    strides = [w, w // 2, w // 2]
+    cfg = dict(width=w, height=h, block_w=vd[2], block_h=vd[3], origin_x=vd[2] // 2, origin_y=vd[3] // 2,
+               grid_w=mw, grid_h=mh, source_step=2)
+    thr = 128
+    out_d = torch.empty((nf, w * h * 3 // 2), dtype=torch.uint8, device=dev)
+    dst_offs = [0, w * h, w * h + (w // 2) * (h // 2)]
+
+    def render(f, src_base, mot_base, dst_base, st):
+        sv.render_warp_device(cfg, thr, False, True, [src_base + o for o in offs], strides, lens, 1, mot_base,
+                              mot_base + mw * mh * 2, [dst_base + o for o in dst_offs], strides, st)
+
+    def step(st):
+        for f in range(nf):
+            render(f, sup_d[f].data_ptr(), planes[f].data_ptr(), out_d[f].data_ptr(), st)
+
+    for _ in range(args.warmup):
+        step(sh)
+    torch.cuda.synchronize()
+    # one render per frame is a short kernel: the step's launches go into a CUDA graph, replayed
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        step(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(_gpu_id(torch, local)) as clk:
+        for e0, e1 in evs:
+            flush.fill_(1)  # inputs partly below L2 size: flush between steps, outside the events
+            e0.record(stream)
+            graph.replay()
+            e1.record(stream)
+        torch.cuda.synchronize()
+    launches = nf * args.steps  # one render_warp_kernel per frame in every replay
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    ms_max = _max_over_ranks(torch, dist, world, ms, dev)
+    value = nf * world * args.steps / (ms_max / 1000.0)
+    # end to end: host super frames and motion planes in, rendered frames out, per step
+    sup_h = torch.empty((nf, fb), dtype=torch.uint8).pin_memory()
+    sup_h.copy_(sup_d[:nf])
+    mot_h = torch.empty_like(planes, device="cpu").pin_memory()
+    mot_h.copy_(planes)
+    out_h = torch.empty((nf, w * h * 3 // 2), dtype=torch.uint8).pin_memory()
+    sup_s = torch.empty((2, fb), dtype=torch.uint8, device=dev)
+    mot_s = torch.empty((2, planes.shape[1]), dtype=torch.int16, device=dev)
+    out_s = torch.empty((2, w * h * 3 // 2), dtype=torch.uint8, device=dev)
+
+    def e2e_step():
+        for f in range(nf):
+            k = f & 1
+            sup_s[k].copy_(sup_h[f], non_blocking=True)
+            mot_s[k].copy_(mot_h[f], non_blocking=True)
+            render(f, sup_s[k].data_ptr(), mot_s[k].data_ptr(), out_s[k].data_ptr(), sh)
+            out_h[f].copy_(out_s[k], non_blocking=True)
+        torch.cuda.synchronize()
+
+    e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(max(args.e2e_steps, 1)):
+        e2e_step()
+    e2e_s = _max_over_ranks(torch, dist, world, time.perf_counter() - t0, dev)
+    e2e_value = nf * world * max(args.e2e_steps, 1) / e2e_s
+    same = bool(torch.equal(out_h.to(dev), out_d))
+    line = None
+    if rank == 0:
+        out_np = out_d.cpu().numpy()
+        sup_np = sup_d[:nf].cpu().numpy()
+        mot_np = planes.cpu().numpy().view(np.uint16).reshape(nf, 4, mh * mw)
+        _, lut = orc.render_luts(thr)
+        ocfg = dict(cfg, chroma_y_div=2)
+
+        def cpu_frame(f):
+            res = []
+            for p in range(3):
+                ph = h // (2 if p else 1)
+                src = sup_np[f][offs[p]: offs[p] + lens[p]]
+                res.append(orc.render_warp_plane(ocfg, p > 0, True, lut, src, strides[p], strides[p] * ph, 1,
+                                                 mot_np[f][0], mot_np[f][1], strides[p], ph))
+            return res
+
+        cpu, parity = None, None
+        if not args.no_cpu:
+            threads = os.cpu_count() or 1
+            t0 = time.perf_counter()
+            with concurrent.futures.ThreadPoolExecutor(threads) as ex:
+                res = list(ex.map(cpu_frame, range(nf)))
+            dt = time.perf_counter() - t0
+            cpu = {"value": nf / dt, "unit": "frames/s", "cores": threads, "kind": "port",
+                   "sample": f"the same {nf} frames, 3 planes each, oracle/ C restatement of renderer.rs's scalar "
+                             f"render, one frame per host thread", "cpu_model": _cpu_model()}
+            ok = all(np.array_equal(np.concatenate([r.reshape(-1) for r in res[f]]), out_np[f]) for f in range(nf))
+            parity = {"frames_checked": nf, "bit_exact": bool(ok)}
+        peak, peak_kind = _peaks()
+        per_frame = 2 * w * h * 3 // 2 + 2 * mw * mh * 2  # sources read once + frame written + one motion set
+        line = {
+            "metric": "SmoothFps single-warp render frames/s at 1080p (bit-exact to the oracle)", "value": value,
+            "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8", "data": "synthetic",
+            "config": {"workload": f"1080p, {nf} frames per step, algorithm 2 (render_mode1_or_2 without masks), "
+                                   f"interpolated motion, threshold {thr}, sources = pel-2 super frames, motion = "
+                                   f"the clip's own vector planes; a step = one CUDA-graph replay of the "
+                                   f"{nf} launches", "frames_per_gpu": nf,
+                       "l2": "a 256 MB write flushes L2 before every step, outside the timed events"},
+            "clocks": clk.summary(),
+            "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": int(nf * (fb + planes.shape[1] * 2)),
+                    "d2h_bytes_per_step": int(nf * w * h * 3 // 2), "api": "svpf_render_warp_device with host copies",
+                    "matches_device_path": same},
+            "gpu_launches": int(launches),
+            "roofline": {"kernel": "render_warp_kernel", "bound": "hbm",
+                         "achieved": per_frame * nf / (ms / args.steps / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": per_frame * nf / (ms / args.steps / 1000) / 1e9 / peak, "traffic": None,
+                         "peak_source": peak_kind, "algorithmic_bytes_per_frame": per_frame,
+                         "note": "one launch per frame (3 planes): two dependent gathers per sample (motion, then "
+                                 "the displaced source), latency-bound"},
+            "cpu_baseline": cpu, "parity_vs_oracle": parity,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_2160p10(args, world: int, rank: int, local: int):
@@ -615,7 +778,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-pairs", type=int, default=0, help="CPU baseline sample (0 = one per host thread)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="1080p", choices=["1080p", "640x360", "2160p10", "batched", "served"])
+    ap.add_argument("--workload", default="1080p",
+                    choices=["1080p", "640x360", "2160p10", "batched", "served", "render"])
     ap.add_argument("--clips", type=int, default=0, help="batched: clips (default 64); served: clips per rate (16)")
     ap.add_argument("--max-len", type=int, default=0, help="longest clip in frames (default: the workload's)")
     ap.add_argument("--rates", default="5,50,200", help="served: arrival rates, clips/s")
@@ -636,6 +800,8 @@ def main():
         return run_served(args, world, rank, local)
     if args.workload == "2160p10":
         return run_2160p10(args, world, rank, local)
+    if args.workload == "render":
+        return run_render(args, world, rank, local)
     global WORKLOAD, METRIC
     if args.workload == "640x360":
         WORKLOAD, METRIC = "640x360", "Analyse frame-pairs/s at 640x360 (bit-exact MVs)"

@@ -20,7 +20,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 CORE = os.path.join(LIB_DIR, "libsvpflow_b200.so")
 SOURCES = ["analyse_nt128.cu", "analyse_nt64.cu", "analyse_nt32.cu", "analyse_nt128b3.cu", "analyse_nt64b6.cu",
            "analyse_nt128p16.cu", "variants.cpp", "params.cpp", "super.cu", "opts.cpp", "capi.cpp", "noalloc.cu",
-           "batch.cpp", "serve.cpp", "vectors.cu"]
+           "batch.cpp", "serve.cpp", "vectors.cu", "render.cu"]
 OBJ_DIR = os.path.join(LIB_DIR, "obj")
 # the VapourSynth plugin: the reference plugin's exports over the same objects
 VS_PLUGIN = os.path.join(LIB_DIR, "libsvpflow1_vs.so")

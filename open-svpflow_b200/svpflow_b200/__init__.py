@@ -39,6 +39,12 @@ _lib = None
 _VP = ctypes.c_void_p
 
 
+class RenderConfig(ctypes.Structure):
+    """svpf_render_config: renderer.rs CpuConfig as SmoothFps fills it."""
+    _fields_ = [(f, ctypes.c_int32) for f in ("width", "height", "block_w", "block_h", "origin_x", "origin_y",
+                                               "grid_w", "grid_h", "source_step")]
+
+
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
@@ -101,6 +107,8 @@ def lib() -> ctypes.CDLL:
             "svpf_server_stats": (None, [_VP, P(I64), P(I64), P(I64), P(I32), P(I64)]),
             "svpf_vector_grid": (I32, [P(I32), P(I32), P(I32)]),
             "svpf_vector_planes_device": (I32, [P(I32), _VP, SZ, I32, I32, I32, I32, _VP, _VP, _VP]),
+            "svpf_render_warp_device": (I32, [P(RenderConfig), I32, I32, I32, P(_VP), P(I64), P(I64), I32, _VP, _VP,
+                                              P(_VP), P(I64), _VP]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -478,3 +486,15 @@ def vector_planes_device(vdata, payloads_ptr: int, payload_len: int, npayloads: 
     v = (ctypes.c_int32 * 16)(*vdata)
     _check(lib().svpf_vector_planes_device(v, payloads_ptr, payload_len, npayloads, frame_w, frame_h, int(raw),
                                            planes_ptr, status_ptr, stream))
+
+
+def render_warp_device(cfg: dict, threshold: int, mode1: bool, interp: bool, src_ptrs, src_strides, src_lens,
+                       src_shift: int, motion_x_ptr: int, motion_y_ptr: int, dst_ptrs, dst_strides, stream: int = 0):
+    """SmoothFps's single-warp render (algorithms 1 / 2, no masks) of one frame's three planes on
+    the device; see svpf_render_warp_device."""
+    c = RenderConfig(**{k: int(cfg[k]) for k, _ in RenderConfig._fields_})
+    arr = lambda t, v: (t * 3)(*[int(x) for x in v])
+    _check(lib().svpf_render_warp_device(ctypes.byref(c), int(threshold), int(mode1), int(interp),
+                                         arr(_VP, src_ptrs), arr(ctypes.c_int64, src_strides),
+                                         arr(ctypes.c_int64, src_lens), int(src_shift), motion_x_ptr, motion_y_ptr,
+                                         arr(_VP, dst_ptrs), arr(ctypes.c_int64, dst_strides), stream))

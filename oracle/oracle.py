@@ -360,6 +360,17 @@ class AnalyseOpts(ctypes.Structure):
                  "refine_satd", "sort")]
 
 
+class RenderConfig(ctypes.Structure):
+    """or_render_config: renderer.rs CpuConfig without the mask scale."""
+    _fields_ = [(f, ctypes.c_int32) for f in ("width", "height", "block_w", "block_h", "origin_x", "origin_y",
+                                               "grid_w", "grid_h", "chroma_y_div", "source_step")]
+
+
+class RPlane(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("len", ctypes.c_size_t), ("stride", ctypes.c_size_t),
+                ("span", ctypes.c_size_t), ("shift", ctypes.c_uint32)]
+
+
 class Vec8(ctypes.Structure):
     _fields_ = [("dx", ctypes.c_int16), ("dy", ctypes.c_int16), ("score", ctypes.c_uint32),
                 ("luma", ctypes.c_uint8), ("pad", ctypes.c_uint8 * 3)]
@@ -441,6 +452,11 @@ def _setup(L):
     L.or_block_cost_lc.argtypes = [P(Planes), P(Planes)] + [ctypes.c_int32] * 9 + [P(ctypes.c_uint32), P(ctypes.c_uint32)]
     L.or_last_counters.argtypes = [P(ctypes.c_uint64)]
     L.or_total_counters.argtypes = [P(ctypes.c_uint64), ctypes.c_int32]
+    if hasattr(L, "or_render_luts"):  # the 8-bit build only
+        L.or_render_luts.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
+        L.or_render_warp_plane.argtypes = [P(RenderConfig), ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                           P(RPlane), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                           ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
     for f in ("or_reduce_dim", "or_auto_levels", "or_super_plane_height", "or_auto_search_levels"):
         getattr(L, f).argtypes = [ctypes.c_int32] * {"or_reduce_dim": 2, "or_auto_levels": 2,
                                                        "or_super_plane_height": 4, "or_auto_search_levels": 6}[f]
@@ -713,3 +729,30 @@ def analyse_clip16(ao: AnalyseOpts, so: SuperOpts, supers: np.ndarray, first: in
     if rc:
         raise RuntimeError("the search indexes out of range on this input (the reference's panic)")
     return out
+
+
+# ---- SmoothFps single-warp render (renderer.rs render_mode1_or_2 without masks)
+def render_luts(threshold: int):
+    """CpuRenderer::set_threshold: (inverse_lut, threshold_lut), int16[2048] each."""
+    inv = np.zeros(2048, dtype=np.int16)
+    thr = np.zeros(2048, dtype=np.int16)
+    lib().or_render_luts(int(threshold), _ptr(inv), _ptr(thr))
+    return inv, thr
+
+
+def render_warp_plane(cfg: dict, chroma: bool, interp: bool, lut: np.ndarray, src: np.ndarray, src_stride: int,
+                      src_span: int, src_shift: int, mx: np.ndarray, my: np.ndarray, dst_stride: int,
+                      dst_rows: int) -> np.ndarray:
+    """render_selected_warp_rows over a whole plane: uint8 [dst_rows, dst_stride] (bytes the reference
+    leaves untouched stay 0)."""
+    c = RenderConfig(**{k: int(cfg[k]) for k, _ in RenderConfig._fields_})
+    src = np.ascontiguousarray(src, dtype=np.uint8).reshape(-1)
+    mx = np.ascontiguousarray(mx, dtype=np.uint16).reshape(-1)
+    my = np.ascontiguousarray(my, dtype=np.uint16).reshape(-1)
+    lut = np.ascontiguousarray(lut, dtype=np.int16)
+    assert mx.size == my.size and lut.size == 2048
+    pl = RPlane(src.ctypes.data, src.size, src_stride, src_span, src_shift)
+    dst = np.zeros(dst_rows * dst_stride, dtype=np.uint8)
+    lib().or_render_warp_plane(ctypes.byref(c), int(chroma), int(interp), _ptr(lut), ctypes.byref(pl), _ptr(mx),
+                               _ptr(my), mx.size, _ptr(dst), dst_stride, dst.size)
+    return dst.reshape(dst_rows, dst_stride)

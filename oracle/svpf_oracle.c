@@ -1897,3 +1897,204 @@ int or_vector_planes(const int32_t vdata[16], const uint8_t *p, size_t len, int3
     free(pvx); free(pvy); free(cx); free(cy);
     return rc;
 }
+
+/* ------------------------------------------------------------------ SmoothFps single-warp render */
+/* crates/svpflow-core/src/renderer.rs, 8-bit samples: CpuRenderer::render_mode1_or_2 (:308-328)
+ * through render_selected_warp_rows (:876-984) without masks, with its helpers: cpu_map
+ * (:3186-3193), set_threshold (:238-250), plane_params (:1539-1606), motion_samples
+ * (:1608-1638), render_tiles (:1925-2010), interpolate_row / interpolate_motion_row /
+ * interpolate_motion (:2582-2637), interp_pair (:2724-2738), interpolation_weights / coeff
+ * (:2740-2770), plane_covers / plane_index / plane_index_checked (:2772-2803), tile_interior
+ * (:2809-2835), sample_plane (:2837-2861), output_row (:2894-2906). The scalar loop is the
+ * definition followed here. On x86-64 the reference takes its SSE warp_tile (:2090-2349) for
+ * interpolated tiles instead: it multiplies the vertical pass in wrapping 16-bit lanes and keeps
+ * the low 16 bits of the horizontal result, which equals the 32-bit scalar arithmetic whenever
+ * |motion| <= 1024 and the weights are <= 32 (LUT entries are trunc((-1024..1023) * t / 256), so
+ * every threshold in 0..256 stays within it). */
+#ifndef OR_PX16
+static const int32_t r_cpu_map[32] = {0, 1, 2, 2, -1, 3, 3, 3, -1, -1, -1, 4, -1, 4, -1, 4,
+                                      -1, -1, -1, -1, -1, -1, -1, -1, 5, -1, -1, -1, 5, -1, -1, 5};
+static int32_t r_map(int32_t v) {
+    int64_t i = (int64_t)v - 1;
+    return (i >= 0 && i < 32) ? r_cpu_map[i] : -1;
+}
+static int16_t r_div256(int32_t v) {
+    int32_t q = v / 256;
+    return (int16_t)(q < -32768 ? -32768 : (q > 32767 ? 32767 : q));
+}
+void or_render_luts(int32_t threshold, int16_t inverse_lut[2048], int16_t threshold_lut[2048]) {
+    int32_t inverse = sat_i64_to_i32((int64_t)256 - threshold);
+    for (int32_t k = 0; k < 2048; k++) {
+        int32_t sample = k - 1024;
+        inverse_lut[k] = r_div256(sat_mul_i32(sample, inverse));
+        threshold_lut[k] = r_div256(sat_mul_i32(sample, threshold));
+    }
+}
+
+typedef struct {
+    i32 width, height, block_w, block_h, origin_x, origin_y, x_shift, y_shift, x_div, y_div, step, max_x, max_y;
+    i32 xw[32][2], yw[32][2];
+} rparams;
+
+static void r_weights(i32 total, i32 shift, i32 w[32][2]) {
+    memset(w, 0, sizeof(i32) * 64);
+    if (total <= 0) return;
+    i32 scale = (shift < 0 ? 0 : shift) >= 32 ? 0 : (i32)(1u << (shift < 0 ? 0 : shift));
+    for (i32 p = 0; p < total && p < 32; p++) {
+        if (shift < 0) { w[p][0] = total - p; w[p][1] = p; }
+        else if (scale == 0) { w[p][0] = 1; w[p][1] = 0; }
+        else {
+            w[p][0] = f64_as_i32(ceil((double)(i32)((u32)(total - p) * (u32)scale) / (double)total - 0.5));
+            w[p][1] = f64_as_i32(ceil((double)(i32)((u32)p * (u32)scale) / (double)total - 0.5));
+        }
+    }
+}
+static i32 r_satsub1_max0(i32 a, i32 b) { /* a.saturating_mul(b).saturating_sub(1).max(0) */
+    i32 m = sat_mul_i32(a, b);
+    i32 s = sat_i64_to_i32((int64_t)m - 1);
+    return s > 0 ? s : 0;
+}
+static void r_params(const or_render_config *c, int chroma, int zero_origin, rparams *p) {
+    i32 cd = c->chroma_y_div;
+    p->origin_x = zero_origin ? 0 : (chroma ? c->origin_x / 2 : c->origin_x);
+    p->origin_y = zero_origin ? 0 : (chroma ? c->origin_y / cd : c->origin_y);
+    p->step = c->source_step;
+    if (chroma) {
+        p->width = c->width / 2; p->height = c->height / cd;
+        p->block_w = c->block_w / 2; p->block_h = c->block_h / cd;
+        p->x_shift = r_map(c->block_w / 2); p->y_shift = r_map(c->block_h / 2);
+        p->x_div = 2; p->y_div = cd;
+        p->max_x = r_satsub1_max0(c->width / 2, c->source_step);
+        p->max_y = r_satsub1_max0(c->height / cd, c->source_step);
+        r_weights(c->block_w / 2, p->x_shift, p->xw);
+        r_weights(c->block_h / cd, p->y_shift, p->yw);
+    } else {
+        p->width = c->width; p->height = c->height;
+        p->block_w = c->block_w; p->block_h = c->block_h;
+        p->x_shift = r_map(c->block_w); p->y_shift = r_map(c->block_h);
+        p->x_div = 1; p->y_div = 1;
+        p->max_x = r_satsub1_max0(c->width, c->source_step);
+        p->max_y = r_satsub1_max0(c->height, c->source_step);
+        r_weights(c->block_w, p->x_shift, p->xw);
+        r_weights(c->block_h, p->y_shift, p->yw);
+    }
+}
+static usize r_index(const or_rplane *pl, usize x, usize y) {
+    if (pl->shift == 0) return y * pl->stride + x;
+    usize mask = ((usize)1 << pl->shift) - 1;
+    usize sub = ((y & mask) << pl->shift) | (x & mask);
+    return sub * pl->span + (y >> pl->shift) * pl->stride + (x >> pl->shift);
+}
+static int r_covers(const or_rplane *pl, const rparams *p) {
+    if (pl->shift != 0 && (pl->shift >= 32 || (i32)(1u << pl->shift) != p->step)) return 0;
+    usize x = (usize)p->max_x, y = (usize)p->max_y;
+    unsigned __int128 idx;
+    if (pl->shift == 0) idx = (unsigned __int128)y * pl->stride + x;
+    else {
+        usize mask = ((usize)1 << pl->shift) - 1;
+        usize sub = ((y & mask) << pl->shift) | (x & mask);
+        idx = (unsigned __int128)sub * pl->span + (unsigned __int128)(y >> pl->shift) * pl->stride + (x >> pl->shift);
+    }
+    return idx < (unsigned __int128)pl->len;
+}
+static i32 r_interp(i32 a, i32 b, i32 total, i32 shift, const i32 w[2]) {
+    i32 s = (i32)((u32)w[0] * (u32)a + (u32)w[1] * (u32)b);
+    if (shift < 0) return total ? s / total : 0;
+    return s >> shift;
+}
+static i32 r_motion(const int16_t *lut, const uint16_t *plane, usize len, usize i) {
+    usize k = i < len ? plane[i] : 1024;
+    return lut[k < 2047 ? k : 2047];
+}
+
+void or_render_warp_plane(const or_render_config *c, int32_t chroma, int32_t interp, const int16_t *lut,
+                          const or_rplane *src, const uint16_t *mx, const uint16_t *my, size_t mlen, uint8_t *dst,
+                          size_t dst_stride, size_t dst_len) {
+    rparams P;
+    r_params(c, chroma, !interp, &P);
+    const rparams *p = &P;
+    i32 gw = (i32)c->grid_w, gh = (i32)c->grid_h;
+    if (p->width <= 0 || p->height <= 0 || p->block_w <= 0 || p->block_h <= 0 || gw <= 0 || gh <= 0) return;
+    i32 rows_end = chroma ? c->height / c->chroma_y_div : c->height;
+    for (i32 gy = -1; gy < gh; gy++) {
+        i32 base_y = gy < 0 ? 0 : p->origin_y + p->block_h * gy;
+        i32 height = gy < 0 ? p->origin_y : p->block_h;
+        if (base_y + p->block_h >= p->height || gy == gh - 1) height = p->height - base_y;
+        i32 end_y = base_y + height < rows_end ? base_y + height : rows_end;
+        i32 clipped_y = base_y > 0 ? base_y : 0;
+        height = end_y - clipped_y;
+        if (height <= 0) continue;
+        for (i32 gx = -1; gx < gw; gx++) {
+            i32 base_x = gx < 0 ? 0 : p->origin_x + p->block_w * gx;
+            i32 width = gx < 0 ? p->origin_x : p->block_w;
+            if (base_x + p->block_w >= p->width || gx == gw - 1) width = p->width - base_x;
+            if (width <= 0) continue;
+            usize x0 = (usize)(gx > 0 ? gx : 0), y0 = (usize)(gy > 0 ? gy : 0);
+            usize nx = (gx >= 0 && gx != gw - 1) ? 1 : 0, ny = (gy >= 0 && gy != gh - 1) ? (usize)gw : 0;
+            usize i00 = y0 * (usize)gw + x0, i01 = i00 + nx, i10 = i00 + ny, i11 = i00 + ny + nx;
+            i32 tx = base_x, ty = clipped_y, local_y0 = clipped_y - base_y;
+            /* motion_samples */
+            i32 sx[4], sy[4];
+            sx[0] = r_motion(lut, mx, mlen, i00) / p->x_div;
+            sy[0] = r_motion(lut, my, mlen, i00) / p->y_div;
+            if (!interp) { for (int q = 1; q < 4; q++) { sx[q] = sx[0]; sy[q] = sy[0]; } }
+            else {
+                usize ii[4] = {i00, i01, i10, i11};
+                for (int q = 1; q < 4; q++) {
+                    sx[q] = r_motion(lut, mx, mlen, ii[q]) / p->x_div;
+                    sy[q] = r_motion(lut, my, mlen, ii[q]) / p->y_div;
+                }
+            }
+            int covers = r_covers(src, p);
+            int direct = 0;
+            if (covers && p->step > 0) { /* tile_interior */
+                i32 mnx = INT32_MAX, mxx = INT32_MIN, mny = INT32_MAX, mxy = INT32_MIN;
+                for (int q = 0; q < 4; q++) {
+                    mnx = sx[q] < mnx ? sx[q] : mnx; mxx = sx[q] > mxx ? sx[q] : mxx;
+                    mny = sy[q] < mny ? sy[q] : mny; mxy = sy[q] > mxy ? sy[q] : mxy;
+                }
+                int64_t st = p->step;
+                direct = (int64_t)tx * st + mnx >= 0 && (int64_t)ty * st + mny >= 0 &&
+                         (int64_t)(tx + width - 1) * st + mxx <= p->max_x && (int64_t)(ty + height - 1) * st + mxy <= p->max_y;
+            }
+            for (i32 y = 0; y < height; y++) {
+                i32 local_y = local_y0 + y;
+                i32 source_y = (ty + y) * p->step;
+                usize row = (usize)(ty + y); /* row_start = 0 */
+                usize start = row * dst_stride + (usize)tx;
+                if (start + (usize)width > dst_len) continue; /* output_row */
+                i32 rx[2], ry[2];
+                if (!interp) { rx[0] = rx[1] = sx[0]; ry[0] = ry[1] = sy[0]; }
+                else {
+                    const i32 *wy = p->yw[local_y < 0 ? 0 : (local_y > 31 ? 31 : local_y)];
+                    rx[0] = r_interp(sx[0], sx[2], p->block_h, p->y_shift, wy);
+                    rx[1] = r_interp(sx[1], sx[3], p->block_h, p->y_shift, wy);
+                    ry[0] = r_interp(sy[0], sy[2], p->block_h, p->y_shift, wy);
+                    ry[1] = r_interp(sy[1], sy[3], p->block_h, p->y_shift, wy);
+                }
+                for (i32 x = 0; x < width; x++) {
+                    i32 px = tx + x, source_x = px * p->step;
+                    const i32 *wx = p->xw[x > 31 ? 31 : x];
+                    i32 dx = rx[0], dy = ry[0];
+                    if (interp) {
+                        dx = r_interp(rx[0], rx[1], p->block_w, p->x_shift, wx);
+                        dy = r_interp(ry[0], ry[1], p->block_w, p->x_shift, wx);
+                    }
+                    i32 xs = source_x + dx, ys = source_y + dy;
+                    uint8_t v;
+                    if (direct) {
+                        usize idx = r_index(src, (usize)(int64_t)xs, (usize)(int64_t)ys);
+                        v = idx < src->len ? src->data[idx] : 0; /* in range by tile_interior + plane_covers */
+                    } else {
+                        xs = xs < 0 ? 0 : (xs > p->max_x ? p->max_x : xs);
+                        ys = ys < 0 ? 0 : (ys > p->max_y ? p->max_y : ys);
+                        usize idx = r_index(src, (usize)xs, (usize)ys);
+                        v = idx < src->len ? src->data[idx] : 0;
+                    }
+                    dst[start + (usize)x] = v;
+                }
+            }
+        }
+    }
+}
+#endif

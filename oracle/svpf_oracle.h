@@ -175,6 +175,21 @@ void or_build_super_many(const or_super_opts *o, const or_px *const *src, or_px 
 void or_vector_grid(const int32_t vdata[16], int32_t *mw, int32_t *mh);
 /* decode_vectors + vector_planes for both sets; out = mvx0 | mvy0 | mvx1 | mvy1 (mw x mh each);
  * returns -1 when the payload does not decode (the reference's None). */
+/* ---- SmoothFps single-warp render (renderer.rs render_mode1_or_2 without masks), 8-bit ---- */
+typedef struct {
+    int32_t width, height, block_w, block_h, origin_x, origin_y, grid_w, grid_h, chroma_y_div, source_step;
+} or_render_config;
+/* A source plane: linear (shift 0) or a super clip's level 0 with its 2^shift x 2^shift sub-planes
+ * `span` bytes apart (renderer.rs Plane::super_plane). */
+typedef struct {
+    const uint8_t *data;
+    size_t len, stride, span;
+    uint32_t shift;
+} or_rplane;
+void or_render_luts(int32_t threshold, int16_t inverse_lut[2048], int16_t threshold_lut[2048]);
+void or_render_warp_plane(const or_render_config *c, int32_t chroma, int32_t interp, const int16_t *lut,
+                          const or_rplane *src, const uint16_t *mx, const uint16_t *my, size_t mlen, uint8_t *dst,
+                          size_t dst_stride, size_t dst_len);
 int or_vector_planes(const int32_t vdata[16], const uint8_t *payload, size_t len, int32_t frame_w, int32_t frame_h,
                      int32_t raw, uint16_t *out);
 

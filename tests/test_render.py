@@ -1,0 +1,322 @@
+"""SmoothFps's single-warp frame render (renderer.rs render_mode1_or_2 without masks).
+
+CPU: the oracle's C restatement against properties of the render (identity, whole-plane shifts,
+super-clip sub-planes) and against a second, independent restatement in Python written from the
+reference's scalar loop (small frames). GPU: svpf_render_warp_device through the C ABI against the
+oracle, bit-exact, over frame and block sizes, thresholds, both modes, interpolation on and off,
+plain and super-clip sources, and after the whole device chain (Super, Analyse, vector planes).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+CPU_MAP = [0, 1, 2, 2, -1, 3, 3, 3, -1, -1, -1, 4, -1, 4, -1, 4, -1, -1, -1, -1, -1, -1, -1, -1, 5, -1, -1, -1, 5,
+           -1, -1, 5]
+
+
+def _cfg(w, h, bw, bh, gw, gh, step=1, ox=None, oy=None):
+    return dict(width=w, height=h, block_w=bw, block_h=bh, origin_x=bw // 2 if ox is None else ox,
+                origin_y=bh // 2 if oy is None else oy, grid_w=gw, grid_h=gh, chroma_y_div=2, source_step=step)
+
+
+def _grid(w, h, bw, bh):
+    """The motion grid of a vector field of bw x bh blocks at half-block steps (extended_grid)."""
+    sx, sy = bw // 2, bh // 2
+    gw, gh = max((w - bw) // sx + 1, 1), max((h - bh) // sy + 1, 1)
+    return gw + ((bw - sx) * gw + sx < w), gh + ((bh - sy) * gh + sy < h)
+
+
+# ---------------------------------------------------------------- a second restatement (Python)
+def _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my):
+    """render_selected_warp_rows, scalar loop (renderer.rs:876-984), in plain Python."""
+    cmap = lambda v: CPU_MAP[v - 1] if 1 <= v <= 32 else -1
+    cd = cfg["chroma_y_div"]
+    zero = not interp
+    if chroma:
+        W, H, BW, BH = cfg["width"] // 2, cfg["height"] // cd, cfg["block_w"] // 2, cfg["block_h"] // cd
+        ox, oy = (0, 0) if zero else (cfg["origin_x"] // 2, cfg["origin_y"] // cd)
+        xs_, ys_ = cmap(cfg["block_w"] // 2), cmap(cfg["block_h"] // 2)
+        xd, yd = 2, cd
+    else:
+        W, H, BW, BH = cfg["width"], cfg["height"], cfg["block_w"], cfg["block_h"]
+        ox, oy = (0, 0) if zero else (cfg["origin_x"], cfg["origin_y"])
+        xs_, ys_ = cmap(BW), cmap(BH)
+        xd, yd = 1, 1
+    step = cfg["source_step"]
+    maxx, maxy = max(W * step - 1, 0), max(H * step - 1, 0)
+
+    def weights(total, sh):
+        out = [(0, 0)] * 32
+        scale = 1 << max(sh, 0)
+        for p in range(min(total, 32)):
+            if sh < 0:
+                out[p] = (total - p, p)
+            else:
+                c = lambda v: int(math.ceil(v * scale / total - 0.5))
+                out[p] = (c(total - p), c(p))
+        return out
+
+    xw, yw = weights(BW, xs_), weights(BH, ys_)
+
+    def ip(a, b, total, sh, w):
+        s = w[0] * a + w[1] * b
+        return int(s / total) if sh < 0 else s >> sh
+
+    def mv(plane, i):
+        k = int(plane[i]) if i < len(plane) else 1024
+        return int(lut[min(k, 2047)])
+
+    def index(x, y):
+        if shift == 0:
+            return y * stride + x
+        m = (1 << shift) - 1
+        return (((y & m) << shift) | (x & m)) * span + (y >> shift) * stride + (x >> shift)
+
+    covers = (shift == 0 or (1 << shift) == step) and index(maxx, maxy) < len(src)
+    gw, gh = cfg["grid_w"], cfg["grid_h"]
+    dst = np.zeros((H, W), dtype=np.uint8)
+    tdiv = lambda a, b: int(a / b)
+    for gy in range(-1, gh):
+        by = 0 if gy < 0 else oy + BH * gy
+        th = oy if gy < 0 else BH
+        if by + BH >= H or gy == gh - 1:
+            th = H - by
+        th = min(by + th, H) - max(by, 0)
+        if th <= 0:
+            continue
+        for gx in range(-1, gw):
+            bx = 0 if gx < 0 else ox + BW * gx
+            tw = ox if gx < 0 else BW
+            if bx + BW >= W or gx == gw - 1:
+                tw = W - bx
+            if tw <= 0:
+                continue
+            i00 = max(gy, 0) * gw + max(gx, 0)
+            nx = 1 if (gx >= 0 and gx != gw - 1) else 0
+            ny = gw if (gy >= 0 and gy != gh - 1) else 0
+            idx = [i00, i00 + nx, i00 + ny, i00 + ny + nx]
+            sx = [tdiv(mv(mx, i), xd) for i in idx]
+            sy = [tdiv(mv(my, i), yd) for i in idx]
+            if not interp:
+                sx, sy = [sx[0]] * 4, [sy[0]] * 4
+            direct = covers and bx * step + min(sx) >= 0 and by * step + min(sy) >= 0 and \
+                (bx + tw - 1) * step + max(sx) <= maxx and (by + th - 1) * step + max(sy) <= maxy
+            for y in range(th):
+                wy = yw[min(y, 31)]
+                rx = [ip(sx[0], sx[2], BH, ys_, wy), ip(sx[1], sx[3], BH, ys_, wy)] if interp else [sx[0]] * 2
+                ry = [ip(sy[0], sy[2], BH, ys_, wy), ip(sy[1], sy[3], BH, ys_, wy)] if interp else [sy[0]] * 2
+                for x in range(tw):
+                    wx = xw[min(x, 31)]
+                    dx = ip(rx[0], rx[1], BW, xs_, wx) if interp else rx[0]
+                    dy = ip(ry[0], ry[1], BW, xs_, wx) if interp else ry[0]
+                    X, Y = (bx + x) * step + dx, (by + y) * step + dy
+                    if not direct:
+                        X, Y = min(max(X, 0), maxx), min(max(Y, 0), maxy)
+                    i = index(X, Y)
+                    dst[by + y, bx + x] = src[i] if i < len(src) else 0
+    return dst
+
+
+def _motion(rng, n, spread):
+    m = rng.integers(1024 - spread, 1024 + spread + 1, size=n).astype(np.uint16)
+    m[rng.random(n) < 0.1] = 1024
+    return m
+
+
+PY_CASES = [  # w, h, block, step (super clip pel), interp, threshold, mode1
+    (40, 24, 8, 1, True, 128, False),
+    (40, 24, 8, 1, False, 200, True),
+    (36, 22, 16, 1, True, 256, False),   # tiles stretched to the frame edge (weights past the block are 0)
+    (20, 12, 32, 1, True, 90, False),    # blocks larger than the frame: overlapping tiles
+    (32, 16, 8, 2, True, 160, True),     # half-pel super planes
+    (24, 16, 4, 4, False, 64, False),    # quarter-pel super planes
+]
+
+
+@pytest.mark.parametrize("case", range(len(PY_CASES)))
+def test_oracle_matches_python_restatement(case):
+    w, h, blk, step, interp, thr, mode1 = PY_CASES[case]
+    rng = np.random.default_rng(case)
+    gw, gh = _grid(w, h, blk, blk)
+    cfg = _cfg(w, h, blk, blk, gw, gh, step)
+    inv, tl = orc.render_luts(thr)
+    lut = inv if mode1 else tl
+    mx, my = _motion(rng, gw * gh, 40), _motion(rng, gw * gh, 40)
+    shift = {1: 0, 2: 1, 4: 2}[step]
+    for chroma in (False, True):
+        pw, ph = (w // 2, h // 2) if chroma else (w, h)
+        stride = pw + 3
+        src = rng.integers(0, 256, size=(step * step) * ph * stride, dtype=np.uint8)
+        span = stride * ph if shift else 0
+        got = orc.render_warp_plane(cfg, chroma, interp, lut, src, stride, span, shift, mx, my, pw, ph)
+        want = _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my)
+        assert np.array_equal(got, want), f"chroma {chroma}: {np.argwhere(got != want)[:3]}"
+
+
+def test_oracle_luts():
+    inv, thr = orc.render_luts(77)
+    s = np.arange(-1024, 1024)
+    assert np.array_equal(thr, np.trunc(s * 77 / 256).astype(np.int16))
+    assert np.array_equal(inv, np.trunc(s * (256 - 77) / 256).astype(np.int16))
+
+
+@pytest.mark.parametrize("interp", [False, True])
+def test_oracle_identity_and_shift(interp):
+    w, h, blk = 64, 48, 16
+    gw, gh = _grid(w, h, blk, blk)
+    cfg = _cfg(w, h, blk, blk, gw, gh)
+    rng = np.random.default_rng(3)
+    src = rng.integers(0, 256, size=(h, w), dtype=np.uint8)
+    neutral = np.full(gw * gh, 1024, np.uint16)
+    _, t128 = orc.render_luts(128)
+    assert np.array_equal(orc.render_warp_plane(cfg, False, interp, t128, src, w, 0, 0, neutral, neutral, w, h), src)
+    _, t256 = orc.render_luts(256)  # threshold 256: the motion is the vector itself
+    mx, my = np.full(gw * gh, 1024 + 5, np.uint16), np.full(gw * gh, 1024 - 3, np.uint16)
+    got = orc.render_warp_plane(cfg, False, interp, t256, src, w, 0, 0, mx, my, w, h)
+    ys = np.clip(np.arange(h)[:, None] - 3, 0, h - 1)
+    xs = np.clip(np.arange(w)[None, :] + 5, 0, w - 1)
+    assert np.array_equal(got, src[ys, xs])
+
+
+def test_oracle_super_subplanes():
+    # on a pel-2 super clip, a half-pel horizontal motion reads the h sub-plane at full-pel positions
+    w, h, blk = 64, 48, 16
+    so = orc.super_opts(w, h, "{pel:2}")
+    from svpflow_b200.synth import make_clip
+
+    frame = make_clip(w, h, 1, seed=5)[0]
+    sup = orc.build_super(so, frame)
+    gw, gh = _grid(w, h, blk, blk)
+    cfg = _cfg(w, h, blk, blk, gw, gh, step=2)
+    _, t256 = orc.render_luts(256)
+    mx, my = np.full(gw * gh, 1025, np.uint16), np.full(gw * gh, 1024, np.uint16)
+    luma = sup[: w * orc.super_height(so)]
+    got = orc.render_warp_plane(cfg, False, True, t256, luma, w, w * h, 1, mx, my, w, h)
+    hplane = luma[w * h: 2 * w * h].reshape(h, w)
+    assert np.array_equal(got, hplane)
+
+
+# ---------------------------------------------------------------- GPU
+GPU_CASES = [  # w, h, block, step, interp, threshold, mode1, source stride pad
+    (1920, 1080, 16, 1, True, 128, False, 0),
+    (1920, 1080, 16, 2, True, 96, True, 0),
+    (1920, 1080, 8, 1, False, 256, False, 64),
+    (640, 360, 32, 1, True, 200, True, 32),
+    (100, 60, 8, 4, True, 40, False, 12),
+    (66, 38, 16, 2, False, 0, True, 2),
+    (20, 12, 32, 1, True, 175, False, 0),
+    (1280, 720, 4, 1, True, 255, True, 0),
+]
+
+
+def _gpu_render_case(case, rng):
+    import torch
+
+    import svpflow_b200 as sv
+
+    w, h, blk, step, interp, thr, mode1, pad = case
+    gw, gh = _grid(w, h, blk, blk)
+    cfg = _cfg(w, h, blk, blk, gw, gh, step)
+    shift = {1: 0, 2: 1, 4: 2}[step]
+    mx, my = _motion(rng, gw * gh, 120), _motion(rng, gw * gh, 120)
+    inv, tl = orc.render_luts(thr)
+    lut = inv if mode1 else tl
+    srcs, wants, dsts = [], [], []
+    for pl in range(3):
+        pw, ph = (w // 2, h // 2) if pl else (w, h)
+        stride = pw + pad
+        src = rng.integers(0, 256, size=(step * step) * ph * stride, dtype=np.uint8)
+        span = stride * ph if shift else 0
+        wants.append(orc.render_warp_plane(cfg, pl > 0, interp, lut, src, stride, span, shift, mx, my, pw + 1, ph))
+        srcs.append((torch.from_numpy(src).cuda(), stride))
+        dsts.append((torch.full((ph, pw + 1), 7, dtype=torch.uint8, device="cuda"), pw + 1))
+    mxd = torch.from_numpy(mx.astype(np.int16)).cuda()
+    myd = torch.from_numpy(my.astype(np.int16)).cuda()
+    sv.render_warp_device(cfg, thr, mode1, interp, [s.data_ptr() for s, _ in srcs], [st for _, st in srcs],
+                          [s.numel() for s, _ in srcs], shift, mxd.data_ptr(), myd.data_ptr(),
+                          [d.data_ptr() for d, _ in dsts], [st for _, st in dsts])
+    torch.cuda.synchronize()
+    for pl in range(3):
+        got = dsts[pl][0].cpu().numpy()
+        want = wants[pl].copy()
+        want[:, -1] = 7  # the column past the plane's width is not written
+        assert np.array_equal(got, want), f"plane {pl}: {np.argwhere(got != want)[:3]}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(len(GPU_CASES)))
+def test_render_matches_oracle(case):
+    _gpu_render_case(GPU_CASES[case], np.random.default_rng(100 + case))
+
+
+@pytest.mark.gpu
+def test_render_after_device_chain():
+    """Super -> Analyse -> vector planes -> render, all on the device, against the oracle's chain."""
+    import torch
+
+    import svpflow_b200 as sv
+    from svpflow_b200.synth import make_clip
+
+    w, h, n = 320, 240, 3
+    sopt, aopt = "{pel:2}", "{block:{w:16,overlap:2},main:{search:{type:3,distance:8,satd:true}}}"
+    clip = make_clip(w, h, n, seed=21, motion=6, objects=2, object_motion=8)
+    sb = sv.Super(w, h, sopt)
+    an = sv.Analyse(sb.sdata, aopt, w, h)
+    so = orc.super_opts(w, h, sopt)
+    ao = orc.analyse_opts(orc.sdata(so), aopt, None, w, h)
+    sup_d = torch.empty((n, sb.output_len()), dtype=torch.uint8, device="cuda")
+    pay_d = torch.empty((n, an.payload_len()), dtype=torch.uint8, device="cuda")
+    scr_d = torch.empty(an.scratch_bytes(n), dtype=torch.uint8, device="cuda")
+    frames_d = torch.from_numpy(clip).cuda()
+    st = torch.cuda.current_stream().cuda_stream
+    sb.build_device(frames_d.data_ptr(), sup_d.data_ptr(), n, st)
+    an.analyse_clip_device(sup_d.data_ptr(), n, 0, n, pay_d.data_ptr(), scr_d.data_ptr(), st)
+    vd = an.vector_header()
+    mw, mh = sv.vector_grid(vd)
+    planes = torch.empty((n, 4 * mw * mh), dtype=torch.int16, device="cuda")
+    status = torch.zeros(n, dtype=torch.int32, device="cuda")
+    sv.vector_planes_device(vd, pay_d.data_ptr(), an.payload_len(), n, w, h, planes.data_ptr(), status.data_ptr())
+    torch.cuda.synchronize()
+    sup_h = orc.build_super_many(so, clip)
+    pays = orc.analyse_clip(ao, so, sup_h, 0, n)
+    hs = orc.super_height(so)
+    cfg = _cfg(w, h, vd[2], vd[3], mw, mh, step=2, ox=vd[2] // 2, oy=vd[3] // 2)
+    offs = [0, w * hs, w * hs + (w // 2) * (hs // 2)]
+    lens = [w * hs, (w // 2) * (hs // 2), (w // 2) * (hs // 2)]
+    strides = [w, w // 2, w // 2]
+    for f in range(n):
+        mp = orc.vector_planes(vd, pays[f], w, h)
+        assert np.array_equal(planes[f].cpu().numpy().view(np.uint16).reshape(4, mh, mw), mp)
+        for mode1, thr in ((False, 100), (True, 100)):
+            which = 1 if mode1 else 0  # mode 1 warps with the second set, mode 2 with the first
+            inv, tl = orc.render_luts(thr)
+            lut = inv if mode1 else tl
+            dsts = [torch.zeros((h // (2 if p else 1), w // (2 if p else 1)), dtype=torch.uint8, device="cuda")
+                    for p in range(3)]
+            base = sup_d[f].data_ptr()
+            mxp = planes[f].data_ptr() + (2 * which) * mw * mh * 2
+            myp = planes[f].data_ptr() + (2 * which + 1) * mw * mh * 2
+            sv.render_warp_device(cfg, thr, mode1, True, [base + o for o in offs], strides, lens, 1, mxp, myp,
+                                  [d.data_ptr() for d in dsts], strides)
+            torch.cuda.synchronize()
+            for p in range(3):
+                pw, ph = strides[p], h // (2 if p else 1)
+                src = sup_h[f][offs[p]: offs[p] + lens[p]]
+                want = orc.render_warp_plane(cfg, p > 0, True, lut, src, pw, pw * ph, 1, mp[2 * which],
+                                             mp[2 * which + 1], pw, ph)
+                assert np.array_equal(dsts[p].cpu().numpy(), want), f"frame {f} mode1 {mode1} plane {p}"
+
+
+@pytest.mark.gpu
+def test_render_rejects_bad_arguments():
+    import svpflow_b200 as sv
+
+    cfg = _cfg(64, 48, 16, 16, 5, 4)
+    args = ([1, 1, 1], [64, 32, 32], [1, 1, 1], 0, 1, 1, [1, 1, 1], [64, 32, 32])
+    with pytest.raises(ValueError, match="threshold"):
+        sv.render_warp_device(cfg, 257, False, True, *args)
+    with pytest.raises(ValueError, match="shift"):
+        sv.render_warp_device(cfg, 10, False, True, *args[:3], 1, *args[4:])
