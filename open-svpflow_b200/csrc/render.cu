@@ -123,13 +123,15 @@ __device__ __forceinline__ int32_t motion(const RenderJob &J, const uint16_t *pl
     return ((k < kLut - 1 ? k : kLut - 1) - 1024) * J.lut_t / 256;
 }
 
-// The source index sample (px, py) of the plane reads: its tile, the motion at the tile's corners,
-// the interpolated displacement, sample_plane's direct or clamped position. -1: nothing to read.
-__device__ __forceinline__ int64_t sample_index(const RenderJob &J, const RenderPlane &p, int32_t px, int32_t py,
-                                                const int32_t (*sxw)[2], const int32_t (*syw)[2]) {
-    int32_t gx, gy, bx, by, tw, th;
-    tile_of(px, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gx, bx, tw);
-    tile_of(py, p.origin_y, p.block_h, p.bh_log2, p.height, J.grid_h, gy, by, th);
+// One tile's motion (motion_samples), whether its reads are direct (plane_covers and
+// tile_interior), and the motion interpolated down to row py (interpolate_motion_row).
+struct TileMotion {
+    int32_t rx0, rx1, ry0, ry1;
+    bool direct;
+};
+__device__ __forceinline__ TileMotion tile_motion(const RenderJob &J, const RenderPlane &p, int32_t gx, int32_t bx,
+                                                  int32_t tw, int32_t gy, int32_t by, int32_t th, int32_t py,
+                                                  const int32_t (*syw)[2]) {
     const int64_t gw = J.grid_w;
     const int64_t i00 = (int64_t)(gy > 0 ? gy : 0) * gw + (gx > 0 ? gx : 0);
     const int64_t nx = (gx >= 0 && gx != J.grid_w - 1) ? 1 : 0, ny = (gy >= 0 && gy != J.grid_h - 1) ? gw : 0;
@@ -148,7 +150,8 @@ __device__ __forceinline__ int64_t sample_index(const RenderJob &J, const Render
 #pragma unroll
         for (int q = 1; q < 4; q++) { sx[q] = sx[0]; sy[q] = sy[0]; }
     }
-    bool direct = false;
+    TileMotion t;
+    t.direct = false;
     if (p.covers && p.step > 0) {  // tile_interior over the whole tile
         int32_t mnx = sx[0], mxx = sx[0], mny = sy[0], mxy = sy[0];
 #pragma unroll
@@ -157,22 +160,33 @@ __device__ __forceinline__ int64_t sample_index(const RenderJob &J, const Render
             mny = min(mny, sy[q]); mxy = max(mxy, sy[q]);
         }
         const int64_t st = p.step;
-        direct = (int64_t)bx * st + mnx >= 0 && (int64_t)by * st + mny >= 0 &&
-                 (int64_t)(bx + tw - 1) * st + mxx <= p.max_x && (int64_t)(by + th - 1) * st + mxy <= p.max_y;
+        t.direct = (int64_t)bx * st + mnx >= 0 && (int64_t)by * st + mny >= 0 &&
+                   (int64_t)(bx + tw - 1) * st + mxx <= p.max_x && (int64_t)(by + th - 1) * st + mxy <= p.max_y;
     }
-    int32_t dx = sx[0], dy = sy[0];
     if (J.interp) {
-        const int32_t ly = min(py - by, kMaxBlock - 1), lx = min(px - bx, kMaxBlock - 1);
-        const int32_t *wy = syw[ly], *wx = sxw[lx];
-        const int32_t rx0 = interp_pair(sx[0], sx[2], p.block_h, p.y_shift, wy);
-        const int32_t rx1 = interp_pair(sx[1], sx[3], p.block_h, p.y_shift, wy);
-        const int32_t ry0 = interp_pair(sy[0], sy[2], p.block_h, p.y_shift, wy);
-        const int32_t ry1 = interp_pair(sy[1], sy[3], p.block_h, p.y_shift, wy);
-        dx = interp_pair(rx0, rx1, p.block_w, p.x_shift, wx);
-        dy = interp_pair(ry0, ry1, p.block_w, p.x_shift, wx);
+        const int32_t *wy = syw[min(py - by, kMaxBlock - 1)];
+        t.rx0 = interp_pair(sx[0], sx[2], p.block_h, p.y_shift, wy);
+        t.rx1 = interp_pair(sx[1], sx[3], p.block_h, p.y_shift, wy);
+        t.ry0 = interp_pair(sy[0], sy[2], p.block_h, p.y_shift, wy);
+        t.ry1 = interp_pair(sy[1], sy[3], p.block_h, p.y_shift, wy);
+    } else {
+        t.rx0 = t.rx1 = sx[0];
+        t.ry0 = t.ry1 = sy[0];
+    }
+    return t;
+}
+// The source index sample (px, py) reads in its tile (interpolate_motion, then sample_plane's
+// direct or clamped position).
+__device__ __forceinline__ int64_t tile_sample(const RenderJob &J, const RenderPlane &p, const TileMotion &t,
+                                               int32_t px, int32_t bx, int32_t py, const int32_t (*sxw)[2]) {
+    int32_t dx = t.rx0, dy = t.ry0;
+    if (J.interp) {
+        const int32_t *wx = sxw[min(px - bx, kMaxBlock - 1)];
+        dx = interp_pair(t.rx0, t.rx1, p.block_w, p.x_shift, wx);
+        dy = interp_pair(t.ry0, t.ry1, p.block_w, p.x_shift, wx);
     }
     int32_t xs = px * p.step + dx, ys = py * p.step + dy;
-    if (!direct) {
+    if (!t.direct) {
         xs = min(max(xs, 0), p.max_x);
         ys = min(max(ys, 0), p.max_y);
     }
@@ -192,10 +206,29 @@ __global__ void __launch_bounds__(256) render_warp_kernel(const __grid_constant_
     const int32_t py = blockIdx.y;
     const int32_t px0 = (blockIdx.x * blockDim.x + threadIdx.x) * kPx;
     if (px0 >= p.width || py >= p.height || p.block_w <= 0 || p.block_h <= 0) return;
-    // kPx consecutive samples per thread: their gathers are independent and overlap
+    // kPx consecutive samples per thread, usually in one tile (its motion is then fetched once)
+    int32_t gy, by, th;
+    tile_of(py, p.origin_y, p.block_h, p.bh_log2, p.height, J.grid_h, gy, by, th);
+    const int32_t pxl = min(px0 + kPx - 1, p.width - 1);
+    int32_t gx, bx, tw, gxl, bxl, twl;
+    tile_of(px0, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gx, bx, tw);
+    tile_of(pxl, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gxl, bxl, twl);
     int64_t si[kPx];
+    if (gx == gxl) {
+        const TileMotion t = tile_motion(J, p, gx, bx, tw, gy, by, th, py, syw);
 #pragma unroll
-    for (int k = 0; k < kPx; k++) si[k] = px0 + k < p.width ? sample_index(J, p, px0 + k, py, sxw, syw) : -1;
+        for (int k = 0; k < kPx; k++) si[k] = px0 + k <= pxl ? tile_sample(J, p, t, px0 + k, bx, py, sxw) : -1;
+    } else {
+#pragma unroll
+        for (int k = 0; k < kPx; k++) {
+            si[k] = -1;
+            if (px0 + k > pxl) continue;
+            int32_t gk, bk, twk;
+            tile_of(px0 + k, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gk, bk, twk);
+            const TileMotion t = tile_motion(J, p, gk, bk, twk, gy, by, th, py, syw);
+            si[k] = tile_sample(J, p, t, px0 + k, bk, py, sxw);
+        }
+    }
     uint8_t v[kPx];
 #pragma unroll
     for (int k = 0; k < kPx; k++) v[k] = (si[k] >= 0 && si[k] < p.src_len) ? __ldg(p.src + si[k]) : (uint8_t)0;
