@@ -158,20 +158,22 @@ typedef struct {
     int32_t grid_w, grid_h;       /* motion-plane size (svpf_vector_grid) */
     int32_t source_step;          /* 1 for frames; the super clip's pel when the sources are super frames */
 } svpf_render_config;
-/* CpuRenderer::render_mode1_or_2 without masks (renderer.rs:308-328, render_selected_warp_rows
- * :876-984) on the device: the three planes of one output frame, each sample the source sample
- * displaced by the motion of (motion_x, motion_y) (uint16 planes of grid_w x grid_h, as
- * svpf_vector_planes_device writes them) scaled by the threshold LUT (set_threshold :238-250,
- * threshold 0..256): mode1 != 0 uses the inverse LUT (256 - threshold) and the caller passes the
- * second source and motion set, mode 2 the threshold LUT with the first, as render_mode1_or_2
- * does. interp: bilinear motion between the four block centres (else one motion per block).
+/* CpuRenderer::render_mode1_or_2 (renderer.rs:308-328, render_selected_warp_rows :876-984) on
+ * the device: the three planes of one output frame, each sample the source sample displaced by the
+ * motion of (motion_x, motion_y) (uint16 planes of grid_w x grid_h, as svpf_vector_planes_device
+ * writes them) scaled by the threshold LUT (set_threshold :238-250, threshold 0..256): mode1 != 0
+ * uses the inverse LUT (256 - threshold) and the caller passes the second source and motion set,
+ * mode 2 the threshold LUT with the first, as render_mode1_or_2 does. interp: bilinear motion
+ * between the four block centres (else one motion per block). mask: NULL, or the mode's mask
+ * plane (grid_w x grid_h bytes; masks.a for mode 1, masks.b for mode 2): each sample is then
+ * mode1_pixel(undisplaced, displaced, alpha) with alpha interpolated from the mask (:1818-1820).
  * src_shift 0: src[] are plain planes (stride bytes per row); log2(source_step): src[] are a
  * super clip's level-0 planes whose sub-planes lie stride x plane-height bytes apart (svpflow2
  * core.rs:3340-3388). Device pointers; asynchronous on `stream`. */
 int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, int32_t mode1, int32_t interp,
                             const uint8_t *const src[3], const int64_t src_stride[3], const int64_t src_len[3],
                             int32_t src_shift, const uint16_t *motion_x, const uint16_t *motion_y,
-                            uint8_t *const dst[3], const int64_t dst_stride[3], void *stream);
+                            const uint8_t *mask, uint8_t *const dst[3], const int64_t dst_stride[3], void *stream);
 
 /* ---------------------------------------------------------------- batched form */
 /* No counterpart in the reference, which analyses one clip at a time, one output frame

@@ -1,11 +1,12 @@
-// render.cu -- SmoothFps's single-warp frame render on the device (algorithms 1 and 2 without
-// masks): each output sample is the source sample displaced by the motion interpolated between
-// the four motion-plane samples around it.
+// render.cu -- SmoothFps's single-warp frame render on the device (algorithms 1 and 2): each output
+// sample is the source sample displaced by the motion interpolated between the four motion-plane
+// samples around it, blended with the undisplaced sample by the mode's mask when one is given.
 //
 // Follows crates/svpflow-core/src/renderer.rs: CpuRenderer::render_mode1_or_2 (:308-328) through
 // render_selected_warp_rows (:876-984), set_threshold (:238-250), plane_params (:1539-1606),
 // motion_samples (:1608-1638), render_tiles (:1925-2010), interpolate_row / interpolate_motion
-// (:2582-2637), interp_pair (:2724-2738), interpolation_weights / coeff (:2740-2770), plane_covers /
+// (:2582-2637), alpha_row / alpha_at_row / alpha_at_absolute (:2639-2722), mode1_pixel (:1818-1820),
+// blend_255 (:3221-3223), interp_pair (:2724-2738), interpolation_weights / coeff (:2740-2770), plane_covers /
 // plane_index (:2772-2790), tile_interior (:2809-2835), sample_plane (:2837-2861), cpu_map
 // (:3186-3193). The reference walks tiles (one per vector block, plus a left column and a top row
 // of width / height origin) and writes each tile's samples; here one thread owns one output
@@ -37,12 +38,14 @@ struct RenderPlane {
     int32_t width, height, block_w, block_h, origin_x, origin_y, x_shift, y_shift, x_div, y_div, step;
     int32_t max_x, max_y, covers;
     int32_t bw_log2, bh_log2;  // log2 of the block size when it is a power of two, else -1
+    int32_t morigin_x, morigin_y;  // the plane's own origin (alpha_at_absolute's mask_params)
     int32_t xw[kMaxBlock][2], yw[kMaxBlock][2];
 };
 
 struct RenderJob {
     RenderPlane pl[3];
     const uint16_t *mx, *my;
+    const uint8_t *mask;  // NULL: no mask; else grid_w x grid_h alphas (mode1_pixel blends)
     int64_t mlen;
     int32_t grid_w, grid_h, interp;
     int32_t lut_t;  // the LUT's factor: threshold (mode 2) or 256 - threshold (mode 1)
@@ -127,8 +130,26 @@ __device__ __forceinline__ int32_t motion(const RenderJob &J, const uint16_t *pl
 // tile_interior), and the motion interpolated down to row py (interpolate_motion_row).
 struct TileMotion {
     int32_t rx0, rx1, ry0, ry1;
+    int32_t ma0, ma1;  // the mask interpolated down to the row (alpha_row)
     bool direct;
 };
+__device__ __forceinline__ int32_t mask_at(const RenderJob &J, int64_t i) {
+    return (i >= 0 && i < J.mlen) ? __ldg(J.mask + i) : 0;
+}
+__device__ __forceinline__ int32_t clamp_byte(int32_t v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
+// alpha_at_absolute (renderer.rs:2687-2722): used for the mask when the motion is not interpolated
+__device__ __forceinline__ int32_t alpha_absolute(const RenderJob &J, const RenderPlane &p, int32_t x, int32_t y) {
+    const int32_t ox = p.morigin_x, oy = p.morigin_y, bw = p.block_w, bh = p.block_h;
+    int32_t ix0 = 0, ix1 = 0, iy0 = 0, iy1 = 0;
+    if (ox <= x) { ix0 = (x - ox) / bw; ix1 = ix0 + 1; }
+    if (oy <= y) { iy0 = (y - oy) / bh; iy1 = iy0 + 1; }
+    const int32_t fx = ox < x ? (x - ox) % bw : 0, fy = oy < y ? (y - oy) % bh : 0;
+    const int64_t gw = J.grid_w;
+    const int32_t tl = mask_at(J, iy0 * gw + ix0), tr = mask_at(J, iy0 * gw + ix1);
+    const int32_t bl = mask_at(J, iy1 * gw + ix0), br = mask_at(J, iy1 * gw + ix1);
+    const int32_t top = ((bw - fx) * tl + fx * tr) / bw, bottom = ((bw - fx) * bl + fx * br) / bw;
+    return clamp_byte(((bh - fy) * top + fy * bottom) / bh);
+}
 __device__ __forceinline__ TileMotion tile_motion(const RenderJob &J, const RenderPlane &p, int32_t gx, int32_t bx,
                                                   int32_t tw, int32_t gy, int32_t by, int32_t th, int32_t py,
                                                   const int32_t (*syw)[2]) {
@@ -152,6 +173,18 @@ __device__ __forceinline__ TileMotion tile_motion(const RenderJob &J, const Rend
     }
     TileMotion t;
     t.direct = false;
+    t.ma0 = t.ma1 = 0;
+    if (J.mask != nullptr) {  // alpha_row
+        const int32_t a = mask_at(J, i00), b = mask_at(J, i00 + nx), cc = mask_at(J, i00 + ny),
+                      d = mask_at(J, i00 + ny + nx);
+        if (J.interp) {
+            const int32_t *wy = syw[min(py - by, kMaxBlock - 1)];
+            t.ma0 = interp_pair(a, cc, p.block_h, p.y_shift, wy);
+            t.ma1 = interp_pair(b, d, p.block_h, p.y_shift, wy);
+        } else {
+            t.ma0 = t.ma1 = a;
+        }
+    }
     if (p.covers && p.step > 0) {  // tile_interior over the whole tile
         int32_t mnx = sx[0], mxx = sx[0], mny = sy[0], mxy = sy[0];
 #pragma unroll
@@ -192,8 +225,15 @@ __device__ __forceinline__ int64_t tile_sample(const RenderJob &J, const RenderP
     }
     return src_index(p, xs, ys);
 }
+// With a mask: the sample's alpha (alpha_at_row, or alpha_at_absolute without interpolation)
+__device__ __forceinline__ int32_t tile_alpha(const RenderJob &J, const RenderPlane &p, const TileMotion &t,
+                                              int32_t px, int32_t bx, int32_t py, const int32_t (*sxw)[2]) {
+    if (!J.interp) return alpha_absolute(J, p, px, py);
+    return clamp_byte(interp_pair(t.ma0, t.ma1, p.block_w, p.x_shift, sxw[min(px - bx, kMaxBlock - 1)]));
+}
 
 // grid: (row length of the widest plane / (256 kPx), rows of the tallest plane, 3 planes)
+template <bool MASK>
 __global__ void __launch_bounds__(256) render_warp_kernel(const __grid_constant__ RenderJob J) {
     const RenderPlane &p = J.pl[blockIdx.z];
     // the plane's interpolation weights in shared memory (indexed per thread)
@@ -214,10 +254,14 @@ __global__ void __launch_bounds__(256) render_warp_kernel(const __grid_constant_
     tile_of(px0, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gx, bx, tw);
     tile_of(pxl, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gxl, bxl, twl);
     int64_t si[kPx];
+    int32_t alpha[kPx];
     if (gx == gxl) {
         const TileMotion t = tile_motion(J, p, gx, bx, tw, gy, by, th, py, syw);
 #pragma unroll
-        for (int k = 0; k < kPx; k++) si[k] = px0 + k <= pxl ? tile_sample(J, p, t, px0 + k, bx, py, sxw) : -1;
+        for (int k = 0; k < kPx; k++) {
+            si[k] = px0 + k <= pxl ? tile_sample(J, p, t, px0 + k, bx, py, sxw) : -1;
+            alpha[k] = MASK && px0 + k <= pxl ? tile_alpha(J, p, t, px0 + k, bx, py, sxw) : 0;
+        }
     } else {
 #pragma unroll
         for (int k = 0; k < kPx; k++) {
@@ -227,11 +271,20 @@ __global__ void __launch_bounds__(256) render_warp_kernel(const __grid_constant_
             tile_of(px0 + k, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gk, bk, twk);
             const TileMotion t = tile_motion(J, p, gk, bk, twk, gy, by, th, py, syw);
             si[k] = tile_sample(J, p, t, px0 + k, bk, py, sxw);
+            alpha[k] = MASK ? tile_alpha(J, p, t, px0 + k, bk, py, sxw) : 0;
         }
     }
     uint8_t v[kPx];
 #pragma unroll
     for (int k = 0; k < kPx; k++) v[k] = (si[k] >= 0 && si[k] < p.src_len) ? __ldg(p.src + si[k]) : (uint8_t)0;
+    if (MASK) {  // mode1_pixel: blend_255(warped, base, alpha), base = the undisplaced sample
+#pragma unroll
+        for (int k = 0; k < kPx; k++) {
+            const int64_t bi = src_index(p, (px0 + k) * p.step, py * p.step);
+            const int32_t base = (px0 + k < p.width && bi >= 0 && bi < p.src_len) ? __ldg(p.src + bi) : 0;
+            v[k] = (uint8_t)clamp_byte(((int32_t)v[k] * (255 - alpha[k]) + base * alpha[k] + 255) >> 8);
+        }
+    }
     uint8_t *out = p.dst + (int64_t)py * p.dst_stride + px0;
 #pragma unroll
     for (int k = 0; k < kPx; k++)
@@ -245,7 +298,7 @@ extern "C" {
 int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, int32_t mode1, int32_t interp,
                             const uint8_t *const src[3], const int64_t src_stride[3], const int64_t src_len[3],
                             int32_t src_shift, const uint16_t *motion_x, const uint16_t *motion_y,
-                            uint8_t *const dst[3], const int64_t dst_stride[3], void *stream) {
+                            const uint8_t *mask, uint8_t *const dst[3], const int64_t dst_stride[3], void *stream) {
     if (int rc = svpf::require_device()) return rc;
     if (!cfg || !src || !src_stride || !src_len || !dst || !dst_stride || !motion_x || !motion_y) {
         svpf::set_last_error("render: null argument");
@@ -269,6 +322,7 @@ int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, in
     J->lut_t = mode1 ? 256 - threshold : threshold;
     J->mx = motion_x;
     J->my = motion_y;
+    J->mask = mask;
     J->mlen = (int64_t)cfg->grid_w * cfg->grid_h;
     J->grid_w = cfg->grid_w;
     J->grid_h = cfg->grid_h;
@@ -292,6 +346,8 @@ int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, in
         p.block_h = c ? cfg->block_h / cd : cfg->block_h;
         p.origin_x = zero ? 0 : (c ? cfg->origin_x / 2 : cfg->origin_x);
         p.origin_y = zero ? 0 : (c ? cfg->origin_y / cd : cfg->origin_y);
+        p.morigin_x = c ? cfg->origin_x / 2 : cfg->origin_x;
+        p.morigin_y = c ? cfg->origin_y / cd : cfg->origin_y;
         p.x_shift = cpu_map(c ? cfg->block_w / 2 : cfg->block_w);
         p.y_shift = cpu_map(c ? cfg->block_h / 2 : cfg->block_h);
         p.x_div = c ? 2 : 1;
@@ -317,7 +373,8 @@ int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, in
     cudaError_t e = cudaSuccess;
     if (most_w > 0 && most_h > 0) {
         dim3 grid((unsigned)((most_w + 256 * kPx - 1) / (256 * kPx)), (unsigned)most_h, 3);
-        render_warp_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(*J);
+        if (mask) render_warp_kernel<true><<<grid, 256, 0, (cudaStream_t)stream>>>(*J);
+        else render_warp_kernel<false><<<grid, 256, 0, (cudaStream_t)stream>>>(*J);
         svpf::add_launches(1);
         e = cudaGetLastError();
     }

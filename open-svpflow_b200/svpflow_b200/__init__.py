@@ -108,7 +108,7 @@ def lib() -> ctypes.CDLL:
             "svpf_vector_grid": (I32, [P(I32), P(I32), P(I32)]),
             "svpf_vector_planes_device": (I32, [P(I32), _VP, SZ, I32, I32, I32, I32, _VP, _VP, _VP]),
             "svpf_render_warp_device": (I32, [P(RenderConfig), I32, I32, I32, P(_VP), P(I64), P(I64), I32, _VP, _VP,
-                                              P(_VP), P(I64), _VP]),
+                                              _VP, P(_VP), P(I64), _VP]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -489,12 +489,14 @@ def vector_planes_device(vdata, payloads_ptr: int, payload_len: int, npayloads: 
 
 
 def render_warp_device(cfg: dict, threshold: int, mode1: bool, interp: bool, src_ptrs, src_strides, src_lens,
-                       src_shift: int, motion_x_ptr: int, motion_y_ptr: int, dst_ptrs, dst_strides, stream: int = 0):
-    """SmoothFps's single-warp render (algorithms 1 / 2, no masks) of one frame's three planes on
-    the device; see svpf_render_warp_device."""
+                       src_shift: int, motion_x_ptr: int, motion_y_ptr: int, dst_ptrs, dst_strides, stream: int = 0,
+                       mask_ptr: int = 0):
+    """SmoothFps's single-warp render (algorithms 1 / 2, with or without the mode's mask) of one
+    frame's three planes on the device; see svpf_render_warp_device."""
     c = RenderConfig(**{k: int(cfg[k]) for k, _ in RenderConfig._fields_})
     arr = lambda t, v: (t * 3)(*[int(x) for x in v])
     _check(lib().svpf_render_warp_device(ctypes.byref(c), int(threshold), int(mode1), int(interp),
                                          arr(_VP, src_ptrs), arr(ctypes.c_int64, src_strides),
                                          arr(ctypes.c_int64, src_lens), int(src_shift), motion_x_ptr, motion_y_ptr,
-                                         arr(_VP, dst_ptrs), arr(ctypes.c_int64, dst_strides), stream))
+                                         mask_ptr or None, arr(_VP, dst_ptrs), arr(ctypes.c_int64, dst_strides),
+                                         stream))

@@ -456,7 +456,7 @@ def _setup(L):
         L.or_render_luts.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
         L.or_render_warp_plane.argtypes = [P(RenderConfig), ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
                                            P(RPlane), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
-                                           ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
     for f in ("or_reduce_dim", "or_auto_levels", "or_super_plane_height", "or_auto_search_levels"):
         getattr(L, f).argtypes = [ctypes.c_int32] * {"or_reduce_dim": 2, "or_auto_levels": 2,
                                                        "or_super_plane_height": 4, "or_auto_search_levels": 6}[f]
@@ -742,7 +742,7 @@ def render_luts(threshold: int):
 
 def render_warp_plane(cfg: dict, chroma: bool, interp: bool, lut: np.ndarray, src: np.ndarray, src_stride: int,
                       src_span: int, src_shift: int, mx: np.ndarray, my: np.ndarray, dst_stride: int,
-                      dst_rows: int) -> np.ndarray:
+                      dst_rows: int, mask: np.ndarray = None) -> np.ndarray:
     """render_selected_warp_rows over a whole plane: uint8 [dst_rows, dst_stride] (bytes the reference
     leaves untouched stay 0)."""
     c = RenderConfig(**{k: int(cfg[k]) for k, _ in RenderConfig._fields_})
@@ -753,6 +753,10 @@ def render_warp_plane(cfg: dict, chroma: bool, interp: bool, lut: np.ndarray, sr
     assert mx.size == my.size and lut.size == 2048
     pl = RPlane(src.ctypes.data, src.size, src_stride, src_span, src_shift)
     dst = np.zeros(dst_rows * dst_stride, dtype=np.uint8)
+    mk = None
+    if mask is not None:
+        mk = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        assert mk.size == mx.size
     lib().or_render_warp_plane(ctypes.byref(c), int(chroma), int(interp), _ptr(lut), ctypes.byref(pl), _ptr(mx),
-                               _ptr(my), mx.size, _ptr(dst), dst_stride, dst.size)
+                               _ptr(my), mx.size, None if mk is None else _ptr(mk), _ptr(dst), dst_stride, dst.size)
     return dst.reshape(dst_rows, dst_stride)

@@ -2007,11 +2007,33 @@ static i32 r_motion(const int16_t *lut, const uint16_t *plane, usize len, usize 
     return lut[k < 2047 ? k : 2047];
 }
 
+/* alpha_at_absolute (:2687-2722) and mask_at (:3209-3219) */
+static i32 r_mask_at(const uint8_t *m, usize len, usize stride, i32 x, i32 y) {
+    if (x < 0 || y < 0) return 0;
+    usize i = sat_add_us(sat_mul_us((usize)y, stride), (usize)x);
+    return i < len ? m[i] : 0;
+}
+static i32 r_byte(i32 v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
+static i32 r_alpha_abs(const uint8_t *m, usize len, const rparams *q, usize stride, i32 x, i32 y) {
+    if (q->block_w <= 0 || q->block_h <= 0) return 0;
+    i32 ix0 = 0, ix1 = 0, iy0 = 0, iy1 = 0;
+    if (q->origin_x <= x) { ix0 = (x - q->origin_x) / q->block_w; ix1 = ix0 + 1; }
+    if (q->origin_y <= y) { iy0 = (y - q->origin_y) / q->block_h; iy1 = iy0 + 1; }
+    i32 fx = q->origin_x < x ? (x - q->origin_x) % q->block_w : 0;
+    i32 fy = q->origin_y < y ? (y - q->origin_y) % q->block_h : 0;
+    i32 tl = r_mask_at(m, len, stride, ix0, iy0), tr = r_mask_at(m, len, stride, ix1, iy0);
+    i32 bl = r_mask_at(m, len, stride, ix0, iy1), br = r_mask_at(m, len, stride, ix1, iy1);
+    i32 top = ((q->block_w - fx) * tl + fx * tr) / q->block_w;
+    i32 bottom = ((q->block_w - fx) * bl + fx * br) / q->block_w;
+    return r_byte(((q->block_h - fy) * top + fy * bottom) / q->block_h);
+}
+
 void or_render_warp_plane(const or_render_config *c, int32_t chroma, int32_t interp, const int16_t *lut,
-                          const or_rplane *src, const uint16_t *mx, const uint16_t *my, size_t mlen, uint8_t *dst,
-                          size_t dst_stride, size_t dst_len) {
-    rparams P;
+                          const or_rplane *src, const uint16_t *mx, const uint16_t *my, size_t mlen,
+                          const uint8_t *mask, uint8_t *dst, size_t dst_stride, size_t dst_len) {
+    rparams P, MP;
     r_params(c, chroma, !interp, &P);
+    r_params(c, chroma, 0, &MP); /* mask_params: the plane's own origin, used without interpolation */
     const rparams *p = &P;
     i32 gw = (i32)c->grid_w, gh = (i32)c->grid_h;
     if (p->width <= 0 || p->height <= 0 || p->block_w <= 0 || p->block_h <= 0 || gw <= 0 || gh <= 0) return;
@@ -2072,6 +2094,17 @@ void or_render_warp_plane(const or_render_config *c, int32_t chroma, int32_t int
                     ry[0] = r_interp(sy[0], sy[2], p->block_h, p->y_shift, wy);
                     ry[1] = r_interp(sy[1], sy[3], p->block_h, p->y_shift, wy);
                 }
+                i32 mrow[2] = {0, 0}; /* alpha_row (:2639-2651) */
+                if (mask) {
+                    i32 ma = r_mask_at(mask, mlen, mlen, (i32)i00, 0), mb = r_mask_at(mask, mlen, mlen, (i32)i01, 0);
+                    i32 mc = r_mask_at(mask, mlen, mlen, (i32)i10, 0), md = r_mask_at(mask, mlen, mlen, (i32)i11, 0);
+                    if (!interp) { mrow[0] = mrow[1] = ma; }
+                    else {
+                        const i32 *wy = p->yw[local_y < 0 ? 0 : (local_y > 31 ? 31 : local_y)];
+                        mrow[0] = r_interp(ma, mc, p->block_h, p->y_shift, wy);
+                        mrow[1] = r_interp(mb, md, p->block_h, p->y_shift, wy);
+                    }
+                }
                 for (i32 x = 0; x < width; x++) {
                     i32 px = tx + x, source_x = px * p->step;
                     const i32 *wx = p->xw[x > 31 ? 31 : x];
@@ -2081,7 +2114,16 @@ void or_render_warp_plane(const or_render_config *c, int32_t chroma, int32_t int
                         dy = r_interp(ry[0], ry[1], p->block_w, p->x_shift, wx);
                     }
                     i32 xs = source_x + dx, ys = source_y + dy;
-                    uint8_t v;
+                    uint8_t v, base = 0;
+                    if (mask) { /* sample_plane at no displacement */
+                        i32 bxs = source_x, bys = source_y;
+                        if (!direct) {
+                            bxs = bxs < 0 ? 0 : (bxs > p->max_x ? p->max_x : bxs);
+                            bys = bys < 0 ? 0 : (bys > p->max_y ? p->max_y : bys);
+                        }
+                        usize bi = r_index(src, (usize)(int64_t)bxs, (usize)(int64_t)bys);
+                        base = bi < src->len ? src->data[bi] : 0;
+                    }
                     if (direct) {
                         usize idx = r_index(src, (usize)(int64_t)xs, (usize)(int64_t)ys);
                         v = idx < src->len ? src->data[idx] : 0; /* in range by tile_interior + plane_covers */
@@ -2090,6 +2132,11 @@ void or_render_warp_plane(const or_render_config *c, int32_t chroma, int32_t int
                         ys = ys < 0 ? 0 : (ys > p->max_y ? p->max_y : ys);
                         usize idx = r_index(src, (usize)xs, (usize)ys);
                         v = idx < src->len ? src->data[idx] : 0;
+                    }
+                    if (mask) { /* mode1_pixel (:1818-1820) = blend_255(warped, base, alpha) (:3221-3223) */
+                        i32 alpha = interp ? r_byte(r_interp(mrow[0], mrow[1], p->block_w, p->x_shift, wx))
+                                           : r_alpha_abs(mask, mlen, &MP, (usize)c->grid_w, px, ty + y);
+                        v = (uint8_t)r_byte(((i32)v * (255 - alpha) + (i32)base * alpha + 255) >> 8);
                     }
                     dst[start + (usize)x] = v;
                 }

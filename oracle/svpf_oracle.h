@@ -187,9 +187,11 @@ typedef struct {
     uint32_t shift;
 } or_rplane;
 void or_render_luts(int32_t threshold, int16_t inverse_lut[2048], int16_t threshold_lut[2048]);
+/* mask: NULL, or the mode's mask plane (grid_w x grid_h bytes, renderer.rs MaskPlanes): each sample
+ * becomes mode1_pixel(base, warped, alpha) */
 void or_render_warp_plane(const or_render_config *c, int32_t chroma, int32_t interp, const int16_t *lut,
-                          const or_rplane *src, const uint16_t *mx, const uint16_t *my, size_t mlen, uint8_t *dst,
-                          size_t dst_stride, size_t dst_len);
+                          const or_rplane *src, const uint16_t *mx, const uint16_t *my, size_t mlen,
+                          const uint8_t *mask, uint8_t *dst, size_t dst_stride, size_t dst_len);
 int or_vector_planes(const int32_t vdata[16], const uint8_t *payload, size_t len, int32_t frame_w, int32_t frame_h,
                      int32_t raw, uint16_t *out);
 

@@ -1,4 +1,4 @@
-"""SmoothFps's single-warp frame render (renderer.rs render_mode1_or_2 without masks).
+"""SmoothFps's single-warp frame render (renderer.rs render_mode1_or_2, with and without masks).
 
 CPU: the oracle's C restatement against properties of the render (identity, whole-plane shifts,
 super-clip sub-planes) and against a second, independent restatement in Python written from the
@@ -30,7 +30,7 @@ def _grid(w, h, bw, bh):
 
 
 # ---------------------------------------------------------------- a second restatement (Python)
-def _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my):
+def _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my, mask=None):
     """render_selected_warp_rows, scalar loop (renderer.rs:876-984), in plain Python."""
     cmap = lambda v: CPU_MAP[v - 1] if 1 <= v <= 32 else -1
     cd = cfg["chroma_y_div"]
@@ -60,6 +60,25 @@ def _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my):
         return out
 
     xw, yw = weights(BW, xs_), weights(BH, ys_)
+    mox, moy = (cfg["origin_x"] // 2, cfg["origin_y"] // cd) if chroma else (cfg["origin_x"], cfg["origin_y"])
+
+    def mask_at(x, y):
+        i = y * cfg["grid_w"] + x
+        return int(mask[i]) if x >= 0 and y >= 0 and i < len(mask) else 0
+
+    def alpha_abs(x, y):  # alpha_at_absolute with the plane's own origin
+        ix0 = ix1 = iy0 = iy1 = 0
+        if mox <= x:
+            ix0 = (x - mox) // BW
+            ix1 = ix0 + 1
+        if moy <= y:
+            iy0 = (y - moy) // BH
+            iy1 = iy0 + 1
+        fx = (x - mox) % BW if mox < x else 0
+        fy = (y - moy) % BH if moy < y else 0
+        top = ((BW - fx) * mask_at(ix0, iy0) + fx * mask_at(ix1, iy0)) // BW
+        bot = ((BW - fx) * mask_at(ix0, iy1) + fx * mask_at(ix1, iy1)) // BW
+        return min(max(((BH - fy) * top + fy * bot) // BH, 0), 255)
 
     def ip(a, b, total, sh, w):
         s = w[0] * a + w[1] * b
@@ -108,6 +127,9 @@ def _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my):
                 wy = yw[min(y, 31)]
                 rx = [ip(sx[0], sx[2], BH, ys_, wy), ip(sx[1], sx[3], BH, ys_, wy)] if interp else [sx[0]] * 2
                 ry = [ip(sy[0], sy[2], BH, ys_, wy), ip(sy[1], sy[3], BH, ys_, wy)] if interp else [sy[0]] * 2
+                if mask is not None:
+                    mk = [int(mask[i]) if i < len(mask) else 0 for i in idx]
+                    mrow = [ip(mk[0], mk[2], BH, ys_, wy), ip(mk[1], mk[3], BH, ys_, wy)] if interp else [mk[0]] * 2
                 for x in range(tw):
                     wx = xw[min(x, 31)]
                     dx = ip(rx[0], rx[1], BW, xs_, wx) if interp else rx[0]
@@ -116,7 +138,13 @@ def _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my):
                     if not direct:
                         X, Y = min(max(X, 0), maxx), min(max(Y, 0), maxy)
                     i = index(X, Y)
-                    dst[by + y, bx + x] = src[i] if i < len(src) else 0
+                    v = int(src[i]) if i < len(src) else 0
+                    if mask is not None:
+                        bi = index((bx + x) * step, (by + y) * step)
+                        base = int(src[bi]) if bi < len(src) else 0
+                        a = min(max(ip(mrow[0], mrow[1], BW, xs_, wx), 0), 255) if interp else alpha_abs(bx + x, by + y)
+                        v = min(max((v * (255 - a) + base * a + 255) >> 8, 0), 255)
+                    dst[by + y, bx + x] = v
     return dst
 
 
@@ -126,33 +154,36 @@ def _motion(rng, n, spread):
     return m
 
 
-PY_CASES = [  # w, h, block, step (super clip pel), interp, threshold, mode1
-    (40, 24, 8, 1, True, 128, False),
-    (40, 24, 8, 1, False, 200, True),
-    (36, 22, 16, 1, True, 256, False),   # tiles stretched to the frame edge (weights past the block are 0)
-    (20, 12, 32, 1, True, 90, False),    # blocks larger than the frame: overlapping tiles
-    (32, 16, 8, 2, True, 160, True),     # half-pel super planes
-    (24, 16, 4, 4, False, 64, False),    # quarter-pel super planes
+PY_CASES = [  # w, h, block, step (super clip pel), interp, threshold, mode1, mask
+    (40, 24, 8, 1, True, 128, False, False),
+    (40, 24, 8, 1, False, 200, True, False),
+    (36, 22, 16, 1, True, 256, False, False),   # tiles stretched to the frame edge (weights past the block are 0)
+    (20, 12, 32, 1, True, 90, False, False),    # blocks larger than the frame: overlapping tiles
+    (32, 16, 8, 2, True, 160, True, False),     # half-pel super planes
+    (24, 16, 4, 4, False, 64, False, False),    # quarter-pel super planes
+    (40, 24, 8, 1, True, 128, True, True),      # masked blend (mode1_pixel), interpolated alpha
+    (36, 22, 16, 2, False, 200, False, True),   # masked blend, alpha_at_absolute
 ]
 
 
 @pytest.mark.parametrize("case", range(len(PY_CASES)))
 def test_oracle_matches_python_restatement(case):
-    w, h, blk, step, interp, thr, mode1 = PY_CASES[case]
+    w, h, blk, step, interp, thr, mode1, masked = PY_CASES[case]
     rng = np.random.default_rng(case)
     gw, gh = _grid(w, h, blk, blk)
     cfg = _cfg(w, h, blk, blk, gw, gh, step)
     inv, tl = orc.render_luts(thr)
     lut = inv if mode1 else tl
     mx, my = _motion(rng, gw * gh, 40), _motion(rng, gw * gh, 40)
+    mask = rng.integers(0, 256, size=gw * gh, dtype=np.uint8) if masked else None
     shift = {1: 0, 2: 1, 4: 2}[step]
     for chroma in (False, True):
         pw, ph = (w // 2, h // 2) if chroma else (w, h)
         stride = pw + 3
         src = rng.integers(0, 256, size=(step * step) * ph * stride, dtype=np.uint8)
         span = stride * ph if shift else 0
-        got = orc.render_warp_plane(cfg, chroma, interp, lut, src, stride, span, shift, mx, my, pw, ph)
-        want = _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my)
+        got = orc.render_warp_plane(cfg, chroma, interp, lut, src, stride, span, shift, mx, my, pw, ph, mask)
+        want = _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my, mask)
         assert np.array_equal(got, want), f"chroma {chroma}: {np.argwhere(got != want)[:3]}"
 
 
@@ -200,15 +231,18 @@ def test_oracle_super_subplanes():
 
 
 # ---------------------------------------------------------------- GPU
-GPU_CASES = [  # w, h, block, step, interp, threshold, mode1, source stride pad
-    (1920, 1080, 16, 1, True, 128, False, 0),
-    (1920, 1080, 16, 2, True, 96, True, 0),
-    (1920, 1080, 8, 1, False, 256, False, 64),
-    (640, 360, 32, 1, True, 200, True, 32),
-    (100, 60, 8, 4, True, 40, False, 12),
-    (66, 38, 16, 2, False, 0, True, 2),
-    (20, 12, 32, 1, True, 175, False, 0),
-    (1280, 720, 4, 1, True, 255, True, 0),
+GPU_CASES = [  # w, h, block, step, interp, threshold, mode1, source stride pad, mask
+    (1920, 1080, 16, 1, True, 128, False, 0, False),
+    (1920, 1080, 16, 2, True, 96, True, 0, False),
+    (1920, 1080, 8, 1, False, 256, False, 64, False),
+    (640, 360, 32, 1, True, 200, True, 32, False),
+    (100, 60, 8, 4, True, 40, False, 12, False),
+    (66, 38, 16, 2, False, 0, True, 2, False),
+    (20, 12, 32, 1, True, 175, False, 0, False),
+    (1280, 720, 4, 1, True, 255, True, 0, False),
+    (1920, 1080, 16, 2, True, 128, True, 0, True),
+    (640, 360, 8, 1, False, 77, False, 8, True),
+    (20, 12, 32, 2, True, 200, False, 0, True),
 ]
 
 
@@ -217,11 +251,12 @@ def _gpu_render_case(case, rng):
 
     import svpflow_b200 as sv
 
-    w, h, blk, step, interp, thr, mode1, pad = case
+    w, h, blk, step, interp, thr, mode1, pad, masked = case
     gw, gh = _grid(w, h, blk, blk)
     cfg = _cfg(w, h, blk, blk, gw, gh, step)
     shift = {1: 0, 2: 1, 4: 2}[step]
     mx, my = _motion(rng, gw * gh, 120), _motion(rng, gw * gh, 120)
+    mask = rng.integers(0, 256, size=gw * gh, dtype=np.uint8) if masked else None
     inv, tl = orc.render_luts(thr)
     lut = inv if mode1 else tl
     srcs, wants, dsts = [], [], []
@@ -230,14 +265,17 @@ def _gpu_render_case(case, rng):
         stride = pw + pad
         src = rng.integers(0, 256, size=(step * step) * ph * stride, dtype=np.uint8)
         span = stride * ph if shift else 0
-        wants.append(orc.render_warp_plane(cfg, pl > 0, interp, lut, src, stride, span, shift, mx, my, pw + 1, ph))
+        wants.append(orc.render_warp_plane(cfg, pl > 0, interp, lut, src, stride, span, shift, mx, my, pw + 1, ph,
+                                           mask))
         srcs.append((torch.from_numpy(src).cuda(), stride))
         dsts.append((torch.full((ph, pw + 1), 7, dtype=torch.uint8, device="cuda"), pw + 1))
     mxd = torch.from_numpy(mx.astype(np.int16)).cuda()
     myd = torch.from_numpy(my.astype(np.int16)).cuda()
+    mkd = torch.from_numpy(mask).cuda() if masked else None
     sv.render_warp_device(cfg, thr, mode1, interp, [s.data_ptr() for s, _ in srcs], [st for _, st in srcs],
                           [s.numel() for s, _ in srcs], shift, mxd.data_ptr(), myd.data_ptr(),
-                          [d.data_ptr() for d, _ in dsts], [st for _, st in dsts])
+                          [d.data_ptr() for d, _ in dsts], [st for _, st in dsts],
+                          mask_ptr=mkd.data_ptr() if masked else 0)
     torch.cuda.synchronize()
     for pl in range(3):
         got = dsts[pl][0].cpu().numpy()
