@@ -174,6 +174,20 @@ int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, in
                             const uint8_t *const src[3], const int64_t src_stride[3], const int64_t src_len[3],
                             int32_t src_shift, const uint16_t *motion_x, const uint16_t *motion_y,
                             const uint8_t *mask, uint8_t *const dst[3], const int64_t dst_stride[3], void *stream);
+/* CpuRenderer::render_mode11_or_13 (renderer.rs:330-438; zero_origin != 0: its zero-origin variant
+ * :356-380) on the device: each sample blends source 0 displaced by motion set 0 (threshold LUT)
+ * with source 1 displaced by motion set 1 (inverse LUT): mode 11 blend_256(mv0, mv1, threshold),
+ * mode 13 (mode13 != 0) blend_256(cur0, cur1, threshold) clamped between mv0 and mv1
+ * (mode11_or_13_pixel :2918-2943). mask_a / mask_b: both NULL, or the two masks whose max_mask
+ * blends the result with the undisplaced blend. Sources, strides and src_shift as for
+ * svpf_render_warp_device; device pointers; asynchronous on `stream`. */
+int svpf_render_blend_device(const svpf_render_config *cfg, int32_t threshold, int32_t mode13, int32_t interp,
+                             int32_t zero_origin, const uint8_t *const src0[3], const int64_t src0_stride[3],
+                             const int64_t src0_len[3], const uint8_t *const src1[3], const int64_t src1_stride[3],
+                             const int64_t src1_len[3], int32_t src_shift, const uint16_t *motion0_x,
+                             const uint16_t *motion0_y, const uint16_t *motion1_x, const uint16_t *motion1_y,
+                             const uint8_t *mask_a, const uint8_t *mask_b, uint8_t *const dst[3],
+                             const int64_t dst_stride[3], void *stream);
 
 /* ---------------------------------------------------------------- batched form */
 /* No counterpart in the reference, which analyses one clip at a time, one output frame

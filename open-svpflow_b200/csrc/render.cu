@@ -1,21 +1,25 @@
-// render.cu -- SmoothFps's single-warp frame render on the device (algorithms 1 and 2): each output
-// sample is the source sample displaced by the motion interpolated between the four motion-plane
-// samples around it, blended with the undisplaced sample by the mode's mask when one is given.
+// render.cu -- SmoothFps's frame render on the device: the single warp of algorithms 1 and 2 and
+// the two-source blend of algorithms 11 and 13. Each output sample reads its source(s) at its
+// position displaced by motion interpolated between the four motion-plane samples around it, and
+// optionally blends with the undisplaced samples by the mode's mask.
 //
 // Follows crates/svpflow-core/src/renderer.rs: CpuRenderer::render_mode1_or_2 (:308-328) through
-// render_selected_warp_rows (:876-984), set_threshold (:238-250), plane_params (:1539-1606),
-// motion_samples (:1608-1638), render_tiles (:1925-2010), interpolate_row / interpolate_motion
-// (:2582-2637), alpha_row / alpha_at_row / alpha_at_absolute (:2639-2722), mode1_pixel (:1818-1820),
-// blend_255 (:3221-3223), interp_pair (:2724-2738), interpolation_weights / coeff (:2740-2770), plane_covers /
-// plane_index (:2772-2790), tile_interior (:2809-2835), sample_plane (:2837-2861), cpu_map
-// (:3186-3193). The reference walks tiles (one per vector block, plus a left column and a top row
-// of width / height origin) and writes each tile's samples; here one thread owns one output
-// sample and finds its tile arithmetically: the last tile in the reference's loop order that
-// covers the sample, since a later tile overwrites an earlier one where they overlap.
+// render_selected_warp_rows (:876-984); render_mode11_or_13 and its zero-origin variant (:330-438)
+// through render_dual_warp_rows (:1031-1172) and mode11_or_13_pixel (:2918-2943); set_threshold
+// (:238-250), plane_params (:1539-1606), motion_samples (:1608-1638), render_tiles (:1925-2010),
+// interpolate_row / interpolate_motion (:2582-2637), alpha_row / alpha_at_row / alpha_at_absolute
+// (:2639-2722), interp_pair (:2724-2738), interpolation_weights / coeff (:2740-2770), plane_covers /
+// plane_index (:2772-2790), tile_interior (:2809-2835), sample_plane (:2837-2861), max_mask
+// (:2908-2915), mode1_pixel / mode13_pixel (:1818-1828), blend_255 / blend_256 / clamp_between
+// (:3221-3231), cpu_map (:3186-3193). The reference walks tiles (one per vector block, plus a left
+// column and a top row of width / height origin) and writes each tile's samples; here one thread
+// owns kPx consecutive output samples of a row and finds their tile arithmetically: the last tile
+// in the reference's loop order that covers them, since a later tile overwrites an earlier one where
+// they overlap. The tile's motion is fetched once when the thread's samples share it.
 //
-// 32-bit arithmetic as the reference's scalar loop. Its x86-64 SSE tile path keeps 16-bit lanes,
-// which give the same values for thresholds 0..256 (|motion| <= 1024, weights <= 32), the only
-// thresholds accepted here.
+// 32-bit arithmetic as the reference's scalar loops. Its x86-64 SSE tile paths keep 16-bit lanes,
+// which give the same values for thresholds 0..256 (|motion| <= 1024, weights <= 32, mask values
+// <= 255), the only thresholds accepted here.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -29,26 +33,31 @@ namespace {
 constexpr int kLut = 2048, kMaxBlock = 32;
 constexpr int kPx = 4;  // output samples per thread
 
+struct Source {  // a plain plane (shift 0) or a super clip's level 0 (sub-planes `span` bytes apart)
+    const uint8_t *p;
+    int64_t len, stride, span;
+    int32_t covers;  // plane_covers
+};
+
 struct RenderPlane {
-    const uint8_t *src;
-    int64_t src_len, src_stride, src_span;
+    Source src[2];
     uint8_t *dst;
     int64_t dst_stride;
-    int32_t src_shift;
-    int32_t width, height, block_w, block_h, origin_x, origin_y, x_shift, y_shift, x_div, y_div, step;
-    int32_t max_x, max_y, covers;
-    int32_t bw_log2, bh_log2;  // log2 of the block size when it is a power of two, else -1
+    int32_t width, height, block_w, block_h, origin_x, origin_y, x_shift, y_shift, x_div, step;
+    int32_t max_x, max_y;
+    int32_t bw_log2, bh_log2;      // log2 of the block size when it is a power of two, else -1
     int32_t morigin_x, morigin_y;  // the plane's own origin (alpha_at_absolute's mask_params)
     int32_t xw[kMaxBlock][2], yw[kMaxBlock][2];
 };
 
 struct RenderJob {
     RenderPlane pl[3];
-    const uint16_t *mx, *my;
-    const uint8_t *mask;  // NULL: no mask; else grid_w x grid_h alphas (mode1_pixel blends)
+    const uint16_t *mx[2], *my[2];  // motion sets 0 and 1 (the single warp uses set 0)
+    const uint8_t *mask[2];         // NULL, one mask, or the two of max_mask
     int64_t mlen;
-    int32_t grid_w, grid_h, interp;
-    int32_t lut_t;  // the LUT's factor: threshold (mode 2) or 256 - threshold (mode 1)
+    int32_t grid_w, grid_h, interp, zero_origin, shift;
+    int32_t lut_t[2];               // LUT factors of the sets: threshold or 256 - threshold
+    int32_t threshold, mode13;      // the two-source blend
 };
 
 // ---- host side: the renderer's per-plane constants
@@ -83,31 +92,41 @@ int32_t sat_step_max(int32_t a, int32_t step) {  // a.saturating_mul(step).satur
     const int32_t s = sat32((int64_t)sat32((int64_t)a * step) - 1);
     return s > 0 ? s : 0;
 }
-bool covers(const RenderPlane &p) {  // plane_covers
-    if (p.src_shift != 0 && (p.src_shift >= 31 || (1 << p.src_shift) != p.step)) return false;
-    const uint64_t x = (uint64_t)p.max_x, y = (uint64_t)p.max_y;
+bool covers(const Source &s, int32_t shift, int32_t step, int32_t max_x, int32_t max_y) {  // plane_covers
+    if (shift != 0 && (shift >= 31 || (1 << shift) != step)) return false;
+    const uint64_t x = (uint64_t)max_x, y = (uint64_t)max_y;
     unsigned __int128 idx;
-    if (p.src_shift == 0) {
-        idx = (unsigned __int128)y * (uint64_t)p.src_stride + x;
+    if (shift == 0) {
+        idx = (unsigned __int128)y * (uint64_t)s.stride + x;
     } else {
-        const uint64_t mask = (1ull << p.src_shift) - 1;
-        const uint64_t sub = ((y & mask) << p.src_shift) | (x & mask);
-        idx = (unsigned __int128)sub * (uint64_t)p.src_span + (unsigned __int128)(y >> p.src_shift) * (uint64_t)p.src_stride +
-              (x >> p.src_shift);
+        const uint64_t mask = (1ull << shift) - 1;
+        const uint64_t sub = ((y & mask) << shift) | (x & mask);
+        idx = (unsigned __int128)sub * (uint64_t)s.span + (unsigned __int128)(y >> shift) * (uint64_t)s.stride +
+              (x >> shift);
     }
-    return idx < (unsigned __int128)(uint64_t)p.src_len;
+    return idx < (unsigned __int128)(uint64_t)s.len;
 }
 
 // ---- device side
-__device__ __forceinline__ int64_t src_index(const RenderPlane &p, int32_t x, int32_t y) {
-    if (p.src_shift == 0) return (int64_t)y * p.src_stride + x;
-    const int32_t mask = (1 << p.src_shift) - 1;
-    const int32_t sub = ((y & mask) << p.src_shift) | (x & mask);
-    return (int64_t)sub * p.src_span + (int64_t)(y >> p.src_shift) * p.src_stride + (x >> p.src_shift);
+__device__ __forceinline__ int64_t src_index(const Source &s, int32_t shift, int32_t x, int32_t y) {
+    if (shift == 0) return (int64_t)y * s.stride + x;
+    const int32_t mask = (1 << shift) - 1;
+    const int32_t sub = ((y & mask) << shift) | (x & mask);
+    return (int64_t)sub * s.span + (int64_t)(y >> shift) * s.stride + (x >> shift);
+}
+__device__ __forceinline__ int32_t load(const Source &s, int64_t i) {
+    return (i >= 0 && i < s.len) ? (int32_t)__ldg(s.p + i) : 0;
 }
 __device__ __forceinline__ int32_t interp_pair(int32_t a, int32_t b, int32_t total, int32_t shift, const int32_t *w) {
     const int32_t s = (int32_t)((uint32_t)w[0] * (uint32_t)a + (uint32_t)w[1] * (uint32_t)b);
     return shift < 0 ? s / total : s >> shift;
+}
+__device__ __forceinline__ int32_t clamp_byte(int32_t v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
+__device__ __forceinline__ int32_t blend256(int32_t a, int32_t b, int32_t w) {
+    return clamp_byte((a * (256 - w) + b * w) >> 8);
+}
+__device__ __forceinline__ int32_t blend255(int32_t a, int32_t b, int32_t w) {
+    return clamp_byte((a * (255 - w) + b * w + 255) >> 8);
 }
 // The last tile of render_tiles' loop along one axis that covers `pos`: index g (-1 for the leading
 // strip), its first sample and its length.
@@ -121,23 +140,17 @@ __device__ __forceinline__ void tile_of(int32_t pos, int32_t origin, int32_t blk
 }
 // motion_value: LUT entry k of set_threshold is trunc((k - 1024) * t / 256), computed here (no
 // saturation for t in 0..256)
-__device__ __forceinline__ int32_t motion(const RenderJob &J, const uint16_t *plane, int64_t i) {
+__device__ __forceinline__ int32_t motion(const RenderJob &J, const uint16_t *plane, int64_t i, int32_t t) {
     const int k = i < J.mlen ? __ldg(plane + i) : 1024;  // NEUTRAL beyond the plane
-    return ((k < kLut - 1 ? k : kLut - 1) - 1024) * J.lut_t / 256;
+    return ((k < kLut - 1 ? k : kLut - 1) - 1024) * t / 256;
 }
-
-// One tile's motion (motion_samples), whether its reads are direct (plane_covers and
-// tile_interior), and the motion interpolated down to row py (interpolate_motion_row).
-struct TileMotion {
-    int32_t rx0, rx1, ry0, ry1;
-    int32_t ma0, ma1;  // the mask interpolated down to the row (alpha_row)
-    bool direct;
-};
+// a mask sample: the mode's mask, or max_mask of the two
 __device__ __forceinline__ int32_t mask_at(const RenderJob &J, int64_t i) {
-    return (i >= 0 && i < J.mlen) ? __ldg(J.mask + i) : 0;
+    if (i < 0 || i >= J.mlen) return 0;
+    const int32_t a = __ldg(J.mask[0] + i);
+    return J.mask[1] ? max(a, (int32_t)__ldg(J.mask[1] + i)) : a;
 }
-__device__ __forceinline__ int32_t clamp_byte(int32_t v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
-// alpha_at_absolute (renderer.rs:2687-2722): used for the mask when the motion is not interpolated
+// alpha_at_absolute (renderer.rs:2687-2722): the mask's alpha on the zero-origin grid
 __device__ __forceinline__ int32_t alpha_absolute(const RenderJob &J, const RenderPlane &p, int32_t x, int32_t y) {
     const int32_t ox = p.morigin_x, oy = p.morigin_y, bw = p.block_w, bh = p.block_h;
     int32_t ix0 = 0, ix1 = 0, iy0 = 0, iy1 = 0;
@@ -150,91 +163,105 @@ __device__ __forceinline__ int32_t alpha_absolute(const RenderJob &J, const Rend
     const int32_t top = ((bw - fx) * tl + fx * tr) / bw, bottom = ((bw - fx) * bl + fx * br) / bw;
     return clamp_byte(((bh - fy) * top + fy * bottom) / bh);
 }
-__device__ __forceinline__ TileMotion tile_motion(const RenderJob &J, const RenderPlane &p, int32_t gx, int32_t bx,
-                                                  int32_t tw, int32_t gy, int32_t by, int32_t th, int32_t py,
-                                                  const int32_t (*syw)[2]) {
+
+struct Tile {  // one tile of render_tiles, seen from one output row
+    int32_t bx, by, tw, th;
+    int64_t i[4];  // motion-plane indices i00, i01, i10, i11
+};
+__device__ __forceinline__ Tile make_tile(const RenderJob &J, int32_t gx, int32_t bx, int32_t tw, int32_t gy,
+                                          int32_t by, int32_t th) {
+    Tile t;
+    t.bx = bx; t.by = by; t.tw = tw; t.th = th;
     const int64_t gw = J.grid_w;
-    const int64_t i00 = (int64_t)(gy > 0 ? gy : 0) * gw + (gx > 0 ? gx : 0);
+    t.i[0] = (int64_t)(gy > 0 ? gy : 0) * gw + (gx > 0 ? gx : 0);
     const int64_t nx = (gx >= 0 && gx != J.grid_w - 1) ? 1 : 0, ny = (gy >= 0 && gy != J.grid_h - 1) ? gw : 0;
-    int32_t sx[4], sy[4];
-    const bool c = p.x_div == 2;  // chroma: motion / 2 in both axes (4:2:0)
-    sx[0] = c ? motion(J, J.mx, i00) / 2 : motion(J, J.mx, i00);
-    sy[0] = c ? motion(J, J.my, i00) / 2 : motion(J, J.my, i00);
-    if (J.interp) {
-        const int64_t ii[3] = {i00 + nx, i00 + ny, i00 + ny + nx};
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-            sx[q + 1] = c ? motion(J, J.mx, ii[q]) / 2 : motion(J, J.mx, ii[q]);
-            sy[q + 1] = c ? motion(J, J.my, ii[q]) / 2 : motion(J, J.my, ii[q]);
-        }
-    } else {
-#pragma unroll
-        for (int q = 1; q < 4; q++) { sx[q] = sx[0]; sy[q] = sy[0]; }
-    }
-    TileMotion t;
-    t.direct = false;
-    t.ma0 = t.ma1 = 0;
-    if (J.mask != nullptr) {  // alpha_row
-        const int32_t a = mask_at(J, i00), b = mask_at(J, i00 + nx), cc = mask_at(J, i00 + ny),
-                      d = mask_at(J, i00 + ny + nx);
-        if (J.interp) {
-            const int32_t *wy = syw[min(py - by, kMaxBlock - 1)];
-            t.ma0 = interp_pair(a, cc, p.block_h, p.y_shift, wy);
-            t.ma1 = interp_pair(b, d, p.block_h, p.y_shift, wy);
-        } else {
-            t.ma0 = t.ma1 = a;
-        }
-    }
-    if (p.covers && p.step > 0) {  // tile_interior over the whole tile
-        int32_t mnx = sx[0], mxx = sx[0], mny = sy[0], mxy = sy[0];
-#pragma unroll
-        for (int q = 1; q < 4; q++) {
-            mnx = min(mnx, sx[q]); mxx = max(mxx, sx[q]);
-            mny = min(mny, sy[q]); mxy = max(mxy, sy[q]);
-        }
-        const int64_t st = p.step;
-        t.direct = (int64_t)bx * st + mnx >= 0 && (int64_t)by * st + mny >= 0 &&
-                   (int64_t)(bx + tw - 1) * st + mxx <= p.max_x && (int64_t)(by + th - 1) * st + mxy <= p.max_y;
-    }
-    if (J.interp) {
-        const int32_t *wy = syw[min(py - by, kMaxBlock - 1)];
-        t.rx0 = interp_pair(sx[0], sx[2], p.block_h, p.y_shift, wy);
-        t.rx1 = interp_pair(sx[1], sx[3], p.block_h, p.y_shift, wy);
-        t.ry0 = interp_pair(sy[0], sy[2], p.block_h, p.y_shift, wy);
-        t.ry1 = interp_pair(sy[1], sy[3], p.block_h, p.y_shift, wy);
-    } else {
-        t.rx0 = t.rx1 = sx[0];
-        t.ry0 = t.ry1 = sy[0];
-    }
+    t.i[1] = t.i[0] + nx; t.i[2] = t.i[0] + ny; t.i[3] = t.i[0] + ny + nx;
     return t;
 }
-// The source index sample (px, py) reads in its tile (interpolate_motion, then sample_plane's
-// direct or clamped position).
-__device__ __forceinline__ int64_t tile_sample(const RenderJob &J, const RenderPlane &p, const TileMotion &t,
-                                               int32_t px, int32_t bx, int32_t py, const int32_t (*sxw)[2]) {
-    int32_t dx = t.rx0, dy = t.ry0;
+
+// One motion set over a tile (motion_samples), interpolated down to row py (interpolate_motion_row),
+// with the extent of its four samples for tile_interior.
+struct SetRow {
+    int32_t rx0, rx1, ry0, ry1;
+    int32_t mnx, mxx, mny, mxy;
+};
+__device__ __forceinline__ SetRow set_row(const RenderJob &J, const RenderPlane &p, const Tile &t, int set,
+                                          int32_t py, const int32_t (*syw)[2]) {
+    const bool c = p.x_div == 2;  // chroma: motion / 2 in both axes (4:2:0)
+    const int32_t lt = J.lut_t[set];
+    int32_t sx[4], sy[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int64_t i = J.interp ? t.i[q] : t.i[0];
+        const int32_t mx = motion(J, J.mx[set], i, lt), my = motion(J, J.my[set], i, lt);
+        sx[q] = c ? mx / 2 : mx;
+        sy[q] = c ? my / 2 : my;
+    }
+    SetRow r;
+    r.mnx = min(min(sx[0], sx[1]), min(sx[2], sx[3]));
+    r.mxx = max(max(sx[0], sx[1]), max(sx[2], sx[3]));
+    r.mny = min(min(sy[0], sy[1]), min(sy[2], sy[3]));
+    r.mxy = max(max(sy[0], sy[1]), max(sy[2], sy[3]));
+    if (J.interp) {
+        const int32_t *wy = syw[min(py - t.by, kMaxBlock - 1)];
+        r.rx0 = interp_pair(sx[0], sx[2], p.block_h, p.y_shift, wy);
+        r.rx1 = interp_pair(sx[1], sx[3], p.block_h, p.y_shift, wy);
+        r.ry0 = interp_pair(sy[0], sy[2], p.block_h, p.y_shift, wy);
+        r.ry1 = interp_pair(sy[1], sy[3], p.block_h, p.y_shift, wy);
+    } else {
+        r.rx0 = r.rx1 = sx[0];
+        r.ry0 = r.ry1 = sy[0];
+    }
+    return r;
+}
+// tile_interior for the sets read in a tile
+__device__ __forceinline__ bool interior(const RenderPlane &p, const Tile &t, const SetRow &r) {
+    const int64_t st = p.step;
+    return (int64_t)t.bx * st + r.mnx >= 0 && (int64_t)t.by * st + r.mny >= 0 &&
+           (int64_t)(t.bx + t.tw - 1) * st + r.mxx <= p.max_x && (int64_t)(t.by + t.th - 1) * st + r.mxy <= p.max_y;
+}
+// the mask interpolated down to row py (alpha_row)
+__device__ __forceinline__ void mask_row(const RenderJob &J, const RenderPlane &p, const Tile &t, int32_t py,
+                                         const int32_t (*syw)[2], int32_t &m0, int32_t &m1) {
+    const int32_t a = mask_at(J, t.i[0]), b = mask_at(J, t.i[1]), cc = mask_at(J, t.i[2]), d = mask_at(J, t.i[3]);
+    if (J.interp) {
+        const int32_t *wy = syw[min(py - t.by, kMaxBlock - 1)];
+        m0 = interp_pair(a, cc, p.block_h, p.y_shift, wy);
+        m1 = interp_pair(b, d, p.block_h, p.y_shift, wy);
+    } else {
+        m0 = m1 = a;
+    }
+}
+// a sample's displaced source position (interpolate_motion, then sample_plane's direct or clamped read)
+__device__ __forceinline__ int64_t warp_index(const RenderJob &J, const RenderPlane &p, const Source &s,
+                                              const SetRow &r, bool direct, int32_t px, int32_t bx, int32_t py,
+                                              const int32_t (*sxw)[2]) {
+    int32_t dx = r.rx0, dy = r.ry0;
     if (J.interp) {
         const int32_t *wx = sxw[min(px - bx, kMaxBlock - 1)];
-        dx = interp_pair(t.rx0, t.rx1, p.block_w, p.x_shift, wx);
-        dy = interp_pair(t.ry0, t.ry1, p.block_w, p.x_shift, wx);
+        dx = interp_pair(r.rx0, r.rx1, p.block_w, p.x_shift, wx);
+        dy = interp_pair(r.ry0, r.ry1, p.block_w, p.x_shift, wx);
     }
     int32_t xs = px * p.step + dx, ys = py * p.step + dy;
-    if (!t.direct) {
+    if (!direct) {
         xs = min(max(xs, 0), p.max_x);
         ys = min(max(ys, 0), p.max_y);
     }
-    return src_index(p, xs, ys);
+    return src_index(s, J.shift, xs, ys);
 }
-// With a mask: the sample's alpha (alpha_at_row, or alpha_at_absolute without interpolation)
-__device__ __forceinline__ int32_t tile_alpha(const RenderJob &J, const RenderPlane &p, const TileMotion &t,
-                                              int32_t px, int32_t bx, int32_t py, const int32_t (*sxw)[2]) {
-    if (!J.interp) return alpha_absolute(J, p, px, py);
-    return clamp_byte(interp_pair(t.ma0, t.ma1, p.block_w, p.x_shift, sxw[min(px - bx, kMaxBlock - 1)]));
+// the mask's alpha at a sample (alpha_at_absolute on the zero-origin grid, else alpha_at_row)
+__device__ __forceinline__ int32_t alpha_at(const RenderJob &J, const RenderPlane &p, int32_t m0, int32_t m1,
+                                            int32_t px, int32_t bx, int32_t py, const int32_t (*sxw)[2]) {
+    if (J.zero_origin) return alpha_absolute(J, p, px, py);
+    if (!J.interp) return clamp_byte(m0);
+    return clamp_byte(interp_pair(m0, m1, p.block_w, p.x_shift, sxw[min(px - bx, kMaxBlock - 1)]));
 }
 
-// grid: (row length of the widest plane / (256 kPx), rows of the tallest plane, 3 planes)
-template <bool MASK>
-__global__ void __launch_bounds__(256) render_warp_kernel(const __grid_constant__ RenderJob J) {
+// DUAL false: the single warp (sources[0], set 0; mode1_pixel with the mask). DUAL true: the
+// two-source blend (set 0 reads source 0, set 1 source 1; mode11_or_13_pixel). Grid: (row length
+// of the widest plane / (256 kPx), rows of the tallest plane, 3 planes).
+template <bool DUAL, bool MASK>
+__global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ RenderJob J) {
     const RenderPlane &p = J.pl[blockIdx.z];
     // the plane's interpolation weights in shared memory (indexed per thread)
     __shared__ int32_t sxw[kMaxBlock][2], syw[kMaxBlock][2];
@@ -246,61 +273,134 @@ __global__ void __launch_bounds__(256) render_warp_kernel(const __grid_constant_
     const int32_t py = blockIdx.y;
     const int32_t px0 = (blockIdx.x * blockDim.x + threadIdx.x) * kPx;
     if (px0 >= p.width || py >= p.height || p.block_w <= 0 || p.block_h <= 0) return;
-    // kPx consecutive samples per thread, usually in one tile (its motion is then fetched once)
     int32_t gy, by, th;
     tile_of(py, p.origin_y, p.block_h, p.bh_log2, p.height, J.grid_h, gy, by, th);
     const int32_t pxl = min(px0 + kPx - 1, p.width - 1);
     int32_t gx, bx, tw, gxl, bxl, twl;
     tile_of(px0, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gx, bx, tw);
     tile_of(pxl, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gxl, bxl, twl);
-    int64_t si[kPx];
+    const bool shared_tile = gx == gxl;  // usually: then the tile's motion is fetched once
+    Tile t = make_tile(J, gx, bx, tw, gy, by, th);
+    SetRow r0 = set_row(J, p, t, 0, py, syw), r1 = r0;
+    if (DUAL) r1 = set_row(J, p, t, 1, py, syw);
+    int32_t m0 = 0, m1 = 0;
+    if (MASK) mask_row(J, p, t, py, syw, m0, m1);
+    auto direct_of = [&]() {  // plane_covers && tile_interior for the tile's sets
+        bool d = p.src[0].covers && p.step > 0 && interior(p, t, r0);
+        if (DUAL) d = d && p.src[1].covers && interior(p, t, r1);
+        return d;
+    };
+    bool direct = direct_of();
+    // indices first, then every load of the thread's samples, so the gathers overlap
+    int64_t i0[kPx], i1[kPx];
     int32_t alpha[kPx];
-    if (gx == gxl) {
-        const TileMotion t = tile_motion(J, p, gx, bx, tw, gy, by, th, py, syw);
 #pragma unroll
-        for (int k = 0; k < kPx; k++) {
-            si[k] = px0 + k <= pxl ? tile_sample(J, p, t, px0 + k, bx, py, sxw) : -1;
-            alpha[k] = MASK && px0 + k <= pxl ? tile_alpha(J, p, t, px0 + k, bx, py, sxw) : 0;
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < kPx; k++) {
-            si[k] = -1;
-            if (px0 + k > pxl) continue;
+    for (int k = 0; k < kPx; k++) {
+        const int32_t px = px0 + k;
+        i0[k] = i1[k] = -1;
+        alpha[k] = 0;
+        if (px > pxl) continue;
+        if (!shared_tile && k > 0) {
             int32_t gk, bk, twk;
-            tile_of(px0 + k, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gk, bk, twk);
-            const TileMotion t = tile_motion(J, p, gk, bk, twk, gy, by, th, py, syw);
-            si[k] = tile_sample(J, p, t, px0 + k, bk, py, sxw);
-            alpha[k] = MASK ? tile_alpha(J, p, t, px0 + k, bk, py, sxw) : 0;
+            tile_of(px, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gk, bk, twk);
+            if (gk != gx) {
+                gx = gk;
+                t = make_tile(J, gk, bk, twk, gy, by, th);
+                r0 = set_row(J, p, t, 0, py, syw);
+                if (DUAL) r1 = set_row(J, p, t, 1, py, syw);
+                if (MASK) mask_row(J, p, t, py, syw, m0, m1);
+                direct = direct_of();
+            }
         }
+        i0[k] = warp_index(J, p, p.src[0], r0, direct, px, t.bx, py, sxw);
+        if (DUAL) i1[k] = warp_index(J, p, p.src[1], r1, direct, px, t.bx, py, sxw);
+        if (MASK) alpha[k] = alpha_at(J, p, m0, m1, px, t.bx, py, sxw);
     }
-    uint8_t v[kPx];
+    const bool bases = MASK || (DUAL && J.mode13);  // the undisplaced samples (px * step <= max_x: no clamp)
+    int32_t v0[kPx], v1[kPx], c0[kPx], c1[kPx];
 #pragma unroll
-    for (int k = 0; k < kPx; k++) v[k] = (si[k] >= 0 && si[k] < p.src_len) ? __ldg(p.src + si[k]) : (uint8_t)0;
-    if (MASK) {  // mode1_pixel: blend_255(warped, base, alpha), base = the undisplaced sample
+    for (int k = 0; k < kPx; k++) {
+        const int32_t px = min(px0 + k, pxl);
+        v0[k] = load(p.src[0], i0[k]);
+        v1[k] = DUAL ? load(p.src[1], i1[k]) : 0;
+        c0[k] = bases ? load(p.src[0], src_index(p.src[0], J.shift, px * p.step, py * p.step)) : 0;
+        c1[k] = bases && DUAL ? load(p.src[1], src_index(p.src[1], J.shift, px * p.step, py * p.step)) : 0;
+    }
+    int32_t out[kPx];
 #pragma unroll
-        for (int k = 0; k < kPx; k++) {
-            const int64_t bi = src_index(p, (px0 + k) * p.step, py * p.step);
-            const int32_t base = (px0 + k < p.width && bi >= 0 && bi < p.src_len) ? __ldg(p.src + bi) : 0;
-            v[k] = (uint8_t)clamp_byte(((int32_t)v[k] * (255 - alpha[k]) + base * alpha[k] + 255) >> 8);
+    for (int k = 0; k < kPx; k++) {
+        int32_t v;
+        if (DUAL) {
+            const int32_t b = blend256(c0[k], c1[k], J.threshold);
+            if (J.mode13) v = min(max(b, min(v0[k], v1[k])), max(v0[k], v1[k]));  // mode13_pixel
+            else v = blend256(v0[k], v1[k], J.threshold);                          // mode11_pixel
+            if (MASK) v = blend255(v, b, alpha[k]);
+        } else {
+            v = MASK ? blend255(v0[k], c0[k], alpha[k]) : v0[k];  // mode1_pixel
         }
+        out[k] = v;
     }
-    uint8_t *out = p.dst + (int64_t)py * p.dst_stride + px0;
+    uint8_t *o = p.dst + (int64_t)py * p.dst_stride + px0;
 #pragma unroll
     for (int k = 0; k < kPx; k++)
-        if (px0 + k < p.width) out[k] = v[k];
+        if (px0 + k <= pxl) o[k] = (uint8_t)out[k];
 }
 
-}  // namespace
+// Per-plane constants of one frame (plane_params for chroma = plane > 0), the sources' layouts and
+// plane_covers; validation of the caller's arguments.
+int setup(RenderJob &J, const svpf_render_config *cfg, int nsrc, const uint8_t *const *const src[2],
+          const int64_t *const stride[2], const int64_t *const len[2], int32_t src_shift, uint8_t *const dst[3],
+          const int64_t dst_stride[3], int32_t &most_w, int32_t &most_h) {
+    const int32_t cd = 2;  // SmoothFps renders 4:2:0 (CpuConfig::chroma_y_div)
+    J.mlen = (int64_t)cfg->grid_w * cfg->grid_h;
+    J.grid_w = cfg->grid_w;
+    J.grid_h = cfg->grid_h;
+    J.shift = src_shift;
+    most_w = most_h = 0;
+    for (int pl = 0; pl < 3; pl++) {
+        RenderPlane &p = J.pl[pl];
+        const bool c = pl > 0;
+        p.dst = dst[pl];
+        p.dst_stride = dst_stride[pl];
+        p.width = c ? cfg->width / 2 : cfg->width;
+        p.height = c ? cfg->height / cd : cfg->height;
+        p.block_w = c ? cfg->block_w / 2 : cfg->block_w;
+        p.block_h = c ? cfg->block_h / cd : cfg->block_h;
+        p.morigin_x = c ? cfg->origin_x / 2 : cfg->origin_x;
+        p.morigin_y = c ? cfg->origin_y / cd : cfg->origin_y;
+        p.origin_x = J.zero_origin ? 0 : p.morigin_x;
+        p.origin_y = J.zero_origin ? 0 : p.morigin_y;
+        p.x_shift = cpu_map(c ? cfg->block_w / 2 : cfg->block_w);
+        p.y_shift = cpu_map(c ? cfg->block_h / 2 : cfg->block_h);
+        p.x_div = c ? 2 : 1;
+        p.step = cfg->source_step;
+        p.max_x = sat_step_max(p.width, p.step);
+        p.max_y = sat_step_max(p.height, p.step);
+        weights(p.block_w, p.x_shift, p.xw);
+        weights(p.block_h, p.y_shift, p.yw);
+        p.bw_log2 = p.block_w > 0 && (p.block_w & (p.block_w - 1)) == 0 ? 31 - __builtin_clz((unsigned)p.block_w) : -1;
+        p.bh_log2 = p.block_h > 0 && (p.block_h & (p.block_h - 1)) == 0 ? 31 - __builtin_clz((unsigned)p.block_h) : -1;
+        if (!p.dst || p.dst_stride < p.width) return SVPF_EINVAL;
+        for (int s = 0; s < nsrc; s++) {
+            Source &S = p.src[s];
+            S.p = src[s][pl];
+            S.len = len[s][pl];
+            S.stride = stride[s][pl];
+            S.span = S.stride * p.height;  // sub-planes of a super clip's level 0
+            if (!S.p || S.stride < 0 || S.len < 0) return SVPF_EINVAL;
+            S.covers = covers(S, src_shift, p.step, p.max_x, p.max_y);
+        }
+        if (p.block_w > 0 && p.block_h > 0) {
+            most_w = p.width > most_w ? p.width : most_w;
+            most_h = p.height > most_h ? p.height : most_h;
+        }
+    }
+    return SVPF_OK;
+}
 
-extern "C" {
-
-int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, int32_t mode1, int32_t interp,
-                            const uint8_t *const src[3], const int64_t src_stride[3], const int64_t src_len[3],
-                            int32_t src_shift, const uint16_t *motion_x, const uint16_t *motion_y,
-                            const uint8_t *mask, uint8_t *const dst[3], const int64_t dst_stride[3], void *stream) {
+int check_common(const svpf_render_config *cfg, int32_t threshold, int32_t src_shift) {
     if (int rc = svpf::require_device()) return rc;
-    if (!cfg || !src || !src_stride || !src_len || !dst || !dst_stride || !motion_x || !motion_y) {
+    if (!cfg) {
         svpf::set_last_error("render: null argument");
         return SVPF_EINVAL;
     }
@@ -312,78 +412,103 @@ int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, in
         svpf::set_last_error("render: super-plane shift must be log2(source_step), pel 1, 2 or 4");
         return SVPF_EINVAL;
     }
-    if (cfg->width <= 0 || cfg->height <= 0 || cfg->grid_w <= 0 || cfg->grid_h <= 0 || cfg->source_step <= 0 ||
-        cfg->block_w <= 0 || cfg->block_h <= 0) {
-        return SVPF_OK;  // render_tiles draws nothing
-    }
-    RenderJob *J = new RenderJob;
-    memset(J, 0, sizeof(*J));
-    // set_threshold: mode 1 warps with the inverse LUT, mode 2 with the threshold LUT
-    J->lut_t = mode1 ? 256 - threshold : threshold;
-    J->mx = motion_x;
-    J->my = motion_y;
-    J->mask = mask;
-    J->mlen = (int64_t)cfg->grid_w * cfg->grid_h;
-    J->grid_w = cfg->grid_w;
-    J->grid_h = cfg->grid_h;
-    J->interp = interp != 0;
-    const int32_t cd = 2;  // SmoothFps renders 4:2:0 (CpuConfig::chroma_y_div)
-    int32_t most_w = 0, most_h = 0;
-    for (int pl = 0; pl < 3; pl++) {
-        RenderPlane &p = J->pl[pl];
-        const bool c = pl > 0;
-        const bool zero = !interp;  // plane_params(chroma, zero_origin = !interp)
-        p.src = src[pl];
-        p.src_len = src_len[pl];
-        p.src_stride = src_stride[pl];
-        p.src_shift = src_shift;
-        p.dst = dst[pl];
-        p.dst_stride = dst_stride[pl];
-        p.width = c ? cfg->width / 2 : cfg->width;
-        p.height = c ? cfg->height / cd : cfg->height;
-        p.src_span = p.src_stride * p.height;  // sub-planes of a super clip's level 0
-        p.block_w = c ? cfg->block_w / 2 : cfg->block_w;
-        p.block_h = c ? cfg->block_h / cd : cfg->block_h;
-        p.origin_x = zero ? 0 : (c ? cfg->origin_x / 2 : cfg->origin_x);
-        p.origin_y = zero ? 0 : (c ? cfg->origin_y / cd : cfg->origin_y);
-        p.morigin_x = c ? cfg->origin_x / 2 : cfg->origin_x;
-        p.morigin_y = c ? cfg->origin_y / cd : cfg->origin_y;
-        p.x_shift = cpu_map(c ? cfg->block_w / 2 : cfg->block_w);
-        p.y_shift = cpu_map(c ? cfg->block_h / 2 : cfg->block_h);
-        p.x_div = c ? 2 : 1;
-        p.y_div = c ? cd : 1;
-        p.step = cfg->source_step;
-        p.max_x = sat_step_max(p.width, p.step);
-        p.max_y = sat_step_max(p.height, p.step);
-        weights(p.block_w, p.x_shift, p.xw);
-        weights(p.block_h, p.y_shift, p.yw);
-        if (!p.src || !p.dst || p.src_stride < 0 || p.dst_stride < p.width || p.src_len < 0) {
-            delete J;
-            svpf::set_last_error("render: bad plane buffers");
-            return SVPF_EINVAL;
-        }
-        p.covers = covers(p);
-        p.bw_log2 = (p.block_w & (p.block_w - 1)) == 0 ? 31 - __builtin_clz((unsigned)p.block_w) : -1;
-        p.bh_log2 = (p.block_h & (p.block_h - 1)) == 0 ? 31 - __builtin_clz((unsigned)p.block_h) : -1;
-        if (p.block_w > 0 && p.block_h > 0) {
-            most_w = p.width > most_w ? p.width : most_w;
-            most_h = p.height > most_h ? p.height : most_h;
-        }
-    }
+    return SVPF_OK;
+}
+bool draws_nothing(const svpf_render_config *cfg) {  // render_tiles returns at once
+    return cfg->width <= 0 || cfg->height <= 0 || cfg->grid_w <= 0 || cfg->grid_h <= 0 || cfg->source_step <= 0 ||
+           cfg->block_w <= 0 || cfg->block_h <= 0;
+}
+int launch(const RenderJob &J, bool dual, bool mask, int32_t most_w, int32_t most_h, void *stream) {
     cudaError_t e = cudaSuccess;
     if (most_w > 0 && most_h > 0) {
         dim3 grid((unsigned)((most_w + 256 * kPx - 1) / (256 * kPx)), (unsigned)most_h, 3);
-        if (mask) render_warp_kernel<true><<<grid, 256, 0, (cudaStream_t)stream>>>(*J);
-        else render_warp_kernel<false><<<grid, 256, 0, (cudaStream_t)stream>>>(*J);
+        cudaStream_t st = (cudaStream_t)stream;
+        if (dual) {
+            if (mask) render_kernel<true, true><<<grid, 256, 0, st>>>(J);
+            else render_kernel<true, false><<<grid, 256, 0, st>>>(J);
+        } else {
+            if (mask) render_kernel<false, true><<<grid, 256, 0, st>>>(J);
+            else render_kernel<false, false><<<grid, 256, 0, st>>>(J);
+        }
         svpf::add_launches(1);
         e = cudaGetLastError();
     }
-    delete J;
     if (e != cudaSuccess) {
         svpf::set_last_error(std::string("render: ") + cudaGetErrorString(e));
         return SVPF_ECUDA;
     }
     return SVPF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, int32_t mode1, int32_t interp,
+                            const uint8_t *const src[3], const int64_t src_stride[3], const int64_t src_len[3],
+                            int32_t src_shift, const uint16_t *motion_x, const uint16_t *motion_y,
+                            const uint8_t *mask, uint8_t *const dst[3], const int64_t dst_stride[3], void *stream) {
+    if (int rc = check_common(cfg, threshold, src_shift)) return rc;
+    if (!src || !src_stride || !src_len || !dst || !dst_stride || !motion_x || !motion_y) {
+        svpf::set_last_error("render: null argument");
+        return SVPF_EINVAL;
+    }
+    if (draws_nothing(cfg)) return SVPF_OK;
+    RenderJob *J = new RenderJob;
+    memset(J, 0, sizeof(*J));
+    // set_threshold: mode 1 warps with the inverse LUT, mode 2 with the threshold LUT
+    J->lut_t[0] = mode1 ? 256 - threshold : threshold;
+    J->mx[0] = motion_x;
+    J->my[0] = motion_y;
+    J->mask[0] = mask;
+    J->interp = interp != 0;
+    J->zero_origin = interp == 0;  // plane_params(chroma, zero_origin = !interp)
+    const uint8_t *const *srcs[2] = {src, nullptr};
+    const int64_t *strides[2] = {src_stride, nullptr}, *lens[2] = {src_len, nullptr};
+    int32_t mw, mh;
+    int rc = setup(*J, cfg, 1, srcs, strides, lens, src_shift, dst, dst_stride, mw, mh);
+    if (rc) svpf::set_last_error("render: bad plane buffers");
+    else rc = launch(*J, false, mask != nullptr, mw, mh, stream);
+    delete J;
+    return rc;
+}
+
+int svpf_render_blend_device(const svpf_render_config *cfg, int32_t threshold, int32_t mode13, int32_t interp,
+                             int32_t zero_origin, const uint8_t *const src0[3], const int64_t src0_stride[3],
+                             const int64_t src0_len[3], const uint8_t *const src1[3], const int64_t src1_stride[3],
+                             const int64_t src1_len[3], int32_t src_shift, const uint16_t *motion0_x,
+                             const uint16_t *motion0_y, const uint16_t *motion1_x, const uint16_t *motion1_y,
+                             const uint8_t *mask_a, const uint8_t *mask_b, uint8_t *const dst[3],
+                             const int64_t dst_stride[3], void *stream) {
+    if (int rc = check_common(cfg, threshold, src_shift)) return rc;
+    if (!src0 || !src0_stride || !src0_len || !src1 || !src1_stride || !src1_len || !dst || !dst_stride ||
+        !motion0_x || !motion0_y || !motion1_x || !motion1_y || (!mask_a) != (!mask_b)) {
+        svpf::set_last_error("render: null argument (masks: both or neither)");
+        return SVPF_EINVAL;
+    }
+    if (draws_nothing(cfg)) return SVPF_OK;
+    RenderJob *J = new RenderJob;
+    memset(J, 0, sizeof(*J));
+    J->lut_t[0] = threshold;        // motion0 with the threshold LUT
+    J->lut_t[1] = 256 - threshold;  // motion1 with the inverse LUT
+    J->mx[0] = motion0_x;
+    J->my[0] = motion0_y;
+    J->mx[1] = motion1_x;
+    J->my[1] = motion1_y;
+    J->mask[0] = mask_a;
+    J->mask[1] = mask_b;
+    J->interp = interp != 0;
+    J->zero_origin = zero_origin != 0 || interp == 0;
+    J->threshold = threshold;
+    J->mode13 = mode13 != 0;
+    const uint8_t *const *srcs[2] = {src0, src1};
+    const int64_t *strides[2] = {src0_stride, src1_stride}, *lens[2] = {src0_len, src1_len};
+    int32_t mw, mh;
+    int rc = setup(*J, cfg, 2, srcs, strides, lens, src_shift, dst, dst_stride, mw, mh);
+    if (rc) svpf::set_last_error("render: bad plane buffers");
+    else rc = launch(*J, true, mask_a != nullptr, mw, mh, stream);
+    delete J;
+    return rc;
 }
 
 }  // extern "C"

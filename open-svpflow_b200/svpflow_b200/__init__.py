@@ -109,6 +109,9 @@ def lib() -> ctypes.CDLL:
             "svpf_vector_planes_device": (I32, [P(I32), _VP, SZ, I32, I32, I32, I32, _VP, _VP, _VP]),
             "svpf_render_warp_device": (I32, [P(RenderConfig), I32, I32, I32, P(_VP), P(I64), P(I64), I32, _VP, _VP,
                                               _VP, P(_VP), P(I64), _VP]),
+            "svpf_render_blend_device": (I32, [P(RenderConfig), I32, I32, I32, I32, P(_VP), P(I64), P(I64), P(_VP),
+                                               P(I64), P(I64), I32, _VP, _VP, _VP, _VP, _VP, _VP, P(_VP), P(I64),
+                                               _VP]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -500,3 +503,20 @@ def render_warp_device(cfg: dict, threshold: int, mode1: bool, interp: bool, src
                                          arr(ctypes.c_int64, src_lens), int(src_shift), motion_x_ptr, motion_y_ptr,
                                          mask_ptr or None, arr(_VP, dst_ptrs), arr(ctypes.c_int64, dst_strides),
                                          stream))
+
+
+def render_blend_device(cfg: dict, threshold: int, mode13: bool, interp: bool, zero_origin: bool, src0_ptrs,
+                        src0_strides, src0_lens, src1_ptrs, src1_strides, src1_lens, src_shift: int, motion0,
+                        motion1, dst_ptrs, dst_strides, masks=None, stream: int = 0):
+    """SmoothFps's two-source blend (algorithms 11 / 13) of one frame's three planes on the device;
+    motion0 / motion1 = (x_ptr, y_ptr) device planes, masks = None or (a_ptr, b_ptr); see
+    svpf_render_blend_device."""
+    c = RenderConfig(**{k: int(cfg[k]) for k, _ in RenderConfig._fields_})
+    arr = lambda t, v: (t * 3)(*[int(x) for x in v])
+    ma, mb = masks if masks else (None, None)
+    _check(lib().svpf_render_blend_device(ctypes.byref(c), int(threshold), int(mode13), int(interp), int(zero_origin),
+                                          arr(_VP, src0_ptrs), arr(ctypes.c_int64, src0_strides),
+                                          arr(ctypes.c_int64, src0_lens), arr(_VP, src1_ptrs),
+                                          arr(ctypes.c_int64, src1_strides), arr(ctypes.c_int64, src1_lens),
+                                          int(src_shift), motion0[0], motion0[1], motion1[0], motion1[1], ma, mb,
+                                          arr(_VP, dst_ptrs), arr(ctypes.c_int64, dst_strides), stream))

@@ -454,6 +454,8 @@ def _setup(L):
     L.or_total_counters.argtypes = [P(ctypes.c_uint64), ctypes.c_int32]
     if hasattr(L, "or_render_luts"):  # the 8-bit build only
         L.or_render_luts.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
+        L.or_render_dual_plane.argtypes = [P(RenderConfig)] + [ctypes.c_int32] * 5 + [P(RPlane), P(RPlane)] + \
+            [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
         L.or_render_warp_plane.argtypes = [P(RenderConfig), ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
                                            P(RPlane), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
@@ -759,4 +761,23 @@ def render_warp_plane(cfg: dict, chroma: bool, interp: bool, lut: np.ndarray, sr
         assert mk.size == mx.size
     lib().or_render_warp_plane(ctypes.byref(c), int(chroma), int(interp), _ptr(lut), ctypes.byref(pl), _ptr(mx),
                                _ptr(my), mx.size, None if mk is None else _ptr(mk), _ptr(dst), dst_stride, dst.size)
+    return dst.reshape(dst_rows, dst_stride)
+
+
+def render_dual_plane(cfg: dict, chroma: bool, interp: bool, zero_origin: bool, mode13: bool, threshold: int,
+                      srcs, strides, spans, shift: int, motion0, motion1, dst_stride: int, dst_rows: int,
+                      mask: np.ndarray = None) -> np.ndarray:
+    """render_mode11_or_13 for one plane: srcs / strides / spans of sources 0 and 1, motion0 / motion1 =
+    (mx, my) of the two sets, mask = max_mask(a, b) or None."""
+    c = RenderConfig(**{k: int(cfg[k]) for k, _ in RenderConfig._fields_})
+    ss = [np.ascontiguousarray(x, dtype=np.uint8).reshape(-1) for x in srcs]
+    pls = [RPlane(ss[i].ctypes.data, ss[i].size, strides[i], spans[i], shift) for i in range(2)]
+    ms = [np.ascontiguousarray(m, dtype=np.uint16).reshape(-1) for m in (*motion0, *motion1)]
+    n = ms[0].size
+    mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+    dst = np.zeros(dst_rows * dst_stride, dtype=np.uint8)
+    lib().or_render_dual_plane(ctypes.byref(c), int(chroma), int(interp), int(zero_origin), int(mode13),
+                               int(threshold), ctypes.byref(pls[0]), ctypes.byref(pls[1]),
+                               *[_ptr(m) for m in ms], n, None if mk is None else _ptr(mk), _ptr(dst), dst_stride,
+                               dst.size)
     return dst.reshape(dst_rows, dst_stride)

@@ -2144,4 +2144,133 @@ void or_render_warp_plane(const or_render_config *c, int32_t chroma, int32_t int
         }
     }
 }
+
+/* render_dual_warp_rows (:1031-1172) with mode11_or_13_pixel (:2918-2943), as render_mode11_or_13
+ * (:330-438) and its zero-origin variant drive it: motion set 0 scaled by the threshold LUT reads
+ * source 0, set 1 scaled by the inverse LUT reads source 1; mask = max_mask(a, b) (:2908-2915) or NULL. */
+static i32 r_blend256(i32 a, i32 b, i32 w) { return r_byte((a * (256 - w) + b * w) >> 8); }
+void or_render_dual_plane(const or_render_config *c, int32_t chroma, int32_t interp, int32_t zero_origin,
+                          int32_t mode13, int32_t threshold, const or_rplane *src0, const or_rplane *src1,
+                          const uint16_t *mx0, const uint16_t *my0, const uint16_t *mx1, const uint16_t *my1,
+                          size_t mlen, const uint8_t *mask, uint8_t *dst, size_t dst_stride, size_t dst_len) {
+    int16_t inv[2048], thr[2048];
+    or_render_luts(threshold, inv, thr);
+    rparams P, MP;
+    r_params(c, chroma, zero_origin, &P);
+    r_params(c, chroma, 0, &MP);
+    const rparams *p = &P;
+    i32 gw = (i32)c->grid_w, gh = (i32)c->grid_h;
+    if (p->width <= 0 || p->height <= 0 || p->block_w <= 0 || p->block_h <= 0 || gw <= 0 || gh <= 0) return;
+    i32 rows_end = chroma ? c->height / c->chroma_y_div : c->height;
+    int covers = r_covers(src0, p) && r_covers(src1, p);
+    for (i32 gy = -1; gy < gh; gy++) {
+        i32 base_y = gy < 0 ? 0 : p->origin_y + p->block_h * gy;
+        i32 height = gy < 0 ? p->origin_y : p->block_h;
+        if (base_y + p->block_h >= p->height || gy == gh - 1) height = p->height - base_y;
+        i32 end_y = base_y + height < rows_end ? base_y + height : rows_end;
+        i32 clipped_y = base_y > 0 ? base_y : 0;
+        height = end_y - clipped_y;
+        if (height <= 0) continue;
+        for (i32 gx = -1; gx < gw; gx++) {
+            i32 base_x = gx < 0 ? 0 : p->origin_x + p->block_w * gx;
+            i32 width = gx < 0 ? p->origin_x : p->block_w;
+            if (base_x + p->block_w >= p->width || gx == gw - 1) width = p->width - base_x;
+            if (width <= 0) continue;
+            usize x0 = (usize)(gx > 0 ? gx : 0), y0 = (usize)(gy > 0 ? gy : 0);
+            usize nx = (gx >= 0 && gx != gw - 1) ? 1 : 0, ny = (gy >= 0 && gy != gh - 1) ? (usize)gw : 0;
+            usize ii[4] = {y0 * (usize)gw + x0, 0, 0, 0};
+            ii[1] = ii[0] + nx; ii[2] = ii[0] + ny; ii[3] = ii[0] + ny + nx;
+            i32 tx = base_x, ty = clipped_y;
+            i32 sx[2][4], sy[2][4];
+            for (int set = 0; set < 2; set++) {
+                const int16_t *lut = set ? inv : thr;
+                const uint16_t *mx = set ? mx1 : mx0, *my = set ? my1 : my0;
+                for (int q = 0; q < 4; q++) {
+                    usize i = interp ? ii[q] : ii[0];
+                    sx[set][q] = r_motion(lut, mx, mlen, i) / p->x_div;
+                    sy[set][q] = r_motion(lut, my, mlen, i) / p->y_div;
+                }
+            }
+            int direct = 0;
+            if (covers && p->step > 0) {
+                i32 mnx = INT32_MAX, mxx = INT32_MIN, mny = INT32_MAX, mxy = INT32_MIN;
+                for (int set = 0; set < 2; set++)
+                    for (int q = 0; q < 4; q++) {
+                        mnx = sx[set][q] < mnx ? sx[set][q] : mnx; mxx = sx[set][q] > mxx ? sx[set][q] : mxx;
+                        mny = sy[set][q] < mny ? sy[set][q] : mny; mxy = sy[set][q] > mxy ? sy[set][q] : mxy;
+                    }
+                int64_t st = p->step;
+                direct = (int64_t)tx * st + mnx >= 0 && (int64_t)ty * st + mny >= 0 &&
+                         (int64_t)(tx + width - 1) * st + mxx <= p->max_x && (int64_t)(ty + height - 1) * st + mxy <= p->max_y;
+            }
+            for (i32 y = 0; y < height; y++) {
+                i32 local_y = clipped_y - base_y + y;
+                i32 source_y = (ty + y) * p->step;
+                usize start = (usize)(ty + y) * dst_stride + (usize)tx;
+                if (start + (usize)width > dst_len) continue;
+                const i32 *wy = p->yw[local_y < 0 ? 0 : (local_y > 31 ? 31 : local_y)];
+                i32 row[2][2][2]; /* set, x/y, left/right */
+                for (int set = 0; set < 2; set++) {
+                    if (!interp) { row[set][0][0] = row[set][0][1] = sx[set][0]; row[set][1][0] = row[set][1][1] = sy[set][0]; }
+                    else {
+                        row[set][0][0] = r_interp(sx[set][0], sx[set][2], p->block_h, p->y_shift, wy);
+                        row[set][0][1] = r_interp(sx[set][1], sx[set][3], p->block_h, p->y_shift, wy);
+                        row[set][1][0] = r_interp(sy[set][0], sy[set][2], p->block_h, p->y_shift, wy);
+                        row[set][1][1] = r_interp(sy[set][1], sy[set][3], p->block_h, p->y_shift, wy);
+                    }
+                }
+                i32 mrow[2] = {0, 0};
+                if (mask) {
+                    i32 m[4];
+                    for (int q = 0; q < 4; q++) m[q] = ii[q] < mlen ? mask[ii[q]] : 0;
+                    if (!interp) { mrow[0] = mrow[1] = m[0]; }
+                    else {
+                        mrow[0] = r_interp(m[0], m[2], p->block_h, p->y_shift, wy);
+                        mrow[1] = r_interp(m[1], m[3], p->block_h, p->y_shift, wy);
+                    }
+                }
+                for (i32 x = 0; x < width; x++) {
+                    i32 px = tx + x, source_x = px * p->step;
+                    const i32 *wx = p->xw[x > 31 ? 31 : x];
+                    i32 v[2], cur[2];
+                    for (int set = 0; set < 2; set++) {
+                        const or_rplane *src = set ? src1 : src0;
+                        i32 dx = row[set][0][0], dy = row[set][1][0];
+                        if (interp) {
+                            dx = r_interp(row[set][0][0], row[set][0][1], p->block_w, p->x_shift, wx);
+                            dy = r_interp(row[set][1][0], row[set][1][1], p->block_w, p->x_shift, wx);
+                        }
+                        i32 xs = source_x + dx, ys = source_y + dy, bxs = source_x, bys = source_y;
+                        if (!direct) {
+                            xs = xs < 0 ? 0 : (xs > p->max_x ? p->max_x : xs);
+                            ys = ys < 0 ? 0 : (ys > p->max_y ? p->max_y : ys);
+                            bxs = bxs > p->max_x ? p->max_x : bxs;
+                            bys = bys > p->max_y ? p->max_y : bys;
+                        }
+                        usize idx = r_index(src, (usize)(int64_t)xs, (usize)(int64_t)ys);
+                        usize bi = r_index(src, (usize)(int64_t)bxs, (usize)(int64_t)bys);
+                        v[set] = idx < src->len ? src->data[idx] : 0;
+                        cur[set] = bi < src->len ? src->data[bi] : 0;
+                    }
+                    i32 motion;
+                    if (mode13) {
+                        i32 b = r_blend256(cur[0], cur[1], threshold);
+                        i32 lo = v[0] < v[1] ? v[0] : v[1], hi = v[0] < v[1] ? v[1] : v[0];
+                        motion = b < lo ? lo : (b > hi ? hi : b);
+                    } else {
+                        motion = r_blend256(v[0], v[1], threshold);
+                    }
+                    if (mask) {
+                        i32 alpha = zero_origin ? r_alpha_abs(mask, mlen, &MP, (usize)c->grid_w, px, ty + y)
+                                                : r_byte(interp ? r_interp(mrow[0], mrow[1], p->block_w, p->x_shift, wx)
+                                                                : mrow[0]);
+                        i32 base = r_blend256(cur[0], cur[1], threshold);
+                        motion = r_byte((motion * (255 - alpha) + base * alpha + 255) >> 8);
+                    }
+                    dst[start + (usize)x] = (uint8_t)motion;
+                }
+            }
+        }
+    }
+}
 #endif

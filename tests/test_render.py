@@ -148,6 +148,159 @@ def _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my, mask=
     return dst
 
 
+def _py_dual(cfg, chroma, interp, zero, mode13, thr, srcs, strides, spans, shift, mot0, mot1, mask=None):
+    """render_dual_warp_rows + mode11_or_13_pixel (renderer.rs:1031-1172, :2918-2943) in plain Python."""
+    cmap = lambda v: CPU_MAP[v - 1] if 1 <= v <= 32 else -1
+    cd = cfg["chroma_y_div"]
+    if chroma:
+        W, H, BW, BH = cfg["width"] // 2, cfg["height"] // cd, cfg["block_w"] // 2, cfg["block_h"] // cd
+        mox, moy = cfg["origin_x"] // 2, cfg["origin_y"] // cd
+        xs_, ys_, xd, yd = cmap(cfg["block_w"] // 2), cmap(cfg["block_h"] // 2), 2, cd
+    else:
+        W, H, BW, BH = cfg["width"], cfg["height"], cfg["block_w"], cfg["block_h"]
+        mox, moy = cfg["origin_x"], cfg["origin_y"]
+        xs_, ys_, xd, yd = cmap(BW), cmap(BH), 1, 1
+    ox, oy = (0, 0) if zero else (mox, moy)
+    step = cfg["source_step"]
+    maxx, maxy = max(W * step - 1, 0), max(H * step - 1, 0)
+
+    def weights(total, sh):
+        out = [(0, 0)] * 32
+        for p in range(min(total, 32)):
+            c = lambda v: int(math.ceil(v * (1 << max(sh, 0)) / total - 0.5))
+            out[p] = (total - p, p) if sh < 0 else (c(total - p), c(p))
+        return out
+
+    xw, yw = weights(BW, xs_), weights(BH, ys_)
+    ip = lambda a, b, total, sh, w: int((w[0] * a + w[1] * b) / total) if sh < 0 else (w[0] * a + w[1] * b) >> sh
+    inv, tl = orc.render_luts(thr)
+    luts = [tl, inv]
+    gw, gh = cfg["grid_w"], cfg["grid_h"]
+    byte = lambda v: min(max(v, 0), 255)
+    b256 = lambda a, b, w: byte((a * (256 - w) + b * w) >> 8)
+
+    def index(k, x, y):
+        if shift == 0:
+            return y * strides[k] + x
+        m = (1 << shift) - 1
+        return (((y & m) << shift) | (x & m)) * spans[k] + (y >> shift) * strides[k] + (x >> shift)
+
+    def mat(x, y):
+        i = y * gw + x
+        return int(mask[i]) if x >= 0 and y >= 0 and i < len(mask) else 0
+
+    def alpha_abs(x, y):
+        ix0 = ix1 = iy0 = iy1 = 0
+        if mox <= x:
+            ix0 = (x - mox) // BW
+            ix1 = ix0 + 1
+        if moy <= y:
+            iy0 = (y - moy) // BH
+            iy1 = iy0 + 1
+        fx = (x - mox) % BW if mox < x else 0
+        fy = (y - moy) % BH if moy < y else 0
+        top = ((BW - fx) * mat(ix0, iy0) + fx * mat(ix1, iy0)) // BW
+        bot = ((BW - fx) * mat(ix0, iy1) + fx * mat(ix1, iy1)) // BW
+        return byte(((BH - fy) * top + fy * bot) // BH)
+
+    covers = all((shift == 0 or (1 << shift) == step) and index(k, maxx, maxy) < len(srcs[k]) for k in range(2))
+    dst = np.zeros((H, W), dtype=np.uint8)
+    for gy in range(-1, gh):
+        by = 0 if gy < 0 else oy + BH * gy
+        th = oy if gy < 0 else BH
+        if by + BH >= H or gy == gh - 1:
+            th = H - by
+        th = min(by + th, H) - max(by, 0)
+        if th <= 0:
+            continue
+        for gx in range(-1, gw):
+            bx = 0 if gx < 0 else ox + BW * gx
+            tw = ox if gx < 0 else BW
+            if bx + BW >= W or gx == gw - 1:
+                tw = W - bx
+            if tw <= 0:
+                continue
+            i00 = max(gy, 0) * gw + max(gx, 0)
+            nx = 1 if (gx >= 0 and gx != gw - 1) else 0
+            ny = gw if (gy >= 0 and gy != gh - 1) else 0
+            idx = [i00, i00 + nx, i00 + ny, i00 + ny + nx] if interp else [i00] * 4
+            S = []
+            for k, (mx, my) in enumerate((mot0, mot1)):
+                mv = lambda pl, i: int(luts[k][min(int(pl[i]) if i < len(pl) else 1024, 2047)])
+                S.append(([int(mv(mx, i) / xd) for i in idx], [int(mv(my, i) / yd) for i in idx]))
+            allx = S[0][0] + S[1][0]
+            ally = S[0][1] + S[1][1]
+            direct = covers and bx * step + min(allx) >= 0 and by * step + min(ally) >= 0 and \
+                (bx + tw - 1) * step + max(allx) <= maxx and (by + th - 1) * step + max(ally) <= maxy
+            for y in range(th):
+                wy = yw[min(y, 31)]
+                rows = []
+                for sx, sy in S:
+                    rows.append(([ip(sx[0], sx[2], BH, ys_, wy), ip(sx[1], sx[3], BH, ys_, wy)],
+                                 [ip(sy[0], sy[2], BH, ys_, wy), ip(sy[1], sy[3], BH, ys_, wy)]) if interp
+                                else ([sx[0]] * 2, [sy[0]] * 2))
+                if mask is not None:
+                    mk = [int(mask[i]) if i < len(mask) else 0 for i in [i00, i00 + nx, i00 + ny, i00 + ny + nx]]
+                    mrow = [ip(mk[0], mk[2], BH, ys_, wy), ip(mk[1], mk[3], BH, ys_, wy)] if interp else [mk[0]] * 2
+                for x in range(tw):
+                    wx = xw[min(x, 31)]
+                    vals, curs = [], []
+                    for k in range(2):
+                        rx, ry = rows[k]
+                        dx = ip(rx[0], rx[1], BW, xs_, wx) if interp else rx[0]
+                        dy = ip(ry[0], ry[1], BW, xs_, wx) if interp else ry[0]
+                        X, Y = (bx + x) * step + dx, (by + y) * step + dy
+                        BX, BY = (bx + x) * step, (by + y) * step
+                        if not direct:
+                            X, Y = min(max(X, 0), maxx), min(max(Y, 0), maxy)
+                            BX, BY = min(BX, maxx), min(BY, maxy)
+                        i, bi = index(k, X, Y), index(k, BX, BY)
+                        vals.append(int(srcs[k][i]) if i < len(srcs[k]) else 0)
+                        curs.append(int(srcs[k][bi]) if bi < len(srcs[k]) else 0)
+                    if mode13:
+                        m = min(max(b256(curs[0], curs[1], thr), min(vals)), max(vals))
+                    else:
+                        m = b256(vals[0], vals[1], thr)
+                    if mask is not None:
+                        if zero:
+                            a = alpha_abs(bx + x, by + y)
+                        else:
+                            a = byte(ip(mrow[0], mrow[1], BW, xs_, wx) if interp else mrow[0])
+                        m = byte((m * (255 - a) + b256(curs[0], curs[1], thr) * a + 255) >> 8)
+                    dst[by + y, bx + x] = m
+    return dst
+
+
+DUAL_CASES = [  # w, h, block, step, interp, zero origin, mode13, threshold, mask
+    (40, 24, 8, 1, True, False, False, 100, False),
+    (40, 24, 8, 1, True, False, True, 200, True),
+    (36, 22, 16, 2, False, True, True, 64, True),
+    (32, 16, 8, 2, True, True, False, 128, True),    # the zero-origin variant with interpolation
+    (20, 12, 32, 1, True, False, True, 30, False),
+]
+
+
+@pytest.mark.parametrize("case", range(len(DUAL_CASES)))
+def test_oracle_dual_matches_python_restatement(case):
+    w, h, blk, step, interp, zero, mode13, thr, masked = DUAL_CASES[case]
+    rng = np.random.default_rng(50 + case)
+    gw, gh = _grid(w, h, blk, blk)
+    cfg = _cfg(w, h, blk, blk, gw, gh, step)
+    mot0 = (_motion(rng, gw * gh, 40), _motion(rng, gw * gh, 40))
+    mot1 = (_motion(rng, gw * gh, 40), _motion(rng, gw * gh, 40))
+    mask = rng.integers(0, 256, size=gw * gh, dtype=np.uint8) if masked else None
+    shift = {1: 0, 2: 1}[step]
+    for chroma in (False, True):
+        pw, ph = (w // 2, h // 2) if chroma else (w, h)
+        strides = [pw + 3, pw + 5]
+        srcs = [rng.integers(0, 256, size=(step * step) * ph * st, dtype=np.uint8) for st in strides]
+        spans = [st * ph if shift else 0 for st in strides]
+        got = orc.render_dual_plane(cfg, chroma, interp, zero, mode13, thr, srcs, strides, spans, shift, mot0, mot1,
+                                    pw, ph, mask)
+        want = _py_dual(cfg, chroma, interp, zero, mode13, thr, srcs, strides, spans, shift, mot0, mot1, mask)
+        assert np.array_equal(got, want), f"chroma {chroma}: {np.argwhere(got != want)[:3]}"
+
+
 def _motion(rng, n, spread):
     m = rng.integers(1024 - spread, 1024 + spread + 1, size=n).astype(np.uint16)
     m[rng.random(n) < 0.1] = 1024
@@ -288,6 +441,58 @@ def _gpu_render_case(case, rng):
 @pytest.mark.parametrize("case", range(len(GPU_CASES)))
 def test_render_matches_oracle(case):
     _gpu_render_case(GPU_CASES[case], np.random.default_rng(100 + case))
+
+
+DUAL_GPU_CASES = [  # w, h, block, step, interp, zero origin, mode13, threshold, mask
+    (1920, 1080, 16, 2, True, False, True, 128, False),
+    (1920, 1080, 16, 1, True, False, False, 40, True),
+    (640, 360, 8, 1, False, True, True, 200, True),
+    (320, 240, 32, 2, True, True, False, 256, True),
+    (66, 38, 16, 4, True, False, True, 0, False),
+    (20, 12, 32, 1, True, False, True, 99, True),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(len(DUAL_GPU_CASES)))
+def test_render_blend_matches_oracle(case):
+    import torch
+
+    import svpflow_b200 as sv
+
+    w, h, blk, step, interp, zero, mode13, thr, masked = DUAL_GPU_CASES[case]
+    rng = np.random.default_rng(200 + case)
+    gw, gh = _grid(w, h, blk, blk)
+    cfg = _cfg(w, h, blk, blk, gw, gh, step)
+    shift = {1: 0, 2: 1, 4: 2}[step]
+    mot = [(_motion(rng, gw * gh, 150), _motion(rng, gw * gh, 150)) for _ in range(2)]
+    ma = rng.integers(0, 256, size=gw * gh, dtype=np.uint8)
+    mb = rng.integers(0, 256, size=gw * gh, dtype=np.uint8)
+    srcs = [[], []]
+    wants, dsts = [], []
+    for pl in range(3):
+        pw, ph = (w // 2, h // 2) if pl else (w, h)
+        strides = [pw + 7 * pl, pw + 3]
+        planes = [rng.integers(0, 256, size=(step * step) * ph * st, dtype=np.uint8) for st in strides]
+        spans = [st * ph if shift else 0 for st in strides]
+        wants.append(orc.render_dual_plane(cfg, pl > 0, interp, zero or not interp, mode13, thr, planes, strides,
+                                           spans, shift, mot[0], mot[1], pw, ph, np.maximum(ma, mb) if masked else None))
+        for k in range(2):
+            srcs[k].append((torch.from_numpy(planes[k]).cuda(), strides[k]))
+        dsts.append(torch.full((ph, pw), 7, dtype=torch.uint8, device="cuda"))
+    dev = lambda a: torch.from_numpy(a.astype(np.int16) if a.dtype == np.uint16 else a).cuda()
+    md = [(dev(x), dev(y)) for x, y in mot]
+    mkd = (dev(ma), dev(mb)) if masked else None
+    sv.render_blend_device(cfg, thr, mode13, interp, zero, [t.data_ptr() for t, _ in srcs[0]],
+                           [st for _, st in srcs[0]], [t.numel() for t, _ in srcs[0]],
+                           [t.data_ptr() for t, _ in srcs[1]], [st for _, st in srcs[1]],
+                           [t.numel() for t, _ in srcs[1]], shift, (md[0][0].data_ptr(), md[0][1].data_ptr()),
+                           (md[1][0].data_ptr(), md[1][1].data_ptr()), [d.data_ptr() for d in dsts],
+                           [d.shape[1] for d in dsts], masks=(mkd[0].data_ptr(), mkd[1].data_ptr()) if masked else None)
+    torch.cuda.synchronize()
+    for pl in range(3):
+        got = dsts[pl].cpu().numpy()
+        assert np.array_equal(got, wants[pl]), f"plane {pl}: {np.argwhere(got != wants[pl])[:3]}"
 
 
 @pytest.mark.gpu
