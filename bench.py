@@ -320,8 +320,39 @@ def run_render(args, world: int, rank: int, local: int):
             graph.replay()
             e1.record(stream)
         torch.cuda.synchronize()
-    launches = nf * args.steps  # one render_warp_kernel per frame in every replay
+    launches = nf * args.steps  # one render_kernel per frame in every replay
     ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    # the two-source blend (algorithm 13) on the same frames: frame f's and f+1's super frames, the
+    # forward set of frame f and the backward set of frame f+1
+    blend_d = torch.empty_like(out_d)
+
+    def blend(f, st):
+        g = min(f + 1, nf - 1)
+        m0 = planes[f].data_ptr()
+        m1 = planes[g].data_ptr() + 2 * mw * mh * 2
+        sv.render_blend_device(cfg, thr, True, True, False, [sup_d[f].data_ptr() + o for o in offs], strides, lens,
+                               [sup_d[f + 1].data_ptr() + o for o in offs], strides, lens, 1, (m0, m0 + mw * mh * 2),
+                               (m1, m1 + mw * mh * 2), [blend_d[f].data_ptr() + o for o in dst_offs], strides, stream=st)
+
+    for f in range(nf):
+        blend(f, sh)
+    torch.cuda.synchronize()
+    bgraph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(bgraph):
+        cs = torch.cuda.current_stream().cuda_stream
+        for f in range(nf):
+            blend(f, cs)
+    torch.cuda.synchronize()
+    bms = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bgraph.replay()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        bms.append(e0.elapsed_time(e1))
+    blend_value = nf / (statistics.mean(bms) / 1000.0)
     ms_max = _max_over_ranks(torch, dist, world, ms, dev)
     value = nf * world * args.steps / (ms_max / 1000.0)
     # end to end: host super frames and motion planes in, rendered frames out, per step
@@ -367,6 +398,22 @@ def run_render(args, world: int, rank: int, local: int):
                                                  mot_np[f][0], mot_np[f][1], strides[p], ph))
             return res
 
+        blend_np = blend_d.cpu().numpy()
+
+        def cpu_blend(f):
+            g = min(f + 1, nf - 1)
+            res = []
+            for p in range(3):
+                ph = h // (2 if p else 1)
+                srcs = [sup_np[f][offs[p]: offs[p] + lens[p]], sup_np[f + 1][offs[p]: offs[p] + lens[p]] if f + 1 < nf
+                        else sup_d[f + 1].cpu().numpy()[offs[p]: offs[p] + lens[p]]]
+                res.append(orc.render_dual_plane(ocfg, p > 0, True, False, True, thr, srcs, [strides[p]] * 2,
+                                                 [strides[p] * ph] * 2, 1, (mot_np[f][0], mot_np[f][1]),
+                                                 (mot_np[g][2], mot_np[g][3]), strides[p], ph))
+            return res
+
+        blend_check = {"frames_checked": 4, "bit_exact": all(
+            np.array_equal(np.concatenate([r.reshape(-1) for r in cpu_blend(f)]), blend_np[f]) for f in range(4))}
         cpu, parity = None, None
         if not args.no_cpu:
             threads = os.cpu_count() or 1
@@ -406,6 +453,9 @@ def run_render(args, world: int, rank: int, local: int):
                          "note": "issue-bound, not HBM-bound: per sample a tile lookup, motion interpolation and "
                                  "an index computation (62 % issue active in the ncu capture)"},
             "cpu_baseline": cpu, "parity_vs_oracle": parity,
+            "blend_mode13": {"value": blend_value, "unit": "frames/s", "kernel": "render_kernel<dual>",
+                             "how": "svpf_render_blend_device (algorithm 13: frames f and f+1, forward and backward "
+                                    "sets), same frames and timing", "parity_vs_oracle": blend_check},
         }
         print(json.dumps(line), flush=True)
     if world > 1:
