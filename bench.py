@@ -407,7 +407,7 @@ def run_render(args, world: int, rank: int, local: int):
                 ph = h // (2 if p else 1)
                 srcs = [sup_np[f][offs[p]: offs[p] + lens[p]], sup_np[f + 1][offs[p]: offs[p] + lens[p]] if f + 1 < nf
                         else sup_d[f + 1].cpu().numpy()[offs[p]: offs[p] + lens[p]]]
-                res.append(orc.render_dual_plane(ocfg, p > 0, True, False, True, thr, srcs, [strides[p]] * 2,
+                res.append(orc.render_dual_plane(ocfg, p > 0, True, False, 13, thr, srcs, [strides[p]] * 2,
                                                  [strides[p] * ph] * 2, 1, (mot_np[f][0], mot_np[f][1]),
                                                  (mot_np[g][2], mot_np[g][3]), strides[p], ph))
             return res

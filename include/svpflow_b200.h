@@ -188,6 +188,20 @@ int svpf_render_blend_device(const svpf_render_config *cfg, int32_t threshold, i
                              const uint16_t *motion0_y, const uint16_t *motion1_x, const uint16_t *motion1_y,
                              const uint8_t *mask_a, const uint8_t *mask_b, uint8_t *const dst[3],
                              const int64_t dst_stride[3], void *stream);
+/* CpuRenderer::render_mode21_or_22 (renderer.rs:571-641) on the device: the reads of
+ * svpf_render_blend_device, each pair of displaced samples blended by the alphas of mask_a and mask_b
+ * (both required): mode 21 blend_256(blend_255(mv0, mv1, a0), blend_255(mv1, mv0, a1), threshold),
+ * mode 22 (mode22 != 0) blend_256(cur0, cur1, threshold) clamped between those two (mode21_pixel /
+ * mode22_pixel :1830-1848); final_mask (optional) blends the result towards blend_256(cur0, cur1,
+ * threshold_limit), threshold_limit from the threshold and mask_scale as set_threshold_value (:256-264)
+ * computes it. No interpolation (interp == 0) puts the grid at zero origin, as the reference does. */
+int svpf_render_masked_device(const svpf_render_config *cfg, int32_t threshold, double mask_scale, int32_t mode22,
+                              int32_t interp, const uint8_t *const src0[3], const int64_t src0_stride[3],
+                              const int64_t src0_len[3], const uint8_t *const src1[3], const int64_t src1_stride[3],
+                              const int64_t src1_len[3], int32_t src_shift, const uint16_t *motion0_x,
+                              const uint16_t *motion0_y, const uint16_t *motion1_x, const uint16_t *motion1_y,
+                              const uint8_t *mask_a, const uint8_t *mask_b, const uint8_t *final_mask,
+                              uint8_t *const dst[3], const int64_t dst_stride[3], void *stream);
 
 /* ---------------------------------------------------------------- batched form */
 /* No counterpart in the reference, which analyses one clip at a time, one output frame

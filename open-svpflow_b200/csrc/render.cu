@@ -1,12 +1,13 @@
 // render.cu -- SmoothFps's frame render on the device: the single warp of algorithms 1 and 2 and
-// the two-source blend of algorithms 11 and 13. Each output sample reads its source(s) at its
+// the two-source blends of algorithms 11, 13, 21 and 22. Each output sample reads its source(s) at its
 // position displaced by motion interpolated between the four motion-plane samples around it, and
 // optionally blends with the undisplaced samples by the mode's mask.
 //
 // Follows crates/svpflow-core/src/renderer.rs: CpuRenderer::render_mode1_or_2 (:308-328) through
 // render_selected_warp_rows (:876-984); render_mode11_or_13 and its zero-origin variant (:330-438)
-// through render_dual_warp_rows (:1031-1172) and mode11_or_13_pixel (:2918-2943); set_threshold
-// (:238-250), plane_params (:1539-1606), motion_samples (:1608-1638), render_tiles (:1925-2010),
+// through render_dual_warp_rows (:1031-1172) and mode11_or_13_pixel (:2918-2943); render_mode21_or_22
+// (:571-641) with mode21_pixel / mode22_pixel (:1830-1848); set_threshold / set_threshold_value
+// (:238-264), plane_params (:1539-1606), motion_samples (:1608-1638), render_tiles (:1925-2010),
 // interpolate_row / interpolate_motion (:2582-2637), alpha_row / alpha_at_row / alpha_at_absolute
 // (:2639-2722), interp_pair (:2724-2738), interpolation_weights / coeff (:2740-2770), plane_covers /
 // plane_index (:2772-2790), tile_interior (:2809-2835), sample_plane (:2837-2861), max_mask
@@ -53,11 +54,12 @@ struct RenderPlane {
 struct RenderJob {
     RenderPlane pl[3];
     const uint16_t *mx[2], *my[2];  // motion sets 0 and 1 (the single warp uses set 0)
-    const uint8_t *mask[2];         // NULL, one mask, or the two of max_mask
+    const uint8_t *mask[3];         // the single warp: [0]; 11 / 13: [0], [1] of max_mask; 21 / 22: a, b, final
     int64_t mlen;
     int32_t grid_w, grid_h, interp, zero_origin, shift;
     int32_t lut_t[2];               // LUT factors of the sets: threshold or 256 - threshold
-    int32_t threshold, mode13;      // the two-source blend
+    int32_t threshold, mode13;      // the two-source blends
+    int32_t mode22, threshold_limit;  // 21 / 22
 };
 
 // ---- host side: the renderer's per-plane constants
@@ -144,22 +146,24 @@ __device__ __forceinline__ int32_t motion(const RenderJob &J, const uint16_t *pl
     const int k = i < J.mlen ? __ldg(plane + i) : 1024;  // NEUTRAL beyond the plane
     return ((k < kLut - 1 ? k : kLut - 1) - 1024) * t / 256;
 }
-// a mask sample: the mode's mask, or max_mask of the two
-__device__ __forceinline__ int32_t mask_at(const RenderJob &J, int64_t i) {
+// a mask sample: sel < 0 -> the mode's mask, or max_mask of the two; sel >= 0 -> mask[sel]
+__device__ __forceinline__ int32_t mask_at(const RenderJob &J, int sel, int64_t i) {
     if (i < 0 || i >= J.mlen) return 0;
+    if (sel >= 0) return __ldg(J.mask[sel] + i);
     const int32_t a = __ldg(J.mask[0] + i);
     return J.mask[1] ? max(a, (int32_t)__ldg(J.mask[1] + i)) : a;
 }
 // alpha_at_absolute (renderer.rs:2687-2722): the mask's alpha on the zero-origin grid
-__device__ __forceinline__ int32_t alpha_absolute(const RenderJob &J, const RenderPlane &p, int32_t x, int32_t y) {
+__device__ __forceinline__ int32_t alpha_absolute(const RenderJob &J, const RenderPlane &p, int sel, int32_t x,
+                                                  int32_t y) {
     const int32_t ox = p.morigin_x, oy = p.morigin_y, bw = p.block_w, bh = p.block_h;
     int32_t ix0 = 0, ix1 = 0, iy0 = 0, iy1 = 0;
     if (ox <= x) { ix0 = (x - ox) / bw; ix1 = ix0 + 1; }
     if (oy <= y) { iy0 = (y - oy) / bh; iy1 = iy0 + 1; }
     const int32_t fx = ox < x ? (x - ox) % bw : 0, fy = oy < y ? (y - oy) % bh : 0;
     const int64_t gw = J.grid_w;
-    const int32_t tl = mask_at(J, iy0 * gw + ix0), tr = mask_at(J, iy0 * gw + ix1);
-    const int32_t bl = mask_at(J, iy1 * gw + ix0), br = mask_at(J, iy1 * gw + ix1);
+    const int32_t tl = mask_at(J, sel, iy0 * gw + ix0), tr = mask_at(J, sel, iy0 * gw + ix1);
+    const int32_t bl = mask_at(J, sel, iy1 * gw + ix0), br = mask_at(J, sel, iy1 * gw + ix1);
     const int32_t top = ((bw - fx) * tl + fx * tr) / bw, bottom = ((bw - fx) * bl + fx * br) / bw;
     return clamp_byte(((bh - fy) * top + fy * bottom) / bh);
 }
@@ -222,8 +226,9 @@ __device__ __forceinline__ bool interior(const RenderPlane &p, const Tile &t, co
 }
 // the mask interpolated down to row py (alpha_row)
 __device__ __forceinline__ void mask_row(const RenderJob &J, const RenderPlane &p, const Tile &t, int32_t py,
-                                         const int32_t (*syw)[2], int32_t &m0, int32_t &m1) {
-    const int32_t a = mask_at(J, t.i[0]), b = mask_at(J, t.i[1]), cc = mask_at(J, t.i[2]), d = mask_at(J, t.i[3]);
+                                         const int32_t (*syw)[2], int sel, int32_t &m0, int32_t &m1) {
+    const int32_t a = mask_at(J, sel, t.i[0]), b = mask_at(J, sel, t.i[1]), cc = mask_at(J, sel, t.i[2]),
+                  d = mask_at(J, sel, t.i[3]);
     if (J.interp) {
         const int32_t *wy = syw[min(py - t.by, kMaxBlock - 1)];
         m0 = interp_pair(a, cc, p.block_h, p.y_shift, wy);
@@ -250,18 +255,22 @@ __device__ __forceinline__ int64_t warp_index(const RenderJob &J, const RenderPl
     return src_index(s, J.shift, xs, ys);
 }
 // the mask's alpha at a sample (alpha_at_absolute on the zero-origin grid, else alpha_at_row)
-__device__ __forceinline__ int32_t alpha_at(const RenderJob &J, const RenderPlane &p, int32_t m0, int32_t m1,
-                                            int32_t px, int32_t bx, int32_t py, const int32_t (*sxw)[2]) {
-    if (J.zero_origin) return alpha_absolute(J, p, px, py);
+__device__ __forceinline__ int32_t alpha_at(const RenderJob &J, const RenderPlane &p, int sel, int32_t m0,
+                                            int32_t m1, int32_t px, int32_t bx, int32_t py, const int32_t (*sxw)[2]) {
+    if (J.zero_origin) return alpha_absolute(J, p, sel, px, py);
     if (!J.interp) return clamp_byte(m0);
     return clamp_byte(interp_pair(m0, m1, p.block_w, p.x_shift, sxw[min(px - bx, kMaxBlock - 1)]));
 }
 
-// DUAL false: the single warp (sources[0], set 0; mode1_pixel with the mask). DUAL true: the
-// two-source blend (set 0 reads source 0, set 1 source 1; mode11_or_13_pixel). Grid: (row length
-// of the widest plane / (256 kPx), rows of the tallest plane, 3 planes).
-template <bool DUAL, bool MASK>
+// KIND 0: the single warp (sources[0], set 0; mode1_pixel with the mask when MASK). KIND 1: the
+// two-source blend of algorithms 11 / 13 (set 0 reads source 0, set 1 source 1; mode11_or_13_pixel,
+// max_mask when MASK). KIND 2: algorithms 21 / 22 (the same reads; mode21_or_22_pixel with alphas
+// from masks a and b, and the final mask when MASK). Grid: (row length of the widest plane /
+// (256 kPx), rows of the tallest plane, 3 planes).
+template <int KIND, bool MASK>
 __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ RenderJob J) {
+    constexpr bool DUAL = KIND > 0;
+    constexpr int NA = KIND == 2 ? (MASK ? 3 : 2) : (MASK ? 1 : 0);  // alphas per sample
     const RenderPlane &p = J.pl[blockIdx.z];
     // the plane's interpolation weights in shared memory (indexed per thread)
     __shared__ int32_t sxw[kMaxBlock][2], syw[kMaxBlock][2];
@@ -283,8 +292,11 @@ __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ Ren
     Tile t = make_tile(J, gx, bx, tw, gy, by, th);
     SetRow r0 = set_row(J, p, t, 0, py, syw), r1 = r0;
     if (DUAL) r1 = set_row(J, p, t, 1, py, syw);
-    int32_t m0 = 0, m1 = 0;
-    if (MASK) mask_row(J, p, t, py, syw, m0, m1);
+    // the mask selectors of the alphas: the mode's (max) mask, or masks a, b, final
+    auto sel_of = [](int a) { return KIND == 2 ? a : -1; };
+    int32_t m0[NA > 0 ? NA : 1], m1[NA > 0 ? NA : 1];
+#pragma unroll
+    for (int a = 0; a < NA; a++) mask_row(J, p, t, py, syw, sel_of(a), m0[a], m1[a]);
     auto direct_of = [&]() {  // plane_covers && tile_interior for the tile's sets
         bool d = p.src[0].covers && p.step > 0 && interior(p, t, r0);
         if (DUAL) d = d && p.src[1].covers && interior(p, t, r1);
@@ -293,12 +305,13 @@ __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ Ren
     bool direct = direct_of();
     // indices first, then every load of the thread's samples, so the gathers overlap
     int64_t i0[kPx], i1[kPx];
-    int32_t alpha[kPx];
+    int32_t alpha[NA > 0 ? NA : 1][kPx];
 #pragma unroll
     for (int k = 0; k < kPx; k++) {
         const int32_t px = px0 + k;
         i0[k] = i1[k] = -1;
-        alpha[k] = 0;
+#pragma unroll
+        for (int a = 0; a < NA; a++) alpha[a][k] = 0;
         if (px > pxl) continue;
         if (!shared_tile && k > 0) {
             int32_t gk, bk, twk;
@@ -308,15 +321,18 @@ __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ Ren
                 t = make_tile(J, gk, bk, twk, gy, by, th);
                 r0 = set_row(J, p, t, 0, py, syw);
                 if (DUAL) r1 = set_row(J, p, t, 1, py, syw);
-                if (MASK) mask_row(J, p, t, py, syw, m0, m1);
+#pragma unroll
+                for (int a = 0; a < NA; a++) mask_row(J, p, t, py, syw, sel_of(a), m0[a], m1[a]);
                 direct = direct_of();
             }
         }
         i0[k] = warp_index(J, p, p.src[0], r0, direct, px, t.bx, py, sxw);
         if (DUAL) i1[k] = warp_index(J, p, p.src[1], r1, direct, px, t.bx, py, sxw);
-        if (MASK) alpha[k] = alpha_at(J, p, m0, m1, px, t.bx, py, sxw);
+#pragma unroll
+        for (int a = 0; a < NA; a++) alpha[a][k] = alpha_at(J, p, sel_of(a), m0[a], m1[a], px, t.bx, py, sxw);
     }
-    const bool bases = MASK || (DUAL && J.mode13);  // the undisplaced samples (px * step <= max_x: no clamp)
+    // the undisplaced samples (px * step <= max_x: no clamp)
+    const bool bases = KIND == 0 ? MASK : (KIND == 1 ? (MASK || J.mode13) : (MASK || J.mode22));
     int32_t v0[kPx], v1[kPx], c0[kPx], c1[kPx];
 #pragma unroll
     for (int k = 0; k < kPx; k++) {
@@ -330,13 +346,18 @@ __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ Ren
 #pragma unroll
     for (int k = 0; k < kPx; k++) {
         int32_t v;
-        if (DUAL) {
+        if (KIND == 2) {  // mode21_or_22_pixel
+            const int32_t ea = blend255(v0[k], v1[k], alpha[0][k]), eb = blend255(v1[k], v0[k], alpha[1][k]);
+            if (J.mode22) v = min(max(blend256(c0[k], c1[k], J.threshold), min(ea, eb)), max(ea, eb));
+            else v = blend256(ea, eb, J.threshold);
+            if (MASK) v = blend255(v, blend256(c0[k], c1[k], J.threshold_limit), alpha[NA - 1][k]);
+        } else if (KIND == 1) {  // mode11_or_13_pixel
             const int32_t b = blend256(c0[k], c1[k], J.threshold);
             if (J.mode13) v = min(max(b, min(v0[k], v1[k])), max(v0[k], v1[k]));  // mode13_pixel
             else v = blend256(v0[k], v1[k], J.threshold);                          // mode11_pixel
-            if (MASK) v = blend255(v, b, alpha[k]);
+            if (MASK) v = blend255(v, b, alpha[0][k]);
         } else {
-            v = MASK ? blend255(v0[k], c0[k], alpha[k]) : v0[k];  // mode1_pixel
+            v = MASK ? blend255(v0[k], c0[k], alpha[0][k]) : v0[k];  // mode1_pixel
         }
         out[k] = v;
     }
@@ -418,17 +439,20 @@ bool draws_nothing(const svpf_render_config *cfg) {  // render_tiles returns at 
     return cfg->width <= 0 || cfg->height <= 0 || cfg->grid_w <= 0 || cfg->grid_h <= 0 || cfg->source_step <= 0 ||
            cfg->block_w <= 0 || cfg->block_h <= 0;
 }
-int launch(const RenderJob &J, bool dual, bool mask, int32_t most_w, int32_t most_h, void *stream) {
+int launch(const RenderJob &J, int kind, bool mask, int32_t most_w, int32_t most_h, void *stream) {
     cudaError_t e = cudaSuccess;
     if (most_w > 0 && most_h > 0) {
         dim3 grid((unsigned)((most_w + 256 * kPx - 1) / (256 * kPx)), (unsigned)most_h, 3);
         cudaStream_t st = (cudaStream_t)stream;
-        if (dual) {
-            if (mask) render_kernel<true, true><<<grid, 256, 0, st>>>(J);
-            else render_kernel<true, false><<<grid, 256, 0, st>>>(J);
+        if (kind == 2) {
+            if (mask) render_kernel<2, true><<<grid, 256, 0, st>>>(J);
+            else render_kernel<2, false><<<grid, 256, 0, st>>>(J);
+        } else if (kind == 1) {
+            if (mask) render_kernel<1, true><<<grid, 256, 0, st>>>(J);
+            else render_kernel<1, false><<<grid, 256, 0, st>>>(J);
         } else {
-            if (mask) render_kernel<false, true><<<grid, 256, 0, st>>>(J);
-            else render_kernel<false, false><<<grid, 256, 0, st>>>(J);
+            if (mask) render_kernel<0, true><<<grid, 256, 0, st>>>(J);
+            else render_kernel<0, false><<<grid, 256, 0, st>>>(J);
         }
         svpf::add_launches(1);
         e = cudaGetLastError();
@@ -468,7 +492,7 @@ int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, in
     int32_t mw, mh;
     int rc = setup(*J, cfg, 1, srcs, strides, lens, src_shift, dst, dst_stride, mw, mh);
     if (rc) svpf::set_last_error("render: bad plane buffers");
-    else rc = launch(*J, false, mask != nullptr, mw, mh, stream);
+    else rc = launch(*J, 0, mask != nullptr, mw, mh, stream);
     delete J;
     return rc;
 }
@@ -506,7 +530,50 @@ int svpf_render_blend_device(const svpf_render_config *cfg, int32_t threshold, i
     int32_t mw, mh;
     int rc = setup(*J, cfg, 2, srcs, strides, lens, src_shift, dst, dst_stride, mw, mh);
     if (rc) svpf::set_last_error("render: bad plane buffers");
-    else rc = launch(*J, true, mask_a != nullptr, mw, mh, stream);
+    else rc = launch(*J, 1, mask_a != nullptr, mw, mh, stream);
+    delete J;
+    return rc;
+}
+
+int svpf_render_masked_device(const svpf_render_config *cfg, int32_t threshold, double mask_scale, int32_t mode22,
+                              int32_t interp, const uint8_t *const src0[3], const int64_t src0_stride[3],
+                              const int64_t src0_len[3], const uint8_t *const src1[3], const int64_t src1_stride[3],
+                              const int64_t src1_len[3], int32_t src_shift, const uint16_t *motion0_x,
+                              const uint16_t *motion0_y, const uint16_t *motion1_x, const uint16_t *motion1_y,
+                              const uint8_t *mask_a, const uint8_t *mask_b, const uint8_t *final_mask,
+                              uint8_t *const dst[3], const int64_t dst_stride[3], void *stream) {
+    if (int rc = check_common(cfg, threshold, src_shift)) return rc;
+    if (!src0 || !src0_stride || !src0_len || !src1 || !src1_stride || !src1_len || !dst || !dst_stride ||
+        !motion0_x || !motion0_y || !motion1_x || !motion1_y || !mask_a || !mask_b) {
+        svpf::set_last_error("render: null argument (masks a and b are required)");
+        return SVPF_EINVAL;
+    }
+    if (draws_nothing(cfg)) return SVPF_OK;
+    RenderJob *J = new RenderJob;
+    memset(J, 0, sizeof(*J));
+    J->lut_t[0] = threshold;
+    J->lut_t[1] = 256 - threshold;
+    J->mx[0] = motion0_x;
+    J->my[0] = motion0_y;
+    J->mx[1] = motion1_x;
+    J->my[1] = motion1_y;
+    J->mask[0] = mask_a;
+    J->mask[1] = mask_b;
+    J->mask[2] = final_mask;
+    J->interp = interp != 0;
+    J->zero_origin = interp == 0;  // render_mode21_or_22 passes zero_origin = !interp
+    J->threshold = threshold;
+    J->mode22 = mode22 != 0;
+    {  // set_threshold_value (renderer.rs:256-264), f64 as the reference
+        const double v = threshold > 126 ? 256.0 - (double)(256 - threshold) * mask_scale : (double)threshold * mask_scale;
+        J->threshold_limit = as_i32(v);
+    }
+    const uint8_t *const *srcs[2] = {src0, src1};
+    const int64_t *strides[2] = {src0_stride, src1_stride}, *lens[2] = {src0_len, src1_len};
+    int32_t mw, mh;
+    int rc = setup(*J, cfg, 2, srcs, strides, lens, src_shift, dst, dst_stride, mw, mh);
+    if (rc) svpf::set_last_error("render: bad plane buffers");
+    else rc = launch(*J, 2, final_mask != nullptr, mw, mh, stream);
     delete J;
     return rc;
 }

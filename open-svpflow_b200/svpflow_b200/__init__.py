@@ -112,6 +112,9 @@ def lib() -> ctypes.CDLL:
             "svpf_render_blend_device": (I32, [P(RenderConfig), I32, I32, I32, I32, P(_VP), P(I64), P(I64), P(_VP),
                                                P(I64), P(I64), I32, _VP, _VP, _VP, _VP, _VP, _VP, P(_VP), P(I64),
                                                _VP]),
+            "svpf_render_masked_device": (I32, [P(RenderConfig), I32, ctypes.c_double, I32, I32, P(_VP), P(I64),
+                                                P(I64), P(_VP), P(I64), P(I64), I32, _VP, _VP, _VP, _VP, _VP, _VP,
+                                                _VP, P(_VP), P(I64), _VP]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -520,3 +523,19 @@ def render_blend_device(cfg: dict, threshold: int, mode13: bool, interp: bool, z
                                           arr(ctypes.c_int64, src1_strides), arr(ctypes.c_int64, src1_lens),
                                           int(src_shift), motion0[0], motion0[1], motion1[0], motion1[1], ma, mb,
                                           arr(_VP, dst_ptrs), arr(ctypes.c_int64, dst_strides), stream))
+
+
+def render_masked_device(cfg: dict, threshold: int, mask_scale: float, mode22: bool, interp: bool, src0_ptrs,
+                         src0_strides, src0_lens, src1_ptrs, src1_strides, src1_lens, src_shift: int, motion0,
+                         motion1, masks, final_mask_ptr, dst_ptrs, dst_strides, stream: int = 0):
+    """SmoothFps's masked two-source blends (algorithms 21 / 22) of one frame on the device; masks =
+    (a_ptr, b_ptr), final_mask_ptr 0 or a device plane; see svpf_render_masked_device."""
+    c = RenderConfig(**{k: int(cfg[k]) for k, _ in RenderConfig._fields_})
+    arr = lambda t, v: (t * 3)(*[int(x) for x in v])
+    _check(lib().svpf_render_masked_device(ctypes.byref(c), int(threshold), float(mask_scale), int(mode22),
+                                           int(interp), arr(_VP, src0_ptrs), arr(ctypes.c_int64, src0_strides),
+                                           arr(ctypes.c_int64, src0_lens), arr(_VP, src1_ptrs),
+                                           arr(ctypes.c_int64, src1_strides), arr(ctypes.c_int64, src1_lens),
+                                           int(src_shift), motion0[0], motion0[1], motion1[0], motion1[1], masks[0],
+                                           masks[1], final_mask_ptr or None, arr(_VP, dst_ptrs),
+                                           arr(ctypes.c_int64, dst_strides), stream))

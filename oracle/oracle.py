@@ -454,8 +454,10 @@ def _setup(L):
     L.or_total_counters.argtypes = [P(ctypes.c_uint64), ctypes.c_int32]
     if hasattr(L, "or_render_luts"):  # the 8-bit build only
         L.or_render_luts.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
-        L.or_render_dual_plane.argtypes = [P(RenderConfig)] + [ctypes.c_int32] * 5 + [P(RPlane), P(RPlane)] + \
-            [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
+        L.or_render_dual_plane.argtypes = [P(RenderConfig)] + [ctypes.c_int32] * 6 + [P(RPlane), P(RPlane)] + \
+            [ctypes.c_void_p] * 4 + [ctypes.c_size_t] + [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_size_t]
+        L.or_render_threshold_limit.restype = ctypes.c_int32
+        L.or_render_threshold_limit.argtypes = [ctypes.c_int32, ctypes.c_double]
         L.or_render_warp_plane.argtypes = [P(RenderConfig), ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
                                            P(RPlane), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
@@ -764,20 +766,25 @@ def render_warp_plane(cfg: dict, chroma: bool, interp: bool, lut: np.ndarray, sr
     return dst.reshape(dst_rows, dst_stride)
 
 
-def render_dual_plane(cfg: dict, chroma: bool, interp: bool, zero_origin: bool, mode13: bool, threshold: int,
+def render_threshold_limit(threshold: int, scale: float) -> int:
+    return lib().or_render_threshold_limit(int(threshold), float(scale))
+
+
+def render_dual_plane(cfg: dict, chroma: bool, interp: bool, zero_origin: bool, mode: int, threshold: int,
                       srcs, strides, spans, shift: int, motion0, motion1, dst_stride: int, dst_rows: int,
-                      mask: np.ndarray = None) -> np.ndarray:
-    """render_mode11_or_13 for one plane: srcs / strides / spans of sources 0 and 1, motion0 / motion1 =
-    (mx, my) of the two sets, mask = max_mask(a, b) or None."""
+                      masks=None, final_mask=None, threshold_limit: int = 0) -> np.ndarray:
+    """render_mode11_or_13 / render_mode21_or_22 for one plane: srcs / strides / spans of sources 0
+    and 1, motion0 / motion1 = (mx, my) of the two sets, masks = (a, b) or None, final_mask for 21 / 22."""
     c = RenderConfig(**{k: int(cfg[k]) for k, _ in RenderConfig._fields_})
     ss = [np.ascontiguousarray(x, dtype=np.uint8).reshape(-1) for x in srcs]
     pls = [RPlane(ss[i].ctypes.data, ss[i].size, strides[i], spans[i], shift) for i in range(2)]
     ms = [np.ascontiguousarray(m, dtype=np.uint16).reshape(-1) for m in (*motion0, *motion1)]
     n = ms[0].size
-    mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+    mk = [None if m is None else np.ascontiguousarray(m, dtype=np.uint8).reshape(-1)
+          for m in ((masks or (None, None))[0], (masks or (None, None))[1], final_mask)]
     dst = np.zeros(dst_rows * dst_stride, dtype=np.uint8)
-    lib().or_render_dual_plane(ctypes.byref(c), int(chroma), int(interp), int(zero_origin), int(mode13),
-                               int(threshold), ctypes.byref(pls[0]), ctypes.byref(pls[1]),
-                               *[_ptr(m) for m in ms], n, None if mk is None else _ptr(mk), _ptr(dst), dst_stride,
-                               dst.size)
+    lib().or_render_dual_plane(ctypes.byref(c), int(chroma), int(interp), int(zero_origin), int(mode),
+                               int(threshold), int(threshold_limit), ctypes.byref(pls[0]), ctypes.byref(pls[1]),
+                               *[_ptr(m) for m in ms], n, *[None if m is None else _ptr(m) for m in mk], _ptr(dst),
+                               dst_stride, dst.size)
     return dst.reshape(dst_rows, dst_stride)

@@ -2145,14 +2145,37 @@ void or_render_warp_plane(const or_render_config *c, int32_t chroma, int32_t int
     }
 }
 
-/* render_dual_warp_rows (:1031-1172) with mode11_or_13_pixel (:2918-2943), as render_mode11_or_13
- * (:330-438) and its zero-origin variant drive it: motion set 0 scaled by the threshold LUT reads
- * source 0, set 1 scaled by the inverse LUT reads source 1; mask = max_mask(a, b) (:2908-2915) or NULL. */
+/* render_dual_warp_rows (:1031-1172) as render_mode11_or_13 (:330-438, and its zero-origin variant)
+ * and render_mode21_or_22 (:571-641) drive it: motion set 0 scaled by the threshold LUT reads source 0,
+ * set 1 scaled by the inverse LUT reads source 1. mode 11 / 13: mode11_or_13_pixel (:2918-2943) with
+ * max_mask(a, b) (:2908-2915) when the masks are given; mode 21 / 22: mode21_or_22_pixel (:615-641)
+ * with alpha0 from mask a, alpha1 from mask b and the final mask blending towards the undisplaced
+ * samples at threshold_limit. */
+int32_t or_render_threshold_limit(int32_t threshold, double scale) {
+    int32_t inverse = sat_i64_to_i32((int64_t)256 - threshold);
+    return threshold > 126 ? f64_as_i32(256.0 - (double)inverse * scale) : f64_as_i32((double)threshold * scale);
+}
 static i32 r_blend256(i32 a, i32 b, i32 w) { return r_byte((a * (256 - w) + b * w) >> 8); }
+static i32 r_alpha(const uint8_t *m, usize mlen, const usize ii[4], const rparams *p, const rparams *mp, usize gw,
+                   int interp, int zero_origin, const i32 *wy, const i32 *wx, i32 px, i32 py) {
+    if (zero_origin) return r_alpha_abs(m, mlen, mp, gw, px, py);
+    i32 v[4];
+    for (int q = 0; q < 4; q++) v[q] = ii[q] < mlen ? m[ii[q]] : 0;
+    if (!interp) return r_byte(v[0]);
+    i32 r0 = r_interp(v[0], v[2], p->block_h, p->y_shift, wy), r1 = r_interp(v[1], v[3], p->block_h, p->y_shift, wy);
+    return r_byte(r_interp(r0, r1, p->block_w, p->x_shift, wx));
+}
 void or_render_dual_plane(const or_render_config *c, int32_t chroma, int32_t interp, int32_t zero_origin,
-                          int32_t mode13, int32_t threshold, const or_rplane *src0, const or_rplane *src1,
-                          const uint16_t *mx0, const uint16_t *my0, const uint16_t *mx1, const uint16_t *my1,
-                          size_t mlen, const uint8_t *mask, uint8_t *dst, size_t dst_stride, size_t dst_len) {
+                          int32_t mode, int32_t threshold, int32_t threshold_limit, const or_rplane *src0,
+                          const or_rplane *src1, const uint16_t *mx0, const uint16_t *my0, const uint16_t *mx1,
+                          const uint16_t *my1, size_t mlen, const uint8_t *mask_a, const uint8_t *mask_b,
+                          const uint8_t *mask_f, uint8_t *dst, size_t dst_stride, size_t dst_len) {
+    int32_t mode13 = mode == 13;
+    uint8_t *mask = NULL; /* modes 11 / 13: max_mask */
+    if ((mode == 11 || mode == 13) && mask_a && mask_b) {
+        mask = malloc(mlen ? mlen : 1);
+        for (usize i = 0; i < mlen; i++) mask[i] = mask_a[i] > mask_b[i] ? mask_a[i] : mask_b[i];
+    }
     int16_t inv[2048], thr[2048];
     or_render_luts(threshold, inv, thr);
     rparams P, MP;
@@ -2253,14 +2276,28 @@ void or_render_dual_plane(const or_render_config *c, int32_t chroma, int32_t int
                         cur[set] = bi < src->len ? src->data[bi] : 0;
                     }
                     i32 motion;
-                    if (mode13) {
+                    if (mode == 21 || mode == 22) {
+                        i32 a0 = r_alpha(mask_a, mlen, ii, p, &MP, (usize)c->grid_w, interp, zero_origin, wy, wx, px, ty + y);
+                        i32 a1 = r_alpha(mask_b, mlen, ii, p, &MP, (usize)c->grid_w, interp, zero_origin, wy, wx, px, ty + y);
+                        i32 a = r_byte((v[0] * (255 - a0) + v[1] * a0 + 255) >> 8);
+                        i32 b = r_byte((v[1] * (255 - a1) + v[0] * a1 + 255) >> 8);
+                        if (mode == 21) motion = r_blend256(a, b, threshold);
+                        else {
+                            i32 m = r_blend256(cur[0], cur[1], threshold), lo = a < b ? a : b, hi = a < b ? b : a;
+                            motion = m < lo ? lo : (m > hi ? hi : m);
+                        }
+                        if (mask_f) {
+                            i32 fa = r_alpha(mask_f, mlen, ii, p, &MP, (usize)c->grid_w, interp, zero_origin, wy, wx, px, ty + y);
+                            motion = r_byte((motion * (255 - fa) + r_blend256(cur[0], cur[1], threshold_limit) * fa + 255) >> 8);
+                        }
+                    } else if (mode13) {
                         i32 b = r_blend256(cur[0], cur[1], threshold);
                         i32 lo = v[0] < v[1] ? v[0] : v[1], hi = v[0] < v[1] ? v[1] : v[0];
                         motion = b < lo ? lo : (b > hi ? hi : b);
                     } else {
                         motion = r_blend256(v[0], v[1], threshold);
                     }
-                    if (mask) {
+                    if (mask && mode != 21 && mode != 22) {
                         i32 alpha = zero_origin ? r_alpha_abs(mask, mlen, &MP, (usize)c->grid_w, px, ty + y)
                                                 : r_byte(interp ? r_interp(mrow[0], mrow[1], p->block_w, p->x_shift, wx)
                                                                 : mrow[0]);
@@ -2272,5 +2309,6 @@ void or_render_dual_plane(const or_render_config *c, int32_t chroma, int32_t int
             }
         }
     }
+    free(mask);
 }
 #endif

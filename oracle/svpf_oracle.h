@@ -192,13 +192,17 @@ void or_render_luts(int32_t threshold, int16_t inverse_lut[2048], int16_t thresh
 void or_render_warp_plane(const or_render_config *c, int32_t chroma, int32_t interp, const int16_t *lut,
                           const or_rplane *src, const uint16_t *mx, const uint16_t *my, size_t mlen,
                           const uint8_t *mask, uint8_t *dst, size_t dst_stride, size_t dst_len);
-/* render_mode11_or_13 (renderer.rs:330-438) for one plane: mode13 != 0 -> mode 13, else 11;
- * zero_origin: the interpolation grid starts at 0 (render_mode11_or_13_zero_origin, or !interp);
- * mask: NULL or max_mask(a, b). */
+/* render_mode11_or_13 (renderer.rs:330-438) / render_mode21_or_22 (:571-641) for one plane, mode 11,
+ * 13, 21 or 22; zero_origin: the interpolation grid starts at 0 (the zero-origin variant, or
+ * !interp); masks a, b (both or neither for 11 / 13, both for 21 / 22) and the final mask (21 / 22,
+ * optional, blending towards blend_256(cur0, cur1, threshold_limit)). */
 void or_render_dual_plane(const or_render_config *c, int32_t chroma, int32_t interp, int32_t zero_origin,
-                          int32_t mode13, int32_t threshold, const or_rplane *src0, const or_rplane *src1,
-                          const uint16_t *mx0, const uint16_t *my0, const uint16_t *mx1, const uint16_t *my1,
-                          size_t mlen, const uint8_t *mask, uint8_t *dst, size_t dst_stride, size_t dst_len);
+                          int32_t mode, int32_t threshold, int32_t threshold_limit, const or_rplane *src0,
+                          const or_rplane *src1, const uint16_t *mx0, const uint16_t *my0, const uint16_t *mx1,
+                          const uint16_t *my1, size_t mlen, const uint8_t *mask_a, const uint8_t *mask_b,
+                          const uint8_t *mask_f, uint8_t *dst, size_t dst_stride, size_t dst_len);
+/* set_threshold_value (renderer.rs:256-264): threshold_limit for a mask scale */
+int32_t or_render_threshold_limit(int32_t threshold, double scale);
 int or_vector_planes(const int32_t vdata[16], const uint8_t *payload, size_t len, int32_t frame_w, int32_t frame_h,
                      int32_t raw, uint16_t *out);
 

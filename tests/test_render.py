@@ -148,8 +148,11 @@ def _py_render(cfg, chroma, interp, lut, src, stride, span, shift, mx, my, mask=
     return dst
 
 
-def _py_dual(cfg, chroma, interp, zero, mode13, thr, srcs, strides, spans, shift, mot0, mot1, mask=None):
-    """render_dual_warp_rows + mode11_or_13_pixel (renderer.rs:1031-1172, :2918-2943) in plain Python."""
+def _py_dual(cfg, chroma, interp, zero, mode, thr, srcs, strides, spans, shift, mot0, mot1, masks=None, final=None,
+             tlimit=0):
+    """render_dual_warp_rows + mode11_or_13_pixel / mode21_or_22_pixel (renderer.rs:1031-1172,
+    :2918-2943, :615-641) in plain Python."""
+    mask = np.maximum(*masks) if masks is not None and mode in (11, 13) else None
     cmap = lambda v: CPU_MAP[v - 1] if 1 <= v <= 32 else -1
     cd = cfg["chroma_y_div"]
     if chroma:
@@ -185,11 +188,13 @@ def _py_dual(cfg, chroma, interp, zero, mode13, thr, srcs, strides, spans, shift
         m = (1 << shift) - 1
         return (((y & m) << shift) | (x & m)) * spans[k] + (y >> shift) * strides[k] + (x >> shift)
 
-    def mat(x, y):
-        i = y * gw + x
-        return int(mask[i]) if x >= 0 and y >= 0 and i < len(mask) else 0
+    def alpha_abs(x, y, mk=None):
+        mk = mask if mk is None else mk
 
-    def alpha_abs(x, y):
+        def mat(x, y):
+            i = y * gw + x
+            return int(mk[i]) if x >= 0 and y >= 0 and i < len(mk) else 0
+
         ix0 = ix1 = iy0 = iy1 = 0
         if mox <= x:
             ix0 = (x - mox) // BW
@@ -257,7 +262,28 @@ def _py_dual(cfg, chroma, interp, zero, mode13, thr, srcs, strides, spans, shift
                         i, bi = index(k, X, Y), index(k, BX, BY)
                         vals.append(int(srcs[k][i]) if i < len(srcs[k]) else 0)
                         curs.append(int(srcs[k][bi]) if bi < len(srcs[k]) else 0)
-                    if mode13:
+                    def alpha_of(mk):  # alpha_at_absolute, or alpha_at_row over the tile's corners
+                        if zero:
+                            return alpha_abs(bx + x, by + y, mk)
+                        c4 = [int(mk[i]) if i < len(mk) else 0 for i in [i00, i00 + nx, i00 + ny, i00 + ny + nx]]
+                        if not interp:
+                            return byte(c4[0])
+                        r = [ip(c4[0], c4[2], BH, ys_, wy), ip(c4[1], c4[3], BH, ys_, wy)]
+                        return byte(ip(r[0], r[1], BW, xs_, wx))
+
+                    b255 = lambda a, b, w: byte((a * (255 - w) + b * w + 255) >> 8)
+                    if mode in (21, 22):
+                        a0, a1 = alpha_of(masks[0]), alpha_of(masks[1])
+                        ea, eb = b255(vals[0], vals[1], a0), b255(vals[1], vals[0], a1)
+                        if mode == 21:
+                            m = b256(ea, eb, thr)
+                        else:
+                            m = min(max(b256(curs[0], curs[1], thr), min(ea, eb)), max(ea, eb))
+                        if final is not None:
+                            m = b255(m, b256(curs[0], curs[1], tlimit), alpha_of(final))
+                        dst[by + y, bx + x] = m
+                        continue
+                    if mode == 13:
                         m = min(max(b256(curs[0], curs[1], thr), min(vals)), max(vals))
                     else:
                         m = b256(vals[0], vals[1], thr)
@@ -271,33 +297,41 @@ def _py_dual(cfg, chroma, interp, zero, mode13, thr, srcs, strides, spans, shift
     return dst
 
 
-DUAL_CASES = [  # w, h, block, step, interp, zero origin, mode13, threshold, mask
-    (40, 24, 8, 1, True, False, False, 100, False),
-    (40, 24, 8, 1, True, False, True, 200, True),
-    (36, 22, 16, 2, False, True, True, 64, True),
-    (32, 16, 8, 2, True, True, False, 128, True),    # the zero-origin variant with interpolation
-    (20, 12, 32, 1, True, False, True, 30, False),
+DUAL_CASES = [  # w, h, block, step, interp, zero origin, mode, threshold, masks (0 none, 2 a+b, 3 a+b+final)
+    (40, 24, 8, 1, True, False, 11, 100, 0),
+    (40, 24, 8, 1, True, False, 13, 200, 2),
+    (36, 22, 16, 2, False, True, 13, 64, 2),
+    (32, 16, 8, 2, True, True, 11, 128, 2),    # the zero-origin variant with interpolation
+    (20, 12, 32, 1, True, False, 13, 30, 0),
+    (40, 24, 8, 1, True, False, 21, 150, 2),
+    (40, 24, 16, 2, True, False, 22, 90, 3),
+    (36, 22, 8, 1, False, True, 21, 200, 3),
+    (32, 16, 8, 2, False, True, 22, 10, 2),
 ]
 
 
 @pytest.mark.parametrize("case", range(len(DUAL_CASES)))
 def test_oracle_dual_matches_python_restatement(case):
-    w, h, blk, step, interp, zero, mode13, thr, masked = DUAL_CASES[case]
+    w, h, blk, step, interp, zero, mode, thr, nmask = DUAL_CASES[case]
     rng = np.random.default_rng(50 + case)
     gw, gh = _grid(w, h, blk, blk)
     cfg = _cfg(w, h, blk, blk, gw, gh, step)
     mot0 = (_motion(rng, gw * gh, 40), _motion(rng, gw * gh, 40))
     mot1 = (_motion(rng, gw * gh, 40), _motion(rng, gw * gh, 40))
-    mask = rng.integers(0, 256, size=gw * gh, dtype=np.uint8) if masked else None
+    masks = (rng.integers(0, 256, size=gw * gh, dtype=np.uint8),
+             rng.integers(0, 256, size=gw * gh, dtype=np.uint8)) if nmask else None
+    final = rng.integers(0, 256, size=gw * gh, dtype=np.uint8) if nmask == 3 else None
+    tlimit = orc.render_threshold_limit(thr, 1.5)
     shift = {1: 0, 2: 1}[step]
     for chroma in (False, True):
         pw, ph = (w // 2, h // 2) if chroma else (w, h)
         strides = [pw + 3, pw + 5]
         srcs = [rng.integers(0, 256, size=(step * step) * ph * st, dtype=np.uint8) for st in strides]
         spans = [st * ph if shift else 0 for st in strides]
-        got = orc.render_dual_plane(cfg, chroma, interp, zero, mode13, thr, srcs, strides, spans, shift, mot0, mot1,
-                                    pw, ph, mask)
-        want = _py_dual(cfg, chroma, interp, zero, mode13, thr, srcs, strides, spans, shift, mot0, mot1, mask)
+        got = orc.render_dual_plane(cfg, chroma, interp, zero, mode, thr, srcs, strides, spans, shift, mot0, mot1, pw,
+                                    ph, masks, final, tlimit)
+        want = _py_dual(cfg, chroma, interp, zero, mode, thr, srcs, strides, spans, shift, mot0, mot1, masks, final,
+                        tlimit)
         assert np.array_equal(got, want), f"chroma {chroma}: {np.argwhere(got != want)[:3]}"
 
 
@@ -475,8 +509,8 @@ def test_render_blend_matches_oracle(case):
         strides = [pw + 7 * pl, pw + 3]
         planes = [rng.integers(0, 256, size=(step * step) * ph * st, dtype=np.uint8) for st in strides]
         spans = [st * ph if shift else 0 for st in strides]
-        wants.append(orc.render_dual_plane(cfg, pl > 0, interp, zero or not interp, mode13, thr, planes, strides,
-                                           spans, shift, mot[0], mot[1], pw, ph, np.maximum(ma, mb) if masked else None))
+        wants.append(orc.render_dual_plane(cfg, pl > 0, interp, zero or not interp, 13 if mode13 else 11, thr, planes,
+                                           strides, spans, shift, mot[0], mot[1], pw, ph, (ma, mb) if masked else None))
         for k in range(2):
             srcs[k].append((torch.from_numpy(planes[k]).cuda(), strides[k]))
         dsts.append(torch.full((ph, pw), 7, dtype=torch.uint8, device="cuda"))
@@ -489,6 +523,57 @@ def test_render_blend_matches_oracle(case):
                            [t.numel() for t, _ in srcs[1]], shift, (md[0][0].data_ptr(), md[0][1].data_ptr()),
                            (md[1][0].data_ptr(), md[1][1].data_ptr()), [d.data_ptr() for d in dsts],
                            [d.shape[1] for d in dsts], masks=(mkd[0].data_ptr(), mkd[1].data_ptr()) if masked else None)
+    torch.cuda.synchronize()
+    for pl in range(3):
+        got = dsts[pl].cpu().numpy()
+        assert np.array_equal(got, wants[pl]), f"plane {pl}: {np.argwhere(got != wants[pl])[:3]}"
+
+
+MASKED_GPU_CASES = [  # w, h, block, step, interp, mode22, threshold, final mask, mask scale
+    (1920, 1080, 16, 2, True, False, 128, True, 1.0),
+    (1920, 1080, 8, 1, True, True, 200, False, 1.5),
+    (640, 360, 16, 1, False, True, 40, True, 0.75),
+    (66, 38, 32, 4, True, False, 256, True, 2.0),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(len(MASKED_GPU_CASES)))
+def test_render_masked_matches_oracle(case):
+    import torch
+
+    import svpflow_b200 as sv
+
+    w, h, blk, step, interp, mode22, thr, with_final, scale = MASKED_GPU_CASES[case]
+    rng = np.random.default_rng(300 + case)
+    gw, gh = _grid(w, h, blk, blk)
+    cfg = _cfg(w, h, blk, blk, gw, gh, step)
+    shift = {1: 0, 2: 1, 4: 2}[step]
+    mot = [(_motion(rng, gw * gh, 150), _motion(rng, gw * gh, 150)) for _ in range(2)]
+    ma, mb, mf = (rng.integers(0, 256, size=gw * gh, dtype=np.uint8) for _ in range(3))
+    tlimit = orc.render_threshold_limit(thr, scale)
+    srcs, wants, dsts = [[], []], [], []
+    for pl in range(3):
+        pw, ph = (w // 2, h // 2) if pl else (w, h)
+        strides = [pw + 5, pw]
+        planes = [rng.integers(0, 256, size=(step * step) * ph * st, dtype=np.uint8) for st in strides]
+        spans = [st * ph if shift else 0 for st in strides]
+        wants.append(orc.render_dual_plane(cfg, pl > 0, interp, not interp, 22 if mode22 else 21, thr, planes,
+                                           strides, spans, shift, mot[0], mot[1], pw, ph, (ma, mb),
+                                           mf if with_final else None, tlimit))
+        for k in range(2):
+            srcs[k].append((torch.from_numpy(planes[k]).cuda(), strides[k]))
+        dsts.append(torch.full((ph, pw), 7, dtype=torch.uint8, device="cuda"))
+    dev = lambda a: torch.from_numpy(a.astype(np.int16) if a.dtype == np.uint16 else a).cuda()
+    md = [(dev(x), dev(y)) for x, y in mot]
+    mad, mbd, mfd = dev(ma), dev(mb), dev(mf)
+    sv.render_masked_device(cfg, thr, scale, mode22, interp, [t.data_ptr() for t, _ in srcs[0]],
+                            [st for _, st in srcs[0]], [t.numel() for t, _ in srcs[0]],
+                            [t.data_ptr() for t, _ in srcs[1]], [st for _, st in srcs[1]],
+                            [t.numel() for t, _ in srcs[1]], shift, (md[0][0].data_ptr(), md[0][1].data_ptr()),
+                            (md[1][0].data_ptr(), md[1][1].data_ptr()), (mad.data_ptr(), mbd.data_ptr()),
+                            mfd.data_ptr() if with_final else 0, [d.data_ptr() for d in dsts],
+                            [d.shape[1] for d in dsts])
     torch.cuda.synchronize()
     for pl in range(3):
         got = dsts[pl].cpu().numpy()
