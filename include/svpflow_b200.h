@@ -202,6 +202,17 @@ int svpf_render_masked_device(const svpf_render_config *cfg, int32_t threshold, 
                               const uint16_t *motion0_y, const uint16_t *motion1_x, const uint16_t *motion1_y,
                               const uint8_t *mask_a, const uint8_t *mask_b, const uint8_t *final_mask,
                               uint8_t *const dst[3], const int64_t dst_stride[3], void *stream);
+/* CpuRenderer::render_mode23 (renderer.rs:644-666, render_mode23_plane_rows_inner :1294-1537) on the
+ * device: four motion sets motion_x/y[0..3] = base0, base1, next0, prev1 (sets 0 and 2 read source 0
+ * with the threshold LUT, 1 and 3 source 1 with the inverse LUT); mode23_pixel (:1850-1868) with
+ * alphas from mask_a and mask_b (required) and final_mask (optional) blending towards
+ * blend_256(cur0, cur1, threshold). Zero origin when interp == 0, as the reference. */
+int svpf_render_mode23_device(const svpf_render_config *cfg, int32_t threshold, int32_t interp,
+                              const uint8_t *const src0[3], const int64_t src0_stride[3], const int64_t src0_len[3],
+                              const uint8_t *const src1[3], const int64_t src1_stride[3], const int64_t src1_len[3],
+                              int32_t src_shift, const uint16_t *const motion_x[4], const uint16_t *const motion_y[4],
+                              const uint8_t *mask_a, const uint8_t *mask_b, const uint8_t *final_mask,
+                              uint8_t *const dst[3], const int64_t dst_stride[3], void *stream);
 
 /* ---------------------------------------------------------------- batched form */
 /* No counterpart in the reference, which analyses one clip at a time, one output frame

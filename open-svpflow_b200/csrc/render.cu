@@ -1,12 +1,13 @@
 // render.cu -- SmoothFps's frame render on the device: the single warp of algorithms 1 and 2 and
-// the two-source blends of algorithms 11, 13, 21 and 22. Each output sample reads its source(s) at its
+// the two-source blends of algorithms 11, 13, 21, 22 and 23. Each output sample reads its source(s) at its
 // position displaced by motion interpolated between the four motion-plane samples around it, and
 // optionally blends with the undisplaced samples by the mode's mask.
 //
 // Follows crates/svpflow-core/src/renderer.rs: CpuRenderer::render_mode1_or_2 (:308-328) through
 // render_selected_warp_rows (:876-984); render_mode11_or_13 and its zero-origin variant (:330-438)
 // through render_dual_warp_rows (:1031-1172) and mode11_or_13_pixel (:2918-2943); render_mode21_or_22
-// (:571-641) with mode21_pixel / mode22_pixel (:1830-1848); set_threshold / set_threshold_value
+// (:571-641) with mode21_pixel / mode22_pixel (:1830-1848); render_mode23 (:644-666) through
+// render_mode23_plane_rows_inner (:1294-1537) with mode23_pixel (:1850-1868); set_threshold / set_threshold_value
 // (:238-264), plane_params (:1539-1606), motion_samples (:1608-1638), render_tiles (:1925-2010),
 // interpolate_row / interpolate_motion (:2582-2637), alpha_row / alpha_at_row / alpha_at_absolute
 // (:2639-2722), interp_pair (:2724-2738), interpolation_weights / coeff (:2740-2770), plane_covers /
@@ -53,11 +54,11 @@ struct RenderPlane {
 
 struct RenderJob {
     RenderPlane pl[3];
-    const uint16_t *mx[2], *my[2];  // motion sets 0 and 1 (the single warp uses set 0)
+    const uint16_t *mx[4], *my[4];  // motion sets (set k reads source k & 1; the single warp uses set 0)
     const uint8_t *mask[3];         // the single warp: [0]; 11 / 13: [0], [1] of max_mask; 21 / 22: a, b, final
     int64_t mlen;
     int32_t grid_w, grid_h, interp, zero_origin, shift;
-    int32_t lut_t[2];               // LUT factors of the sets: threshold or 256 - threshold
+    int32_t lut_t[4];               // LUT factors of the sets: threshold or 256 - threshold
     int32_t threshold, mode13;      // the two-source blends
     int32_t mode22, threshold_limit;  // 21 / 22
 };
@@ -262,15 +263,17 @@ __device__ __forceinline__ int32_t alpha_at(const RenderJob &J, const RenderPlan
     return clamp_byte(interp_pair(m0, m1, p.block_w, p.x_shift, sxw[min(px - bx, kMaxBlock - 1)]));
 }
 
-// KIND 0: the single warp (sources[0], set 0; mode1_pixel with the mask when MASK). KIND 1: the
+// KIND 0: the single warp (source 0, set 0; mode1_pixel with the mask when MASK). KIND 1: the
 // two-source blend of algorithms 11 / 13 (set 0 reads source 0, set 1 source 1; mode11_or_13_pixel,
-// max_mask when MASK). KIND 2: algorithms 21 / 22 (the same reads; mode21_or_22_pixel with alphas
-// from masks a and b, and the final mask when MASK). Grid: (row length of the widest plane /
-// (256 kPx), rows of the tallest plane, 3 planes).
+// max_mask when MASK). KIND 2: algorithms 21 / 22 (the same reads; mode21_or_22_pixel with alphas from
+// masks a and b, and the final mask when MASK). KIND 3: algorithm 23 (sets base0, base1, next0, prev1,
+// set k reading source k & 1; mode23_pixel with masks a and b, and the final mask when MASK).
+// Grid: (row length of the widest plane / (256 kPx), rows of the tallest plane, 3 planes).
 template <int KIND, bool MASK>
 __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ RenderJob J) {
     constexpr bool DUAL = KIND > 0;
-    constexpr int NA = KIND == 2 ? (MASK ? 3 : 2) : (MASK ? 1 : 0);  // alphas per sample
+    constexpr int NS = KIND == 0 ? 1 : (KIND == 3 ? 4 : 2);          // motion sets
+    constexpr int NA = KIND >= 2 ? (MASK ? 3 : 2) : (MASK ? 1 : 0);  // alphas per sample
     const RenderPlane &p = J.pl[blockIdx.z];
     // the plane's interpolation weights in shared memory (indexed per thread)
     __shared__ int32_t sxw[kMaxBlock][2], syw[kMaxBlock][2];
@@ -290,26 +293,29 @@ __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ Ren
     tile_of(pxl, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gxl, bxl, twl);
     const bool shared_tile = gx == gxl;  // usually: then the tile's motion is fetched once
     Tile t = make_tile(J, gx, bx, tw, gy, by, th);
-    SetRow r0 = set_row(J, p, t, 0, py, syw), r1 = r0;
-    if (DUAL) r1 = set_row(J, p, t, 1, py, syw);
+    SetRow r[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) r[k] = set_row(J, p, t, k, py, syw);
     // the mask selectors of the alphas: the mode's (max) mask, or masks a, b, final
-    auto sel_of = [](int a) { return KIND == 2 ? a : -1; };
+    auto sel_of = [](int a) { return KIND >= 2 ? a : -1; };
     int32_t m0[NA > 0 ? NA : 1], m1[NA > 0 ? NA : 1];
 #pragma unroll
     for (int a = 0; a < NA; a++) mask_row(J, p, t, py, syw, sel_of(a), m0[a], m1[a]);
     auto direct_of = [&]() {  // plane_covers && tile_interior for the tile's sets
-        bool d = p.src[0].covers && p.step > 0 && interior(p, t, r0);
-        if (DUAL) d = d && p.src[1].covers && interior(p, t, r1);
+        bool d = p.src[0].covers && p.step > 0 && (!DUAL || p.src[1].covers);
+#pragma unroll
+        for (int k = 0; k < NS; k++) d = d && interior(p, t, r[k]);
         return d;
     };
     bool direct = direct_of();
     // indices first, then every load of the thread's samples, so the gathers overlap
-    int64_t i0[kPx], i1[kPx];
+    int64_t idx[NS][kPx];
     int32_t alpha[NA > 0 ? NA : 1][kPx];
 #pragma unroll
     for (int k = 0; k < kPx; k++) {
         const int32_t px = px0 + k;
-        i0[k] = i1[k] = -1;
+#pragma unroll
+        for (int q = 0; q < NS; q++) idx[q][k] = -1;
 #pragma unroll
         for (int a = 0; a < NA; a++) alpha[a][k] = 0;
         if (px > pxl) continue;
@@ -319,52 +325,61 @@ __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ Ren
             if (gk != gx) {
                 gx = gk;
                 t = make_tile(J, gk, bk, twk, gy, by, th);
-                r0 = set_row(J, p, t, 0, py, syw);
-                if (DUAL) r1 = set_row(J, p, t, 1, py, syw);
+#pragma unroll
+                for (int q = 0; q < NS; q++) r[q] = set_row(J, p, t, q, py, syw);
 #pragma unroll
                 for (int a = 0; a < NA; a++) mask_row(J, p, t, py, syw, sel_of(a), m0[a], m1[a]);
                 direct = direct_of();
             }
         }
-        i0[k] = warp_index(J, p, p.src[0], r0, direct, px, t.bx, py, sxw);
-        if (DUAL) i1[k] = warp_index(J, p, p.src[1], r1, direct, px, t.bx, py, sxw);
+#pragma unroll
+        for (int q = 0; q < NS; q++) idx[q][k] = warp_index(J, p, p.src[q & 1], r[q], direct, px, t.bx, py, sxw);
 #pragma unroll
         for (int a = 0; a < NA; a++) alpha[a][k] = alpha_at(J, p, sel_of(a), m0[a], m1[a], px, t.bx, py, sxw);
     }
     // the undisplaced samples (px * step <= max_x: no clamp)
-    const bool bases = KIND == 0 ? MASK : (KIND == 1 ? (MASK || J.mode13) : (MASK || J.mode22));
-    int32_t v0[kPx], v1[kPx], c0[kPx], c1[kPx];
+    const bool bases = KIND == 0 ? MASK : (KIND == 1 ? (MASK || J.mode13) : (KIND == 2 ? (MASK || J.mode22) : MASK));
+    int32_t v[NS][kPx], c0[kPx], c1[kPx];
 #pragma unroll
     for (int k = 0; k < kPx; k++) {
         const int32_t px = min(px0 + k, pxl);
-        v0[k] = load(p.src[0], i0[k]);
-        v1[k] = DUAL ? load(p.src[1], i1[k]) : 0;
+#pragma unroll
+        for (int q = 0; q < NS; q++) v[q][k] = load(p.src[q & 1], idx[q][k]);
         c0[k] = bases ? load(p.src[0], src_index(p.src[0], J.shift, px * p.step, py * p.step)) : 0;
         c1[k] = bases && DUAL ? load(p.src[1], src_index(p.src[1], J.shift, px * p.step, py * p.step)) : 0;
     }
     int32_t out[kPx];
 #pragma unroll
     for (int k = 0; k < kPx; k++) {
-        int32_t v;
-        if (KIND == 2) {  // mode21_or_22_pixel
-            const int32_t ea = blend255(v0[k], v1[k], alpha[0][k]), eb = blend255(v1[k], v0[k], alpha[1][k]);
-            if (J.mode22) v = min(max(blend256(c0[k], c1[k], J.threshold), min(ea, eb)), max(ea, eb));
-            else v = blend256(ea, eb, J.threshold);
-            if (MASK) v = blend255(v, blend256(c0[k], c1[k], J.threshold_limit), alpha[NA - 1][k]);
+        int32_t o;
+        if (KIND == 3) {  // mode23_pixel: a, b, c, d = base0, base1, next0, prev1 samples
+            const int32_t a = v[0][k], b = v[1 % NS][k], c = v[2 % NS][k], d = v[3 % NS][k];
+            const int32_t lo = min(a, b), hi = max(a, b);
+            const int32_t i0 = blend255(a, min(max(d, lo), hi), alpha[0][k]);
+            const int32_t i1 = blend255(b, min(max(c, lo), hi), alpha[1 % NA][k]);
+            o = blend256(i0, i1, J.threshold);
+            if (MASK) o = blend255(o, blend256(c0[k], c1[k], J.threshold), alpha[NA - 1][k]);
+        } else if (KIND == 2) {  // mode21_or_22_pixel
+            const int32_t v0 = v[0][k], v1 = v[1 % NS][k];
+            const int32_t ea = blend255(v0, v1, alpha[0][k]), eb = blend255(v1, v0, alpha[1 % NA][k]);
+            if (J.mode22) o = min(max(blend256(c0[k], c1[k], J.threshold), min(ea, eb)), max(ea, eb));
+            else o = blend256(ea, eb, J.threshold);
+            if (MASK) o = blend255(o, blend256(c0[k], c1[k], J.threshold_limit), alpha[NA - 1][k]);
         } else if (KIND == 1) {  // mode11_or_13_pixel
-            const int32_t b = blend256(c0[k], c1[k], J.threshold);
-            if (J.mode13) v = min(max(b, min(v0[k], v1[k])), max(v0[k], v1[k]));  // mode13_pixel
-            else v = blend256(v0[k], v1[k], J.threshold);                          // mode11_pixel
-            if (MASK) v = blend255(v, b, alpha[0][k]);
+            const int32_t v0 = v[0][k], v1 = v[1 % NS][k];
+            const int32_t bl = blend256(c0[k], c1[k], J.threshold);
+            if (J.mode13) o = min(max(bl, min(v0, v1)), max(v0, v1));  // mode13_pixel
+            else o = blend256(v0, v1, J.threshold);                     // mode11_pixel
+            if (MASK) o = blend255(o, bl, alpha[0][k]);
         } else {
-            v = MASK ? blend255(v0[k], c0[k], alpha[0][k]) : v0[k];  // mode1_pixel
+            o = MASK ? blend255(v[0][k], c0[k], alpha[0][k]) : v[0][k];  // mode1_pixel
         }
-        out[k] = v;
+        out[k] = o;
     }
-    uint8_t *o = p.dst + (int64_t)py * p.dst_stride + px0;
+    uint8_t *dst = p.dst + (int64_t)py * p.dst_stride + px0;
 #pragma unroll
     for (int k = 0; k < kPx; k++)
-        if (px0 + k <= pxl) o[k] = (uint8_t)out[k];
+        if (px0 + k <= pxl) dst[k] = (uint8_t)out[k];
 }
 
 // Per-plane constants of one frame (plane_params for chroma = plane > 0), the sources' layouts and
@@ -444,7 +459,10 @@ int launch(const RenderJob &J, int kind, bool mask, int32_t most_w, int32_t most
     if (most_w > 0 && most_h > 0) {
         dim3 grid((unsigned)((most_w + 256 * kPx - 1) / (256 * kPx)), (unsigned)most_h, 3);
         cudaStream_t st = (cudaStream_t)stream;
-        if (kind == 2) {
+        if (kind == 3) {
+            if (mask) render_kernel<3, true><<<grid, 256, 0, st>>>(J);
+            else render_kernel<3, false><<<grid, 256, 0, st>>>(J);
+        } else if (kind == 2) {
             if (mask) render_kernel<2, true><<<grid, 256, 0, st>>>(J);
             else render_kernel<2, false><<<grid, 256, 0, st>>>(J);
         } else if (kind == 1) {
@@ -574,6 +592,44 @@ int svpf_render_masked_device(const svpf_render_config *cfg, int32_t threshold, 
     int rc = setup(*J, cfg, 2, srcs, strides, lens, src_shift, dst, dst_stride, mw, mh);
     if (rc) svpf::set_last_error("render: bad plane buffers");
     else rc = launch(*J, 2, final_mask != nullptr, mw, mh, stream);
+    delete J;
+    return rc;
+}
+
+int svpf_render_mode23_device(const svpf_render_config *cfg, int32_t threshold, int32_t interp,
+                              const uint8_t *const src0[3], const int64_t src0_stride[3], const int64_t src0_len[3],
+                              const uint8_t *const src1[3], const int64_t src1_stride[3], const int64_t src1_len[3],
+                              int32_t src_shift, const uint16_t *const motion_x[4], const uint16_t *const motion_y[4],
+                              const uint8_t *mask_a, const uint8_t *mask_b, const uint8_t *final_mask,
+                              uint8_t *const dst[3], const int64_t dst_stride[3], void *stream) {
+    if (int rc = check_common(cfg, threshold, src_shift)) return rc;
+    bool ok = src0 && src0_stride && src0_len && src1 && src1_stride && src1_len && dst && dst_stride && motion_x &&
+              motion_y && mask_a && mask_b;
+    for (int k = 0; ok && k < 4; k++) ok = motion_x[k] && motion_y[k];
+    if (!ok) {
+        svpf::set_last_error("render: null argument (four motion sets and masks a, b are required)");
+        return SVPF_EINVAL;
+    }
+    if (draws_nothing(cfg)) return SVPF_OK;
+    RenderJob *J = new RenderJob;
+    memset(J, 0, sizeof(*J));
+    for (int k = 0; k < 4; k++) {  // base0, base1, next0, prev1: threshold LUT for 0 / 2, inverse for 1 / 3
+        J->mx[k] = motion_x[k];
+        J->my[k] = motion_y[k];
+        J->lut_t[k] = (k & 1) ? 256 - threshold : threshold;
+    }
+    J->mask[0] = mask_a;
+    J->mask[1] = mask_b;
+    J->mask[2] = final_mask;
+    J->interp = interp != 0;
+    J->zero_origin = interp == 0;  // render_mode23 renders at zero origin when not interpolating
+    J->threshold = threshold;
+    const uint8_t *const *srcs[2] = {src0, src1};
+    const int64_t *strides[2] = {src0_stride, src1_stride}, *lens[2] = {src0_len, src1_len};
+    int32_t mw, mh;
+    int rc = setup(*J, cfg, 2, srcs, strides, lens, src_shift, dst, dst_stride, mw, mh);
+    if (rc) svpf::set_last_error("render: bad plane buffers");
+    else rc = launch(*J, 3, final_mask != nullptr, mw, mh, stream);
     delete J;
     return rc;
 }

@@ -115,6 +115,8 @@ def lib() -> ctypes.CDLL:
             "svpf_render_masked_device": (I32, [P(RenderConfig), I32, ctypes.c_double, I32, I32, P(_VP), P(I64),
                                                 P(I64), P(_VP), P(I64), P(I64), I32, _VP, _VP, _VP, _VP, _VP, _VP,
                                                 _VP, P(_VP), P(I64), _VP]),
+            "svpf_render_mode23_device": (I32, [P(RenderConfig), I32, I32, P(_VP), P(I64), P(I64), P(_VP), P(I64),
+                                                P(I64), I32, P(_VP), P(_VP), _VP, _VP, _VP, P(_VP), P(I64), _VP]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -539,3 +541,20 @@ def render_masked_device(cfg: dict, threshold: int, mask_scale: float, mode22: b
                                            int(src_shift), motion0[0], motion0[1], motion1[0], motion1[1], masks[0],
                                            masks[1], final_mask_ptr or None, arr(_VP, dst_ptrs),
                                            arr(ctypes.c_int64, dst_strides), stream))
+
+
+def render_mode23_device(cfg: dict, threshold: int, interp: bool, src0_ptrs, src0_strides, src0_lens, src1_ptrs,
+                         src1_strides, src1_lens, src_shift: int, motions, masks, final_mask_ptr, dst_ptrs,
+                         dst_strides, stream: int = 0):
+    """SmoothFps's algorithm 23 (four motion sets: base0, base1, next0, prev1 as (x_ptr, y_ptr)) of one
+    frame on the device; masks = (a_ptr, b_ptr); see svpf_render_mode23_device."""
+    c = RenderConfig(**{k: int(cfg[k]) for k, _ in RenderConfig._fields_})
+    arr = lambda t, v: (t * 3)(*[int(x) for x in v])
+    mx = (_VP * 4)(*[m[0] for m in motions])
+    my = (_VP * 4)(*[m[1] for m in motions])
+    _check(lib().svpf_render_mode23_device(ctypes.byref(c), int(threshold), int(interp), arr(_VP, src0_ptrs),
+                                           arr(ctypes.c_int64, src0_strides), arr(ctypes.c_int64, src0_lens),
+                                           arr(_VP, src1_ptrs), arr(ctypes.c_int64, src1_strides),
+                                           arr(ctypes.c_int64, src1_lens), int(src_shift), mx, my, masks[0], masks[1],
+                                           final_mask_ptr or None, arr(_VP, dst_ptrs), arr(ctypes.c_int64, dst_strides),
+                                           stream))

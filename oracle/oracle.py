@@ -456,6 +456,8 @@ def _setup(L):
         L.or_render_luts.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
         L.or_render_dual_plane.argtypes = [P(RenderConfig)] + [ctypes.c_int32] * 6 + [P(RPlane), P(RPlane)] + \
             [ctypes.c_void_p] * 4 + [ctypes.c_size_t] + [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_size_t]
+        L.or_render_mode23_plane.argtypes = [P(RenderConfig)] + [ctypes.c_int32] * 3 + [P(RPlane), P(RPlane)] + \
+            [ctypes.c_void_p] * 2 + [ctypes.c_size_t] + [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_size_t]
         L.or_render_threshold_limit.restype = ctypes.c_int32
         L.or_render_threshold_limit.argtypes = [ctypes.c_int32, ctypes.c_double]
         L.or_render_warp_plane.argtypes = [P(RenderConfig), ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
@@ -787,4 +789,22 @@ def render_dual_plane(cfg: dict, chroma: bool, interp: bool, zero_origin: bool, 
                                int(threshold), int(threshold_limit), ctypes.byref(pls[0]), ctypes.byref(pls[1]),
                                *[_ptr(m) for m in ms], n, *[None if m is None else _ptr(m) for m in mk], _ptr(dst),
                                dst_stride, dst.size)
+    return dst.reshape(dst_rows, dst_stride)
+
+
+def render_mode23_plane(cfg: dict, chroma: bool, interp: bool, threshold: int, srcs, strides, spans, shift: int,
+                        motions, masks, final_mask, dst_stride: int, dst_rows: int) -> np.ndarray:
+    """render_mode23 for one plane: motions = 4 (mx, my) sets (base0, base1, next0, prev1), masks = (a, b)."""
+    c = RenderConfig(**{k: int(cfg[k]) for k, _ in RenderConfig._fields_})
+    ss = [np.ascontiguousarray(x, dtype=np.uint8).reshape(-1) for x in srcs]
+    pls = [RPlane(ss[i].ctypes.data, ss[i].size, strides[i], spans[i], shift) for i in range(2)]
+    mx = [np.ascontiguousarray(m[0], dtype=np.uint16).reshape(-1) for m in motions]
+    my = [np.ascontiguousarray(m[1], dtype=np.uint16).reshape(-1) for m in motions]
+    px_ = (ctypes.c_void_p * 4)(*[m.ctypes.data for m in mx])
+    py_ = (ctypes.c_void_p * 4)(*[m.ctypes.data for m in my])
+    mk = [None if m is None else np.ascontiguousarray(m, dtype=np.uint8).reshape(-1) for m in (*masks, final_mask)]
+    dst = np.zeros(dst_rows * dst_stride, dtype=np.uint8)
+    lib().or_render_mode23_plane(ctypes.byref(c), int(chroma), int(interp), int(threshold), ctypes.byref(pls[0]),
+                                 ctypes.byref(pls[1]), px_, py_, mx[0].size,
+                                 *[None if m is None else _ptr(m) for m in mk], _ptr(dst), dst_stride, dst.size)
     return dst.reshape(dst_rows, dst_stride)

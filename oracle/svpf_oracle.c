@@ -2311,4 +2311,119 @@ void or_render_dual_plane(const or_render_config *c, int32_t chroma, int32_t int
     }
     free(mask);
 }
+
+/* render_mode23_plane_rows_inner (:1294-1537) with mode23_pixel (:1850-1868): four motion sets (base0
+ * and next0 with the threshold LUT reading source 0, base1 and prev1 with the inverse LUT reading
+ * source 1), alphas t0 / t1 from masks a / b, the optional final mask towards blend_256(base_a,
+ * base_b, threshold); zero origin when not interpolated. */
+void or_render_mode23_plane(const or_render_config *c, int32_t chroma, int32_t interp, int32_t threshold,
+                            const or_rplane *src0, const or_rplane *src1, const uint16_t *const mxs[4],
+                            const uint16_t *const mys[4], size_t mlen, const uint8_t *mask_a, const uint8_t *mask_b,
+                            const uint8_t *mask_f, uint8_t *dst, size_t dst_stride, size_t dst_len) {
+    int16_t inv[2048], thr[2048];
+    or_render_luts(threshold, inv, thr);
+    int zero_origin = !interp;
+    rparams P, MP;
+    r_params(c, chroma, zero_origin, &P);
+    r_params(c, chroma, 0, &MP);
+    const rparams *p = &P;
+    i32 gw = (i32)c->grid_w, gh = (i32)c->grid_h;
+    if (p->width <= 0 || p->height <= 0 || p->block_w <= 0 || p->block_h <= 0 || gw <= 0 || gh <= 0) return;
+    i32 rows_end = chroma ? c->height / c->chroma_y_div : c->height;
+    int covers = r_covers(src0, p) && r_covers(src1, p);
+    for (i32 gy = -1; gy < gh; gy++) {
+        i32 base_y = gy < 0 ? 0 : p->origin_y + p->block_h * gy;
+        i32 height = gy < 0 ? p->origin_y : p->block_h;
+        if (base_y + p->block_h >= p->height || gy == gh - 1) height = p->height - base_y;
+        i32 end_y = base_y + height < rows_end ? base_y + height : rows_end;
+        i32 clipped_y = base_y > 0 ? base_y : 0;
+        height = end_y - clipped_y;
+        if (height <= 0) continue;
+        for (i32 gx = -1; gx < gw; gx++) {
+            i32 base_x = gx < 0 ? 0 : p->origin_x + p->block_w * gx;
+            i32 width = gx < 0 ? p->origin_x : p->block_w;
+            if (base_x + p->block_w >= p->width || gx == gw - 1) width = p->width - base_x;
+            if (width <= 0) continue;
+            usize x0 = (usize)(gx > 0 ? gx : 0), y0 = (usize)(gy > 0 ? gy : 0);
+            usize nx = (gx >= 0 && gx != gw - 1) ? 1 : 0, ny = (gy >= 0 && gy != gh - 1) ? (usize)gw : 0;
+            usize ii[4] = {y0 * (usize)gw + x0, 0, 0, 0};
+            ii[1] = ii[0] + nx; ii[2] = ii[0] + ny; ii[3] = ii[0] + ny + nx;
+            i32 tx = base_x, ty = clipped_y;
+            i32 sx[4][4], sy[4][4];
+            for (int set = 0; set < 4; set++) {
+                const int16_t *lut = (set & 1) ? inv : thr;
+                for (int q = 0; q < 4; q++) {
+                    usize i = interp ? ii[q] : ii[0];
+                    sx[set][q] = r_motion(lut, mxs[set], mlen, i) / p->x_div;
+                    sy[set][q] = r_motion(lut, mys[set], mlen, i) / p->y_div;
+                }
+            }
+            int direct = 0;
+            if (covers && p->step > 0) {
+                i32 mnx = INT32_MAX, mxx = INT32_MIN, mny = INT32_MAX, mxy = INT32_MIN;
+                for (int set = 0; set < 4; set++)
+                    for (int q = 0; q < 4; q++) {
+                        mnx = sx[set][q] < mnx ? sx[set][q] : mnx; mxx = sx[set][q] > mxx ? sx[set][q] : mxx;
+                        mny = sy[set][q] < mny ? sy[set][q] : mny; mxy = sy[set][q] > mxy ? sy[set][q] : mxy;
+                    }
+                int64_t st = p->step;
+                direct = (int64_t)tx * st + mnx >= 0 && (int64_t)ty * st + mny >= 0 &&
+                         (int64_t)(tx + width - 1) * st + mxx <= p->max_x && (int64_t)(ty + height - 1) * st + mxy <= p->max_y;
+            }
+            for (i32 y = 0; y < height; y++) {
+                i32 local_y = clipped_y - base_y + y;
+                i32 source_y = (ty + y) * p->step;
+                usize start = (usize)(ty + y) * dst_stride + (usize)tx;
+                if (start + (usize)width > dst_len) continue;
+                const i32 *wy = p->yw[local_y < 0 ? 0 : (local_y > 31 ? 31 : local_y)];
+                i32 row[4][2][2];
+                for (int set = 0; set < 4; set++) {
+                    if (!interp) { row[set][0][0] = row[set][0][1] = sx[set][0]; row[set][1][0] = row[set][1][1] = sy[set][0]; }
+                    else {
+                        row[set][0][0] = r_interp(sx[set][0], sx[set][2], p->block_h, p->y_shift, wy);
+                        row[set][0][1] = r_interp(sx[set][1], sx[set][3], p->block_h, p->y_shift, wy);
+                        row[set][1][0] = r_interp(sy[set][0], sy[set][2], p->block_h, p->y_shift, wy);
+                        row[set][1][1] = r_interp(sy[set][1], sy[set][3], p->block_h, p->y_shift, wy);
+                    }
+                }
+                for (i32 x = 0; x < width; x++) {
+                    i32 px = tx + x, source_x = px * p->step;
+                    const i32 *wx = p->xw[x > 31 ? 31 : x];
+                    i32 v[4];
+                    for (int set = 0; set < 4; set++) {
+                        const or_rplane *src = (set & 1) ? src1 : src0;
+                        i32 dx = row[set][0][0], dy = row[set][1][0];
+                        if (interp) {
+                            dx = r_interp(row[set][0][0], row[set][0][1], p->block_w, p->x_shift, wx);
+                            dy = r_interp(row[set][1][0], row[set][1][1], p->block_w, p->x_shift, wx);
+                        }
+                        i32 xs = source_x + dx, ys = source_y + dy;
+                        if (!direct) {
+                            xs = xs < 0 ? 0 : (xs > p->max_x ? p->max_x : xs);
+                            ys = ys < 0 ? 0 : (ys > p->max_y ? p->max_y : ys);
+                        }
+                        usize idx = r_index(src, (usize)(int64_t)xs, (usize)(int64_t)ys);
+                        v[set] = idx < src->len ? src->data[idx] : 0;
+                    }
+                    i32 a = v[0], b = v[1], cc = v[2], d = v[3];
+                    i32 t0 = r_alpha(mask_a, mlen, ii, p, &MP, (usize)c->grid_w, interp, zero_origin, wy, wx, px, ty + y);
+                    i32 t1 = r_alpha(mask_b, mlen, ii, p, &MP, (usize)c->grid_w, interp, zero_origin, wy, wx, px, ty + y);
+                    i32 lo = a < b ? a : b, hi = a < b ? b : a;
+                    i32 dcl = d < lo ? lo : (d > hi ? hi : d), ccl = cc < lo ? lo : (cc > hi ? hi : cc);
+                    i32 i0 = r_byte((a * (255 - t0) + dcl * t0 + 255) >> 8);
+                    i32 i1 = r_byte((b * (255 - t1) + ccl * t1 + 255) >> 8);
+                    i32 motion = r_blend256(i0, i1, threshold);
+                    if (mask_f) {
+                        i32 bxs = source_x > p->max_x ? p->max_x : source_x, bys = source_y > p->max_y ? p->max_y : source_y;
+                        usize b0 = r_index(src0, (usize)bxs, (usize)bys), b1 = r_index(src1, (usize)bxs, (usize)bys);
+                        i32 ba = b0 < src0->len ? src0->data[b0] : 0, bb = b1 < src1->len ? src1->data[b1] : 0;
+                        i32 fa = r_alpha(mask_f, mlen, ii, p, &MP, (usize)c->grid_w, interp, zero_origin, wy, wx, px, ty + y);
+                        motion = r_byte((motion * (255 - fa) + r_blend256(ba, bb, threshold) * fa + 255) >> 8);
+                    }
+                    dst[start + (usize)x] = (uint8_t)motion;
+                }
+            }
+        }
+    }
+}
 #endif

@@ -201,6 +201,12 @@ void or_render_dual_plane(const or_render_config *c, int32_t chroma, int32_t int
                           const or_rplane *src1, const uint16_t *mx0, const uint16_t *my0, const uint16_t *mx1,
                           const uint16_t *my1, size_t mlen, const uint8_t *mask_a, const uint8_t *mask_b,
                           const uint8_t *mask_f, uint8_t *dst, size_t dst_stride, size_t dst_len);
+/* render_mode23 (renderer.rs:644-666) for one plane: motion sets base0, base1, next0, prev1 (mxs / mys),
+ * masks a, b (required) and the optional final mask. */
+void or_render_mode23_plane(const or_render_config *c, int32_t chroma, int32_t interp, int32_t threshold,
+                            const or_rplane *src0, const or_rplane *src1, const uint16_t *const mxs[4],
+                            const uint16_t *const mys[4], size_t mlen, const uint8_t *mask_a, const uint8_t *mask_b,
+                            const uint8_t *mask_f, uint8_t *dst, size_t dst_stride, size_t dst_len);
 /* set_threshold_value (renderer.rs:256-264): threshold_limit for a mask scale */
 int32_t or_render_threshold_limit(int32_t threshold, double scale);
 int or_vector_planes(const int32_t vdata[16], const uint8_t *payload, size_t len, int32_t frame_w, int32_t frame_h,

@@ -297,6 +297,161 @@ def _py_dual(cfg, chroma, interp, zero, mode, thr, srcs, strides, spans, shift, 
     return dst
 
 
+def _py_mode23(cfg, chroma, interp, thr, srcs, strides, spans, shift, motions, masks, final=None):
+    """render_mode23_plane_rows_inner + mode23_pixel (renderer.rs:1294-1537, :1850-1868) in plain Python."""
+    cmap = lambda v: CPU_MAP[v - 1] if 1 <= v <= 32 else -1
+    cd = cfg["chroma_y_div"]
+    zero = not interp
+    if chroma:
+        W, H, BW, BH = cfg["width"] // 2, cfg["height"] // cd, cfg["block_w"] // 2, cfg["block_h"] // cd
+        mox, moy = cfg["origin_x"] // 2, cfg["origin_y"] // cd
+        xs_, ys_, xd, yd = cmap(cfg["block_w"] // 2), cmap(cfg["block_h"] // 2), 2, cd
+    else:
+        W, H, BW, BH = cfg["width"], cfg["height"], cfg["block_w"], cfg["block_h"]
+        mox, moy = cfg["origin_x"], cfg["origin_y"]
+        xs_, ys_, xd, yd = cmap(BW), cmap(BH), 1, 1
+    ox, oy = (0, 0) if zero else (mox, moy)
+    step = cfg["source_step"]
+    maxx, maxy = max(W * step - 1, 0), max(H * step - 1, 0)
+
+    def weights(total, sh):
+        out = [(0, 0)] * 32
+        for p in range(min(total, 32)):
+            c = lambda v: int(math.ceil(v * (1 << max(sh, 0)) / total - 0.5))
+            out[p] = (total - p, p) if sh < 0 else (c(total - p), c(p))
+        return out
+
+    xw, yw = weights(BW, xs_), weights(BH, ys_)
+    ip = lambda a, b, total, sh, w: int((w[0] * a + w[1] * b) / total) if sh < 0 else (w[0] * a + w[1] * b) >> sh
+    inv, tl = orc.render_luts(thr)
+    gw, gh = cfg["grid_w"], cfg["grid_h"]
+    byte = lambda v: min(max(v, 0), 255)
+    b256 = lambda a, b, w: byte((a * (256 - w) + b * w) >> 8)
+    b255 = lambda a, b, w: byte((a * (255 - w) + b * w + 255) >> 8)
+
+    def index(k, x, y):
+        if shift == 0:
+            return y * strides[k] + x
+        m = (1 << shift) - 1
+        return (((y & m) << shift) | (x & m)) * spans[k] + (y >> shift) * strides[k] + (x >> shift)
+
+    def alpha_abs(x, y, mk):
+        def mat(x, y):
+            i = y * gw + x
+            return int(mk[i]) if x >= 0 and y >= 0 and i < len(mk) else 0
+        ix0 = ix1 = iy0 = iy1 = 0
+        if mox <= x:
+            ix0 = (x - mox) // BW
+            ix1 = ix0 + 1
+        if moy <= y:
+            iy0 = (y - moy) // BH
+            iy1 = iy0 + 1
+        fx = (x - mox) % BW if mox < x else 0
+        fy = (y - moy) % BH if moy < y else 0
+        top = ((BW - fx) * mat(ix0, iy0) + fx * mat(ix1, iy0)) // BW
+        bot = ((BW - fx) * mat(ix0, iy1) + fx * mat(ix1, iy1)) // BW
+        return byte(((BH - fy) * top + fy * bot) // BH)
+
+    covers = all((shift == 0 or (1 << shift) == step) and index(k, maxx, maxy) < len(srcs[k]) for k in range(2))
+    dst = np.zeros((H, W), dtype=np.uint8)
+    for gy in range(-1, gh):
+        by = 0 if gy < 0 else oy + BH * gy
+        th = oy if gy < 0 else BH
+        if by + BH >= H or gy == gh - 1:
+            th = H - by
+        th = min(by + th, H) - max(by, 0)
+        if th <= 0:
+            continue
+        for gx in range(-1, gw):
+            bx = 0 if gx < 0 else ox + BW * gx
+            tw = ox if gx < 0 else BW
+            if bx + BW >= W or gx == gw - 1:
+                tw = W - bx
+            if tw <= 0:
+                continue
+            i00 = max(gy, 0) * gw + max(gx, 0)
+            nx = 1 if (gx >= 0 and gx != gw - 1) else 0
+            ny = gw if (gy >= 0 and gy != gh - 1) else 0
+            corners = [i00, i00 + nx, i00 + ny, i00 + ny + nx]
+            idx = corners if interp else [i00] * 4
+            S = []
+            for k, (mx, my) in enumerate(motions):
+                lut = inv if k & 1 else tl
+                mv = lambda pl, i: int(lut[min(int(pl[i]) if i < len(pl) else 1024, 2047)])
+                S.append(([int(mv(mx, i) / xd) for i in idx], [int(mv(my, i) / yd) for i in idx]))
+            allx = [v for sx, _ in S for v in sx]
+            ally = [v for _, sy in S for v in sy]
+            direct = covers and bx * step + min(allx) >= 0 and by * step + min(ally) >= 0 and \
+                (bx + tw - 1) * step + max(allx) <= maxx and (by + th - 1) * step + max(ally) <= maxy
+            for y in range(th):
+                wy = yw[min(y, 31)]
+
+                def alpha_of(mk, x):
+                    if zero:
+                        return alpha_abs(bx + x, by + y, mk)
+                    c4 = [int(mk[i]) if i < len(mk) else 0 for i in corners]
+                    r = [ip(c4[0], c4[2], BH, ys_, wy), ip(c4[1], c4[3], BH, ys_, wy)]
+                    return byte(ip(r[0], r[1], BW, xs_, xw[min(x, 31)]))
+
+                for x in range(tw):
+                    wx = xw[min(x, 31)]
+                    vals = []
+                    for k, (sx, sy) in enumerate(S):
+                        if interp:
+                            rx = [ip(sx[0], sx[2], BH, ys_, wy), ip(sx[1], sx[3], BH, ys_, wy)]
+                            ry = [ip(sy[0], sy[2], BH, ys_, wy), ip(sy[1], sy[3], BH, ys_, wy)]
+                            dx, dy = ip(rx[0], rx[1], BW, xs_, wx), ip(ry[0], ry[1], BW, xs_, wx)
+                        else:
+                            dx, dy = sx[0], sy[0]
+                        X, Y = (bx + x) * step + dx, (by + y) * step + dy
+                        if not direct:
+                            X, Y = min(max(X, 0), maxx), min(max(Y, 0), maxy)
+                        i = index(k & 1, X, Y)
+                        vals.append(int(srcs[k & 1][i]) if i < len(srcs[k & 1]) else 0)
+                    a, b, c, d = vals
+                    lo, hi = min(a, b), max(a, b)
+                    i0 = b255(a, min(max(d, lo), hi), alpha_of(masks[0], x))
+                    i1 = b255(b, min(max(c, lo), hi), alpha_of(masks[1], x))
+                    m = b256(i0, i1, thr)
+                    if final is not None:
+                        BX, BY = min((bx + x) * step, maxx), min((by + y) * step, maxy)
+                        i, j = index(0, BX, BY), index(1, BX, BY)
+                        ba = int(srcs[0][i]) if i < len(srcs[0]) else 0
+                        bb = int(srcs[1][j]) if j < len(srcs[1]) else 0
+                        m = b255(m, b256(ba, bb, thr), alpha_of(final, x))
+                    dst[by + y, bx + x] = m
+    return dst
+
+
+M23_CASES = [  # w, h, block, step, interp, threshold, final mask
+    (40, 24, 8, 1, True, 128, False),
+    (40, 24, 16, 2, True, 60, True),
+    (36, 22, 8, 1, False, 200, True),
+    (20, 12, 32, 2, False, 0, False),
+]
+
+
+@pytest.mark.parametrize("case", range(len(M23_CASES)))
+def test_oracle_mode23_matches_python_restatement(case):
+    w, h, blk, step, interp, thr, with_final = M23_CASES[case]
+    rng = np.random.default_rng(70 + case)
+    gw, gh = _grid(w, h, blk, blk)
+    cfg = _cfg(w, h, blk, blk, gw, gh, step)
+    motions = [(_motion(rng, gw * gh, 40), _motion(rng, gw * gh, 40)) for _ in range(4)]
+    masks = tuple(rng.integers(0, 256, size=gw * gh, dtype=np.uint8) for _ in range(2))
+    final = rng.integers(0, 256, size=gw * gh, dtype=np.uint8) if with_final else None
+    shift = {1: 0, 2: 1}[step]
+    for chroma in (False, True):
+        pw, ph = (w // 2, h // 2) if chroma else (w, h)
+        strides = [pw + 1, pw + 6]
+        srcs = [rng.integers(0, 256, size=(step * step) * ph * st, dtype=np.uint8) for st in strides]
+        spans = [st * ph if shift else 0 for st in strides]
+        got = orc.render_mode23_plane(cfg, chroma, interp, thr, srcs, strides, spans, shift, motions, masks, final,
+                                      pw, ph)
+        want = _py_mode23(cfg, chroma, interp, thr, srcs, strides, spans, shift, motions, masks, final)
+        assert np.array_equal(got, want), f"chroma {chroma}: {np.argwhere(got != want)[:3]}"
+
+
 DUAL_CASES = [  # w, h, block, step, interp, zero origin, mode, threshold, masks (0 none, 2 a+b, 3 a+b+final)
     (40, 24, 8, 1, True, False, 11, 100, 0),
     (40, 24, 8, 1, True, False, 13, 200, 2),
@@ -574,6 +729,53 @@ def test_render_masked_matches_oracle(case):
                             (md[1][0].data_ptr(), md[1][1].data_ptr()), (mad.data_ptr(), mbd.data_ptr()),
                             mfd.data_ptr() if with_final else 0, [d.data_ptr() for d in dsts],
                             [d.shape[1] for d in dsts])
+    torch.cuda.synchronize()
+    for pl in range(3):
+        got = dsts[pl].cpu().numpy()
+        assert np.array_equal(got, wants[pl]), f"plane {pl}: {np.argwhere(got != wants[pl])[:3]}"
+
+
+M23_GPU_CASES = [  # w, h, block, step, interp, threshold, final mask
+    (1920, 1080, 16, 2, True, 128, True),
+    (1280, 720, 8, 1, True, 77, False),
+    (640, 360, 16, 4, False, 200, True),
+    (20, 12, 32, 1, True, 256, True),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(len(M23_GPU_CASES)))
+def test_render_mode23_matches_oracle(case):
+    import torch
+
+    import svpflow_b200 as sv
+
+    w, h, blk, step, interp, thr, with_final = M23_GPU_CASES[case]
+    rng = np.random.default_rng(400 + case)
+    gw, gh = _grid(w, h, blk, blk)
+    cfg = _cfg(w, h, blk, blk, gw, gh, step)
+    shift = {1: 0, 2: 1, 4: 2}[step]
+    motions = [(_motion(rng, gw * gh, 150), _motion(rng, gw * gh, 150)) for _ in range(4)]
+    ma, mb, mf = (rng.integers(0, 256, size=gw * gh, dtype=np.uint8) for _ in range(3))
+    srcs, wants, dsts = [[], []], [], []
+    for pl in range(3):
+        pw, ph = (w // 2, h // 2) if pl else (w, h)
+        strides = [pw + 2, pw + 9]
+        planes = [rng.integers(0, 256, size=(step * step) * ph * st, dtype=np.uint8) for st in strides]
+        spans = [st * ph if shift else 0 for st in strides]
+        wants.append(orc.render_mode23_plane(cfg, pl > 0, interp, thr, planes, strides, spans, shift, motions, (ma, mb),
+                                             mf if with_final else None, pw, ph))
+        for k in range(2):
+            srcs[k].append((torch.from_numpy(planes[k]).cuda(), strides[k]))
+        dsts.append(torch.full((ph, pw), 7, dtype=torch.uint8, device="cuda"))
+    dev = lambda a: torch.from_numpy(a.astype(np.int16) if a.dtype == np.uint16 else a).cuda()
+    md = [(dev(x), dev(y)) for x, y in motions]
+    mad, mbd, mfd = dev(ma), dev(mb), dev(mf)
+    sv.render_mode23_device(cfg, thr, interp, [t.data_ptr() for t, _ in srcs[0]], [st for _, st in srcs[0]],
+                            [t.numel() for t, _ in srcs[0]], [t.data_ptr() for t, _ in srcs[1]],
+                            [st for _, st in srcs[1]], [t.numel() for t, _ in srcs[1]], shift,
+                            [(x.data_ptr(), y.data_ptr()) for x, y in md], (mad.data_ptr(), mbd.data_ptr()),
+                            mfd.data_ptr() if with_final else 0, [d.data_ptr() for d in dsts], [d.shape[1] for d in dsts])
     torch.cuda.synchronize()
     for pl in range(3):
         got = dsts[pl].cpu().numpy()
