@@ -88,6 +88,20 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def _chain(an, nf: int, a_ms: float) -> dict:
+    """The non-roofline bound: every pair of a launch runs concurrently (one CTA each), so the launch
+    lasts about one pair's serial block chain; per level-0 block of one direction."""
+    vd = an.vector_header()
+    sms = _sm_count()
+    waves = -(-nf // (3 * sms)) if nf > 2 * sms else 1  # 3-CTA shape above 2 pairs per SM, else one wave
+    l0 = vd[11] * vd[12]
+    return {"pairs_in_flight": min(nf, 3 * sms if nf > 2 * sms else nf), "waves": waves,
+            "pair_latency_ms": a_ms / waves, "level0_blocks_per_direction": l0,
+            "us_per_level0_block": a_ms / waves * 1000.0 / max(l0, 1),
+            "note": "blocks of a level run in the reference's serial order (each reads its processed "
+                    "neighbours); the time per block, not issue or memory throughput, bounds one pair"}
+
+
 def _config(nframes: int, world: int) -> dict:
     c = CONFIGS[WORKLOAD]
     return {
@@ -1018,6 +1032,7 @@ def main():
             "roofline": roof,
             "cpu_baseline": cpu,
             "parity_vs_oracle": parity,
+            "serial_chain": _chain(an, nf, a_ms),
             "super_ms_per_step": statistics.mean(super_ms), "analyse_ms_per_step": statistics.mean(analyse_ms),
         }
         print(json.dumps(line), flush=True)
