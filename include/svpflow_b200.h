@@ -169,7 +169,9 @@ typedef struct {
  * mode1_pixel(undisplaced, displaced, alpha) with alpha interpolated from the mask (:1818-1820).
  * src_shift 0: src[] are plain planes (stride bytes per row); log2(source_step): src[] are a
  * super clip's level-0 planes whose sub-planes lie stride x plane-height bytes apart (svpflow2
- * core.rs:3340-3388). Device pointers; asynchronous on `stream`. */
+ * core.rs:3340-3388); src_len bounds every read. dst[p] must hold the plane's rows (height, or
+ * height / 2 for chroma) of dst_stride[p] >= width bytes; motion (and mask) planes hold grid_w x
+ * grid_h entries. Device pointers; asynchronous on `stream`. */
 int svpf_render_warp_device(const svpf_render_config *cfg, int32_t threshold, int32_t mode1, int32_t interp,
                             const uint8_t *const src[3], const int64_t src_stride[3], const int64_t src_len[3],
                             int32_t src_shift, const uint16_t *motion_x, const uint16_t *motion_y,
