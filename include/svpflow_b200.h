@@ -147,6 +147,25 @@ int svpf_vector_grid(const int32_t *vdata, int32_t *motion_w, int32_t *motion_h)
 int svpf_vector_planes_device(const int32_t *vdata, const uint8_t *payloads_dev, size_t payload_len, int32_t npayloads,
                               int32_t frame_w, int32_t frame_h, int32_t raw, uint16_t *planes_dev, int32_t *status_dev,
                               void *stream);
+/* SmoothFps' mask planes for the frame it interpolates at `phase` (0..256) between a payload's two
+ * frames (svpflow2 core.rs:1154-1195, :1467-1499, :1605-1616): per payload five byte planes of
+ * motion_w x motion_h, cover0 | cover1 | area0 | area1 | area_max. cover0 / cover1 = coverage_mask
+ * (crates/svpflow-core/src/renderer.rs:1738-1763) of the current set at 256 - phase and of the
+ * previous set at phase, `cover_percent` strong (the mask.cover option); area0 / area1 =
+ * magnitude_mask (:1647-1678) of the previous / current set with area_scale and area_sharp (the
+ * mask.area options); area_max = max_mask (:2908-2915) of the two. cover0, cover1 are the masks
+ * svpf_render_masked_device / svpf_render_mode23_device take and area_max their final mask; area0,
+ * area1 are the masks of svpf_render_blend_device, and area0 (algorithm 1) or area1 (algorithm 2)
+ * the mask of svpf_render_warp_device. scratch_dev holds svpf_render_masks_scratch bytes.
+ * Payloads (payload_len a multiple of 4) and scratch are 4-byte aligned; the overlap lies in
+ * 0..block - 1 and grid_w * grid_h * block area <= 2^30 (every Analyse field). status_dev[i] = 1
+ * where payload i does not decode (its planes are left as they were). Bytes equal the reference's,
+ * except that area_sharp != 1 goes through CUDA's pow (2 ulp), which can move a byte by one where
+ * 255 * value lies within a few ulp of an integer. Asynchronous on `stream`. */
+int64_t svpf_render_masks_scratch(const int32_t *vdata, int32_t npayloads);
+int svpf_render_masks_device(const int32_t *vdata, const uint8_t *payloads_dev, size_t payload_len, int32_t npayloads,
+                             int32_t phase, int32_t cover_percent, double area_scale, double area_sharp,
+                             uint8_t *masks_dev, void *scratch_dev, int32_t *status_dev, void *stream);
 
 /* ---------------------------------------------------------------- frame render (SmoothFps) */
 /* renderer.rs CpuConfig (crates/svpflow-core/src/renderer.rs:34-46) as SmoothFps fills it

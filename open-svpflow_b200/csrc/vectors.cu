@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "../../include/svpflow_b200.h"
 #include "handles.h"
 
@@ -109,6 +111,163 @@ __global__ void vector_planes_kernel(const PlaneJob J) {
     }
 }
 
+// ---------------------------------------------------------------- mask planes
+// SmoothFps' masks for one interpolated frame (svpflow2 core.rs:1154-1195, :1467-1499, :1605-1616):
+// renderer.rs coverage_mask (:1738-1763) = splat_coverage (:2945-3062) + window_3x3 (:3064-3100) +
+// finish_coverage (:3102-3134), and magnitude_mask (:1647-1678) with scale_magnitude (:3245-3260).
+// The splat's weights are >= 0 when 0 <= overlap < block, so every partial sum is bounded by
+// grid_w * grid_h * block area; the host admits only fields where that is <= INT32_MAX, which makes
+// the reference's saturating and wrapping adds plain adds and the atomic sums order-independent.
+// TruncDiv (:3149-3184) divides exactly (truncating), so plain '/' restates it.
+
+struct MaskJob {
+    const uint8_t *payloads;
+    int64_t payload_len;
+    uint8_t *masks;       // per payload: cover0 | cover1 | area0 | area1 | max(area0, area1), each mw x mh
+    int32_t *sums;        // per payload: two (mw + 2) x (mh + 2) splat planes
+    int *status;
+    int32_t flags, gw, gh, mw, mh;
+    int32_t bw, bh, xs, ys, denom, phase, area, sharp_is_one;
+    double strength, area_scale, area_sharp;
+};
+
+__device__ __forceinline__ bool mask_regions(const MaskJob &J, const uint8_t *p, int64_t &off_prev,
+                                             int64_t &off_cur) {
+    const int64_t count = (int64_t)J.gw * J.gh;
+    const int64_t first = 0x40, second = first + 4 + count * 8;
+    bool ok = true;
+    const bool hdr = rd32(p, J.payload_len, 0, ok) == 16 && rd32(p, J.payload_len, 4, ok) == 0xA0 &&
+                     rd32(p, J.payload_len, 8, ok) == J.flags;
+    const int marker = (int)(2 * count + 1);
+    const bool has_prev = (J.flags & 1) != 0, has_cur = (J.flags & 2) != 0;
+    if (has_prev && rd32(p, J.payload_len, first, ok) != marker) ok = false;
+    if (has_cur && rd32(p, J.payload_len, second, ok) != marker) ok = false;
+    if (has_prev && first + 4 + count * 8 > J.payload_len) ok = false;
+    if (has_cur && second + 4 + count * 8 > J.payload_len) ok = false;
+    off_prev = has_prev ? first + 4 : second + 4;  // previous falls back to current
+    off_cur = has_cur ? second + 4 : first + 4;    // and current to previous
+    return ok && hdr && (has_prev || has_cur);
+}
+
+// grid: (vectors / 256, payloads, 2). z = 0: mask 0 splats the current set at 256 - phase;
+// z = 1: mask 1 splats the previous set at phase (coverage_mask's opposite_set).
+__global__ void mask_splat_kernel(const MaskJob J) {
+    const int64_t f = blockIdx.y;
+    const int which = blockIdx.z;
+    const uint8_t *p = J.payloads + f * J.payload_len;
+    int64_t off_prev, off_cur;
+    if (!mask_regions(J, p, off_prev, off_cur)) return;
+    const int64_t count = (int64_t)J.gw * J.gh;
+    const int64_t stride = (int64_t)J.mw + 2;
+    int32_t *acc = J.sums + (f * 2 + which) * stride * ((int64_t)J.mh + 2);
+    const int64_t off = which ? off_prev : off_cur;
+    const int t = which ? J.phase : 256 - J.phase;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < count; k += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(k % J.gw), y = (int)(k / J.gw);
+        const unsigned raw0 = *reinterpret_cast<const unsigned *>(p + off + k * 8);
+        const int vdx = (int)(short)(raw0 >> 16), vdy = (int)(short)(raw0 & 0xFFFF);
+        const int sx = x * J.xs + (t * vdx) / J.denom;
+        const int sy = y * J.ys + (t * vdy) / J.denom;
+        // floor division (the reference biases negative numerators by 1 - step)
+        const int left = (sx + ((1 - J.xs) & (sx >> 31))) / J.xs;
+        const int top = (sy + ((1 - J.ys) & (sy >> 31))) / J.ys;
+        const int right = left + 1, bottom = top + 1;
+        const int next_x = right * J.xs;
+        const int lw = next_x - sx, tw = J.ys * bottom - sy, rw = sx + J.bw - next_x, bwt = J.bh - tw;
+        // the interior path and add_point's four conditions both reduce to: corners inside mw x mh
+        const bool l_in = left >= 0 && left < J.mw, r_in = right >= 0 && right < J.mw;
+        const bool t_in = top >= 0 && top < J.mh, b_in = bottom >= 0 && bottom < J.mh;
+        if (t_in && l_in) atomicAdd(acc + (int64_t)top * stride + left, lw * tw);
+        if (t_in && r_in) atomicAdd(acc + (int64_t)top * stride + right, tw * rw);
+        if (b_in && r_in) atomicAdd(acc + (int64_t)bottom * stride + right, rw * bwt);
+        if (b_in && l_in) atomicAdd(acc + (int64_t)bottom * stride + left, lw * bwt);
+    }
+}
+
+__device__ __forceinline__ uint8_t coverage_byte(double v) {
+    if (!isfinite(v)) return 0;
+    const int i = __double2int_rz(v);  // saturating, as Rust's `as i32`
+    return i >= 255 ? 255 : (uint8_t)(i & 0xFF);
+}
+__device__ __forceinline__ uint8_t clamp_u8(double v) {
+    if (!isfinite(v) || v <= 0.0) return 0;
+    if (v >= 255.0) return 255;
+    return (uint8_t)__double2int_rz(v);
+}
+
+// grid: (points / 256, payloads): window_3x3 + finish_coverage for both masks, and both magnitude masks.
+__global__ void mask_finish_kernel(const MaskJob J) {
+    const int64_t f = blockIdx.y;
+    const uint8_t *p = J.payloads + f * J.payload_len;
+    int64_t off_prev, off_cur;
+    if (!mask_regions(J, p, off_prev, off_cur)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) J.status[f] = 1;
+        return;
+    }
+    const int64_t n = (int64_t)J.mw * J.mh;
+    const int64_t stride = (int64_t)J.mw + 2, plane = stride * ((int64_t)J.mh + 2);
+    const int32_t *acc = J.sums + f * 2 * plane;
+    uint8_t *out = J.masks + f * 5 * n;
+    const double area_f = (double)J.area;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % J.mw), y = (int)(i / J.mw);
+        const int x0 = x > 0 ? x - 1 : 0, y0 = y > 0 ? y - 1 : 0;
+        for (int m = 0; m < 2; m++) {
+            int s = 0;  // the 3x3 window around (x, y); rows / columns past the plane hold 0
+            for (int yy = y0; yy <= y + 1; yy++)
+                for (int xx = x0; xx <= x + 1; xx++) s += __ldg(acc + m * plane + (int64_t)yy * stride + xx);
+            const int covered = s >> 3;
+            const int remaining = J.area <= covered ? 0 : J.area - covered;
+            out[m * n + i] = coverage_byte(__ddiv_rn(__dmul_rn(__dmul_rn((double)remaining, J.strength), 256.0), area_f));
+        }
+        // magnitude_mask's fill: columns past the grid repeat the row's last vector, rows past it
+        // repeat the grid's bottom-left one
+        int64_t si = -1;
+        if (J.gw > 0 && J.gh > 0) si = y < J.gh ? (int64_t)y * J.gw + (x < J.gw ? x : J.gw - 1) : (int64_t)(J.gh - 1) * J.gw;
+        uint8_t a[2] = {0, 0};
+        if (si >= 0)
+            for (int s = 0; s < 2; s++) {
+                const unsigned raw1 = *reinterpret_cast<const unsigned *>(p + (s ? off_cur : off_prev) + si * 8 + 4);
+                double v = __ddiv_rn(__dmul_rn(__dmul_rn(4.0, (double)(raw1 & 0xFFFFFFu)), J.area_scale), area_f);
+                if (!J.sharp_is_one) v = pow(v, J.area_sharp);
+                a[s] = clamp_u8(__dmul_rn(v, 255.0));
+            }
+        out[2 * n + i] = a[0];
+        out[3 * n + i] = a[1];
+        out[4 * n + i] = a[0] > a[1] ? a[0] : a[1];
+    }
+}
+
+bool mask_job(const int32_t *vdata, MaskJob &J, std::string &err) {
+    VecHdr h;
+    if (!read_vdata(vdata, h)) {
+        err = "not a vector header";
+        return false;
+    }
+    J.flags = h.flags;
+    J.gw = h.gw > 0 ? h.gw : 0;
+    J.gh = h.gh > 0 ? h.gh : 0;
+    J.mw = extended_grid(h.bw, h.ox, h.gw, h.w);
+    J.mh = extended_grid(h.bh, h.oy, h.gh, h.h);
+    if (J.mw < 0) J.mw = 0;
+    if (J.mh < 0) J.mh = 0;
+    J.bw = h.bw > 1 ? h.bw : 1;
+    J.bh = h.bh > 1 ? h.bh : 1;
+    if (h.ox < 0 || h.oy < 0 || h.ox >= J.bw || h.oy >= J.bh) {
+        err = "overlap outside 0..block - 1";
+        return false;
+    }
+    if ((int64_t)J.gw * J.gh * J.bw * J.bh > INT32_MAX / 2 || (int64_t)(J.mw + 2) * (J.mh + 2) > INT32_MAX) {
+        err = "vector field too large for 32-bit coverage sums";
+        return false;
+    }
+    J.xs = J.bw - h.ox;
+    J.ys = J.bh - h.oy;
+    J.denom = (int32_t)((uint32_t)(h.marker > 1 ? h.marker : 1) << 8);
+    J.area = (int64_t)J.bw * J.bh > INT32_MAX ? INT32_MAX : J.bw * J.bh;
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -134,8 +293,12 @@ int svpf_vector_planes_device(const int32_t *vdata, const uint8_t *payloads_dev,
         return SVPF_EINVAL;
     }
     if (npayloads <= 0) return SVPF_OK;
-    if (!payloads_dev || !planes_dev || !status_dev || payload_len < 0x40) {
+    if (!payloads_dev || !planes_dev || !status_dev || payload_len < 0x40 || npayloads > 65535) {
         svpf::set_last_error("bad buffers");
+        return SVPF_EINVAL;
+    }
+    if ((payload_len & 3) || ((uintptr_t)payloads_dev & 3) || ((uintptr_t)planes_dev & 1)) {
+        svpf::set_last_error("payloads must be 4-byte aligned");
         return SVPF_EINVAL;
     }
     PlaneJob J;
@@ -168,6 +331,74 @@ int svpf_vector_planes_device(const int32_t *vdata, const uint8_t *payloads_dev,
     }
     if (e != cudaSuccess) {
         svpf::set_last_error(std::string("vector planes: ") + cudaGetErrorString(e));
+        return SVPF_ECUDA;
+    }
+    return SVPF_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int64_t svpf_render_masks_scratch(const int32_t *vdata, int32_t npayloads) {
+    MaskJob J;
+    std::string err;
+    if (npayloads < 0 || !mask_job(vdata, J, err)) return -1;
+    return (int64_t)npayloads * 2 * ((int64_t)J.mw + 2) * ((int64_t)J.mh + 2) * (int64_t)sizeof(int32_t);
+}
+
+int svpf_render_masks_device(const int32_t *vdata, const uint8_t *payloads_dev, size_t payload_len, int32_t npayloads,
+                             int32_t phase, int32_t cover_percent, double area_scale, double area_sharp,
+                             uint8_t *masks_dev, void *scratch_dev, int32_t *status_dev, void *stream) {
+    if (int rc = svpf::require_device()) return rc;
+    MaskJob J;
+    std::string err;
+    if (!mask_job(vdata, J, err)) {
+        svpf::set_last_error(err);
+        return SVPF_EINVAL;
+    }
+    if (phase < 0 || phase > 256 || cover_percent < 0) {
+        svpf::set_last_error("phase must be in 0..256 and cover >= 0");
+        return SVPF_EINVAL;
+    }
+    if (npayloads <= 0) return SVPF_OK;
+    if (!payloads_dev || !masks_dev || !scratch_dev || !status_dev || payload_len < 0x40 || npayloads > 65535) {
+        svpf::set_last_error("bad buffers");
+        return SVPF_EINVAL;
+    }
+    if ((payload_len & 3) || ((uintptr_t)payloads_dev & 3) || ((uintptr_t)scratch_dev & 3)) {
+        svpf::set_last_error("payloads and scratch must be 4-byte aligned");
+        return SVPF_EINVAL;
+    }
+    J.payloads = payloads_dev;
+    J.payload_len = (int64_t)payload_len;
+    J.masks = masks_dev;
+    J.sums = static_cast<int32_t *>(scratch_dev);
+    J.status = status_dev;
+    J.phase = phase;
+    J.strength = (double)cover_percent / 100.0;
+    J.area_scale = area_scale;
+    J.area_sharp = area_sharp;
+    J.sharp_is_one = area_sharp == 1.0;  // pow(x, 1) is x exactly, in libm and here
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t n = (int64_t)J.mw * J.mh, count = (int64_t)J.gw * J.gh;
+    const size_t sums = (size_t)npayloads * 2 * ((size_t)J.mw + 2) * ((size_t)J.mh + 2) * sizeof(int32_t);
+    cudaError_t e = cudaMemsetAsync(status_dev, 0, sizeof(int32_t) * (size_t)npayloads, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(scratch_dev, 0, sums, st);
+    if (e == cudaSuccess && count > 0 && n > 0 && J.denom != 0) {  // splat_coverage returns early on denom 0
+        dim3 grid((unsigned)((count + 255) / 256 < 65535 ? (count + 255) / 256 : 65535), (unsigned)npayloads, 2);
+        mask_splat_kernel<<<grid, 256, 0, st>>>(J);
+        svpf::add_launches(1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && n > 0) {
+        dim3 grid((unsigned)((n + 255) / 256 < 65535 ? (n + 255) / 256 : 65535), (unsigned)npayloads);
+        mask_finish_kernel<<<grid, 256, 0, st>>>(J);
+        svpf::add_launches(1);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        svpf::set_last_error(std::string("mask planes: ") + cudaGetErrorString(e));
         return SVPF_ECUDA;
     }
     return SVPF_OK;

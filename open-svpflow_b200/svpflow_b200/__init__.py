@@ -107,6 +107,9 @@ def lib() -> ctypes.CDLL:
             "svpf_server_stats": (None, [_VP, P(I64), P(I64), P(I64), P(I32), P(I64)]),
             "svpf_vector_grid": (I32, [P(I32), P(I32), P(I32)]),
             "svpf_vector_planes_device": (I32, [P(I32), _VP, SZ, I32, I32, I32, I32, _VP, _VP, _VP]),
+            "svpf_render_masks_scratch": (I64, [P(I32), I32]),
+            "svpf_render_masks_device": (I32, [P(I32), _VP, SZ, I32, I32, I32, ctypes.c_double, ctypes.c_double,
+                                               _VP, _VP, _VP, _VP]),
             "svpf_render_warp_device": (I32, [P(RenderConfig), I32, I32, I32, P(_VP), P(I64), P(I64), I32, _VP, _VP,
                                               _VP, P(_VP), P(I64), _VP]),
             "svpf_render_blend_device": (I32, [P(RenderConfig), I32, I32, I32, I32, P(_VP), P(I64), P(I64), P(_VP),
@@ -494,6 +497,26 @@ def vector_planes_device(vdata, payloads_ptr: int, payload_len: int, npayloads: 
     v = (ctypes.c_int32 * 16)(*vdata)
     _check(lib().svpf_vector_planes_device(v, payloads_ptr, payload_len, npayloads, frame_w, frame_h, int(raw),
                                            planes_ptr, status_ptr, stream))
+
+
+def render_masks_scratch(vdata, npayloads: int) -> int:
+    """Bytes of device scratch render_masks_device needs for `npayloads` payloads."""
+    v = (ctypes.c_int32 * 16)(*vdata)
+    n = lib().svpf_render_masks_scratch(v, int(npayloads))
+    if n < 0:
+        raise ValueError("not a vector header the mask planes take")
+    return n
+
+
+def render_masks_device(vdata, payloads_ptr: int, payload_len: int, npayloads: int, phase: int, masks_ptr: int,
+                        scratch_ptr: int, status_ptr: int, cover: int = 100, area_scale: float = 1.0,
+                        area_sharp: float = 1.0, stream: int = 0):
+    """SmoothFps's mask planes (cover0 | cover1 | area0 | area1 | area_max per payload, motion-grid
+    sized bytes) for the frame at `phase` on device buffers; see svpf_render_masks_device."""
+    v = (ctypes.c_int32 * 16)(*vdata)
+    _check(lib().svpf_render_masks_device(v, payloads_ptr, payload_len, npayloads, int(phase), int(cover),
+                                          float(area_scale), float(area_sharp), masks_ptr, scratch_ptr, status_ptr,
+                                          stream))
 
 
 def render_warp_device(cfg: dict, threshold: int, mode1: bool, interp: bool, src_ptrs, src_strides, src_lens,

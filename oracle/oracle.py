@@ -444,6 +444,8 @@ def _setup(L):
     L.or_vector_grid.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.or_vector_planes.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32,
                                    ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
+    L.or_render_masks.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, ctypes.c_int32,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
     L.or_hadamard4_satd.argtypes = [P(ctypes.c_int32)]
     L.or_adapt_lambda.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
     L.or_exact_lambda.argtypes = [P(AnalyseOpts), ctypes.c_int32, ctypes.c_int32]
@@ -705,6 +707,19 @@ def vector_planes(vdata, payload: np.ndarray, frame_w: int, frame_h: int, raw: b
     v = (ctypes.c_int32 * 16)(*vdata)
     rc = lib().or_vector_planes(v, _ptr(payload), payload.size, frame_w, frame_h, int(raw), out.ctypes.data)
     return None if rc else out.reshape(4, mh, mw)
+
+
+def render_masks(vdata, payload: np.ndarray, phase: int, cover: int = 100, area_scale: float = 1.0,
+                 area_sharp: float = 1.0):
+    """SmoothFps' mask planes for one payload at `phase` -> uint8 [5, mh, mw] = cover0, cover1, area0,
+    area1, max(area0, area1); None when the payload does not decode."""
+    mw, mh = vector_grid(vdata)
+    out = np.zeros(5 * max(mw, 0) * max(mh, 0), dtype=np.uint8)
+    payload = np.ascontiguousarray(payload, dtype=np.uint8)
+    v = (ctypes.c_int32 * 16)(*vdata)
+    rc = lib().or_render_masks(v, _ptr(payload), payload.size, int(phase), int(cover), float(area_scale),
+                               float(area_sharp), out.ctypes.data)
+    return None if rc else out.reshape(5, mh, mw)
 
 
 # ---- 10-bit extension (uint16 samples), same options as the 8-bit path

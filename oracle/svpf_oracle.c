@@ -1834,7 +1834,9 @@ static int rd_i32(const uint8_t *p, size_t len, size_t off, int32_t *v) { /* rea
     return 1;
 }
 /* decode_region (:455-481): 0 when the region does not decode */
-static int decode_region(const uint8_t *p, size_t len, size_t off, size_t count, int16_t *dx, int16_t *dy) {
+/* score: NULL, or the vectors' 24-bit scores (DecodedVector::score) */
+static int decode_region(const uint8_t *p, size_t len, size_t off, size_t count, int16_t *dx, int16_t *dy,
+                         uint32_t *score) {
     int32_t m;
     if (!rd_i32(p, len, off, &m) || (i64)m != (i64)(2 * count + 1)) return 0;
     for (size_t i = 0; i < count; i++) {
@@ -1843,6 +1845,7 @@ static int decode_region(const uint8_t *p, size_t len, size_t off, size_t count,
         uint32_t rot = ((uint32_t)r0 >> 16) | ((uint32_t)r0 << 16); /* rotate_right(16) */
         dx[i] = (int16_t)(rot & 0xFFFF);
         dy[i] = (int16_t)(rot >> 16);
+        if (score) score[i] = (uint32_t)r1 & 0x00FFFFFFu;
     }
     return 1;
 }
@@ -1864,8 +1867,8 @@ int or_vector_planes(const int32_t vdata[16], const uint8_t *p, size_t len, int3
     size_t count = (size_t)gw * (size_t)gh, first = 0x40, second = first + 4 + count * 8;
     int16_t *pvx = calloc(count + 1, 2), *pvy = calloc(count + 1, 2), *cx = calloc(count + 1, 2),
             *cy = calloc(count + 1, 2);
-    int okp = (flags & 1) ? decode_region(p, len, first, count, pvx, pvy) : 0;
-    int okc = (flags & 2) ? decode_region(p, len, second, count, cx, cy) : 0;
+    int okp = (flags & 1) ? decode_region(p, len, first, count, pvx, pvy, NULL) : 0;
+    int okc = (flags & 2) ? decode_region(p, len, second, count, cx, cy, NULL) : 0;
     int rc = 0;
     if (((flags & 1) && !okp) || ((flags & 2) && !okc) || (!okp && !okc)) rc = -1;
     else {
@@ -1895,6 +1898,157 @@ int or_vector_planes(const int32_t vdata[16], const uint8_t *p, size_t len, int3
             }
     }
     free(pvx); free(pvy); free(cx); free(cy);
+    return rc;
+}
+
+/* ------------------------------------------------------------------ SmoothFps mask planes */
+/* The masks SmoothFps derives from one payload's vectors (svpflow2 core.rs:1154-1195 magnitude,
+ * :1467-1499 coverage, :1605-1616 max_mask), for the VectorContext it builds there: block
+ * max(bw, 1) x max(bh, 1), origin = the overlap, scale base = max(marker, 1), the payload's grid,
+ * planes of the motion grid's size. Restated from renderer.rs: magnitude_mask (:1647-1678),
+ * coverage_mask (:1738-1763), splat_coverage (:2945-3062), window_3x3 (:3064-3100),
+ * finish_coverage (:3102-3134), add_point (:3136-3147), TruncDiv (:3149-3184), scale_magnitude /
+ * clamp_u8 (:3245-3260), coverage_byte (:3262-3273), max_mask (:2908-2915).
+ * TruncDiv::div(v) = v / d truncated for every v: for d > 0 and |v| < 2^40 / d the magic product
+ * (|v| * ceil(2^40 / d)) >> 40 overshoots |v| / d by |v| * e / (d * 2^40) with e < d, less than 1 / d,
+ * so the floor is the exact quotient; elsewhere it divides. */
+typedef struct { i32 bw, bh, base, ox, oy, gw, gh; } or_mctx;
+static i32 m_div(i32 v, i32 d) { return d == 0 ? 0 : (d == -1 ? (i32)(0u - (u32)v) : v / d); }
+static void m_add_point(i32 *acc, usize len, i32 width, i32 x, i32 y, i32 w) {
+    if (x < 0 || y < 0) return;
+    usize i = sat_add_us(sat_mul_us((usize)y, (usize)width + 2), (usize)x);
+    if (i < len) acc[i] = sat_add_i32(acc[i], w);
+}
+static void m_splat(const or_mctx *c, const int16_t *vdx, const int16_t *vdy, i32 *acc, usize len, i32 w, i32 h,
+                    i32 threshold) {
+    if (c->gw <= 0 || c->gh <= 0 || w <= 0 || h <= 0) return;
+    i32 xs = sat_i64_to_i32((i64)c->bw - c->ox), ys = sat_i64_to_i32((i64)c->bh - c->oy);
+    i32 denom = (i32)((u32)c->base << 8);
+    if (xs == 0 || ys == 0 || denom == 0) return;
+    i32 xb = sat_i64_to_i32((i64)1 - xs), yb = sat_i64_to_i32((i64)1 - ys);
+    usize stride = (usize)w + 2;
+    for (i32 y = 0; y < c->gh; y++) {
+        i32 x_base = 0;
+        for (i32 x = 0; x < c->gw; x++) {
+            usize k = (usize)y * (usize)c->gw + (usize)x;
+            i32 dx = m_div((i32)((u32)threshold * (u32)(i32)vdx[k]), denom);
+            i32 dy = m_div((i32)((u32)threshold * (u32)(i32)vdy[k]), denom);
+            i32 sx = sat_add_i32(x_base, dx), sy = sat_add_i32(sat_mul_i32(ys, y), dy);
+            i32 left = m_div(sx + (xb & (sx >> 31)), xs), top = m_div(sy + (yb & (sy >> 31)), ys);
+            i32 right = left + 1, bottom = top + 1;
+            i32 next_x = sat_mul_i32(right, xs);
+            i32 lw = next_x - sx, tw = sat_mul_i32(ys, bottom) - sy, rw = sx + c->bw - next_x, bw = c->bh - tw;
+            int interior = left >= 0 && right < w && top >= 0 && bottom < h;
+            usize base = interior ? sat_add_us(sat_mul_us((usize)top, stride), (usize)left) : 0;
+            if (interior && sat_add_us(sat_add_us(base, stride), 2) <= len) {
+                acc[base] += lw * tw;
+                acc[base + 1] += tw * rw;
+                acc[base + stride] += lw * bw;
+                acc[base + stride + 1] += rw * bw;
+            } else {
+                if (top >= 0 && top < h && left >= 0 && left < w) m_add_point(acc, len, w, left, top, sat_mul_i32(lw, tw));
+                if (left >= -1 && top >= 0 && top < h && right < w) m_add_point(acc, len, w, right, top, sat_mul_i32(tw, rw));
+                if (top >= -1 && bottom < h && left >= -1 && right < w)
+                    m_add_point(acc, len, w, right, bottom, sat_mul_i32(rw, bw));
+                if (left >= 0 && top >= -1 && bottom < h && left < w)
+                    m_add_point(acc, len, w, left, bottom, sat_mul_i32(lw, bw));
+            }
+            x_base = sat_add_i32(x_base, xs);
+        }
+    }
+}
+static void m_window3x3(const i32 *pt, i32 *sums, usize stride, usize len) {
+    usize rows = len / stride;
+    for (usize r = 0; r < rows; r++) {
+        const i32 *s = pt + r * stride;
+        i32 *o = sums + r * stride;
+        o[0] = s[0];
+        o[1] = s[1] + s[0];
+        for (usize x = 2; x < stride; x++) o[x] = s[x] + s[x - 1] + s[x - 2];
+    }
+    for (usize y = rows; y-- > 1;) {
+        i32 *cur = sums + y * stride;
+        const i32 *r1 = sums + (y - 1) * stride, *r2 = y >= 2 ? sums + (y - 2) * stride : NULL;
+        for (usize x = 0; x < stride; x++) cur[x] += r1[x] + (r2 ? r2[x] : 0);
+    }
+}
+static uint8_t m_coverage_byte(double v) {
+    if (!isfinite(v)) return 0;
+    i32 i = f64_as_i32(v);
+    return i >= 255 ? 255 : (uint8_t)(i & 0xFF);
+}
+static uint8_t m_clamp_u8(double v) {
+    if (!isfinite(v) || v <= 0.0) return 0;
+    if (v >= 255.0) return 255;
+    return (uint8_t)v;
+}
+static void m_coverage(const or_mctx *c, const int16_t *vdx, const int16_t *vdy, uint8_t *out, i32 w, i32 h,
+                       i32 strength_percent, i32 threshold) {
+    usize stride = (usize)w + 2, len = stride * ((usize)h + 2);
+    i32 *pt = calloc(len + 1, sizeof(i32)), *sums = calloc(len + 1, sizeof(i32));
+    m_splat(c, vdx, vdy, pt, len, w, h, threshold);
+    m_window3x3(pt, sums, stride, len);
+    i32 area = imax(sat_mul_i32(c->bw, c->bh), 1);
+    double strength = (double)strength_percent / 100.0, area_f = (double)area;
+    for (i32 y = 0; y < h; y++)
+        for (i32 x = 0; x < w; x++) {
+            i32 covered = sums[(usize)(y + 1) * stride + (usize)x + 1] >> 3;
+            i32 remaining = area <= covered ? 0 : area - covered;
+            out[(usize)y * (usize)w + (usize)x] = m_coverage_byte((double)remaining * strength * 256.0 / area_f);
+        }
+    free(pt);
+    free(sums);
+}
+static void m_magnitude(const or_mctx *c, const uint32_t *score, uint8_t *out, i32 w, i32 h, double scale,
+                        double exponent) {
+    i32 area = imax(sat_mul_i32(c->bw, c->bh), 1);
+    for (i32 y = 0; y < h; y++)
+        for (i32 x = 0; x < w; x++) {
+            usize i = (usize)y * (usize)w + (usize)x;
+            if (x < c->gw && y < c->gh)
+                out[i] = m_clamp_u8(pow(4.0 * (double)score[(usize)y * (usize)c->gw + (usize)x] * scale / (double)area,
+                                        exponent) * 255.0);
+            else if (x > 0) out[i] = out[i - 1];
+            else if (y > 0) out[i] = out[i - (usize)w];
+            else out[i] = 0;
+        }
+}
+int or_render_masks(const int32_t vdata[16], const uint8_t *p, size_t len, int32_t phase, int32_t cover,
+                    double area_scale, double area_sharp, uint8_t *out) {
+    int32_t flags = vdata[1], gw = imax(vdata[11], 0), gh = imax(vdata[12], 0), v;
+    if (vdata[0] != 0xA0) return -1;
+    if (!rd_i32(p, len, 0, &v) || v != 16 || !rd_i32(p, len, 4, &v) || v != 0xA0 || !rd_i32(p, len, 8, &v) ||
+        v != flags)
+        return -1;
+    size_t count = (size_t)gw * (size_t)gh, first = 0x40, second = first + 4 + count * 8;
+    int16_t *vx[2], *vy[2];
+    uint32_t *sc[2];
+    int ok[2];
+    for (int s = 0; s < 2; s++) {
+        vx[s] = calloc(count + 1, 2); vy[s] = calloc(count + 1, 2); sc[s] = calloc(count + 1, 4);
+    }
+    ok[0] = (flags & 1) ? decode_region(p, len, first, count, vx[0], vy[0], sc[0]) : 0;
+    ok[1] = (flags & 2) ? decode_region(p, len, second, count, vx[1], vy[1], sc[1]) : 0;
+    int rc = 0;
+    if (((flags & 1) && !ok[0]) || ((flags & 2) && !ok[1]) || (!ok[0] && !ok[1])) rc = -1;
+    else {
+        for (int s = 0; s < 2; s++)
+            if (!ok[s]) { /* previous falls back to current and vice versa */
+                memcpy(vx[s], vx[1 - s], count * 2); memcpy(vy[s], vy[1 - s], count * 2); memcpy(sc[s], sc[1 - s], count * 4);
+            }
+        int32_t mw, mh;
+        or_vector_grid(vdata, &mw, &mh);
+        mw = imax(mw, 0); mh = imax(mh, 0);
+        or_mctx c = {imax(vdata[2], 1), imax(vdata[3], 1), imax(vdata[4], 1), vdata[9], vdata[10], gw, gh};
+        size_t n = (size_t)mw * (size_t)mh;
+        /* coverage of mask 0 splats the current set at 256 - phase, mask 1 the previous set at phase */
+        m_coverage(&c, vx[1], vy[1], out, mw, mh, cover, 256 - phase);
+        m_coverage(&c, vx[0], vy[0], out + n, mw, mh, cover, phase);
+        m_magnitude(&c, sc[0], out + 2 * n, mw, mh, area_scale, area_sharp);
+        m_magnitude(&c, sc[1], out + 3 * n, mw, mh, area_scale, area_sharp);
+        for (size_t i = 0; i < n; i++) out[4 * n + i] = out[2 * n + i] > out[3 * n + i] ? out[2 * n + i] : out[3 * n + i];
+    }
+    for (int s = 0; s < 2; s++) { free(vx[s]); free(vy[s]); free(sc[s]); }
     return rc;
 }
 

@@ -211,6 +211,11 @@ void or_render_mode23_plane(const or_render_config *c, int32_t chroma, int32_t i
 int32_t or_render_threshold_limit(int32_t threshold, double scale);
 int or_vector_planes(const int32_t vdata[16], const uint8_t *payload, size_t len, int32_t frame_w, int32_t frame_h,
                      int32_t raw, uint16_t *out);
+/* SmoothFps' mask planes for one payload at `phase` (0..256): out = cover0 | cover1 | area0 | area1 |
+ * max(area0, area1), mw x mh bytes each (coverage_mask at 256 - phase / phase with `cover` percent,
+ * magnitude_mask with area_scale, area_sharp); -1 when the payload does not decode. */
+int or_render_masks(const int32_t vdata[16], const uint8_t *payload, size_t len, int32_t phase, int32_t cover,
+                    double area_scale, double area_sharp, uint8_t *out);
 
 /* ---- primitives exposed for known-answer tests ---- */
 uint32_t or_hadamard4_satd(const int32_t diff[16]);
