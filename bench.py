@@ -303,8 +303,9 @@ def run_render(args, world: int, rank: int, local: int):
     offs = [0, w * hs, w * hs + (w // 2) * (hs // 2)]
     lens = [w * hs, (w // 2) * (hs // 2), (w // 2) * (hs // 2)]
     strides = [w, w // 2, w // 2]
-    cfg = dict(width=w, height=h, block_w=vd[2], block_h=vd[3], origin_x=vd[2] // 2, origin_y=vd[3] // 2,
-               grid_w=mw, grid_h=mh, source_step=2)
+    # SmoothFps's render configuration: the effective block (block - overlap), origin at half the block
+    cfg = dict(width=w, height=h, block_w=vd[2] - vd[9], block_h=vd[3] - vd[10], origin_x=vd[2] // 2,
+               origin_y=vd[3] // 2, grid_w=mw, grid_h=mh, source_step=2)
     thr = 128
     out_d = torch.empty((nf, w * h * 3 // 2), dtype=torch.uint8, device=dev)
     dst_offs = [0, w * h, w * h + (w // 2) * (h // 2)]
@@ -367,6 +368,51 @@ def run_render(args, world: int, rank: int, local: int):
         torch.cuda.synchronize()
         bms.append(e0.elapsed_time(e1))
     blend_value = nf / (statistics.mean(bms) / 1000.0)
+    # algorithm 21 as SmoothFps runs it from the payloads: the mask planes of all payloads (mask.cover
+    # 100, mask.area 100 -> area scale 0.01) and the masked render of frames f and f+1 with the
+    # coverage masks and the max magnitude mask as the final one
+    ascale = 0.01
+    masks_d = torch.empty((nf, 5 * mw * mh), dtype=torch.uint8, device=dev)
+    mscr = torch.empty(sv.render_masks_scratch(vd, nf), dtype=torch.uint8, device=dev)
+    mstat = torch.zeros(nf, dtype=torch.int32, device=dev)
+    masked_d = torch.empty_like(out_d)
+    nm = mw * mh
+
+    def masked_step(st):
+        sv.render_masks_device(vd, pay_d.data_ptr(), pl, nf, thr, masks_d.data_ptr(), mscr.data_ptr(),
+                               mstat.data_ptr(), cover=100, area_scale=ascale, stream=st)
+        for f in range(nf):
+            g = min(f + 1, nf - 1)
+            m0, m1, mk = planes[f].data_ptr(), planes[g].data_ptr() + 4 * nm, masks_d[f].data_ptr()
+            sv.render_masked_device(cfg, thr, ascale, False, True, [sup_d[f].data_ptr() + o for o in offs], strides,
+                                    lens, [sup_d[f + 1].data_ptr() + o for o in offs], strides, lens, 1,
+                                    (m0, m0 + 2 * nm), (m1, m1 + 2 * nm), (mk, mk + nm), mk + 4 * nm,
+                                    [masked_d[f].data_ptr() + o for o in dst_offs], strides, stream=st)
+
+    masked_step(sh)
+    torch.cuda.synchronize()
+    mgraph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(mgraph):
+        masked_step(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    mms, kms = [], []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        mgraph.replay()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        mms.append(e0.elapsed_time(e1))
+        flush.fill_(1)  # the mask planes alone, for the split
+        e0.record(stream)
+        sv.render_masks_device(vd, pay_d.data_ptr(), pl, nf, thr, masks_d.data_ptr(), mscr.data_ptr(),
+                               mstat.data_ptr(), cover=100, area_scale=ascale, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        kms.append(e0.elapsed_time(e1))
+    masked_value = nf / (statistics.mean(mms) / 1000.0)
+    masks_us_per_payload = statistics.mean(kms) * 1000.0 / nf
     ms_max = _max_over_ranks(torch, dist, world, ms, dev)
     value = nf * world * args.steps / (ms_max / 1000.0)
     # end to end: host super frames and motion planes in, rendered frames out, per step
@@ -426,6 +472,30 @@ def run_render(args, world: int, rank: int, local: int):
                                                  (mot_np[g][2], mot_np[g][3]), strides[p], ph))
             return res
 
+        masks_np = masks_d.cpu().numpy().reshape(nf, 5, mh, mw)
+        pay_np = pay_d.cpu().numpy()
+        masked_np = masked_d.cpu().numpy()
+        tlimit = orc.render_threshold_limit(thr, ascale)
+
+        def cpu_masked(f):
+            g = min(f + 1, nf - 1)
+            om = orc.render_masks(vd, pay_np[f], thr, 100, ascale)
+            res = []
+            for p in range(3):
+                ph = h // (2 if p else 1)
+                srcs = [sup_np[f][offs[p]: offs[p] + lens[p]], sup_np[f + 1][offs[p]: offs[p] + lens[p]]]
+                res.append(orc.render_dual_plane(ocfg, p > 0, True, False, 21, thr, srcs, [strides[p]] * 2,
+                                                 [strides[p] * ph] * 2, 1, (mot_np[f][0], mot_np[f][1]),
+                                                 (mot_np[g][2], mot_np[g][3]), strides[p], ph, (om[0], om[1]), om[4],
+                                                 tlimit))
+            return om, res
+
+        masked_ok = True
+        for f in range(3):
+            om, res = cpu_masked(f)
+            masked_ok &= bool(np.array_equal(masks_np[f], om)) and bool(
+                np.array_equal(np.concatenate([r.reshape(-1) for r in res]), masked_np[f]))
+        masked_check = {"frames_checked": 3, "bit_exact": masked_ok}
         blend_check = {"frames_checked": 4, "bit_exact": all(
             np.array_equal(np.concatenate([r.reshape(-1) for r in cpu_blend(f)]), blend_np[f]) for f in range(4))}
         cpu, parity = None, None
@@ -470,6 +540,12 @@ def run_render(args, world: int, rank: int, local: int):
             "blend_mode13": {"value": blend_value, "unit": "frames/s", "kernel": "render_kernel<dual>",
                              "how": "svpf_render_blend_device (algorithm 13: frames f and f+1, forward and backward "
                                     "sets), same frames and timing", "parity_vs_oracle": blend_check},
+            "masked_mode21": {"value": masked_value, "unit": "frames/s",
+                              "mask_planes_us_per_payload": masks_us_per_payload,
+                              "how": f"svpf_render_masks_device for the {nf} payloads (phase {thr}, cover 100, area "
+                                     f"scale {ascale}) + svpf_render_masked_device per frame (algorithm 21, final "
+                                     "mask = max magnitude), one CUDA-graph replay per step, same timing",
+                              "parity_vs_oracle": masked_check},
         }
         print(json.dumps(line), flush=True)
     if world > 1:

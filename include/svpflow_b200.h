@@ -172,7 +172,7 @@ int svpf_render_masks_device(const int32_t *vdata, const uint8_t *payloads_dev, 
  * (svpflow2 core.rs:1501-1517); chroma is 4:2:0. */
 typedef struct {
     int32_t width, height;        /* frame size */
-    int32_t block_w, block_h;     /* the vectors' block (vdata[2], vdata[3]) */
+    int32_t block_w, block_h;     /* the vectors' effective block: block - overlap (vdata[2] - vdata[9], vdata[3] - vdata[10]) */
     int32_t origin_x, origin_y;   /* vdata block / 2 */
     int32_t grid_w, grid_h;       /* motion-plane size (svpf_vector_grid) */
     int32_t source_step;          /* 1 for frames; the super clip's pel when the sources are super frames */
