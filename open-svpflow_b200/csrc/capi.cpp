@@ -242,6 +242,8 @@ int svpf_super_build_device(const svpf_super *s, const uint8_t *src_dev, int64_t
                             uint8_t *dst_dev, int32_t nframes, void *stream) {
     if (int rc = check_device()) return rc;
     if (nframes < 0 || (nframes > 0 && (!src_dev || !dst_dev))) return fail(SVPF_EINVAL, "bad buffers");
+    if (s->L.px_bytes == 2 && (((uintptr_t)src_dev | (uintptr_t)dst_dev) & 1))
+        return fail(SVPF_EINVAL, "16-bit frames must be 2-byte aligned");
     SuperDev D = s->D;
     if (src_y_stride > 0 || src_c_stride > 0) {
         if (src_y_stride < s->so.width || src_c_stride < s->so.width / 2) return fail(SVPF_EINVAL, "source pitch below width");
@@ -330,13 +332,27 @@ size_t svpf_analyser_scratch_bytes(const svpf_analyser *a, int32_t npairs) {
     return (size_t)(kStatusBytes + align256((int64_t)npairs * (int64_t)sizeof(PairRef)) + (int64_t)npairs * a->P.scratch_per_pair);
 }
 
+// The kernels write payload words (4 bytes), keep 8-byte fields in the scratch and read 16-bit
+// samples as such: misaligned buffers would fault, so they are refused here.
+static int check_alignment(const svpf_analyser *a, const uint8_t *super, const uint8_t *payloads, const void *scratch) {
+    if (a->P.px_bytes == 2 && ((uintptr_t)super & 1)) return fail(SVPF_EINVAL, "16-bit super frames must be 2-byte aligned");
+    if ((uintptr_t)payloads & 3) return fail(SVPF_EINVAL, "payloads must be 4-byte aligned");
+    if ((uintptr_t)scratch & 15) return fail(SVPF_EINVAL, "scratch must be 16-byte aligned");
+    return SVPF_OK;
+}
+
 int svpf_analyse_pairs_device(const svpf_analyser *a, const uint8_t *const *cur_dev, const uint8_t *const *ref_dev,
                               int32_t npairs, uint8_t *payloads_dev, void *scratch_dev, void *stream) {
     if (int rc = check_device()) return rc;
     if (npairs <= 0) return SVPF_OK;
     if (!cur_dev || !ref_dev || !payloads_dev || !scratch_dev) return fail(SVPF_EINVAL, "bad buffers");
+    if (int rc = check_alignment(a, nullptr, payloads_dev, scratch_dev)) return rc;
     std::vector<PairRef> pr((size_t)npairs);
-    for (int32_t i = 0; i < npairs; i++) pr[(size_t)i] = PairRef{cur_dev[i], ref_dev[i]};
+    for (int32_t i = 0; i < npairs; i++) {
+        if (int rc = check_alignment(a, cur_dev[i], nullptr, nullptr)) return rc;
+        if (int rc = check_alignment(a, ref_dev[i], nullptr, nullptr)) return rc;
+        pr[(size_t)i] = PairRef{cur_dev[i], ref_dev[i]};
+    }
     int rc = launch_pairs(a, pr.data(), nullptr, 0, 0, npairs, payloads_dev, scratch_dev, (cudaStream_t)stream);
     if (rc == SVPF_OK) CU(cudaStreamSynchronize((cudaStream_t)stream));  // the pair table is staged from `pr`
     return rc;
@@ -348,6 +364,7 @@ int svpf_clip_analyse_device(const svpf_analyser *a, const uint8_t *supers_dev, 
     if (count <= 0) return SVPF_OK;
     if (first < 0 || first + count > nframes || !supers_dev || !payloads_dev || !scratch_dev)
         return fail(SVPF_EINVAL, "bad frame range or buffers");
+    if (int rc = check_alignment(a, supers_dev, payloads_dev, scratch_dev)) return rc;
     return launch_pairs(a, nullptr, supers_dev, nframes, first, count, payloads_dev, scratch_dev, (cudaStream_t)stream);
 }
 

@@ -75,6 +75,9 @@ extern "C" int svpf_clip_analyse_device_noalloc(const svpf_analyser *a, const ui
     if (first < 0 || first + count > nframes || !supers_dev || !payloads_dev)
         return noalloc_fail(SVPF_EINVAL, "bad frame range or buffers");
     const AnalyseParams &P = *analyser_params(a);
+    if ((uintptr_t)payloads_dev & 3) return noalloc_fail(SVPF_EINVAL, "payloads must be 4-byte aligned");
+    if (P.px_bytes == 2 && ((uintptr_t)supers_dev & 1))
+        return noalloc_fail(SVPF_EINVAL, "16-bit super frames must be 2-byte aligned");
     const size_t need = kStatusBytes + (size_t)count * (size_t)P.scratch_per_pair;
     if (need > kNoAllocScratchBytes)
         return noalloc_fail(SVPF_EINVAL, "svpf_clip_analyse_device_noalloc: " + std::to_string(count) +

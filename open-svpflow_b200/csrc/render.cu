@@ -455,6 +455,11 @@ bool draws_nothing(const svpf_render_config *cfg) {  // render_tiles returns at 
            cfg->block_w <= 0 || cfg->block_h <= 0;
 }
 int launch(const RenderJob &J, int kind, bool mask, int32_t most_w, int32_t most_h, void *stream) {
+    for (int k = 0; k < 4; k++)  // uint16 loads from an odd address would fault
+        if (((uintptr_t)J.mx[k] | (uintptr_t)J.my[k]) & 1) {
+            svpf::set_last_error("render: motion planes must be 2-byte aligned");
+            return SVPF_EINVAL;
+        }
     cudaError_t e = cudaSuccess;
     if (most_w > 0 && most_h > 0) {
         dim3 grid((unsigned)((most_w + 256 * kPx - 1) / (256 * kPx)), (unsigned)most_h, 3);

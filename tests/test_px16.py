@@ -200,3 +200,35 @@ def test_batch_and_server_reject_16bit():
             srv.submit(sb, an, clip10(64, 48, 2, seed=1))
     finally:
         srv.close()
+
+
+@pytest.mark.gpu
+def test_device_entries_refuse_misaligned_buffers():
+    # payload words, 8-byte scratch fields and 16-bit samples would fault at unaligned addresses:
+    # each entry point refuses them before launching (the buffers are real and large enough)
+    import torch
+
+    sv = _sv()
+    w, h, n = 64, 48, 2
+    sb8 = sv.Super(w, h, "{pel:2}")
+    an8 = sv.Analyse(sb8.sdata, "{}", w, h)
+    sb10 = sv.Super(w, h, "{pel:2}", bits=10)
+    an10 = sv.Analyse(sb10.sdata, "{}", w, h, bits=10)
+    big = lambda k: torch.zeros(k + 64, dtype=torch.uint8, device="cuda")
+    sup8, sup10 = big(n * sb8.output_len()), big(n * sb10.output_len())
+    frames10 = big(n * sb10.source_len())
+    pay = big(n * max(an8.payload_len(), an10.payload_len()))
+    scr = big(max(an8.scratch_bytes(n), an10.scratch_bytes(n)))
+    sv.reset_kernel_launches()
+    with pytest.raises(ValueError, match="payloads"):
+        an8.analyse_clip_device(sup8.data_ptr(), n, 0, 1, pay.data_ptr() + 2, scr.data_ptr())
+    with pytest.raises(ValueError, match="scratch"):
+        an8.analyse_clip_device(sup8.data_ptr(), n, 0, 1, pay.data_ptr(), scr.data_ptr() + 8)
+    with pytest.raises(ValueError, match="payloads"):
+        an8.analyse_pairs_device([sup8.data_ptr()], [sup8.data_ptr() + sb8.output_len()], pay.data_ptr() + 1,
+                                 scr.data_ptr())
+    with pytest.raises(ValueError, match="2-byte"):
+        sb10.build_device(frames10.data_ptr() + 1, sup10.data_ptr(), n)
+    with pytest.raises(ValueError, match="2-byte"):
+        an10.analyse_clip_device(sup10.data_ptr() + 1, n, 0, 1, pay.data_ptr(), scr.data_ptr())
+    assert sv.kernel_launches() == 0

@@ -850,3 +850,6 @@ def test_render_rejects_bad_arguments():
         sv.render_warp_device(cfg, 257, False, True, *args)
     with pytest.raises(ValueError, match="shift"):
         sv.render_warp_device(cfg, 10, False, True, *args[:3], 1, *args[4:])
+    # odd motion-plane addresses are refused before any launch (uint16 loads there would fault)
+    with pytest.raises(ValueError, match="aligned"):
+        sv.render_warp_device(cfg, 10, False, True, *args[:4], 3, 3, *args[6:])

@@ -82,3 +82,18 @@ def test_noalloc_rejects_requests_above_its_scratch():
     assert rc == SVPF_EINVAL
     assert "static scratch" in sv.lib().svpf_last_error().decode()
     assert sv.kernel_launches() == 0
+
+
+def test_noalloc_rejects_misaligned_payloads():
+    import torch
+
+    # payload words are written 4 bytes at a time: an unaligned buffer is refused before any launch
+    n = 2
+    sv, an, supers, stream = _setup(64, 48, n + 1, "{pel:2}", "{}", seed=6)
+    out = torch.empty(n * an.payload_len() + 16, dtype=torch.uint8, device=supers.device)
+    f = _noalloc(sv.lib())
+    sv.reset_kernel_launches()
+    rc = f(an.handle, supers.data_ptr(), n + 1, 0, n, out.data_ptr() + 2, stream)
+    assert rc == SVPF_EINVAL
+    assert "aligned" in sv.lib().svpf_last_error().decode()
+    assert sv.kernel_launches() == 0
