@@ -69,6 +69,8 @@ TRAFFIC_PER_PAIR = 341.8e6 / 17
 # DRAM bytes of one 1080p render launch with the 8 x 8 effective block (ncu capture: 4.13 MB read,
 # the written frame stays in L2)
 RENDER_TRAFFIC_PER_FRAME = 4.13e6
+# graph replays per timed render step (about 40 ms, so the clock sampler sees the step)
+RENDER_REPLAYS = 48
 # int32 lanes per SM on sm_100 and the SM clock ceiling, for the nominal integer peak
 INT32_LANES_PER_SM = 128
 SM_MAX_MHZ = 1965.0
@@ -134,6 +136,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            t0 = time.time()  # nvidia-smi takes a moment to start: let its first sample land first
+            while not self.lines and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
@@ -329,14 +334,16 @@ def run_render(args, world: int, rank: int, local: int):
     torch.cuda.synchronize()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    reps = RENDER_REPLAYS  # a step replays the graph this often, so the clock samples land inside the timing
     with ClockSampler(_gpu_id(torch, local)) as clk:
         for e0, e1 in evs:
             flush.fill_(1)  # inputs partly below L2 size: flush between steps, outside the events
             e0.record(stream)
-            graph.replay()
+            for _ in range(reps):
+                graph.replay()
             e1.record(stream)
         torch.cuda.synchronize()
-    launches = nf * args.steps  # one render_kernel per frame in every replay
+    launches = nf * reps * args.steps  # one render_kernel per frame in every replay
     ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
     # the two-source blend (algorithm 13) on the same frames: frame f's and f+1's super frames, the
     # forward set of frame f and the backward set of frame f+1
@@ -415,7 +422,7 @@ def run_render(args, world: int, rank: int, local: int):
     masked_value = nf / (statistics.mean(mms) / 1000.0)
     masks_us_per_payload = statistics.mean(kms) * 1000.0 / nf
     ms_max = _max_over_ranks(torch, dist, world, ms, dev)
-    value = nf * world * args.steps / (ms_max / 1000.0)
+    value = nf * reps * world * args.steps / (ms_max / 1000.0)
     # end to end: host super frames and motion planes in, rendered frames out, per step
     sup_h = torch.empty((nf, fb), dtype=torch.uint8).pin_memory()
     sup_h.copy_(sup_d[:nf])
@@ -520,23 +527,24 @@ def run_render(args, world: int, rank: int, local: int):
             "dtype": "u8", "data": "synthetic",
             "config": {"workload": f"1080p, {nf} frames per step, algorithm 2 (render_mode1_or_2 without masks), "
                                    f"interpolated motion, threshold {thr}, sources = pel-2 super frames, motion = "
-                                   f"the clip's own vector planes; a step = one CUDA-graph replay of the "
-                                   f"{nf} launches", "frames_per_gpu": nf,
-                       "l2": "a 256 MB write flushes L2 before every step, outside the timed events"},
+                                   f"the clip's own vector planes; a step = {reps} CUDA-graph replays of the "
+                                   f"{nf} launches", "frames_per_gpu": nf, "frames_per_step": nf * reps,
+                       "l2": "a 256 MB write flushes L2 before every step, outside the timed events; the 32 "
+                             "frames' super frames (500 MB) exceed L2 within a step"},
             "clocks": clk.summary(),
             "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": int(nf * (fb + planes.shape[1] * 2)),
                     "d2h_bytes_per_step": int(nf * w * h * 3 // 2), "api": "svpf_render_warp_device with host copies",
                     "matches_device_path": same},
             "gpu_launches": int(launches),
-            "roofline": {"kernel": "render_warp_kernel", "bound": "hbm",
-                         "achieved": per_frame * nf / (ms / args.steps / 1000) / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": per_frame * nf / (ms / args.steps / 1000) / 1e9 / peak,
-                         "traffic": RENDER_TRAFFIC_PER_FRAME * nf,
+            "roofline": {"kernel": "render_kernel<0, 0> (single warp)", "bound": "hbm",
+                         "achieved": per_frame * nf * reps / (ms / args.steps / 1000) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": per_frame * nf * reps / (ms / args.steps / 1000) / 1e9 / peak,
+                         "traffic": RENDER_TRAFFIC_PER_FRAME * nf * reps,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch (1080p "
-                                           "frame; the output stays in L2), x frames",
+                                           "frame; the output stays in L2), x frames per step",
                          "peak_source": peak_kind, "algorithmic_bytes_per_frame": per_frame,
                          "note": "issue-bound, not HBM-bound: per sample a tile lookup, motion interpolation and "
-                                 "an index computation (62 % issue active in the ncu capture)"},
+                                 "an index computation (72 % issue active in the ncu capture)"},
             "cpu_baseline": cpu, "parity_vs_oracle": parity,
             "blend_mode13": {"value": blend_value, "unit": "frames/s", "kernel": "render_kernel<dual>",
                              "how": "svpf_render_blend_device (algorithm 13: frames f and f+1, forward and backward "
