@@ -345,14 +345,13 @@ def run_render(args, world: int, rank: int, local: int):
         torch.cuda.synchronize()
     launches = nf * reps * args.steps  # one render_kernel per frame in every replay
     ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-    # the two-source blend (algorithm 13) on the same frames: frame f's and f+1's super frames, the
-    # forward set of frame f and the backward set of frame f+1
+    # the two-source blend (algorithm 13) on the same frames as SmoothFps feeds it: frame f's and
+    # f+1's super frames, the two vector sets of frame f's payload
     blend_d = torch.empty_like(out_d)
 
     def blend(f, st):
-        g = min(f + 1, nf - 1)
         m0 = planes[f].data_ptr()
-        m1 = planes[g].data_ptr() + 2 * mw * mh * 2
+        m1 = planes[f].data_ptr() + 2 * mw * mh * 2
         sv.render_blend_device(cfg, thr, True, True, False, [sup_d[f].data_ptr() + o for o in offs], strides, lens,
                                [sup_d[f + 1].data_ptr() + o for o in offs], strides, lens, 1, (m0, m0 + mw * mh * 2),
                                (m1, m1 + mw * mh * 2), [blend_d[f].data_ptr() + o for o in dst_offs], strides, stream=st)
@@ -390,8 +389,7 @@ def run_render(args, world: int, rank: int, local: int):
         sv.render_masks_device(vd, pay_d.data_ptr(), pl, nf, thr, masks_d.data_ptr(), mscr.data_ptr(),
                                mstat.data_ptr(), cover=100, area_scale=ascale, stream=st)
         for f in range(nf):
-            g = min(f + 1, nf - 1)
-            m0, m1, mk = planes[f].data_ptr(), planes[g].data_ptr() + 4 * nm, masks_d[f].data_ptr()
+            m0, m1, mk = planes[f].data_ptr(), planes[f].data_ptr() + 4 * nm, masks_d[f].data_ptr()
             sv.render_masked_device(cfg, thr, ascale, False, True, [sup_d[f].data_ptr() + o for o in offs], strides,
                                     lens, [sup_d[f + 1].data_ptr() + o for o in offs], strides, lens, 1,
                                     (m0, m0 + 2 * nm), (m1, m1 + 2 * nm), (mk, mk + nm), mk + 4 * nm,
@@ -469,7 +467,7 @@ def run_render(args, world: int, rank: int, local: int):
         blend_np = blend_d.cpu().numpy()
 
         def cpu_blend(f):
-            g = min(f + 1, nf - 1)
+            g = f
             res = []
             for p in range(3):
                 ph = h // (2 if p else 1)
@@ -486,7 +484,7 @@ def run_render(args, world: int, rank: int, local: int):
         tlimit = orc.render_threshold_limit(thr, ascale)
 
         def cpu_masked(f):
-            g = min(f + 1, nf - 1)
+            g = f
             om = orc.render_masks(vd, pay_np[f], thr, 100, ascale)
             res = []
             for p in range(3):
@@ -547,8 +545,8 @@ def run_render(args, world: int, rank: int, local: int):
                                  "an index computation (72 % issue active in the ncu capture)"},
             "cpu_baseline": cpu, "parity_vs_oracle": parity,
             "blend_mode13": {"value": blend_value, "unit": "frames/s", "kernel": "render_kernel<dual>",
-                             "how": "svpf_render_blend_device (algorithm 13: frames f and f+1, forward and backward "
-                                    "sets), same frames and timing", "parity_vs_oracle": blend_check},
+                             "how": "svpf_render_blend_device (algorithm 13: frames f and f+1, the two vector sets "
+                                    "of frame f's payload), same frames and timing", "parity_vs_oracle": blend_check},
             "masked_mode21": {"value": masked_value, "unit": "frames/s",
                               "mask_planes_us_per_payload": masks_us_per_payload,
                               "how": f"svpf_render_masks_device for the {nf} payloads (phase {thr}, cover 100, area "

@@ -301,8 +301,8 @@ def test_device_masks_reject_bad_arguments():
 
 @pytest.mark.gpu
 def test_masked_render_after_device_chain():
-    """Super -> Analyse -> vector planes + mask planes -> algorithm 21 / 22 render, all on the device,
-    against the oracle's chain."""
+    """Super -> Analyse -> vector planes + mask planes -> algorithm 21 / 22 / 23 render, all on the
+    device, against the oracle's chain."""
     import torch
 
     import svpflow_b200 as sv
@@ -367,3 +367,23 @@ def test_masked_render_after_device_chain():
                                              [pw * ph, pw * ph], 1, (mp[0], mp[1]), (mp[2], mp[3]), pw, ph,
                                              (om[0], om[1]), om[4], tlimit)
                 assert np.array_equal(dsts[p].cpu().numpy(), want), f"frame {f} mode22 {mode22} plane {p}"
+    # algorithm 23 at frame 1 as SmoothFps feeds it: the frame's own two sets, the next payload's
+    # previous set (next0) and the previous payload's current set (prev1), all from vector planes
+    f = 1
+    mp = [orc.vector_planes(vd, pays[k], w, h) for k in range(3)]
+    om = orc.render_masks(vd, pays[f], phase, cover, scale)
+    dsts = [torch.zeros((h // (2 if p else 1), w // (2 if p else 1)), dtype=torch.uint8, device="cuda") for p in range(3)]
+    pl = [planes[k].data_ptr() for k in range(3)]
+    sets = [(pl[1], pl[1] + 2 * nm), (pl[1] + 4 * nm, pl[1] + 6 * nm), (pl[2], pl[2] + 2 * nm), (pl[0] + 4 * nm, pl[0] + 6 * nm)]
+    mk = masks[f].data_ptr()
+    b0, b1 = sup_d[f].data_ptr(), sup_d[f + 1].data_ptr()
+    sv.render_mode23_device(cfg, phase, True, [b0 + o for o in offs], strides, lens, [b1 + o for o in offs], strides,
+                            lens, 1, sets, (mk, mk + nm), mk + 4 * nm, [d.data_ptr() for d in dsts], strides)
+    torch.cuda.synchronize()
+    for p in range(3):
+        pw, ph = strides[p], h // (2 if p else 1)
+        srcs = [sup_h[f][offs[p]: offs[p] + lens[p]], sup_h[f + 1][offs[p]: offs[p] + lens[p]]]
+        motions = [(mp[1][0], mp[1][1]), (mp[1][2], mp[1][3]), (mp[2][0], mp[2][1]), (mp[0][2], mp[0][3])]
+        want = orc.render_mode23_plane(cfg, p > 0, True, phase, srcs, [pw, pw], [pw * ph, pw * ph], 1, motions,
+                                       (om[0], om[1]), om[4], pw, ph)
+        assert np.array_equal(dsts[p].cpu().numpy(), want), f"algorithm 23, plane {p}"
