@@ -28,7 +28,9 @@ Other workloads (one JSON line each, same keys):
                        and the parity check use the oracle's uint16 build.
   --workload render    SmoothFps's single-warp render (algorithm 2, no masks) of 32 1080p frames
                        from their pel-2 super frames and vector planes; frames/s, CPU leg = the
-                       oracle's render on all host threads, every frame compared.
+                       oracle's render on all host threads, every frame compared. Beside it:
+                       algorithm 13 (two sources) and algorithm 21 with its mask planes made
+                       from the payloads in the same step, each checked on a few frames.
   --workload served    Poisson arrivals of clips (360p..2160p, 8-600 frames) into the
                        continuous-batching server under an HBM budget, at each --rates value;
                        p50 / p99 per-frame-pair latency (arrival of the clip to its payload in
