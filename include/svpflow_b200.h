@@ -162,7 +162,7 @@ int svpf_vector_planes_device(const int32_t *vdata, const uint8_t *payloads_dev,
  * where payload i does not decode (its planes are left as they were). Bytes equal the reference's,
  * except that area_sharp != 1 goes through CUDA's pow (2 ulp), which can move a byte by one where
  * 255 * value lies within a few ulp of an integer. Asynchronous on `stream`. */
-int64_t svpf_render_masks_scratch(const int32_t *vdata, int32_t npayloads);
+int64_t svpf_render_masks_scratch(const int32_t *vdata, int32_t npayloads); /* -1 (and svpf_last_error) if refused */
 int svpf_render_masks_device(const int32_t *vdata, const uint8_t *payloads_dev, size_t payload_len, int32_t npayloads,
                              int32_t phase, int32_t cover_percent, double area_scale, double area_sharp,
                              uint8_t *masks_dev, void *scratch_dev, int32_t *status_dev, void *stream);

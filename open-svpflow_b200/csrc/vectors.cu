@@ -343,7 +343,10 @@ extern "C" {
 int64_t svpf_render_masks_scratch(const int32_t *vdata, int32_t npayloads) {
     MaskJob J;
     std::string err;
-    if (npayloads < 0 || !mask_job(vdata, J, err)) return -1;
+    if (npayloads < 0 || !mask_job(vdata, J, err)) {
+        svpf::set_last_error(npayloads < 0 ? std::string("negative payload count") : err);
+        return -1;
+    }
     return (int64_t)npayloads * 2 * ((int64_t)J.mw + 2) * ((int64_t)J.mh + 2) * (int64_t)sizeof(int32_t);
 }
 

@@ -504,7 +504,7 @@ def render_masks_scratch(vdata, npayloads: int) -> int:
     v = (ctypes.c_int32 * 16)(*vdata)
     n = lib().svpf_render_masks_scratch(v, int(npayloads))
     if n < 0:
-        raise ValueError("not a vector header the mask planes take")
+        raise ValueError(lib().svpf_last_error().decode(errors="replace"))
     return n
 
 
