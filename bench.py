@@ -499,13 +499,20 @@ def run_render(args, world: int, rank: int, local: int):
             return om, res
 
         masked_ok = True
-        for f in range(3):
-            om, res = cpu_masked(f)
+        t0 = time.perf_counter()
+        masked_res = [cpu_masked(f) for f in range(3)]
+        masked_cpu = 3 / (time.perf_counter() - t0)
+        for f, (om, res) in enumerate(masked_res):
             masked_ok &= bool(np.array_equal(masks_np[f], om)) and bool(
                 np.array_equal(np.concatenate([r.reshape(-1) for r in res]), masked_np[f]))
-        masked_check = {"frames_checked": 3, "bit_exact": masked_ok}
+        masked_check = {"frames_checked": 3, "bit_exact": masked_ok,
+                        "oracle_frames_per_s_one_thread": masked_cpu}
+        t0 = time.perf_counter()
+        blend_res = [cpu_blend(f) for f in range(4)]
+        blend_cpu = 4 / (time.perf_counter() - t0)
         blend_check = {"frames_checked": 4, "bit_exact": all(
-            np.array_equal(np.concatenate([r.reshape(-1) for r in cpu_blend(f)]), blend_np[f]) for f in range(4))}
+            np.array_equal(np.concatenate([r.reshape(-1) for r in blend_res[f]]), blend_np[f]) for f in range(4)),
+            "oracle_frames_per_s_one_thread": blend_cpu}
         cpu, parity = None, None
         if not args.no_cpu:
             threads = os.cpu_count() or 1

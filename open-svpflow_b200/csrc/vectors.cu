@@ -57,29 +57,35 @@ __device__ __forceinline__ uint16_t centered(int v) {
     return (uint16_t)(v + kNeutral);
 }
 
+// decode_vectors' checks on one payload (every thread reads the same few words): header, region
+// markers, region lengths. On success, the byte offsets of the two sets' first vectors, the
+// previous set falling back to the current one and vice versa.
+__device__ __forceinline__ bool decode_regions(const uint8_t *p, int64_t len, int32_t flags, int64_t count,
+                                               int64_t &off_prev, int64_t &off_cur) {
+    const int64_t first = 0x40, second = first + 4 + count * 8;
+    bool ok = true;
+    const bool hdr = rd32(p, len, 0, ok) == 16 && rd32(p, len, 4, ok) == 0xA0 && rd32(p, len, 8, ok) == flags;
+    const int marker = (int)(2 * count + 1);
+    const bool has_prev = (flags & 1) != 0, has_cur = (flags & 2) != 0;
+    if (has_prev && rd32(p, len, first, ok) != marker) ok = false;
+    if (has_cur && rd32(p, len, second, ok) != marker) ok = false;
+    if (has_prev && first + 4 + count * 8 > len) ok = false;
+    if (has_cur && second + 4 + count * 8 > len) ok = false;
+    off_prev = has_prev ? first + 4 : second + 4;
+    off_cur = has_cur ? second + 4 : first + 4;
+    return ok && hdr && (has_prev || has_cur);
+}
+
 // grid: (positions / 256, payloads)
 __global__ void vector_planes_kernel(const PlaneJob J) {
     const int64_t f = blockIdx.y;
     const uint8_t *p = J.payloads + f * J.payload_len;
     const int64_t count = (int64_t)J.gw * J.gh;
-    const int64_t first = 0x40, second = first + 4 + count * 8;
-    // decode_vectors' checks (every thread reads the same few words)
-    bool ok = true;
-    const bool hdr = rd32(p, J.payload_len, 0, ok) == 16 && rd32(p, J.payload_len, 4, ok) == 0xA0 &&
-                     rd32(p, J.payload_len, 8, ok) == J.flags;
-    const int marker = (int)(2 * count + 1);
-    bool has_prev = (J.flags & 1) != 0, has_cur = (J.flags & 2) != 0;
-    if (has_prev && rd32(p, J.payload_len, first, ok) != marker) ok = false;
-    if (has_cur && rd32(p, J.payload_len, second, ok) != marker) ok = false;
-    if (has_prev && first + 4 + count * 8 > J.payload_len) ok = false;
-    if (has_cur && second + 4 + count * 8 > J.payload_len) ok = false;
-    ok = ok && hdr && (has_prev || has_cur);
-    if (!ok) {
+    int64_t off_prev, off_cur;
+    if (!decode_regions(p, J.payload_len, J.flags, count, off_prev, off_cur)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) J.status[f] = 1;
         return;
     }
-    const int64_t off_prev = has_prev ? first + 4 : second + 4;  // previous falls back to current
-    const int64_t off_cur = has_cur ? second + 4 : first + 4;    // and current to previous
     const int64_t n = (int64_t)J.mw * J.mh;
     uint16_t *out = J.planes + f * 4 * n;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -133,20 +139,7 @@ struct MaskJob {
 
 __device__ __forceinline__ bool mask_regions(const MaskJob &J, const uint8_t *p, int64_t &off_prev,
                                              int64_t &off_cur) {
-    const int64_t count = (int64_t)J.gw * J.gh;
-    const int64_t first = 0x40, second = first + 4 + count * 8;
-    bool ok = true;
-    const bool hdr = rd32(p, J.payload_len, 0, ok) == 16 && rd32(p, J.payload_len, 4, ok) == 0xA0 &&
-                     rd32(p, J.payload_len, 8, ok) == J.flags;
-    const int marker = (int)(2 * count + 1);
-    const bool has_prev = (J.flags & 1) != 0, has_cur = (J.flags & 2) != 0;
-    if (has_prev && rd32(p, J.payload_len, first, ok) != marker) ok = false;
-    if (has_cur && rd32(p, J.payload_len, second, ok) != marker) ok = false;
-    if (has_prev && first + 4 + count * 8 > J.payload_len) ok = false;
-    if (has_cur && second + 4 + count * 8 > J.payload_len) ok = false;
-    off_prev = has_prev ? first + 4 : second + 4;  // previous falls back to current
-    off_cur = has_cur ? second + 4 : first + 4;    // and current to previous
-    return ok && hdr && (has_prev || has_cur);
+    return decode_regions(p, J.payload_len, J.flags, (int64_t)J.gw * J.gh, off_prev, off_cur);
 }
 
 // grid: (vectors / 256, payloads, 2). z = 0: mask 0 splats the current set at 256 - phase;
