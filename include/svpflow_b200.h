@@ -167,6 +167,21 @@ int svpf_render_masks_device(const int32_t *vdata, const uint8_t *payloads_dev, 
                              int32_t phase, int32_t cover_percent, double area_scale, double area_sharp,
                              uint8_t *masks_dev, void *scratch_dev, int32_t *status_dev, void *stream);
 
+/* SmoothFps's scene limits (svpflow2 options.rs SceneLimits; SmoothFps's defaults: blocks 20, zero
+ * 200, m1 1600, m2 2800, scene 4000), as metadata.rs SceneThresholds reads them. */
+typedef struct {
+    int32_t blocks_pct, zero, m1, m2, scene;
+} svpf_scene_limits;
+/* SmoothFps's scene class (0 steady .. 3 scene change) of each payload (svpflow2 core.rs:2079-2100:
+ * metadata.rs analyze_scene, crates/svpflow-core/src/metadata.rs:349-361, over the previous and
+ * current sets, each falling back to the other; 3 when the payload holds neither), with the
+ * scene.luma gamma (default 1.5). classes_dev[i] = -1 and status_dev[i] = 1 where payload i does not
+ * decode. Payloads (payload_len a multiple of 4) are 4-byte aligned. Bit-exact: the luma curve is
+ * tabulated on the host with libm's pow. Asynchronous on `stream`. */
+int svpf_scene_class_device(const int32_t *vdata, const uint8_t *payloads_dev, size_t payload_len, int32_t npayloads,
+                            double luma_gamma, const svpf_scene_limits *limits, int32_t *classes_dev,
+                            int32_t *status_dev, void *stream);
+
 /* ---------------------------------------------------------------- frame render (SmoothFps) */
 /* renderer.rs CpuConfig (crates/svpflow-core/src/renderer.rs:34-46) as SmoothFps fills it
  * (svpflow2 core.rs:1501-1517); chroma is 4:2:0. */

@@ -7,6 +7,7 @@
 // (:1870-1874), centered (:3237-3243), as SmoothFps calls them (svpflow2 core.rs:962-1001): the
 // "previous" set falls back to the current one and vice versa.
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #include <string>
@@ -231,6 +232,71 @@ __global__ void mask_finish_kernel(const MaskJob J) {
     }
 }
 
+// ---------------------------------------------------------------- scene class
+// SmoothFps's scene class of a payload (svpflow2 core.rs:2079-2100): metadata.rs analyze_scene
+// (:349-361) = luma_map (:275-297) + classify_scene (:299-347). luma_byte (:523-526) of
+// (previous luma + current luma) / denom takes at most 511 inputs, so the host tabulates it with
+// libm's pow (the reference's own) and the kernel only looks it up: the counts are integer.
+struct SceneJob {
+    const uint8_t *payloads;
+    int64_t payload_len;
+    int32_t *classes, *status;
+    int32_t flags, gw, gh;
+    int32_t blocks_pct, zero, m1, m2, scene;
+    uint8_t luma[512];  // luma_byte of (a + b) / denom, a + b in 0..510
+};
+
+// grid: (payloads); one CTA reduces one payload's four counts
+__global__ void __launch_bounds__(256) scene_class_kernel(const __grid_constant__ SceneJob J) {
+    __shared__ int cnt[4];  // considered, scene, m2, m1
+    const int64_t f = blockIdx.x;
+    const uint8_t *p = J.payloads + f * J.payload_len;
+    const int64_t count = (int64_t)J.gw * J.gh;
+    bool ok = true;
+    const bool hdr = rd32(p, J.payload_len, 0, ok) == 16 && rd32(p, J.payload_len, 4, ok) == 0xA0 &&
+                     rd32(p, J.payload_len, 8, ok) == J.flags;
+    if (!(ok && hdr)) {
+        if (threadIdx.x == 0) { J.status[f] = 1; J.classes[f] = -1; }
+        return;
+    }
+    if ((J.flags & 3) == 0) {  // no vector set: scene_class returns 3
+        if (threadIdx.x == 0) J.classes[f] = 3;
+        return;
+    }
+    int64_t off_prev, off_cur;
+    if (!decode_regions(p, J.payload_len, J.flags, count, off_prev, off_cur)) {
+        if (threadIdx.x == 0) { J.status[f] = 1; J.classes[f] = -1; }
+        return;
+    }
+    if (threadIdx.x < 4) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    int c[4] = {0, 0, 0, 0};
+    for (int64_t i = threadIdx.x; i < count; i += blockDim.x) {
+        const unsigned lp = *reinterpret_cast<const unsigned *>(p + off_prev + i * 8 + 4) >> 24;
+        const unsigned wc = *reinterpret_cast<const unsigned *>(p + off_cur + i * 8 + 4);
+        const int l = max((int)J.luma[lp + (wc >> 24)], 1);
+        const long long s255 = (long long)(wc & 0xFFFFFFu) * 255;
+        const int score = (int)(s255 > INT32_MAX ? INT32_MAX : s255) / l;  // saturating_mul, then /
+        if (score < J.zero) continue;
+        c[0]++;
+        if (score >= J.scene) c[1]++;
+        else if (score >= J.m2) c[2]++;
+        else if (score >= J.m1) c[3]++;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        int v = c[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt[k], v);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int required = (int)((unsigned)cnt[0] * (unsigned)J.blocks_pct) / 100;
+        const int high = cnt[1] + cnt[2], mid = high + cnt[3];
+        J.classes[f] = cnt[1] >= required ? 3 : (high >= required ? 2 : (mid >= required ? 1 : 0));
+    }
+}
+
 bool mask_job(const int32_t *vdata, MaskJob &J, std::string &err) {
     VecHdr h;
     if (!read_vdata(vdata, h)) {
@@ -395,6 +461,61 @@ int svpf_render_masks_device(const int32_t *vdata, const uint8_t *payloads_dev, 
     }
     if (e != cudaSuccess) {
         svpf::set_last_error(std::string("mask planes: ") + cudaGetErrorString(e));
+        return SVPF_ECUDA;
+    }
+    return SVPF_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int svpf_scene_class_device(const int32_t *vdata, const uint8_t *payloads_dev, size_t payload_len, int32_t npayloads,
+                            double luma_gamma, const svpf_scene_limits *limits, int32_t *classes_dev,
+                            int32_t *status_dev, void *stream) {
+    if (int rc = svpf::require_device()) return rc;
+    VecHdr h;
+    if (!read_vdata(vdata, h) || !limits) {
+        svpf::set_last_error(limits ? "not a vector header" : "null scene limits");
+        return SVPF_EINVAL;
+    }
+    if (npayloads <= 0) return SVPF_OK;
+    if (!payloads_dev || !classes_dev || !status_dev || payload_len < 0x40 || npayloads > INT32_MAX / 2) {
+        svpf::set_last_error("bad buffers");
+        return SVPF_EINVAL;
+    }
+    if ((payload_len & 3) || ((uintptr_t)payloads_dev & 3)) {
+        svpf::set_last_error("payloads must be 4-byte aligned");
+        return SVPF_EINVAL;
+    }
+    SceneJob J;
+    J.payloads = payloads_dev;
+    J.payload_len = (int64_t)payload_len;
+    J.classes = classes_dev;
+    J.status = status_dev;
+    J.flags = h.flags;
+    J.gw = h.gw > 0 ? h.gw : 0;
+    J.gh = h.gh > 0 ? h.gh : 0;
+    J.blocks_pct = limits->blocks_pct;
+    J.zero = limits->zero;
+    J.m1 = limits->m1;
+    J.m2 = limits->m2;
+    J.scene = limits->scene;
+    const double denom = h.marker == 3 ? 510.0 : 255.0;
+    for (int k = 0; k < 512; k++) {  // luma_byte: (value^gamma * 255) as i32, .max(20) & 0xFF
+        const double v = pow(((double)k) / denom, luma_gamma) * 255.0;
+        const int32_t scaled = v != v ? 0 : (v >= 2147483647.0 ? INT32_MAX : (v <= -2147483648.0 ? INT32_MIN : (int32_t)v));
+        J.luma[k] = (uint8_t)((scaled > 20 ? scaled : 20) & 0xFF);
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(status_dev, 0, sizeof(int32_t) * (size_t)npayloads, st);
+    if (e == cudaSuccess) {
+        scene_class_kernel<<<(unsigned)npayloads, 256, 0, st>>>(J);
+        svpf::add_launches(1);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        svpf::set_last_error(std::string("scene class: ") + cudaGetErrorString(e));
         return SVPF_ECUDA;
     }
     return SVPF_OK;

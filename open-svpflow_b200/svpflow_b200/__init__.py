@@ -45,6 +45,11 @@ class RenderConfig(ctypes.Structure):
                                                "grid_w", "grid_h", "source_step")]
 
 
+class SceneLimits(ctypes.Structure):
+    """svpf_scene_limits: SmoothFps's scene limits."""
+    _fields_ = [(f, ctypes.c_int32) for f in ("blocks_pct", "zero", "m1", "m2", "scene")]
+
+
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
@@ -107,6 +112,8 @@ def lib() -> ctypes.CDLL:
             "svpf_server_stats": (None, [_VP, P(I64), P(I64), P(I64), P(I32), P(I64)]),
             "svpf_vector_grid": (I32, [P(I32), P(I32), P(I32)]),
             "svpf_vector_planes_device": (I32, [P(I32), _VP, SZ, I32, I32, I32, I32, _VP, _VP, _VP]),
+            "svpf_scene_class_device": (I32, [P(I32), _VP, SZ, I32, ctypes.c_double, P(SceneLimits), _VP, _VP,
+                                              _VP]),
             "svpf_render_masks_scratch": (I64, [P(I32), I32]),
             "svpf_render_masks_device": (I32, [P(I32), _VP, SZ, I32, I32, I32, ctypes.c_double, ctypes.c_double,
                                                _VP, _VP, _VP, _VP]),
@@ -497,6 +504,17 @@ def vector_planes_device(vdata, payloads_ptr: int, payload_len: int, npayloads: 
     v = (ctypes.c_int32 * 16)(*vdata)
     _check(lib().svpf_vector_planes_device(v, payloads_ptr, payload_len, npayloads, frame_w, frame_h, int(raw),
                                            planes_ptr, status_ptr, stream))
+
+
+def scene_class_device(vdata, payloads_ptr: int, payload_len: int, npayloads: int, classes_ptr: int, status_ptr: int,
+                       gamma: float = 1.5, blocks: int = 20, zero: int = 200, m1: int = 1600, m2: int = 2800,
+                       scene: int = 4000, stream: int = 0):
+    """SmoothFps's scene class (int32 per payload, -1 where it does not decode) on device buffers;
+    see svpf_scene_class_device."""
+    v = (ctypes.c_int32 * 16)(*vdata)
+    lim = SceneLimits(int(blocks), int(zero), int(m1), int(m2), int(scene))
+    _check(lib().svpf_scene_class_device(v, payloads_ptr, payload_len, npayloads, float(gamma), ctypes.byref(lim),
+                                         classes_ptr, status_ptr, stream))
 
 
 def render_masks_scratch(vdata, npayloads: int) -> int:

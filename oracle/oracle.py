@@ -446,6 +446,9 @@ def _setup(L):
                                    ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
     L.or_render_masks.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, ctypes.c_int32,
                                   ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
+    L.or_scene_class.restype = ctypes.c_int32
+    L.or_scene_class.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_double] + \
+        [ctypes.c_int32] * 5
     L.or_hadamard4_satd.argtypes = [P(ctypes.c_int32)]
     L.or_adapt_lambda.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
     L.or_exact_lambda.argtypes = [P(AnalyseOpts), ctypes.c_int32, ctypes.c_int32]
@@ -720,6 +723,16 @@ def render_masks(vdata, payload: np.ndarray, phase: int, cover: int = 100, area_
     rc = lib().or_render_masks(v, _ptr(payload), payload.size, int(phase), int(cover), float(area_scale),
                                float(area_sharp), out.ctypes.data)
     return None if rc else out.reshape(5, mh, mw)
+
+
+def scene_class(vdata, payload: np.ndarray, gamma: float = 1.5, blocks: int = 20, zero: int = 200, m1: int = 1600,
+                m2: int = 2800, scene: int = 4000) -> int:
+    """SmoothFps's scene class (0..3) of one payload; -1 when it does not decode. Defaults: the
+    scene.luma gamma and the scene limits SmoothFps uses in its default mode."""
+    payload = np.ascontiguousarray(payload, dtype=np.uint8)
+    v = (ctypes.c_int32 * 16)(*vdata)
+    return lib().or_scene_class(v, _ptr(payload), payload.size, float(gamma), int(blocks), int(zero), int(m1),
+                                int(m2), int(scene))
 
 
 # ---- 10-bit extension (uint16 samples), same options as the 8-bit path

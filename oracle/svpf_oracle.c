@@ -1834,9 +1834,9 @@ static int rd_i32(const uint8_t *p, size_t len, size_t off, int32_t *v) { /* rea
     return 1;
 }
 /* decode_region (:455-481): 0 when the region does not decode */
-/* score: NULL, or the vectors' 24-bit scores (DecodedVector::score) */
+/* score / luma: NULL, or the vectors' 24-bit scores and luma bytes (DecodedVector::score, ::luma) */
 static int decode_region(const uint8_t *p, size_t len, size_t off, size_t count, int16_t *dx, int16_t *dy,
-                         uint32_t *score) {
+                         uint32_t *score, uint8_t *luma) {
     int32_t m;
     if (!rd_i32(p, len, off, &m) || (i64)m != (i64)(2 * count + 1)) return 0;
     for (size_t i = 0; i < count; i++) {
@@ -1846,6 +1846,7 @@ static int decode_region(const uint8_t *p, size_t len, size_t off, size_t count,
         dx[i] = (int16_t)(rot & 0xFFFF);
         dy[i] = (int16_t)(rot >> 16);
         if (score) score[i] = (uint32_t)r1 & 0x00FFFFFFu;
+        if (luma) luma[i] = (uint8_t)((uint32_t)r1 >> 24);
     }
     return 1;
 }
@@ -1867,8 +1868,8 @@ int or_vector_planes(const int32_t vdata[16], const uint8_t *p, size_t len, int3
     size_t count = (size_t)gw * (size_t)gh, first = 0x40, second = first + 4 + count * 8;
     int16_t *pvx = calloc(count + 1, 2), *pvy = calloc(count + 1, 2), *cx = calloc(count + 1, 2),
             *cy = calloc(count + 1, 2);
-    int okp = (flags & 1) ? decode_region(p, len, first, count, pvx, pvy, NULL) : 0;
-    int okc = (flags & 2) ? decode_region(p, len, second, count, cx, cy, NULL) : 0;
+    int okp = (flags & 1) ? decode_region(p, len, first, count, pvx, pvy, NULL, NULL) : 0;
+    int okc = (flags & 2) ? decode_region(p, len, second, count, cx, cy, NULL, NULL) : 0;
     int rc = 0;
     if (((flags & 1) && !okp) || ((flags & 2) && !okc) || (!okp && !okc)) rc = -1;
     else {
@@ -2027,8 +2028,8 @@ int or_render_masks(const int32_t vdata[16], const uint8_t *p, size_t len, int32
     for (int s = 0; s < 2; s++) {
         vx[s] = calloc(count + 1, 2); vy[s] = calloc(count + 1, 2); sc[s] = calloc(count + 1, 4);
     }
-    ok[0] = (flags & 1) ? decode_region(p, len, first, count, vx[0], vy[0], sc[0]) : 0;
-    ok[1] = (flags & 2) ? decode_region(p, len, second, count, vx[1], vy[1], sc[1]) : 0;
+    ok[0] = (flags & 1) ? decode_region(p, len, first, count, vx[0], vy[0], sc[0], NULL) : 0;
+    ok[1] = (flags & 2) ? decode_region(p, len, second, count, vx[1], vy[1], sc[1], NULL) : 0;
     int rc = 0;
     if (((flags & 1) && !ok[0]) || ((flags & 2) && !ok[1]) || (!ok[0] && !ok[1])) rc = -1;
     else {
@@ -2050,6 +2051,55 @@ int or_render_masks(const int32_t vdata[16], const uint8_t *p, size_t len, int32
     }
     for (int s = 0; s < 2; s++) { free(vx[s]); free(vy[s]); free(sc[s]); }
     return rc;
+}
+
+/* ------------------------------------------------------------------ SmoothFps scene class */
+/* SmoothFps's scene class of one payload (svpflow2 core.rs:2079-2100): metadata.rs analyze_scene
+ * (:349-361) = luma_map (:275-297, with luma_byte :523-526) over the previous / current sets (each
+ * falling back to the other) and classify_scene (:299-347) over the current set. */
+static uint8_t sc_luma_byte(double value, double gamma) {
+    const i32 scaled = f64_as_i32(pow(value, gamma) * 255.0);
+    return (uint8_t)((scaled > 20 ? scaled : 20) & 0xFF);
+}
+int32_t or_scene_class(const int32_t vdata[16], const uint8_t *p, size_t len, double gamma, int32_t blocks_pct,
+                       int32_t zero, int32_t m1, int32_t m2, int32_t scene) {
+    int32_t flags = vdata[1], gw = imax(vdata[11], 0), gh = imax(vdata[12], 0), v;
+    if (vdata[0] != 0xA0) return -1;
+    if (!rd_i32(p, len, 0, &v) || v != 16 || !rd_i32(p, len, 4, &v) || v != 0xA0 || !rd_i32(p, len, 8, &v) ||
+        v != flags)
+        return -1;
+    size_t count = (size_t)gw * (size_t)gh, first = 0x40, second = first + 4 + count * 8;
+    int16_t *dx = calloc(count + 1, 2), *dy = calloc(count + 1, 2);
+    uint32_t *sc[2] = {calloc(count + 1, 4), calloc(count + 1, 4)};
+    uint8_t *lu[2] = {calloc(count + 1, 1), calloc(count + 1, 1)}, *map = calloc(count + 1, 1);
+    int okp = (flags & 1) ? decode_region(p, len, first, count, dx, dy, sc[0], lu[0]) : 0;
+    int okc = (flags & 2) ? decode_region(p, len, second, count, dx, dy, sc[1], lu[1]) : 0;
+    int32_t cls;
+    if (((flags & 1) && !okp) || ((flags & 2) && !okc)) cls = -1;   /* decode_vectors -> None */
+    else if (!okp && !okc) cls = 3;                                  /* no set: scene_class returns 3 */
+    else {
+        const int ip = okp ? 0 : 1, ic = okc ? 1 : 0;               /* the fallbacks */
+        const double denom = vdata[4] == 3 ? 510.0 : 255.0;
+        for (size_t i = 0; i < count; i++)
+            map[i] = sc_luma_byte(((double)lu[ip][i] + (double)lu[ic][i]) / denom, gamma);
+        i32 scene_n = 0, m2_n = 0, m1_n = 0, considered = 0;
+        for (i32 y = 0; y < gh; y++)
+            for (i32 x = 0; x < gw; x++) {
+                const size_t i = (size_t)y * (size_t)gw + (size_t)x;
+                const i32 l = imax((i32)map[i], 1);
+                const i32 score = sat_mul_i32((i32)sc[ic][i], 255) / l;
+                if (score < zero) continue;
+                considered++;
+                if (score >= scene) scene_n++;
+                else if (score >= m2) m2_n++;
+                else if (score >= m1) m1_n++;
+            }
+        const i32 required = (i32)((u32)considered * (u32)blocks_pct) / 100;
+        const i32 high = scene_n + m2_n, mid = high + m1_n;
+        cls = scene_n >= required ? 3 : (high >= required ? 2 : (mid >= required ? 1 : 0));
+    }
+    free(dx); free(dy); free(sc[0]); free(sc[1]); free(lu[0]); free(lu[1]); free(map);
+    return cls;
 }
 
 /* ------------------------------------------------------------------ SmoothFps single-warp render */

@@ -216,6 +216,10 @@ int or_vector_planes(const int32_t vdata[16], const uint8_t *payload, size_t len
  * magnitude_mask with area_scale, area_sharp); -1 when the payload does not decode. */
 int or_render_masks(const int32_t vdata[16], const uint8_t *payload, size_t len, int32_t phase, int32_t cover,
                     double area_scale, double area_sharp, uint8_t *out);
+/* SmoothFps's scene class (0..3) of one payload with the scene.luma gamma and the scene limits;
+ * -1 when the payload does not decode. */
+int32_t or_scene_class(const int32_t vdata[16], const uint8_t *payload, size_t len, double gamma, int32_t blocks_pct,
+                       int32_t zero, int32_t m1, int32_t m2, int32_t scene);
 
 /* ---- primitives exposed for known-answer tests ---- */
 uint32_t or_hadamard4_satd(const int32_t diff[16]);
