@@ -159,9 +159,10 @@ int svpf_vector_planes_device(const int32_t *vdata, const uint8_t *payloads_dev,
  * the mask of svpf_render_warp_device. scratch_dev holds svpf_render_masks_scratch bytes.
  * Payloads (payload_len a multiple of 4) and scratch are 4-byte aligned; the overlap lies in
  * 0..block - 1 and grid_w * grid_h * block area <= 2^30 (every Analyse field). status_dev[i] = 1
- * where payload i does not decode (its planes are left as they were). Bytes equal the reference's,
- * except that area_sharp != 1 goes through CUDA's pow (2 ulp), which can move a byte by one where
- * 255 * value lies within a few ulp of an integer. Asynchronous on `stream`. */
+ * where payload i does not decode (its planes are left as they were). Bytes equal the reference's
+ * for area_sharp >= 0.001 and area_scale >= 0 (the magnitude byte's steps are found on the host with
+ * libm's pow); other settings evaluate pow on the device (CUDA's, within 2 ulp of libm's).
+ * Asynchronous on `stream`. */
 int64_t svpf_render_masks_scratch(const int32_t *vdata, int32_t npayloads); /* -1 (and svpf_last_error) if refused */
 int svpf_render_masks_device(const int32_t *vdata, const uint8_t *payloads_dev, size_t payload_len, int32_t npayloads,
                              int32_t phase, int32_t cover_percent, double area_scale, double area_sharp,

@@ -9,7 +9,9 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
 
+#include <mutex>
 #include <string>
 
 #include "../../include/svpflow_b200.h"
@@ -134,8 +136,10 @@ struct MaskJob {
     int32_t *sums;        // per payload: two (mw + 2) x (mh + 2) splat planes
     int *status;
     int32_t flags, gw, gh, mw, mh;
-    int32_t bw, bh, xs, ys, denom, phase, area, sharp_is_one;
+    int32_t bw, bh, xs, ys, denom, phase, area, sharp_is_one, mag_steps;
     double strength, area_scale, area_sharp;
+    // mag_steps: the magnitude byte is the number of these scores at or below the vector's score
+    uint32_t mag_thr[255];
 };
 
 __device__ __forceinline__ bool mask_regions(const MaskJob &J, const uint8_t *p, int64_t &off_prev,
@@ -198,6 +202,11 @@ __global__ void mask_finish_kernel(const MaskJob J) {
         if (blockIdx.x == 0 && threadIdx.x == 0) J.status[f] = 1;
         return;
     }
+    __shared__ uint32_t thr[255];
+    if (J.mag_steps) {  // the whole block takes this branch or returned above
+        for (int k = threadIdx.x; k < 255; k += blockDim.x) thr[k] = J.mag_thr[k];
+        __syncthreads();
+    }
     const int64_t n = (int64_t)J.mw * J.mh;
     const int64_t stride = (int64_t)J.mw + 2, plane = stride * ((int64_t)J.mh + 2);
     const int32_t *acc = J.sums + f * 2 * plane;
@@ -222,9 +231,20 @@ __global__ void mask_finish_kernel(const MaskJob J) {
         if (si >= 0)
             for (int s = 0; s < 2; s++) {
                 const unsigned raw1 = *reinterpret_cast<const unsigned *>(p + (s ? off_cur : off_prev) + si * 8 + 4);
-                double v = __ddiv_rn(__dmul_rn(__dmul_rn(4.0, (double)(raw1 & 0xFFFFFFu)), J.area_scale), area_f);
-                if (!J.sharp_is_one) v = pow(v, J.area_sharp);
-                a[s] = clamp_u8(__dmul_rn(v, 255.0));
+                const unsigned score = raw1 & 0xFFFFFFu;
+                if (J.mag_steps) {  // count the step scores <= score (they ascend)
+                    int lo = 0, hi = 255;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (thr[mid] <= score) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    a[s] = (uint8_t)lo;
+                } else {
+                    double v = __ddiv_rn(__dmul_rn(__dmul_rn(4.0, (double)score), J.area_scale), area_f);
+                    if (!J.sharp_is_one) v = pow(v, J.area_sharp);
+                    a[s] = clamp_u8(__dmul_rn(v, 255.0));
+                }
             }
         out[2 * n + i] = a[0];
         out[3 * n + i] = a[1];
@@ -295,6 +315,39 @@ __global__ void __launch_bounds__(256) scene_class_kernel(const __grid_constant_
         const int high = cnt[1] + cnt[2], mid = high + cnt[3];
         J.classes[f] = cnt[1] >= required ? 3 : (high >= required ? 2 : (mid >= required ? 1 : 0));
     }
+}
+
+// scale_magnitude (renderer.rs:3245-3260) on the host, with libm's pow as the reference
+uint8_t magnitude_byte(uint32_t score, double scale, double sharp, int32_t area) {
+    const double v = pow(4.0 * (double)score * scale / (double)area, sharp) * 255.0;
+    if (!isfinite(v) || v <= 0.0) return 0;
+    if (v >= 255.0) return 255;
+    return (uint8_t)v;
+}
+// For sharp >= 1e-3 and scale >= 0 the byte is a non-decreasing step function of the 24-bit score
+// (scores one apart differ by >= 2^-24 relative, so pow's sub-ulp error cannot reorder them): the
+// smallest score reaching each byte 1..255 (2^24 = never) makes the device result libm's exactly.
+bool magnitude_steps(double scale, double sharp, int32_t area, uint32_t thr[255]) {
+    if (!(sharp >= 1e-3) || !isfinite(sharp) || !(scale >= 0.0) || !isfinite(scale) || area <= 0) return false;
+    static std::mutex mu;
+    static double c_scale = -1.0, c_sharp = -1.0;
+    static int32_t c_area = -1;
+    static uint32_t c_thr[255];
+    std::lock_guard<std::mutex> lk(mu);
+    if (scale != c_scale || sharp != c_sharp || area != c_area) {
+        for (int k = 1; k <= 255; k++) {
+            uint32_t lo = 0, hi = 1u << 24;  // first score in [lo, hi) whose byte reaches k; hi = none
+            while (lo < hi) {
+                const uint32_t mid = lo + ((hi - lo) >> 1);
+                if (magnitude_byte(mid, scale, sharp, area) >= k) hi = mid;
+                else lo = mid + 1;
+            }
+            c_thr[k - 1] = lo;
+        }
+        c_scale = scale; c_sharp = sharp; c_area = area;
+    }
+    memcpy(thr, c_thr, sizeof(c_thr));
+    return true;
 }
 
 bool mask_job(const int32_t *vdata, MaskJob &J, std::string &err) {
@@ -442,6 +495,7 @@ int svpf_render_masks_device(const int32_t *vdata, const uint8_t *payloads_dev, 
     J.area_scale = area_scale;
     J.area_sharp = area_sharp;
     J.sharp_is_one = area_sharp == 1.0;  // pow(x, 1) is x exactly, in libm and here
+    J.mag_steps = magnitude_steps(area_scale, area_sharp, J.area, J.mag_thr) ? 1 : 0;
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t n = (int64_t)J.mw * J.mh, count = (int64_t)J.gw * J.gh;
     const size_t sums = (size_t)npayloads * 2 * ((size_t)J.mw + 2) * ((size_t)J.mh + 2) * sizeof(int32_t);

@@ -222,10 +222,6 @@ def _device_masks(vd, pays, phase, cover, scale, sharp):
     return masks.cpu().numpy().reshape(n, 5, mh, mw), status.cpu().numpy()
 
 
-def _near_integer(v):
-    return np.abs(v - np.round(v)) <= 1e-12 * np.maximum(np.abs(v), 1.0)
-
-
 GPU_CASES = [  # w, h, analyse opt, phases, cover, area scale, area sharp, random spread, big vectors
     (320, 240, "{block:{w:16,overlap:2},main:{search:{type:3,distance:8,satd:true}}}", (0, 77, 128, 256), 100, 1.0,
      1.0, 0, False),
@@ -249,27 +245,54 @@ def test_device_masks_match_oracle(case):
         pays = np.stack([pays[0], _random_field(rng, pays[1], vd, spread, big), pays[2]])
     bad = pays.copy()
     bad[2, 8] ^= 3  # flags word: this payload must not decode
-    mw, mh = orc.vector_grid(vd)
     for phase in phases:
         got, status = _device_masks(vd, bad, phase, cover, scale, sharp)
         assert list(status) == [0, 0, 1]
         assert (got[2] == 3).all(), "an undecodable payload's planes are left as they were"
         for f in range(2):
             want = orc.render_masks(vd, bad[f], phase, cover, scale, sharp)
-            assert np.array_equal(got[f][:2], want[:2]), f"payload {f} phase {phase}: coverage differs"
-            if sharp == 1.0:
-                assert np.array_equal(got[f][2:], want[2:]), f"payload {f}: magnitude differs"
-                continue
-            # CUDA's pow is within 2 ulp of libm's: a byte may move by one only where 255 * value
-            # sits on an integer
-            prev, cur = _sets(bad[f])
-            for k, rec in ((2, prev), (3, cur)):
-                diff = got[f][k] != want[k]
-                if diff.any():
-                    v = _area_values(vd, rec, mw, mh, scale, sharp)
-                    assert (np.abs(got[f][k].astype(int) - want[k])[diff] == 1).all()
-                    assert _near_integer(v[diff]).all(), f"payload {f} plane {k}: {np.argwhere(diff)[:4]}"
-            assert np.array_equal(got[f][4], np.maximum(got[f][2], got[f][3]))
+            assert np.array_equal(got[f], want), f"payload {f} phase {phase}: planes differ"
+
+
+def _magnitude_byte(score, scale, sharp, area):
+    v = math.pow(4.0 * score * scale / area, sharp) * 255.0
+    if not math.isfinite(v) or v <= 0.0:
+        return 0
+    return 255 if v >= 255.0 else int(v)
+
+
+def _steps(scale, sharp, area):
+    """The smallest 24-bit score reaching each magnitude byte 1..255 (2^24: none)."""
+    out = []
+    for k in range(1, 256):
+        lo, hi = 0, 1 << 24
+        while lo < hi:
+            mid = (lo + hi) // 2
+            if _magnitude_byte(mid, scale, sharp, area) >= k:
+                hi = mid
+            else:
+                lo = mid + 1
+        out.append(lo)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scale,sharp", [(0.01, 0.6), (0.002, 2.5), (0.0256, 1.0), (1.0, 1.5), (0.3, 0.25)])
+def test_device_magnitude_bytes_exact_at_every_step(scale, sharp):
+    # scores right at, below and above every step of the byte: the device's step count must give
+    # the oracle's (libm pow) byte at each of them
+    vd, pays, _ = _payloads(w=320, h=240, n=2, aopt="{block:{w:8,overlap:0},main:{search:{type:2,distance:2}}}")
+    count = vd[11] * vd[12]
+    area = max(vd[2], 1) * max(vd[3], 1)
+    steps = sorted({t + d for t in _steps(scale, sharp, area) for d in (-1, 0, 1) if 0 <= t + d < (1 << 24)})
+    scores = np.resize(np.array(steps + [0, (1 << 24) - 1], dtype=np.int64), count)
+    p = pays[0]
+    for region in range(2):
+        p = _with_vectors(p, vd, np.zeros(count), np.zeros(count), np.roll(scores, region), region)
+    got, status = _device_masks(vd, p[None, :], 128, 100, scale, sharp)
+    want = orc.render_masks(vd, p, 128, 100, scale, sharp)
+    assert status[0] == 0
+    assert np.array_equal(got[0][2:], want[2:]), f"{np.argwhere(got[0][2:] != want[2:])[:4]}"
 
 
 @pytest.mark.gpu
