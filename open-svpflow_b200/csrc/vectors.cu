@@ -6,6 +6,7 @@
 // and renderer.rs: vector_planes (:1680-1726), clamp_to_frame (:1728-1736), sample_index
 // (:1870-1874), centered (:3237-3243), as SmoothFps calls them (svpflow2 core.rs:962-1001): the
 // "previous" set falls back to the current one and vice versa.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -19,6 +20,7 @@
 
 namespace {
 
+namespace cg = cooperative_groups;
 constexpr int kNeutral = 1024, kMaxVector = 1023;
 
 struct VecHdr {  // vector_data(), from the 16-int vdata header
@@ -266,32 +268,38 @@ struct SceneJob {
     uint8_t luma[512];  // luma_byte of (a + b) / denom, a + b in 0..510
 };
 
-// grid: (payloads); one CTA reduces one payload's four counts
-__global__ void __launch_bounds__(256) scene_class_kernel(const __grid_constant__ SceneJob J) {
-    __shared__ int cnt[4];  // considered, scene, m2, m1
-    const int64_t f = blockIdx.x;
+// grid: (kSceneCtas x payloads); a cluster of kSceneCtas CTAs reduces one payload: each CTA counts
+// its share of the vectors into the four bins (warp shuffles), adds them into the lead CTA's shared
+// counters through distributed shared memory, and the lead CTA derives the class after the
+// cluster barrier.
+constexpr int kSceneCtas = 8;
+__global__ void __cluster_dims__(kSceneCtas, 1, 1) __launch_bounds__(256)
+    scene_class_kernel(const __grid_constant__ SceneJob J) {
+    __shared__ int cnt[4];  // considered, scene, m2, m1 (the lead CTA's are the payload's)
+    cg::cluster_group cluster = cg::this_cluster();
+    const unsigned rank = cluster.block_rank();
+    const int64_t f = blockIdx.x / kSceneCtas;
     const uint8_t *p = J.payloads + f * J.payload_len;
     const int64_t count = (int64_t)J.gw * J.gh;
+    // the same checks in every CTA of the cluster, so all of them return or none does
     bool ok = true;
     const bool hdr = rd32(p, J.payload_len, 0, ok) == 16 && rd32(p, J.payload_len, 4, ok) == 0xA0 &&
                      rd32(p, J.payload_len, 8, ok) == J.flags;
+    int64_t off_prev = 0, off_cur = 0;
+    const bool sets = (J.flags & 3) != 0;
+    if (ok && hdr && sets) ok = decode_regions(p, J.payload_len, J.flags, count, off_prev, off_cur);
     if (!(ok && hdr)) {
-        if (threadIdx.x == 0) { J.status[f] = 1; J.classes[f] = -1; }
+        if (rank == 0 && threadIdx.x == 0) { J.status[f] = 1; J.classes[f] = -1; }
         return;
     }
-    if ((J.flags & 3) == 0) {  // no vector set: scene_class returns 3
-        if (threadIdx.x == 0) J.classes[f] = 3;
-        return;
-    }
-    int64_t off_prev, off_cur;
-    if (!decode_regions(p, J.payload_len, J.flags, count, off_prev, off_cur)) {
-        if (threadIdx.x == 0) { J.status[f] = 1; J.classes[f] = -1; }
+    if (!sets) {  // no vector set: scene_class returns 3
+        if (rank == 0 && threadIdx.x == 0) J.classes[f] = 3;
         return;
     }
     if (threadIdx.x < 4) cnt[threadIdx.x] = 0;
-    __syncthreads();
+    cluster.sync();  // the lead CTA's counters are zero before anyone adds
     int c[4] = {0, 0, 0, 0};
-    for (int64_t i = threadIdx.x; i < count; i += blockDim.x) {
+    for (int64_t i = (int64_t)rank * blockDim.x + threadIdx.x; i < count; i += (int64_t)kSceneCtas * blockDim.x) {
         const unsigned lp = *reinterpret_cast<const unsigned *>(p + off_prev + i * 8 + 4) >> 24;
         const unsigned wc = *reinterpret_cast<const unsigned *>(p + off_cur + i * 8 + 4);
         const int l = max((int)J.luma[lp + (wc >> 24)], 1);
@@ -303,14 +311,15 @@ __global__ void __launch_bounds__(256) scene_class_kernel(const __grid_constant_
         else if (score >= J.m2) c[2]++;
         else if (score >= J.m1) c[3]++;
     }
+    int *lead = cluster.map_shared_rank(cnt, 0);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         int v = c[k];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt[k], v);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(lead + k, v);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    cluster.sync();  // every CTA's counts are in
+    if (rank == 0 && threadIdx.x == 0) {
         const int required = (int)((unsigned)cnt[0] * (unsigned)J.blocks_pct) / 100;
         const int high = cnt[1] + cnt[2], mid = high + cnt[3];
         J.classes[f] = cnt[1] >= required ? 3 : (high >= required ? 2 : (mid >= required ? 1 : 0));
@@ -534,7 +543,7 @@ int svpf_scene_class_device(const int32_t *vdata, const uint8_t *payloads_dev, s
         return SVPF_EINVAL;
     }
     if (npayloads <= 0) return SVPF_OK;
-    if (!payloads_dev || !classes_dev || !status_dev || payload_len < 0x40 || npayloads > INT32_MAX / 2) {
+    if (!payloads_dev || !classes_dev || !status_dev || payload_len < 0x40 || npayloads > (1 << 24)) {
         svpf::set_last_error("bad buffers");
         return SVPF_EINVAL;
     }
@@ -564,7 +573,7 @@ int svpf_scene_class_device(const int32_t *vdata, const uint8_t *payloads_dev, s
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(status_dev, 0, sizeof(int32_t) * (size_t)npayloads, st);
     if (e == cudaSuccess) {
-        scene_class_kernel<<<(unsigned)npayloads, 256, 0, st>>>(J);
+        scene_class_kernel<<<(unsigned)npayloads * kSceneCtas, 256, 0, st>>>(J);
         svpf::add_launches(1);
         e = cudaGetLastError();
     }
