@@ -421,6 +421,39 @@ def run_render(args, world: int, rank: int, local: int):
         kms.append(e0.elapsed_time(e1))
     masked_value = nf / (statistics.mean(mms) / 1000.0)
     masks_us_per_payload = statistics.mean(kms) * 1000.0 / nf
+    # algorithm 23 as SmoothFps feeds it (frames 1..nf-2): frame f's two sets, the next payload's
+    # previous set and the previous payload's current set, the coverage masks of frame f and the max
+    # magnitude mask, on the mask planes made above
+    m23_d = torch.empty_like(out_d)
+
+    def m23_frame(f, st):
+        pl_ = [planes[k].data_ptr() for k in (f - 1, f, f + 1)]
+        sets = [(pl_[1], pl_[1] + 2 * nm), (pl_[1] + 4 * nm, pl_[1] + 6 * nm), (pl_[2], pl_[2] + 2 * nm),
+                (pl_[0] + 4 * nm, pl_[0] + 6 * nm)]
+        mk = masks_d[f].data_ptr()
+        sv.render_mode23_device(cfg, thr, True, [sup_d[f].data_ptr() + o for o in offs], strides, lens,
+                                [sup_d[f + 1].data_ptr() + o for o in offs], strides, lens, 1, sets, (mk, mk + nm),
+                                mk + 4 * nm, [m23_d[f].data_ptr() + o for o in dst_offs], strides, stream=st)
+
+    for f in range(1, nf - 1):
+        m23_frame(f, sh)
+    torch.cuda.synchronize()
+    m23_graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(m23_graph):
+        cs = torch.cuda.current_stream().cuda_stream
+        for f in range(1, nf - 1):
+            m23_frame(f, cs)
+    torch.cuda.synchronize()
+    m23_ms = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m23_graph.replay()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        m23_ms.append(e0.elapsed_time(e1))
+    m23_value = (nf - 2) / (statistics.mean(m23_ms) / 1000.0)
     # the scene class of every payload (one launch), timed the same way
     scls = torch.empty(nf, dtype=torch.int32, device=dev)
     sstat = torch.empty(nf, dtype=torch.int32, device=dev)
@@ -519,6 +552,27 @@ def run_render(args, world: int, rank: int, local: int):
         for f, (om, res) in enumerate(masked_res):
             masked_ok &= bool(np.array_equal(masks_np[f], om)) and bool(
                 np.array_equal(np.concatenate([r.reshape(-1) for r in res]), masked_np[f]))
+        m23_np = m23_d.cpu().numpy()
+
+        def cpu_m23(f):
+            om = orc.render_masks(vd, pay_np[f], thr, 100, ascale)
+            res = []
+            for p in range(3):
+                ph = h // (2 if p else 1)
+                srcs = [sup_np[f][offs[p]: offs[p] + lens[p]], sup_np[f + 1][offs[p]: offs[p] + lens[p]]]
+                motions = [(mot_np[f][0], mot_np[f][1]), (mot_np[f][2], mot_np[f][3]),
+                           (mot_np[f + 1][0], mot_np[f + 1][1]), (mot_np[f - 1][2], mot_np[f - 1][3])]
+                res.append(orc.render_mode23_plane(ocfg, p > 0, True, thr, srcs, [strides[p]] * 2,
+                                                   [strides[p] * ph] * 2, 1, motions, (om[0], om[1]), om[4],
+                                                   strides[p], ph))
+            return res
+
+        t0 = time.perf_counter()
+        m23_res = [cpu_m23(f) for f in (1, 2)]
+        m23_cpu = 2 / (time.perf_counter() - t0)
+        m23_check = {"frames_checked": 2, "bit_exact": all(
+            np.array_equal(np.concatenate([r.reshape(-1) for r in m23_res[i]]), m23_np[f])
+            for i, f in enumerate((1, 2))), "oracle_frames_per_s_one_thread": m23_cpu}
         scls_np = scls.cpu().numpy()
         scene_check = {"payloads_checked": nf, "bit_exact": bool(all(
             int(scls_np[f]) == orc.scene_class(vd, pay_np[f]) for f in range(nf)))}
@@ -579,6 +633,11 @@ def run_render(args, world: int, rank: int, local: int):
                                      f"scale {ascale}) + svpf_render_masked_device per frame (algorithm 21, final "
                                      "mask = max magnitude), one CUDA-graph replay per step, same timing",
                               "parity_vs_oracle": masked_check},
+            "mode23": {"value": m23_value, "unit": "frames/s",
+                       "how": f"svpf_render_mode23_device for frames 1..{nf - 2} (frame f's sets, the next "
+                              "payload's previous set, the previous payload's current set; frame f's coverage "
+                              "masks and max magnitude mask), one CUDA-graph replay per step, same timing",
+                       "parity_vs_oracle": m23_check},
             "scene_class": {"us_per_payload": scene_us_per_payload, "how": f"svpf_scene_class_device over the {nf} "
                             "payloads, one launch, CUDA events, L2 flushed before", "parity_vs_oracle": scene_check},
         }

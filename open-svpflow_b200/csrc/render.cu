@@ -17,7 +17,8 @@
 // column and a top row of width / height origin) and writes each tile's samples; here one thread
 // owns kPx consecutive output samples of a row and finds their tile arithmetically: the last tile
 // in the reference's loop order that covers them, since a later tile overwrites an earlier one where
-// they overlap. The tile's motion is fetched once when the thread's samples share it.
+// they overlap. The tile's motion is fetched once when the thread's samples share it; a thread runs
+// kBatch batches of kPx samples and keeps the tile state between them.
 //
 // 32-bit arithmetic as the reference's scalar loops. Its x86-64 SSE tile paths keep 16-bit lanes,
 // which give the same values for thresholds 0..256 (|motion| <= 1024, weights <= 32, mask values
@@ -33,7 +34,8 @@
 namespace {
 
 constexpr int kLut = 2048, kMaxBlock = 32;
-constexpr int kPx = 4;  // output samples per thread
+constexpr int kPx = 4;     // output samples per batch
+constexpr int kBatch = 2;  // batches per thread: the tile state carries over when they share a tile
 
 struct Source {  // a plain plane (shift 0) or a super clip's level 0 (sub-planes `span` bytes apart)
     const uint8_t *p;
@@ -268,9 +270,13 @@ __device__ __forceinline__ int32_t alpha_at(const RenderJob &J, const RenderPlan
 // max_mask when MASK). KIND 2: algorithms 21 / 22 (the same reads; mode21_or_22_pixel with alphas from
 // masks a and b, and the final mask when MASK). KIND 3: algorithm 23 (sets base0, base1, next0, prev1,
 // set k reading source k & 1; mode23_pixel with masks a and b, and the final mask when MASK).
-// Grid: (row length of the widest plane / (256 kPx), rows of the tallest plane, 3 planes).
+// Grid: (row length of the widest plane / (256 kPx kBatch), rows of the tallest plane, 3 planes).
+// Resident CTAs per SM the registers are budgeted for, per kind, as measured on 1080p frames: the
+// masked two-source kinds gain a third CTA at 80 registers (algorithm 21: +31 %); algorithm 23
+// spills at 80 and keeps two.
 template <int KIND, bool MASK>
-__global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ RenderJob J) {
+__global__ void __launch_bounds__(256, KIND == 0 ? (MASK ? 4 : 5) : (KIND == 1 ? (MASK ? 3 : 4) : (KIND == 2 ? 3 : 2)))
+    render_kernel(const __grid_constant__ RenderJob J) {
     constexpr bool DUAL = KIND > 0;
     constexpr int NS = KIND == 0 ? 1 : (KIND == 3 ? 4 : 2);          // motion sets
     constexpr int NA = KIND >= 2 ? (MASK ? 3 : 2) : (MASK ? 1 : 0);  // alphas per sample
@@ -283,15 +289,12 @@ __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ Ren
     }
     __syncthreads();
     const int32_t py = blockIdx.y;
-    const int32_t px0 = (blockIdx.x * blockDim.x + threadIdx.x) * kPx;
-    if (px0 >= p.width || py >= p.height || p.block_w <= 0 || p.block_h <= 0) return;
+    const int32_t pxa = (blockIdx.x * blockDim.x + threadIdx.x) * (kPx * kBatch);
+    if (pxa >= p.width || py >= p.height || p.block_w <= 0 || p.block_h <= 0) return;
     int32_t gy, by, th;
     tile_of(py, p.origin_y, p.block_h, p.bh_log2, p.height, J.grid_h, gy, by, th);
-    const int32_t pxl = min(px0 + kPx - 1, p.width - 1);
-    int32_t gx, bx, tw, gxl, bxl, twl;
-    tile_of(px0, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gx, bx, tw);
-    tile_of(pxl, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gxl, bxl, twl);
-    const bool shared_tile = gx == gxl;  // usually: then the tile's motion is fetched once
+    int32_t gx, bx, tw;
+    tile_of(pxa, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gx, bx, tw);
     Tile t = make_tile(J, gx, bx, tw, gy, by, th);
     SetRow r[NS];
 #pragma unroll
@@ -308,7 +311,26 @@ __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ Ren
         return d;
     };
     bool direct = direct_of();
-    // indices first, then every load of the thread's samples, so the gathers overlap
+    for (int bt = 0; bt < kBatch; bt++) {
+    const int32_t px0 = pxa + bt * kPx;
+    if (px0 >= p.width) break;
+    const int32_t pxl = min(px0 + kPx - 1, p.width - 1);
+    int32_t gxl, bxl, twl;
+    if (bt > 0) {  // the batch's first sample may start another tile
+        tile_of(px0, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gxl, bxl, twl);
+        if (gxl != gx) {
+            gx = gxl;
+            t = make_tile(J, gxl, bxl, twl, gy, by, th);
+#pragma unroll
+            for (int q = 0; q < NS; q++) r[q] = set_row(J, p, t, q, py, syw);
+#pragma unroll
+            for (int a = 0; a < NA; a++) mask_row(J, p, t, py, syw, sel_of(a), m0[a], m1[a]);
+            direct = direct_of();
+        }
+    }
+    tile_of(pxl, p.origin_x, p.block_w, p.bw_log2, p.width, J.grid_w, gxl, bxl, twl);
+    const bool shared_tile = gx == gxl;  // usually: then the tile's motion is fetched once
+    // indices first, then every load of the batch's samples, so the gathers overlap
     int64_t idx[NS][kPx];
     int32_t alpha[NA > 0 ? NA : 1][kPx];
 #pragma unroll
@@ -380,6 +402,7 @@ __global__ void __launch_bounds__(256) render_kernel(const __grid_constant__ Ren
 #pragma unroll
     for (int k = 0; k < kPx; k++)
         if (px0 + k <= pxl) dst[k] = (uint8_t)out[k];
+    }
 }
 
 // Per-plane constants of one frame (plane_params for chroma = plane > 0), the sources' layouts and
@@ -462,7 +485,7 @@ int launch(const RenderJob &J, int kind, bool mask, int32_t most_w, int32_t most
         }
     cudaError_t e = cudaSuccess;
     if (most_w > 0 && most_h > 0) {
-        dim3 grid((unsigned)((most_w + 256 * kPx - 1) / (256 * kPx)), (unsigned)most_h, 3);
+        dim3 grid((unsigned)((most_w + 256 * kPx * kBatch - 1) / (256 * kPx * kBatch)), (unsigned)most_h, 3);
         cudaStream_t st = (cudaStream_t)stream;
         if (kind == 3) {
             if (mask) render_kernel<3, true><<<grid, 256, 0, st>>>(J);
