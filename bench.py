@@ -70,7 +70,7 @@ UNIT = "frame-pairs/s"
 TRAFFIC_PER_PAIR = 341.8e6 / 17
 # DRAM bytes of one 1080p render launch with the 8 x 8 effective block (ncu capture: 4.13 MB read,
 # the written frame stays in L2)
-RENDER_TRAFFIC_PER_FRAME = 4.13e6
+RENDER_TRAFFIC_PER_FRAME = 4.14e6
 # graph replays per timed render step (about 40 ms, so the clock sampler sees the step)
 RENDER_REPLAYS = 48
 # int32 lanes per SM on sm_100 and the SM clock ceiling, for the nominal integer peak
@@ -622,7 +622,7 @@ def run_render(args, world: int, rank: int, local: int):
                                            "frame; the output stays in L2), x frames per step",
                          "peak_source": peak_kind, "algorithmic_bytes_per_frame": per_frame,
                          "note": "issue-bound, not HBM-bound: per sample a tile lookup, motion interpolation and "
-                                 "an index computation (72 % issue active in the ncu capture)"},
+                                 "an index computation (67 % issue active in the ncu capture)"},
             "cpu_baseline": cpu, "parity_vs_oracle": parity,
             "blend_mode13": {"value": blend_value, "unit": "frames/s", "kernel": "render_kernel<dual>",
                              "how": "svpf_render_blend_device (algorithm 13: frames f and f+1, the two vector sets "
