@@ -127,8 +127,8 @@ __global__ void vector_planes_kernel(const PlaneJob J) {
 // renderer.rs coverage_mask (:1738-1763) = splat_coverage (:2945-3062) + window_3x3 (:3064-3100) +
 // finish_coverage (:3102-3134), and magnitude_mask (:1647-1678) with scale_magnitude (:3245-3260).
 // The splat's weights are >= 0 when 0 <= overlap < block, so every partial sum is bounded by
-// grid_w * grid_h * block area; the host admits only fields where that is <= INT32_MAX, which makes
-// the reference's saturating and wrapping adds plain adds and the atomic sums order-independent.
+// grid_w * grid_h * block area; the host admits only fields where that is <= 2^30, which makes the
+// reference's saturating and wrapping adds plain adds and the atomic sums order-independent.
 // TruncDiv (:3149-3184) divides exactly (truncating), so plain '/' restates it.
 
 struct MaskJob {
