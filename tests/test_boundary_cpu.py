@@ -130,8 +130,17 @@ def test_compute_entry_points_fail_loudly_without_a_gpu():
     sb = sv.Super(64, 48, "{pel:2}")
     an = sv.Analyse(sb.sdata, "{block:{w:8}}", 64, 48)
     frames = np.zeros((2, sb.source_len()), np.uint8)
-    for call in (lambda: sb.build_many(frames), lambda: an.analyse_clip(sb, frames),
-                 lambda: sv.Batch([(sb, an, 2)]), lambda: sv.Server(1 << 30)):
+    vd = an.vector_header()
+    cfg = dict(width=64, height=48, block_w=8, block_h=8, origin_x=4, origin_y=4, grid_w=8, grid_h=6, source_step=1)
+    calls = (lambda: sb.build_many(frames), lambda: an.analyse_clip(sb, frames),
+             lambda: sv.Batch([(sb, an, 2)]), lambda: sv.Server(1 << 30),
+             # the payload consumers refuse before touching their (here dummy) device pointers
+             lambda: sv.vector_planes_device(vd, 16, 4096, 1, 64, 48, 16, 16),
+             lambda: sv.render_masks_device(vd, 16, 4096, 1, 128, 16, 16, 16),
+             lambda: sv.scene_class_device(vd, 16, 4096, 1, 16, 16),
+             lambda: sv.render_warp_device(cfg, 128, False, True, [16] * 3, [64, 32, 32], [1] * 3, 0, 16, 16,
+                                           [16] * 3, [64, 32, 32]))
+    for call in calls:
         with pytest.raises(sv.SvpfError, match="no CUDA device") as e:
             call()
         assert e.value.code == sv.SVPF_ECUDA
