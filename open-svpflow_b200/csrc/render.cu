@@ -272,8 +272,8 @@ __device__ __forceinline__ int32_t alpha_at(const RenderJob &J, const RenderPlan
 // set k reading source k & 1; mode23_pixel with masks a and b, and the final mask when MASK).
 // Grid: (row length of the widest plane / (256 kPx kBatch), rows of the tallest plane, 3 planes).
 // Resident CTAs per SM the registers are budgeted for, per kind, as measured on 1080p frames: the
-// masked two-source kinds gain a third CTA at 80 registers (algorithm 21: +31 %); algorithm 23
-// spills at 80 and keeps two.
+// masked two-source kinds gain a third CTA at 80 registers (algorithm 21: +31 %; a fourth at 64
+// spills and loses 4 %); algorithm 23 spills at 80 and keeps two.
 template <int KIND, bool MASK>
 __global__ void __launch_bounds__(256, KIND == 0 ? (MASK ? 4 : 5) : (KIND == 1 ? (MASK ? 3 : 4) : (KIND == 2 ? 3 : 2)))
     render_kernel(const __grid_constant__ RenderJob J) {
