@@ -554,6 +554,38 @@ def test_oracle_identity_and_shift(interp):
     assert np.array_equal(got, src[ys, xs])
 
 
+@pytest.mark.parametrize("interp", [False, True])
+def test_oracle_dual_known_answers(interp):
+    # zero motion: both warps read the undisplaced samples a (frame 0) and b (frame 1), so
+    # algorithms 11 and 13 give blend_256(a, b, t); 21 / 22 with masks 0 give blend_256(a, b, t) too
+    # (blend_255(v, _, 0) = v), with masks 255 blend_256(b, a, t); 23 with its four zero sets and
+    # masks 0 gives blend_256(a, b, t) again
+    w, h, blk = 64, 48, 16
+    gw, gh = _grid(w, h, blk, blk)
+    cfg = _cfg(w, h, blk, blk, gw, gh)
+    rng = np.random.default_rng(4)
+    a = rng.integers(0, 256, size=(h, w), dtype=np.uint8)
+    b = rng.integers(0, 256, size=(h, w), dtype=np.uint8)
+    zero = (np.full(gw * gh, 1024, np.uint16), np.full(gw * gh, 1024, np.uint16))
+    m0, m255 = np.zeros(gw * gh, np.uint8), np.full(gw * gh, 255, np.uint8)
+    A, B = a.astype(np.int64), b.astype(np.int64)
+    for t in (0, 77, 128, 256):
+        want = ((A * (256 - t) + B * t) >> 8).astype(np.uint8)
+        swap = ((B * (256 - t) + A * t) >> 8).astype(np.uint8)
+        common = (cfg, False, interp, not interp)
+        for mode in (11, 13):
+            got = orc.render_dual_plane(*common, mode, t, [a, b], [w, w], [0, 0], 0, zero, zero, w, h)
+            assert np.array_equal(got, want), (mode, t)
+        for mode in (21, 22):
+            got = orc.render_dual_plane(*common, mode, t, [a, b], [w, w], [0, 0], 0, zero, zero, w, h, (m0, m0))
+            assert np.array_equal(got, want), (mode, t)
+        got = orc.render_dual_plane(*common, 21, t, [a, b], [w, w], [0, 0], 0, zero, zero, w, h, (m255, m255))
+        assert np.array_equal(got, swap), t
+        got = orc.render_mode23_plane(cfg, False, interp, t, [a, b], [w, w], [0, 0], 0, [zero] * 4, (m0, m0), None,
+                                      w, h)
+        assert np.array_equal(got, want), t
+
+
 def test_oracle_super_subplanes():
     # on a pel-2 super clip, a half-pel horizontal motion reads the h sub-plane at full-pel positions
     w, h, blk = 64, 48, 16
