@@ -276,6 +276,22 @@ def _steps(scale, sharp, area):
     return out
 
 
+@pytest.mark.parametrize("scale,sharp,area", [(0.01, 0.6, 256), (0.002, 2.5, 64), (0.0256, 1.0, 256),
+                                              (1.0, 1.5, 1024), (0.3, 0.25, 64), (0.05, 0.001, 256)])
+def test_magnitude_byte_is_a_step_function_of_the_score(scale, sharp, area):
+    # the premise of the device's exact magnitude bytes: with libm's pow the byte never decreases as
+    # the 24-bit score grows, so counting the step scores at or below a score gives its byte
+    import bisect
+
+    steps = _steps(scale, sharp, area)
+    assert steps == sorted(steps)
+    rng = np.random.default_rng(1)
+    sample = set(rng.integers(0, 1 << 24, size=20000).tolist())
+    sample |= {t + d for t in steps for d in (-2, -1, 0, 1, 2) if 0 <= t + d < (1 << 24)}
+    for sc in sorted(sample):
+        assert _magnitude_byte(sc, scale, sharp, area) == bisect.bisect_right(steps, sc), sc
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("scale,sharp", [(0.01, 0.6), (0.002, 2.5), (0.0256, 1.0), (1.0, 1.5), (0.3, 0.25)])
 def test_device_magnitude_bytes_exact_at_every_step(scale, sharp):
