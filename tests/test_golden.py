@@ -1,5 +1,8 @@
 """Frozen digests (tests/golden/oracle_digests.json, made by tests/golden/make_golden.py):
-the oracle must keep producing them (CPU), and the GPU path must produce the same bytes."""
+the oracle must keep producing them (CPU), and the GPU path must produce the same bytes. The
+payload consumers' digests (tests/golden/consumer_digests.json, made by
+tests/golden/make_consumer_golden.py) guard the oracle's vector planes, mask planes, scene classes
+and renders the same way."""
 import hashlib
 import json
 import os
@@ -7,10 +10,17 @@ import os
 import numpy as np
 import pytest
 
+from golden import make_consumer_golden as consumers
 from golden.make_golden import CASES, compute
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = json.load(open(os.path.join(HERE, "golden", "oracle_digests.json")))["cases"]
+CGOLD = json.load(open(os.path.join(HERE, "golden", "consumer_digests.json")))["cases"]
+
+
+@pytest.mark.parametrize("name", sorted(consumers.CASES))
+def test_oracle_consumers_match_frozen_digests(name):
+    assert consumers.compute(name) == CGOLD[name]
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
