@@ -399,6 +399,7 @@ def analyse_from_opt(opt, sdata, src_w=0, src_h=0):
     o.refine_search_type = as_i32(first(int_at(ref0, ("search", "type")) if ref0 is not None else None, o.search_type))
     o.refine_distance = as_i32(first(int_at(ref0, ("search", "distance")) if ref0 is not None else None, o.distance))
     o.refine_satd = first(bool_at(ref0, ("search", "satd")) if ref0 is not None else None, o.fine_satd)
+    o.sort = first(bool_at(t, ("main", "search", "sort")), bool_at(t, ("sort",)), True)
     levels = max(min(auto_search_levels(w, h, bw, bh, ox, oy), lv), 1)
     ml = int_at(t, ("main", "levels"))
     if ml is not None and ml > 0:
@@ -1052,8 +1053,69 @@ def rescale(field, w, h, blk):
         v[2] = (sc & U32) & 0xFFFFFF
 
 
+def exact_clip(mv, bounds):  # :1269-1273
+    a, b, c, d = bounds
+    return min(max(mv[0], a), max(c - 1, a)), min(max(mv[1], b), max(d - 1, b))
+
+
+def recalculate(S, R, o, field, ogw, ogh):
+    """exact_recalculate (:1326-1451): the level-0 field resampled onto blocks of half the size,
+    each re-searched from its bilinear-interpolated parent vector when the parent's score is high."""
+    if o.refine_thsad is None:
+        return field
+    obw, obh, oox, ooy = o.block_w, o.block_h, o.overlap_x, o.overlap_y
+    bw, bh, ox, oy = output_block(o)
+    gw, gh = grid(o, bw, bh, ox, oy)
+    osx, osy = max(obw - oox, 1), max(obh - ooy, 1)
+    sx, sy = max(bw - ox, 1), max(bh - oy, 1)
+    pel = max(o.pel, 1)
+    lw, lh = S.size(0)
+    out = [None] * (gw * gh)
+
+    def get(x, y):
+        return field[min(max(y, 0), ogh - 1) * ogw + min(max(x, 0), ogw - 1)]
+
+    for by in range(gh):
+        backwards = o.sort and by & 1
+        for pos in range(gw):
+            bx = gw - 1 - pos if backwards else pos
+            cx, cy = tdiv(bw, 2) + sx * bx, tdiv(bh, 2) + sy * by
+            px0, py0 = tdiv(cx - tdiv(obw, 2), osx), tdiv(cy - tdiv(obh, 2), osy)
+            dxw = max(cx - (tdiv(obw, 2) + osx * px0), 0)
+            dyw = max(cy - (tdiv(obh, 2) + osy * py0), 0)
+            corners = (get(px0, py0), get(px0 + 1, py0), get(px0, py0 + 1), get(px0 + 1, py0 + 1))
+
+            def bilinear(k):  # i64 with div_euclid (floor, the divisors are positive)
+                a, b, c, d = (v[k] for v in corners)
+                top = a * osx + dxw * (b - a)
+                bottom = c * osx + dxw * (d - c)
+                return (top + (dyw * (bottom - top)) // osy) // osx
+
+            mv = (as_i32(bilinear(0)), as_i32(bilinear(1)))
+            parent = tdiv(bilinear(2) * (bw * bh), obw * obh)  # i64 `/` truncates
+            border = bx == 0 or by == 0 or bx == gw - 1 or by == gh - 1
+            factor = 3 if border and bw > 4 else 1
+            ebw, ebh = (tdiv(bw, 2), tdiv(bh, 2)) if factor == 3 else (bw, bh)
+            epx = bx * sx + (tdiv(bw, 4) if factor == 3 else 0)
+            epy = by * sy + (tdiv(bh, 4) if factor == 3 else 0)
+            bounds = mv_bounds(epx, epy, ebw, ebh, lw, lh, pel)
+            pred = exact_clip(mv, bounds)
+            best = [pred, min(max(parent, 0), U32), max(parent, 0)]
+            if parent > tdiv(o.refine_thsad, factor):
+                sad = exact_sad(S, R, 0, epx, epy, ebw, ebh, pred, o.refine_satd, pel, True)
+                best = [pred, sad, sad]
+                c = Ctx()
+                c.S, c.R, c.level, c.px, c.py, c.bw, c.bh, c.pel = S, R, 0, epx, epy, ebw, ebh, pel
+                c.satd, c.chroma, c.pred, c.bounds = o.refine_satd, True, pred, bounds
+                c.lam = 0 if by == 0 else tdiv(o.lambda_ >> 2, factor)
+                c.pnew = tdiv(o.pnew, factor)
+                refine(c, o.refine_search_type, abs(o.refine_distance), best)
+            out[by * gw + bx] = [i16(best[0][0]), i16(best[0][1]), sat_u32(best[1] * factor),
+                                 luma_dc(S, 0, epx, epy, ebw, ebh)]
+    return out
+
+
 def analyse_pair(cur: Planes, ref: Planes, o):
-    assert o.refine_thsad is None, "refine pass not restated in the small oracle"
     dirs = [d for d, bit in ((0, 2), (1, 1)) if o.vectors & bit]
     bidir = len(dirs) == 2
     st = {d: dict(field=None, order=[], glob=(0, 0), proj=None) for d in dirs}
@@ -1079,6 +1141,9 @@ def analyse_pair(cur: Planes, ref: Planes, o):
                 reorder(s["order"], s["next"], gw, gh, o.block_w, o.block_h)
             s["field"] = s["next"]
         fgw, fgh = gw, gh
+    for d in dirs:
+        a, b = (cur, ref) if d == 0 else (ref, cur)
+        st[d]["field"] = recalculate(a, b, o, st[d]["field"], fgw, fgh)
     bw = output_block(o)[0]
     for d in dirs:
         rescale(st[d]["field"], o.width, o.height, bw)

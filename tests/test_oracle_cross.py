@@ -18,6 +18,12 @@ CASES = [
     (64, 48, 6, "{pel:2}", "{vectors:2,block:{w:8,overlap:1},main:{penalty:{pnew:-40},search:{type:3,distance:5}}}"),
     (96, 64, 7, "{pel:1}", "{block:{w:16,overlap:3},main:{search:{type:3,distance:8,coarse:{bad:{sad:1,range:3}}}}}"),
     (64, 48, 8, "{pel:2}", "{main:{search:{distance:0}}}"),
+    # refine[0].thsad set: exact_recalculate onto half-size blocks (the second restatement's own copy)
+    (64, 48, 9, "{pel:2}", "{refine:[{thsad:200,search:{type:2,distance:3,satd:true}}]}"),
+    (96, 64, 10, "{pel:2}", "{block:{w:16,overlap:2},main:{search:{type:3,distance:6}},refine:[{thsad:50}]}"),
+    (64, 48, 11, "{pel:4}", "{block:{w:8,overlap:0},refine:[{thsad:0,search:{type:4,distance:2}}]}"),
+    (96, 64, 12, "{pel:1}", "{vectors:1,block:{w:32,overlap:1},refine:[{thsad:100,search:{type:3,distance:8}}]}"),
+    (80, 48, 13, "{pel:2}", "{main:{search:{sort:false}},refine:[{thsad:20,search:{type:2,distance:2}}]}"),
 ]
 
 
