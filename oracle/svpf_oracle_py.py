@@ -942,6 +942,37 @@ def luma_dc(S, level, px, py, bw, bh):
     return 0 if n == 0 else min(s // n, 255)
 
 
+def plane_activity(data, stride, row, x, width, height, satd):  # :1517-1553
+    area = width * height
+    vals = [[data[(row + y) * stride + x + i] for i in range(width)] for y in range(height)]
+    mean = (sum(map(sum, vals)) & U32) // area
+    if not satd:
+        return (sum(abs(v - mean) for r in vals for v in r) & U32) // area
+    total = 0
+    for y in range(0, height, 4):
+        for x0 in range(0, width, 4):
+            d = [data[(row + y + dy) * stride + x + x0 + dx] - mean for dy in range(4) for dx in range(4)]
+            total += had4(d)
+    return ((total & U32) >> 1) // area
+
+
+def block_activity(S, level, px, py, bw, bh, satd):  # :1486-1515
+    lw, lh = S.size(level)
+    x = px - (1 if level > 0 and px + bw >= lw else 0)
+    y = py - (1 if level > 0 and py + bh >= lh else 0)
+    luma = plane_activity(S.y, S.ys, S.yoff(level) + y, x, bw, bh, satd)
+    cw, ch = tdiv(bw, 2), tdiv(bh, 2)
+    u = plane_activity(S.u, S.cs, S.coff(level) + tdiv(py, 2), tdiv(px, 2), cw, ch, satd)
+    v = plane_activity(S.v, S.cs, S.coff(level) + tdiv(py, 2), tdiv(px, 2), cw, ch, satd)
+    return (luma + u + v) & U32
+
+
+def adaptive_radius(radius, activity):  # :1478-1484
+    if activity < 2:
+        return 0
+    return ((radius * min(((255 * activity) & U32) // 150, 255)) >> 8) + 1
+
+
 def search_level(S, R, o, level, glob, prev, field, gw, gh, order):
     bw0, bh0 = o.block_w, o.block_h
     stx, sty = max(bw0 - o.overlap_x, 1), max(bh0 - o.overlap_y, 1)
@@ -982,7 +1013,8 @@ def search_level(S, R, o, level, glob, prev, field, gw, gh, order):
             lv = float("nan")
         lam = f64_as_i32(21474836.47 if lv != lv else min(lv, 21474836.47))
         radius = base_r
-        assert not (level > 0 and o.coarse_distance < 0), "adaptive radius not restated in the small oracle"
+        if level > 0 and o.coarse_distance < 0:
+            radius = adaptive_radius(base_r, block_activity(S, level, px, py, bw, bh, satd))
         seeds = [(field[ny * gw + nx][0], field[ny * gw + nx][1])
                  for ny in range(max(by - 1, 0), min(by + 1, gh - 1) + 1)
                  for nx in range(max(bx - 1, 0), min(bx + 1, gw - 1) + 1) if (nx, ny) in done]

@@ -24,6 +24,9 @@ CASES = [
     (64, 48, 11, "{pel:4}", "{block:{w:8,overlap:0},refine:[{thsad:0,search:{type:4,distance:2}}]}"),
     (96, 64, 12, "{pel:1}", "{vectors:1,block:{w:32,overlap:1},refine:[{thsad:100,search:{type:3,distance:8}}]}"),
     (80, 48, 13, "{pel:2}", "{main:{search:{sort:false}},refine:[{thsad:20,search:{type:2,distance:2}}]}"),
+    # coarse.distance < 0: the coarse levels' radius adapts to each block's activity (SAD / SATD forms)
+    (96, 64, 14, "{pel:2}", "{block:{w:8,overlap:0},main:{search:{type:2,distance:2,coarse:{distance:-6}}}}"),
+    (96, 64, 15, "{pel:2}", "{main:{search:{type:3,distance:4,coarse:{distance:-8,satd:false,type:3}}}}"),
 ]
 
 
