@@ -11,11 +11,18 @@ import numpy as np
 import pytest
 
 from golden import make_consumer_golden as consumers
+from golden import make_golden16 as golden16
 from golden.make_golden import CASES, compute
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = json.load(open(os.path.join(HERE, "golden", "oracle_digests.json")))["cases"]
 CGOLD = json.load(open(os.path.join(HERE, "golden", "consumer_digests.json")))["cases"]
+GOLD16 = json.load(open(os.path.join(HERE, "golden", "oracle16_digests.json")))["cases"]
+
+
+@pytest.mark.parametrize("name", sorted(golden16.CASES))
+def test_oracle16_matches_frozen_digests(name):
+    assert golden16.compute(name) == GOLD16[name]
 
 
 @pytest.mark.parametrize("name", sorted(consumers.CASES))
