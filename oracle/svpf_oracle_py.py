@@ -17,6 +17,14 @@ U64 = (1 << 64) - 1
 U32 = (1 << 32) - 1
 I32MAX, I32MIN = (1 << 31) - 1, -(1 << 31)
 I64MAX = (1 << 63) - 1
+# sample width: 8-bit as the reference; set_sample_bits(10) gives this project's 10-bit extension
+# (uint16 samples: clamps at 1023, chroma default 512, payload block luma = mean >> 2)
+PX_MAX, PX_MID, DC_SHIFT = 255, 128, 0
+
+
+def set_sample_bits(bits: int):
+    global PX_MAX, PX_MID, DC_SHIFT
+    PX_MAX, PX_MID, DC_SHIFT = (1023, 512, 2) if bits > 8 else (255, 128, 0)
 
 
 def us(v):  # `i32 as usize` / wrapping usize arithmetic
@@ -230,13 +238,13 @@ def _reduce(buf, stride, drow0, dw, dh, srow0, sw, sh):
         else:
             st = sy - 2
             rows.append([min((smp(st, x) + smp(st + 5, x) + 5 * (smp(st + 1, x) + smp(st + 4, x))
-                              + 10 * (smp(st + 2, x) + smp(st + 3, x)) + 16) >> 5, 255) for x in range(sw)])
+                              + 10 * (smp(st + 2, x) + smp(st + 3, x)) + 16) >> 5, PX_MAX) for x in range(sw)])
     for dy in range(dh):
         row = rows[dy]
         _h6(row, dw)
         base = (drow0 + dy) * stride
         n = min(sw, max(len(buf) - base, 0))
-        buf[base:base + n] = bytes(row[:n])
+        buf[base:base + n] = row[:n]
 
 
 def _h6(row, dw):
@@ -257,7 +265,7 @@ def _h6(row, dw):
         pk = src[k] if k < n else src[n - 1]
         v = (left + pk + 10 * (g(src, k - 3, 0) + g(src, k - 2, 0)) + 5 * (g(src, k - 4, 0) + g(src, (k - 1) & ~1, 0))
              + 16) >> 5
-        row[i + 1] = min(v, 255)
+        row[i + 1] = min(v, PX_MAX)
         left = g(src, k - 3, 0)
     for i in range(max(dw - 1, 1), dw):
         a = g(src, 2 * i, 0)
@@ -280,7 +288,7 @@ def _bilinear(d, s, r0, w, h):
             if (V + y) * s + x < L:
                 d[(V + y) * s + x] = avg(a, b)
     n = min(w, max(L - V * s, 0), max(L - r0 * s, 0))
-    d[V * s:V * s + n] = bytes(d[r0 * s:r0 * s + n])
+    d[V * s:V * s + n] = d[r0 * s:r0 * s + n]
     for y in range(h):
         for x in range(w):
             a = get(d, (r0 + y) * s + x, 0)
@@ -288,14 +296,14 @@ def _bilinear(d, s, r0, w, h):
             if (HV + y) * s + x < L:
                 d[(HV + y) * s + x] = avg(a, b)
     n = min(w, max(L - HV * s, 0), max(L - (r0 * s + 1), 0))
-    d[HV * s:HV * s + n] = bytes(d[r0 * s + 1:r0 * s + 1 + n])
+    d[HV * s:HV * s + n] = d[r0 * s + 1:r0 * s + 1 + n]
 
 
 def _half(b, i, step, p, n):
     if p < 2 or p + 4 >= n:
         return b[i] if p + 1 == n else avg(b[i], b[i + step])
     v = b[i - 2 * step] + b[i + 3 * step] + 5 * (4 * b[i] - b[i - step] + 4 * b[i + step] - b[i + 2 * step]) + 16
-    return clamp(v >> 5, 0, 255)
+    return clamp(v >> 5, 0, PX_MAX)
 
 
 def _bicubic(d, s, r0, w, h):
@@ -311,17 +319,20 @@ def _bicubic(d, s, r0, w, h):
             d[(p3 + y) * s + x] = _half(d, (p2 + y) * s + x, 1, x, w)
 
 
-def build_super(o, frame: bytes) -> bytes:
-    """SuperBuilder::build on one packed I420 frame (portable.rs:94-148)."""
+def build_super(o, frame):
+    """SuperBuilder::build on one packed I420 frame (portable.rs:94-148): bytes in, bytes out at 8
+    bits; a sequence of samples in, a list of samples out at 10 bits."""
     w, h = o.width, o.height
     cw, ch = w // 2, h // 2
     sh = super_plane_height(h, o.pel, o.levels, o.full)
-    y, u, v = bytearray(w * sh), bytearray(cw * (sh // 2)), bytearray(cw * (sh // 2))
-    f = bytes(frame)
+    wide = PX_MAX > 255
+    y, u, v = ([0] * (w * sh), [0] * (cw * (sh // 2)), [0] * (cw * (sh // 2))) if wide else \
+        (bytearray(w * sh), bytearray(cw * (sh // 2)), bytearray(cw * (sh // 2)))
+    f = [int(x) for x in frame] if wide else bytes(frame)
     build_plane(y, w, f[:w * h], w, w, h, w, h, False, o)
     build_plane(u, cw, f[w * h:w * h + cw * ch], cw, cw, ch, w, h, True, o)
     build_plane(v, cw, f[w * h + cw * ch:], cw, cw, ch, w, h, True, o)
-    return bytes(y + u + v)
+    return list(y) + list(u) + list(v) if wide else bytes(y + u + v)
 
 
 # ------------------------------------------------------------------ analyse_opts.rs
@@ -549,8 +560,8 @@ def cost_edge(S, R, level, px, py, bw, bh, mx, my, satd, pel):  # block_cost_edg
             sy, ry = clamp(ccy + row, 0, max(clh - 1, 0)), clamp(cry + row, 0, max(clh - 1, 0))
             for col in range(cw):
                 sx, rx = clamp(ccx + col, 0, max(clw - 1, 0)), clamp(crx + col, 0, max(clw - 1, 0))
-                C = sat_u32(C + abs(get(S.u, (co + sy) * S.cs + sx, 128) - get(R.u, (cref + ry) * R.cs + rx, 128)))
-                C = sat_u32(C + abs(get(S.v, (co + sy) * S.cs + sx, 128) - get(R.v, (cref + ry) * R.cs + rx, 128)))
+                C = sat_u32(C + abs(get(S.u, (co + sy) * S.cs + sx, PX_MID) - get(R.u, (cref + ry) * R.cs + rx, PX_MID)))
+                C = sat_u32(C + abs(get(S.v, (co + sy) * S.cs + sx, PX_MID) - get(R.v, (cref + ry) * R.cs + rx, PX_MID)))
     return L, sat_u32(C * 4)
 
 
@@ -649,8 +660,8 @@ def chroma_x4(S, R, level, pel, mx, my, px, py, bw, bh, lw, lh, satd):  # chroma
             rx = clamp(as_i32(cpx) + col + mcx, 0, clw - 1)
             if sx >= clw:
                 break
-            t = sat_u32(t + abs(get(S.u, (co + sy) * S.cs + sx, 128) - get(R.u, (cref + ry) * R.cs + rx, 128)))
-            t = sat_u32(t + abs(get(S.v, (co + sy) * S.cs + sx, 128) - get(R.v, (cref + ry) * R.cs + rx, 128)))
+            t = sat_u32(t + abs(get(S.u, (co + sy) * S.cs + sx, PX_MID) - get(R.u, (cref + ry) * R.cs + rx, PX_MID)))
+            t = sat_u32(t + abs(get(S.v, (co + sy) * S.cs + sx, PX_MID) - get(R.v, (cref + ry) * R.cs + rx, PX_MID)))
     return sat_u32(t * 4)
 
 
@@ -939,7 +950,7 @@ def luma_dc(S, level, px, py, bw, bh):
                 break
             s += get(S.y, (yo + y) * S.ys + x, 0)
             n += 1
-    return 0 if n == 0 else min(s // n, 255)
+    return 0 if n == 0 else min((s // n) >> DC_SHIFT, 255)
 
 
 def plane_activity(data, stride, row, x, width, height, satd):  # :1517-1553
@@ -1201,5 +1212,6 @@ def pack(o, prev, cur) -> bytes:
 
 def analyse(so, opt, cur_super: bytes, ref_super: bytes, src_w=0, src_h=0) -> bytes:
     o = analyse_from_opt(opt, pack_data(so), src_w, src_h)
-    bwd, fwd = analyse_pair(Planes(so, bytes(cur_super)), Planes(so, bytes(ref_super)), o)
+    conv = (lambda a: [int(x) for x in a]) if PX_MAX > 255 else bytes
+    bwd, fwd = analyse_pair(Planes(so, conv(cur_super)), Planes(so, conv(ref_super)), o)
     return pack(o, bwd, fwd)
