@@ -40,6 +40,41 @@ def test_oracle_planes_follow_the_payload():
     assert orc.vector_planes(vd, bad, w, h) is None
 
 
+def _clamp_to_frame(v, pos, block, frame):  # renderer.rs clamp_to_frame
+    if v + pos < 0:
+        return -pos
+    if v + block + pos > frame:
+        return max(frame - block - pos, 0)
+    return v
+
+
+@pytest.mark.parametrize("frame", [(160, 96), (120, 70)])
+def test_oracle_planes_clamp_to_the_frame(frame):
+    # raw = False: each vector is clamped so its block stays inside the frame, at the block's
+    # position x * (block - overlap); vectors beyond +-1023 become the neutral 1024
+    vd, pays, _ = _payloads()
+    mw, mh = orc.vector_grid(vd)
+    bw, bh, stx, sty = vd[2], vd[3], vd[2] - vd[9], vd[3] - vd[10]
+    rng = np.random.default_rng(5)
+    p = pays[1].copy()
+    count = vd[11] * vd[12]
+    words = p[0x44: 0x44 + 8 * count].view(np.uint32).reshape(count, 2).copy()
+    dx, dy = rng.integers(-1100, 1100, size=count), rng.integers(-1100, 1100, size=count)
+    words[:, 0] = (dx.astype(np.int64).astype(np.uint32) << 16) | (dy.astype(np.int64) & 0xFFFF).astype(np.uint32)
+    p[0x44: 0x44 + 8 * count] = words.reshape(-1).view(np.uint8)
+    got = orc.vector_planes(vd, p, frame[0], frame[1])
+    d = decode(p)["previous"]
+    for y in range(mh):
+        for x in range(mw):
+            k = min(y, vd[12] - 1) * vd[11] + min(x, vd[11] - 1)
+            vx, vy = int(d["dx"][k]), int(d["dy"][k])
+            if abs(vx) > 1023 or abs(vy) > 1023:
+                want = (1024, 1024)
+            else:
+                want = (_clamp_to_frame(vx, x * stx, bw, frame[0]) + 1024, _clamp_to_frame(vy, y * sty, bh, frame[1]) + 1024)
+            assert (got[0][y, x], got[1][y, x]) == want, (x, y)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("aopt", ["{block:{w:16,overlap:2},main:{search:{type:3,distance:8}}}",
                                   "{vectors:1,block:{w:8,overlap:0},main:{search:{type:2,distance:4}}}",
