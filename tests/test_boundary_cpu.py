@@ -144,3 +144,21 @@ def test_compute_entry_points_fail_loudly_without_a_gpu():
         with pytest.raises(sv.SvpfError, match="no CUDA device") as e:
             call()
         assert e.value.code == sv.SVPF_ECUDA
+
+
+@pytest.mark.parametrize("lang,std", [("c", "c99"), ("c++", "c++11")])
+def test_header_is_plain_c_and_cxx(lang, std):
+    """include/svpflow_b200.h is the C ABI a foreign host binds: it must compile on its own as strict
+    C99 and C++11 (no torch or CUDA types in the signatures), warning-free."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc" if lang == "c" else "g++")
+    if cc is None:
+        pytest.skip("no host compiler")
+    header = os.path.join(ROOT, "include", "svpflow_b200.h")
+    r = subprocess.run([cc, "-x", lang, f"-std={std}", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only",
+                        header], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    src = open(header).read()
+    assert "torch" not in src and "cuda_runtime" not in src and "at::" not in src
