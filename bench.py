@@ -75,6 +75,14 @@ RENDER_TRAFFIC_PER_FRAME = 4.14e6
 RENDER_REPLAYS = 48
 # int32 lanes per SM on sm_100 and the SM clock ceiling, for the nominal integer peak
 INT32_LANES_PER_SM = 128
+# the CPU legs time this many frame pairs per host thread, so that their figure is a throughput
+# (dynamic scheduling over many pairs) rather than the latency of the slowest pair
+CPU_PAIRS_PER_THREAD = 4
+# the batched object of the default line runs this launch shape (the one svpf_batch_autotune picks
+# for the 64-clip mix), so the default run spends no time on autotune trials
+BATCH_SHAPE = "nt32_b8:8"
+# the served object's arrival rates, clips/s: below the server's capacity, and the configuration's lowest
+SERVED_RATES = "0.25,5"
 SM_MAX_MHZ = 1965.0
 
 
@@ -183,15 +191,23 @@ def _gpu_id(torch, dev: int) -> str:
         return str(dev)
 
 
+_CPU_CLIPS = {}
+
+
 def cpu_reference(nframes_total: int, threads: int, pairs: int, seed: int = 1000):
     """Times the oracle (CPU restatement of the reference) on `pairs` output frames of the
-    workload: Super over the frames they need, then Analyse, on `threads` host threads."""
+    workload: Super over the frames they need, then Analyse, on `threads` host threads.
+    The clip (frames 0..pairs of the seeded workload clip) is made once per seed."""
     from oracle import oracle as orc
 
     c = CONFIGS[WORKLOAD]
     w, h = c["width"], c["height"]
     n = pairs + 1
-    clip = make_clip(w, h, n, seed=seed, motion=c["motion"], objects=c["objects"], object_motion=c["object_motion"])
+    key = (WORKLOAD, n, seed)
+    if key not in _CPU_CLIPS:
+        _CPU_CLIPS[key] = make_clip(w, h, n, seed=seed, motion=c["motion"], objects=c["objects"],
+                                    object_motion=c["object_motion"])
+    clip = _CPU_CLIPS[key]
     so = orc.super_opts(w, h, SUPER_OPT[WORKLOAD])
     ao = orc.analyse_opts(orc.sdata(so), ANALYSE_OPT[WORKLOAD], None, w, h)
     orc.total_counters(reset=True)
@@ -214,6 +230,13 @@ def _cpu_model() -> str:
     return "unknown"
 
 
+def _spread(v) -> dict:
+    """Mean, min, max and relative standard deviation of per-step figures."""
+    m = statistics.mean(v)
+    return {"mean": m, "min": min(v), "max": max(v), "n": len(v),
+            "rel_stdev": (statistics.stdev(v) / m) if len(v) > 1 and m else 0.0}
+
+
 def _one_core(pairs: int = 2) -> dict:
     """The same oracle on one host thread over `pairs` output frames (the per-core figure)."""
     dt, _, _ = cpu_reference(240, 1, pairs, seed=1999)
@@ -224,23 +247,25 @@ def run_reference(args, rank: int):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    pairs = min(max(args.cpu_pairs or threads, 2), 239)
+    pairs = min(max(args.cpu_pairs or CPU_PAIRS_PER_THREAD * threads, 2), 239)
     times = []
     for i in range(args.warmup + args.steps):
-        dt, _, _ = cpu_reference(240, threads, pairs, seed=1000 + i)
+        dt, _, _ = cpu_reference(240, threads, pairs, seed=1000)
         if i >= args.warmup:
             times.append(dt)
     total = sum(times)
     value = pairs * args.steps / total
-    sample = (f"{pairs} consecutive output frames (Super + Analyse, 1080p clip) per step on {threads} host threads; "
-              f"oracle/ C restatement of the reference (the Rust reference cannot be built here)")
+    sample = (f"output frames 0..{pairs - 1} of the seeded 1080p clip (Super + Analyse) per step, "
+              f"{pairs / threads:.1f} frame pairs per host thread on {threads} threads (throughput, not one "
+              f"pair's latency); oracle/ C restatement of the reference (the Rust reference cannot be built here)")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": _config(240, 1),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
-                         "cpu_model": _cpu_model(), "one_core": _one_core()},
+                         "cpu_model": _cpu_model(), "one_core": _one_core(),
+                         "step_pairs_per_s": _spread([pairs / t for t in times])},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -790,6 +815,39 @@ def run_2160p10(args, world: int, rank: int, local: int):
         dist.destroy_process_group()
 
 
+def _batch_oracle_sample(torch, dev, b, clips, mix) -> dict:
+    """Oracle parity of the batch on a sample: for every (resolution, block) shape of the mix, the
+    first and last output frame of its first clip (the last frame pairs with itself), checked
+    byte for byte against the CPU restatement on all host threads."""
+    from oracle import oracle as orc
+
+    seen, checked, equal = set(), [], True
+    jobs = []
+    for i, ((sb, an, n), (w, h, _, blk, _)) in enumerate(zip(clips, mix)):
+        if (w, h, blk) in seen:
+            continue
+        seen.add((w, h, blk))
+        jobs.append((i, w, h, n, blk))
+    threads = os.cpu_count() or 1
+    for i, w, h, n, blk in jobs:
+        sb, an, _ = clips[i]
+        fl = sb.source_len()
+        frames = torch.as_tensor(_DevBytes(b.frames_device(i), fl * n), device=dev).cpu().numpy().reshape(n, fl)
+        pl = an.payload_len()
+        pays = torch.as_tensor(_DevBytes(b.payloads_device(i), pl * n), device=dev).cpu().numpy().reshape(n, pl)
+        so = orc.super_opts(w, h, SUPER_OPT["1080p"])
+        ao = orc.analyse_opts(orc.sdata(so), analyse_opt_for_block(blk), None, w, h)
+        need = sorted({0, 1, n - 1})
+        supers = orc.build_super_many(so, frames[need], threads)
+        sup = dict(zip(need, supers))
+        for f in sorted({0, n - 1}):
+            want = orc.analyse(ao, so, sup[f], sup[min(f + 1, n - 1)])
+            ok = bool(np.array_equal(want, pays[f]))
+            equal = equal and ok
+            checked.append({"clip": i, "shape": f"{w}x{h}/b{blk}", "frame": f, "bit_exact": ok})
+    return {"pairs_checked": len(checked), "bit_exact": equal, "sample": checked}
+
+
 def run_batched(args, world: int, rank: int, local: int):
     """Config 4: many clips of uneven size in one persistent launch, against per-clip launches."""
     torch, dist = _init_dist(world, local)
@@ -817,7 +875,14 @@ def run_batched(args, world: int, rank: int, local: int):
     host_frames = [fr.cpu().pin_memory() for _, _, fr in clips]  # for the end-to-end run
     clips = [(sb, an, fr.shape[0]) for sb, an, fr in clips]      # the batch holds the device frames now
     torch.cuda.empty_cache()
-    tune = b.autotune() if not args.no_autotune else {"trial_pairs_per_s": None, **b.shape()}
+    if args.shape:  # a fixed launch shape (no autotune trial): "name" or "name:tiles_per_lane"
+        name, _, tpl = args.shape.partition(":")
+        b.set_shape(sv.Batch.variants().index(name), int(tpl or 8))
+        tune = {"trial_pairs_per_s": None, **b.shape(), "chosen_by": f"fixed by --shape {args.shape} (no autotune trial)"}
+    elif args.no_autotune:
+        tune = {"trial_pairs_per_s": None, **b.shape(), "chosen_by": "default shape (no autotune trial)"}
+    else:
+        tune = {**b.autotune(), "chosen_by": "svpf_batch_autotune on this batch"}
     stream = torch.cuda.Stream(dev)
     sh = stream.cuda_stream
     pairs = b.pairs
@@ -865,6 +930,9 @@ def run_batched(args, world: int, rank: int, local: int):
             same = same and bool(torch.equal(got, pay_d[:L]))
     plain_ms = _max_over_ranks(torch, dist, world, plain_ms, dev)
     plain_value = total_pairs / (plain_ms / 1000.0)
+    oracle_check = None
+    if rank == 0 and not args.no_cpu:
+        oracle_check = _batch_oracle_sample(torch, dev, b, clips, [m for i, m in enumerate(mix) if i % world == rank])
 
     # end to end through the host-buffer batch call (pinned frames in, payloads out)
     del sup_d, pay_d, scr_d
@@ -906,6 +974,7 @@ def run_batched(args, world: int, rank: int, local: int):
                                "how": "Super + svpf_clip_analyse_device per clip, clips one after another"},
             "batched_over_plain": value / plain_value,
             "payloads_equal_plain": same,
+            "parity_vs_oracle": oracle_check,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(sum(t.numel() for t in host_frames)),
                     "d2h_bytes_per_step": int(sum(t.numel() for t in host_pay)),
                     "api": "svpf_batch_run (host buffers)", "matches_device_path": e2e_same},
@@ -916,6 +985,24 @@ def run_batched(args, world: int, rank: int, local: int):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _served_oracle_sample(clip_desc, frames: np.ndarray, pay: np.ndarray) -> dict:
+    """Oracle parity of one served clip: its first and last output frame (the last pairs with
+    itself) against the CPU restatement."""
+    from oracle import oracle as orc
+
+    _, w, h, n, _ = clip_desc
+    so = orc.super_opts(w, h, SUPER_OPT["1080p"])
+    ao = orc.analyse_opts(orc.sdata(so), ANALYSE_OPT["1080p"], None, w, h)
+    need = sorted({0, 1, n - 1})
+    sup = dict(zip(need, orc.build_super_many(so, frames[need], os.cpu_count() or 1)))
+    out = []
+    for f in sorted({0, n - 1}):
+        want = orc.analyse(ao, so, sup[f], sup[min(f + 1, n - 1)])
+        out.append({"frame": f, "bit_exact": bool(np.array_equal(want, pay[f]))})
+    return {"clip": f"{w}x{h}, {n} frames", "pairs_checked": len(out), "bit_exact": all(o["bit_exact"] for o in out),
+            "sample": out}
 
 
 def run_served(args, world: int, rank: int, local: int):
@@ -947,6 +1034,7 @@ def run_served(args, world: int, rank: int, local: int):
     sb0, an0 = handles[(base[k_small][1], base[k_small][2])]
     want_small = an0.analyse_clip(sb0, frames[k_small])
     sweep = []
+    oracle_small = None
     for wi, rate in enumerate(rates):
         arrivals = [t for (t, _, _, _, _) in served_stream(nclips, rate, seed=5 + rank, max_len=args.max_len or 600)]
         srv = sv.Server(budget, max_active=args.max_active, chunk_pairs=args.chunk)
@@ -972,6 +1060,8 @@ def run_served(args, world: int, rank: int, local: int):
             done_last = max(done_last, fin)
             if k == k_small:
                 identical = bool(np.array_equal(pay, want_small))
+                if oracle_small is None and not args.no_cpu:
+                    oracle_small = _served_oracle_sample(base[k_small], frames[k_small], pay)
         span_s = (done_last - t_start) / 1e9
         st = srv.stats()
         srv.close()
@@ -981,6 +1071,17 @@ def run_served(args, world: int, rank: int, local: int):
                       "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
                       "peak_active_clips": st["peak_active"], "peak_device_gb": st["peak_device_bytes"] / 2 ** 30,
                       "kernel_launches": st["kernel_launches"], "small_clip_identical_to_alone": identical})
+    # the same clips through the plain per-clip host-buffer path (svpf_clip_analyse), one after another
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k, (_, w, h, n, _) in enumerate(base):
+        sb, an = handles[(w, h)]
+        an.analyse_clip(sb, frames[k])
+    plain_s = _max_over_ranks(torch, dist, world, time.perf_counter() - t0, dev)
+    plain = {"value": total_pairs / plain_s, "unit": UNIT, "s": plain_s,
+             "how": "svpf_clip_analyse (host frames in, payloads out) per clip, clips one after another"}
+    for r in sweep:
+        r["over_plain"] = r["pairs_per_s"] / plain["value"]
     if rank == 0:
         best = max(sweep, key=lambda r: r["pairs_per_s"])
         line = {
@@ -995,6 +1096,8 @@ def run_served(args, world: int, rank: int, local: int):
                        "generation_s": gen_s,
                        "latency": "clip arrival to that pair's payload in host memory"},
             "sweep": sweep,
+            "plain_per_clip": plain,
+            "parity_vs_oracle": oracle_small,
             "e2e": {"value": best["pairs_per_s"], "unit": UNIT,
                     "h2d_bytes_per_step": int(sum(f.nbytes for f in frames)),
                     "d2h_bytes_per_step": int(sum(handles[(w, h)][1].payload_len() * n for (_, w, h, n, _) in base)),
@@ -1026,6 +1129,9 @@ def main():
     ap.add_argument("--max-active", type=int, default=8, help="served: clips in flight")
     ap.add_argument("--chunk", type=int, default=32, help="served: output frames per launch")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--shape", default="", help="batched: fixed launch shape name[:tiles_per_lane], no autotune")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="1080p: leave out the batched and served objects of the default line")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1168,7 +1274,7 @@ def main():
         parity = None
         if not args.no_cpu:
             threads = os.cpu_count() or 1
-            pairs = min(args.cpu_pairs or threads, nf - 1)
+            pairs = min(args.cpu_pairs or CPU_PAIRS_PER_THREAD * threads, nf - 1)
             dt, pay_cpu, _ = cpu_reference(nf, threads, pairs, seed=1000 + rank)
             from oracle import oracle as orc
 
@@ -1185,8 +1291,9 @@ def main():
                               f"sample, 111 per SATD 4x4 tile)",
                 "peak_source": "nominal: SMs x 128 int32 lanes x max SM clock (no measured integer peak)"}
             cpu = {"value": pairs / dt, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"output frames 0..{pairs - 1} of the same clip (Super + Analyse) on {threads} host "
-                             f"threads, oracle/ C restatement of the reference (AVX2 interior SAD/SATD)",
+                   "sample": f"output frames 0..{pairs - 1} of the same clip (Super + Analyse), "
+                             f"{pairs / threads:.1f} frame pairs per host thread on {threads} threads (throughput), "
+                             f"oracle/ C restatement of the reference (AVX2 interior SAD/SATD)",
                    "cpu_model": _cpu_model(), "one_core": _one_core()}
             parity = {"pairs_checked": pairs,
                       "bit_exact": bool(np.array_equal(pay_cpu, pay_d[:pairs].cpu().numpy()))}
@@ -1205,10 +1312,64 @@ def main():
             "serial_chain": _chain(an, nf, a_ms),
             "super_ms_per_step": statistics.mean(super_ms), "analyse_ms_per_step": statistics.mean(analyse_ms),
         }
+        if world == 1 and WORKLOAD == "1080p" and not args.no_sub:
+            # the metric's other two halves (batched vs plain, served p50/p99), each in its own
+            # process after this one's buffers are released
+            del frames_d, supers_d, pay_d, scratch_d, pinned, out_host
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+            line["batched"] = _sub_batched(args)
+            line["served"] = _sub_served(args)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _sub_line(extra, timeout_s: int) -> dict:
+    """Runs this script on another workload in a child process and returns its JSON line."""
+    cmd = [sys.executable, os.path.abspath(__file__), *extra]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        return {"error": f"{' '.join(extra)}: no result within {timeout_s} s"}
+    for ln in reversed(r.stdout.splitlines()):
+        if ln.startswith("{"):
+            return json.loads(ln)
+    return {"error": f"{' '.join(extra)}: rc {r.returncode}: {r.stderr[-600:]}"}
+
+
+def _sub_batched(args) -> dict:
+    """Config 4 in the default line: the 64-clip mix in one persistent launch (CUDA-graph replay)
+    against the same clips through the plain per-clip path, with oracle parity on a sample."""
+    extra = ["--workload", "batched", "--steps", "1", "--warmup", "1", "--e2e-steps", "0", "--shape", BATCH_SHAPE]
+    if args.no_cpu:
+        extra.append("--no-cpu")
+    b = _sub_line(extra, 1500)
+    if "error" in b:
+        return b
+    keep = ("metric", "value", "unit", "ms_per_step", "plain_per_clip", "batched_over_plain", "payloads_equal_plain",
+            "parity_vs_oracle", "launch_shape", "clocks", "gpu_launches")
+    out = {k: b.get(k) for k in keep}
+    out["config"] = {k: b["config"].get(k) for k in ("workload", "clips", "pairs", "pairs_by_shape",
+                                                      "device_bytes_per_gpu")}
+    out["timing"] = "one graph replay of the whole batch timed with CUDA events after one untimed replay"
+    return out
+
+
+def _sub_served(args) -> dict:
+    """Config 5 in the default line: Poisson arrivals into the continuous-batching server at one
+    rate below the server's capacity and one above it (the configuration's lowest rate)."""
+    extra = ["--workload", "served", "--rates", SERVED_RATES]
+    if args.no_cpu:
+        extra.append("--no-cpu")
+    sl = _sub_line(extra, 1500)
+    if "error" in sl:
+        return sl
+    keep = ("metric", "value", "unit", "sweep", "plain_per_clip", "parity_vs_oracle", "gpu_launches")
+    out = {k: sl.get(k) for k in keep}
+    out["config"] = sl.get("config")
+    return out
 
 
 if __name__ == "__main__":

@@ -1,8 +1,13 @@
-"""The batched and served forms (GPU): every payload equals the plain per-clip path's
-(which the parity suite holds to the oracle), for every launch shape, alone and in a mix
-of clips of uneven size, length and options. Tolerance: zero (integer work)."""
+"""The batched and served forms (GPU): every payload equals the oracle's (the CPU
+restatement of the reference, on the same frames and options) and the plain per-clip
+path's, for every launch shape, alone and in a mix of clips of uneven size, length and
+options; served clips overlap on the device. Tolerance: zero (integer work)."""
+import os
+
 import numpy as np
 import pytest
+
+from oracle import oracle as orc
 
 pytestmark = pytest.mark.gpu
 
@@ -33,6 +38,25 @@ def _plain(clips):
     return [an.analyse_clip(sb, clip) for sb, an, clip in clips]
 
 
+def _oracle(clips, mix=MIX):
+    """Every output frame of every clip from the oracle (frame n pairs with min(n + delta, last))."""
+    out = []
+    for (sb, an, clip), (w, h, n, _, sopt, aopt) in zip(clips, mix):
+        so = orc.super_opts(w, h, sopt)
+        ao = orc.analyse_opts(orc.sdata(so), aopt, None, w, h)
+        supers = orc.build_super_many(so, clip, os.cpu_count() or 1)
+        out.append(orc.analyse_clip(ao, so, supers, 0, n, os.cpu_count() or 1))
+    return out
+
+
+def _expect(clips, mix=MIX):
+    """The oracle's payloads, after checking that the plain per-clip path gives the same."""
+    want = _oracle(clips, mix)
+    for i, (g, w_) in enumerate(zip(_plain(clips), want)):
+        assert np.array_equal(g, w_), f"plain path: clip {i} differs from the oracle"
+    return want
+
+
 class _Dev:
     """A raw device byte range as a torch tensor (CUDA array interface; no copy)."""
 
@@ -50,7 +74,7 @@ def test_batch_matches_plain_for_every_shape():
     import svpflow_b200 as sv
 
     clips = _clips()
-    want = _plain(clips)
+    want = _expect(clips)
     b = sv.Batch([(sb, an, clip.shape[0]) for sb, an, clip in clips])
     assert b.pairs == sum(c[2].shape[0] for c in clips)
     for v in range(len(sv.Batch.variants())):
@@ -68,7 +92,7 @@ def test_batch_device_replay_and_autotune():
     import svpflow_b200 as sv
 
     clips = _clips(MIX[:3])
-    want = _plain(clips)
+    want = _expect(clips, MIX[:3])
     b = sv.Batch([(sb, an, clip.shape[0]) for sb, an, clip in clips])
     for i, (_, _, clip) in enumerate(clips):  # fill the batch's frame buffers on the device
         ptr = b.frames_device(i)
@@ -96,7 +120,7 @@ def test_server_results_equal_alone_and_in_the_mix():
     import svpflow_b200 as sv
 
     clips = _clips()
-    want = _plain(clips)
+    want = _expect(clips)
     # a budget below two of the largest clips, so admission has to wait for memory
     chunk = 2
     need = [c[2].nbytes + (c[0].output_len() + c[1].payload_len()) * c[2].shape[0] +
@@ -131,5 +155,36 @@ def test_server_rejects_a_clip_over_budget():
     try:
         with pytest.raises(ValueError, match="more device memory than the server's budget"):
             srv.submit(sb, an, clip)
+    finally:
+        srv.close()
+
+
+def test_served_clips_overlap_on_the_device():
+    """Continuous batching: clips admitted together run concurrently on the GPU. Four copies of a
+    clip whose launches fill few SMs, served with four slots, finish in far less than four times
+    the span of one copy served alone (one after another they would take four times as long),
+    and every copy's payloads equal the oracle's."""
+    import svpflow_b200 as sv
+
+    mix = [(640, 360, 9, 21, "{pel:2}", "{block:{w:16,overlap:3},main:{search:{type:3,distance:8,satd:true}}}")]
+    (sb, an, clip), = _clips(mix)
+    want = _expect([(sb, an, clip)], mix)[0]
+    srv = sv.Server(8 << 30, max_active=4, chunk_pairs=16)
+    try:
+        srv.wait(srv.submit(sb, an, clip))  # warm-up (module load, pools)
+        spans_alone = []
+        for _ in range(3):
+            pay, _, (arr, _, fin) = srv.wait(srv.submit(sb, an, clip))
+            spans_alone.append(fin - arr)
+            assert np.array_equal(pay, want)
+        alone = min(spans_alone)
+        ids = [srv.submit(sb, an, clip) for _ in range(4)]
+        res = [srv.wait(r) for r in ids]
+        t0 = min(r[2][0] for r in res)
+        t1 = max(r[2][2] for r in res)
+        for pay, _, _ in res:
+            assert np.array_equal(pay, want)
+        assert srv.stats()["peak_active"] >= 2
+        assert (t1 - t0) < 2.5 * alone, f"four clips took {(t1 - t0) / 1e6:.1f} ms, one alone {alone / 1e6:.1f} ms"
     finally:
         srv.close()

@@ -97,3 +97,28 @@ def test_analyse_matches_oracle(case):
         j = min(i + max(ao.delta, 1), n - 1)
         want = orc.analyse(ao, so, supers[i], supers[j])
         assert got[i].tobytes() == want.tobytes(), f"output frame {i}: " + first_difference(got[i], want)
+
+
+def test_analyse_full_1080p_matches_oracle():
+    """The benchmark's own configuration at its full frame size: 1920x1080, Super {pel:2}, block 16,
+    overlap 8, UMH r16, SATD + chroma, both directions, over 3 frames of the seeded benchmark clip
+    (motion ranges of the 1080p workload); output frame 2 is the last frame paired with itself
+    (analyse_filter.rs:279)."""
+    import os
+
+    from svpflow_b200.synth import ANALYSE_OPT, CONFIGS, SUPER_OPT
+
+    sv = _sv()
+    c = CONFIGS["1080p"]
+    w, h, n = c["width"], c["height"], 3
+    clip = _clip(w, h, n, seed=1000, motion=c["motion"], objects=c["objects"], object_motion=c["object_motion"])
+    sb = sv.Super(w, h, SUPER_OPT["1080p"])
+    an = sv.Analyse(sb.sdata, ANALYSE_OPT["1080p"], w, h)
+    so = orc.super_opts(w, h, SUPER_OPT["1080p"])
+    ao = orc.analyse_opts(orc.sdata(so), ANALYSE_OPT["1080p"], None, w, h)
+    supers = orc.build_super_many(so, clip, os.cpu_count() or 1)
+    assert np.array_equal(sb.build_many(clip), supers)
+    want = orc.analyse_clip(ao, so, supers, 0, n, os.cpu_count() or 1)
+    got = an.analyse_clip(sb, clip)
+    for i in range(n):
+        assert got[i].tobytes() == want[i].tobytes(), f"output frame {i}: " + first_difference(got[i], want[i])
