@@ -9,15 +9,18 @@
 //
 // The array is a file-scope device variable: every GPU that loads this library holds
 // its kNoAllocScratchBytes until the process exits. Host code cannot use the array's
-// name as a device address, so the address is fetched once per device with
-// cudaGetSymbolAddress (the first call on a device does this set-up). All calls share
-// the one array and it keeps what the last call left there: the status word is cleared
-// on every call, and the search itself writes every scratch word before reading it.
-// Two calls whose kernels overlap on the GPU (different streams, no ordering between
-// them) race on the array and give undefined results; order them on one stream.
+// name as a device address, so every call looks the address up with
+// cudaGetSymbolAddress on the current device (cheap once the module is loaded, and
+// never stale: a device reset or a new primary context gives the array a new address,
+// which the next call picks up). All calls share the one array and it keeps what the
+// last call left there: the status word is cleared on every call, and the search itself
+// writes every scratch word before reading it. Two calls whose kernels overlap on the
+// GPU (different streams, no ordering between them) race on the array and give
+// undefined results; order them on one stream. Each call reads the kernel's status back
+// into host memory and synchronises its stream, so it cannot be made on a stream that is
+// being captured into a CUDA graph.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/svpflow_b200.h"
@@ -31,10 +34,6 @@ constexpr size_t kStatusBytes = 256;                // status word at the head o
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-unsigned char *g_scratch_addr[kMaxDevices] = {};
-
 }  // namespace
 
 namespace {
@@ -44,21 +43,14 @@ int noalloc_fail(int code, const std::string &msg) {
     return code;
 }
 
-// The device address of g_noalloc_scratch on the current device (set-up on first use).
+// The device address of g_noalloc_scratch in the current device's context, looked up
+// on every call (nothing is cached across calls, so no address outlives its context).
 int scratch_address(unsigned char **out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return noalloc_fail(SVPF_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(SVPF_ECUDA, "device ordinal out of range");
-    std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return noalloc_fail(SVPF_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch_addr[dev] = (unsigned char *)p;
-    }
-    *out = g_scratch_addr[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return noalloc_fail(SVPF_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    *out = (unsigned char *)p;
     return SVPF_OK;
 }
 

@@ -2,7 +2,8 @@
 
 It exists for callers that may not allocate device memory (a frame server's per-frame
 callback, or a host that forbids allocations after start-up); its scratch is a fixed
-array inside the library. Called through the C ABI, twice in a row, it must give the
+array inside the library. Called through the C ABI, twice in a row, after a call on
+another clip with other options has left its own data in the array, it must give the
 same payloads as svpf_clip_analyse_device with caller-provided scratch: the work is
 integer, so the tolerance is zero (byte equality). Requests beyond the fixed array are
 rejected with SVPF_EINVAL before anything is launched.
@@ -44,19 +45,40 @@ def _setup(w, h, nframes, sopt, aopt, seed):
     return sv, an, supers, stream
 
 
+def _with_scratch(sv, an, supers, n, stream):
+    """The payloads of the existing entry point, svpf_clip_analyse_device, with caller scratch."""
+    import torch
+
+    dev = supers.device
+    want = torch.empty((n, an.payload_len()), dtype=torch.uint8, device=dev)
+    scratch = torch.empty(an.scratch_bytes(n), dtype=torch.uint8, device=dev)
+    an.analyse_clip_device(supers.data_ptr(), n, 0, n, want.data_ptr(), scratch.data_ptr(), stream)
+    sv.Analyser.device_status(scratch.data_ptr(), stream)
+    return want
+
+
 def test_noalloc_matches_clip_analyse_device_twice():
     import torch
+
+    # First a different clip with other options (block 8, exhaustive search, one direction,
+    # another grid and payload length), so the shared array holds another call's leftovers when
+    # the checked calls run: they must not read anything they did not write themselves.
+    m = 4
+    sv, an_o, supers_o, stream = _setup(
+        256, 144, m, "{pel:1}", "{vectors:1,block:{w:8,overlap:1},main:{search:{type:4,distance:4}}}", seed=3)
+    f = _noalloc(sv.lib())
+    other = torch.full((m, an_o.payload_len()), 0x5A, dtype=torch.uint8, device=supers_o.device)
+    rc = f(an_o.handle, supers_o.data_ptr(), m, 0, m, other.data_ptr(), stream)
+    assert rc == 0, sv.lib().svpf_last_error().decode()
+    want_o = _with_scratch(sv, an_o, supers_o, m, stream)
+    assert np.array_equal(other.cpu().numpy(), want_o.cpu().numpy()), "the first clip's payloads differ"
 
     n = 5
     sv, an, supers, stream = _setup(
         320, 180, n, "{pel:2}", "{block:{w:16,overlap:3},main:{search:{type:3,distance:16,satd:true}}}", seed=11)
     pl = an.payload_len()
     dev = supers.device
-    want = torch.empty((n, pl), dtype=torch.uint8, device=dev)
-    scratch = torch.empty(an.scratch_bytes(n), dtype=torch.uint8, device=dev)
-    an.analyse_clip_device(supers.data_ptr(), n, 0, n, want.data_ptr(), scratch.data_ptr(), stream)
-    sv.Analyser.device_status(scratch.data_ptr(), stream)
-    f = _noalloc(sv.lib())
+    want = _with_scratch(sv, an, supers, n, stream)
     for call in range(2):
         got = torch.full((n, pl), 0xA5, dtype=torch.uint8, device=dev)
         rc = f(an.handle, supers.data_ptr(), n, 0, n, got.data_ptr(), stream)
