@@ -12,7 +12,10 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
+#include <thread>
+#include <vector>
 #include <string>
 
 #include "../../include/svpflow_b200.h"
@@ -131,6 +134,8 @@ __global__ void vector_planes_kernel(const PlaneJob J) {
 // reference's saturating and wrapping adds plain adds and the atomic sums order-independent.
 // TruncDiv (:3149-3184) divides exactly (truncating), so plain '/' restates it.
 
+constexpr int kMagRuns = 512;  // the most runs of equal magnitude bytes a setting may have
+
 struct MaskJob {
     const uint8_t *payloads;
     int64_t payload_len;
@@ -138,10 +143,14 @@ struct MaskJob {
     int32_t *sums;        // per payload: two (mw + 2) x (mh + 2) splat planes
     int *status;
     int32_t flags, gw, gh, mw, mh;
-    int32_t bw, bh, xs, ys, denom, phase, area, sharp_is_one, mag_steps;
+    int32_t bw, bh, xs, ys, denom, phase, area, sharp_is_one, mag_steps, mag_runs;
     double strength, area_scale, area_sharp;
     // mag_steps: the magnitude byte is the number of these scores at or below the vector's score
     uint32_t mag_thr[255];
+    // mag_runs > 0 (any other setting): the byte of a score is mag_run_byte[i] for the last run i
+    // with mag_run_start[i] <= score (mag_run_start[0] = 0)
+    uint32_t mag_run_start[kMagRuns];
+    uint8_t mag_run_byte[kMagRuns];
 };
 
 __device__ __forceinline__ bool mask_regions(const MaskJob &J, const uint8_t *p, int64_t &off_prev,
@@ -205,8 +214,16 @@ __global__ void mask_finish_kernel(const MaskJob J) {
         return;
     }
     __shared__ uint32_t thr[255];
+    __shared__ uint32_t run_start[kMagRuns];
+    __shared__ uint8_t run_byte[kMagRuns];
     if (J.mag_steps) {  // the whole block takes this branch or returned above
         for (int k = threadIdx.x; k < 255; k += blockDim.x) thr[k] = J.mag_thr[k];
+        __syncthreads();
+    } else if (J.mag_runs) {
+        for (int k = threadIdx.x; k < J.mag_runs; k += blockDim.x) {
+            run_start[k] = J.mag_run_start[k];
+            run_byte[k] = J.mag_run_byte[k];
+        }
         __syncthreads();
     }
     const int64_t n = (int64_t)J.mw * J.mh;
@@ -242,6 +259,14 @@ __global__ void mask_finish_kernel(const MaskJob J) {
                         else hi = mid;
                     }
                     a[s] = (uint8_t)lo;
+                } else if (J.mag_runs) {  // the last run starting at or below score
+                    int lo = 0, hi = J.mag_runs - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (run_start[mid] <= score) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    a[s] = run_byte[lo];
                 } else {
                     double v = __ddiv_rn(__dmul_rn(__dmul_rn(4.0, (double)score), J.area_scale), area_f);
                     if (!J.sharp_is_one) v = pow(v, J.area_sharp);
@@ -356,6 +381,58 @@ bool magnitude_steps(double scale, double sharp, int32_t area, uint32_t thr[255]
         c_scale = scale; c_sharp = sharp; c_area = area;
     }
     memcpy(thr, c_thr, sizeof(c_thr));
+    return true;
+}
+
+// Every other setting (sharpness below 1e-3 or not positive, negative or non-finite scale): libm's
+// byte for each of the 2^24 scores, as runs of equal bytes (a handful for any setting: the byte is
+// a monotone function of the score, or NaN-to-0 apart from score 0). False when there are more
+// than kMagRuns runs; the kernel then calls CUDA's pow (bytes not guaranteed equal to libm's).
+bool magnitude_runs(double scale, double sharp, int32_t area, uint32_t *start, uint8_t *byte, int32_t *nruns) {
+    if (area <= 0) return false;
+    static std::mutex mu;
+    static double c_scale = 0.0, c_sharp = 0.0;
+    static int32_t c_area = -1, c_n = 0;
+    static uint32_t c_start[kMagRuns];
+    static uint8_t c_byte[kMagRuns];
+    std::lock_guard<std::mutex> lk(mu);
+    const bool same = c_area == area && memcmp(&c_scale, &scale, sizeof(double)) == 0 &&
+                      memcmp(&c_sharp, &sharp, sizeof(double)) == 0;
+    if (!same) {
+        constexpr uint32_t kScores = 1u << 24;
+        const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        std::vector<std::vector<std::pair<uint32_t, uint8_t>>> part(nt);
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; t++)
+            th.emplace_back([&, t] {
+                const uint32_t a = (uint32_t)((uint64_t)kScores * t / nt), b = (uint32_t)((uint64_t)kScores * (t + 1) / nt);
+                int prev = -1;
+                for (uint32_t sc = a; sc < b; sc++) {
+                    const uint8_t v = magnitude_byte(sc, scale, sharp, area);
+                    if (v != prev) {
+                        part[t].push_back({sc, v});
+                        prev = v;
+                        if (part[t].size() > (size_t)kMagRuns) return;
+                    }
+                }
+            });
+        for (auto &x : th) x.join();
+        int n = 0;
+        bool ok = true;
+        for (unsigned t = 0; t < nt && ok; t++)
+            for (auto &r : part[t]) {
+                if (n > 0 && c_byte[n - 1] == r.second) continue;  // a run that continues across threads
+                if (n == kMagRuns || part[t].size() > (size_t)kMagRuns) { ok = false; break; }
+                c_start[n] = r.first;
+                c_byte[n] = r.second;
+                n++;
+            }
+        c_scale = scale; c_sharp = sharp; c_area = area; c_n = ok ? n : 0;
+    }
+    if (c_n == 0) return false;
+    memcpy(start, c_start, sizeof(uint32_t) * (size_t)c_n);
+    memcpy(byte, c_byte, (size_t)c_n);
+    *nruns = c_n;
     return true;
 }
 
@@ -505,6 +582,9 @@ int svpf_render_masks_device(const int32_t *vdata, const uint8_t *payloads_dev, 
     J.area_sharp = area_sharp;
     J.sharp_is_one = area_sharp == 1.0;  // pow(x, 1) is x exactly, in libm and here
     J.mag_steps = magnitude_steps(area_scale, area_sharp, J.area, J.mag_thr) ? 1 : 0;
+    J.mag_runs = 0;
+    if (!J.mag_steps && !magnitude_runs(area_scale, area_sharp, J.area, J.mag_run_start, J.mag_run_byte, &J.mag_runs))
+        J.mag_runs = 0;
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t n = (int64_t)J.mw * J.mh, count = (int64_t)J.gw * J.gh;
     const size_t sums = (size_t)npayloads * 2 * ((size_t)J.mw + 2) * ((size_t)J.mh + 2) * sizeof(int32_t);

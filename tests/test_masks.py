@@ -312,6 +312,29 @@ def test_device_magnitude_bytes_exact_at_every_step(scale, sharp):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("scale,sharp", [(0.01, 0.0005), (0.3, 0.0), (0.01, -0.5), (-1.0, 2.0), (-0.5, 0.5),
+                                         (-0.02, 3.0), (float("inf"), 1.0), (0.01, float("nan"))])
+def test_device_magnitude_bytes_exact_for_every_setting(scale, sharp):
+    # settings outside the step table (sharpness below 1e-3 or not positive, negative or non-finite
+    # scale): the host tabulates libm's byte over all 2^24 scores as runs, so the device's bytes
+    # equal the oracle's (libm pow) at any score; checked at random scores and at the edges
+    vd, pays, _ = _payloads(w=320, h=240, n=2, aopt="{block:{w:8,overlap:0},main:{search:{type:2,distance:2}}}")
+    count = vd[11] * vd[12]
+    rng = np.random.default_rng(17)
+    special = [0, 1, 2, 3, 255, 256, (1 << 24) - 2, (1 << 24) - 1] + [1 << k for k in range(24)]
+    scores = np.concatenate([np.array(special, dtype=np.int64),
+                             rng.integers(0, 1 << 24, size=count, dtype=np.int64),
+                             np.exp(rng.uniform(0, math.log(1 << 24), size=count)).astype(np.int64)])[:count]
+    p = pays[0]
+    for region in range(2):
+        p = _with_vectors(p, vd, np.zeros(count), np.zeros(count), np.roll(scores, 7 * region), region)
+    got, status = _device_masks(vd, p[None, :], 128, 100, scale, sharp)
+    want = orc.render_masks(vd, p, 128, 100, scale, sharp)
+    assert status[0] == 0
+    assert np.array_equal(got[0][2:], want[2:]), f"{np.argwhere(got[0][2:] != want[2:])[:4]}"
+
+
+@pytest.mark.gpu
 def test_device_masks_reject_bad_arguments():
     import torch
 
