@@ -198,6 +198,200 @@ __global__ void __launch_bounds__(256) super_reduce_kernel(SuperDev D, T *__rest
     }
 }
 
+
+// ---- 8-bit fast paths: rows processed in 16-byte (level 0) and 4-byte (pyramid) words. Used
+// when every row of the source and super frames starts on a 16-byte boundary; the kernels
+// above serve every other geometry and the uint16 format. Both give the same bytes.
+
+// rounded-up byte average of four packed bytes (avg_epu8, super_build.rs:250-253)
+__device__ __forceinline__ uint32_t avgu4(uint32_t a, uint32_t b) { return (a | b) - (((a ^ b) >> 1) & 0x7F7F7F7Fu); }
+__device__ __forceinline__ uint4 avg16(uint4 a, uint4 b) {
+    return make_uint4(avgu4(a.x, b.x), avgu4(a.y, b.y), avgu4(a.z, b.z), avgu4(a.w, b.w));
+}
+// bytes 1..16 of (a, next byte)
+__device__ __forceinline__ uint4 shift1(uint4 a, uint32_t next) {
+    return make_uint4(__funnelshift_r(a.x, a.y, 8), __funnelshift_r(a.y, a.z, 8), __funnelshift_r(a.z, a.w, 8),
+                      __funnelshift_r(a.w, next, 8));
+}
+
+// 16 bytes of sub-plane p of row y from x0 on, by the closed forms of super_level0_kernel
+// (out of line: only the chunks at the right edge and in the last row take it).
+// subpel: bilinear sub-pixel planes are filled (pel >= 2, gpu <= 1, full, scale.up 0).
+__device__ __noinline__ uint4 level0_edge_chunk(bool subpel, const uint8_t *s0, int64_t sst, int w, int h, int64_t S,
+                                                int y, int x0, int p) {
+    const L0View<uint8_t> V{s0, sst, w, h, S};
+    const PlaneGeo g{w, h, S, 0, 0, sst, 0};
+    uint32_t wd0 = 0, wd1 = 0, wd2 = 0, wd3 = 0;
+    for (int q = 0; q < 16; q++) {
+        const int x = x0 + q;
+        unsigned v = 0;
+        if (p == 0) {
+            if (g.w > 0) v = V.L(y, x);
+        } else if (subpel && p <= 3 && x < g.w) {
+            if (p == 1) v = V.h_val(y, x);
+            else if (p == 2) v = y == 0 ? V.L(0, x) : avg8(V.L(y, x), V.flat((int64_t)(y + 1) * S + x));
+            else v = y == 0 ? V.flat(1 + x) : avg8(V.L(y, x), V.flat((int64_t)(y + 1) * S + 1 + x));
+        }
+        const uint32_t b = (v & 0xFFu) << (8 * (q & 3));
+        if (q < 4) wd0 |= b;
+        else if (q < 8) wd1 |= b;
+        else if (q < 12) wd2 |= b;
+        else wd3 |= b;
+    }
+    return make_uint4(wd0, wd1, wd2, wd3);
+}
+
+// The level-0 region (copy + edge extension, super_build.rs:45-67; bilinear pel-2 planes,
+// :179-224; zero sub-planes otherwise), one 16-byte chunk of one row per thread, every
+// sub-plane of that chunk. grid: x = chunks of the pitch / 128, y = plane row, z = frame x planes.
+__global__ void __launch_bounds__(128, 8) super_level0_vec_kernel(SuperDev D, const uint8_t *__restrict__ src,
+                                                               uint8_t *__restrict__ dst, int plane0, int nplanes) {
+    const int plane = plane0 + (int)(blockIdx.z % (unsigned)nplanes);
+    const int64_t f = blockIdx.z / (unsigned)nplanes;
+    const PlaneGeo g = plane_geo(D, plane);
+    const int y = blockIdx.y;
+    const int S = (int)g.stride, w = g.w, h = g.h;
+    const int x0 = (blockIdx.x * 128 + threadIdx.x) * 16;
+    if (y >= h || x0 >= S) return;
+    const int nsub = D.full ? D.pel * D.pel : 1;
+    const bool bil = D.pel >= 2 && D.gpu <= 1 && D.full && D.scale_up == 0;
+    const uint8_t *s0 = src + f * D.src_frame_bytes + g.src_off;
+    const int sst = (int)g.src_stride;
+    uint8_t *o = dst + f * D.frame_bytes + g.out_off + (int64_t)y * S + x0;
+    const int64_t pstep = (int64_t)h * S;  // one sub-plane further down
+    const uint4 zero = make_uint4(0, 0, 0, 0);
+    // sub-planes whose row y exists in the buffer (a super frame can have fewer rows than the
+    // level-0 region, e.g. full:false, super_opts.rs:77-95)
+    int np = 0;
+    while (np < nsub && (int64_t)np * h + y < g.rows) np++;
+    if (np == 0) return;
+    if (np == nsub && x0 + 16 < w && y + 1 < h) {  // interior chunk: x + 1 and y + 1 stay inside the plane
+        const uint8_t *r0 = s0 + (int64_t)y * sst + x0;
+        const uint4 A = *reinterpret_cast<const uint4 *>(r0);
+        *reinterpret_cast<uint4 *>(o) = A;
+        if (nsub > 1) {
+            uint4 p1 = zero, p2 = zero, p3 = zero;
+            if (bil) {
+                const uint4 As = shift1(A, r0[16]);
+                p1 = avg16(A, As);
+                if (y == 0) {  // the v and hv planes' first rows are copies (copy_row, :205, :223)
+                    p2 = A;
+                    p3 = As;
+                } else {
+                    const uint8_t *r1 = r0 + sst;
+                    const uint4 B = *reinterpret_cast<const uint4 *>(r1);
+                    p2 = avg16(A, B);
+                    p3 = avg16(A, shift1(B, r1[16]));
+                }
+            }
+            *reinterpret_cast<uint4 *>(o + pstep) = p1;
+            *reinterpret_cast<uint4 *>(o + 2 * pstep) = p2;
+            *reinterpret_cast<uint4 *>(o + 3 * pstep) = p3;
+            for (int p = 4; p < nsub; p++) *reinterpret_cast<uint4 *>(o + p * pstep) = zero;
+        }
+        return;
+    }
+    // chunks at the right edge and the last row: the closed forms of the scalar kernel
+    const bool subpel = D.pel >= 2 && D.gpu <= 1 && D.full && D.scale_up == 0;
+    for (int p = 0; p < np; p++)
+        *reinterpret_cast<uint4 *>(o + p * pstep) = level0_edge_chunk(subpel, s0, g.src_stride, w, h, g.stride, y, x0, p);
+}
+
+// reduce_6tap + horizontal_6tap_inplace (super_build.rs:254-357) for every level of one
+// plane of one frame: one CTA walks the pyramid level by level, kRows output rows at a time:
+// the vertical pass, 4 columns per thread in halfword lanes, into shared memory, then the
+// horizontal pass, 4 output bytes per thread. Each output row receives src_w bytes (dst_w
+// filtered values, then the vertical-only intermediates, :302-306) and zeros up to the pitch.
+constexpr int kRows = 8;
+__global__ void __launch_bounds__(512) super_pyramid_kernel(SuperDev D, uint8_t *__restrict__ dst) {
+    extern __shared__ __align__(16) uint8_t inter_all[];
+    const int plane = (int)(blockIdx.x % 3u);
+    const int64_t f = blockIdx.x / 3u;
+    const PlaneGeo g = plane_geo(D, plane);
+    const bool c = plane > 0;
+    const int S = (int)g.stride, SW = S >> 2;
+    uint8_t *base = dst + f * D.frame_bytes + g.out_off;
+    const int rows = (int)g.rows;
+    for (int lv = 0; lv + 1 < D.levels; lv++) {
+        const int src_w = c ? D.lw[lv] / 2 : D.lw[lv], src_h = c ? D.lh[lv] / 2 : D.lh[lv];
+        const int dst_w = c ? D.lw[lv + 1] / 2 : D.lw[lv + 1], dst_h = c ? D.lh[lv + 1] / 2 : D.lh[lv + 1];
+        const int srow0 = (int)(c ? D.row_c[lv] : D.row_y[lv]);
+        const int drow0 = (int)(c ? D.row_c[lv + 1] : D.row_y[lv + 1]);
+        const bool active = D.scale_down == 4 && dst_w > 0 && src_w > 0 && src_h > 0;
+        const int iw = (src_w + 3) >> 2;  // intermediate words per row
+        for (int r0 = 0; r0 < dst_h; r0 += kRows) {
+            const int nr = min(kRows, dst_h - r0);
+            if (active) {
+                for (int t = threadIdx.x; t < nr * iw; t += blockDim.x) {
+                    const int r = t / iw, xw = t - r * iw;
+                    const int dy = r0 + r, sy = 2 * dy;
+                    const uint32_t *col = reinterpret_cast<const uint32_t *>(base + (int64_t)srow0 * S) + xw;
+                    auto row = [&](int yy) -> uint32_t { return srow0 + yy < rows ? col[(int64_t)yy * SW] : 0u; };
+                    uint32_t v;
+                    if (dy == 0 || dy + 1 == dst_h || sy - 2 < 0 || sy + 3 >= src_h) {
+                        const int y0 = min(sy, src_h - 1), y1 = min(sy + 1, src_h - 1);
+                        v = avgu4(row(y0), row(y1));
+                    } else {
+                        const uint32_t a0 = row(sy - 2), a1 = row(sy - 1), a2 = row(sy), a3 = row(sy + 1),
+                                       a4 = row(sy + 2), a5 = row(sy + 3);
+                        const uint32_t m = 0x00FF00FFu;
+                        const uint32_t e = (a0 & m) + (a5 & m) + 5u * ((a1 & m) + (a4 & m)) +
+                                           10u * ((a2 & m) + (a3 & m)) + 0x00100010u;
+                        const uint32_t od = ((a0 >> 8) & m) + ((a5 >> 8) & m) + 5u * (((a1 >> 8) & m) + ((a4 >> 8) & m)) +
+                                            10u * (((a2 >> 8) & m) + ((a3 >> 8) & m)) + 0x00100010u;
+                        v = ((e >> 5) & m) | (((od >> 5) & m) << 8);  // each lane <= 255: weights sum to 32
+                    }
+                    reinterpret_cast<uint32_t *>(inter_all)[r * iw + xw] = v;
+                }
+            }
+            __syncthreads();
+            for (int t = threadIdx.x; t < nr * SW; t += blockDim.x) {
+                const int r = t / SW, xw = t - r * SW;
+                const int dy = r0 + r;
+                uint32_t word = 0;
+                if (active) {
+                    const uint8_t *in = inter_all + r * iw * 4;
+                    auto get = [&](int i, unsigned dflt) -> unsigned { return i < src_w ? in[i] : dflt; };
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int i = xw * 4 + q;
+                        unsigned v = 0;
+                        if (i < dst_w) {
+                            if (dst_w <= 2) {
+                                const unsigned a = get(2 * i, 0);
+                                v = avg8(a, get(2 * i + 1, a));
+                            } else if (i == 0 || i == dst_w - 1) {
+                                const unsigned a = i == 0 ? in[0] : get(2 * i, 0);
+                                v = avg8(a, get(2 * i + 1, a));
+                            } else {
+                                const unsigned left = i == 1 ? avg8(in[0], get(1, in[0])) : get(2 * i - 2, 0);
+                                const unsigned pk = get(2 * i + 3, in[src_w - 1]);
+                                const unsigned sm = left + pk + 10u * (get(2 * i, 0) + get(2 * i + 1, 0)) +
+                                                    5u * (get(2 * i - 1, 0) + get(2 * i + 2, 0)) + 16u;
+                                v = min(sm >> 5, 255u);
+                            }
+                        } else if (i < src_w) {
+                            v = in[i];
+                        }
+                        word |= v << (8 * q);
+                    }
+                }
+                if (drow0 + dy < rows) reinterpret_cast<uint32_t *>(base + (int64_t)(drow0 + dy) * S)[xw] = word;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Every row start of the source and super frames on a 16-byte boundary, 8-bit samples, and
+// no bicubic planes: the fast paths apply.
+bool vec_ok(const SuperDev &D, const void *src, const void *dst) {
+    auto a16 = [](int64_t v) { return (v & 15) == 0; };
+    return D.px_bytes == 1 && D.scale_up != 2 && D.width >= 2 && (((uintptr_t)src | (uintptr_t)dst) & 15) == 0 &&
+           a16(D.y_stride) && a16(D.c_stride) && a16(D.y_len) && a16(D.c_len) && a16(D.frame_bytes) &&
+           a16(D.src_y_stride) && a16(D.src_c_stride) && a16(D.src_y_len) && a16(D.src_c_len) &&
+           a16(D.src_frame_bytes) && D.y_rows * D.y_stride < (1ll << 31) && D.c_stride >= 4;
+}
 }  // namespace
 
 namespace {
@@ -219,9 +413,50 @@ int launch_super_t(const SuperDev &D, const T *src, T *dst, int nframes, cudaStr
 }
 }  // namespace
 
+// The fast paths: level 0 in two launches (luma, then both chroma planes), then the whole
+// pyramid in one launch of a CTA per frame and plane (enough CTAs to fill the GPU; a launch of
+// a few frames takes the per-level kernels, which spread one level over many CTAs).
+int launch_super_vec(const SuperDev &D, const uint8_t *src, uint8_t *dst, int nframes, int sms, cudaStream_t stream) {
+    int n = 0;
+    for (int pl = 0; pl < 2; pl++) {
+        const int64_t S = pl ? D.c_stride : D.y_stride;
+        const int h = pl ? D.height / 2 : D.height;
+        if (h <= 0) continue;
+        dim3 g((unsigned)((S / 16 + 127) / 128), (unsigned)h, (unsigned)(nframes * (pl ? 2 : 1)));
+        super_level0_vec_kernel<<<g, 128, 0, stream>>>(D, src, dst, pl ? 1 : 0, pl ? 2 : 1);
+        n++;
+    }
+    if (D.levels <= 1) return n;
+    if (3 * nframes >= sms) {
+        const size_t smem = (size_t)kRows * (size_t)((D.lw[0] + 3) & ~3);
+        super_pyramid_kernel<<<(unsigned)(3 * nframes), 512, smem, stream>>>(D, dst);
+        return n + 1;
+    }
+    for (int lv = 0; lv + 1 < D.levels; lv++) {
+        const int rows = D.lh[lv + 1];
+        if (rows <= 0) continue;
+        const size_t smem = (size_t)(D.lw[lv] > 0 ? D.lw[lv] : 1);
+        dim3 g((unsigned)rows, 3, (unsigned)nframes);
+        super_reduce_kernel<uint8_t><<<g, 256, smem, stream>>>(D, dst, lv);
+        n++;
+    }
+    return n;
+}
+
 cudaError_t launch_super(const SuperDev &D, const uint8_t *src, uint8_t *dst, int nframes, cudaStream_t stream,
                          int *launches) {
     if (nframes <= 0) return cudaSuccess;
+    static int sms = [] {
+        int dev = 0, v = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return 148;
+        return v;
+    }();
+    if (vec_ok(D, src, dst)) {
+        const int n = launch_super_vec(D, src, dst, nframes, sms, stream);
+        if (launches) *launches += n;
+        return cudaGetLastError();
+    }
     const int n = D.px_bytes == 2
                       ? launch_super_t(D, reinterpret_cast<const uint16_t *>(src), reinterpret_cast<uint16_t *>(dst),
                                        nframes, stream)

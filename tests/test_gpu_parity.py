@@ -55,6 +55,31 @@ def test_super_matches_oracle(w, h, opt):
             pytest.fail(f"frame {i}: {len(bad)} bytes differ, first at {bad[0]} (row {bad[0] // w})")
 
 
+MANY_CASES = [  # launches of at least 50 frames take the one-CTA-per-frame-and-plane pyramid kernel
+    (192, 108, "{pel:2}", 50),
+    (320, 240, "{pel:1, full:false}", 52),  # fewer super-frame rows than the level-0 region
+    (640, 360, "{pel:4}", 50),
+    (1280, 720, "{pel:2}", 50),
+    (200, 120, "{pel:2}", 60),               # widths that are not multiples of 16: the per-row kernels
+]
+
+
+@pytest.mark.parametrize("w,h,opt,n", MANY_CASES)
+def test_super_many_frames_matches_oracle(w, h, opt, n):
+    import os
+
+    sv = _sv()
+    clip = _clip(w, h, n, seed=w + 3 * h)
+    sb = sv.Super(w, h, opt)
+    so = orc.super_opts(w, h, opt)
+    got = sb.build_many(clip)
+    want = orc.build_super_many(so, clip, os.cpu_count() or 1)
+    for i in range(n):
+        if not np.array_equal(got[i], want[i]):
+            bad = np.nonzero(got[i] != want[i])[0]
+            pytest.fail(f"frame {i}: {len(bad)} bytes differ, first at {bad[0]}")
+
+
 ANALYSE_CASES = [
     # (w, h, super opt, analyse opt, frames)
     (640, 360, "{pel:1}", "{block:{w:16,overlap:0},main:{search:{type:2,distance:2,satd:false,coarse:{satd:false}}}}", 3),
