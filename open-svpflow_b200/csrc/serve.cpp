@@ -48,6 +48,8 @@ namespace {
 
 inline int64_t al256(int64_t v) { return (v + 255) & ~(int64_t)255; }
 
+constexpr int kCancelled = -2;  // Request::status of a request withdrawn before admission
+
 constexpr int kLanes = 4;  // streams per slot: a clip's chunks run on them round-robin
 
 struct Request;
@@ -93,7 +95,7 @@ struct svpf_server {
     std::vector<uint8_t *> retired;             // outgrown staging buffers, freed at destroy
     std::deque<Request *> pending;
     std::map<int64_t, std::unique_ptr<Request>> requests;
-    int64_t next_id = 1, admitted = 0, completed = 0;
+    int64_t next_id = 1, admitted = 0, completed = 0, cancelled = 0;
     std::atomic<int64_t> launches{0};
     std::mutex mu;
     std::condition_variable cv;       // scheduler wake-ups
@@ -369,11 +371,32 @@ int svpf_server_wait(svpf_server *s, int64_t request, int64_t *times) {
     if (times) { times[0] = r->arrival_ns; times[1] = r->admit_ns; times[2] = r->done_ns; }
     const int st = r->status;
     s->requests.erase(it);
+    if (st == kCancelled) return sfail(SVPF_ECANCELED, "request cancelled before it was admitted");
     if (st < 0) return sfail(SVPF_EINVAL, "server shut down before the request started");
     if (st & 1) return sfail(SVPF_EPANIC, "SVAnalyse: the reference indexes out of range on this input (it panics)");
     if (st == 4) return sfail(SVPF_ECUDA, "enqueueing the request failed");
     if (st) return sfail(SVPF_EUNSUP, "SVAnalyse: unsupported input on the device path");
     return SVPF_OK;
+}
+
+int svpf_server_cancel(svpf_server *s, int64_t request) {
+    if (!s) return sfail(SVPF_EINVAL, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(request);
+    if (it == s->requests.end()) return sfail(SVPF_EINVAL, "unknown request");
+    Request *r = it->second.get();
+    for (auto p = s->pending.begin(); p != s->pending.end(); ++p) {
+        if (*p != r) continue;
+        s->pending.erase(p);
+        r->status = kCancelled;
+        r->done = true;
+        r->done_ns = s->now_ns();
+        s->cancelled++;
+        s->done_cv.notify_all();
+        s->cv.notify_all();  // the request behind it may fit now
+        return SVPF_OK;
+    }
+    return sfail(SVPF_EINVAL, r->done ? "request already finished" : "request already admitted: it runs to completion");
 }
 
 int64_t svpf_server_now_ns(const svpf_server *s) { return s->now_ns(); }

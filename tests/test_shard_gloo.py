@@ -1,6 +1,9 @@
 """The multi-process path on CPU (gloo, world size 2): frame ranges with their halos cover a
-clip exactly once, ranks analysing only their own source frames reproduce the
-single-process payloads (oracle), and the timing reduction takes the slowest rank."""
+clip exactly once; the library's analyse_clip_shard / gather_payloads, with each rank analysing
+only its own slice of source frames, reproduce the single-process payloads; the timing
+reduction takes the slowest rank. The CUDA library cannot run here, so the analyser these
+ranks call is a stand-in with the library's analyse_clip signature that computes with the
+oracle (the checker); the sharding code under test is the product's."""
 import os
 import socket
 
@@ -9,7 +12,8 @@ import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from svpflow_b200.shard import clips_of_rank, frame_range, halo_range, max_over_ranks, pair_frames
+from svpflow_b200.shard import (analyse_clip_shard, clips_of_rank, frame_range, gather_payloads, halo_range,
+                                max_over_ranks, pair_frames, shard_clip)
 
 W, H, N, SOPT, AOPT = 96, 64, 7, "{pel:2}", "{delta:2,block:{w:8,overlap:2},main:{search:{type:2,distance:3}}}"
 
@@ -49,23 +53,25 @@ def _rank(rank, world, port, out):
         clip = make_clip(W, H, N, seed=21)
         so = orc.super_opts(W, H, SOPT)
         ao = orc.analyse_opts(orc.sdata(so), AOPT, None, W, H)
-        first, count = frame_range(N, world, rank)
-        lo, hi = halo_range(N, ao.delta, first, count)
-        sup = orc.build_super_many(so, clip[lo:hi])  # only this rank's frames
-        pays = [None] * count
-        for k in range(first, first + count):
-            a, b = pair_frames(N, ao.delta, k)
-            pays[k - first] = orc.analyse(ao, so, sup[a - lo], sup[b - lo])
-        gathered = [None] * world
-        dist.all_gather_object(gathered, (first, [p.tobytes() for p in pays]))
+        seen = []
+
+        class _OracleAnalyser:  # the library's Analyser.analyse_clip signature, computed by the oracle
+            delta = ao.delta
+
+            def analyse_clip(self, _sb, frames, first, count):
+                seen.append(frames.shape[0])  # only this rank's slice of source frames arrives here
+                return orc.analyse_clip(ao, so, orc.build_super_many(so, frames), first, count)
+
+        first, pays = analyse_clip_shard(_OracleAnalyser(), None, clip)
+        lo, hi, f2, count = shard_clip(N, ao.delta, world, rank)
+        assert first == f2 and len(pays) == count and seen == [hi - lo]
+        joined = gather_payloads(first, pays, N)
         slowest = max_over_ranks(1.0 + rank)
         if rank == 0:
             full = orc.analyse_clip(ao, so, orc.build_super_many(so, clip), 0, N)
-            joined = [None] * N
-            for f0, ps in gathered:
-                for i, p in enumerate(ps):
-                    joined[f0 + i] = p
-            out.put((all(joined[i] == full[i].tobytes() for i in range(N)), slowest))
+            out.put((bool(np.array_equal(joined, full)), slowest))
+        else:
+            assert joined is None
     finally:
         dist.destroy_process_group()
 
