@@ -53,11 +53,12 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
+from svpflow_b200.shard import clips_of_rank, shard_clip  # noqa: E402
 from svpflow_b200.synth import (ANALYSE_OPT, CONFIGS, SUPER_OPT, analyse_opt_for_block, batched_mix,  # noqa: E402
                                  make_clip, make_clip_device, served_stream)
 
 WORKLOAD = "1080p"  # the single-clip workload of a run: "1080p" (default) or "640x360"
-METRIC = "Analyse frame-pairs/s at 1080p (bit-exact MVs)"
+METRIC = "Analyse frame-pairs/s at 1080p (bit-exact MVs), batched vs plain; p99 latency"
 DESC = {
     "1080p": "1080p YUV420P8 {n}-frame synthetic clip per GPU, Super {s}, Analyse {a} (block 16, overlap 8, "
              "UMH r16, SATD+chroma, fwd+bwd)",
@@ -73,8 +74,18 @@ TRAFFIC_PER_PAIR = 341.8e6 / 17
 RENDER_TRAFFIC_PER_FRAME = 4.14e6
 # graph replays per timed render step (about 40 ms, so the clock sampler sees the step)
 RENDER_REPLAYS = 48
-# int32 lanes per SM on sm_100 and the SM clock ceiling, for the nominal integer peak
+# int32 lanes per SM on sm_100 (64 on the ALU pipe, 64 IMAD on the FMA-heavy pipe; ncu's pipe counters
+# of the Analyse kernel put the ALU pipe's peak at 2 warp instructions per SM cycle) and the SM clock
+# ceiling, for the nominal integer peak
 INT32_LANES_PER_SM = 128
+# integer ops per frame pair (oracle counts of the workloads' compares), when the CPU leg is skipped
+OPS_PER_PAIR = {"1080p": 19.38e9}
+# why the Analyse kernel reaches the fraction it does, from the ncu capture in
+# profiles/analyse_kernel_1080p_17f.md: issue-active x (algorithmic ops / executed lane slots)
+ROOF_DECOMPOSITION = {"issue_active": 0.358, "useful_lane_fraction": 0.19,
+                      "source": "ncu capture of a 17-pair 1080p launch (1 CTA per SM): 3.16 G warp instructions "
+                                "= 101 G lane slots per pair for 19.4 G algorithmic ops",
+                      "kernel_version": "before the level-0 look-ahead"}
 # the CPU legs time this many frame pairs per host thread, so that their figure is a throughput
 # (dynamic scheduling over many pairs) rather than the latency of the slowest pair
 CPU_PAIRS_PER_THREAD = 4
@@ -115,15 +126,18 @@ def _chain(an, nf: int, a_ms: float) -> dict:
                     "neighbours); the time per block, not issue or memory throughput, bounds one pair"}
 
 
-def _config(nframes: int, world: int) -> dict:
+def _config(nframes: int, world: int, shard_frames: bool = False) -> dict:
     c = CONFIGS[WORKLOAD]
     return {
         "workload": DESC[WORKLOAD].format(n=nframes, s=SUPER_OPT[WORKLOAD], a=ANALYSE_OPT[WORKLOAD]),
-        "width": c["width"], "height": c["height"], "frames_per_gpu": nframes,
-        "pairs_per_step": nframes * world,
+        "width": c["width"], "height": c["height"],
+        "frames_per_gpu": -(-nframes // world) if shard_frames else nframes,
+        "pairs_per_step": nframes if shard_frames else nframes * world,
         "l2": ("inputs larger than L2 (240 super frames = 3.7 GB per GPU)" if WORKLOAD == "1080p" else
                "inputs smaller than L2: a 256 MB write flushes L2 before every step, outside the timed events"),
-        "parallelism": f"dp{world} (frame ranges per GPU, no collective)" if world > 1 else "single GPU",
+        "parallelism": ((f"dp{world}: one clip split into contiguous frame ranges (svpflow_b200.shard), no collective"
+                         if shard_frames else f"dp{world}: a clip per GPU, no collective")
+                        if world > 1 else "single GPU"),
     }
 
 
@@ -786,12 +800,15 @@ def run_2160p10(args, world: int, rank: int, local: int):
             parity = {"pairs_checked": pairs, "bit_exact": bool(np.array_equal(pay_cpu, pay_host[:pairs]))}
             ops_pair = orc.integer_ops(cnt) / pairs
             int_peak = INT32_LANES_PER_SM * _sm_count() * SM_MAX_MHZ * 1e6
-            roof["integer"] = {
+            hbm = {k: roof.pop(k) for k in ("bound", "achieved", "peak", "unit", "frac", "peak_source")}
+            roof.update({
                 "bound": "int32 pipe", "achieved": ops_pair * nf / (a_ms / 1000) / 1e12, "peak": int_peak / 1e12,
                 "unit": "Tops/s", "frac": ops_pair * nf / (a_ms / 1000) / int_peak, "ops_per_pair": ops_pair,
                 "evaluations_per_pair": cnt[0] / pairs, "samples_compared_per_pair": (cnt[1] + cnt[2]) / pairs,
                 "satd_share": (cnt[3] + cnt[4]) / max(cnt[1] + cnt[2], 1),
-                "peak_source": "nominal: SMs x 128 int32 lanes x max SM clock (no measured integer peak)"}
+                "peak_source": f"nominal: {_sm_count()} SMs x {INT32_LANES_PER_SM} int32 lanes (64 ALU + 64 IMAD on "
+                               f"the FMA-heavy pipe) x {SM_MAX_MHZ:.0f} MHz; no measured integer peak exists",
+                "hbm": hbm})
         line = {
             "metric": "Analyse frame-pairs/s at 2160p 10-bit (bit-exact to the oracle)", "value": value, "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -856,7 +873,7 @@ def run_batched(args, world: int, rank: int, local: int):
     dev = torch.device("cuda", local)
     nclips = args.clips or 64
     mix = batched_mix(nclips, max_len=args.max_len or 240)
-    mine = [c for i, c in enumerate(mix) if i % world == rank]  # clips are sharded whole across ranks
+    mine = [mix[i] for i in clips_of_rank(len(mix), world, rank)]  # clips are sharded whole across ranks
     c2 = CONFIGS["1080p"]
     clips = []
     t0 = time.perf_counter()
@@ -1130,6 +1147,10 @@ def main():
     ap.add_argument("--chunk", type=int, default=32, help="served: output frames per launch")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--shape", default="", help="batched: fixed launch shape name[:tiles_per_lane], no autotune")
+    ap.add_argument("--no-lookahead", action="store_true", help="Analyse without look-ahead (A/B timing)")
+    ap.add_argument("--lookahead", type=int, default=1, help="look-ahead levels: 1 level 0, 2 coarser, 3 all")
+    ap.add_argument("--shard", default="clips", choices=["clips", "frames"],
+                    help="N>1: a clip per GPU (weak scaling, default) or one clip split in frame ranges (strong)")
     ap.add_argument("--no-sub", action="store_true",
                     help="1080p: leave out the batched and served objects of the default line")
     args = ap.parse_args()
@@ -1164,15 +1185,26 @@ def main():
     dev = torch.device("cuda", local)
     c = CONFIGS[WORKLOAD]
     w, h, nf = c["width"], c["height"], args.frames or c["frames"]
-    clip = make_clip(w, h, nf, seed=1000 + rank, motion=c["motion"], objects=c["objects"],
-                     object_motion=c["object_motion"])
     sb = sv.Super(w, h, SUPER_OPT[WORKLOAD])
     an = sv.Analyse(sb.sdata, ANALYSE_OPT[WORKLOAD], w, h)
+    an.set_lookahead(0 if args.no_lookahead else args.lookahead)
+    shard_frames = args.shard == "frames" and world > 1
+    if shard_frames:  # one clip split into frame ranges (strong scaling): this rank's slice and outputs
+        clip = make_clip(w, h, nf, seed=1000, motion=c["motion"], objects=c["objects"],
+                         object_motion=c["object_motion"])
+        lo, hi, a_first, a_count = shard_clip(nf, an.delta, world, rank)
+        clip = np.ascontiguousarray(clip[lo:hi])
+        a_first -= lo
+    else:  # a clip per rank (weak scaling)
+        clip = make_clip(w, h, nf, seed=1000 + rank, motion=c["motion"], objects=c["objects"],
+                         object_motion=c["object_motion"])
+        a_first, a_count = 0, nf
+    n_src = clip.shape[0]  # source frames this rank uploads and builds super frames for
     fb, pl = sb.output_len(), an.payload_len()
     frames_d = torch.from_numpy(clip).to(dev)
-    supers_d = torch.empty((nf, fb), dtype=torch.uint8, device=dev)
-    pay_d = torch.empty((nf, pl), dtype=torch.uint8, device=dev)
-    scratch_d = torch.empty(an.scratch_bytes(nf), dtype=torch.uint8, device=dev)
+    supers_d = torch.empty((n_src, fb), dtype=torch.uint8, device=dev)
+    pay_d = torch.empty((a_count, pl), dtype=torch.uint8, device=dev)
+    scratch_d = torch.empty(an.scratch_bytes(a_count), dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
 
@@ -1184,10 +1216,11 @@ def main():
             flush.fill_(1)
         if ev:
             ev[0].record(stream)
-        sb.build_device(frames_d.data_ptr(), supers_d.data_ptr(), nf, sh)
+        sb.build_device(frames_d.data_ptr(), supers_d.data_ptr(), n_src, sh)
         if ev:
             ev[1].record(stream)
-        an.analyse_clip_device(supers_d.data_ptr(), nf, 0, nf, pay_d.data_ptr(), scratch_d.data_ptr(), sh)
+        an.analyse_clip_device(supers_d.data_ptr(), n_src, a_first, a_count, pay_d.data_ptr(), scratch_d.data_ptr(),
+                               sh)
         if ev:
             ev[2].record(stream)
 
@@ -1212,6 +1245,7 @@ def main():
     if world > 1:
         dist.barrier()
     sv.Analyser.device_status(scratch_d.data_ptr(), sh)
+    la = sv.Analyser.lookahead_stats(scratch_d.data_ptr(), sh)  # the last step's level-0 look-ahead counters
     ms = start.elapsed_time(stop)
     super_ms = [e[0].elapsed_time(e[1]) for e in evs]
     analyse_ms = [e[1].elapsed_time(e[2]) for e in evs]
@@ -1221,14 +1255,15 @@ def main():
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
-    value = nf * world * args.steps / (ms_max / 1000.0)
+    total_pairs = nf if shard_frames else nf * world  # output frames of the whole job per step
+    value = total_pairs * args.steps / (ms_max / 1000.0)
 
     # end to end through the host-buffer API: pinned host frames in, payloads out
     pinned = torch.from_numpy(clip).pin_memory()
     host_frames = pinned.numpy()
-    out_host = torch.empty((nf, pl), dtype=torch.uint8).pin_memory().numpy()
+    out_host = torch.empty((a_count, pl), dtype=torch.uint8).pin_memory().numpy()
     def e2e_step():
-        rc = sv.lib().svpf_clip_analyse(an.handle, sb.handle, host_frames.ctypes.data, nf, 0, nf,
+        rc = sv.lib().svpf_clip_analyse(an.handle, sb.handle, host_frames.ctypes.data, n_src, a_first, a_count,
                                         out_host.ctypes.data)
         if rc:
             raise RuntimeError(sv.lib().svpf_last_error().decode())
@@ -1246,7 +1281,7 @@ def main():
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = nf * world * args.e2e_steps / float(t.item())
+        e2e_value = total_pairs * args.e2e_steps / float(t.item())
         same = bool(np.array_equal(out_host, pay_d.cpu().numpy()))
 
     line = None
@@ -1254,42 +1289,50 @@ def main():
         peak, peak_kind = _peaks()
         a_ms = statistics.mean(analyse_ms)
         s_ms = statistics.mean(super_ms)
-        alg_analyse = nf * (2 * fb + pl)  # algorithmic bytes of one Analyse launch: 2 super frames + payload per pair
-        alg_super = nf * (sb.source_len() + fb)  # one Super launch sequence: source read + super frame write
-        roof = {
-            "kernel": "analyse_kernel (one CTA per frame pair, fwd/bwd halves)",
-            "bound": "hbm", "achieved": alg_analyse / (a_ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
-            "frac": alg_analyse / (a_ms / 1000) / 1e9 / peak,
-            "traffic": TRAFFIC_PER_PAIR * nf if WORKLOAD == "1080p" else None,
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 17-pair launch, per pair x pairs",
-            "peak_source": peak_kind,
-            "algorithmic_bytes_per_launch": alg_analyse, "avg_launch_ms": a_ms,
-            "note": "integer- and dependency-chain-bound block search; the HBM fraction shows how far from "
-                    "HBM-bound it is",
-            "super": {"bound": "hbm", "achieved": alg_super / (s_ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
-                      "frac": alg_super / (s_ms / 1000) / 1e9 / peak, "avg_launch_ms": s_ms,
-                      "algorithmic_bytes_per_launch": alg_super},
-        }
+        alg_analyse = a_count * (2 * fb + pl)  # algorithmic bytes of one Analyse launch: 2 super frames + payload per pair
+        alg_super = n_src * (sb.source_len() + fb)  # one Super launch sequence: source read + super frame write
+        int_peak = INT32_LANES_PER_SM * _sm_count() * SM_MAX_MHZ * 1e6
+        ops_pair = OPS_PER_PAIR.get(WORKLOAD)
+        ops_src = "constant from an earlier oracle count of the same workload (CPU leg not run)"
         cpu = None
         parity = None
+        cnt = None
         if not args.no_cpu:
             threads = os.cpu_count() or 1
-            pairs = min(args.cpu_pairs or CPU_PAIRS_PER_THREAD * threads, nf - 1)
+            pairs = min(args.cpu_pairs or CPU_PAIRS_PER_THREAD * threads, a_count - 1)
             dt, pay_cpu, _ = cpu_reference(nf, threads, pairs, seed=1000 + rank)
             from oracle import oracle as orc
 
             cnt = cpu_reference.counters
             ops_pair = orc.integer_ops(cnt) / pairs
-            int_peak = INT32_LANES_PER_SM * _sm_count() * SM_MAX_MHZ * 1e6
-            roof["integer"] = {
-                "bound": "int32 pipe", "achieved": ops_pair * nf / (a_ms / 1000) / 1e12,
-                "peak": int_peak / 1e12, "unit": "Tops/s", "frac": ops_pair * nf / (a_ms / 1000) / int_peak,
-                "ops_per_pair": ops_pair, "evaluations_per_pair": cnt[0] / pairs,
-                "samples_compared_per_pair": (cnt[1] + cnt[2]) / pairs,
-                "satd_share": (cnt[3] + cnt[4]) / max(cnt[1] + cnt[2], 1),
-                "ops_source": f"compares the oracle executed on output frames 0..{pairs - 1} (2 ops per SAD "
-                              f"sample, 111 per SATD 4x4 tile)",
-                "peak_source": "nominal: SMs x 128 int32 lanes x max SM clock (no measured integer peak)"}
+            ops_src = (f"compares the oracle executed on output frames 0..{pairs - 1} (2 ops per SAD sample, 111 "
+                       f"per SATD 4x4 tile)")
+        # the Analyse kernel's primary bound: the int32 pipes (no dense contraction, little HBM traffic)
+        roof = {
+            "kernel": "analyse_kernel (one CTA per frame pair, fwd/bwd halves; level 0 one block per warp)",
+            "bound": "int32 pipe", "unit": "Tops/s", "peak": int_peak / 1e12,
+            "achieved": ops_pair * a_count / (a_ms / 1000) / 1e12 if ops_pair else None,
+            "frac": ops_pair * a_count / (a_ms / 1000) / int_peak if ops_pair else None,
+            "traffic": TRAFFIC_PER_PAIR * a_count if WORKLOAD == "1080p" else None,
+            "traffic_unit": "bytes per launch",
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 17-pair launch, per pair x pairs",
+            "ops_per_pair": ops_pair, "ops_source": ops_src, "avg_launch_ms": a_ms,
+            "peak_source": f"nominal: {_sm_count()} SMs x {INT32_LANES_PER_SM} int32 lanes (64 on the ALU pipe + 64 "
+                           f"IMAD on the FMA-heavy pipe) x {SM_MAX_MHZ:.0f} MHz; no measured integer peak exists",
+            "decomposition": ROOF_DECOMPOSITION,
+            "hbm": {"bound": "hbm", "achieved": alg_analyse / (a_ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+                    "frac": alg_analyse / (a_ms / 1000) / 1e9 / peak, "peak_source": peak_kind,
+                    "algorithmic_bytes_per_launch": alg_analyse,
+                    "note": "2 super frames + payload per pair: far from HBM-bound"},
+            "super": {"bound": "hbm", "achieved": alg_super / (s_ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+                      "frac": alg_super / (s_ms / 1000) / 1e9 / peak, "avg_launch_ms": s_ms,
+                      "algorithmic_bytes_per_launch": alg_super, "peak_source": peak_kind},
+        }
+        if cnt is not None:
+            roof["evaluations_per_pair"] = cnt[0] / pairs
+            roof["samples_compared_per_pair"] = (cnt[1] + cnt[2]) / pairs
+            roof["satd_share"] = (cnt[3] + cnt[4]) / max(cnt[1] + cnt[2], 1)
+        if not args.no_cpu:
             cpu = {"value": pairs / dt, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"output frames 0..{pairs - 1} of the same clip (Super + Analyse), "
                              f"{pairs / threads:.1f} frame pairs per host thread on {threads} threads (throughput), "
@@ -1299,17 +1342,23 @@ def main():
                       "bit_exact": bool(np.array_equal(pay_cpu, pay_d[:pairs].cpu().numpy()))}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8", "data": "synthetic", "config": _config(nf, world),
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "strong" if shard_frames else "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic", "config": _config(nf, world, shard_frames),
             "clocks": clk.summary(),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(clip.nbytes),
-                    "d2h_bytes_per_step": int(nf * pl), "api": "svpf_clip_analyse (host buffers)",
+                    "d2h_bytes_per_step": int(a_count * pl), "api": "svpf_clip_analyse (host buffers)",
                     "matches_device_path": same},
             "gpu_launches": int(launches),
             "roofline": roof,
             "cpu_baseline": cpu,
             "parity_vs_oracle": parity,
-            "serial_chain": _chain(an, nf, a_ms),
+            "serial_chain": _chain(an, a_count, a_ms),
+            "lookahead": {**la, "levels": 0 if args.no_lookahead else args.lookahead,
+                          "rerun_fraction": la["reruns"] / la["blocks"] if la["blocks"] else None,
+                          "note": "one block per warp in flight; each block re-checks the neighbour seeds "
+                                  "committed after it started and re-runs its refinement when one wins "
+                                  "(level-0 counters of the last timed step)"},
             "super_ms_per_step": statistics.mean(super_ms), "analyse_ms_per_step": statistics.mean(analyse_ms),
         }
         if world == 1 and WORKLOAD == "1080p" and not args.no_sub:

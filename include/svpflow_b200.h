@@ -34,6 +34,7 @@ typedef struct svpf_analyser svpf_analyser;
 #define SVPF_ECUDA (-2)    /* CUDA runtime error or no usable device */
 #define SVPF_EPANIC (-3)   /* input on which the reference indexes out of range (it would panic) */
 #define SVPF_EUNSUP (-4)   /* option combination not available on the device path */
+#define SVPF_ECANCELED (-5) /* served request cancelled before it was admitted (svpf_server_cancel) */
 
 /* Thread-local text of the last error. */
 const char *svpf_last_error(void);
@@ -113,16 +114,28 @@ int svpf_clip_analyse_device(const svpf_analyser *a, const uint8_t *supers_dev, 
 /* Status of the last device launch that used `scratch_dev` (synchronises `stream`):
  * SVPF_OK, or SVPF_EPANIC when a pair hit an input the reference cannot process. */
 int svpf_device_status(const void *scratch_dev, void *stream);
+/* No counterpart in the reference (a tuning knob). Level 0 runs with look-ahead by default:
+ * each warp of a search direction takes its own block in the reference's order, searches it
+ * without the neighbour vectors not yet committed, then, in order, re-checks the reference's
+ * selection with them and repeats the refinement when one wins; results are bit-identical
+ * with it on or off. `levels`: 0 off, 1 level 0 only (the default), 2 the coarser levels only,
+ * 3 every level. Affects launches made after the call. */
+int svpf_analyser_set_lookahead(svpf_analyser *a, int32_t levels);
+/* The look-ahead counters of the last device launch on `scratch_dev` (synchronises `stream`):
+ * out[0] level-0 blocks, out[1] blocks with deferred neighbour seeds, out[2] deferred seeds
+ * evaluated, out[3] refinements run again. */
+int svpf_device_lookahead_stats(const void *scratch_dev, void *stream, int64_t out[4]);
 /* No counterpart in the reference. The same Analyse over a clip as
  * svpf_clip_analyse_device, for callers that cannot allocate device memory (a frame
  * server's per-frame callback, where cudaMalloc can synchronise the device and stall other
  * streams, or a host that forbids allocations after start-up): the kernel's scratch is a
  * fixed 32 MiB array inside this library (every GPU that loads the library holds it until
  * exit), so no scratch argument is taken and nothing is allocated. Returns SVPF_EINVAL when
- * `count` pairs need more than that array (use fewer pairs per call). The first call on a
- * device looks the array up (set-up); make that first call before any stream capture. Calls
- * share the array: calls whose kernels overlap on the GPU race, so order them on one
- * stream. Synchronises `stream` and returns the kernel's status (SVPF_OK, SVPF_EPANIC). */
+ * `count` pairs need more than that array (use fewer pairs per call). Every call looks the
+ * array's device address up in the current context. Calls share the array: calls whose
+ * kernels overlap on the GPU race, so order them on one stream. Synchronises `stream` and
+ * returns the kernel's status (SVPF_OK, SVPF_EPANIC); because it synchronises, it must not
+ * be called on a stream that is being captured into a CUDA graph. */
 int svpf_clip_analyse_device_noalloc(const svpf_analyser *a, const uint8_t *supers_dev, int32_t nframes,
                                      int32_t first, int32_t count, uint8_t *payloads_dev, void *stream);
 /* Whole clip from host source frames: Super over every frame, then Analyse for output
@@ -313,6 +326,11 @@ int svpf_server_submit(svpf_server *s, const svpf_super *sup, const svpf_analyse
 /* Blocks until the request finished and returns its status; times[0..2] (optional)
  * receive its arrival, admission and completion times on the server clock. */
 int svpf_server_wait(svpf_server *s, int64_t request, int64_t *times);
+/* Withdraws a request that has not been admitted yet: it never runs, its buffers are no longer
+ * used when this returns SVPF_OK, and svpf_server_wait on it returns SVPF_ECANCELED. A request
+ * already admitted runs to completion (its work is queued on the device): SVPF_EINVAL, as for
+ * an unknown or finished request. */
+int svpf_server_cancel(svpf_server *s, int64_t request);
 int64_t svpf_server_now_ns(const svpf_server *s);       /* the server clock, ns */
 void svpf_server_stats(svpf_server *s, int64_t *admitted, int64_t *completed, int64_t *peak_device_bytes,
                        int32_t *peak_active, int64_t *kernel_launches);

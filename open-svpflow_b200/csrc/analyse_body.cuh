@@ -69,7 +69,12 @@ enum : uint8_t { LM_DIRECT = 1, LM_SATD_MASK = 2, LM_SAD_BREAK = 3, LM_EDGE = 4,
 enum : uint8_t { CM_NONE = 0, CM_DIRECT = 1, CM_SAD_BREAK = 3, CM_EDGE = 4 };
 enum : int { BK_EXH = 1, BK_UMH, BK_HEX6, BK_HEX3, BK_RING };
 
-constexpr int ST_PANIC = 1;  // status bit: the reference indexes out of range here (it would panic)
+constexpr int ST_PANIC = 1;    // status bit: the reference indexes out of range here (it would panic)
+constexpr int ST_TIMEOUT = 4;  // status bit: a bounded wait inside the kernel ran out (internal error)
+// A wait on another warp's commit gives up after this many SM cycles (about 0.5 s at 1.9 GHz;
+// a level-0 block takes well under a millisecond). After one wait of a direction has given
+// up, its other waits return at once, so a failure costs one bound, not one per block.
+constexpr long long kWaitCycles = 1000000000LL;
 
 struct Cand {
     int64_t l_sbase, l_rbase, c_sbase, c_rbase;  // flat bases of the direct read paths
@@ -80,22 +85,30 @@ struct Cand {
     uint8_t lmode, cmode, lsatd, csatd;
 };
 
+// Shared state of one search direction. A block is searched by a group of warps: the whole
+// direction (coarser levels), or one warp (level 0 with look-ahead, one block per warp in
+// flight). Per-warp entries are indexed by the warp's place in the direction; a group's
+// entries are those of its first warp (Ctx::wbase).
 struct DirSh {
     long long K[2][NW];                   // per-warp best (cost, index, sad) of a step, double-buffered
     int I[2][NW];
     unsigned S[2][NW];
-    unsigned slotL[2][MAXSLOT];                     // special-candidate results (exact_sad values)
-    long long rk[2][NGMAX], rm[2][NGMAX];           // exact sequential scan: per-group cost, motion
+    unsigned slotL[NW][2][MAXSLOT];       // per group: special-candidate results (exact_sad values)
+    long long rk[2][NGMAX], rm[2][NGMAX]; // exact sequential scan: per-group cost, motion
     unsigned rs[2][NGMAX];
     int ri[2][NGMAX];
     unsigned char rv[2][NGMAX];
+    int committed;                        // look-ahead: blocks of the level committed so far (in order)
+    int late_;                            // look-ahead: a hand-over wait gave up
+    int unsafe_;                          // look-ahead: the level has an input the reference panics on
+    int bad_count;                        // look-ahead: bad-SAD blocks committed so far (:605)
     int gx, gy;           // global predictor (doubled) for the next level
     int order_len;
     int abort_;
-    // The block's source pixels, 4 per entry: luma (bw/4 x bh), then U and V (cw/4 x crows).
-    // A plane searched with SATD holds 16-bit pairs (x = pixels 0,1; y = pixels 2,3), a
-    // SAD plane the packed word in x.
-    uint2 srcp[384];
+    // Per group: the block's source pixels, 4 per entry: luma (bw/4 x bh), then U and V
+    // (cw/4 x crows). A plane searched with SATD holds 16-bit pairs (x = pixels 0,1;
+    // y = pixels 2,3), a SAD plane the packed word in x.
+    uint2 srcp[NW][384];
     int2 clist[NW][32 * MW];  // per warp: the step's candidates passing the cuts, in order (mv, index)
     long long r64[NW][3];
     int r32[NW][2];
@@ -612,10 +625,18 @@ struct Ctx {
     Geo G;
     Planes S, R;
     int level, d, tid, satd, pel;
+    int nw, wbase;   // warps of the group searching the block, and its first warp in the direction;
+                     // tid is the thread's index in that group
     int grp_lanes;   // G: lanes per candidate (power of two)
     int pnew;        // new-candidate penalty of the current search (opts.pnew; pnew / factor in the refine pass)
     int tl, tcp;     // 4x4 luma tiles, 4x4 tiles per chroma plane of one candidate
 };
+
+// Barrier of the group searching a block: the direction's named barrier, or the warp.
+__device__ __forceinline__ void gsync(const Ctx &x) {
+    if (x.nw == 1) __syncwarp();
+    else dbar(x.d);
+}
 
 // Per-block constants, identical in every thread of a direction.
 struct BlkC {
@@ -734,15 +755,19 @@ __device__ __noinline__ Res slow_lane(const AnalyseParams *P, const LevelInfo *L
 // Lanes per candidate for a step of n candidates: the widest power-of-two group (at most a
 // warp, at least the level's G) that still puts every candidate in one round. Small steps
 // (a hexagon, a ring, the special candidates) then finish in fewer tiles per lane.
-__device__ __forceinline__ int step_lanes(int G, int n) {
-    while (G < 32 && NW * (16 / G) >= n) G <<= 1;
+__device__ __forceinline__ int step_lanes(int G, int n, int nw) {
+    while (G < 32 && nw * (16 / G) >= n) G <<= 1;
     return G;
 }
 
 // Work of one lane (`sub` of G) on one candidate: its share of the 4x4 tiles.
 // kind 0: block at (b.px, b.py); 1: the same mv on the block at (px, py) (general path);
 // 2: the block's luma pixel sum (block_luma_dc).
+#ifdef SVPF_EVAL_NOINLINE
+__device__ __noinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, int px, int py, int mvx, int mvy,
+#else
 __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, int px, int py, int mvx, int mvy,
+#endif
                                          bool chroma, int sub, int G) {
     const int TL = x.tl, TCp = x.tcp;
     int lref = 0, cref = 0;
@@ -807,7 +832,7 @@ __device__ __forceinline__ void finalize(const Res &r, unsigned &L, unsigned &C)
 // and the new best cost / sad when accepted.
 __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s, int &ph, const Gen &g, int lambda,
                                           int predx, int predy, long long &best_cost, unsigned &best_sad, int &win) {
-    const int lane = x.tid & 31, warp = x.tid >> 5;
+    const int lane = x.tid & 31, warp = x.tid >> 5, wi = x.wbase + warp;  // wi: the warp's place in the direction
     const bool serial = x.pnew < -256;
     const int pnew = x.pnew;
     long long bk = 0x7FFFFFFFFFFFFFFFLL;
@@ -833,20 +858,21 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
             }
             const unsigned m = __ballot_sync(0xFFFFFFFFu, ok);
             if (ok)  // |mv| <= pel * plane size, so each component fits a halfword
-                s.clist[warp][total + __popc(m & lt_mask)] =
+                s.clist[wi][total + __popc(m & lt_mask)] =
                     make_int2((int)(((unsigned)mv.x & 0xFFFFu) | ((unsigned)mv.y << 16)), i);
             total += __popc(m);
         }
         __syncwarp();
-        const int G = step_lanes(x.grp_lanes, total);
-        const int grp = warp * (32 / G) + lane / G, sub = lane & (G - 1), NG = NW * (32 / G);
+        const int G = step_lanes(x.grp_lanes, total, x.nw);
+        const int grp = warp * (32 / G) + lane / G, sub = lane & (G - 1), NG = x.nw * (32 / G);
+        const int rb = x.wbase * 32;  // the group's entries of the sequential-scan arrays
         for (int r0 = 0; r0 < total; r0 += NG) {
             const int rk = r0 + grp;
             const bool act = rk < total;
             int i = 0;
             int2 mv = make_int2(0, 0);
             if (act) {  // the rk-th passing candidate
-                const int2 e = s.clist[warp][rk];
+                const int2 e = s.clist[wi][rk];
                 i = e.y;
                 mv = make_int2((int)(short)(e.x & 0xFFFF), e.x >> 16);
             }
@@ -874,7 +900,7 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                 for (; t < x.tl; t += G) {
                     const int ty = t >> b.lgtx, tx = t & (b.tilesx - 1);
                     const px_t *rp = rl + (ty * 4 * ys + tx * 4);
-                    const uint2 *sp = s.srcp + ((ty * 4) << b.lgtx) + tx;
+                    const uint2 *sp = s.srcp[x.wbase] + ((ty * 4) << b.lgtx) + tx;
                     r.L += b.satd_mode ? tile_satd_p(sp, b.tilesx, rp, ys) : tile_sad_p(sp, b.tilesx, rp, ys);
                 }
 #pragma unroll 1
@@ -885,7 +911,7 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                     const int ty = ct >> b.lgctx, tx = ct & (b.ctilesx - 1);
                     if (ty * 4 >= b.crows) continue;
                     const px_t *rp = (pl ? x.R.v : x.R.u) + cref + (ty * 4 * cs + tx * 4);
-                    const uint2 *sp = s.srcp + nlw + pl * b.ctilesx * b.crows + ((ty * 4) << b.lgctx) + tx;
+                    const uint2 *sp = s.srcp[x.wbase] + nlw + pl * b.ctilesx * b.crows + ((ty * 4) << b.lgctx) + tx;
                     const unsigned v = x.satd ? tile_satd_p(sp, b.ctilesx, rp, cs) : tile_sad_p(sp, b.ctilesx, rp, cs);
                     if (pl) r.V += v; else r.U += v;
                 }
@@ -902,12 +928,12 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
             }
             if (serial) {  // exact sequential semantics for penalties that can be negative
                 if (sub == 0) {
-                    s.rk[ph][grp] = K; s.rm[ph][grp] = motion; s.rs[ph][grp] = sad; s.rv[ph][grp] = act;
-                    s.ri[ph][grp] = i;
+                    s.rk[ph][rb + grp] = K; s.rm[ph][rb + grp] = motion; s.rs[ph][rb + grp] = sad;
+                    s.rv[ph][rb + grp] = act; s.ri[ph][rb + grp] = i;
                 }
-                dbar(x.d);
+                gsync(x);
                 const int m = imin(NG, total - r0);
-                for (int j = 0; j < m; j++) {
+                for (int j = rb; j < rb + m; j++) {
                     if (s.rm[ph][j] >= best_cost) continue;
                     if (s.rk[ph][j] < best_cost) { best_cost = s.rk[ph][j]; best_sad = s.rs[ph][j]; win = s.ri[ph][j]; }
                 }
@@ -926,14 +952,15 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
         const unsigned os = __shfl_xor_sync(0xFFFFFFFFu, bs, o);
         if (ok_ < bk || (ok_ == bk && oi < bi)) { bk = ok_; bi = oi; bs = os; }
     }
-    if (lane == 0) { s.K[ph][warp] = bk; s.I[ph][warp] = bi; s.S[ph][warp] = bs; }
-    dbar(x.d);
-    bk = s.K[ph][0]; bi = s.I[ph][0]; bs = s.S[ph][0];
-#pragma unroll
-    for (int w = 1; w < NW; w++) {
-        const long long k = s.K[ph][w];
-        const int ii = s.I[ph][w];
-        if (k < bk || (k == bk && ii < bi)) { bk = k; bi = ii; bs = s.S[ph][w]; }
+    if (x.nw > 1) {  // combine the group's warps (one warp already holds its result in every lane)
+        if (lane == 0) { s.K[ph][wi] = bk; s.I[ph][wi] = bi; s.S[ph][wi] = bs; }
+        gsync(x);
+        bk = s.K[ph][x.wbase]; bi = s.I[ph][x.wbase]; bs = s.S[ph][x.wbase];
+        for (int w = x.wbase + 1; w < x.wbase + x.nw; w++) {
+            const long long k = s.K[ph][w];
+            const int ii = s.I[ph][w];
+            if (k < bk || (k == bk && ii < bi)) { bk = k; bi = ii; bs = s.S[ph][w]; }
+        }
     }
     ph ^= 1;
     if (bi != 0x7FFFFFFF && bk < best_cost) { best_cost = bk; best_sad = bs; win = bi; }
@@ -1055,16 +1082,18 @@ enum { S_REFINE, S_HEX_START, S_HEX_ITER, S_HEX_EXIT, S_BAD, S_BAD_RING, S_FINAL
 __device__ __forceinline__ void stage_source(const Ctx &x, DirSh &s, const BlkC &b) {
     if (b.fast_src) {
         const int nlw = b.tilesx * b.bh;
-        for (int t = x.tid; t < nlw; t += NT) {
+        const int nth = x.nw * 32;
+        uint2 *sp = s.srcp[x.wbase];
+        for (int t = x.tid; t < nlw; t += nth) {
             const int row = t >> b.lgtx, col = t & (b.tilesx - 1);
-            s.srcp[t] = stage4(x.S.y + b.lsrc + row * x.G.ys32 + col * 4, b.satd_mode != 0);
+            sp[t] = stage4(x.S.y + b.lsrc + row * x.G.ys32 + col * 4, b.satd_mode != 0);
         }
         if (b.chroma && b.cfast_src) {
             const int nc = b.ctilesx * b.crows;
-            for (int t = x.tid; t < 2 * nc; t += NT) {
+            for (int t = x.tid; t < 2 * nc; t += nth) {
                 const int pl = t >= nc, u = t - pl * nc;
                 const int row = u >> b.lgctx, col = u & (b.ctilesx - 1);
-                s.srcp[nlw + t] = stage4((pl ? x.S.v : x.S.u) + b.csrc + row * x.G.cs32 + col * 4, x.satd != 0);
+                sp[nlw + t] = stage4((pl ? x.S.v : x.S.u) + b.csrc + row * x.G.cs32 + col * 4, x.satd != 0);
             }
         }
     }
@@ -1074,8 +1103,17 @@ __device__ __forceinline__ void stage_source(const Ctx &x, DirSh &s, const BlkC 
 // exact_hex2 :942-1033, exact_umh :1036-1119, the expansion :611-672): a state machine
 // replicated in every thread of the direction, issuing one evaluation step at a time.
 // (ppx, ppy): predictor of the motion penalty; (own_x, own_y): the block's own predictor,
-// which the bad-SAD expansion switches to.
-__device__ __forceinline__ void run_search_steps(const Ctx &x, const BlkC &b, DirSh &s, int &ph, bool refine, int stype,
+// which the bad-SAD expansion switches to. `stage`: RS_ALL runs the refinement and the
+// expansion, RS_REFINE_ONLY stops where the expansion's test begins, RS_BAD_ONLY starts
+// there (the look-ahead runs the two apart: the test reads the bad count of the blocks
+// committed before), RS_NONE runs nothing.
+enum { RS_NONE, RS_ALL, RS_REFINE_ONLY, RS_BAD_ONLY };
+#ifdef SVPF_RS_NOINLINE
+__device__ __noinline__ void run_search_steps(
+#else
+__device__ __forceinline__ void run_search_steps(
+#endif
+const Ctx &x, const BlkC &b, DirSh &s, int &ph, int stage, int stype,
                                                  int radius, int lambda, int ppx, int ppy, int own_x, int own_y,
                                                  int64_t idx, int &bad_count, int &bmx, int &bmy, unsigned &bsad,
                                                  long long &bcost) {
@@ -1083,13 +1121,17 @@ __device__ __forceinline__ void run_search_steps(const Ctx &x, const BlkC &b, Di
     const LevelInfo &L = *x.L;
     const int level = x.level;
     int predx = ppx, predy = ppy;
-    int state = refine ? S_REFINE : S_STORE;
+    int state = stage == RS_NONE ? S_STORE : (stage == RS_BAD_ONLY ? S_BAD : S_REFINE);
     int hbx = 0, hby = 0, hdir = -2, hi = 0, hrad = 0, hret = 0, bad_r = 0, bad_max = 0;
     unsigned found = 0;
     for (;;) {
         Gen g{0, 0, 0, 0, 0, 0, 0};
         bool sets_mv = true, issue = false;
         while (!issue && state != S_STORE) {
+            if (state == S_BAD && stage == RS_REFINE_ONLY) {
+                state = S_STORE;
+                break;
+            }
             if (state == S_REFINE) {
                 if (stype == 4) { g = make_gen(BK_EXH, bmx, bmy, radius, 0, 0); issue = true; state = S_BAD; }
                 else if (stype == 3) {
@@ -1241,8 +1283,9 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
         n += nseeds;
         const int dcslot = n++;
         // ---- evaluate the special slots
-        const int G = step_lanes(x.grp_lanes, n);
-        const int grp = warp * (32 / G) + lane / G, sub = lane & (G - 1), NG = NW * (32 / G);
+        const int G = step_lanes(x.grp_lanes, n, x.nw);
+        const int grp = warp * (32 / G) + lane / G, sub = lane & (G - 1), NG = x.nw * (32 / G);
+        unsigned (*slotL)[MAXSLOT] = s.slotL[x.wbase];
         for (int j0 = 0; j0 < n; j0 += NG) {
             const int j = j0 + grp;
             const bool act = j < n;
@@ -1266,14 +1309,14 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
                 unsigned Lv, Cv;
                 if (kind == 2) { Lv = r.L; Cv = 0; }
                 else finalize(r, Lv, Cv);
-                s.slotL[ph][j] = ch ? sat_add(Lv, Cv) : Lv;  // exact_sad: luma (+ chroma)
+                slotL[ph][j] = ch ? sat_add(Lv, Cv) : Lv;  // exact_sad: luma (+ chroma)
             }
         }
-        dbar(x.d);
+        gsync(x);
         const int phs = ph;
         ph ^= 1;
         // ---- selection among the special candidates (:716-747)
-        const unsigned pred_score = rs_slot >= 0 ? s.slotL[phs][rs_slot] : interp.y;
+        const unsigned pred_score = rs_slot >= 0 ? slotL[phs][rs_slot] : interp.y;
         const bool field_valid = pred_score != 0xFFFFFFFFu;
         int bmx = 0, bmy = 0;
         unsigned bsad;
@@ -1281,31 +1324,31 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
         bool refine = false;
         int lambda = 0, radius = 0, stype = 0, ppx = imv.x, ppy = imv.y;
         if (level == 0 && P.distance == 0) {
-            if (field_valid) { bmx = imv.x; bmy = imv.y; bsad = s.slotL[phs][0]; }
-            else bsad = s.slotL[phs][zslot];
+            if (field_valid) { bmx = imv.x; bmy = imv.y; bsad = slotL[phs][0]; }
+            else bsad = slotL[phs][zslot];
             bcost = (long long)bsad;
         } else {
-            if (field_valid) { bmx = imv.x; bmy = imv.y; bsad = s.slotL[phs][0]; bcost = (long long)bsad; }
+            if (field_valid) { bmx = imv.x; bmy = imv.y; bsad = slotL[phs][0]; bcost = (long long)bsad; }
             else { bsad = 0xFFFFFFFFu; bcost = 0x7FFFFFFFFFFFFFFFLL; }
             if (prev_slot >= 0) {
-                const unsigned sd = s.slotL[phs][prev_slot];
+                const unsigned sd = slotL[phs][prev_slot];
                 const long long cst = (long long)sd + (((long long)P.prev * sd) >> 8);
                 if (cst < bcost) { bmx = pmx; bmy = pmy; bsad = sd; bcost = cst; ppx = pmx; ppy = pmy; }
             }
             {
-                const unsigned sd = s.slotL[phs][gslot];
+                const unsigned sd = slotL[phs][gslot];
                 const long long cst = (long long)sd + (((long long)P.pglobal * sd) >> 8);
                 if (cst < bcost) { bmx = gxv; bmy = gyv; bsad = sd; bcost = cst; }
             }
             {
-                const unsigned sd = s.slotL[phs][zslot];
+                const unsigned sd = slotL[phs][zslot];
                 const long long cst = (long long)sd + (((long long)P.pzero * sd) >> 8);
                 if (cst < bcost) { bmx = 0; bmy = 0; bsad = sd; bcost = cst; }
             }
 #pragma unroll
             for (int q = 0; q < 8; q++) {
                 if (q >= nseeds) break;
-                const unsigned sd = s.slotL[phs][nslot0 + q];
+                const unsigned sd = slotL[phs][nslot0 + q];
                 const long long cst = (long long)sd + (((long long)P.pnbour * sd) >> 8);
                 if (cst < bcost) { bmx = sdx[q]; bmy = sdy[q]; bsad = sd; bcost = cst; }
             }
@@ -1321,9 +1364,9 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
             stype = (edge && level == 1) ? 0 : L.search_type;
             refine = true;
         }
-        const unsigned dcsum = s.slotL[phs][dcslot];
-        run_search_steps(x, b, s, ph, refine, stype, radius, lambda, ppx, ppy, imv.x, imv.y, idx, bad_count, bmx, bmy,
-                         bsad, bcost);
+        const unsigned dcsum = slotL[phs][dcslot];
+        run_search_steps(x, b, s, ph, refine ? RS_ALL : RS_NONE, stype, radius, lambda, ppx, ppy, imv.x, imv.y, idx,
+                         bad_count, bmx, bmy, bsad, bcost);
         // ---- store (:673-679)
         const int rows = b.py >= 0 ? imax(0, imin(b.bh, L.lh - b.py)) : 0;
         const int cols = b.px >= 0 ? imax(0, imin(b.bw, L.lw - b.px)) : 0;
@@ -1339,6 +1382,348 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
         last_val = v;
     }
 }
+
+// ---- level 0 with look-ahead (speculative and exact) ------------------------------------
+// The calling warp waits until blocks 0 .. k-1 of the level are committed (*committed counts
+// them; the committing warp stores its results, fences, then bumps the count). Bounded: false once
+// kWaitCycles have passed or another warp of the direction has given up (the caller flags
+// ST_TIMEOUT and carries on, so every warp still reaches its barriers). The fence after the wait
+// makes the committed blocks' stores visible to every lane.
+__device__ __forceinline__ bool wait_commits(volatile int *committed, int64_t k, volatile int *late) {
+    const long long t0 = clock64();
+    for (;;) {
+        const int seen = (int64_t)*committed >= k;
+        if (__all_sync(0xFFFFFFFFu, seen)) break;
+        const int give_up = *late || clock64() - t0 > kWaitCycles;
+        if (__shfl_sync(0xFFFFFFFFu, give_up, 0)) {
+            if ((threadIdx.x & 31) == 0) *late = 1;
+            return false;
+        }
+        __nanosleep(32);
+    }
+    __threadfence_block();
+    return true;
+}
+
+// exact_search_level (:480-681) with D = NW blocks in flight per direction, one per warp
+// ("look-ahead"). Warp w searches blocks w, w + D, w + 2D, ... of the level's order. Of what a
+// block reads, only these can come from the blocks searched just before it: the vectors of its
+// processed neighbours, taken as seeds (:570-585); at level > 0 an edge block's predictor, the
+// current vector of an inner cell (:520-549); the bad-SAD count (:605-616). Everything else
+// (the interpolated predictor of an inner block, lambda, radius, search type, the
+// previous-frame, zero and global candidates) comes from the coarser level, the other direction
+// and the block itself. A warp starts block k once it has committed block k - D, so cells
+// processed at order positions <= k - D hold their final vectors; seeds from the at most D - 1
+// cells processed at positions in (k - D, k) are "deferred": the block's special candidates and
+// its refinement run without them. The warp then waits for block k - 1's commit (a count of
+// committed blocks in shared memory: blocks commit in the reference's order) and replays the
+// reference's selection
+// with the deferred seeds at their places in the scan: :740-746 keep the first candidate of
+// minimal cost, i.e. the least (cost, place), so the speculative best stands unless a deferred
+// seed costs less, or the same at an earlier place. If one wins with another vector, the
+// refinement runs again from it; with the same vector (hence the same SAD) the refinement
+// already run is the reference's. The bad-SAD test and expansion run after the hand-over, with
+// the count of the blocks before. An edge block whose predictor cell is among the deferred ones
+// waits for block k - 1 first and runs without look-ahead. Stored vectors are the reference's in
+// every case; on the 1080p workload fewer than 1 % of level-0 blocks run their refinement twice.
+// A level with an input on which the reference would panic takes search_level instead.
+// stats (nullable): [0] blocks, [1] blocks with deferred seeds, [2] deferred seeds evaluated
+// (the others had the vector of a candidate already evaluated), [3] refinements run again.
+__device__ __forceinline__ void search_level_spec(const Ctx &xd, DirSh &s, DirScratch &ds, const uint2 *prevp, int *status,
+                                                  unsigned long long *stats) {
+    const AnalyseParams &P = *xd.P;
+    const LevelInfo &L = *xd.L;
+    const int level = xd.level, gw = L.gw, gh = L.gh;
+    uint2 *field = ds.vec[level & 1];
+    uint8_t *lumaf = ds.luma[level & 1];
+    const int64_t order_len = s.order_len;
+    const bool smallest = L.smallest != 0;
+    constexpr int D = NW;
+    const int g = xd.tid >> 5, lane = xd.tid & 31;
+    Ctx x = xd;
+    x.nw = 1;
+    x.wbase = g;
+    x.tid = lane;
+    if (xd.tid == 0) { s.committed = 0; s.late_ = 0; s.bad_count = 0; }
+    dbar(xd.d);
+    int ph = 0;
+    unsigned long long n_blk = 0, n_def = 0, n_eval = 0, n_rerun = 0;
+    bool late = false;
+    unsigned (*slotL)[MAXSLOT] = s.slotL[g];
+    auto wait_prev = [&](int64_t k) {  // block k - 1 is committed (and its stores visible) after this
+        if (k > 0 && !wait_commits(&s.committed, k, &s.late_)) late = true;
+    };
+    auto pos_of = [&](int nx, int ny) -> int64_t {
+        return level == 0 ? initial_order_pos(gw, gh, nx, ny) : (int64_t)ds.pos[(int64_t)ny * gw + nx];
+    };
+    for (int64_t k = g; k < order_len; k += D) {
+        const int2 bxy = level == 0 ? initial_order_at(gw, gh, k) : unpack_xy(ds.order[k]);
+        const int bx = bxy.x, by = bxy.y;
+        const int64_t idx = (int64_t)by * gw + bx;
+        int px = (level > 0 && bx == gw - 1) ? L.lw - P.block_w : bx * P.step_x;
+        int py = (level > 0 && by == gh - 1) ? L.lh - P.block_h : by * P.step_y;
+        px += L.pxoff;
+        py += L.pyoff;
+        const bool edge = level > 0 && (bx == gw - 1 || by == gh - 1);
+        const int sxi = imin(bx, gw - 2), syi = imin(by, gh - 2);
+        const int64_t sidx = (int64_t)syi * gw + sxi;
+        // an edge block's predictor is its inner cell's current vector: when another warp may not
+        // have committed that cell yet, take the hand-over first (the block runs without look-ahead)
+        bool waited = false;
+        if (edge) {
+            const int64_t p = pos_of(sxi, syi);
+            if (p < k && p > k - D) { wait_prev(k); waited = true; }
+        }
+        const uint2 interp = field[edge ? sidx : idx];
+        const int2 imv = vmv(interp);
+        BlkC b;
+        make_blk(x, px, py, !smallest, b);
+        stage_source(x, s, b);
+        // ---- special candidates (exact_search_block, :708-746), as in search_level, without
+        // the deferred seeds
+        int n = 1, rs_slot = -1, prev_slot = -1;
+        if (edge && !smallest) rs_slot = n++;  // re-score the predictor at its source block (:536-549)
+        int pmx = 0, pmy = 0;
+        if (prevp) {
+            const uint2 pv = prevp[idx];
+            if (pv.y != 0xFFFFFFFFu && pv.y > 0) {
+                const int2 pm = vmv(pv);
+                pmx = pm.x; pmy = pm.y;
+                prev_slot = n++;
+            }
+        }
+        const int zslot = n++, gslot = n++, nslot0 = n;
+        const int gxv = s.gx, gyv = s.gy;
+        int sdx[8], sdy[8], sq[8];        // seeds evaluated now: vector, place among the block's seeds
+        int dq0 = 0, dq1 = 0, dq2 = 0;    // deferred seeds: place among the block's seeds ...
+        int64_t dc0 = 0, dc1 = 0, dc2 = 0;  // ... and cell
+        int nseeds = 0, nall = 0, ndef = 0;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            const int ny = by - 1 + q / 3, nx = bx - 1 + q % 3;
+            if (ny < 0 || ny >= gh || nx < 0 || nx >= gw) continue;
+            const int64_t p = pos_of(nx, ny);
+            if (p >= k) continue;
+            const int64_t ci = (int64_t)ny * gw + nx;
+            if (!waited && p > k - D) {  // searched by another warp, maybe not yet committed
+                if (ndef == 0) { dq0 = nall; dc0 = ci; }
+                else if (ndef == 1) { dq1 = nall; dc1 = ci; }
+                else { dq2 = nall; dc2 = ci; }
+                ndef++;
+            } else {
+                const int2 nm = vmv(field[ci]);
+#pragma unroll
+                for (int t = 0; t < 8; t++)
+                    if (t == nseeds) { sdx[t] = nm.x; sdy[t] = nm.y; sq[t] = nall; }
+                nseeds++;
+            }
+            nall++;  // at most 8: levels with more processed neighbours take search_level
+        }
+        n += nseeds;
+        const int dcslot = n++;
+        {
+            const int G = step_lanes(x.grp_lanes, n, 1);
+            const int grp = lane / G, sub = lane & (G - 1), NG = 32 / G;
+            for (int j0 = 0; j0 < n; j0 += NG) {
+                const int j = j0 + grp;
+                const bool act = j < n;
+                int kind = 0, mx = 0, my = 0;
+                bool ch = !smallest;
+                if (j == 0) { mx = imv.x; my = imv.y; }
+                else if (j == rs_slot) { mx = imv.x; my = imv.y; kind = 1; ch = true; }
+                else if (j == prev_slot) { mx = pmx; my = pmy; }
+                else if (j == zslot) { mx = 0; my = 0; }
+                else if (j == gslot) { mx = gxv; my = gyv; }
+                else if (j == dcslot) { kind = 2; ch = false; }
+                else if (j >= nslot0 && j < nslot0 + nseeds) {
+#pragma unroll
+                    for (int t = 0; t < 8; t++)
+                        if (t == j - nslot0) { mx = sdx[t]; my = sdy[t]; }
+                }
+                Res r{0, 0, 0, 0, 0, 0};
+                if (act) r = eval_lane(x, b, kind, sxi * P.step_x, syi * P.step_y, mx, my, ch, sub, G);
+                group_sum3(r, G);
+                if (act && sub == 0) {
+                    unsigned Lv, Cv;
+                    if (kind == 2) { Lv = r.L; Cv = 0; }
+                    else finalize(r, Lv, Cv);
+                    slotL[ph][j] = ch ? sat_add(Lv, Cv) : Lv;
+                }
+            }
+        }
+        __syncwarp();
+        const int phs = ph;
+        ph ^= 1;
+        // ---- selection (:716-747); places in the reference's scan: field 0, previous 1,
+        // global 2, zero 3, the neighbour seeds 4 + their place among the seeds
+        const unsigned pred_score = rs_slot >= 0 ? slotL[phs][rs_slot] : interp.y;
+        const bool field_valid = pred_score != 0xFFFFFFFFu;
+        int bmx = 0, bmy = 0, bpos = -1;
+        unsigned bsad;
+        long long bcost;
+        bool refine = false;
+        int lambda = 0, radius = 0, stype = 0, ppx = imv.x, ppy = imv.y;
+        if (level == 0 && P.distance == 0) {  // level 0 without a search: the field's vector or zero
+            if (field_valid) { bmx = imv.x; bmy = imv.y; bsad = slotL[phs][0]; }
+            else bsad = slotL[phs][zslot];
+            bcost = (long long)bsad;
+        } else {
+            if (field_valid) { bmx = imv.x; bmy = imv.y; bsad = slotL[phs][0]; bcost = (long long)bsad; bpos = 0; }
+            else { bsad = 0xFFFFFFFFu; bcost = 0x7FFFFFFFFFFFFFFFLL; }
+            if (prev_slot >= 0) {
+                const unsigned sd = slotL[phs][prev_slot];
+                const long long cst = (long long)sd + (((long long)P.prev * sd) >> 8);
+                if (cst < bcost) { bmx = pmx; bmy = pmy; bsad = sd; bcost = cst; ppx = pmx; ppy = pmy; bpos = 1; }
+            }
+            {
+                const unsigned sd = slotL[phs][gslot];
+                const long long cst = (long long)sd + (((long long)P.pglobal * sd) >> 8);
+                if (cst < bcost) { bmx = gxv; bmy = gyv; bsad = sd; bcost = cst; bpos = 2; }
+            }
+            {
+                const unsigned sd = slotL[phs][zslot];
+                const long long cst = (long long)sd + (((long long)P.pzero * sd) >> 8);
+                if (cst < bcost) { bmx = 0; bmy = 0; bsad = sd; bcost = cst; bpos = 3; }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (q >= nseeds) break;
+                const unsigned sd = slotL[phs][nslot0 + q];
+                const long long cst = (long long)sd + (((long long)P.pnbour * sd) >> 8);
+                if (cst < bcost) { bmx = sdx[q]; bmy = sdy[q]; bsad = sd; bcost = cst; bpos = 4 + sq[q]; }
+            }
+            lambda = adapt_lambda(L.lambda_base, L.lsad, pred_score);
+            radius = L.base_radius;
+            if (level > 0 && P.coarse_distance < 0) {
+                const unsigned act = plane_activity(x.S.y, x.G.ylen, x.G.ys, L.y_off + b.py2, b.px2, b.bw, b.bh, x.satd) +
+                                     plane_activity(x.S.u, x.G.clen, x.G.cs, L.c_off + py / 2, px / 2, b.bw / 2, b.bh / 2, x.satd) +
+                                     plane_activity(x.S.v, x.G.clen, x.G.cs, L.c_off + py / 2, px / 2, b.bw / 2, b.bh / 2, x.satd);
+                radius = adaptive_radius(radius, act);
+            }
+            stype = (edge && level == 1) ? 0 : L.search_type;
+            refine = true;
+        }
+        const long long sel_cost = bcost;
+        const int sel_x = bmx, sel_y = bmy;
+        bcost = (long long)bsad;
+        const unsigned dcsum = slotL[phs][dcslot];
+        int bad_unused = 0;
+        run_search_steps(x, b, s, ph, refine ? RS_REFINE_ONLY : RS_NONE, stype, radius, lambda, ppx, ppy, imv.x, imv.y,
+                         idx, bad_unused, bmx, bmy, bsad, bcost);
+        if (!waited) wait_prev(k);
+        n_blk++;
+        if (refine && ndef > 0) {
+            n_def++;
+            long long cb = sel_cost;
+            int cpos = bpos, cx = sel_x, cy = sel_y;
+            unsigned csad = 0;
+            bool dwin = false;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                if (j >= ndef) break;
+                const int64_t ci = j == 0 ? dc0 : (j == 1 ? dc1 : dc2);
+                const int pos = 4 + (j == 0 ? dq0 : (j == 1 ? dq1 : dq2));
+                const int2 m = vmv(field[ci]);
+                // its exact_sad: from an evaluated candidate with the same vector (same block, same
+                // reads), else evaluated now
+                unsigned sd = 0;
+                bool have = true;
+                if (m.x == imv.x && m.y == imv.y) sd = slotL[phs][0];
+                else if (prev_slot >= 0 && m.x == pmx && m.y == pmy) sd = slotL[phs][prev_slot];
+                else if (m.x == 0 && m.y == 0) sd = slotL[phs][zslot];
+                else if (m.x == gxv && m.y == gyv) sd = slotL[phs][gslot];
+                else {
+                    have = false;
+#pragma unroll
+                    for (int t = 0; t < 8; t++)
+                        if (!have && t < nseeds && sdx[t] == m.x && sdy[t] == m.y) { sd = slotL[phs][nslot0 + t]; have = true; }
+                }
+                if (!have) {
+                    Res r = eval_lane(x, b, 0, 0, 0, m.x, m.y, !smallest, lane, 32);
+                    group_sum3(r, 32);
+                    unsigned Lv, Cv;
+                    finalize(r, Lv, Cv);
+                    sd = !smallest ? sat_add(Lv, Cv) : Lv;
+                    n_eval++;
+                }
+                const long long cst = (long long)sd + (((long long)P.pnbour * sd) >> 8);
+                if (cst < cb || (cst == cb && pos < cpos)) { cb = cst; cpos = pos; cx = m.x; cy = m.y; csad = sd; dwin = true; }
+            }
+            if (dwin && (cx != sel_x || cy != sel_y)) {  // a deferred seed with another vector wins
+                n_rerun++;
+                bmx = cx; bmy = cy; bsad = csad; bcost = (long long)csad;
+                run_search_steps(x, b, s, ph, RS_REFINE_ONLY, stype, radius, lambda, ppx, ppy, imv.x, imv.y, idx,
+                                 bad_unused, bmx, bmy, bsad, bcost);
+            }
+        }
+        if (refine && level > 0) {  // the bad-SAD test and expansion (:604-672) with the blocks' count so far
+            int bad_count = s.bad_count;
+            run_search_steps(x, b, s, ph, RS_BAD_ONLY, stype, radius, lambda, ppx, ppy, imv.x, imv.y, idx, bad_count,
+                             bmx, bmy, bsad, bcost);
+            if (lane == 0) s.bad_count = bad_count;
+        }
+        // ---- store (:673-679) and hand the order on to the next block's warp
+        const int rows = b.py >= 0 ? imax(0, imin(b.bh, L.lh - b.py)) : 0;
+        const int cols = b.px >= 0 ? imax(0, imin(b.bw, L.lw - b.px)) : 0;
+        const unsigned cnt = (unsigned)(rows * cols);
+        unsigned dc = (cnt ? dcsum / cnt : 0) >> DC_SHIFT;
+        if (dc > 255) dc = 255;
+        if (lane == 0) {
+            field[idx] = mkvec(bmx, bmy, smallest ? sat_mul(bsad, 3) : bsad);
+            lumaf[idx] = (uint8_t)dc;
+            __threadfence_block();  // the block's stores (and bad_count) before the count that publishes them
+            *(volatile int *)&s.committed = (int)(k + 1);
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        if (late) { atomicOr(status, ST_TIMEOUT); s.abort_ = 1; }
+        if (stats && level == 0) {
+            atomicAdd(stats + 0, n_blk);
+            atomicAdd(stats + 1, n_def);
+            atomicAdd(stats + 2, n_eval);
+            atomicAdd(stats + 3, n_rerun);
+        }
+    }
+    dbar(xd.d);
+}
+
+// Whether search_level_spec may run this level: it takes neither the reference's panics
+// (search_level reports them at the block where the reference stops) nor grids below 3 x 3.
+// Called by every thread of the direction; the answer is the same in all of them.
+__device__ __forceinline__ bool level_spec_ok(const Ctx &x, DirSh &s, DirScratch &ds) {
+    const LevelInfo &L = *x.L;
+    const int level = x.level, gw = L.gw, gh = L.gh;
+    const int64_t ncell = (int64_t)gw * gh, order_len = s.order_len;
+    if (gw < 3 || gh < 3) return false;
+    if (x.tid == 0) s.unsafe_ = 0;
+    dbar(x.d);
+    int bad = 0;
+    for (int64_t k = x.tid; k < order_len && !bad; k += NT) {
+        const int2 bxy = level == 0 ? initial_order_at(gw, gh, k) : unpack_xy(ds.order[k]);
+        const int bx = bxy.x, by = bxy.y;
+        const int64_t idx = (int64_t)by * gw + bx;
+        const int64_t sidx = (int64_t)imin(by, gh - 2) * gw + imin(bx, gw - 2);
+        if (sidx < 0 || sidx >= ncell || idx < 0 || idx >= ncell || bx < 0 || by < 0 || bx >= gw || by >= gh) {
+            bad = 1;
+            break;
+        }
+        int nproc = 0;
+        for (int q = 0; q < 9; q++) {
+            const int ny = by - 1 + q / 3, nx = bx - 1 + q % 3;
+            if (ny < 0 || ny >= gh || nx < 0 || nx >= gw) continue;
+            const int64_t p = level == 0 ? initial_order_pos(gw, gh, nx, ny) : (int64_t)ds.pos[(int64_t)ny * gw + nx];
+            nproc += p < k;
+        }
+        if (nproc > 8) bad = 1;
+    }
+    if (bad) s.unsafe_ = 1;
+    dbar(x.d);
+    const bool ok = s.unsafe_ == 0;
+    dbar(x.d);
+    return ok;
+}
+
 __device__ __forceinline__ long long floor_div(long long a, long long b) {  // i64::div_euclid for b > 0
     const long long q = a / b;
     return (a % b != 0 && a < 0) ? q - 1 : q;
@@ -1407,7 +1792,7 @@ __device__ __forceinline__ void refine_pass(Ctx &x, DirSh &s, DirScratch &ds) {
             const bool search = parent > (long long)threshold;
             stage_source(x, s, b);
             {  // slot 0: exact_sad at the clipped predictor (when searching); slot 1: block_luma_dc
-                const int Gl = step_lanes(x.grp_lanes, 2), lane = x.tid & 31, grp = (x.tid >> 5) * (32 / Gl) + lane / Gl;
+                const int Gl = step_lanes(x.grp_lanes, 2, x.nw), lane = x.tid & 31, grp = (x.tid >> 5) * (32 / Gl) + lane / Gl;
                 const int sub = lane & (Gl - 1);
                 const bool act = (grp == 0 && search) || grp == 1;
                 Res r{0, 0, 0, 0, 0, 0};
@@ -1417,7 +1802,7 @@ __device__ __forceinline__ void refine_pass(Ctx &x, DirSh &s, DirScratch &ds) {
                     unsigned Lv, Cv;
                     if (grp == 1) { Lv = r.L; Cv = 0; }
                     else finalize(r, Lv, Cv);
-                    s.slotL[ph][grp] = grp == 0 ? sat_add(Lv, Cv) : Lv;
+                    s.slotL[x.wbase][ph][grp] = grp == 0 ? sat_add(Lv, Cv) : Lv;
                 }
             }
             dbar(x.d);
@@ -1427,14 +1812,14 @@ __device__ __forceinline__ void refine_pass(Ctx &x, DirSh &s, DirScratch &ds) {
             unsigned bsad = parent < 0 ? 0u : (parent > 0xFFFFFFFFLL ? 0xFFFFFFFFu : (unsigned)parent);
             long long bcost = parent < 0 ? 0 : parent;
             if (search) {
-                bsad = s.slotL[phs][0];
+                bsad = s.slotL[x.wbase][phs][0];
                 bcost = (long long)bsad;
                 const int lambda = by == 0 ? 0 : (P.lambda >> 2) / factor;
                 int bad = 0;
-                run_search_steps(x, b, s, ph, true, P.refine_search_type, abs(P.refine_distance), lambda, pmx, pmy, pmx,
+                run_search_steps(x, b, s, ph, RS_ALL, P.refine_search_type, abs(P.refine_distance), lambda, pmx, pmy, pmx,
                                  pmy, 0, bad, bmx, bmy, bsad, bcost);
             }
-            const unsigned dcsum = s.slotL[phs][1];
+            const unsigned dcsum = s.slotL[x.wbase][phs][1];
             const int rows = b.py >= 0 ? imax(0, imin(b.bh, lh - b.py)) : 0;
             const int cols = b.px >= 0 ? imax(0, imin(b.bw, lw - b.px)) : 0;
             const unsigned cnt = (unsigned)(rows * cols);
@@ -1569,7 +1954,8 @@ __device__ void reorder(const Ctx &x, DirSh &s, const uint2 *field, int gw, int 
 // configuration does not search (vectors 1 or 2 under a 2-direction batch CTA) only
 // take part in the CTA-wide barriers. Status bits go to *status.
 __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const PairRef pr, uint8_t *__restrict__ pay,
-                                                 uint8_t *__restrict__ scr, int *status, int &cta_abort) {
+                                                 uint8_t *__restrict__ scr, int *status, int &cta_abort,
+                                                 unsigned long long *spec_stats) {
     extern __shared__ __align__(16) unsigned char smem[];
     const bool bidir = P.vectors == 3;
     const int half = (int)(threadIdx.x / NT);
@@ -1596,6 +1982,8 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
     x.P = &P;
     x.d = half;
     x.tid = tid;
+    x.nw = NW;
+    x.wbase = 0;
     x.S = Planes{src, src + P.y_len, src + P.y_len + P.c_len};
     x.R = Planes{ref, ref + P.y_len, ref + P.y_len + P.c_len};
     if (threadIdx.x == 0) cta_abort = 0;
@@ -1745,7 +2133,10 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
         __syncthreads();  // both directions' projections of this level are ready
         if (!s.abort_) {
             const uint2 *prevp = (first) ? nullptr : other_proj[level & 1];
-            search_level(x, s, ds, prevp, status);
+            if (NW > 1 && (P.lookahead & (level == 0 ? 1 : 2)) && level_spec_ok(x, s, ds))
+                search_level_spec(x, s, ds, prevp, status, spec_stats);
+            else
+                search_level(x, s, ds, prevp, status);
         }
         dbar(half);
         if (!s.abort_ && level > 0) {
@@ -1783,6 +2174,8 @@ __device__ __noinline__ void finish_pair(const AnalyseParams *Pp, const PairRef 
         x.P = &P;
         x.d = half;
         x.tid = tid;
+        x.nw = NW;
+        x.wbase = 0;
         x.S = Planes{src, src + P.y_len, src + P.y_len + P.c_len};
         x.R = Planes{ref, ref + P.y_len, ref + P.y_len + P.c_len};
         const LevelInfo &L0 = P.lv[0];
@@ -1837,7 +2230,7 @@ __global__ void __launch_bounds__(2 * NT, SVPF_MINB)
         pr.ref = psrc.clip + n2 * psrc.frame_bytes;
     }
     uint8_t *scr = scratch + pair * P.scratch_per_pair;
-    analyse_pair_dev(P, pr, payloads + pair * P.payload_len, scr, status, cta_abort);
+    analyse_pair_dev(P, pr, payloads + pair * P.payload_len, scr, status, cta_abort, psrc.stats);
     __syncthreads();
     if (!cta_abort) finish_pair(&P, pr, payloads + pair * P.payload_len, scr);
 }
@@ -1865,7 +2258,7 @@ __global__ void __launch_bounds__(2 * NT, SVPF_MINB)
             for (int i = threadIdx.x; i < (int)(sizeof(AnalyseParams) / 16); i += blockDim.x) dst[i] = src[i];
         }
         __syncthreads();
-        analyse_pair_dev(P, bi.pair, bi.payload, scr, clip_status + bi.clip, cta_abort);
+        analyse_pair_dev(P, bi.pair, bi.payload, scr, clip_status + bi.clip, cta_abort, nullptr);
         __syncthreads();
         if (!cta_abort) finish_pair(&P, bi.pair, bi.payload, scr);
         __syncthreads();  // P, item_sh and the shared search state are reused by the next item

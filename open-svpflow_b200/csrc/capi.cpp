@@ -43,6 +43,8 @@ int check_device() {
 }
 
 constexpr int64_t kStatusBytes = 256;
+// level-0 look-ahead counters (4 x uint64) inside the status area, cleared with it
+constexpr int64_t kStatsOffset = 64;
 inline int64_t align256(int64_t v) { return (v + 255) & ~(int64_t)255; }
 
 struct DevBuf {
@@ -148,6 +150,7 @@ int launch_pairs(const svpf_analyser *a, const PairRef *host_pairs, const uint8_
         src.nframes = nframes;
         src.delta = a->o.delta > 1 ? a->o.delta : 1;
     }
+    src.stats = (unsigned long long *)(scr + kStatsOffset);
     int nl = 0;
     cudaError_t e = launch_analyse(a->P, src, count, payloads_dev, scr + kStatusBytes + table, (int *)scr, st, &nl);
     g_launches += nl;
@@ -160,6 +163,7 @@ int read_status(const void *scratch_dev, cudaStream_t st) {
     CU(cudaMemcpyAsync(&status, scratch_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
     if (status & 1) return fail(SVPF_EPANIC, "SVAnalyse: the reference indexes out of range on this input (it panics)");
+    if (status & 4) return fail(SVPF_ECUDA, "SVAnalyse: an internal wait of the Analyse kernel gave up (results invalid)");
     if (status) return fail(SVPF_EUNSUP, "SVAnalyse: unsupported input on the device path");
     return SVPF_OK;
 }
@@ -371,6 +375,25 @@ int svpf_clip_analyse_device(const svpf_analyser *a, const uint8_t *supers_dev, 
 int svpf_device_status(const void *scratch_dev, void *stream) {
     if (int rc = check_device()) return rc;
     return read_status(scratch_dev, (cudaStream_t)stream);
+}
+
+int svpf_analyser_set_lookahead(svpf_analyser *a, int32_t levels) {
+    if (!a) return fail(SVPF_EINVAL, "null analyser");
+    if (levels < 0 || levels > 3) return fail(SVPF_EINVAL, "look-ahead levels must be 0..3");
+    std::lock_guard<std::mutex> lk(a->mu);
+    a->P.lookahead = levels;
+    return SVPF_OK;
+}
+
+int svpf_device_lookahead_stats(const void *scratch_dev, void *stream, int64_t out[4]) {
+    if (int rc = check_device()) return rc;
+    if (!scratch_dev || !out) return fail(SVPF_EINVAL, "bad buffers");
+    unsigned long long v[4] = {0, 0, 0, 0};
+    CU(cudaMemcpyAsync(v, (const uint8_t *)scratch_dev + kStatsOffset, sizeof(v), cudaMemcpyDeviceToHost,
+                       (cudaStream_t)stream));
+    CU(cudaStreamSynchronize((cudaStream_t)stream));
+    for (int i = 0; i < 4; i++) out[i] = (int64_t)v[i];
+    return SVPF_OK;
 }
 
 int svpf_analyse(svpf_analyser *a, const uint8_t *cur_super, const uint8_t *ref_super, uint8_t *payload) {

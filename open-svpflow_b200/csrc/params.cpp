@@ -34,6 +34,7 @@ bool build_analyse_params(const AnalyseOpts &o, const SuperLayout &Lay, AnalyseP
     P.px_bytes = Lay.px_bytes;
     P.lambda = o.lambda;
     P.tiles_per_lane = 8;
+    P.lookahead = 1;
     // per level
     int64_t max_cells = 1, max_order = 1;
     for (int lv = 0; lv < o.levels; lv++) {

@@ -39,6 +39,7 @@ struct PairSrc {
     const uint8_t *clip;
     int64_t frame_bytes;
     int32_t first, nframes, delta;
+    unsigned long long *stats;  // nullable: level-0 look-ahead counters (see search_level0_spec)
 };
 
 // One work item of a batch launch: a frame pair of some clip and where its payload goes.

@@ -106,6 +106,9 @@ struct alignas(16) AnalyseParams {
     int32_t rescale_denom;
     int32_t tiles_per_lane;   // 4x4 tiles one lane evaluates per candidate (2, 4 or 8): a launch tuning knob
     int32_t px_bytes;         // 1: 8-bit samples; 2: uint16 samples (the 10-bit extension)
+    int32_t lookahead;        // look-ahead (one block per warp in flight, exact either way): bit 0 level 0
+                              // (the default), bit 1 the coarser levels (slower: measured); a tuning knob
+    int32_t pad0_, pad1_, pad2_;
     int64_t payload_len;
     int32_t header[16];       // payload words 0x00..0x3C
     // per-pair scratch layout (bytes)

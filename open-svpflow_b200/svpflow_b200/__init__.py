@@ -26,7 +26,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libsvpflow_b200.so")
 REFERENCE_VERSION = 1_174_405_393  # svpGetVersion, crates/svpflow1/src/abi.rs:3
 
-SVPF_OK, SVPF_EINVAL, SVPF_ECUDA, SVPF_EPANIC, SVPF_EUNSUP = 0, -1, -2, -3, -4
+SVPF_OK, SVPF_EINVAL, SVPF_ECUDA, SVPF_EPANIC, SVPF_EUNSUP, SVPF_ECANCELED = 0, -1, -2, -3, -4, -5
 
 
 class SvpfError(RuntimeError):
@@ -85,6 +85,8 @@ def lib() -> ctypes.CDLL:
             "svpf_analyse_pairs_device": (I32, [_VP, P(_VP), P(_VP), I32, _VP, _VP, _VP]),
             "svpf_clip_analyse_device": (I32, [_VP, _VP, I32, I32, I32, _VP, _VP, _VP]),
             "svpf_device_status": (I32, [_VP, _VP]),
+            "svpf_analyser_set_lookahead": (I32, [_VP, I32]),
+            "svpf_device_lookahead_stats": (I32, [_VP, _VP, P(I64)]),
             "svpf_clip_analyse": (I32, [_VP, _VP, _VP, I32, I32, I32, _VP]),
             "svpf_kernel_launches": (I64, []),
             "svpf_kernel_launches_reset": (None, []),
@@ -108,6 +110,7 @@ def lib() -> ctypes.CDLL:
             "svpf_server_destroy": (None, [_VP]),
             "svpf_server_submit": (I32, [_VP, _VP, _VP, _VP, I32, _VP, _VP, P(I64)]),
             "svpf_server_wait": (I32, [_VP, I64, P(I64)]),
+            "svpf_server_cancel": (I32, [_VP, I64]),
             "svpf_server_now_ns": (I64, [_VP]),
             "svpf_server_stats": (None, [_VP, P(I64), P(I64), P(I64), P(I32), P(I64)]),
             "svpf_vector_grid": (I32, [P(I32), P(I32), P(I32)]),
@@ -336,6 +339,18 @@ class Analyser:
         r = (_VP * n)(*ref_ptrs)
         _check(lib().svpf_analyse_pairs_device(self._h, c, r, n, payloads_ptr, scratch_ptr, stream))
 
+    def set_lookahead(self, levels):
+        """Look-ahead at level 0 only (True / 1, the default), every level (3), the coarser levels
+        only (2) or off (False / 0); results are identical either way."""
+        _check(lib().svpf_analyser_set_lookahead(self._h, 1 if levels is True else int(levels)))
+
+    @staticmethod
+    def lookahead_stats(scratch_ptr: int, stream: int = 0) -> dict:
+        """Counters of the last device launch on that scratch."""
+        v = (ctypes.c_int64 * 4)()
+        _check(lib().svpf_device_lookahead_stats(scratch_ptr, stream, v))
+        return {"blocks": v[0], "deferred_blocks": v[1], "deferred_evaluated": v[2], "reruns": v[3]}
+
     @staticmethod
     def device_status(scratch_ptr: int, stream: int = 0):
         _check(lib().svpf_device_status(scratch_ptr, stream))
@@ -480,6 +495,11 @@ class Server:
         keep = self._live.pop(request)
         _check(rc)
         return keep[3], keep[4], (t[0], t[1], t[2])
+
+    def cancel(self, request: int):
+        """Withdraws a request that has not been admitted yet (its wait() then raises with
+        code SVPF_ECANCELED); an admitted request runs to completion (ValueError)."""
+        _check(lib().svpf_server_cancel(self._h, request))
 
     def stats(self) -> dict:
         a, c, pb, l = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()

@@ -188,3 +188,40 @@ def test_served_clips_overlap_on_the_device():
         assert (t1 - t0) < 2.5 * alone, f"four clips took {(t1 - t0) / 1e6:.1f} ms, one alone {alone / 1e6:.1f} ms"
     finally:
         srv.close()
+
+
+def test_server_cancels_a_request_before_admission():
+    """svpf_server_cancel withdraws a queued request (its wait reports SVPF_ECANCELED and it never
+    runs); admitted, finished and unknown requests cannot be cancelled; the requests around the
+    cancelled one complete with the oracle's payloads."""
+    import svpflow_b200 as sv
+
+    mix = [(1280, 720, 12, 31, "{pel:2}", "{block:{w:16,overlap:3},main:{search:{type:3,distance:16,satd:true}}}"),
+           (192, 128, 3, 32, "{pel:2}", "{block:{w:8,overlap:2},main:{search:{type:3,distance:6,satd:true}}}"),
+           (160, 96, 4, 33, "{pel:1}", "{vectors:1,block:{w:16,overlap:0},main:{search:{type:2,distance:2}}}")]
+    clips = _clips(mix)
+    want = _oracle(clips, mix)
+    import time
+
+    srv = sv.Server(8 << 30, max_active=1, chunk_pairs=4)
+    try:
+        ids = [srv.submit(*clips[0])]
+        t0 = time.time()
+        while srv.stats()["admitted"] < 1 and time.time() - t0 < 10:  # the scheduler thread takes it up
+            time.sleep(0.001)
+        ids += [srv.submit(sb, an, clip) for sb, an, clip in clips[1:]]  # one slot: these wait for the 1st
+        srv.cancel(ids[1])
+        with pytest.raises(ValueError, match="admitted|finished"):
+            srv.cancel(ids[0])
+        with pytest.raises(ValueError, match="unknown request"):
+            srv.cancel(10 ** 9)
+        with pytest.raises(sv.SvpfError) as e:
+            srv.wait(ids[1])
+        assert e.value.code == sv.SVPF_ECANCELED
+        for k in (0, 2):
+            pay, _, _ = srv.wait(ids[k])
+            assert np.array_equal(pay, want[k]), f"clip {k} differs from the oracle"
+        st = srv.stats()
+        assert st["admitted"] == 2 and st["completed"] == 2
+    finally:
+        srv.close()
