@@ -15,6 +15,8 @@
 // carries this project's 10-bit extension (samples 0..1023, the same arithmetic with the
 // clamps at 1023 instead of 255).
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "svpf_device.h"
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(256) super_reduce_kernel(SuperDev D, T *__rest
 }
 
 
-// ---- 8-bit fast paths: rows processed in 16-byte (level 0) and 4-byte (pyramid) words. Used
+// ---- 8-bit fast paths: rows processed in 16-byte (level 0) and 4-byte (reduction) words. Used
 // when every row of the source and super frames starts on a 16-byte boundary; the kernels
 // above serve every other geometry and the uint16 format. Both give the same bytes.
 
@@ -242,17 +244,14 @@ __device__ __noinline__ uint4 level0_edge_chunk(bool subpel, const uint8_t *s0, 
 }
 
 // The level-0 region (copy + edge extension, super_build.rs:45-67; bilinear pel-2 planes,
-// :179-224; zero sub-planes otherwise), one 16-byte chunk of one row per thread, every
-// sub-plane of that chunk. grid: x = chunks of the pitch / 128, y = plane row, z = frame x planes.
-__global__ void __launch_bounds__(128, 8) super_level0_vec_kernel(SuperDev D, const uint8_t *__restrict__ src,
-                                                               uint8_t *__restrict__ dst, int plane0, int nplanes) {
-    const int plane = plane0 + (int)(blockIdx.z % (unsigned)nplanes);
-    const int64_t f = blockIdx.z / (unsigned)nplanes;
+// :179-224; zero sub-planes otherwise) of one 16-byte chunk of one row, every sub-plane of it.
+// EDGE: the chunks reaching past the row's last sample (x0 + 16 > w) and those of the last row, by
+// the scalar kernel's closed forms; otherwise the other chunks, in 16-byte words.
+template <bool EDGE>
+__device__ __forceinline__ void level0_chunk(const SuperDev &D, const uint8_t *__restrict__ src,
+                                             uint8_t *__restrict__ dst, int plane, int64_t f, int y, int x0) {
     const PlaneGeo g = plane_geo(D, plane);
-    const int y = blockIdx.y;
     const int S = (int)g.stride, w = g.w, h = g.h;
-    const int x0 = (blockIdx.x * 128 + threadIdx.x) * 16;
-    if (y >= h || x0 >= S) return;
     const int nsub = D.full ? D.pel * D.pel : 1;
     const bool bil = D.pel >= 2 && D.gpu <= 1 && D.full && D.scale_up == 0;
     const uint8_t *s0 = src + f * D.src_frame_bytes + g.src_off;
@@ -265,14 +264,20 @@ __global__ void __launch_bounds__(128, 8) super_level0_vec_kernel(SuperDev D, co
     int np = 0;
     while (np < nsub && (int64_t)np * h + y < g.rows) np++;
     if (np == 0) return;
-    if (np == nsub && x0 + 16 < w && y + 1 < h) {  // interior chunk: x + 1 and y + 1 stay inside the plane
+    if (!EDGE) {
+        if (x0 + 16 > w || y + 1 >= h) return;  // the edge kernel's
         const uint8_t *r0 = s0 + (int64_t)y * sst + x0;
         const uint4 A = *reinterpret_cast<const uint4 *>(r0);
         *reinterpret_cast<uint4 *>(o) = A;
         if (nsub > 1) {
             uint4 p1 = zero, p2 = zero, p3 = zero;
             if (bil) {
-                const uint4 As = shift1(A, r0[16]);
+                // the byte after the chunk in the super frame's flat memory (fill_bilinear_pel2 reads
+                // it): the next sample; at the row's end the edge-extended padding (pitch > w) or the
+                // next row's first sample (pitch == w)
+                const bool last = x0 + 16 == w;
+                const uint32_t nextA = !last ? r0[16] : (S > w ? (A.w >> 24) : r0[sst - x0]);
+                const uint4 As = shift1(A, nextA);
                 p1 = avg16(A, As);
                 if (y == 0) {  // the v and hv planes' first rows are copies (copy_row, :205, :223)
                     p2 = A;
@@ -281,116 +286,201 @@ __global__ void __launch_bounds__(128, 8) super_level0_vec_kernel(SuperDev D, co
                     const uint8_t *r1 = r0 + sst;
                     const uint4 B = *reinterpret_cast<const uint4 *>(r1);
                     p2 = avg16(A, B);
-                    p3 = avg16(A, shift1(B, r1[16]));
+                    // the byte after row y+1's chunk; past the last source row (pitch == w) it is the
+                    // h plane's first byte, avg(L(0,0), L(0,1))
+                    const uint32_t nextB = !last ? r1[16]
+                                         : (S > w ? (B.w >> 24)
+                                                  : (y + 2 < h ? r1[sst - x0] : avg8(s0[0], s0[w > 1 ? 1 : 0])));
+                    p3 = avg16(A, shift1(B, nextB));
                 }
             }
-            *reinterpret_cast<uint4 *>(o + pstep) = p1;
-            *reinterpret_cast<uint4 *>(o + 2 * pstep) = p2;
-            *reinterpret_cast<uint4 *>(o + 3 * pstep) = p3;
-            for (int p = 4; p < nsub; p++) *reinterpret_cast<uint4 *>(o + p * pstep) = zero;
+            if (np > 1) *reinterpret_cast<uint4 *>(o + pstep) = p1;
+            if (np > 2) *reinterpret_cast<uint4 *>(o + 2 * pstep) = p2;
+            if (np > 3) *reinterpret_cast<uint4 *>(o + 3 * pstep) = p3;
+            for (int p = 4; p < np; p++) *reinterpret_cast<uint4 *>(o + p * pstep) = zero;
         }
         return;
     }
-    // chunks at the right edge and the last row: the closed forms of the scalar kernel
     const bool subpel = D.pel >= 2 && D.gpu <= 1 && D.full && D.scale_up == 0;
     for (int p = 0; p < np; p++)
         *reinterpret_cast<uint4 *>(o + p * pstep) = level0_edge_chunk(subpel, s0, g.src_stride, w, h, g.stride, y, x0, p);
 }
 
-// reduce_6tap + horizontal_6tap_inplace (super_build.rs:254-357) for every level of one
-// plane of one frame: one CTA walks the pyramid level by level, kRows output rows at a time:
-// the vertical pass, 4 columns per thread in halfword lanes, into shared memory, then the
-// horizontal pass, 4 output bytes per thread. Each output row receives src_w bytes (dst_w
-// filtered values, then the vertical-only intermediates, :302-306) and zeros up to the pitch.
-constexpr int kRows = 8;
-__global__ void __launch_bounds__(512) super_pyramid_kernel(SuperDev D, uint8_t *__restrict__ dst) {
-    extern __shared__ __align__(16) uint8_t inter_all[];
-    const int plane = (int)(blockIdx.x % 3u);
-    const int64_t f = blockIdx.x / 3u;
+// Every chunk of `nplanes` planes from plane0 on (luma, or both chroma planes) of every frame: a
+// grid of resident CTAs strides over the items (frame, plane, row, chunk), so CTAs are few and
+// each thread streams many chunks.
+__global__ void __launch_bounds__(256, 4) super_level0_vec_kernel(SuperDev D, const uint8_t *__restrict__ src,
+                                                               uint8_t *__restrict__ dst, int plane0, int nplanes,
+                                                               int h, int chunks, uint32_t nitems) {
+    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < nitems; it += gridDim.x * blockDim.x) {
+        const uint32_t c = it % (uint32_t)chunks, r = it / (uint32_t)chunks;
+        const uint32_t y = r % (uint32_t)h, fp = r / (uint32_t)h;
+        level0_chunk<false>(D, src, dst, plane0 + (int)(fp % (uint32_t)nplanes), fp / (uint32_t)nplanes, (int)y,
+                            (int)c * 16);
+    }
+}
+
+// The edge chunks: per frame and plane, chunks [ce, chunks) of rows 0 .. h-2 (those reaching past
+// the row's last sample), then the whole last row (ce = the chunks the vector kernel takes).
+__global__ void __launch_bounds__(128) super_level0_edge_kernel(SuperDev D, const uint8_t *__restrict__ src,
+                                                                uint8_t *__restrict__ dst, int plane0, int nplanes, int h,
+                                                                int chunks, int ce, uint32_t nitems) {
+    const uint32_t ne = (uint32_t)(chunks - ce), per = (uint32_t)(h - 1) * ne + (uint32_t)chunks;
+    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < nitems; it += gridDim.x * blockDim.x) {
+        const uint32_t e = it % per, fp = it / per;
+        int y, c;
+        if (e < (uint32_t)(h - 1) * ne) {
+            y = (int)(e / ne);
+            c = ce + (int)(e % ne);
+        } else {
+            y = h - 1;
+            c = (int)(e - (uint32_t)(h - 1) * ne);
+        }
+        level0_chunk<true>(D, src, dst, plane0 + (int)(fp % (uint32_t)nplanes), fp / (uint32_t)nplanes, y, c * 16);
+    }
+}
+
+// reduce_6tap + horizontal_6tap_inplace (super_build.rs:254-357) in 32-bit words. Each output
+// row receives src_w bytes (dst_w filtered values, then the vertical-only intermediates,
+// :302-306) and zeros up to the pitch.
+// Bytes k1 and k2 (k2 - k1 <= 3) of the little-endian byte string W[0..3] that starts 4 bytes
+// before the output word's first source byte, as the two low bytes of a halfword pair.
+template <int K1, int K2>
+__device__ __forceinline__ uint32_t pair_bytes(const uint32_t (&W)[4]) {
+    constexpr int j = (K1 + 4) / 4, i1 = K1 + 4 - 4 * j, i2 = K2 + 4 - 4 * j;
+    static_assert(j >= 0 && j + 1 < 4 && i2 < 8, "bytes within two neighbouring words");
+    return __byte_perm(W[j], W[j + 1], (unsigned)(i1 | (i1 << 4) | (i2 << 8) | (i2 << 12))) & 0x00FF00FFu;
+}
+// horizontal_6tap_inplace's interior formula (:332-345) for outputs 2q and 2q + 1 of a word, in
+// halfword lanes: output j = p[2j-2] + p[2j+3] + 10 (p[2j] + p[2j+1]) + 5 (p[2j-1] + p[2j+2]), + 16 >> 5.
+template <int Q>
+__device__ __forceinline__ uint32_t h6tap_pair(const uint32_t (&W)[4]) {
+    constexpr int m = 4 * Q;  // source byte offset of the pair's first output, relative to 8 * word
+    const uint32_t s = pair_bytes<m - 2, m>(W) + pair_bytes<m + 3, m + 5>(W) +
+                       10u * (pair_bytes<m, m + 2>(W) + pair_bytes<m + 1, m + 3>(W)) +
+                       5u * (pair_bytes<m - 1, m + 1>(W) + pair_bytes<m + 2, m + 4>(W)) + 0x00100010u;
+    return (s >> 5) & 0x00FF00FFu;  // each lane <= 255: the weights sum to 32
+}
+
+// Output rows [r0, r0 + nr) of level lv + 1 of one plane of one frame, from level lv: the vertical
+// 6-tap into shared memory (a thread walks down one column word: consecutive output rows share four
+// of their six source rows, so it keeps them in registers and loads two rows per output row; 4
+// columns in halfword lanes), then the horizontal 6-tap, 4 output bytes per 32-bit store. Called by
+// the whole CTA.
+__device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restrict__ dst, uint8_t *inter_all, int plane,
+                                            int64_t f, int lv, int r0, int nr) {
     const PlaneGeo g = plane_geo(D, plane);
     const bool c = plane > 0;
     const int S = (int)g.stride, SW = S >> 2;
     uint8_t *base = dst + f * D.frame_bytes + g.out_off;
     const int rows = (int)g.rows;
-    for (int lv = 0; lv + 1 < D.levels; lv++) {
-        const int src_w = c ? D.lw[lv] / 2 : D.lw[lv], src_h = c ? D.lh[lv] / 2 : D.lh[lv];
-        const int dst_w = c ? D.lw[lv + 1] / 2 : D.lw[lv + 1], dst_h = c ? D.lh[lv + 1] / 2 : D.lh[lv + 1];
-        const int srow0 = (int)(c ? D.row_c[lv] : D.row_y[lv]);
-        const int drow0 = (int)(c ? D.row_c[lv + 1] : D.row_y[lv + 1]);
-        const bool active = D.scale_down == 4 && dst_w > 0 && src_w > 0 && src_h > 0;
-        const int iw = (src_w + 3) >> 2;  // intermediate words per row
-        for (int r0 = 0; r0 < dst_h; r0 += kRows) {
-            const int nr = min(kRows, dst_h - r0);
-            if (active) {
-                for (int t = threadIdx.x; t < nr * iw; t += blockDim.x) {
-                    const int r = t / iw, xw = t - r * iw;
-                    const int dy = r0 + r, sy = 2 * dy;
-                    const uint32_t *col = reinterpret_cast<const uint32_t *>(base + (int64_t)srow0 * S) + xw;
-                    auto row = [&](int yy) -> uint32_t { return srow0 + yy < rows ? col[(int64_t)yy * SW] : 0u; };
-                    uint32_t v;
-                    if (dy == 0 || dy + 1 == dst_h || sy - 2 < 0 || sy + 3 >= src_h) {
-                        const int y0 = min(sy, src_h - 1), y1 = min(sy + 1, src_h - 1);
-                        v = avgu4(row(y0), row(y1));
+    const int src_w = c ? D.lw[lv] / 2 : D.lw[lv], src_h = c ? D.lh[lv] / 2 : D.lh[lv];
+    const int dst_w = c ? D.lw[lv + 1] / 2 : D.lw[lv + 1], dst_h = c ? D.lh[lv + 1] / 2 : D.lh[lv + 1];
+    const int srow0 = (int)(c ? D.row_c[lv] : D.row_y[lv]);
+    const int drow0 = (int)(c ? D.row_c[lv + 1] : D.row_y[lv + 1]);
+    const bool active = D.scale_down == 4 && dst_w > 0 && src_w > 0 && src_h > 0;
+    const int iw = (src_w + 3) >> 2;  // intermediate words per row
+    if (active) {
+        const uint32_t m = 0x00FF00FFu;
+        for (int xw = threadIdx.x; xw < iw; xw += blockDim.x) {
+            const uint32_t *col = reinterpret_cast<const uint32_t *>(base + (int64_t)srow0 * S) + xw;
+            auto row = [&](int yy) -> uint32_t { return srow0 + yy < rows ? col[(int64_t)yy * SW] : 0u; };
+            uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+            int have = -1000;  // the window holds source rows have-2 .. have+3
+            for (int r = 0; r < nr; r++) {
+                const int dy = r0 + r, sy = 2 * dy;
+                uint32_t v;
+                if (dy == 0 || dy + 1 == dst_h || sy - 2 < 0 || sy + 3 >= src_h) {
+                    const int y0 = min(sy, src_h - 1), y1 = min(sy + 1, src_h - 1);
+                    v = avgu4(row(y0), row(y1));
+                } else {
+                    if (have == sy - 2) {
+                        a0 = a2; a1 = a3; a2 = a4; a3 = a5;
+                        a4 = row(sy + 2); a5 = row(sy + 3);
                     } else {
-                        const uint32_t a0 = row(sy - 2), a1 = row(sy - 1), a2 = row(sy), a3 = row(sy + 1),
-                                       a4 = row(sy + 2), a5 = row(sy + 3);
-                        const uint32_t m = 0x00FF00FFu;
-                        const uint32_t e = (a0 & m) + (a5 & m) + 5u * ((a1 & m) + (a4 & m)) +
-                                           10u * ((a2 & m) + (a3 & m)) + 0x00100010u;
-                        const uint32_t od = ((a0 >> 8) & m) + ((a5 >> 8) & m) + 5u * (((a1 >> 8) & m) + ((a4 >> 8) & m)) +
-                                            10u * (((a2 >> 8) & m) + ((a3 >> 8) & m)) + 0x00100010u;
-                        v = ((e >> 5) & m) | (((od >> 5) & m) << 8);  // each lane <= 255: weights sum to 32
+                        a0 = row(sy - 2); a1 = row(sy - 1); a2 = row(sy); a3 = row(sy + 1);
+                        a4 = row(sy + 2); a5 = row(sy + 3);
                     }
-                    reinterpret_cast<uint32_t *>(inter_all)[r * iw + xw] = v;
+                    have = sy;
+                    const uint32_t e = (a0 & m) + (a5 & m) + 5u * ((a1 & m) + (a4 & m)) +
+                                       10u * ((a2 & m) + (a3 & m)) + 0x00100010u;
+                    const uint32_t od = ((a0 >> 8) & m) + ((a5 >> 8) & m) + 5u * (((a1 >> 8) & m) + ((a4 >> 8) & m)) +
+                                        10u * (((a2 >> 8) & m) + ((a3 >> 8) & m)) + 0x00100010u;
+                    v = ((e >> 5) & m) | (((od >> 5) & m) << 8);  // each lane <= 255: weights sum to 32
                 }
+                reinterpret_cast<uint32_t *>(inter_all)[r * iw + xw] = v;
             }
-            __syncthreads();
-            for (int t = threadIdx.x; t < nr * SW; t += blockDim.x) {
-                const int r = t / SW, xw = t - r * SW;
-                const int dy = r0 + r;
-                uint32_t word = 0;
-                if (active) {
-                    const uint8_t *in = inter_all + r * iw * 4;
-                    auto get = [&](int i, unsigned dflt) -> unsigned { return i < src_w ? in[i] : dflt; };
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const int i = xw * 4 + q;
-                        unsigned v = 0;
-                        if (i < dst_w) {
-                            if (dst_w <= 2) {
-                                const unsigned a = get(2 * i, 0);
-                                v = avg8(a, get(2 * i + 1, a));
-                            } else if (i == 0 || i == dst_w - 1) {
-                                const unsigned a = i == 0 ? in[0] : get(2 * i, 0);
-                                v = avg8(a, get(2 * i + 1, a));
-                            } else {
-                                const unsigned left = i == 1 ? avg8(in[0], get(1, in[0])) : get(2 * i - 2, 0);
-                                const unsigned pk = get(2 * i + 3, in[src_w - 1]);
-                                const unsigned sm = left + pk + 10u * (get(2 * i, 0) + get(2 * i + 1, 0)) +
-                                                    5u * (get(2 * i - 1, 0) + get(2 * i + 2, 0)) + 16u;
-                                v = min(sm >> 5, 255u);
-                            }
-                        } else if (i < src_w) {
-                            v = in[i];
-                        }
-                        word |= v << (8 * q);
-                    }
-                }
-                if (drow0 + dy < rows) reinterpret_cast<uint32_t *>(base + (int64_t)(drow0 + dy) * S)[xw] = word;
-            }
-            __syncthreads();
         }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nr * SW; t += blockDim.x) {
+        const int r = t / SW, xw = t - r * SW;
+        const int dy = r0 + r;
+        uint32_t word = 0;
+        if (active && xw >= 1 && 4 * xw + 5 <= dst_w && 8 * xw + 9 < src_w) {
+            // four interior outputs: source bytes 8xw-2 .. 8xw+9 of the row, in halfword lanes
+            const uint32_t *in32 = reinterpret_cast<const uint32_t *>(inter_all) + r * iw + 2 * xw - 1;
+            const uint32_t W[4] = {in32[0], in32[1], in32[2], in32[3]};
+            word = __byte_perm(h6tap_pair<0>(W), h6tap_pair<1>(W), 0x6420);
+        } else if (active) {
+            const uint8_t *in = inter_all + r * iw * 4;
+            auto get = [&](int i, unsigned dflt) -> unsigned { return i < src_w ? in[i] : dflt; };
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int i = xw * 4 + q;
+                unsigned v = 0;
+                if (i < dst_w) {
+                    if (dst_w <= 2) {
+                        const unsigned a = get(2 * i, 0);
+                        v = avg8(a, get(2 * i + 1, a));
+                    } else if (i == 0 || i == dst_w - 1) {
+                        const unsigned a = i == 0 ? in[0] : get(2 * i, 0);
+                        v = avg8(a, get(2 * i + 1, a));
+                    } else {
+                        const unsigned left = i == 1 ? avg8(in[0], get(1, in[0])) : get(2 * i - 2, 0);
+                        const unsigned pk = get(2 * i + 3, in[src_w - 1]);
+                        const unsigned sm = left + pk + 10u * (get(2 * i, 0) + get(2 * i + 1, 0)) +
+                                            5u * (get(2 * i - 1, 0) + get(2 * i + 2, 0)) + 16u;
+                        v = min(sm >> 5, 255u);
+                    }
+                } else if (i < src_w) {
+                    v = in[i];
+                }
+                word |= v << (8 * q);
+            }
+        }
+        if (drow0 + dy < rows) reinterpret_cast<uint32_t *>(base + (int64_t)(drow0 + dy) * S)[xw] = word;
+    }
+    __syncthreads();
+}
+
+// One pyramid level of every plane of every frame: a grid of resident CTAs strides over bands of
+// `band` output rows (frame, plane, band), each CTA doing a band's vertical then horizontal pass.
+__global__ void __launch_bounds__(256) super_reduce_band_kernel(SuperDev D, uint8_t *__restrict__ dst, int lv, int band,
+                                                                int nb_y, int nb_c, uint32_t nitems) {
+    extern __shared__ __align__(16) uint8_t inter_all[];
+    const uint32_t per = (uint32_t)(nb_y + 2 * nb_c);
+    for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const uint32_t e = it % per;
+        const int64_t f = it / per;
+        int plane, b;
+        if (e < (uint32_t)nb_y) { plane = 0; b = (int)e; }
+        else { plane = 1 + (int)((e - nb_y) / (uint32_t)nb_c); b = (int)((e - nb_y) % (uint32_t)nb_c); }
+        const int dst_h = plane ? D.lh[lv + 1] / 2 : D.lh[lv + 1];
+        const int r0 = b * band;
+        reduce_band(D, dst, inter_all, plane, f, lv, r0, min(band, dst_h - r0));
     }
 }
 
 // Every row start of the source and super frames on a 16-byte boundary, 8-bit samples, and
 // no bicubic planes: the fast paths apply.
-bool vec_ok(const SuperDev &D, const void *src, const void *dst) {
+bool vec_ok(const SuperDev &D, const void *src, const void *dst, int nframes) {
     auto a16 = [](int64_t v) { return (v & 15) == 0; };
     return D.px_bytes == 1 && D.scale_up != 2 && D.width >= 2 && (((uintptr_t)src | (uintptr_t)dst) & 15) == 0 &&
            a16(D.y_stride) && a16(D.c_stride) && a16(D.y_len) && a16(D.c_len) && a16(D.frame_bytes) &&
            a16(D.src_y_stride) && a16(D.src_c_stride) && a16(D.src_y_len) && a16(D.src_c_len) &&
-           a16(D.src_frame_bytes) && D.y_rows * D.y_stride < (1ll << 31) && D.c_stride >= 4;
+           a16(D.src_frame_bytes) && D.y_rows * D.y_stride < (1ll << 31) && D.c_stride >= 4 &&
+           (int64_t)nframes * D.height * (D.y_stride / 16) < (1ll << 31);
 }
 }  // namespace
 
@@ -413,31 +503,35 @@ int launch_super_t(const SuperDev &D, const T *src, T *dst, int nframes, cudaStr
 }
 }  // namespace
 
-// The fast paths: level 0 in two launches (luma, then both chroma planes), then the whole
-// pyramid in one launch of a CTA per frame and plane (enough CTAs to fill the GPU; a launch of
-// a few frames takes the per-level kernels, which spread one level over many CTAs).
+// The fast paths: level 0 in two launches each (luma, then both chroma planes; the chunks inside
+// the rows, then the edge chunks), then one launch per pyramid level over bands of rows of every
+// plane and frame.
 int launch_super_vec(const SuperDev &D, const uint8_t *src, uint8_t *dst, int nframes, int sms, cudaStream_t stream) {
     int n = 0;
     for (int pl = 0; pl < 2; pl++) {
         const int64_t S = pl ? D.c_stride : D.y_stride;
         const int h = pl ? D.height / 2 : D.height;
         if (h <= 0) continue;
-        dim3 g((unsigned)((S / 16 + 127) / 128), (unsigned)h, (unsigned)(nframes * (pl ? 2 : 1)));
-        super_level0_vec_kernel<<<g, 128, 0, stream>>>(D, src, dst, pl ? 1 : 0, pl ? 2 : 1);
-        n++;
-    }
-    if (D.levels <= 1) return n;
-    if (3 * nframes >= sms) {
-        const size_t smem = (size_t)kRows * (size_t)((D.lw[0] + 3) & ~3);
-        super_pyramid_kernel<<<(unsigned)(3 * nframes), 512, smem, stream>>>(D, dst);
-        return n + 1;
+        const int nplanes = pl ? 2 : 1, chunks = (int)(S / 16);
+        const uint32_t nitems = (uint32_t)((int64_t)nframes * nplanes * h * chunks);
+        const int grid = (int)std::min<int64_t>((nitems + 255) / 256, (int64_t)sms * 4);
+        super_level0_vec_kernel<<<grid, 256, 0, stream>>>(D, src, dst, pl ? 1 : 0, nplanes, h, chunks, nitems);
+        const int w = pl ? D.width / 2 : D.width;
+        const int ce = std::min(w / 16, chunks);  // chunks with x0 + 16 <= w: the vector kernel's
+        const uint32_t nedge = (uint32_t)((int64_t)nframes * nplanes * ((int64_t)(h - 1) * (chunks - ce) + chunks));
+        super_level0_edge_kernel<<<(int)std::min<int64_t>((nedge + 127) / 128, (int64_t)sms * 8), 128, 0, stream>>>(
+            D, src, dst, pl ? 1 : 0, nplanes, h, chunks, ce, nedge);
+        n += 2;
     }
     for (int lv = 0; lv + 1 < D.levels; lv++) {
-        const int rows = D.lh[lv + 1];
-        if (rows <= 0) continue;
-        const size_t smem = (size_t)(D.lw[lv] > 0 ? D.lw[lv] : 1);
-        dim3 g((unsigned)rows, 3, (unsigned)nframes);
-        super_reduce_kernel<uint8_t><<<g, 256, smem, stream>>>(D, dst, lv);
+        const int dh_y = D.lh[lv + 1], dh_c = D.lh[lv + 1] / 2;
+        if (dh_y <= 0) continue;
+        const int row_bytes = (D.lw[lv] + 3) & ~3;  // the level's widest intermediate row (luma)
+        const int band = std::max(1, std::min(16, (32 << 10) / std::max(row_bytes, 1)));
+        const int nb_y = (dh_y + band - 1) / band, nb_c = (dh_c + band - 1) / band;
+        const uint32_t nitems = (uint32_t)((int64_t)nframes * (nb_y + 2 * nb_c));
+        const int grid = (int)std::min<int64_t>(nitems, (int64_t)sms * 8);
+        super_reduce_band_kernel<<<grid, 256, (size_t)band * row_bytes, stream>>>(D, dst, lv, band, nb_y, nb_c, nitems);
         n++;
     }
     return n;
@@ -452,7 +546,7 @@ cudaError_t launch_super(const SuperDev &D, const uint8_t *src, uint8_t *dst, in
             return 148;
         return v;
     }();
-    if (vec_ok(D, src, dst)) {
+    if (vec_ok(D, src, dst, nframes)) {
         const int n = launch_super_vec(D, src, dst, nframes, sms, stream);
         if (launches) *launches += n;
         return cudaGetLastError();
