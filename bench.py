@@ -1148,6 +1148,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--shape", default="", help="batched: fixed launch shape name[:tiles_per_lane], no autotune")
     ap.add_argument("--no-lookahead", action="store_true", help="Analyse without look-ahead (A/B timing)")
+    ap.add_argument("--size", default="", help="WxH: the 1080p / 640x360 workload's options at another frame size")
     ap.add_argument("--lookahead", type=int, default=1, help="look-ahead levels: 1 level 0, 2 coarser, 3 all")
     ap.add_argument("--shard", default="clips", choices=["clips", "frames"],
                     help="N>1: a clip per GPU (weak scaling, default) or one clip split in frame ranges (strong)")
@@ -1185,6 +1186,9 @@ def main():
     dev = torch.device("cuda", local)
     c = CONFIGS[WORKLOAD]
     w, h, nf = c["width"], c["height"], args.frames or c["frames"]
+    if args.size:  # the workload's options and motion at another frame size (profiling cases; no CPU leg)
+        w, h = (int(v) for v in args.size.lower().split("x"))
+        args.no_cpu = True
     sb = sv.Super(w, h, SUPER_OPT[WORKLOAD])
     an = sv.Analyse(sb.sdata, ANALYSE_OPT[WORKLOAD], w, h)
     an.set_lookahead(0 if args.no_lookahead else args.lookahead)
@@ -1361,7 +1365,9 @@ def main():
                                   "(level-0 counters of the last timed step)"},
             "super_ms_per_step": statistics.mean(super_ms), "analyse_ms_per_step": statistics.mean(analyse_ms),
         }
-        if world == 1 and WORKLOAD == "1080p" and not args.no_sub:
+        if args.size:
+            line["config"].update(width=w, height=h, workload=f"{w}x{h}: " + line["config"]["workload"])
+        if world == 1 and WORKLOAD == "1080p" and not args.no_sub and not args.size:
             # the metric's other two halves (batched vs plain, served p50/p99), each in its own
             # process after this one's buffers are released
             del frames_d, supers_d, pay_d, scratch_d, pinned, out_host

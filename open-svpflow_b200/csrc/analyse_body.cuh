@@ -43,6 +43,14 @@
 #if !defined(SVPF_NT) || !defined(SVPF_MINB) || !defined(SVPF_VARIANT)
 #error "define SVPF_NT, SVPF_MINB and SVPF_VARIANT before including analyse_body.cuh"
 #endif
+// SVPF_LOOKAHEAD: the shape runs the look-ahead (search_level_spec) when the parameter block asks
+// for it. Only the 128-thread shapes with two CTAs per SM (128 registers) do: there it measured
+// faster (the 1080p clip: 125.2 -> 134.3 pairs/s); with three CTAs per SM at 80 registers the
+// independent warps' instruction fetches cost more than the overlap gains (297 pairs at 960x540:
+// 593 -> 692 ms), so the other shapes keep the serial order.
+#ifndef SVPF_LOOKAHEAD
+#define SVPF_LOOKAHEAD 0
+#endif
 
 namespace svpf {
 namespace SVPF_VARIANT {
@@ -2133,7 +2141,7 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
         __syncthreads();  // both directions' projections of this level are ready
         if (!s.abort_) {
             const uint2 *prevp = (first) ? nullptr : other_proj[level & 1];
-            if (NW > 1 && (P.lookahead & (level == 0 ? 1 : 2)) && level_spec_ok(x, s, ds))
+            if (SVPF_LOOKAHEAD && NW > 1 && (P.lookahead & (level == 0 ? 1 : 2)) && level_spec_ok(x, s, ds))
                 search_level_spec(x, s, ds, prevp, status, spec_stats);
             else
                 search_level(x, s, ds, prevp, status);

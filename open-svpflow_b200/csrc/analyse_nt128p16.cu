@@ -4,4 +4,5 @@
 #define SVPF_MINB 2
 #define SVPF_VARIANT nt128p16
 #define SVPF_PX16 1
+#define SVPF_LOOKAHEAD 1
 #include "analyse_body.cuh"
