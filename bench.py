@@ -67,8 +67,8 @@ DESC = {
 }
 UNIT = "frame-pairs/s"
 # DRAM bytes per frame pair of the Analyse kernel at 1080p (ncu capture of a 17-pair launch:
-# 291.6 MB read + 50.2 MB written)
-TRAFFIC_PER_PAIR = 341.8e6 / 17
+# 290.6 MB read + 49.3 MB written)
+TRAFFIC_PER_PAIR = 339.9e6 / 17
 # DRAM bytes of one 1080p render launch with the 8 x 8 effective block (ncu capture: 4.13 MB read,
 # the written frame stays in L2)
 RENDER_TRAFFIC_PER_FRAME = 4.14e6
@@ -82,10 +82,10 @@ INT32_LANES_PER_SM = 128
 OPS_PER_PAIR = {"1080p": 19.38e9}
 # why the Analyse kernel reaches the fraction it does, from the ncu capture in
 # profiles/analyse_kernel_1080p_17f.md: issue-active x (algorithmic ops / executed lane slots)
-ROOF_DECOMPOSITION = {"issue_active": 0.358, "useful_lane_fraction": 0.19,
-                      "source": "ncu capture of a 17-pair 1080p launch (1 CTA per SM): 3.16 G warp instructions "
-                                "= 101 G lane slots per pair for 19.4 G algorithmic ops",
-                      "kernel_version": "before the level-0 look-ahead"}
+ROOF_DECOMPOSITION = {"issue_active": 0.375, "useful_lane_fraction": 0.24,
+                      "source": "ncu capture of a 17-pair 1080p launch (1 CTA per SM, the nt128 shape with the "
+                                "level-0 look-ahead): 2.53 G warp instructions = 80.8 G lane slots per pair for "
+                                "19.4 G algorithmic ops (profiles/analyse_kernel_1080p_17f.md)"}
 # the CPU legs time this many frame pairs per host thread, so that their figure is a throughput
 # (dynamic scheduling over many pairs) rather than the latency of the slowest pair
 CPU_PAIRS_PER_THREAD = 4

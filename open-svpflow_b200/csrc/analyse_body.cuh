@@ -97,6 +97,10 @@ struct Cand {
 // direction (coarser levels), or one warp (level 0 with look-ahead, one block per warp in
 // flight). Per-warp entries are indexed by the warp's place in the direction; a group's
 // entries are those of its first warp (Ctx::wbase).
+// Groups that stage a block's source at once: one per warp with the look-ahead, else one per
+// direction (shared memory not used for staging is L1 cache for the rest).
+constexpr int kSrcGroups = SVPF_LOOKAHEAD ? NW : 1;
+
 struct DirSh {
     long long K[2][NW];                   // per-warp best (cost, index, sad) of a step, double-buffered
     int I[2][NW];
@@ -116,7 +120,7 @@ struct DirSh {
     // Per group: the block's source pixels, 4 per entry: luma (bw/4 x bh), then U and V
     // (cw/4 x crows). A plane searched with SATD holds 16-bit pairs (x = pixels 0,1;
     // y = pixels 2,3), a SAD plane the packed word in x.
-    uint2 srcp[NW][384];
+    uint2 srcp[kSrcGroups][384];
     int2 clist[NW][32 * MW];  // per warp: the step's candidates passing the cuts, in order (mv, index)
     long long r64[NW][3];
     int r32[NW][2];
@@ -908,7 +912,7 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                 for (; t < x.tl; t += G) {
                     const int ty = t >> b.lgtx, tx = t & (b.tilesx - 1);
                     const px_t *rp = rl + (ty * 4 * ys + tx * 4);
-                    const uint2 *sp = s.srcp[x.wbase] + ((ty * 4) << b.lgtx) + tx;
+                    const uint2 *sp = s.srcp[kSrcGroups > 1 ? x.wbase : 0] + ((ty * 4) << b.lgtx) + tx;
                     r.L += b.satd_mode ? tile_satd_p(sp, b.tilesx, rp, ys) : tile_sad_p(sp, b.tilesx, rp, ys);
                 }
 #pragma unroll 1
@@ -919,7 +923,8 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                     const int ty = ct >> b.lgctx, tx = ct & (b.ctilesx - 1);
                     if (ty * 4 >= b.crows) continue;
                     const px_t *rp = (pl ? x.R.v : x.R.u) + cref + (ty * 4 * cs + tx * 4);
-                    const uint2 *sp = s.srcp[x.wbase] + nlw + pl * b.ctilesx * b.crows + ((ty * 4) << b.lgctx) + tx;
+                    const uint2 *sp = s.srcp[kSrcGroups > 1 ? x.wbase : 0] + nlw + pl * b.ctilesx * b.crows +
+                                      ((ty * 4) << b.lgctx) + tx;
                     const unsigned v = x.satd ? tile_satd_p(sp, b.ctilesx, rp, cs) : tile_sad_p(sp, b.ctilesx, rp, cs);
                     if (pl) r.V += v; else r.U += v;
                 }
@@ -1091,7 +1096,7 @@ __device__ __forceinline__ void stage_source(const Ctx &x, DirSh &s, const BlkC 
     if (b.fast_src) {
         const int nlw = b.tilesx * b.bh;
         const int nth = x.nw * 32;
-        uint2 *sp = s.srcp[x.wbase];
+        uint2 *sp = s.srcp[kSrcGroups > 1 ? x.wbase : 0];
         for (int t = x.tid; t < nlw; t += nth) {
             const int row = t >> b.lgtx, col = t & (b.tilesx - 1);
             sp[t] = stage4(x.S.y + b.lsrc + row * x.G.ys32 + col * 4, b.satd_mode != 0);

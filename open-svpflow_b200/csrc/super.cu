@@ -363,10 +363,10 @@ __device__ __forceinline__ uint32_t h6tap_pair(const uint32_t (&W)[4]) {
 }
 
 // Output rows [r0, r0 + nr) of level lv + 1 of one plane of one frame, from level lv: the vertical
-// 6-tap into shared memory (a thread walks down one column word: consecutive output rows share four
-// of their six source rows, so it keeps them in registers and loads two rows per output row; 4
-// columns in halfword lanes), then the horizontal 6-tap, 4 output bytes per 32-bit store. Called by
-// the whole CTA.
+// 6-tap into shared memory (the band's rows in two halves; a thread walks down one 16-byte column
+// chunk, keeping in registers the four source rows consecutive output rows share, so it loads two
+// rows per output row; bytes in halfword lanes), then the horizontal 6-tap, 4 output bytes per
+// 32-bit store. Called by the whole CTA.
 __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restrict__ dst, uint8_t *inter_all, int plane,
                                             int64_t f, int lv, int r0, int nr) {
     const PlaneGeo g = plane_geo(D, plane);
@@ -379,20 +379,35 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
     const int srow0 = (int)(c ? D.row_c[lv] : D.row_y[lv]);
     const int drow0 = (int)(c ? D.row_c[lv + 1] : D.row_y[lv + 1]);
     const bool active = D.scale_down == 4 && dst_w > 0 && src_w > 0 && src_h > 0;
-    const int iw = (src_w + 3) >> 2;  // intermediate words per row
+    const int iw = (src_w + 3) >> 2;        // intermediate words per row
+    const int iq = (iw + 3) >> 2, ist = 4 * iq;  // 16-byte chunks per row; shared-memory row stride (words)
     if (active) {
+        // the band's rows in two halves, each walked down by its own threads; a thread takes a
+        // 16-byte column chunk (the pitch is a multiple of 16, so the chunk stays inside the row)
         const uint32_t m = 0x00FF00FFu;
-        for (int xw = threadIdx.x; xw < iw; xw += blockDim.x) {
-            const uint32_t *col = reinterpret_cast<const uint32_t *>(base + (int64_t)srow0 * S) + xw;
-            auto row = [&](int yy) -> uint32_t { return srow0 + yy < rows ? col[(int64_t)yy * SW] : 0u; };
-            uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+        const int hr = (nr + 1) >> 1;
+        const uint4 z4 = make_uint4(0, 0, 0, 0);
+        auto vert = [&](uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t a4, uint32_t a5) -> uint32_t {
+            const uint32_t e = (a0 & m) + (a5 & m) + 5u * ((a1 & m) + (a4 & m)) + 10u * ((a2 & m) + (a3 & m)) +
+                               0x00100010u;
+            const uint32_t od = ((a0 >> 8) & m) + ((a5 >> 8) & m) + 5u * (((a1 >> 8) & m) + ((a4 >> 8) & m)) +
+                                10u * (((a2 >> 8) & m) + ((a3 >> 8) & m)) + 0x00100010u;
+            return ((e >> 5) & m) | (((od >> 5) & m) << 8);  // each lane <= 255: weights sum to 32
+        };
+        for (int t = threadIdx.x; t < 2 * iq; t += blockDim.x) {
+            const int cq = t % iq, half = t / iq;
+            const int ra = half * hr, rb = min(nr, ra + hr);
+            const uint4 *col = reinterpret_cast<const uint4 *>(base + (int64_t)srow0 * S) + cq;
+            const int SQ = S >> 4;
+            auto row = [&](int yy) -> uint4 { return srow0 + yy < rows ? col[(int64_t)yy * SQ] : z4; };
+            uint4 a0 = z4, a1 = z4, a2 = z4, a3 = z4, a4 = z4, a5 = z4;
             int have = -1000;  // the window holds source rows have-2 .. have+3
-            for (int r = 0; r < nr; r++) {
+            for (int r = ra; r < rb; r++) {
                 const int dy = r0 + r, sy = 2 * dy;
-                uint32_t v;
+                uint4 v;
                 if (dy == 0 || dy + 1 == dst_h || sy - 2 < 0 || sy + 3 >= src_h) {
-                    const int y0 = min(sy, src_h - 1), y1 = min(sy + 1, src_h - 1);
-                    v = avgu4(row(y0), row(y1));
+                    const uint4 p = row(min(sy, src_h - 1)), q = row(min(sy + 1, src_h - 1));
+                    v = make_uint4(avgu4(p.x, q.x), avgu4(p.y, q.y), avgu4(p.z, q.z), avgu4(p.w, q.w));
                 } else {
                     if (have == sy - 2) {
                         a0 = a2; a1 = a3; a2 = a4; a3 = a5;
@@ -402,13 +417,10 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
                         a4 = row(sy + 2); a5 = row(sy + 3);
                     }
                     have = sy;
-                    const uint32_t e = (a0 & m) + (a5 & m) + 5u * ((a1 & m) + (a4 & m)) +
-                                       10u * ((a2 & m) + (a3 & m)) + 0x00100010u;
-                    const uint32_t od = ((a0 >> 8) & m) + ((a5 >> 8) & m) + 5u * (((a1 >> 8) & m) + ((a4 >> 8) & m)) +
-                                        10u * (((a2 >> 8) & m) + ((a3 >> 8) & m)) + 0x00100010u;
-                    v = ((e >> 5) & m) | (((od >> 5) & m) << 8);  // each lane <= 255: weights sum to 32
+                    v = make_uint4(vert(a0.x, a1.x, a2.x, a3.x, a4.x, a5.x), vert(a0.y, a1.y, a2.y, a3.y, a4.y, a5.y),
+                                   vert(a0.z, a1.z, a2.z, a3.z, a4.z, a5.z), vert(a0.w, a1.w, a2.w, a3.w, a4.w, a5.w));
                 }
-                reinterpret_cast<uint32_t *>(inter_all)[r * iw + xw] = v;
+                reinterpret_cast<uint4 *>(inter_all)[(r * ist >> 2) + cq] = v;
             }
         }
     }
@@ -419,11 +431,11 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
         uint32_t word = 0;
         if (active && xw >= 1 && 4 * xw + 5 <= dst_w && 8 * xw + 9 < src_w) {
             // four interior outputs: source bytes 8xw-2 .. 8xw+9 of the row, in halfword lanes
-            const uint32_t *in32 = reinterpret_cast<const uint32_t *>(inter_all) + r * iw + 2 * xw - 1;
+            const uint32_t *in32 = reinterpret_cast<const uint32_t *>(inter_all) + r * ist + 2 * xw - 1;
             const uint32_t W[4] = {in32[0], in32[1], in32[2], in32[3]};
             word = __byte_perm(h6tap_pair<0>(W), h6tap_pair<1>(W), 0x6420);
         } else if (active) {
-            const uint8_t *in = inter_all + r * iw * 4;
+            const uint8_t *in = inter_all + r * ist * 4;
             auto get = [&](int i, unsigned dflt) -> unsigned { return i < src_w ? in[i] : dflt; };
 #pragma unroll
             for (int q = 0; q < 4; q++) {
@@ -456,7 +468,7 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
 
 // One pyramid level of every plane of every frame: a grid of resident CTAs strides over bands of
 // `band` output rows (frame, plane, band), each CTA doing a band's vertical then horizontal pass.
-__global__ void __launch_bounds__(256) super_reduce_band_kernel(SuperDev D, uint8_t *__restrict__ dst, int lv, int band,
+__global__ void __launch_bounds__(256, 4) super_reduce_band_kernel(SuperDev D, uint8_t *__restrict__ dst, int lv, int band,
                                                                 int nb_y, int nb_c, uint32_t nitems) {
     extern __shared__ __align__(16) uint8_t inter_all[];
     const uint32_t per = (uint32_t)(nb_y + 2 * nb_c);
@@ -526,11 +538,11 @@ int launch_super_vec(const SuperDev &D, const uint8_t *src, uint8_t *dst, int nf
     for (int lv = 0; lv + 1 < D.levels; lv++) {
         const int dh_y = D.lh[lv + 1], dh_c = D.lh[lv + 1] / 2;
         if (dh_y <= 0) continue;
-        const int row_bytes = (D.lw[lv] + 3) & ~3;  // the level's widest intermediate row (luma)
+        const int row_bytes = (D.lw[lv] + 15) & ~15;  // the level's widest intermediate row (luma), 16-byte rows
         const int band = std::max(1, std::min(16, (32 << 10) / std::max(row_bytes, 1)));
         const int nb_y = (dh_y + band - 1) / band, nb_c = (dh_c + band - 1) / band;
         const uint32_t nitems = (uint32_t)((int64_t)nframes * (nb_y + 2 * nb_c));
-        const int grid = (int)std::min<int64_t>(nitems, (int64_t)sms * 8);
+        const int grid = (int)std::min<int64_t>(nitems, (int64_t)sms * 4);
         super_reduce_band_kernel<<<grid, 256, (size_t)band * row_bytes, stream>>>(D, dst, lv, band, nb_y, nb_c, nitems);
         n++;
     }
