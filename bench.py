@@ -1296,8 +1296,9 @@ def main():
         alg_analyse = a_count * (2 * fb + pl)  # algorithmic bytes of one Analyse launch: 2 super frames + payload per pair
         alg_super = n_src * (sb.source_len() + fb)  # one Super launch sequence: source read + super frame write
         int_peak = INT32_LANES_PER_SM * _sm_count() * SM_MAX_MHZ * 1e6
-        ops_pair = OPS_PER_PAIR.get(WORKLOAD)
-        ops_src = "constant from an earlier oracle count of the same workload (CPU leg not run)"
+        ops_pair = None if args.size else OPS_PER_PAIR.get(WORKLOAD)  # the constants hold at the workload's size
+        ops_src = ("no count at this frame size (CPU leg not run)" if args.size else
+                   "constant from an earlier oracle count of the same workload (CPU leg not run)")
         cpu = None
         parity = None
         cnt = None
@@ -1317,7 +1318,7 @@ def main():
             "bound": "int32 pipe", "unit": "Tops/s", "peak": int_peak / 1e12,
             "achieved": ops_pair * a_count / (a_ms / 1000) / 1e12 if ops_pair else None,
             "frac": ops_pair * a_count / (a_ms / 1000) / int_peak if ops_pair else None,
-            "traffic": TRAFFIC_PER_PAIR * a_count if WORKLOAD == "1080p" else None,
+            "traffic": TRAFFIC_PER_PAIR * a_count if WORKLOAD == "1080p" and not args.size else None,
             "traffic_unit": "bytes per launch",
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 17-pair launch, per pair x pairs",
             "ops_per_pair": ops_pair, "ops_source": ops_src, "avg_launch_ms": a_ms,

@@ -492,20 +492,71 @@ __device__ __forceinline__ uint32_t pairs_lo(uint32_t w) { return __byte_perm(w,
 __device__ __forceinline__ uint32_t pairs_hi(uint32_t w) { return __byte_perm(w, 0u, 0x4342); }  // bytes 2, 3
 
 #ifndef SVPF_PX16
+// 8-bit SATD runs in f16x2 instead: a sample s becomes the half 1024 + s (exponent of 1024,
+// s in the mantissa: one byte permute), so a difference of two samples is exact, and so is
+// every later value (integers of magnitude <= 8 * 255 = 2040 <= 2048, where halves are
+// exact). The four-row sums go to f32. Same arithmetic as satd_rows, fewer instructions
+// (the f16x2 add / sub / max are single instructions; |x| clears the sign bits).
+__device__ __forceinline__ uint32_t bias_lo(uint32_t w) { return __byte_perm(w, 0x64646464u, 0x4140); }
+__device__ __forceinline__ uint32_t bias_hi(uint32_t w) { return __byte_perm(w, 0x64646464u, 0x4342); }
+__device__ __forceinline__ uint32_t h2add(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("add.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t h2sub(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("sub.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t h2max(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("max.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t h2abs(uint32_t a) { return a & 0x7FFF7FFFu; }
+// acc + both halves of h, in f32 (sm_100 mixed-precision add)
+__device__ __forceinline__ float f32_add_h2(float acc, uint32_t h) {
+    asm("{.reg .b16 l, h; mov.b32 {l, h}, %1; add.rn.f32.f16 %0, l, %0; add.rn.f32.f16 %0, h, %0;}"
+        : "+f"(acc) : "r"(h));
+    return acc;
+}
+// d01 / d23: the rows' differences as f16 pairs (samples 0,1 and 2,3)
+__device__ __forceinline__ unsigned satd_rows_h(const uint32_t d01[4], const uint32_t d23[4]) {
+    uint32_t h0[4], h1[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const uint32_t c = h2add(d01[r], d23[r]), e = h2sub(d01[r], d23[r]);
+        const uint32_t p = __byte_perm(c, e, 0x5410), q = __byte_perm(c, e, 0x7632);
+        h0[r] = h2add(p, q);
+        h1[r] = h2sub(p, q);
+    }
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const uint32_t *h = k ? h1 : h0;
+        const uint32_t a0 = h2add(h[0], h[1]), a1 = h2sub(h[0], h[1]);
+        const uint32_t a2 = h2add(h[2], h[3]), a3 = h2sub(h[2], h[3]);
+        acc = f32_add_h2(acc, h2max(h2abs(a0), h2abs(a2)));
+        acc = f32_add_h2(acc, h2max(h2abs(a1), h2abs(a3)));
+    }
+    return 2u * (unsigned)acc;
+}
 __device__ __forceinline__ uint32_t ld4u(const uint8_t *p) {
     const uintptr_t a = (uintptr_t)p;
     const uint32_t *q = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
     return __funnelshift_r(__ldg(q), __ldg(q + 1), (unsigned)(a & 3) * 8u);
 }
-// four samples as halfword pairs
-__device__ __forceinline__ uint2 ld4p(const px_t *p) {
+// four samples as biased f16 pairs
+__device__ __forceinline__ uint2 ld4h(const px_t *p) {
     const uint32_t w = ld4u(p);
-    return make_uint2(pairs_lo(w), pairs_hi(w));
+    return make_uint2(bias_lo(w), bias_hi(w));
 }
-// The staged entry of 4 source samples for a plane searched with SATD (pairs) or SAD (word).
+// The staged entry of 4 source samples for a plane searched with SATD (biased f16 pairs) or
+// SAD (the packed word).
 __device__ __forceinline__ uint2 stage4(const px_t *p, bool satd) {
     const uint32_t w = ld4u(p);
-    return satd ? make_uint2(pairs_lo(w), pairs_hi(w)) : make_uint2(w, 0u);
+    return satd ? make_uint2(bias_lo(w), bias_hi(w)) : make_uint2(w, 0u);
 }
 __device__ __forceinline__ unsigned sad4(uint2 staged, const px_t *rp) {
     return __dp4a(__vabsdiffu4(staged.x, ld4u(rp)), 0x01010101u, 0u);
@@ -538,6 +589,15 @@ __device__ __forceinline__ unsigned sum4(const px_t *p) {
 // tiles with both blocks in global memory (special candidates)
 __device__ __forceinline__ unsigned tile_satd(const px_t *sp, const px_t *rp, int st) {
     uint32_t d01[4], d23[4];
+#ifndef SVPF_PX16
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const uint2 a = ld4h(sp + r * st), b = ld4h(rp + r * st);
+        d01[r] = h2sub(a.x, b.x);
+        d23[r] = h2sub(a.y, b.y);
+    }
+    return satd_rows_h(d01, d23);
+#else
 #pragma unroll
     for (int r = 0; r < 4; r++) {
         const uint2 a = ld4p(sp + r * st), b = ld4p(rp + r * st);
@@ -545,6 +605,7 @@ __device__ __forceinline__ unsigned tile_satd(const px_t *sp, const px_t *rp, in
         d23[r] = __vsub2(a.y, b.y);
     }
     return satd_rows(d01, d23);
+#endif
 }
 __device__ __forceinline__ unsigned tile_sad(const px_t *sp, const px_t *rp, int st) {
     unsigned s = 0;
@@ -555,6 +616,15 @@ __device__ __forceinline__ unsigned tile_sad(const px_t *sp, const px_t *rp, int
 // tiles over the staged source (see DirSh::srcp)
 __device__ __forceinline__ unsigned tile_satd_p(const uint2 *sp, int spp, const px_t *rp, int st) {
     uint32_t d01[4], d23[4];
+#ifndef SVPF_PX16
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const uint2 a = sp[r * spp], b = ld4h(rp + r * st);
+        d01[r] = h2sub(a.x, b.x);
+        d23[r] = h2sub(a.y, b.y);
+    }
+    return satd_rows_h(d01, d23);
+#else
 #pragma unroll
     for (int r = 0; r < 4; r++) {
         const uint2 a = sp[r * spp], b = ld4p(rp + r * st);
@@ -562,6 +632,7 @@ __device__ __forceinline__ unsigned tile_satd_p(const uint2 *sp, int spp, const 
         d23[r] = __vsub2(a.y, b.y);
     }
     return satd_rows(d01, d23);
+#endif
 }
 __device__ __forceinline__ unsigned tile_sad_p(const uint2 *sp, int spp, const px_t *rp, int st) {
     unsigned s = 0;
@@ -1620,61 +1691,76 @@ __device__ __forceinline__ void search_level_spec(const Ctx &xd, DirSh &s, DirSc
         const int sel_x = bmx, sel_y = bmy;
         bcost = (long long)bsad;
         const unsigned dcsum = slotL[phs][dcslot];
-        int bad_unused = 0;
-        run_search_steps(x, b, s, ph, refine ? RS_REFINE_ONLY : RS_NONE, stype, radius, lambda, ppx, ppy, imv.x, imv.y,
-                         idx, bad_unused, bmx, bmy, bsad, bcost);
-        if (!waited) wait_prev(k);
-        n_blk++;
-        if (refine && ndef > 0) {
-            n_def++;
-            long long cb = sel_cost;
-            int cpos = bpos, cx = sel_x, cy = sel_y;
-            unsigned csad = 0;
-            bool dwin = false;
+        // One call site of the search state machine (it is inlined, so each site is a copy of the
+        // evaluation code): pass 0 the refinement with the seeds known at the start; pass 1 the
+        // refinement again from a deferred seed that wins; pass 2 the bad-SAD test and expansion
+        // (:604-672) with the count of the blocks committed before.
+        int stage = refine ? RS_REFINE_ONLY : RS_NONE, pass = 0, bad_count = 0;
+        for (;;) {
+            run_search_steps(x, b, s, ph, stage, stype, radius, lambda, ppx, ppy, imv.x, imv.y, idx, bad_count, bmx,
+                             bmy, bsad, bcost);
+            if (pass == 0) {
+                if (!waited) wait_prev(k);
+                n_blk++;
+                if (refine && ndef > 0) {
+                    n_def++;
+                    long long cb = sel_cost;
+                    int cpos = bpos, cx = sel_x, cy = sel_y;
+                    unsigned csad = 0;
+                    bool dwin = false;
 #pragma unroll
-            for (int j = 0; j < 3; j++) {
-                if (j >= ndef) break;
-                const int64_t ci = j == 0 ? dc0 : (j == 1 ? dc1 : dc2);
-                const int pos = 4 + (j == 0 ? dq0 : (j == 1 ? dq1 : dq2));
-                const int2 m = vmv(field[ci]);
-                // its exact_sad: from an evaluated candidate with the same vector (same block, same
-                // reads), else evaluated now
-                unsigned sd = 0;
-                bool have = true;
-                if (m.x == imv.x && m.y == imv.y) sd = slotL[phs][0];
-                else if (prev_slot >= 0 && m.x == pmx && m.y == pmy) sd = slotL[phs][prev_slot];
-                else if (m.x == 0 && m.y == 0) sd = slotL[phs][zslot];
-                else if (m.x == gxv && m.y == gyv) sd = slotL[phs][gslot];
-                else {
-                    have = false;
+                    for (int j = 0; j < 3; j++) {
+                        if (j >= ndef) break;
+                        const int64_t ci = j == 0 ? dc0 : (j == 1 ? dc1 : dc2);
+                        const int pos = 4 + (j == 0 ? dq0 : (j == 1 ? dq1 : dq2));
+                        const int2 m = vmv(field[ci]);
+                        // its exact_sad: from an evaluated candidate with the same vector (same block,
+                        // same reads), else evaluated now
+                        unsigned sd = 0;
+                        bool have = true;
+                        if (m.x == imv.x && m.y == imv.y) sd = slotL[phs][0];
+                        else if (prev_slot >= 0 && m.x == pmx && m.y == pmy) sd = slotL[phs][prev_slot];
+                        else if (m.x == 0 && m.y == 0) sd = slotL[phs][zslot];
+                        else if (m.x == gxv && m.y == gyv) sd = slotL[phs][gslot];
+                        else {
+                            have = false;
 #pragma unroll
-                    for (int t = 0; t < 8; t++)
-                        if (!have && t < nseeds && sdx[t] == m.x && sdy[t] == m.y) { sd = slotL[phs][nslot0 + t]; have = true; }
+                            for (int t = 0; t < 8; t++)
+                                if (!have && t < nseeds && sdx[t] == m.x && sdy[t] == m.y) {
+                                    sd = slotL[phs][nslot0 + t];
+                                    have = true;
+                                }
+                        }
+                        if (!have) {
+                            Res r = eval_lane(x, b, 0, 0, 0, m.x, m.y, !smallest, lane, 32);
+                            group_sum3(r, 32);
+                            unsigned Lv, Cv;
+                            finalize(r, Lv, Cv);
+                            sd = !smallest ? sat_add(Lv, Cv) : Lv;
+                            n_eval++;
+                        }
+                        const long long cst = (long long)sd + (((long long)P.pnbour * sd) >> 8);
+                        if (cst < cb || (cst == cb && pos < cpos)) {
+                            cb = cst; cpos = pos; cx = m.x; cy = m.y; csad = sd; dwin = true;
+                        }
+                    }
+                    if (dwin && (cx != sel_x || cy != sel_y)) {  // a deferred seed with another vector wins
+                        n_rerun++;
+                        bmx = cx; bmy = cy; bsad = csad; bcost = (long long)csad;
+                        pass = 1;
+                        continue;
+                    }
                 }
-                if (!have) {
-                    Res r = eval_lane(x, b, 0, 0, 0, m.x, m.y, !smallest, lane, 32);
-                    group_sum3(r, 32);
-                    unsigned Lv, Cv;
-                    finalize(r, Lv, Cv);
-                    sd = !smallest ? sat_add(Lv, Cv) : Lv;
-                    n_eval++;
-                }
-                const long long cst = (long long)sd + (((long long)P.pnbour * sd) >> 8);
-                if (cst < cb || (cst == cb && pos < cpos)) { cb = cst; cpos = pos; cx = m.x; cy = m.y; csad = sd; dwin = true; }
             }
-            if (dwin && (cx != sel_x || cy != sel_y)) {  // a deferred seed with another vector wins
-                n_rerun++;
-                bmx = cx; bmy = cy; bsad = csad; bcost = (long long)csad;
-                run_search_steps(x, b, s, ph, RS_REFINE_ONLY, stype, radius, lambda, ppx, ppy, imv.x, imv.y, idx,
-                                 bad_unused, bmx, bmy, bsad, bcost);
+            if (pass < 2 && refine && level > 0) {
+                bad_count = s.bad_count;
+                stage = RS_BAD_ONLY;
+                pass = 2;
+                continue;
             }
+            break;
         }
-        if (refine && level > 0) {  // the bad-SAD test and expansion (:604-672) with the blocks' count so far
-            int bad_count = s.bad_count;
-            run_search_steps(x, b, s, ph, RS_BAD_ONLY, stype, radius, lambda, ppx, ppy, imv.x, imv.y, idx, bad_count,
-                             bmx, bmy, bsad, bcost);
-            if (lane == 0) s.bad_count = bad_count;
-        }
+        if (pass == 2 && lane == 0) s.bad_count = bad_count;
         // ---- store (:673-679) and hand the order on to the next block's warp
         const int rows = b.py >= 0 ? imax(0, imin(b.bh, L.lh - b.py)) : 0;
         const int cols = b.px >= 0 ? imax(0, imin(b.bw, L.lw - b.px)) : 0;
