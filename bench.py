@@ -1149,7 +1149,8 @@ def main():
     ap.add_argument("--shape", default="", help="batched: fixed launch shape name[:tiles_per_lane], no autotune")
     ap.add_argument("--no-lookahead", action="store_true", help="Analyse without look-ahead (A/B timing)")
     ap.add_argument("--size", default="", help="WxH: the 1080p / 640x360 workload's options at another frame size")
-    ap.add_argument("--lookahead", type=int, default=1, help="look-ahead levels: 1 level 0, 2 coarser, 3 all")
+    ap.add_argument("--lookahead", type=int, default=5,
+                    help="look-ahead bits: 1 level 0, 2 coarser levels, 4 level 0 in its own launch (default 5)")
     ap.add_argument("--shard", default="clips", choices=["clips", "frames"],
                     help="N>1: a clip per GPU (weak scaling, default) or one clip split in frame ranges (strong)")
     ap.add_argument("--no-sub", action="store_true",
@@ -1314,7 +1315,9 @@ def main():
                        f"per SATD 4x4 tile)")
         # the Analyse kernel's primary bound: the int32 pipes (no dense contraction, little HBM traffic)
         roof = {
-            "kernel": "analyse_kernel (one CTA per frame pair, fwd/bwd halves; level 0 one block per warp)",
+            "kernel": ("Analyse: analyse_kernel (one CTA per frame pair, fwd/bwd halves: the coarser levels), "
+                       "analyse_level0_kernel (one CTA per warp: level 0 with look-ahead), analyse_finish_kernel; "
+                       "timed together"),
             "bound": "int32 pipe", "unit": "Tops/s", "peak": int_peak / 1e12,
             "achieved": ops_pair * a_count / (a_ms / 1000) / 1e12 if ops_pair else None,
             "frac": ops_pair * a_count / (a_ms / 1000) / int_peak if ops_pair else None,
@@ -1359,7 +1362,7 @@ def main():
             "cpu_baseline": cpu,
             "parity_vs_oracle": parity,
             "serial_chain": _chain(an, a_count, a_ms),
-            "lookahead": {**la, "levels": 0 if args.no_lookahead else args.lookahead,
+            "lookahead": {**la, "mode": 0 if args.no_lookahead else args.lookahead,
                           "rerun_fraction": la["reruns"] / la["blocks"] if la["blocks"] else None,
                           "note": "one block per warp in flight; each block re-checks the neighbour seeds "
                                   "committed after it started and re-runs its refinement when one wins "

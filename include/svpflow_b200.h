@@ -118,10 +118,12 @@ int svpf_device_status(const void *scratch_dev, void *stream);
  * each warp of a search direction takes its own block in the reference's order, searches it
  * without the neighbour vectors not yet committed, then, in order, re-checks the reference's
  * selection with them and repeats the refinement when one wins; results are bit-identical
- * with it on or off. `levels`: 0 off, 1 level 0 only (the default), 2 the coarser levels only,
- * 3 every level. Only the 128-thread launch shape with two CTAs per SM runs it (the plain path's
- * shape for launches of at most two frame pairs per SM); the others always keep the serial order.
- * Affects launches made after the call. */
+ * with it on or off. `levels` is a bit set: 1 level 0, 2 the coarser levels, 4 level 0 spread
+ * over the GPU (with 1: a launch of its own with one CTA per warp, so every SM carries the same
+ * share of the walking warps; the pair kernel and a finish kernel run before and after it).
+ * 0 turns it off; the default is 5. Only the 128-thread launch shape with two CTAs per SM runs
+ * it (the plain path's shape for launches of at most two frame pairs per SM); the others always
+ * keep the serial order. Affects launches made after the call. */
 int svpf_analyser_set_lookahead(svpf_analyser *a, int32_t levels);
 /* The look-ahead counters of the last device launch on `scratch_dev` (synchronises `stream`):
  * out[0] level-0 blocks, out[1] blocks with deferred neighbour seeds, out[2] deferred seeds

@@ -96,20 +96,21 @@ struct Cand {
 // Shared state of one search direction. A block is searched by a group of warps: the whole
 // direction (coarser levels), or one warp (level 0 with look-ahead, one block per warp in
 // flight). Per-warp entries are indexed by the warp's place in the direction; a group's
-// entries are those of its first warp (Ctx::wbase).
-// Groups that stage a block's source at once: one per warp with the look-ahead, else one per
-// direction (shared memory not used for staging is L1 cache for the rest).
-constexpr int kSrcGroups = SVPF_LOOKAHEAD ? NW : 1;
-
-struct DirSh {
-    long long K[2][NW];                   // per-warp best (cost, index, sad) of a step, double-buffered
-    int I[2][NW];
-    unsigned S[2][NW];
-    unsigned slotL[NW][2][MAXSLOT];       // per group: special-candidate results (exact_sad values)
-    long long rk[2][NGMAX], rm[2][NGMAX]; // exact sequential scan: per-group cost, motion
-    unsigned rs[2][NGMAX];
-    int ri[2][NGMAX];
-    unsigned char rv[2][NGMAX];
+// entries are those of its first warp (Ctx::wbase). W: the warps it holds state for (the
+// direction's, or one for a CTA of the level-0 kernel).
+template <int W>
+struct DirShT {
+    // Groups that stage a block's source at once: one per warp with the look-ahead, else one per
+    // direction (shared memory not used for staging is L1 cache for the rest).
+    static constexpr int kSrc = (SVPF_LOOKAHEAD && W > 1) ? W : 1;
+    long long K[2][W];                    // per-warp best (cost, index, sad) of a step, double-buffered
+    int I[2][W];
+    unsigned S[2][W];
+    unsigned slotL[W][2][MAXSLOT];        // per group: special-candidate results (exact_sad values)
+    long long rk[2][W * 32], rm[2][W * 32];  // exact sequential scan: per-group cost, motion
+    unsigned rs[2][W * 32];
+    int ri[2][W * 32];
+    unsigned char rv[2][W * 32];
     int committed;                        // look-ahead: blocks of the level committed so far (in order)
     int late_;                            // look-ahead: a hand-over wait gave up
     int unsafe_;                          // look-ahead: the level has an input the reference panics on
@@ -118,13 +119,15 @@ struct DirSh {
     int order_len;
     int abort_;
     // Per group: the block's source pixels, 4 per entry: luma (bw/4 x bh), then U and V
-    // (cw/4 x crows). A plane searched with SATD holds 16-bit pairs (x = pixels 0,1;
-    // y = pixels 2,3), a SAD plane the packed word in x.
-    uint2 srcp[kSrcGroups][384];
-    int2 clist[NW][32 * MW];  // per warp: the step's candidates passing the cuts, in order (mv, index)
-    long long r64[NW][3];
-    int r32[NW][2];
+    // (cw/4 x crows). A plane searched with SATD holds biased f16 pairs (8-bit samples; see
+    // satd_rows_h) or 16-bit pairs (x = pixels 0,1; y = pixels 2,3), a SAD plane the packed word in x.
+    uint2 srcp[kSrc][384];
+    int2 clist[W][32 * MW];  // per warp: the step's candidates passing the cuts, in order (mv, index)
+    long long r64[W][3];
+    int r32[W][2];
 };
+using DirSh = DirShT<NW>;  // a search direction of the pair kernels
+using WarpSh = DirShT<1>;  // a CTA (one warp) of the level-0 kernel
 
 struct Planes {
     const px_t *y, *u, *v;
@@ -913,7 +916,8 @@ __device__ __forceinline__ void finalize(const Res &r, unsigned &L, unsigned &C)
 // ballot bitmask, identical in every warp), then groups take the passing candidates
 // in order. On return, identically in every thread: win = accepted candidate or -1,
 // and the new best cost / sad when accepted.
-__device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s, int &ph, const Gen &g, int lambda,
+template <class SH>
+__device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, SH &s, int &ph, const Gen &g, int lambda,
                                           int predx, int predy, long long &best_cost, unsigned &best_sad, int &win) {
     const int lane = x.tid & 31, warp = x.tid >> 5, wi = x.wbase + warp;  // wi: the warp's place in the direction
     const bool serial = x.pnew < -256;
@@ -928,7 +932,7 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
         const long long cut = best_cost;
         // this warp's copy of the passing candidates, in candidate order (every warp
         // computes the same list, so no barrier is needed)
-#pragma unroll
+#pragma unroll 1
         for (int w = 0; w < MW; w++) {
             if (base + w * 32 >= g.n) break;  // uniform
             const int i = base + w * 32 + lane;
@@ -983,7 +987,7 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                 for (; t < x.tl; t += G) {
                     const int ty = t >> b.lgtx, tx = t & (b.tilesx - 1);
                     const px_t *rp = rl + (ty * 4 * ys + tx * 4);
-                    const uint2 *sp = s.srcp[kSrcGroups > 1 ? x.wbase : 0] + ((ty * 4) << b.lgtx) + tx;
+                    const uint2 *sp = s.srcp[SH::kSrc > 1 ? x.wbase : 0] + ((ty * 4) << b.lgtx) + tx;
                     r.L += b.satd_mode ? tile_satd_p(sp, b.tilesx, rp, ys) : tile_sad_p(sp, b.tilesx, rp, ys);
                 }
 #pragma unroll 1
@@ -994,7 +998,7 @@ __device__ __forceinline__ void eval_step(const Ctx &x, const BlkC &b, DirSh &s,
                     const int ty = ct >> b.lgctx, tx = ct & (b.ctilesx - 1);
                     if (ty * 4 >= b.crows) continue;
                     const px_t *rp = (pl ? x.R.v : x.R.u) + cref + (ty * 4 * cs + tx * 4);
-                    const uint2 *sp = s.srcp[kSrcGroups > 1 ? x.wbase : 0] + nlw + pl * b.ctilesx * b.crows +
+                    const uint2 *sp = s.srcp[SH::kSrc > 1 ? x.wbase : 0] + nlw + pl * b.ctilesx * b.crows +
                                       ((ty * 4) << b.lgctx) + tx;
                     const unsigned v = x.satd ? tile_satd_p(sp, b.ctilesx, rp, cs) : tile_sad_p(sp, b.ctilesx, rp, cs);
                     if (pl) r.V += v; else r.U += v;
@@ -1163,11 +1167,12 @@ __device__ __forceinline__ uint2 mkvec(int dx, int dy, unsigned score) {
 enum { S_REFINE, S_HEX_START, S_HEX_ITER, S_HEX_EXIT, S_BAD, S_BAD_RING, S_FINAL_RING, S_STORE };
 
 // The block's source pixels into shared memory (DirSh::srcp) for the fast path.
-__device__ __forceinline__ void stage_source(const Ctx &x, DirSh &s, const BlkC &b) {
+template <class SH>
+__device__ __forceinline__ void stage_source(const Ctx &x, SH &s, const BlkC &b) {
     if (b.fast_src) {
         const int nlw = b.tilesx * b.bh;
         const int nth = x.nw * 32;
-        uint2 *sp = s.srcp[kSrcGroups > 1 ? x.wbase : 0];
+        uint2 *sp = s.srcp[SH::kSrc > 1 ? x.wbase : 0];
         for (int t = x.tid; t < nlw; t += nth) {
             const int row = t >> b.lgtx, col = t & (b.tilesx - 1);
             sp[t] = stage4(x.S.y + b.lsrc + row * x.G.ys32 + col * 4, b.satd_mode != 0);
@@ -1192,12 +1197,13 @@ __device__ __forceinline__ void stage_source(const Ctx &x, DirSh &s, const BlkC 
 // there (the look-ahead runs the two apart: the test reads the bad count of the blocks
 // committed before), RS_NONE runs nothing.
 enum { RS_NONE, RS_ALL, RS_REFINE_ONLY, RS_BAD_ONLY };
+template <class SH>
 #ifdef SVPF_RS_NOINLINE
 __device__ __noinline__ void run_search_steps(
 #else
 __device__ __forceinline__ void run_search_steps(
 #endif
-const Ctx &x, const BlkC &b, DirSh &s, int &ph, int stage, int stype,
+const Ctx &x, const BlkC &b, SH &s, int &ph, int stage, int stype,
                                                  int radius, int lambda, int ppx, int ppy, int own_x, int own_y,
                                                  int64_t idx, int &bad_count, int &bmx, int &bmy, unsigned &bsad,
                                                  long long &bcost) {
@@ -1472,7 +1478,9 @@ __device__ __forceinline__ void search_level(const Ctx &x, DirSh &s, DirScratch 
 // them; the committing warp stores its results, fences, then bumps the count). Bounded: false once
 // kWaitCycles have passed or another warp of the direction has given up (the caller flags
 // ST_TIMEOUT and carries on, so every warp still reaches its barriers). The fence after the wait
-// makes the committed blocks' stores visible to every lane.
+// makes the committed blocks' stores visible to every lane. XSM: the count and the stores it
+// publishes are in global memory, written by warps on other SMs.
+template <bool XSM>
 __device__ __forceinline__ bool wait_commits(volatile int *committed, int64_t k, volatile int *late) {
     const long long t0 = clock64();
     for (;;) {
@@ -1485,7 +1493,8 @@ __device__ __forceinline__ bool wait_commits(volatile int *committed, int64_t k,
         }
         __nanosleep(32);
     }
-    __threadfence_block();
+    if (XSM) __threadfence();
+    else __threadfence_block();
     return true;
 }
 
@@ -1513,29 +1522,36 @@ __device__ __forceinline__ bool wait_commits(volatile int *committed, int64_t k,
 // A level with an input on which the reference would panic takes search_level instead.
 // stats (nullable): [0] blocks, [1] blocks with deferred seeds, [2] deferred seeds evaluated
 // (the others had the vector of a candidate already evaluated), [3] refinements run again.
-__device__ __forceinline__ void search_level_spec(const Ctx &xd, DirSh &s, DirScratch &ds, const uint2 *prevp, int *status,
-                                                  unsigned long long *stats) {
-    const AnalyseParams &P = *xd.P;
-    const LevelInfo &L = *xd.L;
-    const int level = xd.level, gw = L.gw, gh = L.gh;
+//
+// spec_walk is one warp's part: blocks g, g + D, ... of the level (x: a one-warp group; x.tid
+// the lane). The count of committed blocks, the flag of a wait that gave up and the
+// direction's abort flag are passed in: in shared memory when the direction's warps share a CTA
+// (XSM false), in the pair's scratch when they are CTAs on different SMs (XSM true, the level-0
+// kernel), where the field's cells written during the level are read from L2 (__ldcg: the SM's
+// L1 is not coherent with the other SMs' stores) and commits fence device-wide.
+template <bool XSM>
+__device__ __forceinline__ uint2 ld_cell(const uint2 *p) {
+    if (XSM) return __ldcg(p);
+    return *p;
+}
+template <bool XSM, class SH>
+__device__ __forceinline__ void spec_walk(const Ctx &x, SH &s, DirScratch &ds, const uint2 *prevp, int g, int64_t order_len,
+                                          int gxv, int gyv, volatile int *committed, volatile int *late_flag,
+                                          int *abort_flag, int *status, unsigned long long *stats) {
+    const AnalyseParams &P = *x.P;
+    const LevelInfo &L = *x.L;
+    const int level = x.level, gw = L.gw, gh = L.gh;
     uint2 *field = ds.vec[level & 1];
     uint8_t *lumaf = ds.luma[level & 1];
-    const int64_t order_len = s.order_len;
     const bool smallest = L.smallest != 0;
     constexpr int D = NW;
-    const int g = xd.tid >> 5, lane = xd.tid & 31;
-    Ctx x = xd;
-    x.nw = 1;
-    x.wbase = g;
-    x.tid = lane;
-    if (xd.tid == 0) { s.committed = 0; s.late_ = 0; s.bad_count = 0; }
-    dbar(xd.d);
+    const int lane = x.tid;
     int ph = 0;
     unsigned long long n_blk = 0, n_def = 0, n_eval = 0, n_rerun = 0;
     bool late = false;
-    unsigned (*slotL)[MAXSLOT] = s.slotL[g];
+    unsigned (*slotL)[MAXSLOT] = s.slotL[x.wbase];
     auto wait_prev = [&](int64_t k) {  // block k - 1 is committed (and its stores visible) after this
-        if (k > 0 && !wait_commits(&s.committed, k, &s.late_)) late = true;
+        if (k > 0 && !wait_commits<XSM>(committed, k, late_flag)) late = true;
     };
     auto pos_of = [&](int nx, int ny) -> int64_t {
         return level == 0 ? initial_order_pos(gw, gh, nx, ny) : (int64_t)ds.pos[(int64_t)ny * gw + nx];
@@ -1558,7 +1574,7 @@ __device__ __forceinline__ void search_level_spec(const Ctx &xd, DirSh &s, DirSc
             const int64_t p = pos_of(sxi, syi);
             if (p < k && p > k - D) { wait_prev(k); waited = true; }
         }
-        const uint2 interp = field[edge ? sidx : idx];
+        const uint2 interp = ld_cell<XSM>(field + (edge ? sidx : idx));
         const int2 imv = vmv(interp);
         BlkC b;
         make_blk(x, px, py, !smallest, b);
@@ -1577,12 +1593,11 @@ __device__ __forceinline__ void search_level_spec(const Ctx &xd, DirSh &s, DirSc
             }
         }
         const int zslot = n++, gslot = n++, nslot0 = n;
-        const int gxv = s.gx, gyv = s.gy;
         int sdx[8], sdy[8], sq[8];        // seeds evaluated now: vector, place among the block's seeds
         int dq0 = 0, dq1 = 0, dq2 = 0;    // deferred seeds: place among the block's seeds ...
         int64_t dc0 = 0, dc1 = 0, dc2 = 0;  // ... and cell
         int nseeds = 0, nall = 0, ndef = 0;
-#pragma unroll
+#pragma unroll 1
         for (int q = 0; q < 9; q++) {
             const int ny = by - 1 + q / 3, nx = bx - 1 + q % 3;
             if (ny < 0 || ny >= gh || nx < 0 || nx >= gw) continue;
@@ -1595,7 +1610,7 @@ __device__ __forceinline__ void search_level_spec(const Ctx &xd, DirSh &s, DirSc
                 else { dq2 = nall; dc2 = ci; }
                 ndef++;
             } else {
-                const int2 nm = vmv(field[ci]);
+                const int2 nm = vmv(ld_cell<XSM>(field + ci));
 #pragma unroll
                 for (int t = 0; t < 8; t++)
                     if (t == nseeds) { sdx[t] = nm.x; sdy[t] = nm.y; sq[t] = nall; }
@@ -1708,12 +1723,12 @@ __device__ __forceinline__ void search_level_spec(const Ctx &xd, DirSh &s, DirSc
                     int cpos = bpos, cx = sel_x, cy = sel_y;
                     unsigned csad = 0;
                     bool dwin = false;
-#pragma unroll
+#pragma unroll 1
                     for (int j = 0; j < 3; j++) {
                         if (j >= ndef) break;
                         const int64_t ci = j == 0 ? dc0 : (j == 1 ? dc1 : dc2);
                         const int pos = 4 + (j == 0 ? dq0 : (j == 1 ? dq1 : dq2));
-                        const int2 m = vmv(field[ci]);
+                        const int2 m = vmv(ld_cell<XSM>(field + ci));
                         // its exact_sad: from an evaluated candidate with the same vector (same block,
                         // same reads), else evaluated now
                         unsigned sd = 0;
@@ -1770,13 +1785,15 @@ __device__ __forceinline__ void search_level_spec(const Ctx &xd, DirSh &s, DirSc
         if (lane == 0) {
             field[idx] = mkvec(bmx, bmy, smallest ? sat_mul(bsad, 3) : bsad);
             lumaf[idx] = (uint8_t)dc;
-            __threadfence_block();  // the block's stores (and bad_count) before the count that publishes them
-            *(volatile int *)&s.committed = (int)(k + 1);
+            // the block's stores (and bad_count) before the count that publishes them
+            if (XSM) __threadfence();
+            else __threadfence_block();
+            *committed = (int)(k + 1);
         }
         __syncwarp();
     }
     if (lane == 0) {
-        if (late) { atomicOr(status, ST_TIMEOUT); s.abort_ = 1; }
+        if (late) { atomicOr(status, ST_TIMEOUT); *abort_flag = 1; }
         if (stats && level == 0) {
             atomicAdd(stats + 0, n_blk);
             atomicAdd(stats + 1, n_def);
@@ -1784,6 +1801,18 @@ __device__ __forceinline__ void search_level_spec(const Ctx &xd, DirSh &s, DirSc
             atomicAdd(stats + 3, n_rerun);
         }
     }
+}
+// The direction's warps of one CTA walk the level together (the count in shared memory).
+__device__ __forceinline__ void search_level_spec(const Ctx &xd, DirSh &s, DirScratch &ds, const uint2 *prevp, int *status,
+                                                  unsigned long long *stats) {
+    if (xd.tid == 0) { s.committed = 0; s.late_ = 0; s.bad_count = 0; }
+    dbar(xd.d);
+    const int g = xd.tid >> 5;
+    Ctx x = xd;
+    x.nw = 1;
+    x.wbase = g;
+    x.tid = xd.tid & 31;
+    spec_walk<false>(x, s, ds, prevp, g, s.order_len, s.gx, s.gy, &s.committed, &s.late_, &s.abort_, status, stats);
     dbar(xd.d);
 }
 
@@ -2048,22 +2077,14 @@ __device__ void reorder(const Ctx &x, DirSh &s, const uint2 *field, int gw, int 
     dbar(x.d);
 }
 
-// One frame pair, both directions: the whole of analyse_pair (:68-226) plus the payload
-// (:2740-2811). Called by every thread of the CTA; threads of a direction the
-// configuration does not search (vectors 1 or 2 under a 2-direction batch CTA) only
-// take part in the CTA-wide barriers. Status bits go to *status.
-__device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const PairRef pr, uint8_t *__restrict__ pay,
-                                                 uint8_t *__restrict__ scr, int *status, int &cta_abort,
-                                                 unsigned long long *spec_stats) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const bool bidir = P.vectors == 3;
-    const int half = (int)(threadIdx.x / NT);
-    const bool idle = !bidir && half == 1;
-    const int d = bidir ? half : ((P.vectors & 2) ? 0 : 1);  // 0 = forward (cur -> ref), 1 = backward
-    const int tid = threadIdx.x % NT;
-    DirSh &s = reinterpret_cast<DirSh *>(smem)[half];
-    const px_t *src = (const px_t *)(d == 0 ? pr.cur : pr.ref);
-    const px_t *ref = (const px_t *)(d == 0 ? pr.ref : pr.cur);
+// The hand-over words of one direction (AnalyseParams::off_ctl) when level 0 runs in the
+// level-0 kernel: the pair kernel leaves the level with GO set (and the count, the global
+// predictor and whether the other direction's projection exists); the level-0 kernel's warps
+// count their commits in COMMITTED and flag a wait that gave up in LATE; ABORT, set by either,
+// tells the finish kernel to leave the pair's payload unwritten (the status word says why).
+enum { CTL_GO, CTL_COMMITTED, CTL_LATE, CTL_GX, CTL_GY, CTL_ABORT, CTL_PREV };
+
+__device__ __forceinline__ DirScratch dir_scratch(const AnalyseParams &P, uint8_t *scr, int d) {
     DirScratch ds;
     ds.vec[0] = (uint2 *)(scr + P.off_field[d]);
     ds.vec[1] = (uint2 *)(scr + P.off_next[d]);
@@ -2077,6 +2098,64 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
     ds.keys = (unsigned long long *)(scr + P.off_keys[d]);
     ds.hist = (unsigned *)(scr + P.off_hist[d]);
     ds.seen = scr + P.off_seen[d];
+    return ds;
+}
+
+// The per-level fields of the search context.
+__device__ __forceinline__ void set_level(Ctx &x, const AnalyseParams &P, int level) {
+    const LevelInfo &L = P.lv[level];
+    x.L = &L;
+    x.level = level;
+    x.satd = L.satd;
+    x.pel = L.pel;
+    x.G.lw = L.lw; x.G.lh = L.lh; x.G.clw = L.lw / 2; x.G.clh = L.lh / 2;
+    x.G.ys = P.y_stride; x.G.cs = P.c_stride; x.G.ylen = P.y_len; x.G.clen = P.c_len;
+    x.G.ys32 = (int)P.y_stride; x.G.cs32 = (int)P.c_stride;
+    x.pnew = P.pnew;
+    x.tl = L.tl;
+    x.tcp = L.tc;
+    {  // lanes per candidate: about `tiles_per_lane` 4x4 tiles per lane
+        const int T = L.tl + (L.smallest ? 0 : 2 * L.tc);
+        const int tpl = iclamp(P.tiles_per_lane, 1, 8);
+        const int want = (T + tpl - 1) / tpl;
+        int g = 1;
+        while (g < want && g < 32) g <<= 1;
+        x.grp_lanes = g;
+    }
+}
+
+// Pair b of a launch (analyse_filter.rs:277-282: frame n pairs with min(n + delta, num_frames - 1)).
+__device__ __forceinline__ PairRef pair_at(const PairSrc &psrc, int64_t pair) {
+    if (psrc.table) return psrc.table[pair];
+    const int64_t n = (int64_t)psrc.first + pair;
+    int64_t n2 = n + psrc.delta;
+    if (n2 > psrc.nframes - 1) n2 = psrc.nframes - 1;
+    PairRef pr;
+    pr.cur = psrc.clip + n * psrc.frame_bytes;
+    pr.ref = psrc.clip + n2 * psrc.frame_bytes;
+    return pr;
+}
+
+// One frame pair, both directions: the whole of analyse_pair (:68-226) plus the payload
+// (:2740-2811). Called by every thread of the CTA; threads of a direction the
+// configuration does not search (vectors 1 or 2 under a 2-direction batch CTA) only
+// take part in the CTA-wide barriers. Status bits go to *status. split: a direction whose
+// level 0 takes the look-ahead leaves it to the level-0 kernel (see CTL_GO) and the finish
+// kernel packs the payload.
+__device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const PairRef pr, uint8_t *__restrict__ pay,
+                                                 uint8_t *__restrict__ scr, int *status, int &cta_abort,
+                                                 unsigned long long *spec_stats, bool split) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const bool bidir = P.vectors == 3;
+    const int half = (int)(threadIdx.x / NT);
+    const bool idle = !bidir && half == 1;
+    const int d = bidir ? half : ((P.vectors & 2) ? 0 : 1);  // 0 = forward (cur -> ref), 1 = backward
+    const int tid = threadIdx.x % NT;
+    DirSh &s = reinterpret_cast<DirSh *>(smem)[half];
+    const px_t *src = (const px_t *)(d == 0 ? pr.cur : pr.ref);
+    const px_t *ref = (const px_t *)(d == 0 ? pr.ref : pr.cur);
+    DirScratch ds = dir_scratch(P, scr, d);
+    int *ctl = (int *)(scr + P.off_ctl[d]);
     Ctx x;
     x.P = &P;
     x.d = half;
@@ -2087,6 +2166,7 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
     x.R = Planes{ref, ref + P.y_len, ref + P.y_len + P.c_len};
     if (threadIdx.x == 0) cta_abort = 0;
     if (tid == 0) { s.abort_ = idle ? 2 : 0; s.gx = 0; s.gy = 0; s.order_len = 0; }
+    if (split && tid == 0 && !idle) { ctl[CTL_GO] = 0; ctl[CTL_ABORT] = 0; }
     __syncthreads();
     const uint2 *other_proj[2] = {nullptr, nullptr};
     {
@@ -2097,24 +2177,7 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
     int pgw = 0, pgh = 0;  // grid of the previous (coarser) level
     for (int level = P.nlevels - 1; level >= 0; level--) {
         const LevelInfo &L = P.lv[level];
-        x.L = &L;
-        x.level = level;
-        x.satd = L.satd;
-        x.pel = L.pel;
-        x.G.lw = L.lw; x.G.lh = L.lh; x.G.clw = L.lw / 2; x.G.clh = L.lh / 2;
-        x.G.ys = P.y_stride; x.G.cs = P.c_stride; x.G.ylen = P.y_len; x.G.clen = P.c_len;
-        x.G.ys32 = (int)P.y_stride; x.G.cs32 = (int)P.c_stride;
-        x.pnew = P.pnew;
-        x.tl = L.tl;
-        x.tcp = L.tc;
-        {  // lanes per candidate: about `tiles_per_lane` 4x4 tiles per lane
-            const int T = L.tl + (L.smallest ? 0 : 2 * L.tc);
-            const int tpl = iclamp(P.tiles_per_lane, 1, 8);
-            const int want = (T + tpl - 1) / tpl;
-            int g = 1;
-            while (g < want && g < 32) g <<= 1;
-            x.grp_lanes = g;
-        }
+        set_level(x, P, level);
         const int gw = L.gw, gh = L.gh;
         const int64_t ncell = (int64_t)gw * gh;
         const bool first = level == P.nlevels - 1;
@@ -2232,10 +2295,18 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
         __syncthreads();  // both directions' projections of this level are ready
         if (!s.abort_) {
             const uint2 *prevp = (first) ? nullptr : other_proj[level & 1];
-            if (SVPF_LOOKAHEAD && NW > 1 && (P.lookahead & (level == 0 ? 1 : 2)) && level_spec_ok(x, s, ds))
-                search_level_spec(x, s, ds, prevp, status, spec_stats);
-            else
+            if (SVPF_LOOKAHEAD && NW > 1 && (P.lookahead & (level == 0 ? 1 : 2)) && level_spec_ok(x, s, ds)) {
+                if (split && level == 0) {  // the level-0 kernel walks it
+                    if (tid == 0) {
+                        ctl[CTL_COMMITTED] = 0; ctl[CTL_LATE] = 0; ctl[CTL_GX] = s.gx; ctl[CTL_GY] = s.gy;
+                        ctl[CTL_PREV] = prevp != nullptr; ctl[CTL_GO] = 1;
+                    }
+                } else {
+                    search_level_spec(x, s, ds, prevp, status, spec_stats);
+                }
+            } else {
                 search_level(x, s, ds, prevp, status);
+            }
         }
         dbar(half);
         if (!s.abort_ && level > 0) {
@@ -2247,6 +2318,7 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
         if (tid == 0 && s.abort_ == 1) cta_abort = 1;
         __syncthreads();
     }
+    if (split && tid == 0 && !idle && s.abort_ == 1) ctl[CTL_ABORT] = 1;
 }
 
 // After the hierarchy: the refine pass when configured, then rescale_scores (:2716-2738)
@@ -2261,11 +2333,7 @@ __device__ __noinline__ void finish_pair(const AnalyseParams *Pp, const PairRef 
     const int d = bidir ? half : ((P.vectors & 2) ? 0 : 1);
     const int tid = threadIdx.x % NT;
     DirSh &s = reinterpret_cast<DirSh *>(smem)[half];
-    DirScratch ds;
-    ds.vec[0] = (uint2 *)(scr + P.off_field[d]);
-    ds.vec[1] = (uint2 *)(scr + P.off_next[d]);
-    ds.luma[0] = scr + P.off_out[d];
-    ds.luma[1] = scr + P.off_out[d] + P.max_cells;
+    DirScratch ds = dir_scratch(P, scr, d);
     if (P.has_refine) {
         const px_t *src = (const px_t *)(d == 0 ? pr.cur : pr.ref);
         const px_t *ref = (const px_t *)(d == 0 ? pr.ref : pr.cur);
@@ -2313,25 +2381,68 @@ __device__ __noinline__ void finish_pair(const AnalyseParams *Pp, const PairRef 
     }
 }
 
+// One CTA per frame pair. split: level 0 (where it takes the look-ahead) and the payload are
+// left to analyse_level0_kernel and analyse_finish_kernel.
 __global__ void __launch_bounds__(2 * NT, SVPF_MINB)
     analyse_kernel(const __grid_constant__ AnalyseParams P, const PairSrc psrc, uint8_t *__restrict__ payloads,
-                   uint8_t *__restrict__ scratch, int *status) {
+                   uint8_t *__restrict__ scratch, int *status, int split) {
     __shared__ int cta_abort;
     const int64_t pair = blockIdx.x;
-    PairRef pr;
-    if (psrc.table) {
-        pr = psrc.table[pair];
-    } else {  // analyse_filter.rs:277-282: frame n pairs with min(n + delta, num_frames - 1)
-        const int64_t n = (int64_t)psrc.first + pair;
-        int64_t n2 = n + psrc.delta;
-        if (n2 > psrc.nframes - 1) n2 = psrc.nframes - 1;
-        pr.cur = psrc.clip + n * psrc.frame_bytes;
-        pr.ref = psrc.clip + n2 * psrc.frame_bytes;
-    }
+    const PairRef pr = pair_at(psrc, pair);
     uint8_t *scr = scratch + pair * P.scratch_per_pair;
-    analyse_pair_dev(P, pr, payloads + pair * P.payload_len, scr, status, cta_abort, psrc.stats);
+    analyse_pair_dev(P, pr, payloads + pair * P.payload_len, scr, status, cta_abort, psrc.stats, split != 0);
     __syncthreads();
-    if (!cta_abort) finish_pair(&P, pr, payloads + pair * P.payload_len, scr);
+    if (!split && !cta_abort) finish_pair(&P, pr, payloads + pair * P.payload_len, scr);
+}
+
+// Level 0 spread over the GPU: one CTA per warp of a search direction, (pair, direction, g) for
+// the pairs first .. of the launch; warp g walks blocks g, g + NW, ... of the level exactly as
+// the pair kernel's look-ahead does, but its partners run on other SMs, so every SM holds about
+// the same number of walking warps whatever the pair count (one CTA per pair leaves some SMs
+// with two pairs and others with one). The warps of a direction wait on one another, so the
+// launch is cooperative: all its CTAs are resident at once, or it does not start.
+constexpr int kLevel0Blocks = 16;  // CTAs per SM: 128 registers per thread
+__global__ void __launch_bounds__(32, kLevel0Blocks)
+    analyse_level0_kernel(const __grid_constant__ AnalyseParams P, const PairSrc psrc, int64_t first,
+                          uint8_t *__restrict__ scratch, int *status) {
+    __shared__ WarpSh s;
+    const int ndir = P.vectors == 3 ? 2 : 1;
+    const int64_t pair = first + blockIdx.x / (ndir * NW);
+    const int rem = (int)(blockIdx.x % (ndir * NW)), half = rem / NW, g = rem % NW;
+    const int d = ndir == 2 ? half : ((P.vectors & 2) ? 0 : 1);
+    uint8_t *scr = scratch + pair * P.scratch_per_pair;
+    int *ctl = (int *)(scr + P.off_ctl[d]);
+    if (!ctl[CTL_GO]) return;  // the pair kernel ran this level itself, or the direction stopped
+    const PairRef pr = pair_at(psrc, pair);
+    const px_t *src = (const px_t *)(d == 0 ? pr.cur : pr.ref);
+    const px_t *ref = (const px_t *)(d == 0 ? pr.ref : pr.cur);
+    DirScratch ds = dir_scratch(P, scr, d);
+    Ctx x;
+    x.P = &P;
+    x.d = 0;
+    x.tid = threadIdx.x;
+    x.nw = 1;
+    x.wbase = 0;
+    x.S = Planes{src, src + P.y_len, src + P.y_len + P.c_len};
+    x.R = Planes{ref, ref + P.y_len, ref + P.y_len + P.c_len};
+    set_level(x, P, 0);
+    const int od = ndir == 2 ? 1 - d : d;
+    const uint2 *prevp = ctl[CTL_PREV] ? (const uint2 *)(scr + P.off_proj[od][0]) : nullptr;
+    spec_walk<true>(x, s, ds, prevp, g, initial_order_len(P.lv[0].gw, P.lv[0].gh), ctl[CTL_GX], ctl[CTL_GY],
+                    ctl + CTL_COMMITTED, ctl + CTL_LATE, ctl + CTL_ABORT, status, psrc.stats);
+}
+
+// After the level-0 kernel: the refine pass, rescale and packing of every pair not stopped.
+__global__ void __launch_bounds__(2 * NT, SVPF_MINB)
+    analyse_finish_kernel(const __grid_constant__ AnalyseParams P, const PairSrc psrc, uint8_t *__restrict__ payloads,
+                          uint8_t *__restrict__ scratch) {
+    const int64_t pair = blockIdx.x;
+    uint8_t *scr = scratch + pair * P.scratch_per_pair;
+    const bool bidir = P.vectors == 3;
+    const int d0 = bidir ? 0 : ((P.vectors & 2) ? 0 : 1);
+    if (((const int *)(scr + P.off_ctl[d0]))[CTL_ABORT] || (bidir && ((const int *)(scr + P.off_ctl[1]))[CTL_ABORT]))
+        return;
+    finish_pair(&P, pair_at(psrc, pair), payloads + pair * P.payload_len, scr);
 }
 
 // Persistent form: a grid sized to the resident CTAs drains the item list in order (the
@@ -2357,7 +2468,7 @@ __global__ void __launch_bounds__(2 * NT, SVPF_MINB)
             for (int i = threadIdx.x; i < (int)(sizeof(AnalyseParams) / 16); i += blockDim.x) dst[i] = src[i];
         }
         __syncthreads();
-        analyse_pair_dev(P, bi.pair, bi.payload, scr, clip_status + bi.clip, cta_abort, nullptr);
+        analyse_pair_dev(P, bi.pair, bi.payload, scr, clip_status + bi.clip, cta_abort, nullptr, false);
         __syncthreads();
         if (!cta_abort) finish_pair(&P, bi.pair, bi.payload, scr);
         __syncthreads();  // P, item_sh and the shared search state are reused by the next item
@@ -2374,6 +2485,8 @@ cudaError_t prepare() {
         cudaError_t e = cudaFuncSetAttribute(analyse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(analyse_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(analyse_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         return e;
     }();
     return once;
@@ -2384,7 +2497,40 @@ cudaError_t launch_plain(const AnalyseParams &P, const PairSrc &psrc, int npairs
     if (npairs <= 0) return cudaSuccess;
     if (cudaError_t e = prepare()) return e;
     const int ndir = P.vectors == 3 ? 2 : 1;
-    analyse_kernel<<<npairs, NT * ndir, sizeof(DirSh) * ndir, stream>>>(P, psrc, payloads, scratch, status_dev);
+    const bool split = SVPF_LOOKAHEAD && NW > 1 && (P.lookahead & 5) == 5;
+    analyse_kernel<<<npairs, NT * ndir, sizeof(DirSh) * ndir, stream>>>(P, psrc, payloads, scratch, status_dev,
+                                                                       split ? 1 : 0);
+    if (launches) *launches += 1;
+    if (!split) return cudaGetLastError();
+    if (cudaError_t e = cudaGetLastError()) return e;
+    // level 0: the CTAs of one launch wait on one another, so each launch takes the pairs whose
+    // CTAs are all resident at once (one launch for up to 296 bidirectional pairs on 148 SMs)
+    static const int resident = [] {
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_level0_kernel, 32, 0) != cudaSuccess)
+            return 0;
+        return sms * per_sm;
+    }();
+    const int64_t group = resident / (ndir * NW);
+    if (group < 1) return cudaErrorCooperativeLaunchTooLarge;
+    for (int64_t f = 0; f < npairs; f += group) {
+        const int64_t n = npairs - f < group ? npairs - f : group;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(n * ndir * NW));
+        cfg.blockDim = dim3(32);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if (cudaError_t e = cudaLaunchKernelEx(&cfg, analyse_level0_kernel, P, psrc, f, scratch, status_dev)) return e;
+        if (launches) *launches += 1;
+    }
+    analyse_finish_kernel<<<npairs, NT * ndir, sizeof(DirSh) * ndir, stream>>>(P, psrc, payloads, scratch);
     if (launches) *launches += 1;
     return cudaGetLastError();
 }

@@ -379,7 +379,7 @@ int svpf_device_status(const void *scratch_dev, void *stream) {
 
 int svpf_analyser_set_lookahead(svpf_analyser *a, int32_t levels) {
     if (!a) return fail(SVPF_EINVAL, "null analyser");
-    if (levels < 0 || levels > 3) return fail(SVPF_EINVAL, "look-ahead levels must be 0..3");
+    if (levels < 0 || levels > 7) return fail(SVPF_EINVAL, "look-ahead mode must be 0..7");
     std::lock_guard<std::mutex> lk(a->mu);
     a->P.lookahead = levels;
     return SVPF_OK;

@@ -34,7 +34,7 @@ bool build_analyse_params(const AnalyseOpts &o, const SuperLayout &Lay, AnalyseP
     P.px_bytes = Lay.px_bytes;
     P.lambda = o.lambda;
     P.tiles_per_lane = 8;
-    P.lookahead = 1;
+    P.lookahead = 5;
     // per level
     int64_t max_cells = 1, max_order = 1;
     for (int lv = 0; lv < o.levels; lv++) {
@@ -161,6 +161,7 @@ bool build_analyse_params(const AnalyseOpts &o, const SuperLayout &Lay, AnalyseP
         P.off_hist[dd] = take(65536 * 4);
         P.off_seen[dd] = take(max_cells);
         P.off_out[dd] = take(max_cells * 2);
+        P.off_ctl[dd] = take(64);
     }
     P.scratch_per_pair = off;
     return true;

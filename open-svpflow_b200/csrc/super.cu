@@ -25,6 +25,9 @@ namespace svpf {
 
 namespace {
 
+// Dynamic shared memory the band kernel may take (a band of one row: 7 rows of the level-0 width).
+constexpr int64_t kBandSmemMax = 200 << 10;
+
 __device__ __forceinline__ unsigned avg8(unsigned a, unsigned b) { return (a + b + 1u) >> 1; }
 
 struct PlaneGeo {
@@ -362,13 +365,21 @@ __device__ __forceinline__ uint32_t h6tap_pair(const uint32_t (&W)[4]) {
     return (s >> 5) & 0x00FF00FFu;  // each lane <= 255: the weights sum to 32
 }
 
-// Output rows [r0, r0 + nr) of level lv + 1 of one plane of one frame, from level lv: the vertical
-// 6-tap into shared memory (the band's rows in two halves; a thread walks down one 16-byte column
-// chunk, keeping in registers the four source rows consecutive output rows share, so it loads two
-// rows per output row; bytes in halfword lanes), then the horizontal 6-tap, 4 output bytes per
-// 32-bit store. Called by the whole CTA.
-__device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restrict__ dst, uint8_t *inter_all, int plane,
-                                            int64_t f, int lv, int r0, int nr) {
+// 16 bytes global -> shared without a register round trip (cp.async); completed by cp_async_wait.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Output rows [r0, r0 + nr) of level lv + 1 of one plane of one frame, from level lv. The source
+// rows the band reads (2 nr + 4 at most) go to shared memory in one burst of 16-byte
+// asynchronous copies (every load of the band in flight at once), then the vertical 6-tap runs
+// over (output row, 16-byte column chunk) pairs into the intermediate rows (bytes in halfword
+// lanes), then the horizontal 6-tap, 4 output bytes per 32-bit store. Called by the whole CTA;
+// `inter` holds nr intermediate rows, `in_sm` the staged source rows.
+__device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restrict__ dst, uint8_t *inter_all,
+                                            uint8_t *in_sm, int plane, int64_t f, int lv, int r0, int nr) {
     const PlaneGeo g = plane_geo(D, plane);
     const bool c = plane > 0;
     const int S = (int)g.stride, SW = S >> 2;
@@ -382,11 +393,21 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
     const int iw = (src_w + 3) >> 2;        // intermediate words per row
     const int iq = (iw + 3) >> 2, ist = 4 * iq;  // 16-byte chunks per row; shared-memory row stride (words)
     if (active) {
-        // the band's rows in two halves, each walked down by its own threads; a thread takes a
-        // 16-byte column chunk (the pitch is a multiple of 16, so the chunk stays inside the row)
-        const uint32_t m = 0x00FF00FFu;
-        const int hr = (nr + 1) >> 1;
         const uint4 z4 = make_uint4(0, 0, 0, 0);
+        // source rows y_lo .. y_hi (the pitch is a multiple of 16, so a chunk stays inside its row;
+        // rows past the buffer read as zeros)
+        const int y_lo = max(2 * r0 - 2, 0), y_hi = min(2 * (r0 + nr - 1) + 3, src_h - 1);
+        const uint4 *col = reinterpret_cast<const uint4 *>(base + (int64_t)srow0 * S);
+        const int SQ = S >> 4;
+        uint4 *in4 = reinterpret_cast<uint4 *>(in_sm);
+        for (int t = threadIdx.x; t < (y_hi - y_lo + 1) * iq; t += blockDim.x) {
+            const int rr = t / iq, cq = t - rr * iq, yy = y_lo + rr;
+            if (srow0 + yy < rows) cp_async16(in4 + t, col + (int64_t)yy * SQ + cq);
+            else in4[t] = z4;
+        }
+        cp_async_wait();
+        __syncthreads();
+        const uint32_t m = 0x00FF00FFu;
         auto vert = [&](uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t a4, uint32_t a5) -> uint32_t {
             const uint32_t e = (a0 & m) + (a5 & m) + 5u * ((a1 & m) + (a4 & m)) + 10u * ((a2 & m) + (a3 & m)) +
                                0x00100010u;
@@ -394,34 +415,21 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
                                 10u * (((a2 >> 8) & m) + ((a3 >> 8) & m)) + 0x00100010u;
             return ((e >> 5) & m) | (((od >> 5) & m) << 8);  // each lane <= 255: weights sum to 32
         };
-        for (int t = threadIdx.x; t < 2 * iq; t += blockDim.x) {
-            const int cq = t % iq, half = t / iq;
-            const int ra = half * hr, rb = min(nr, ra + hr);
-            const uint4 *col = reinterpret_cast<const uint4 *>(base + (int64_t)srow0 * S) + cq;
-            const int SQ = S >> 4;
-            auto row = [&](int yy) -> uint4 { return srow0 + yy < rows ? col[(int64_t)yy * SQ] : z4; };
-            uint4 a0 = z4, a1 = z4, a2 = z4, a3 = z4, a4 = z4, a5 = z4;
-            int have = -1000;  // the window holds source rows have-2 .. have+3
-            for (int r = ra; r < rb; r++) {
-                const int dy = r0 + r, sy = 2 * dy;
-                uint4 v;
-                if (dy == 0 || dy + 1 == dst_h || sy - 2 < 0 || sy + 3 >= src_h) {
-                    const uint4 p = row(min(sy, src_h - 1)), q = row(min(sy + 1, src_h - 1));
-                    v = make_uint4(avgu4(p.x, q.x), avgu4(p.y, q.y), avgu4(p.z, q.z), avgu4(p.w, q.w));
-                } else {
-                    if (have == sy - 2) {
-                        a0 = a2; a1 = a3; a2 = a4; a3 = a5;
-                        a4 = row(sy + 2); a5 = row(sy + 3);
-                    } else {
-                        a0 = row(sy - 2); a1 = row(sy - 1); a2 = row(sy); a3 = row(sy + 1);
-                        a4 = row(sy + 2); a5 = row(sy + 3);
-                    }
-                    have = sy;
-                    v = make_uint4(vert(a0.x, a1.x, a2.x, a3.x, a4.x, a5.x), vert(a0.y, a1.y, a2.y, a3.y, a4.y, a5.y),
-                                   vert(a0.z, a1.z, a2.z, a3.z, a4.z, a5.z), vert(a0.w, a1.w, a2.w, a3.w, a4.w, a5.w));
-                }
-                reinterpret_cast<uint4 *>(inter_all)[(r * ist >> 2) + cq] = v;
+        for (int t = threadIdx.x; t < nr * iq; t += blockDim.x) {
+            const int r = t / iq, cq = t - r * iq;
+            auto row = [&](int yy) -> uint4 { return in4[(yy - y_lo) * iq + cq]; };
+            const int dy = r0 + r, sy = 2 * dy;
+            uint4 v;
+            if (dy == 0 || dy + 1 == dst_h || sy - 2 < 0 || sy + 3 >= src_h) {
+                const uint4 p = row(min(sy, src_h - 1)), q = row(min(sy + 1, src_h - 1));
+                v = make_uint4(avgu4(p.x, q.x), avgu4(p.y, q.y), avgu4(p.z, q.z), avgu4(p.w, q.w));
+            } else {
+                const uint4 a0 = row(sy - 2), a1 = row(sy - 1), a2 = row(sy), a3 = row(sy + 1), a4 = row(sy + 2),
+                            a5 = row(sy + 3);
+                v = make_uint4(vert(a0.x, a1.x, a2.x, a3.x, a4.x, a5.x), vert(a0.y, a1.y, a2.y, a3.y, a4.y, a5.y),
+                               vert(a0.z, a1.z, a2.z, a3.z, a4.z, a5.z), vert(a0.w, a1.w, a2.w, a3.w, a4.w, a5.w));
             }
+            reinterpret_cast<uint4 *>(inter_all)[t] = v;  // row r at r * ist words
         }
     }
     __syncthreads();
@@ -469,8 +477,8 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
 // One pyramid level of every plane of every frame: a grid of resident CTAs strides over bands of
 // `band` output rows (frame, plane, band), each CTA doing a band's vertical then horizontal pass.
 __global__ void __launch_bounds__(256, 4) super_reduce_band_kernel(SuperDev D, uint8_t *__restrict__ dst, int lv, int band,
-                                                                int nb_y, int nb_c, uint32_t nitems) {
-    extern __shared__ __align__(16) uint8_t inter_all[];
+                                                                int nb_y, int nb_c, uint32_t nitems, int inter_bytes) {
+    extern __shared__ __align__(16) uint8_t inter_all[];  // band intermediate rows, then the staged source rows
     const uint32_t per = (uint32_t)(nb_y + 2 * nb_c);
     for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
         const uint32_t e = it % per;
@@ -480,7 +488,7 @@ __global__ void __launch_bounds__(256, 4) super_reduce_band_kernel(SuperDev D, u
         else { plane = 1 + (int)((e - nb_y) / (uint32_t)nb_c); b = (int)((e - nb_y) % (uint32_t)nb_c); }
         const int dst_h = plane ? D.lh[lv + 1] / 2 : D.lh[lv + 1];
         const int r0 = b * band;
-        reduce_band(D, dst, inter_all, plane, f, lv, r0, min(band, dst_h - r0));
+        reduce_band(D, dst, inter_all, inter_all + inter_bytes, plane, f, lv, r0, min(band, dst_h - r0));
     }
 }
 
@@ -488,6 +496,7 @@ __global__ void __launch_bounds__(256, 4) super_reduce_band_kernel(SuperDev D, u
 // no bicubic planes: the fast paths apply.
 bool vec_ok(const SuperDev &D, const void *src, const void *dst, int nframes) {
     auto a16 = [](int64_t v) { return (v & 15) == 0; };
+    if ((int64_t)7 * ((D.width + 15) & ~15) > kBandSmemMax) return false;  // a band of one row must fit
     return D.px_bytes == 1 && D.scale_up != 2 && D.width >= 2 && (((uintptr_t)src | (uintptr_t)dst) & 15) == 0 &&
            a16(D.y_stride) && a16(D.c_stride) && a16(D.y_len) && a16(D.c_len) && a16(D.frame_bytes) &&
            a16(D.src_y_stride) && a16(D.src_c_stride) && a16(D.src_y_len) && a16(D.src_c_len) &&
@@ -538,12 +547,14 @@ int launch_super_vec(const SuperDev &D, const uint8_t *src, uint8_t *dst, int nf
     for (int lv = 0; lv + 1 < D.levels; lv++) {
         const int dh_y = D.lh[lv + 1], dh_c = D.lh[lv + 1] / 2;
         if (dh_y <= 0) continue;
-        const int row_bytes = (D.lw[lv] + 15) & ~15;  // the level's widest intermediate row (luma), 16-byte rows
-        const int band = std::max(1, std::min(16, (32 << 10) / std::max(row_bytes, 1)));
+        const int row_bytes = (D.lw[lv] + 15) & ~15;  // the level's widest row (luma), 16-byte rows
+        // band rows of intermediates + 2 band + 4 staged source rows in about 54 KB: four CTAs per SM
+        const int band = std::max(1, std::min(16, ((54 << 10) / std::max(row_bytes, 1) - 4) / 3));
         const int nb_y = (dh_y + band - 1) / band, nb_c = (dh_c + band - 1) / band;
         const uint32_t nitems = (uint32_t)((int64_t)nframes * (nb_y + 2 * nb_c));
         const int grid = (int)std::min<int64_t>(nitems, (int64_t)sms * 4);
-        super_reduce_band_kernel<<<grid, 256, (size_t)band * row_bytes, stream>>>(D, dst, lv, band, nb_y, nb_c, nitems);
+        const size_t smem = (size_t)(3 * band + 4) * row_bytes;
+        super_reduce_band_kernel<<<grid, 256, smem, stream>>>(D, dst, lv, band, nb_y, nb_c, nitems, band * row_bytes);
         n++;
     }
     return n;
@@ -559,6 +570,9 @@ cudaError_t launch_super(const SuperDev &D, const uint8_t *src, uint8_t *dst, in
         return v;
     }();
     if (vec_ok(D, src, dst, nframes)) {
+        static const cudaError_t attr = cudaFuncSetAttribute(super_reduce_band_kernel,
+                                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBandSmemMax);
+        if (attr != cudaSuccess) return attr;
         const int n = launch_super_vec(D, src, dst, nframes, sms, stream);
         if (launches) *launches += n;
         return cudaGetLastError();

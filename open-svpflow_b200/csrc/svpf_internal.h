@@ -106,8 +106,9 @@ struct alignas(16) AnalyseParams {
     int32_t rescale_denom;
     int32_t tiles_per_lane;   // 4x4 tiles one lane evaluates per candidate (2, 4 or 8): a launch tuning knob
     int32_t px_bytes;         // 1: 8-bit samples; 2: uint16 samples (the 10-bit extension)
-    int32_t lookahead;        // look-ahead (one block per warp in flight, exact either way): bit 0 level 0
-                              // (the default), bit 1 the coarser levels (slower: measured); a tuning knob
+    int32_t lookahead;        // look-ahead (one block per warp in flight, exact either way): bit 0 level 0,
+                              // bit 1 the coarser levels (slower: measured), bit 2 level 0 spread over
+                              // the GPU (its own launch, one CTA per warp); a tuning knob, default 5
     int32_t pad0_, pad1_, pad2_;
     int64_t payload_len;
     int32_t header[16];       // payload words 0x00..0x3C
@@ -115,6 +116,7 @@ struct alignas(16) AnalyseParams {
     int64_t max_cells, max_order;
     int64_t off_field[2], off_next[2], off_proj[2][2], off_order[2], off_order2[2], off_pos[2];
     int64_t off_keys[2], off_hist[2], off_seen[2], off_out[2];
+    int64_t off_ctl[2];       // per direction: the hand-over words of the level-0 kernel (CTL_*)
     int64_t scratch_per_pair;
 };
 

@@ -340,9 +340,10 @@ class Analyser:
         _check(lib().svpf_analyse_pairs_device(self._h, c, r, n, payloads_ptr, scratch_ptr, stream))
 
     def set_lookahead(self, levels):
-        """Look-ahead at level 0 only (True / 1, the default), every level (3), the coarser levels
-        only (2) or off (False / 0); results are identical either way."""
-        _check(lib().svpf_analyser_set_lookahead(self._h, 1 if levels is True else int(levels)))
+        """Look-ahead bits: 1 level 0, 2 the coarser levels, 4 level 0 spread over the GPU in a
+        launch of its own (with 1). True is the default (5), False / 0 off; results are identical
+        either way."""
+        _check(lib().svpf_analyser_set_lookahead(self._h, 5 if levels is True else int(levels)))
 
     @staticmethod
     def lookahead_stats(scratch_ptr: int, stream: int = 0) -> dict:

@@ -1,6 +1,7 @@
 """Level-0 look-ahead (GPU): each warp of a search direction takes its own level-0 block in the
 reference's order, searches it without the neighbour vectors other warps have not committed
-yet, and re-checks the reference's selection with them before it commits in order. The
+yet, and re-checks the reference's selection with them before it commits in order, the warps
+either in the pair's CTA or (mode bit 4) as CTAs of their own spread over the SMs. The
 payloads must equal the oracle's and those of the same launch without look-ahead, byte for
 byte, for every launch shape (one to four warps per direction); the counters show that seeds
 were deferred and re-checked. Tolerance: zero (integer work)."""
@@ -65,12 +66,12 @@ def test_lookahead_is_exact(case):
     ao = orc.analyse_opts(orc.sdata(so), aopt, None, w, h)
     want = orc.analyse_clip(ao, so, orc.build_super_many(so, clip, os.cpu_count() or 1), 0, n, os.cpu_count() or 1)
     off, st_off = _run(an, sb, clip, 0)
-    for levels in (1, 2):  # level 0 only, the coarser levels only
+    for levels in (1, 2, 5, 6):  # level 0 in the pair's CTA; the coarser levels; level 0 spread (+ coarser)
         got, _ = _run(an, sb, clip, levels)
         for i in range(n):
             assert got[i].tobytes() == want[i].tobytes(), (f"look-ahead {levels}, output frame {i}: " +
                                                            first_difference(got[i], want[i]))
-    on, st = _run(an, sb, clip, 3)
+    on, st = _run(an, sb, clip, 7)
     for i in range(n):
         assert on[i].tobytes() == want[i].tobytes(), f"look-ahead, output frame {i}: " + first_difference(on[i], want[i])
         assert off[i].tobytes() == want[i].tobytes(), f"serial, output frame {i}: " + first_difference(off[i], want[i])
@@ -109,3 +110,38 @@ def test_lookahead_every_launch_shape_matches_the_oracle():
                 assert np.array_equal(g, w_), f"shape {sv.Batch.variants()[v]}: clip {i} differs from the oracle"
     finally:
         b.close()
+
+
+def test_spread_level0_in_several_launches():
+    """More pairs than one cooperative level-0 launch holds (296 bidirectional pairs on 148
+    SMs): the pairs go in groups, each group's warps in a launch of their own. The 10-bit build
+    takes the look-ahead shape at any pair count, so a 700-pair clip runs three groups."""
+    import torch
+
+    import svpflow_b200 as sv
+    from test_px16 import clip10
+
+    w, h, sopt, aopt, _ = CASES[5]
+    n = 700
+    clip = clip10(w, h, n, seed=777, motion=3, objects=2, object_motion=6)
+    sb = sv.Super(w, h, sopt, bits=10)
+    an = sv.Analyse(sb.sdata, aopt, w, h, bits=10)
+    so = orc.super_opts(w, h, sopt)
+    ao = orc.analyse_opts(orc.sdata(so), aopt, None, w, h)
+    want = orc.analyse_clip16(ao, so, orc.build_super_many16(so, clip), 0, n)
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    frames = torch.from_numpy(clip.view(np.uint8).copy()).to(dev)
+    supers = torch.empty((n, sb.output_len()), dtype=torch.uint8, device=dev)
+    pay = torch.empty((n, an.payload_len()), dtype=torch.uint8, device=dev)
+    scr = torch.empty(an.scratch_bytes(n), dtype=torch.uint8, device=dev)
+    sb.build_device(frames.data_ptr(), supers.data_ptr(), n, st)
+    an.set_lookahead(5)
+    an.analyse_clip_device(supers.data_ptr(), n, 0, n, pay.data_ptr(), scr.data_ptr(), st)
+    sv.Analyser.device_status(scr.data_ptr(), st)
+    stats = sv.Analyser.lookahead_stats(scr.data_ptr(), st)
+    got = pay.cpu().numpy()
+    for i in range(n):
+        assert got[i].tobytes() == want[i].tobytes(), f"output frame {i}: " + first_difference(got[i], want[i])
+    vd = an.vector_header()
+    assert stats["blocks"] == n * 2 * vd[11] * vd[12]
