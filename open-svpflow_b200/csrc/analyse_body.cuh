@@ -2401,14 +2401,18 @@ __global__ void __launch_bounds__(2 * NT, SVPF_MINB)
 // the same number of walking warps whatever the pair count (one CTA per pair leaves some SMs
 // with two pairs and others with one). The warps of a direction wait on one another, so the
 // launch is cooperative: all its CTAs are resident at once, or it does not start.
-constexpr int kLevel0Blocks = 16;  // CTAs per SM: 128 registers per thread
-__global__ void __launch_bounds__(32, kLevel0Blocks)
+constexpr int kLevel0Warps = 1;    // warps per CTA (of one direction)
+constexpr int kLevel0PerSM = 16;   // warps per SM: 128 registers per thread
+__global__ void __launch_bounds__(32 * kLevel0Warps, kLevel0PerSM / kLevel0Warps)
     analyse_level0_kernel(const __grid_constant__ AnalyseParams P, const PairSrc psrc, int64_t first,
                           uint8_t *__restrict__ scratch, int *status) {
-    __shared__ WarpSh s;
+    __shared__ WarpSh sh[kLevel0Warps];
+    constexpr int per_dir = NW / kLevel0Warps;  // CTAs per direction
     const int ndir = P.vectors == 3 ? 2 : 1;
-    const int64_t pair = first + blockIdx.x / (ndir * NW);
-    const int rem = (int)(blockIdx.x % (ndir * NW)), half = rem / NW, g = rem % NW;
+    const int64_t pair = first + blockIdx.x / (ndir * per_dir);
+    const int rem = (int)(blockIdx.x % (ndir * per_dir)), half = rem / per_dir;
+    const int w = (int)(threadIdx.x >> 5), g = (rem % per_dir) * kLevel0Warps + w;
+    WarpSh &s = sh[w];
     const int d = ndir == 2 ? half : ((P.vectors & 2) ? 0 : 1);
     uint8_t *scr = scratch + pair * P.scratch_per_pair;
     int *ctl = (int *)(scr + P.off_ctl[d]);
@@ -2420,7 +2424,7 @@ __global__ void __launch_bounds__(32, kLevel0Blocks)
     Ctx x;
     x.P = &P;
     x.d = 0;
-    x.tid = threadIdx.x;
+    x.tid = (int)(threadIdx.x & 31);
     x.nw = 1;
     x.wbase = 0;
     x.S = Planes{src, src + P.y_len, src + P.y_len + P.c_len};
@@ -2509,17 +2513,20 @@ cudaError_t launch_plain(const AnalyseParams &P, const PairSrc &psrc, int npairs
         int dev = 0, sms = 0, per_sm = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_level0_kernel, 32, 0) != cudaSuccess)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_level0_kernel, 32 * kLevel0Warps, 0) !=
+                cudaSuccess)
             return 0;
-        return sms * per_sm;
+        return sms * per_sm * kLevel0Warps;  // warps
     }();
-    const int64_t group = resident / (ndir * NW);
-    if (group < 1) return cudaErrorCooperativeLaunchTooLarge;
+    const int64_t most = resident / (ndir * NW);
+    if (most < 1) return cudaErrorCooperativeLaunchTooLarge;
+    const int64_t launches_needed = (npairs + most - 1) / most;
+    const int64_t group = (npairs + launches_needed - 1) / launches_needed;  // even groups
     for (int64_t f = 0; f < npairs; f += group) {
         const int64_t n = npairs - f < group ? npairs - f : group;
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(n * ndir * NW));
-        cfg.blockDim = dim3(32);
+        cfg.gridDim = dim3((unsigned)(n * ndir * NW / kLevel0Warps));
+        cfg.blockDim = dim3(32 * kLevel0Warps);
         cfg.dynamicSmemBytes = 0;
         cfg.stream = stream;
         cudaLaunchAttribute attr[1];

@@ -365,6 +365,16 @@ __device__ __forceinline__ uint32_t h6tap_pair(const uint32_t (&W)[4]) {
     return (s >> 5) & 0x00FF00FFu;  // each lane <= 255: the weights sum to 32
 }
 
+// n / d for 0 <= n, 1 <= d with n * d < 2^32 by one high multiply: with m = ceil(2^32 / d) the
+// error n (m d - 2^32) / 2^32 < 1 never carries past the next multiple of d (the band kernel's
+// loop indices: n < 16 rows x 8192 words, d <= 8192).
+struct FastDiv {
+    uint32_t m;
+    int d;
+    __device__ __forceinline__ explicit FastDiv(int d_) : m(d_ > 1 ? 0xFFFFFFFFu / (uint32_t)d_ + 1u : 0u), d(d_) {}
+    __device__ __forceinline__ int div(int n) const { return d > 1 ? (int)__umulhi((uint32_t)n, m) : n; }
+};
+
 // 16 bytes global -> shared without a register round trip (cp.async); completed by cp_async_wait.
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
@@ -400,8 +410,9 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
         const uint4 *col = reinterpret_cast<const uint4 *>(base + (int64_t)srow0 * S);
         const int SQ = S >> 4;
         uint4 *in4 = reinterpret_cast<uint4 *>(in_sm);
+        const FastDiv div_iq(iq);
         for (int t = threadIdx.x; t < (y_hi - y_lo + 1) * iq; t += blockDim.x) {
-            const int rr = t / iq, cq = t - rr * iq, yy = y_lo + rr;
+            const int rr = div_iq.div(t), cq = t - rr * iq, yy = y_lo + rr;
             if (srow0 + yy < rows) cp_async16(in4 + t, col + (int64_t)yy * SQ + cq);
             else in4[t] = z4;
         }
@@ -416,7 +427,7 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
             return ((e >> 5) & m) | (((od >> 5) & m) << 8);  // each lane <= 255: weights sum to 32
         };
         for (int t = threadIdx.x; t < nr * iq; t += blockDim.x) {
-            const int r = t / iq, cq = t - r * iq;
+            const int r = div_iq.div(t), cq = t - r * iq;
             auto row = [&](int yy) -> uint4 { return in4[(yy - y_lo) * iq + cq]; };
             const int dy = r0 + r, sy = 2 * dy;
             uint4 v;
@@ -433,16 +444,21 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
         }
     }
     __syncthreads();
+    const FastDiv div_sw(SW);
     for (int t = threadIdx.x; t < nr * SW; t += blockDim.x) {
-        const int r = t / SW, xw = t - r * SW;
+        const int r = div_sw.div(t), xw = t - r * SW;
         const int dy = r0 + r;
         uint32_t word = 0;
-        if (active && xw >= 1 && 4 * xw + 5 <= dst_w && 8 * xw + 9 < src_w) {
+        if (!active || 4 * xw >= src_w) {
+            // past the row's src_w bytes: zeros
+        } else if (4 * xw >= dst_w && 4 * xw + 4 <= src_w) {
+            word = reinterpret_cast<const uint32_t *>(inter_all)[r * ist + xw];  // vertical-only intermediates
+        } else if (xw >= 1 && 4 * xw + 5 <= dst_w && 8 * xw + 9 < src_w) {
             // four interior outputs: source bytes 8xw-2 .. 8xw+9 of the row, in halfword lanes
             const uint32_t *in32 = reinterpret_cast<const uint32_t *>(inter_all) + r * ist + 2 * xw - 1;
             const uint32_t W[4] = {in32[0], in32[1], in32[2], in32[3]};
             word = __byte_perm(h6tap_pair<0>(W), h6tap_pair<1>(W), 0x6420);
-        } else if (active) {
+        } else {
             const uint8_t *in = inter_all + r * ist * 4;
             auto get = [&](int i, unsigned dflt) -> unsigned { return i < src_w ? in[i] : dflt; };
 #pragma unroll

@@ -19,9 +19,9 @@ const AnalyseVariant &analyse_variant(int i) {
     return kVariants[(i >= 0 && i < analyse_variant_count()) ? i : 0];
 }
 
-// More pairs than two per SM: the 80-register shape keeps three pairs per SM resident (the
-// fastest for full launches); otherwise the 128-register shape, which is faster per pair.
-// uint16 samples have one compiled shape.
+// The 128-register shape, whose level 0 spreads over the GPU by default; with that off, more
+// pairs than two per SM take the 80-register shape (three pairs per SM resident). uint16
+// samples have one compiled shape.
 cudaError_t launch_analyse(const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,
                            uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches) {
     if (P.px_bytes == 2) return nt128p16::launch_plain(P, src, npairs, payloads, scratch, status_dev, stream, launches);
@@ -31,7 +31,9 @@ cudaError_t launch_analyse(const AnalyseParams &P, const PairSrc &src, int npair
             return 0;
         return n;
     }();
-    if (sms > 0 && npairs > 2 * sms)
+    // more pairs than two per SM: the 3-CTA shape, unless level 0 is spread over the GPU, which
+    // balances the SMs at any pair count (900 pairs at 960x540: 581.9 -> 754.1 pairs/s)
+    if (sms > 0 && npairs > 2 * sms && (P.lookahead & 5) != 5)
         return nt128b3::launch_plain(P, src, npairs, payloads, scratch, status_dev, stream, launches);
     return nt128::launch_plain(P, src, npairs, payloads, scratch, status_dev, stream, launches);
 }
