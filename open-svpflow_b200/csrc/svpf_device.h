@@ -91,6 +91,9 @@ cudaError_t launch_analyse(const AnalyseParams &P, const PairSrc &src, int npair
 // The same with a given launch shape (analyse_variant index).
 cudaError_t launch_analyse_shape(int variant, const AnalyseParams &P, const PairSrc &src, int npairs, uint8_t *payloads,
                                  uint8_t *scratch, int *status_dev, cudaStream_t stream, int *launches);
-constexpr int kShapeShared = 3;  // nt128_b3: the shape for launches that share SMs with others
+// The shape of the server's chunk launches, which share the GPU with other clips' chunks: nt128,
+// whose level 0 spreads over the SMs (measured at 5 clips/s against nt128_b3: 83.0 against 60.4
+// pairs/s, p50 7.9 against 13.1 s, p99 25.7 against 36.5 s).
+constexpr int kShapeShared = 0;
 
 }  // namespace svpf
