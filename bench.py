@@ -80,12 +80,14 @@ RENDER_REPLAYS = 48
 INT32_LANES_PER_SM = 128
 # integer ops per frame pair (oracle counts of the workloads' compares), when the CPU leg is skipped
 OPS_PER_PAIR = {"1080p": 19.38e9}
-# why the Analyse kernel reaches the fraction it does, from the ncu capture in
-# profiles/analyse_kernel_1080p_17f.md: issue-active x (algorithmic ops / executed lane slots)
-ROOF_DECOMPOSITION = {"issue_active": 0.375, "useful_lane_fraction": 0.24,
-                      "source": "ncu capture of a 17-pair 1080p launch (1 CTA per SM, the nt128 shape with the "
-                                "level-0 look-ahead): 2.53 G warp instructions = 80.8 G lane slots per pair for "
-                                "19.4 G algorithmic ops (profiles/analyse_kernel_1080p_17f.md)"}
+# why the Analyse launch reaches the fraction it does, from the ncu counters of the 240-pair launch
+# in profiles/analyse_1080p_240_counters.md: issue utilisation (warp instructions / (4 schedulers x
+# SMs x the launch's SM cycles)) x useful lane fraction (algorithmic ops / executed lane slots)
+ROOF_DECOMPOSITION = {"issue_active": 0.332, "useful_lane_fraction": 0.312,
+                      "source": "ncu counters of the 240-pair 1080p launch (analyse_kernel 142.1 G + "
+                                "analyse_level0_kernel 323.2 G + analyse_finish_kernel 0.03 G warp instructions "
+                                "in 1204.5 ms): 1.94 G warp instructions = 62.1 G lane slots per pair for 19.4 G "
+                                "algorithmic ops (profiles/analyse_1080p_240_counters.md)"}
 # the CPU legs time this many frame pairs per host thread, so that their figure is a throughput
 # (dynamic scheduling over many pairs) rather than the latency of the slowest pair
 CPU_PAIRS_PER_THREAD = 4
