@@ -66,9 +66,11 @@ DESC = {
                "hex2 r2, luma SAD + chroma, fwd+bwd)",
 }
 UNIT = "frame-pairs/s"
-# DRAM bytes per frame pair of the Analyse kernel at 1080p (ncu capture of a 17-pair launch:
-# 290.6 MB read + 49.3 MB written)
-TRAFFIC_PER_PAIR = 339.9e6 / 17
+# DRAM bytes per frame pair of the Analyse launch at 1080p: ncu's dram__bytes_read.sum +
+# dram__bytes_write.sum of the three kernels of the 240-pair launch (one-pass counters):
+# analyse_kernel 5.57 + 0.74 GB, analyse_level0_kernel 15.51 + 0.40 GB, analyse_finish_kernel
+# 0.14 + 0.08 GB (profiles/analyse_1080p_240_counters.md)
+TRAFFIC_PER_PAIR = 22.44e9 / 240
 # DRAM bytes of one 1080p render launch with the 8 x 8 effective block (ncu capture: 4.13 MB read,
 # the written frame stays in L2)
 RENDER_TRAFFIC_PER_FRAME = 4.14e6
@@ -1325,7 +1327,8 @@ def main():
             "frac": ops_pair * a_count / (a_ms / 1000) / int_peak if ops_pair else None,
             "traffic": TRAFFIC_PER_PAIR * a_count if WORKLOAD == "1080p" and not args.size else None,
             "traffic_unit": "bytes per launch",
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 17-pair launch, per pair x pairs",
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the three kernels of the "
+                               "240-pair launch, per pair x pairs"),
             "ops_per_pair": ops_pair, "ops_source": ops_src, "avg_launch_ms": a_ms,
             "peak_source": f"nominal: {_sm_count()} SMs x {INT32_LANES_PER_SM} int32 lanes (64 on the ALU pipe + 64 "
                            f"IMAD on the FMA-heavy pipe) x {SM_MAX_MHZ:.0f} MHz; no measured integer peak exists",

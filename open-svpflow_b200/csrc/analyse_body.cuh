@@ -69,6 +69,7 @@ constexpr unsigned DC_SHIFT = 0;
 constexpr int NT = SVPF_NT;        // threads per search direction
 static_assert(NT == 32 || NT == 64 || NT == 128, "threads per direction");
 constexpr int NW = NT / 32;
+static_assert(NW <= 4, "the look-ahead keeps at most NW - 1 = 3 deferred seeds per block");
 constexpr int NGMAX = NW * 32;     // candidate groups of a direction when a group is one lane
 constexpr int MAXSLOT = 16;        // special-candidate slots of a block
 constexpr int MW = 4;              // validity mask words per chunk of a search step: 128 candidates
@@ -123,6 +124,10 @@ struct DirShT {
     // satd_rows_h) or 16-bit pairs (x = pixels 0,1; y = pixels 2,3), a SAD plane the packed word in x.
     uint2 srcp[kSrc][384];
     int2 clist[W][32 * MW];  // per warp: the step's candidates passing the cuts, in order (mv, index)
+    int2 seedv[W][8];        // look-ahead, per group: the block's seeds evaluated at once (vector) ...
+    int seedq[W][8];         // ... and their places among the block's processed neighbours;
+    long long defc[W][3];    // the deferred seeds' cells (at most NW - 1 = 3) ...
+    int defq[W][3];          // ... and places
     long long r64[W][3];
     int r32[W][2];
 };
@@ -1593,9 +1598,11 @@ __device__ __forceinline__ void spec_walk(const Ctx &x, SH &s, DirScratch &ds, c
             }
         }
         const int zslot = n++, gslot = n++, nslot0 = n;
-        int sdx[8], sdy[8], sq[8];        // seeds evaluated now: vector, place among the block's seeds
-        int dq0 = 0, dq1 = 0, dq2 = 0;    // deferred seeds: place among the block's seeds ...
-        int64_t dc0 = 0, dc1 = 0, dc2 = 0;  // ... and cell
+        // seeds evaluated now and deferred seeds, in shared memory (written by lane 0; the values are
+        // the same in every lane)
+        int2 *sv = s.seedv[x.wbase];
+        int *sq = s.seedq[x.wbase], *dq = s.defq[x.wbase];
+        long long *dcell = s.defc[x.wbase];
         int nseeds = 0, nall = 0, ndef = 0;
 #pragma unroll 1
         for (int q = 0; q < 9; q++) {
@@ -1605,19 +1612,16 @@ __device__ __forceinline__ void spec_walk(const Ctx &x, SH &s, DirScratch &ds, c
             if (p >= k) continue;
             const int64_t ci = (int64_t)ny * gw + nx;
             if (!waited && p > k - D) {  // searched by another warp, maybe not yet committed
-                if (ndef == 0) { dq0 = nall; dc0 = ci; }
-                else if (ndef == 1) { dq1 = nall; dc1 = ci; }
-                else { dq2 = nall; dc2 = ci; }
+                if (lane == 0) { dq[ndef] = nall; dcell[ndef] = ci; }
                 ndef++;
             } else {
                 const int2 nm = vmv(ld_cell<XSM>(field + ci));
-#pragma unroll
-                for (int t = 0; t < 8; t++)
-                    if (t == nseeds) { sdx[t] = nm.x; sdy[t] = nm.y; sq[t] = nall; }
+                if (lane == 0) { sv[nseeds] = nm; sq[nseeds] = nall; }
                 nseeds++;
             }
             nall++;  // at most 8: levels with more processed neighbours take search_level
         }
+        __syncwarp();
         n += nseeds;
         const int dcslot = n++;
         {
@@ -1634,11 +1638,7 @@ __device__ __forceinline__ void spec_walk(const Ctx &x, SH &s, DirScratch &ds, c
                 else if (j == zslot) { mx = 0; my = 0; }
                 else if (j == gslot) { mx = gxv; my = gyv; }
                 else if (j == dcslot) { kind = 2; ch = false; }
-                else if (j >= nslot0 && j < nslot0 + nseeds) {
-#pragma unroll
-                    for (int t = 0; t < 8; t++)
-                        if (t == j - nslot0) { mx = sdx[t]; my = sdy[t]; }
-                }
+                else if (j >= nslot0 && j < nslot0 + nseeds) { mx = sv[j - nslot0].x; my = sv[j - nslot0].y; }
                 Res r{0, 0, 0, 0, 0, 0};
                 if (act) r = eval_lane(x, b, kind, sxi * P.step_x, syi * P.step_y, mx, my, ch, sub, G);
                 group_sum3(r, G);
@@ -1684,12 +1684,11 @@ __device__ __forceinline__ void spec_walk(const Ctx &x, SH &s, DirScratch &ds, c
                 const long long cst = (long long)sd + (((long long)P.pzero * sd) >> 8);
                 if (cst < bcost) { bmx = 0; bmy = 0; bsad = sd; bcost = cst; bpos = 3; }
             }
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                if (q >= nseeds) break;
+#pragma unroll 1
+            for (int q = 0; q < nseeds; q++) {
                 const unsigned sd = slotL[phs][nslot0 + q];
                 const long long cst = (long long)sd + (((long long)P.pnbour * sd) >> 8);
-                if (cst < bcost) { bmx = sdx[q]; bmy = sdy[q]; bsad = sd; bcost = cst; bpos = 4 + sq[q]; }
+                if (cst < bcost) { bmx = sv[q].x; bmy = sv[q].y; bsad = sd; bcost = cst; bpos = 4 + sq[q]; }
             }
             lambda = adapt_lambda(L.lambda_base, L.lsad, pred_score);
             radius = L.base_radius;
@@ -1724,10 +1723,9 @@ __device__ __forceinline__ void spec_walk(const Ctx &x, SH &s, DirScratch &ds, c
                     unsigned csad = 0;
                     bool dwin = false;
 #pragma unroll 1
-                    for (int j = 0; j < 3; j++) {
-                        if (j >= ndef) break;
-                        const int64_t ci = j == 0 ? dc0 : (j == 1 ? dc1 : dc2);
-                        const int pos = 4 + (j == 0 ? dq0 : (j == 1 ? dq1 : dq2));
+                    for (int j = 0; j < ndef; j++) {
+                        const int64_t ci = dcell[j];
+                        const int pos = 4 + dq[j];
                         const int2 m = vmv(ld_cell<XSM>(field + ci));
                         // its exact_sad: from an evaluated candidate with the same vector (same block,
                         // same reads), else evaluated now
@@ -1739,9 +1737,8 @@ __device__ __forceinline__ void spec_walk(const Ctx &x, SH &s, DirScratch &ds, c
                         else if (m.x == gxv && m.y == gyv) sd = slotL[phs][gslot];
                         else {
                             have = false;
-#pragma unroll
-                            for (int t = 0; t < 8; t++)
-                                if (!have && t < nseeds && sdx[t] == m.x && sdy[t] == m.y) {
+                            for (int t = 0; t < nseeds && !have; t++)
+                                if (sv[t].x == m.x && sv[t].y == m.y) {
                                     sd = slotL[phs][nslot0 + t];
                                     have = true;
                                 }
