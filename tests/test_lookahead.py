@@ -145,3 +145,42 @@ def test_spread_level0_in_several_launches():
         assert got[i].tobytes() == want[i].tobytes(), f"output frame {i}: " + first_difference(got[i], want[i])
     vd = an.vector_header()
     assert stats["blocks"] == n * 2 * vd[11] * vd[12]
+
+
+def test_spread_level0_in_a_cuda_graph():
+    """The three launches of a spread Analyse (pair kernel, cooperative level-0 kernel, finish
+    kernel) captured into a CUDA graph and replayed give the payloads of a direct call."""
+    import torch
+
+    import svpflow_b200 as sv
+    from svpflow_b200.synth import make_clip
+
+    w, h, sopt, aopt, n = CASES[0]
+    clip = make_clip(w, h, n, seed=901, motion=6, objects=3, object_motion=12)
+    sb = sv.Super(w, h, sopt)
+    an = sv.Analyse(sb.sdata, aopt, w, h)
+    an.set_lookahead(5)
+    dev = torch.device("cuda", 0)
+    frames = torch.from_numpy(clip).to(dev)
+    supers = torch.empty((n, sb.output_len()), dtype=torch.uint8, device=dev)
+    direct = torch.empty((n, an.payload_len()), dtype=torch.uint8, device=dev)
+    replayed = torch.zeros_like(direct)
+    scr = torch.empty(an.scratch_bytes(n), dtype=torch.uint8, device=dev)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    sb.build_device(frames.data_ptr(), supers.data_ptr(), n, st)
+    an.analyse_clip_device(supers.data_ptr(), n, 0, n, direct.data_ptr(), scr.data_ptr(), st)
+    sv.Analyser.device_status(scr.data_ptr(), st)
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(g, stream=side):
+            an.analyse_clip_device(supers.data_ptr(), n, 0, n, replayed.data_ptr(), scr.data_ptr(),
+                                   side.cuda_stream)
+    torch.cuda.current_stream(dev).wait_stream(side)
+    for _ in range(2):
+        g.replay()
+    torch.cuda.synchronize()
+    sv.Analyser.device_status(scr.data_ptr(), st)
+    assert torch.equal(direct, replayed)
+    del g
