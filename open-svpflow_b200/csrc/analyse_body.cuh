@@ -2177,7 +2177,8 @@ __device__ __forceinline__ void analyse_pair_dev(const AnalyseParams &P, const P
     int pgw = 0, pgh = 0;  // grid of the previous (coarser) level
     for (int level = P.nlevels - 1; level >= 0; level--) {
         const LevelInfo &L = P.lv[level];
-        set_level(x, P, level);
+        // the coarser levels of a split launch: twice the tiles per lane (217.0 against 215.2 pairs/s)
+        set_level(x, P, level, split && level > 0 ? 2 : 1);
         const int gw = L.gw, gh = L.gh;
         const int64_t ncell = (int64_t)gw * gh;
         const bool first = level == P.nlevels - 1;
