@@ -4,8 +4,10 @@
 // analyse_nt32.cu, analyse_nt128b3.cu, analyse_nt64b6.cu): SVPF_NT = threads per search
 // direction, SVPF_MINB = resident CTAs per SM the register budget is cut for (2, 4, 8: 128
 // registers per thread; 3, 6: 80), SVPF_VARIANT = the variant's namespace. Each variant
-// exports a plain launcher (one CTA per pair) and a persistent batch launcher (CTAs
-// drain a device work queue of frame pairs from many clips).
+// exports a plain launcher (one CTA per pair; in the look-ahead shapes, by default, the pair
+// kernel runs the coarser levels, a cooperative level-0 kernel with one CTA per warp walks
+// level 0 across the SMs and a finish kernel packs the payloads) and a persistent batch
+// launcher (CTAs drain a device work queue of frame pairs from many clips).
 //
 // Restates crates/svpflow1/src/analyse_search.rs:68-2811 for the GPU:
 //   * one CTA per frame pair; its two halves (NT threads each) run the forward search
@@ -31,8 +33,9 @@
 //     read path (edge-shifted, clamped, masked; :1638-2351) through cand_setup, which
 //     keeps the reference's wrapping index arithmetic.
 //
-// Integer/indexing work: no tensor cores, no reduced precision. The two f64 formulas
-// (adapt_lambda, exact_lambda) are IEEE-exact (exact_lambda is host-precomputed).
+// Integer/indexing work: no tensor cores. 8-bit SATD runs in f16x2 on values that halves hold
+// exactly (see satd_rows_h); the two f64 formulas (adapt_lambda, exact_lambda) are IEEE-exact
+// (exact_lambda is host-precomputed).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
