@@ -162,3 +162,19 @@ def test_header_is_plain_c_and_cxx(lang, std):
     assert r.returncode == 0, r.stderr
     src = open(header).read()
     assert "torch" not in src and "cuda_runtime" not in src and "at::" not in src
+
+
+def test_lookahead_mode_bits():
+    """svpf_analyser_set_lookahead takes the bit set 0..7 (1 level 0, 2 the coarser levels, 4
+    level 0 spread over the GPU) and rejects anything else; setting it needs no GPU."""
+    import svpflow_b200 as sv
+
+    sb = sv.Super(64, 48, "{pel:2}")
+    an = sv.Analyse(sb.sdata, "{}", 64, 48)
+    for mode in range(8):
+        an.set_lookahead(mode)
+    an.set_lookahead(True)
+    an.set_lookahead(False)
+    for bad in (-1, 8):
+        with pytest.raises(ValueError, match="look-ahead mode must be 0..7"):
+            an.set_lookahead(bad)
