@@ -68,9 +68,9 @@ DESC = {
 UNIT = "frame-pairs/s"
 # DRAM bytes per frame pair of the Analyse launch at 1080p: ncu's dram__bytes_read.sum +
 # dram__bytes_write.sum of the three kernels of the 240-pair launch (one-pass counters):
-# analyse_kernel 5.57 + 0.74 GB, analyse_level0_kernel 15.51 + 0.40 GB, analyse_finish_kernel
+# analyse_kernel 5.55 + 0.77 GB, analyse_level0_kernel 16.17 + 0.40 GB, analyse_finish_kernel
 # 0.14 + 0.08 GB (profiles/analyse_1080p_240_counters.md)
-TRAFFIC_PER_PAIR = 22.44e9 / 240
+TRAFFIC_PER_PAIR = 23.11e9 / 240
 # DRAM bytes of one 1080p render launch with the 8 x 8 effective block (ncu capture: 4.13 MB read,
 # the written frame stays in L2)
 RENDER_TRAFFIC_PER_FRAME = 4.14e6
@@ -85,10 +85,10 @@ OPS_PER_PAIR = {"1080p": 19.38e9}
 # why the Analyse launch reaches the fraction it does, from the ncu counters of the 240-pair launch
 # in profiles/analyse_1080p_240_counters.md: issue utilisation (warp instructions / (4 schedulers x
 # SMs x the launch's SM cycles)) x useful lane fraction (algorithmic ops / executed lane slots)
-ROOF_DECOMPOSITION = {"issue_active": 0.332, "useful_lane_fraction": 0.312,
-                      "source": "ncu counters of the 240-pair 1080p launch (analyse_kernel 142.1 G + "
-                                "analyse_level0_kernel 323.2 G + analyse_finish_kernel 0.03 G warp instructions "
-                                "in 1204.5 ms): 1.94 G warp instructions = 62.1 G lane slots per pair for 19.4 G "
+ROOF_DECOMPOSITION = {"issue_active": 0.341, "useful_lane_fraction": 0.332,
+                      "source": "ncu counters of the 240-pair 1080p launch (analyse_kernel 142.9 G + "
+                                "analyse_level0_kernel 295.0 G + analyse_finish_kernel 0.03 G warp instructions "
+                                "in 1105.5 ms): 1.82 G warp instructions = 58.4 G lane slots per pair for 19.4 G "
                                 "algorithmic ops (profiles/analyse_1080p_240_counters.md)"}
 # the CPU legs time this many frame pairs per host thread, so that their figure is a throughput
 # (dynamic scheduling over many pairs) rather than the latency of the slowest pair
