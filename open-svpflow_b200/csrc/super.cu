@@ -388,8 +388,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_al
 // over (output row, 16-byte column chunk) pairs into the intermediate rows (bytes in halfword
 // lanes), then the horizontal 6-tap, 4 output bytes per 32-bit store. Called by the whole CTA;
 // `inter` holds nr intermediate rows, `in_sm` the staged source rows.
+// lv0_src (level 0 only, nullable): read level 0's full-pel rows from the source frames instead of the
+// super frames (the same bytes below the level's width; the rest is never used).
 __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restrict__ dst, uint8_t *inter_all,
-                                            uint8_t *in_sm, int plane, int64_t f, int lv, int r0, int nr) {
+                                            uint8_t *in_sm, int plane, int64_t f, int lv, int r0, int nr,
+                                            const uint8_t *__restrict__ lv0_src = nullptr) {
     const PlaneGeo g = plane_geo(D, plane);
     const bool c = plane > 0;
     const int S = (int)g.stride, SW = S >> 2;
@@ -407,13 +410,15 @@ __device__ __forceinline__ void reduce_band(const SuperDev &D, uint8_t *__restri
         // source rows y_lo .. y_hi (the pitch is a multiple of 16, so a chunk stays inside its row;
         // rows past the buffer read as zeros)
         const int y_lo = max(2 * r0 - 2, 0), y_hi = min(2 * (r0 + nr - 1) + 3, src_h - 1);
-        const uint4 *col = reinterpret_cast<const uint4 *>(base + (int64_t)srow0 * S);
-        const int SQ = S >> 4;
+        const uint4 *col = reinterpret_cast<const uint4 *>(
+            lv0_src ? lv0_src + f * D.src_frame_bytes + g.src_off : base + (int64_t)srow0 * S);
+        const int SQ = (int)((lv0_src ? g.src_stride : (int64_t)S) >> 4);
+        const int have = lv0_src ? src_h : rows - srow0;  // source frames hold every level-0 row
         uint4 *in4 = reinterpret_cast<uint4 *>(in_sm);
         const FastDiv div_iq(iq);
         for (int t = threadIdx.x; t < (y_hi - y_lo + 1) * iq; t += blockDim.x) {
             const int rr = div_iq.div(t), cq = t - rr * iq, yy = y_lo + rr;
-            if (srow0 + yy < rows) cp_async16(in4 + t, col + (int64_t)yy * SQ + cq);
+            if (yy < have) cp_async16(in4 + t, col + (int64_t)yy * SQ + cq);
             else in4[t] = z4;
         }
         cp_async_wait();
@@ -508,6 +513,47 @@ __global__ void __launch_bounds__(256, 4) super_reduce_band_kernel(SuperDev D, u
     }
 }
 
+// Level 0 and the level 0 -> 1 reduction in one launch. One CTA in kL01Split streams the level-0
+// chunks of every plane, as super_level0_vec_kernel does: that work is bound by memory. The others
+// reduce level-1 bands: that work is bound by instruction issue. They read level 0's full-pel rows from the
+// source frames, so they need nothing the streaming CTAs write, and the two kinds of work share every
+// SM instead of running one after the other.
+constexpr uint32_t kL01Split = 2;  // measured: 1 in 2 CTAs streaming 1.34 ms, 1 in 4 2.47 ms
+__global__ void __launch_bounds__(256, 4) super_level01_kernel(SuperDev D, const uint8_t *__restrict__ src,
+                                                            uint8_t *__restrict__ dst, int chunks_y, int chunks_c,
+                                                            uint32_t items_y, uint32_t items_c, int band, int nb_y,
+                                                            int nb_c, uint32_t nbands, int inter_bytes) {
+    extern __shared__ __align__(16) uint8_t inter_all[];
+    // one CTA in kL01Split streams level 0, the others reduce bands (grid: a multiple of kL01Split)
+    const uint32_t groups = gridDim.x / kL01Split, grp = blockIdx.x / kL01Split, role = blockIdx.x % kL01Split;
+    if (role == 0) {
+        const uint32_t cta = grp;
+        const uint32_t hy = (uint32_t)D.height, hc = (uint32_t)(D.height / 2), step = groups * blockDim.x;
+        for (uint32_t it = cta * blockDim.x + threadIdx.x; it < items_y; it += step) {
+            const uint32_t c = it % (uint32_t)chunks_y, r = it / (uint32_t)chunks_y;
+            level0_chunk<false>(D, src, dst, 0, r / hy, (int)(r % hy), (int)c * 16);
+        }
+        for (uint32_t it = cta * blockDim.x + threadIdx.x; it < items_c; it += step) {
+            const uint32_t c = it % (uint32_t)chunks_c, r = it / (uint32_t)chunks_c;
+            const uint32_t y = r % hc, fp = r / hc;
+            level0_chunk<false>(D, src, dst, 1 + (int)(fp & 1u), fp >> 1, (int)y, (int)c * 16);
+        }
+        return;
+    }
+    const uint32_t cta = grp * (kL01Split - 1) + role - 1, nband_ctas = groups * (kL01Split - 1);
+    const uint32_t per = (uint32_t)(nb_y + 2 * nb_c);
+    for (uint32_t it = cta; it < nbands; it += nband_ctas) {
+        const uint32_t e = it % per;
+        const int64_t f = it / per;
+        int plane, b;
+        if (e < (uint32_t)nb_y) { plane = 0; b = (int)e; }
+        else { plane = 1 + (int)((e - nb_y) / (uint32_t)nb_c); b = (int)((e - nb_y) % (uint32_t)nb_c); }
+        const int dst_h = plane ? D.lh[1] / 2 : D.lh[1];
+        const int r0 = b * band;
+        reduce_band(D, dst, inter_all, inter_all + inter_bytes, plane, f, 0, r0, min(band, dst_h - r0), src);
+    }
+}
+
 // Every row start of the source and super frames on a 16-byte boundary, 8-bit samples, and
 // no bicubic planes: the fast paths apply.
 bool vec_ok(const SuperDev &D, const void *src, const void *dst, int nframes) {
@@ -543,29 +589,51 @@ int launch_super_t(const SuperDev &D, const T *src, T *dst, int nframes, cudaStr
 // The fast paths: level 0 in two launches each (luma, then both chroma planes; the chunks inside
 // the rows, then the edge chunks), then one launch per pyramid level over bands of rows of every
 // plane and frame.
+// A level's band height: band rows of intermediates + 2 band + 4 staged source rows in about 54 KB,
+// so four 256-thread CTAs fit an SM.
+int band_rows(int row_bytes) { return std::max(1, std::min(16, ((54 << 10) / std::max(row_bytes, 1) - 4) / 3)); }
+
 int launch_super_vec(const SuperDev &D, const uint8_t *src, uint8_t *dst, int nframes, int sms, cudaStream_t stream) {
     int n = 0;
+    // level 0 and level 1 together (super_level01_kernel) when there is a level 1 of both planes and
+    // the super frames hold every level-0 row (the source then stands in for them; a `full:false`
+    // frame is shorter, and the rows it lacks read as zeros)
+    const bool fused = D.levels > 1 && D.lh[1] / 2 > 0 && D.height / 2 > 0 && D.row_y[0] + D.lh[0] <= D.y_rows &&
+                       D.row_c[0] + D.lh[0] / 2 <= D.c_rows;
+    if (fused) {
+        const int chunks_y = (int)(D.y_stride / 16), chunks_c = (int)(D.c_stride / 16);
+        const uint32_t items_y = (uint32_t)((int64_t)nframes * D.height * chunks_y);
+        const uint32_t items_c = (uint32_t)((int64_t)nframes * 2 * (D.height / 2) * chunks_c);
+        const int row_bytes = (D.lw[0] + 15) & ~15, band = band_rows(row_bytes);
+        const int nb_y = (D.lh[1] + band - 1) / band, nb_c = (D.lh[1] / 2 + band - 1) / band;
+        const uint32_t nbands = (uint32_t)((int64_t)nframes * (nb_y + 2 * nb_c));
+        super_level01_kernel<<<sms * 4, 256, (size_t)(3 * band + 4) * row_bytes, stream>>>(
+            D, src, dst, chunks_y, chunks_c, items_y, items_c, band, nb_y, nb_c, nbands, band * row_bytes);
+        n++;
+    }
     for (int pl = 0; pl < 2; pl++) {
         const int64_t S = pl ? D.c_stride : D.y_stride;
         const int h = pl ? D.height / 2 : D.height;
         if (h <= 0) continue;
         const int nplanes = pl ? 2 : 1, chunks = (int)(S / 16);
-        const uint32_t nitems = (uint32_t)((int64_t)nframes * nplanes * h * chunks);
-        const int grid = (int)std::min<int64_t>((nitems + 255) / 256, (int64_t)sms * 4);
-        super_level0_vec_kernel<<<grid, 256, 0, stream>>>(D, src, dst, pl ? 1 : 0, nplanes, h, chunks, nitems);
+        if (!fused) {
+            const uint32_t nitems = (uint32_t)((int64_t)nframes * nplanes * h * chunks);
+            const int grid = (int)std::min<int64_t>((nitems + 255) / 256, (int64_t)sms * 4);
+            super_level0_vec_kernel<<<grid, 256, 0, stream>>>(D, src, dst, pl ? 1 : 0, nplanes, h, chunks, nitems);
+            n++;
+        }
         const int w = pl ? D.width / 2 : D.width;
         const int ce = std::min(w / 16, chunks);  // chunks with x0 + 16 <= w: the vector kernel's
         const uint32_t nedge = (uint32_t)((int64_t)nframes * nplanes * ((int64_t)(h - 1) * (chunks - ce) + chunks));
         super_level0_edge_kernel<<<(int)std::min<int64_t>((nedge + 127) / 128, (int64_t)sms * 8), 128, 0, stream>>>(
             D, src, dst, pl ? 1 : 0, nplanes, h, chunks, ce, nedge);
-        n += 2;
+        n++;
     }
-    for (int lv = 0; lv + 1 < D.levels; lv++) {
+    for (int lv = fused ? 1 : 0; lv + 1 < D.levels; lv++) {
         const int dh_y = D.lh[lv + 1], dh_c = D.lh[lv + 1] / 2;
         if (dh_y <= 0) continue;
         const int row_bytes = (D.lw[lv] + 15) & ~15;  // the level's widest row (luma), 16-byte rows
-        // band rows of intermediates + 2 band + 4 staged source rows in about 54 KB: four CTAs per SM
-        const int band = std::max(1, std::min(16, ((54 << 10) / std::max(row_bytes, 1) - 4) / 3));
+        const int band = band_rows(row_bytes);
         const int nb_y = (dh_y + band - 1) / band, nb_c = (dh_c + band - 1) / band;
         const uint32_t nitems = (uint32_t)((int64_t)nframes * (nb_y + 2 * nb_c));
         const int grid = (int)std::min<int64_t>(nitems, (int64_t)sms * 4);
@@ -586,8 +654,14 @@ cudaError_t launch_super(const SuperDev &D, const uint8_t *src, uint8_t *dst, in
         return v;
     }();
     if (vec_ok(D, src, dst, nframes)) {
-        static const cudaError_t attr = cudaFuncSetAttribute(super_reduce_band_kernel,
-                                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBandSmemMax);
+        static const cudaError_t attr = [] {
+            cudaError_t e = cudaFuncSetAttribute(super_reduce_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)kBandSmemMax);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(super_level01_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kBandSmemMax);
+            return e;
+        }();
         if (attr != cudaSuccess) return attr;
         const int n = launch_super_vec(D, src, dst, nframes, sms, stream);
         if (launches) *launches += n;
