@@ -65,3 +65,15 @@ def test_f16_satd_extreme_tiles():
         assert np.array_equal(got, want)
     # a flat difference has only the DC coefficient, 16 x 255
     assert satd_int(np.full((1, 4, 4), 255, np.uint8), np.zeros((1, 4, 4), np.uint8))[0] == 16 * 255
+
+
+def test_integer_transform_is_the_oracles_satd():
+    # the transform restated above is the oracle's 4x4 SATD (its restatement of the reference's
+    # hadamard, analyse_search.rs:2305-2702), so the f16 form computes the reference's value
+    from oracle import oracle as orc
+
+    rng = np.random.default_rng(3)
+    src = rng.integers(0, 256, size=(400, 4, 4), dtype=np.uint8)
+    ref = rng.integers(0, 256, size=(400, 4, 4), dtype=np.uint8)
+    want = [orc.hadamard4((src[i].astype(int) - ref[i].astype(int)).reshape(-1)) for i in range(len(src))]
+    assert np.array_equal(satd_int(src, ref), np.array(want))
