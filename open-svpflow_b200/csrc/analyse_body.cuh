@@ -857,11 +857,7 @@ __device__ __forceinline__ int step_lanes(int G, int n, int nw) {
 // Work of one lane (`sub` of G) on one candidate: its share of the 4x4 tiles.
 // kind 0: block at (b.px, b.py); 1: the same mv on the block at (px, py) (general path);
 // 2: the block's luma pixel sum (block_luma_dc).
-#ifdef SVPF_EVAL_NOINLINE
-__device__ __noinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, int px, int py, int mvx, int mvy,
-#else
 __device__ __forceinline__ Res eval_lane(const Ctx &x, const BlkC &b, int kind, int px, int py, int mvx, int mvy,
-#endif
                                          bool chroma, int sub, int G) {
     const int TL = x.tl, TCp = x.tcp;
     int lref = 0, cref = 0;
@@ -1206,12 +1202,7 @@ __device__ __forceinline__ void stage_source(const Ctx &x, SH &s, const BlkC &b)
 // committed before), RS_NONE runs nothing.
 enum { RS_NONE, RS_ALL, RS_REFINE_ONLY, RS_BAD_ONLY };
 template <class SH>
-#ifdef SVPF_RS_NOINLINE
-__device__ __noinline__ void run_search_steps(
-#else
-__device__ __forceinline__ void run_search_steps(
-#endif
-const Ctx &x, const BlkC &b, SH &s, int &ph, int stage, int stype,
+__device__ __forceinline__ void run_search_steps(const Ctx &x, const BlkC &b, SH &s, int &ph, int stage, int stype,
                                                  int radius, int lambda, int ppx, int ppy, int own_x, int own_y,
                                                  int64_t idx, int &bad_count, int &bmx, int &bmy, unsigned &bsad,
                                                  long long &bcost) {
